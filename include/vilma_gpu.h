@@ -1,0 +1,156 @@
+/*
+ * vilma_gpu.h — C-ABI of the B200 backend for VILMA v2's viscoelastic time step.
+ *
+ * Plain C: opaque handle, plain pointers and sizes, int status (0 = ok), no
+ * exit or abort inside the library. A nonzero status leaves a message in
+ * vg_last_error(handle) (or vg_last_error(NULL) for failures before a handle
+ * exists); the Fortran shim turns it into `error stop '<msg>'`, the reference's
+ * own error convention (e.g. src/vilma_radial_fe.f90:177-187,
+ * src/vilma_timestep.f90:221-222).
+ *
+ * Array conventions (all host arrays are contiguous, Fortran-compatible):
+ *   grid fields   (nphi, nlat), phi fastest, colatitude north first
+ *                 (src/vilma_sht.f90:11-15; src/vilma_coupling.f90:678-682)
+ *   spectra       complex(c_double) of length nlm = (lmax+1)(lmax+2)/2,
+ *                 interleaved (re, im), m-major lm order with l ascending
+ *                 inside each m (the SHTns order of sht_grid_lmidx,
+ *                 src/vilma_sht.f90:349-354), orthonormal, no Condon-Shortley
+ *                 phase, m > 0 counted twice for a real field
+ *   memory state  six arrays A/B/C re/im of shape (NLAM=4, ne, nk) in the
+ *                 reference's degree-grouped slot order k (src/vilma_response.f90:
+ *                 629-648, the restart layout of src/vilma_io.f90:12-18)
+ * Times are seconds inside the library; vg_update takes years like
+ * solid_earth_update (src/vilma_coupling.f90:336-345).
+ *
+ * Threading: one host thread per handle; a handle owns one CUDA stream and all
+ * device state (the reference forbids calls from a host parallel region,
+ * src/vilma_tensor_sh.f90:153-163).
+ */
+#ifndef VILMA_GPU_H
+#define VILMA_GPU_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define VG_MAX_LAYER 16
+
+enum { VG_RHEOL_ELASTIC = 0, VG_RHEOL_MAXWELL = 1, VG_RHEOL_FLUID = 2 };
+enum { VG_SCHEME_FE = 0 };
+enum { VG_VISC3D_FP64 = 0, VG_VISC3D_SPLIT_TC = 1 };
+
+/* The &vilma namelist record restricted to what the time step reads
+ * (src/vilma_params.f90:26-205). Defaults: vg_params_default. */
+typedef struct vg_params {
+  /* Gauss grid (src/vilma_params.f90:45-48): nlat/nphi must be given. */
+  int lmax, nlat, nphi;
+  /* layered earth, surface-first (earth = "custom", src/vilma_earth_structure.f90:82-116) */
+  int n_layer;
+  double r_earth;
+  double r_bot[VG_MAX_LAYER], r_top[VG_MAX_LAYER];
+  double rho[VG_MAX_LAYER], mu[VG_MAX_LAYER], eta[VG_MAX_LAYER];
+  int rheology[VG_MAX_LAYER];
+  /* radial elements per layer; all zero => the reference depth-target rule
+   * (src/vilma_radial_fe.f90:43-50, 140-224). No reference counterpart. */
+  int ne_layer[VG_MAX_LAYER];
+  /* response (src/vilma_params.f90:65-70, 135-158) */
+  int scheme;        /* VG_SCHEME_FE ("fe") */
+  int deg1_cm;       /* 1: deg1_frame = "cm", 0: "cf" */
+  double skip_tol;   /* drift-solve skip gate, src/vilma_response.f90:88-93 */
+  double visc3d_tol; /* 1-D/3-D element split [dex] */
+  double dt_init;    /* [s]; 0 => 1 kyr (src/vilma_coupling.f90:258) */
+  /* explicit stepper (src/vilma_timestep.f90:51-61) */
+  double cfl, guard_growth, dt_min, dt_max;
+  /* sea-level equation (src/vilma_params.f90:73-78; src/vilma_sle.f90:57-98) */
+  int sle_n_outer, sle_n_inner;
+  double sle_tol;
+  int sle_fixed_ocean, sle_subgrid, sle_warm_start;
+  /* rotational feedback (src/vilma_params.f90:96); not implemented: must be 0 */
+  int rotation;
+  /* precision of the 3-D Legendre contractions (no reference counterpart) */
+  int visc3d_precision;
+} vg_params;
+
+typedef struct vg_info {
+  int lmax, nlat, nphi, nlm, nr, ne, ndof, nk, ne3d;
+  int n_sub_last;         /* sub-steps taken by the last vg_update */
+  long long n_accept, n_reject, n_solve, n_drift_solved;
+  double time_yr;         /* model time [yr] */
+  double worst_mass_resid;
+  double bsl;             /* barystatic sea level diagnostic [m] */
+  int n_outer_last, n_inner_last, n_coast_flip_last;
+} vg_info;
+
+typedef struct vg_handle vg_handle;
+
+/* Fill p with the reference defaults (src/vilma_params.f90:26-205) and the
+ * 4-layer synthetic earth used by the benchmarks of this backend. */
+int vg_params_default(vg_params* p);
+
+/* solid_earth_init, build part (src/vilma_coupling.f90:144-156, 252-318):
+ * Gauss grid, radial mesh, per-degree operators assembled and factored on the
+ * device, unit-load gains, zero memory. Replaces build_sht + build_solver. */
+int vg_create(const vg_params* p, vg_handle** out);
+
+/* solid_earth_init, data part: reference bed z_bed_eq and reference ice
+ * h_ice_eq on the Gauss grid (the `grid` argument absent: data already on
+ * Gauss, src/vilma_coupling.f90:166-170), optional current ice h_ice_init
+ * (NULL => h_ice_eq). Sets rsl = 0, z_bed = z_bed_eq, C = C0. */
+int vg_set_reference(vg_handle* h, const double* z_bed_eq, const double* h_ice_eq,
+                     const double* h_ice_init);
+
+/* Laterally varying viscosity: log10 viscosity perturbation per element on
+ * the Gauss grid, (nphi, nlat, ne) (response_enable_lateral_visc,
+ * src/vilma_response.f90:994-1053). */
+int vg_enable_visc3d(vg_handle* h, const double* pert);
+
+/* solid_earth_update (src/vilma_coupling.f90:336-437) without rotation:
+ * advance by dt_yr years with the ice linearly interpolated from the carried
+ * ice to h_ice (stepper_advance, src/vilma_timestep.f90:79-227). h_ice is a
+ * host array. */
+int vg_update(vg_handle* h, const double* h_ice, double dt_yr);
+/* Same, with h_ice a device pointer (nphi*nlat doubles) on the handle's GPU. */
+int vg_update_device(vg_handle* h, const double* d_h_ice, double dt_yr);
+
+/* Outputs of the coupling record (se%rsl, se%z_bed, se%gg%C, se%sigma_lm,
+ * src/vilma_coupling.f90:71-140). Any pointer may be NULL. */
+int vg_get_fields(vg_handle* h, double* rsl, double* z_bed, double* C, double* sigma_lm);
+/* Device pointer of the rsl field (read-only, valid until vg_destroy). */
+int vg_rsl_device(vg_handle* h, const double** d_rsl);
+int vg_get_info(vg_handle* h, vg_info* info);
+
+/* Response-level operators (src/vilma_response.f90:43-52, 266-319) for a run
+ * without the sea-level equation (bench_visc3d style): begin_step freezes the
+ * drift from the current memory; apply returns u_lm, n_lm for a load sigma_lm;
+ * advance commits the forward-Euler memory update with sigma_lm and adds dt. */
+int vg_response_set_dt(vg_handle* h, double dt_s);
+int vg_response_begin_step(vg_handle* h);
+int vg_response_apply(vg_handle* h, const double* sigma_lm, double* u_lm, double* n_lm);
+int vg_response_advance(vg_handle* h, const double* sigma_lm);
+/* elastic per-degree gains gu, gn, gv (0..lmax) (src/vilma_response.f90:603-627) */
+int vg_get_gains(vg_handle* h, double* gu, double* gn, double* gv);
+/* surface drift dUa, dFa, dVa (complex, nk each, interleaved) of the last begin_step */
+int vg_get_drift(vg_handle* h, double* dUa, double* dFa, double* dVa);
+
+/* Prognostic state in the restart layout (src/vilma_io.f90:12-18, 414-569):
+ * six arrays of NLAM*ne*nk doubles (A re, A im, B re, B im, C re, C im) and the
+ * model time [s]. */
+int vg_get_state(vg_handle* h, double* Are, double* Aim, double* Bre, double* Bim,
+                 double* Cre, double* Cim, double* time_s);
+int vg_set_state(vg_handle* h, const double* Are, const double* Aim, const double* Bre,
+                 const double* Bim, const double* Cre, const double* Cim, double time_s);
+
+/* Gauss-grid transforms on the device (sht_grid_synthesis / _analysis,
+ * src/vilma_sht.f90:204-226), host arrays in and out. */
+int vg_sht_analysis(vg_handle* h, const double* f, double* q_lm);
+int vg_sht_synthesis(vg_handle* h, const double* q_lm, double* f);
+
+int vg_destroy(vg_handle* h);
+const char* vg_last_error(const vg_handle* h);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* VILMA_GPU_H */

@@ -1,0 +1,231 @@
+"""ctypes binding of the CPU oracle (liboracle.so) — test infrastructure only.
+
+Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg use this;
+the product library never does. The C API mirrors include/vilma_gpu.h with an
+`orc_` prefix, so both sides are driven by the same calls.
+"""
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+from fastearth3d_b200.abi import VgInfo, VgParams
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB = os.path.join(_HERE, "liboracle.so")
+_lib = None
+
+_P = C.POINTER(C.c_double)
+_VP = C.c_void_p
+
+
+def build():
+    subprocess.run(["make", "-s", "-C", _HERE], check=True)
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(_LIB):
+            build()
+        L = C.CDLL(_LIB)
+        for name, args in [
+            ("orc_params_default", [C.POINTER(VgParams)]),
+            ("orc_create", [C.POINTER(VgParams), C.POINTER(_VP)]),
+            ("orc_destroy", [_VP]),
+            ("orc_set_reference", [_VP, _P, _P, _P]),
+            ("orc_enable_visc3d", [_VP, _P]),
+            ("orc_update", [_VP, _P, C.c_double]),
+            ("orc_get_fields", [_VP, _P, _P, _P, _P]),
+            ("orc_get_info", [_VP, C.POINTER(VgInfo)]),
+            ("orc_response_set_dt", [_VP, C.c_double]),
+            ("orc_response_begin_step", [_VP]),
+            ("orc_response_apply", [_VP, _P, _P, _P]),
+            ("orc_response_advance", [_VP, _P]),
+            ("orc_get_gains", [_VP, _P, _P, _P]),
+            ("orc_get_drift", [_VP, _P, _P, _P]),
+            ("orc_get_state", [_VP, _P, _P, _P, _P, _P, _P, _P]),
+            ("orc_set_state", [_VP, _P, _P, _P, _P, _P, _P, C.c_double]),
+            ("orc_sht_analysis", [_VP, _P, _P]),
+            ("orc_sht_synthesis", [_VP, _P, _P]),
+            ("orc_love_numbers", [C.POINTER(VgParams), C.c_int, C.c_int, _P, _P, _P]),
+            ("orc_band_dense_solve", [C.c_int, _P, _P, _P]),
+            ("orc_dense_operator", [C.POINTER(VgParams), C.c_int, C.c_int, _P, C.POINTER(C.c_int)]),
+            ("orc_tensor_synth", [_VP, _P, _P]),
+            ("orc_tensor_analysis", [_VP, _P, _P]),
+            ("orc_grid", [_VP, _P, _P]),
+            ("orc_mesh", [_VP, _P, C.POINTER(C.c_int)]),
+        ]:
+            f = getattr(L, name)
+            f.argtypes = args
+            f.restype = C.c_int
+        L.orc_last_error.argtypes = [_VP]
+        L.orc_last_error.restype = C.c_char_p
+        L.orc_surface_integral.argtypes = [_VP, _P]
+        L.orc_surface_integral.restype = C.c_double
+        _lib = L
+    return _lib
+
+
+def ptr(a):
+    if a is None:
+        return None
+    assert a.dtype == np.float64 and a.flags.c_contiguous
+    return a.ctypes.data_as(_P)
+
+
+def default_params():
+    p = VgParams()
+    lib().orc_params_default(C.byref(p))
+    return p
+
+
+def _check(rc, h=None):
+    if rc != 0:
+        raise RuntimeError(lib().orc_last_error(h).decode())
+
+
+def love_numbers(p, jmin, jmax):
+    n = jmax - jmin + 1
+    h, l, k = np.zeros(n), np.zeros(n), np.zeros(n)
+    _check(lib().orc_love_numbers(C.byref(p), jmin, jmax, ptr(h), ptr(l), ptr(k)))
+    return h, l, k
+
+
+def band_dense_solve(A, b):
+    A = np.asfortranarray(A, dtype=np.float64)
+    n = A.shape[0]
+    flat = np.ascontiguousarray(A.T.reshape(-1))  # column-major flattening
+    x = np.zeros(n)
+    _check(lib().orc_band_dense_solve(n, ptr(flat), ptr(np.ascontiguousarray(b, dtype=np.float64)), ptr(x)))
+    return x
+
+
+def dense_operator(p, j, with_uniq=True):
+    nd = C.c_int(0)
+    lib().orc_dense_operator(C.byref(p), j, int(with_uniq), None, C.byref(nd))
+    flat = np.zeros(nd.value * nd.value)
+    lib().orc_dense_operator(C.byref(p), j, int(with_uniq), ptr(flat), C.byref(nd))
+    return flat.reshape(nd.value, nd.value).T  # column-major -> A[i, k]
+
+
+class Oracle:
+    """One oracle model instance (solid_earth_init/update restated on the CPU)."""
+
+    def __init__(self, p):
+        self.p = p
+        h = _VP()
+        _check(lib().orc_create(C.byref(p), C.byref(h)))
+        self.h = h
+        info = self.info()
+        self.nlm, self.nk, self.ne, self.nr = info.nlm, info.nk, info.ne, info.nr
+        self.ng = p.nphi * p.nlat
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            lib().orc_destroy(self.h)
+            self.h = None
+
+    def _c(self, rc):
+        _check(rc, self.h)
+
+    def info(self):
+        i = VgInfo()
+        self._c(lib().orc_get_info(self.h, C.byref(i)))
+        return i
+
+    def set_reference(self, z_bed_eq, h_ice_eq, h_ice_init=None):
+        self._c(lib().orc_set_reference(self.h, ptr(z_bed_eq), ptr(h_ice_eq), ptr(h_ice_init)))
+
+    def enable_visc3d(self, pert):
+        self._c(lib().orc_enable_visc3d(self.h, ptr(np.ascontiguousarray(pert, dtype=np.float64))))
+
+    def update(self, h_ice, dt_yr):
+        self._c(lib().orc_update(self.h, ptr(np.ascontiguousarray(h_ice, dtype=np.float64)), dt_yr))
+
+    def fields(self):
+        rsl, zb, Cf = np.zeros(self.ng), np.zeros(self.ng), np.zeros(self.ng)
+        sig = np.zeros(2 * self.nlm)
+        self._c(lib().orc_get_fields(self.h, ptr(rsl), ptr(zb), ptr(Cf), ptr(sig)))
+        return rsl, zb, Cf, sig[0::2] + 1j * sig[1::2]
+
+    def state(self):
+        n = 4 * self.ne * self.nk
+        arrs = [np.zeros(n) for _ in range(6)]
+        t = C.c_double(0)
+        self._c(lib().orc_get_state(self.h, *[ptr(a) for a in arrs], C.byref(t)))
+        return arrs, t.value
+
+    def set_state(self, arrs, t):
+        arrs = [np.ascontiguousarray(a, dtype=np.float64) for a in arrs]
+        self._c(lib().orc_set_state(self.h, *[ptr(a) for a in arrs], t))
+
+    def set_dt(self, dt_s):
+        self._c(lib().orc_response_set_dt(self.h, dt_s))
+
+    def begin_step(self):
+        self._c(lib().orc_response_begin_step(self.h))
+
+    def apply(self, sigma):
+        s = np.zeros(2 * self.nlm)
+        s[0::2], s[1::2] = sigma.real, sigma.imag
+        u, n = np.zeros(2 * self.nlm), np.zeros(2 * self.nlm)
+        self._c(lib().orc_response_apply(self.h, ptr(s), ptr(u), ptr(n)))
+        return u[0::2] + 1j * u[1::2], n[0::2] + 1j * n[1::2]
+
+    def advance(self, sigma):
+        s = np.zeros(2 * self.nlm)
+        s[0::2], s[1::2] = sigma.real, sigma.imag
+        self._c(lib().orc_response_advance(self.h, ptr(s)))
+
+    def gains(self):
+        L = self.p.lmax + 1
+        gu, gn, gv = np.zeros(L), np.zeros(L), np.zeros(L)
+        self._c(lib().orc_get_gains(self.h, ptr(gu), ptr(gn), ptr(gv)))
+        return gu, gn, gv
+
+    def drift(self):
+        a = [np.zeros(2 * self.nk) for _ in range(3)]
+        self._c(lib().orc_get_drift(self.h, *[ptr(x) for x in a]))
+        return [x[0::2] + 1j * x[1::2] for x in a]
+
+    def analysis(self, f):
+        q = np.zeros(2 * self.nlm)
+        self._c(lib().orc_sht_analysis(self.h, ptr(np.ascontiguousarray(f, dtype=np.float64)), ptr(q)))
+        return q[0::2] + 1j * q[1::2]
+
+    def synthesis(self, q):
+        s = np.zeros(2 * self.nlm)
+        s[0::2], s[1::2] = q.real, q.imag
+        f = np.zeros(self.ng)
+        self._c(lib().orc_sht_synthesis(self.h, ptr(s), ptr(f)))
+        return f
+
+    def tensor_synth(self, c):
+        """c: (4, nlm) complex -> dyad (6, ng)"""
+        s = np.zeros(2 * 4 * self.nlm)
+        cf = np.ascontiguousarray(c).reshape(-1)
+        s[0::2], s[1::2] = cf.real, cf.imag
+        d = np.zeros(6 * self.ng)
+        self._c(lib().orc_tensor_synth(self.h, ptr(s), ptr(d)))
+        return d.reshape(6, self.ng)
+
+    def tensor_analysis(self, dyad):
+        c = np.zeros(2 * 4 * self.nlm)
+        self._c(lib().orc_tensor_analysis(self.h, ptr(np.ascontiguousarray(dyad, dtype=np.float64).reshape(-1)), ptr(c)))
+        return (c[0::2] + 1j * c[1::2]).reshape(4, self.nlm)
+
+    def grid(self):
+        colat, w = np.zeros(self.p.nlat), np.zeros(self.p.nlat)
+        self._c(lib().orc_grid(self.h, ptr(colat), ptr(w)))
+        return colat, w
+
+    def surface_integral(self, f):
+        return lib().orc_surface_integral(self.h, ptr(np.ascontiguousarray(f, dtype=np.float64)))
+
+    def mesh(self):
+        r = np.zeros(self.nr)
+        lay = (C.c_int * self.ne)()
+        self._c(lib().orc_mesh(self.h, ptr(r), lay))
+        return r, np.array(lay[:])

@@ -1,0 +1,422 @@
+// CPU ORACLE — test infrastructure only (see orc.hpp).
+// The coupling driver (solid_earth_init/update, src/vilma_coupling.f90) and a
+// C API mirroring include/vilma_gpu.h with an `orc_` prefix, so the tests can
+// drive the oracle and the CUDA library through the same calls.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <exception>
+#include <stdexcept>
+#include <string>
+
+#include "../include/vilma_gpu.h"
+#include "orc.hpp"
+
+using namespace orc;
+
+struct OrcHandle {
+  vg_params p;
+  Earth earth;
+  Mesh mesh;
+  Sht sht;
+  Response R;
+  SleSolver sle;
+  Stepper st;
+  std::vector<double> z_bed_eq, h_ice_eq, h_ice, rsl, z_bed, C, C0;
+  std::vector<cplx> sigma_lm;
+  double time_yr = 0.0, bsl = 0.0;
+  SleResult last;
+  std::string err;
+};
+
+static std::string g_err;
+
+extern "C" {
+
+int orc_params_default(vg_params* p) {
+  std::memset(p, 0, sizeof(*p));
+  const double km = 1e3;
+  p->lmax = 16;
+  p->nlat = 17;
+  p->nphi = 34;
+  p->n_layer = 4;
+  p->r_earth = 6371.0 * km;
+  const double rb[4] = {6301.0 * km, 5701.0 * km, 3480.0 * km, 0.0};
+  const double rt[4] = {6371.0 * km, 6301.0 * km, 5701.0 * km, 3480.0 * km};
+  const double rho[4] = {3300.0, 3450.0, 4900.0, 10900.0};
+  const double mu[4] = {0.7e11, 0.9e11, 2.0e11, 0.0};
+  const double eta[4] = {1e300, 5e20, 2e21, 0.0};
+  const int rh[4] = {VG_RHEOL_ELASTIC, VG_RHEOL_MAXWELL, VG_RHEOL_MAXWELL, VG_RHEOL_FLUID};
+  for (int i = 0; i < 4; ++i) {
+    p->r_bot[i] = rb[i];
+    p->r_top[i] = rt[i];
+    p->rho[i] = rho[i];
+    p->mu[i] = mu[i];
+    p->eta[i] = eta[i];
+    p->rheology[i] = rh[i];
+  }
+  p->scheme = VG_SCHEME_FE;
+  p->deg1_cm = 1;
+  p->skip_tol = 1e-4;
+  p->visc3d_tol = 1e-3;
+  p->dt_init = 0.0;
+  p->cfl = 1.0;
+  p->guard_growth = 1e3;
+  p->dt_min = 0.0;
+  p->dt_max = 1.7976931348623157e308;
+  p->sle_n_outer = 3;
+  p->sle_n_inner = 20;
+  p->sle_tol = 1e-7;
+  p->sle_fixed_ocean = 0;
+  p->sle_subgrid = 1;
+  p->sle_warm_start = 1;
+  p->rotation = 0;
+  p->visc3d_precision = VG_VISC3D_FP64;
+  return 0;
+}
+
+int orc_create(const vg_params* p, OrcHandle** out) {
+  try {
+    if (p->rotation) throw std::runtime_error("rotation is not part of the oracle");
+    OrcHandle* h = new OrcHandle();
+    h->p = *p;
+    h->earth.r_earth = p->r_earth;
+    for (int i = 0; i < p->n_layer; ++i) {
+      Layer L;
+      L.r_bot = p->r_bot[i];
+      L.r_top = p->r_top[i];
+      L.rho = p->rho[i];
+      L.mu = p->mu[i];
+      L.eta = p->eta[i];
+      L.rheology = p->rheology[i];
+      h->earth.layers.push_back(L);
+    }
+    h->mesh = radial_mesh_build(h->earth, p->ne_layer);
+    sht_init(h->sht, p->lmax, p->nlat, p->nphi);
+    double dt0 = p->dt_init > 0.0 ? p->dt_init : KYR;
+    h->R.deg1_cm = p->deg1_cm != 0;
+    h->R.skip_tol = p->skip_tol;
+    h->R.visc3d_tol = p->visc3d_tol;
+    response_init_ve(h->R, h->earth, h->mesh, h->sht, dt0);
+    h->sle.n_outer = p->sle_n_outer;
+    h->sle.n_inner = p->sle_n_inner;
+    h->sle.tol = p->sle_tol;
+    h->sle.fixed_ocean = p->sle_fixed_ocean != 0;
+    h->sle.subgrid = p->sle_subgrid != 0;
+    h->sle.warm_start = p->sle_warm_start != 0;
+    h->st.cfl = p->cfl;
+    h->st.guard_growth = p->guard_growth;
+    h->st.dt_min = p->dt_min;
+    h->st.dt_max = p->dt_max;
+    h->sigma_lm.assign(h->sht.nlm, 0.0);
+    *out = h;
+    return 0;
+  } catch (const std::exception& ex) {
+    g_err = ex.what();
+    return 1;
+  }
+}
+
+int orc_destroy(OrcHandle* h) {
+  delete h;
+  return 0;
+}
+
+const char* orc_last_error(const OrcHandle* h) { return h ? h->err.c_str() : g_err.c_str(); }
+
+int orc_set_reference(OrcHandle* h, const double* z_bed_eq, const double* h_ice_eq, const double* h_ice_init) {
+  const int ng = h->sht.nphi * h->sht.nlat;
+  h->z_bed_eq.assign(z_bed_eq, z_bed_eq + ng);
+  h->h_ice_eq.assign(h_ice_eq, h_ice_eq + ng);
+  h->h_ice.assign(h_ice_init ? h_ice_init : h_ice_eq, (h_ice_init ? h_ice_init : h_ice_eq) + ng);
+  h->rsl.assign(ng, 0.0);
+  h->z_bed = h->z_bed_eq;
+  h->C0.assign(ng, 0.0);
+  ocean_function(ng, h->z_bed_eq.data(), h->h_ice_eq.data(), h->C0.data());
+  h->C = h->C0;
+  return 0;
+}
+
+int orc_enable_visc3d(OrcHandle* h, const double* pert) {
+  sht_calibrate_n6(h->sht);
+  response_enable_lateral_visc(h->R, h->sht, pert);
+  return 0;
+}
+
+// vilma_coupling.f90:572-597 update_bsl
+static void update_bsl(OrcHandle* h) {
+  const int ng = h->sht.nphi * h->sht.nlat;
+  double c_int = sht_surface_integral(h->sht, h->C.data());
+  if (c_int > 0.0) {
+    std::vector<double> t(ng);
+    for (int i = 0; i < ng; ++i) t[i] = h->h_ice[i] * (1.0 - h->C[i]) - h->h_ice_eq[i] * (1.0 - h->C0[i]);
+    h->bsl = -(RHO_ICE / RHO_WATER) * sht_surface_integral(h->sht, t.data()) / c_int;
+  } else {
+    h->bsl = 0.0;
+  }
+}
+
+// vilma_coupling.f90:336-437 solid_earth_update (rotation off)
+int orc_update(OrcHandle* h, const double* h_ice, double dt_yr) {
+  const int ng = h->sht.nphi * h->sht.nlat;
+  double dt = dt_yr * SEC_PER_YEAR;
+  double t0 = h->time_yr * SEC_PER_YEAR, t1 = t0 + dt;
+  std::vector<double> ice_new(h_ice, h_ice + ng);
+  int rc = stepper_advance(h->st, h->sht, h->R, h->sle, h->z_bed_eq.data(), h->h_ice.data(), ice_new.data(),
+                           h->h_ice_eq.data(), t0, t1, h->rsl.data(), h->C.data(), nullptr, h->sigma_lm.data());
+  if (rc) {
+    h->err = "vilma_timestep: explicit guard sub-step collapsed (viscosity too stiff for FE)";
+    return rc;
+  }
+  h->h_ice = ice_new;
+  for (int i = 0; i < ng; ++i) h->z_bed[i] = h->z_bed_eq[i] - h->rsl[i];
+  h->time_yr += dt_yr;
+  update_bsl(h);
+  return 0;
+}
+
+int orc_get_fields(OrcHandle* h, double* rsl, double* z_bed, double* C, double* sigma_lm) {
+  const int ng = h->sht.nphi * h->sht.nlat;
+  if (rsl) std::copy(h->rsl.begin(), h->rsl.end(), rsl);
+  if (z_bed) std::copy(h->z_bed.begin(), h->z_bed.end(), z_bed);
+  if (C) std::copy(h->C.begin(), h->C.begin() + ng, C);
+  if (sigma_lm)
+    for (int lm = 0; lm < h->sht.nlm; ++lm) {
+      sigma_lm[2 * lm] = h->sigma_lm[lm].real();
+      sigma_lm[2 * lm + 1] = h->sigma_lm[lm].imag();
+    }
+  return 0;
+}
+
+int orc_get_info(OrcHandle* h, vg_info* info) {
+  std::memset(info, 0, sizeof(*info));
+  info->lmax = h->sht.lmax;
+  info->nlat = h->sht.nlat;
+  info->nphi = h->sht.nphi;
+  info->nlm = h->sht.nlm;
+  info->nr = h->R.nr;
+  info->ne = h->R.ne;
+  info->ndof = h->R.ndof;
+  info->nk = h->R.nk;
+  info->ne3d = h->R.ne3d;
+  info->n_sub_last = h->st.n_sub_last;
+  info->n_accept = h->st.n_accept;
+  info->n_reject = h->st.n_reject;
+  info->n_solve = h->st.n_solve;
+  info->n_drift_solved = h->R.n_solved;
+  info->time_yr = h->time_yr;
+  info->worst_mass_resid = h->st.worst_mass_resid;
+  info->bsl = h->bsl;
+  return 0;
+}
+
+int orc_response_set_dt(OrcHandle* h, double dt_s) {
+  response_set_dt(h->R, dt_s);
+  return 0;
+}
+int orc_response_begin_step(OrcHandle* h) {
+  response_begin_step(h->R, h->sht);
+  return 0;
+}
+int orc_response_apply(OrcHandle* h, const double* sigma_lm, double* u_lm, double* n_lm) {
+  const int nlm = h->sht.nlm;
+  std::vector<cplx> s(nlm), u(nlm), n(nlm);
+  for (int lm = 0; lm < nlm; ++lm) s[lm] = cplx(sigma_lm[2 * lm], sigma_lm[2 * lm + 1]);
+  response_apply(h->R, h->sht, s.data(), u.data(), n.data());
+  for (int lm = 0; lm < nlm; ++lm) {
+    u_lm[2 * lm] = u[lm].real();
+    u_lm[2 * lm + 1] = u[lm].imag();
+    n_lm[2 * lm] = n[lm].real();
+    n_lm[2 * lm + 1] = n[lm].imag();
+  }
+  return 0;
+}
+int orc_response_advance(OrcHandle* h, const double* sigma_lm) {
+  const int nlm = h->sht.nlm;
+  std::vector<cplx> s(nlm);
+  for (int lm = 0; lm < nlm; ++lm) s[lm] = cplx(sigma_lm[2 * lm], sigma_lm[2 * lm + 1]);
+  response_advance(h->R, h->sht, s.data());
+  h->R.time += h->R.dt;
+  return 0;
+}
+int orc_get_gains(OrcHandle* h, double* gu, double* gn, double* gv) {
+  for (int l = 0; l <= h->R.lmax; ++l) {
+    if (gu) gu[l] = h->R.gu[l];
+    if (gn) gn[l] = h->R.gn[l];
+    if (gv) gv[l] = h->R.gv[l];
+  }
+  return 0;
+}
+int orc_get_drift(OrcHandle* h, double* dUa, double* dFa, double* dVa) {
+  for (int k = 0; k < h->R.nk; ++k) {
+    if (dUa) {
+      dUa[2 * k] = h->R.dUa[k].real();
+      dUa[2 * k + 1] = h->R.dUa[k].imag();
+    }
+    if (dFa) {
+      dFa[2 * k] = h->R.dFa[k].real();
+      dFa[2 * k + 1] = h->R.dFa[k].imag();
+    }
+    if (dVa) {
+      dVa[2 * k] = h->R.dVa[k].real();
+      dVa[2 * k + 1] = h->R.dVa[k].imag();
+    }
+  }
+  return 0;
+}
+// state in the reference (NLAM, ne, nk) layout == the oracle's [k][e][lam]
+int orc_get_state(OrcHandle* h, double* Are, double* Aim, double* Bre, double* Bim, double* Cre, double* Cim,
+                  double* time_s) {
+  std::copy(h->R.Are.begin(), h->R.Are.end(), Are);
+  std::copy(h->R.Aim.begin(), h->R.Aim.end(), Aim);
+  std::copy(h->R.Bre.begin(), h->R.Bre.end(), Bre);
+  std::copy(h->R.Bim.begin(), h->R.Bim.end(), Bim);
+  std::copy(h->R.Cre.begin(), h->R.Cre.end(), Cre);
+  std::copy(h->R.Cim.begin(), h->R.Cim.end(), Cim);
+  if (time_s) *time_s = h->R.time;
+  return 0;
+}
+int orc_set_state(OrcHandle* h, const double* Are, const double* Aim, const double* Bre, const double* Bim,
+                  const double* Cre, const double* Cim, double time_s) {
+  size_t n = h->R.Are.size();
+  h->R.Are.assign(Are, Are + n);
+  h->R.Aim.assign(Aim, Aim + n);
+  h->R.Bre.assign(Bre, Bre + n);
+  h->R.Bim.assign(Bim, Bim + n);
+  h->R.Cre.assign(Cre, Cre + n);
+  h->R.Cim.assign(Cim, Cim + n);
+  h->R.time = time_s;
+  return 0;
+}
+int orc_sht_analysis(OrcHandle* h, const double* f, double* q) {
+  std::vector<cplx> c(h->sht.nlm);
+  sht_analysis(h->sht, f, c.data());
+  for (int lm = 0; lm < h->sht.nlm; ++lm) {
+    q[2 * lm] = c[lm].real();
+    q[2 * lm + 1] = c[lm].imag();
+  }
+  return 0;
+}
+int orc_sht_synthesis(OrcHandle* h, const double* q, double* f) {
+  std::vector<cplx> c(h->sht.nlm);
+  for (int lm = 0; lm < h->sht.nlm; ++lm) c[lm] = cplx(q[2 * lm], q[2 * lm + 1]);
+  sht_synth(h->sht, c.data(), f);
+  return 0;
+}
+
+// ---- stand-alone pieces for the known-answer tests -----------------------
+// Elastic loading Love numbers of a layered earth at degree j
+// (test_benchmark_love.f90 path: mesh, assemble, unit-load solve, loading_love).
+int orc_love_numbers(const vg_params* p, int jmin, int jmax, double* h_out, double* l_out, double* k_out) {
+  try {
+    Earth e;
+    e.r_earth = p->r_earth;
+    for (int i = 0; i < p->n_layer; ++i) {
+      Layer L;
+      L.r_bot = p->r_bot[i];
+      L.r_top = p->r_top[i];
+      L.rho = p->rho[i];
+      L.mu = p->mu[i];
+      L.eta = p->eta[i];
+      L.rheology = p->rheology[i];
+      e.layers.push_back(L);
+    }
+    Mesh m = radial_mesh_build(e, p->ne_layer);
+#pragma omp parallel for schedule(dynamic)
+    for (int j = jmin; j <= jmax; ++j) {
+      RadialOp op;
+      radial_operator_assemble(op, e, m, j);
+      std::vector<double> b(op.ndof), x(op.ndof);
+      radial_operator_load_rhs(op, 1.0, b.data());
+      radial_operator_solve_vec(op, b.data(), x.data(), nullptr);
+      double hh, ll, kk;
+      loading_love(e, j, 1.0, x[idx_u(op.nr - 1)], x[idx_v(op.nr - 1)], x[idx_f(op.nr - 1)], hh, ll, kk);
+      h_out[j - jmin] = hh;
+      l_out[j - jmin] = ll;
+      k_out[j - jmin] = kk;
+    }
+    return 0;
+  } catch (const std::exception& ex) {
+    g_err = ex.what();
+    return 1;
+  }
+}
+
+// Band LU of a dense n x n matrix (column-major) through the band machinery,
+// solved for one RHS (test_band.f90 path).
+int orc_band_dense_solve(int n, const double* A, const double* b, double* x) {
+  std::vector<int> rows, cols;
+  std::vector<double> vals;
+  for (int k = 0; k < n; ++k)
+    for (int i = 0; i < n; ++i)
+      if (A[(size_t)k * n + i] != 0.0) {
+        rows.push_back(i + 1);
+        cols.push_back(k + 1);
+        vals.push_back(A[(size_t)k * n + i]);
+      }
+  Band B;
+  if (!band_build(B, n, rows, cols, vals)) return 2;
+  for (int i = 0; i < n; ++i) x[i] = b[i];
+  band_solve(B, x);
+  return 0;
+}
+
+// Dense per-degree operator (with the E_uniq term for j = 1), for the symmetry check.
+int orc_dense_operator(const vg_params* p, int j, int with_uniq, double* A, int* nd_out) {
+  Earth e;
+  e.r_earth = p->r_earth;
+  for (int i = 0; i < p->n_layer; ++i) {
+    Layer L;
+    L.r_bot = p->r_bot[i];
+    L.r_top = p->r_top[i];
+    L.rho = p->rho[i];
+    L.mu = p->mu[i];
+    L.eta = p->eta[i];
+    L.rheology = p->rheology[i];
+    e.layers.push_back(L);
+  }
+  Mesh m = radial_mesh_build(e, p->ne_layer);
+  int nd = ndof_of(m.nr);
+  *nd_out = nd;
+  if (A) {
+    std::vector<double> D = build_dense_operator(e, m, j, with_uniq != 0);
+    std::copy(D.begin(), D.end(), A);
+  }
+  return 0;
+}
+
+// tensor synth/analysis round trip on the handle's grid (test_tensor_sh path)
+int orc_tensor_synth(OrcHandle* h, const double* c /* 4*nlm complex, channel-major */, double* dyad) {
+  sht_calibrate_n6(h->sht);
+  std::vector<cplx> cc((size_t)4 * h->sht.nlm);
+  for (size_t t = 0; t < cc.size(); ++t) cc[t] = cplx(c[2 * t], c[2 * t + 1]);
+  tensor_synth(h->sht, cc.data(), dyad);
+  return 0;
+}
+int orc_tensor_analysis(OrcHandle* h, const double* dyad, double* c) {
+  sht_calibrate_n6(h->sht);
+  std::vector<cplx> cc((size_t)4 * h->sht.nlm);
+  tensor_analysis(h->sht, dyad, cc.data());
+  for (size_t t = 0; t < cc.size(); ++t) {
+    c[2 * t] = cc[t].real();
+    c[2 * t + 1] = cc[t].imag();
+  }
+  return 0;
+}
+int orc_grid(OrcHandle* h, double* colat, double* wts) {
+  for (int j = 0; j < h->sht.nlat; ++j) {
+    if (colat) colat[j] = h->sht.colat[j];
+    if (wts) wts[j] = h->sht.wts[j];
+  }
+  return 0;
+}
+double orc_surface_integral(OrcHandle* h, const double* f) { return sht_surface_integral(h->sht, f); }
+int orc_mesh(OrcHandle* h, double* r, int* elem_layer) {
+  for (int i = 0; i < h->mesh.nr; ++i)
+    if (r) r[i] = h->mesh.r[i];
+  for (int e = 0; e < h->mesh.ne; ++e)
+    if (elem_layer) elem_layer[e] = h->mesh.elem_layer[e];
+  return 0;
+}
+
+}  // extern "C"

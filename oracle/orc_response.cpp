@@ -1,0 +1,459 @@
+// CPU ORACLE — test infrastructure only (see orc.hpp).
+// Viscoelastic field driver: per-degree operators and unit-load response,
+// Maxwell memory kernel, drift solve with the skip gate, affine apply, the
+// forward-Euler memory advance, and the pseudo-spectral 3-D advance.
+#include <algorithm>
+#include <cmath>
+#include <stdexcept>
+
+#include "orc.hpp"
+
+namespace orc {
+
+// vilma_viscoelastic.f90:329-359 strain_coeffs
+static inline void strain_coeffs(double u1, double u2, double v1, double v2, double Jr, double a[4],
+                                 double b[4], double c[4]) {
+  a[0] = -u1 + u2;
+  b[0] = 0.0;
+  c[0] = 0.0;
+  a[1] = -v1 + v2;
+  b[1] = u1 - v1;
+  c[1] = u2 - v2;
+  a[2] = 0.0;
+  b[2] = -u1 / Jr + 0.5 * v1;
+  c[2] = -u2 / Jr + 0.5 * v2;
+  a[3] = 0.0;
+  b[3] = 0.5 * v1;
+  c[3] = 0.5 * v2;
+  if (Jr <= 2.0) {
+    b[3] = 0.0;
+    c[3] = 0.0;
+  }
+}
+
+// vilma_viscoelastic.f90:361-371 ve_strain_constants
+static void ve_strain_constants(double Jr, double norm[4], double sa[16], double sb[16], double sc[16]) {
+  norm[0] = 1.0;
+  norm[1] = 0.5 * Jr;
+  norm[2] = 2.0 * Jr * Jr;
+  norm[3] = 2.0 * Jr * (Jr - 2.0);
+  const double unit[4][4] = {{1, 0, 0, 0}, {0, 1, 0, 0}, {0, 0, 1, 0}, {0, 0, 0, 1}};
+  for (int t = 0; t < 4; ++t)
+    strain_coeffs(unit[t][0], unit[t][1], unit[t][2], unit[t][3], Jr, &sa[t * 4], &sb[t * 4], &sc[t * 4]);
+}
+
+// vilma_viscoelastic.f90:441-480 dissipative_rhs; A/B/C are (4, ne) [e][lam]
+static void dissipative_rhs(int ne, const double* r, const double* sa, const double* sb, const double* sc,
+                            const double* norm, const double* Am, const double* Bm, const double* Cm,
+                            double* f) {
+  const double xg = 0.5773502691896257;
+  const double gp[2] = {-xg, xg};
+  for (int e = 0; e < ne; ++e) {
+    double rk = r[e], rk1 = r[e + 1], h = rk1 - rk;
+    double floc[4] = {0, 0, 0, 0};
+    for (int ig = 0; ig < 2; ++ig) {
+      double ra = 0.5 * (h * gp[ig] + rk + rk1);
+      double psik = (rk1 - ra) / h, psik1 = (ra - rk) / h;
+      double tauV[4];
+      for (int m = 0; m < 4; ++m)
+        tauV[m] = Am[e * 4 + m] / h + Bm[e * 4 + m] * psik / ra + Cm[e * 4 + m] * psik1 / ra;
+      for (int t = 0; t < 4; ++t) {
+        double D = 0.0;
+        for (int m = 0; m < 4; ++m) {
+          double deps = sa[t * 4 + m] / h + sb[t * 4 + m] * psik / ra + sc[t * 4 + m] * psik1 / ra;
+          D = D + norm[m] * tauV[m] * deps;
+        }
+        floc[t] = floc[t] - D * ra * ra * h * 0.5;
+      }
+    }
+    f[idx_u(e)] += floc[0];
+    f[idx_u(e + 1)] += floc[1];
+    f[idx_v(e)] += floc[2];
+    f[idx_v(e + 1)] += floc[3];
+  }
+}
+
+// vilma_viscoelastic.f90:482-589 advance_memory, forward-Euler branch (:577-584)
+static void advance_memory_fe(int ne, const double* mu, const double* Mk, const double* Un, const double* Vn,
+                              double Jr, double* Am, double* Bm, double* Cm, const char* active) {
+  for (int e = 0; e < ne; ++e) {
+    if (active && !active[e]) continue;
+    double a[4], b[4], c[4];
+    strain_coeffs(Un[e], Un[e + 1], Vn[e], Vn[e + 1], Jr, a, b, c);
+    double Me = Mk[e];
+    double om = 1.0 - Me, two_muM = 2.0 * mu[e] * Me;
+    for (int m = 0; m < 4; ++m) {
+      Am[e * 4 + m] = om * Am[e * 4 + m] - two_muM * a[m];
+      Bm[e * 4 + m] = om * Bm[e * 4 + m] - two_muM * b[m];
+      Cm[e * 4 + m] = om * Cm[e * 4 + m] - two_muM * c[m];
+    }
+  }
+}
+
+// vilma_response.f90:386-420 response_deg1_to_cm
+static void deg1_to_cm(const RadialOp& op, double* x) {
+  if (op.nullmode.empty()) return;
+  double fa_n = op.nullmode[idx_f(op.nr - 1)];
+  if (fa_n == 0.0) return;
+  double c = -x[idx_f(op.nr - 1)] / fa_n;
+  for (int i = 0; i < op.ndof; ++i) x[i] = x[i] + c * op.nullmode[i];
+}
+
+// vilma_response.f90:542-677 response_init_ve
+void response_init_ve(Response& R, const Earth& e, const Mesh& m, const Sht& s, double dt) {
+  R.lmax = s.lmax;
+  R.nlm = s.nlm;
+  R.nr = m.nr;
+  R.ne = m.ne;
+  R.ndof = ndof_of(m.nr);
+  R.dt = dt;
+  R.time = 0.0;
+  R.a = e.r_earth;
+  R.g = earth_gravity_at(e, e.r_earth);
+  R.r = m.r;
+  R.mu.assign(R.ne, 0.0);
+  R.Mk.assign(R.ne, 0.0);
+  R.MkPerDt.assign(R.ne, 0.0);
+  R.active1d.assign(R.ne, 1);
+  for (int el = 0; el < R.ne; ++el) {
+    const Layer& L = e.layers[m.elem_layer[el]];
+    R.mu[el] = L.mu;
+    if (L.rheology == RHEOL_MAXWELL) {
+      R.Mk[el] = R.mu[el] * dt / L.eta;
+      R.MkPerDt[el] = R.mu[el] / L.eta;
+    }
+  }
+  const int L = R.lmax, nr = R.nr;
+  R.Jr.assign(L + 1, 0.0);
+  R.nrmc.assign((size_t)(L + 1) * 4, 0.0);
+  R.sa.assign((size_t)(L + 1) * 16, 0.0);
+  R.sb = R.sa;
+  R.sc = R.sa;
+  R.gu.assign(L + 1, 0.0);
+  R.gn.assign(L + 1, 0.0);
+  R.gv.assign(L + 1, 0.0);
+  R.xUn.assign((size_t)(L + 1) * nr, 0.0);
+  R.xVn.assign((size_t)(L + 1) * nr, 0.0);
+  R.ops.assign(L + 1, RadialOp());
+  R.gn[0] = 4.0 * PI * GRAV_G * R.a / R.g;
+  std::vector<double> b(R.ndof), x(R.ndof);
+  for (int l = 1; l <= L; ++l) {
+    R.Jr[l] = (double)l * (double)(l + 1);
+    ve_strain_constants(R.Jr[l], &R.nrmc[l * 4], &R.sa[l * 16], &R.sb[l * 16], &R.sc[l * 16]);
+  }
+#pragma omp parallel for schedule(dynamic)
+  for (int l = 1; l <= L; ++l) {
+    std::vector<double> bb(R.ndof), xx(R.ndof);
+    radial_operator_assemble(R.ops[l], e, m, l);
+    radial_operator_load_rhs(R.ops[l], 1.0, bb.data());
+    radial_operator_solve_vec(R.ops[l], bb.data(), xx.data(), nullptr);
+    if (l == 1 && R.deg1_cm) deg1_to_cm(R.ops[l], xx.data());
+    R.gu[l] = xx[idx_u(nr - 1)];
+    R.gn[l] = -xx[idx_f(nr - 1)] / R.g;
+    R.gv[l] = xx[idx_v(nr - 1)];
+    for (int node = 0; node < nr; ++node) {
+      R.xUn[(size_t)l * nr + node] = xx[idx_u(node)];
+      R.xVn[(size_t)l * nr + node] = xx[idx_v(node)];
+    }
+  }
+  if (L >= 1 && !R.deg1_cm) R.gn[1] = 0.0;
+  // degree-grouped slot map
+  R.nk = 0;
+  for (int l = 1; l <= L; ++l) R.nk += std::min(l, s.mmax) + 1;
+  R.k2lm.assign(R.nk, 0);
+  R.kdeg.assign(R.nk, 0);
+  R.kbeg.assign(L + 2, 0);
+  int k = 0;
+  for (int l = 1; l <= L; ++l) {
+    R.kbeg[l] = k;
+    for (int mm = 0; mm <= std::min(l, s.mmax); ++mm) {
+      R.k2lm[k] = s.lmidx(l, mm);
+      R.kdeg[k] = l;
+      ++k;
+    }
+  }
+  R.kbeg[L + 1] = k;
+  const size_t nmem = (size_t)R.nk * R.ne * 4;
+  R.Are.assign(nmem, 0.0);
+  R.Aim = R.Are;
+  R.Bre = R.Are;
+  R.Bim = R.Are;
+  R.Cre = R.Are;
+  R.Cim = R.Are;
+  R.dUa.assign(R.nk, 0.0);
+  R.dFa = R.dUa;
+  R.dVa = R.dUa;
+  R.dUn_re.assign((size_t)R.nk * nr, 0.0);
+  R.dUn_im = R.dUn_re;
+  R.dVn_re = R.dUn_re;
+  R.dVn_im = R.dUn_re;
+  R.mnorm.assign(R.nk, 0.0);
+}
+
+// vilma_response.f90:811-826 absmax6
+static double absmax6(int n, const double* x1, const double* x2, const double* x3, const double* x4,
+                      const double* x5, const double* x6) {
+  double amax = 0.0;
+  for (int i = 0; i < n; ++i) {
+    amax = std::max(amax, std::fabs(x1[i]));
+    amax = std::max(amax, std::fabs(x2[i]));
+    amax = std::max(amax, std::fabs(x3[i]));
+    amax = std::max(amax, std::fabs(x4[i]));
+    amax = std::max(amax, std::fabs(x5[i]));
+    amax = std::max(amax, std::fabs(x6[i]));
+  }
+  return amax;
+}
+
+// vilma_response.f90:679-809 ve_response_begin -> solve_drift
+void response_begin_step(Response& R, const Sht& s) {
+  (void)s;
+  const int nb = 4 * R.ne, nr = R.nr;
+#pragma omp parallel for schedule(static)
+  for (int k = 0; k < R.nk; ++k) {
+    size_t o = (size_t)k * nb;
+    R.mnorm[k] = absmax6(nb, &R.Are[o], &R.Bre[o], &R.Cre[o], &R.Aim[o], &R.Bim[o], &R.Cim[o]);
+  }
+  double mx = 0.0;
+  for (int k = 0; k < R.nk; ++k) mx = std::max(mx, R.mnorm[k]);
+  const double thr = R.skip_tol * mx;
+  long solved = 0;
+#pragma omp parallel reduction(+ : solved)
+  {
+    std::vector<double> fre(R.ndof), fim(R.ndof), xre(R.ndof), xim(R.ndof);
+#pragma omp for schedule(dynamic)
+    for (int l = 1; l <= R.lmax; ++l) {
+      for (int k = R.kbeg[l]; k < R.kbeg[l + 1]; ++k) {
+        if (R.mnorm[k] <= thr) {
+          R.dUa[k] = 0.0;
+          R.dFa[k] = 0.0;
+          R.dVa[k] = 0.0;
+          for (int node = 0; node < nr; ++node) {
+            R.dUn_re[(size_t)k * nr + node] = 0.0;
+            R.dUn_im[(size_t)k * nr + node] = 0.0;
+            R.dVn_re[(size_t)k * nr + node] = 0.0;
+            R.dVn_im[(size_t)k * nr + node] = 0.0;
+          }
+          continue;
+        }
+        ++solved;
+        std::fill(fre.begin(), fre.end(), 0.0);
+        std::fill(fim.begin(), fim.end(), 0.0);
+        size_t o = (size_t)k * nb;
+        dissipative_rhs(R.ne, R.r.data(), &R.sa[l * 16], &R.sb[l * 16], &R.sc[l * 16], &R.nrmc[l * 4],
+                        &R.Are[o], &R.Bre[o], &R.Cre[o], fre.data());
+        dissipative_rhs(R.ne, R.r.data(), &R.sa[l * 16], &R.sb[l * 16], &R.sc[l * 16], &R.nrmc[l * 4],
+                        &R.Aim[o], &R.Bim[o], &R.Cim[o], fim.data());
+        radial_operator_solve_vec(R.ops[l], fre.data(), xre.data(), nullptr);
+        radial_operator_solve_vec(R.ops[l], fim.data(), xim.data(), nullptr);
+        if (l == 1 && R.deg1_cm) {
+          deg1_to_cm(R.ops[l], xre.data());
+          deg1_to_cm(R.ops[l], xim.data());
+        }
+        R.dUa[k] = cplx(xre[idx_u(nr - 1)], xim[idx_u(nr - 1)]);
+        R.dFa[k] = cplx(xre[idx_f(nr - 1)], xim[idx_f(nr - 1)]);
+        R.dVa[k] = cplx(xre[idx_v(nr - 1)], xim[idx_v(nr - 1)]);
+        if (l == 1 && !R.deg1_cm) R.dFa[k] = 0.0;
+        for (int node = 0; node < nr; ++node) {
+          R.dUn_re[(size_t)k * nr + node] = xre[idx_u(node)];
+          R.dUn_im[(size_t)k * nr + node] = xim[idx_u(node)];
+          R.dVn_re[(size_t)k * nr + node] = xre[idx_v(node)];
+          R.dVn_im[(size_t)k * nr + node] = xim[idx_v(node)];
+        }
+      }
+    }
+  }
+  R.n_solved += solved;
+  R.n_drift++;
+}
+
+// vilma_response.f90:842-864 ve_response_apply
+void response_apply(const Response& R, const Sht& s, const cplx* sigma, cplx* u, cplx* n) {
+  for (int lm = 0; lm < s.nlm; ++lm) {
+    u[lm] = 0.0;
+    n[lm] = 0.0;
+  }
+  int lm0 = s.lmidx(0, 0);
+  u[lm0] = R.gu[0] * sigma[lm0];
+  n[lm0] = R.gn[0] * sigma[lm0];
+  for (int k = 0; k < R.nk; ++k) {
+    int l = R.kdeg[k], lm = R.k2lm[k];
+    u[lm] = R.gu[l] * sigma[lm] + R.dUa[k];
+    n[lm] = R.gn[l] * sigma[lm] - R.dFa[k] / R.g;
+  }
+}
+
+// ------------------------------------------------------------- 3-D advance
+// vilma_response.f90:1227-1272 gather_tensor_coeffs (spheroidal channels);
+// blocks are (4, nlm) channel-major here: c[lam*nlm + lm].
+static void gather_tensor_coeffs(const Response& R, const Sht& s, const cplx* sigma, int e, cplx* cma,
+                                 cplx* cmb, cplx* cmc, cplx* cea, cplx* ceb, cplx* cec) {
+  const int nlm = s.nlm, nr = R.nr;
+  for (int t = 0; t < 4 * nlm; ++t) cma[t] = cmb[t] = cmc[t] = cea[t] = ceb[t] = cec[t] = 0.0;
+  for (int k = 0; k < R.nk; ++k) {
+    int l = R.kdeg[k], lm = R.k2lm[k];
+    double sre = sigma[lm].real(), sim = sigma[lm].imag();
+    const double* xu = &R.xUn[(size_t)l * nr];
+    const double* xv = &R.xVn[(size_t)l * nr];
+    size_t kn = (size_t)k * nr;
+    double Ur = sre * xu[e] + R.dUn_re[kn + e], Ui = sim * xu[e] + R.dUn_im[kn + e];
+    double Ur1 = sre * xu[e + 1] + R.dUn_re[kn + e + 1], Ui1 = sim * xu[e + 1] + R.dUn_im[kn + e + 1];
+    double Vr = sre * xv[e] + R.dVn_re[kn + e], Vi = sim * xv[e] + R.dVn_im[kn + e];
+    double Vr1 = sre * xv[e + 1] + R.dVn_re[kn + e + 1], Vi1 = sim * xv[e + 1] + R.dVn_im[kn + e + 1];
+    double ar[4], br[4], cr[4], ai[4], bi[4], ci[4];
+    strain_coeffs(Ur, Ur1, Vr, Vr1, R.Jr[l], ar, br, cr);
+    strain_coeffs(Ui, Ui1, Vi, Vi1, R.Jr[l], ai, bi, ci);
+    size_t o = ((size_t)k * R.ne + e) * 4;
+    for (int lam = 0; lam < 4; ++lam) {
+      cea[lam * nlm + lm] = cplx(ar[lam], ai[lam]);
+      ceb[lam * nlm + lm] = cplx(br[lam], bi[lam]);
+      cec[lam * nlm + lm] = cplx(cr[lam], ci[lam]);
+      cma[lam * nlm + lm] = cplx(R.Are[o + lam], R.Aim[o + lam]);
+      cmb[lam * nlm + lm] = cplx(R.Bre[o + lam], R.Bim[o + lam]);
+      cmc[lam * nlm + lm] = cplx(R.Cre[o + lam], R.Cim[o + lam]);
+    }
+  }
+}
+
+// vilma_response.f90:1274-1319 advance_shape_tensor (increment form)
+static void advance_shape_tensor(const Response& R, const Sht& s, int e, cplx* c, const cplx* eps,
+                                 double* dtau, double* deps, cplx* cdel) {
+  const size_t ng = (size_t)s.nphi * s.nlat;
+  double twoMu = 2.0 * R.mu[e];
+  tensor_synth(s, c, dtau);
+  tensor_synth(s, eps, deps);
+  const double* M = &R.Mk3[(size_t)e * ng];
+  for (int p = 0; p < 6; ++p)
+    for (size_t g = 0; g < ng; ++g) dtau[p * ng + g] = -M[g] * (dtau[p * ng + g] + twoMu * deps[p * ng + g]);
+  tensor_analysis(s, dtau, cdel);
+  for (int t = 0; t < 4 * s.nlm; ++t) c[t] = c[t] + cdel[t];
+}
+
+// vilma_response.f90:1171-1225 advance_memory_3d
+static void advance_memory_3d(Response& R, const Sht& s, const cplx* sigma) {
+  if (R.ne3d == 0) return;
+  const int nlm = s.nlm;
+  const size_t ng = (size_t)s.nphi * s.nlat;
+#pragma omp parallel
+  {
+    std::vector<cplx> cma(4 * nlm), cmb(4 * nlm), cmc(4 * nlm), cea(4 * nlm), ceb(4 * nlm),
+        cec(4 * nlm), cdel(4 * nlm);
+    std::vector<double> dtau(6 * ng), deps(6 * ng);
+#pragma omp for schedule(dynamic)
+    for (int ei = 0; ei < R.ne3d; ++ei) {
+      int e = R.e3d[ei];
+      gather_tensor_coeffs(R, s, sigma, e, cma.data(), cmb.data(), cmc.data(), cea.data(), ceb.data(),
+                           cec.data());
+      advance_shape_tensor(R, s, e, cma.data(), cea.data(), dtau.data(), deps.data(), cdel.data());
+      advance_shape_tensor(R, s, e, cmb.data(), ceb.data(), dtau.data(), deps.data(), cdel.data());
+      advance_shape_tensor(R, s, e, cmc.data(), cec.data(), dtau.data(), deps.data(), cdel.data());
+      for (int k = 0; k < R.nk; ++k) {
+        int lm = R.k2lm[k];
+        size_t o = ((size_t)k * R.ne + e) * 4;
+        for (int lam = 0; lam < 4; ++lam) {
+          R.Are[o + lam] = cma[lam * nlm + lm].real();
+          R.Aim[o + lam] = cma[lam * nlm + lm].imag();
+          R.Bre[o + lam] = cmb[lam * nlm + lm].real();
+          R.Bim[o + lam] = cmb[lam * nlm + lm].imag();
+          R.Cre[o + lam] = cmc[lam * nlm + lm].real();
+          R.Cim[o + lam] = cmc[lam * nlm + lm].imag();
+        }
+      }
+    }
+  }
+}
+
+// vilma_response.f90:944-992 vilma_advance
+void response_advance(Response& R, const Sht& s, const cplx* sigma) {
+  if (R.lat_visc) advance_memory_3d(R, s, sigma);
+  const int nr = R.nr;
+#pragma omp parallel
+  {
+    std::vector<double> Ure(nr), Uim(nr), Vre(nr), Vim(nr);
+#pragma omp for schedule(static)
+    for (int k = 0; k < R.nk; ++k) {
+      int l = R.kdeg[k], lm = R.k2lm[k];
+      double sre = sigma[lm].real(), sim = sigma[lm].imag();
+      const double* xu = &R.xUn[(size_t)l * nr];
+      const double* xv = &R.xVn[(size_t)l * nr];
+      size_t kn = (size_t)k * nr;
+      for (int node = 0; node < nr; ++node) {
+        Ure[node] = sre * xu[node] + R.dUn_re[kn + node];
+        Uim[node] = sim * xu[node] + R.dUn_im[kn + node];
+        Vre[node] = sre * xv[node] + R.dVn_re[kn + node];
+        Vim[node] = sim * xv[node] + R.dVn_im[kn + node];
+      }
+      size_t o = (size_t)k * R.ne * 4;
+      advance_memory_fe(R.ne, R.mu.data(), R.Mk.data(), Ure.data(), Vre.data(), R.Jr[l], &R.Are[o], &R.Bre[o],
+                        &R.Cre[o], R.active1d.data());
+      advance_memory_fe(R.ne, R.mu.data(), R.Mk.data(), Uim.data(), Vim.data(), R.Jr[l], &R.Aim[o], &R.Bim[o],
+                        &R.Cim[o], R.active1d.data());
+    }
+  }
+  R.n_mem++;
+}
+
+// vilma_response.f90:1665-1680 response_set_dt
+void response_set_dt(Response& R, double dt) {
+  R.dt = dt;
+  for (int e = 0; e < R.ne; ++e) R.Mk[e] = R.MkPerDt[e] * dt;
+  if (R.lat_visc)
+    for (size_t g = 0; g < R.Mk3.size(); ++g) R.Mk3[g] = R.MkPerDt3[g] * dt;
+}
+
+// vilma_response.f90:1783-1793
+double response_max_rate(const Response& R) {
+  double rate = 0.0;
+  for (double v : R.MkPerDt) rate = std::max(rate, v);
+  if (R.lat_visc)
+    for (double v : R.MkPerDt3) rate = std::max(rate, v);
+  return rate;
+}
+
+// vilma_response.f90:1795-1811
+double response_memory_norm(const Response& R) {
+  const int nb = 4 * R.ne;
+  double nrm = 0.0;
+#pragma omp parallel for reduction(max : nrm) schedule(static)
+  for (int k = 0; k < R.nk; ++k) {
+    size_t o = (size_t)k * nb;
+    nrm = std::max(nrm, absmax6(nb, &R.Are[o], &R.Aim[o], &R.Bre[o], &R.Bim[o], &R.Cre[o], &R.Cim[o]));
+  }
+  return nrm;
+}
+
+// vilma_response.f90:994-1053 response_enable_lateral_visc (spheroidal channels)
+void response_enable_lateral_visc(Response& R, const Sht& s, const double* pert) {
+  const size_t ng = (size_t)s.nphi * s.nlat;
+  R.MkPerDt3.assign(ng * R.ne, 0.0);
+  R.Mk3.assign(ng * R.ne, 0.0);
+  for (int e = 0; e < R.ne; ++e)
+    for (size_t g = 0; g < ng; ++g) R.MkPerDt3[e * ng + g] = R.MkPerDt[e] * std::pow(10.0, -pert[e * ng + g]);
+  std::fill(R.active1d.begin(), R.active1d.end(), 1);
+  R.ne3d = 0;
+  for (int e = 0; e < R.ne; ++e) {
+    if (R.MkPerDt[e] == 0.0) continue;
+    double mx = -1e300, mn = 1e300, sum = 0.0;
+    for (size_t g = 0; g < ng; ++g) {
+      mx = std::max(mx, pert[e * ng + g]);
+      mn = std::min(mn, pert[e * ng + g]);
+    }
+    if (mx - mn > R.visc3d_tol) {
+      R.active1d[e] = 0;
+      R.ne3d++;
+    } else {
+      for (size_t g = 0; g < ng; ++g) sum += pert[e * ng + g];
+      double mean_pert = sum / (double)ng;
+      R.MkPerDt[e] = R.MkPerDt[e] * std::pow(10.0, -mean_pert);
+    }
+  }
+  for (int e = 0; e < R.ne; ++e) R.Mk[e] = R.MkPerDt[e] * R.dt;
+  for (size_t g = 0; g < R.Mk3.size(); ++g) R.Mk3[g] = R.MkPerDt3[g] * R.dt;
+  R.e3d.clear();
+  for (int e = 0; e < R.ne; ++e)
+    if (!R.active1d[e]) R.e3d.push_back(e);
+  R.ne3d = (int)R.e3d.size();
+  R.lat_visc = true;
+}
+
+}  // namespace orc

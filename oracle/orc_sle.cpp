@@ -1,0 +1,200 @@
+// CPU ORACLE — test infrastructure only (see orc.hpp).
+// Sea-level equation (migrating coastline, subgrid term, grounded-ice masking)
+// and the forward-Euler sub-stepping driver with its reactive guard.
+#include <algorithm>
+#include <cmath>
+#include <stdexcept>
+
+#include "orc.hpp"
+
+namespace orc {
+
+// vilma_sle.f90:407-425 ocean_function
+void ocean_function(int n, const double* topo, const double* ice, double* C) {
+  for (int i = 0; i < n; ++i) C[i] = (topo[i] < 0.0 && RHO_ICE * ice[i] < -RHO_WATER * topo[i]) ? 1.0 : 0.0;
+}
+
+// vilma_sle.f90:124-405 sle_solve (FE / first-order response: one memory pass)
+void sle_solve(SleSolver& sle, const Sht& s, Response& R, const double* d_ice, const double* ice,
+               const double* topo0, double* rsl, double* C, SleResult& res, bool report_only,
+               cplx* sigma_out, const double* s_rot) {
+  const int ng = s.nphi * s.nlat, nlm = s.nlm;
+  sle.n_solve++;
+  std::vector<double> load(ng), u(ng, 0.0), N(ng, 0.0), Sraw(ng), rsl_new(ng), C0(ng), wcorr(ng, 0.0),
+      C_next(ng), d_ice_g(ng, 0.0), tmp(ng), ice_ref(ng);
+  std::vector<cplx> load_lm(nlm), u_lm(nlm), N_lm(nlm);
+  const double rho_ratio = RHO_ICE / RHO_WATER;
+  if (!sle.warm_start)
+    for (int i = 0; i < ng; ++i) rsl[i] = 0.0;
+  double dphi = 0.0, ice_int = 0.0, zeta_int = 0.0, C_int = 0.0, Cs_int = 0.0;
+  res.n_inner_last = 0;
+  res.resid = 0.0;
+  res.n_outer_done = 0;
+  res.n_coast_flip = 0;
+  for (int i = 0; i < ng; ++i) ice_ref[i] = ice[i] - d_ice[i];
+  ocean_function(ng, topo0, ice_ref.data(), C0.data());
+  response_begin_step(R, s);
+  auto assemble_load = [&]() {
+    for (int i = 0; i < ng; ++i) load[i] = RHO_ICE * d_ice_g[i] + RHO_WATER * (C[i] * rsl[i]) + wcorr[i];
+  };
+  for (int io = 1; io <= sle.n_outer; ++io) {
+    if (sle.fixed_ocean) {
+      if (io == 1)
+        for (int i = 0; i < ng; ++i) C[i] = C0[i];
+    } else if (io == 1) {
+      for (int i = 0; i < ng; ++i) tmp[i] = topo0[i] - rsl[i];
+      ocean_function(ng, tmp.data(), ice, C);
+    } else {
+      for (int i = 0; i < ng; ++i) C[i] = C_next[i];
+    }
+    for (int i = 0; i < ng; ++i) d_ice_g[i] = ice[i] * (1.0 - C[i]) - (ice[i] - d_ice[i]) * (1.0 - C0[i]);
+    C_int = sht_surface_integral(s, C);
+    if (C_int <= 0.0) break;
+    ice_int = -rho_ratio * sht_surface_integral(s, d_ice_g.data());
+    if (sle.subgrid) {
+      for (int i = 0; i < ng; ++i) {
+        wcorr[i] = -RHO_WATER * topo0[i] * (C[i] - C0[i]);
+        tmp[i] = topo0[i] * (C[i] - C0[i]);
+      }
+      zeta_int = sht_surface_integral(s, tmp.data());
+    } else {
+      std::fill(wcorr.begin(), wcorr.end(), 0.0);
+      zeta_int = 0.0;
+    }
+    for (int ii = 1; ii <= sle.n_inner; ++ii) {
+      assemble_load();
+      sht_analysis(s, load.data(), load_lm.data());
+      response_apply(R, s, load_lm.data(), u_lm.data(), N_lm.data());
+      sht_synth(s, u_lm.data(), u.data());
+      sht_synth(s, N_lm.data(), N.data());
+      for (int i = 0; i < ng; ++i) {
+        Sraw[i] = N[i] - u[i];
+        if (s_rot) Sraw[i] = Sraw[i] + s_rot[i];
+        tmp[i] = C[i] * Sraw[i];
+      }
+      Cs_int = sht_surface_integral(s, tmp.data());
+      dphi = (ice_int - Cs_int + zeta_int) / C_int;
+      double dmax = 0.0, smax = 0.0;
+      for (int i = 0; i < ng; ++i) {
+        rsl_new[i] = Sraw[i] + dphi;
+        dmax = std::max(dmax, std::fabs(C[i] * (rsl_new[i] - rsl[i])));
+      }
+      for (int i = 0; i < ng; ++i) {
+        rsl[i] = rsl_new[i];
+        smax = std::max(smax, std::fabs(C[i] * rsl[i]));
+      }
+      res.n_inner_last = ii;
+      res.resid = dmax;
+      if (dmax <= sle.tol * std::max(smax, 2.2250738585072014e-308)) break;
+    }
+    res.n_outer_done = io;
+    sle.n_outer_tot++;
+    sle.n_inner_tot += res.n_inner_last;
+    if (sle.fixed_ocean) break;
+    for (int i = 0; i < ng; ++i) tmp[i] = topo0[i] - rsl[i];
+    ocean_function(ng, tmp.data(), ice, C_next.data());
+    int flips = 0;
+    for (int i = 0; i < ng; ++i) flips += (C_next[i] != C[i]);
+    res.n_coast_flip = flips;
+    if (flips == 0) break;
+  }
+  assemble_load();
+  sht_analysis(s, load.data(), load_lm.data());
+  if (!report_only) {
+    response_advance(R, s, load_lm.data());
+    R.time += R.dt;
+  }
+  if (sigma_out)
+    for (int lm = 0; lm < nlm; ++lm) sigma_out[lm] = load_lm[lm];
+  for (int i = 0; i < ng; ++i) tmp[i] = C[i] * rsl[i];
+  Cs_int = sht_surface_integral(s, tmp.data()) - zeta_int;
+  res.ocean_frac = C_int / (16.0 * std::atan(1.0));
+  if (std::fabs(ice_int) > 0.0)
+    res.mass_resid = std::fabs(Cs_int - ice_int) / std::fabs(ice_int);
+  else
+    res.mass_resid = std::fabs(Cs_int);
+  res.esl = dphi;
+}
+
+// vilma_timestep.f90:79-227 stepper_advance, explicit (forward-Euler) branch.
+// The rollback snapshot is held here (response_save_state/restore_state).
+int stepper_advance(Stepper& st, const Sht& s, Response& R, SleSolver& sle, const double* topo0,
+                    const double* ice0, const double* ice1, const double* ice_ref, double t0, double t1,
+                    double* rsl, double* C, const double* s_rot, cplx* sigma_out) {
+  const int ng = s.nphi * s.nlat;
+  const double span = t1 - t0;
+  std::vector<cplx> sig_last(s.nlm, 0.0);
+  st.worst_mass_resid = 0.0;
+  std::vector<double> ice_now(ng), dice_now(ng), rsl_n(ng);
+  SleResult res;
+  if (span <= 0.0) {
+    for (int i = 0; i < ng; ++i) {
+      ice_now[i] = ice0[i];
+      dice_now[i] = ice0[i] - ice_ref[i];
+    }
+    sle_solve(sle, s, R, dice_now.data(), ice_now.data(), topo0, rsl, C, res, true, sig_last.data(), s_rot);
+    st.worst_mass_resid = res.mass_resid;
+    if (sigma_out) std::copy(sig_last.begin(), sig_last.end(), sigma_out);
+    return 0;
+  }
+  double rate = response_max_rate(R);
+  double dt_stab = rate > 0.0 ? st.cfl / rate : span;
+  dt_stab = std::min(dt_stab, st.dt_max);
+  if (st.dt_min > 0.0) dt_stab = std::max(dt_stab, st.dt_min);
+  int n_sub = std::max(1, (int)std::ceil(span / dt_stab - 1.0e-9));
+  st.n_sub_last = n_sub;
+  double dt = span / (double)n_sub;
+  double t = t0;
+  double tau_run = response_memory_norm(R);
+  std::vector<double> sAre, sAim, sBre, sBim, sCre, sCim;
+  while (true) {
+    if (t >= t1 - 1.0e-9 * span) break;
+    dt = std::min(dt, t1 - t);
+    rsl_n.assign(rsl, rsl + ng);
+    double tau0 = response_memory_norm(R);
+    sAre = R.Are;
+    sAim = R.Aim;
+    sBre = R.Bre;
+    sBim = R.Bim;
+    sCre = R.Cre;
+    sCim = R.Cim;
+    double time_s = R.time;
+    response_set_dt(R, dt);
+    {  // solve_at(t + dt)
+      double frac = (t + dt - t0) / span;
+      for (int i = 0; i < ng; ++i) {
+        ice_now[i] = ice0[i] + frac * (ice1[i] - ice0[i]);
+        dice_now[i] = ice_now[i] - ice_ref[i];
+      }
+      st.n_solve++;
+      sle_solve(sle, s, R, dice_now.data(), ice_now.data(), topo0, rsl, C, res, false, sig_last.data(), s_rot);
+      st.worst_mass_resid = std::max(st.worst_mass_resid, res.mass_resid);
+    }
+    double err_inf = response_memory_norm(R);
+    bool finite = err_inf <= 1.7976931348623157e308;
+    double scale = std::max(tau0, tau_run);
+    bool accept = scale <= 0.0 ? finite : (finite && err_inf <= st.guard_growth * scale);
+    if (accept) {
+      tau_run = std::max(tau_run, err_inf);
+      t = t + dt;
+      st.n_accept++;
+      dt = std::min(span / (double)n_sub, 2.0 * dt);
+    } else {
+      R.Are = sAre;
+      R.Aim = sAim;
+      R.Bre = sBre;
+      R.Bim = sBim;
+      R.Cre = sCre;
+      R.Cim = sCim;
+      R.time = time_s;
+      std::copy(rsl_n.begin(), rsl_n.end(), rsl);
+      st.n_reject++;
+      dt = 0.5 * dt;
+      if (dt <= 1.0e-12 * span) return 1;
+    }
+  }
+  if (sigma_out) std::copy(sig_last.begin(), sig_last.end(), sigma_out);
+  return 0;
+}
+
+}  // namespace orc
