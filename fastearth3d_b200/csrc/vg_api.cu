@@ -1,0 +1,334 @@
+// C-ABI entry points (include/vilma_gpu.h). Every call returns an int status;
+// failures are caught here and their message is kept for vg_last_error. No
+// exit or abort inside the library.
+#include <cmath>
+#include <cstring>
+#include <string>
+
+#include "vg_internal.cuh"
+
+using vg::DArr;
+using vg::Error;
+
+static thread_local std::string g_last_error;
+
+template <class F>
+static int guarded(vg_handle* h, F&& f) {
+  try {
+    f();
+    return 0;
+  } catch (const std::exception& ex) {
+    if (h)
+      h->err = ex.what();
+    else
+      g_last_error = ex.what();
+    return 1;
+  }
+}
+
+static void need(vg_handle* h, bool cond, const char* msg) {
+  (void)h;
+  if (!cond) throw Error(msg);
+}
+
+extern "C" {
+
+int vg_params_default(vg_params* p) {
+  if (!p) return 1;
+  std::memset(p, 0, sizeof(*p));
+  const double km = 1e3;
+  p->lmax = 16;
+  p->nlat = 17;
+  p->nphi = 34;
+  p->n_layer = 4;
+  p->r_earth = 6371.0 * km;
+  const double rb[4] = {6301.0 * km, 5701.0 * km, 3480.0 * km, 0.0};
+  const double rt[4] = {6371.0 * km, 6301.0 * km, 5701.0 * km, 3480.0 * km};
+  const double rho[4] = {3300.0, 3450.0, 4900.0, 10900.0};
+  const double mu[4] = {0.7e11, 0.9e11, 2.0e11, 0.0};
+  const double eta[4] = {1e300, 5e20, 2e21, 0.0};
+  const int rh[4] = {VG_RHEOL_ELASTIC, VG_RHEOL_MAXWELL, VG_RHEOL_MAXWELL, VG_RHEOL_FLUID};
+  for (int i = 0; i < 4; ++i) {
+    p->r_bot[i] = rb[i];
+    p->r_top[i] = rt[i];
+    p->rho[i] = rho[i];
+    p->mu[i] = mu[i];
+    p->eta[i] = eta[i];
+    p->rheology[i] = rh[i];
+  }
+  p->scheme = VG_SCHEME_FE;
+  p->deg1_cm = 1;
+  p->skip_tol = 1e-4;
+  p->visc3d_tol = 1e-3;
+  p->dt_init = 0.0;
+  p->cfl = 1.0;
+  p->guard_growth = 1e3;
+  p->dt_min = 0.0;
+  p->dt_max = 1.7976931348623157e308;
+  p->sle_n_outer = 3;
+  p->sle_n_inner = 20;
+  p->sle_tol = 1e-7;
+  p->sle_fixed_ocean = 0;
+  p->sle_subgrid = 1;
+  p->sle_warm_start = 1;
+  p->rotation = 0;
+  p->visc3d_precision = VG_VISC3D_FP64;
+  return 0;
+}
+
+int vg_create(const vg_params* p, vg_handle** out) {
+  if (!p || !out) {
+    g_last_error = "vg_create: null argument";
+    return 1;
+  }
+  *out = nullptr;
+  vg_handle* h = new vg_handle();
+  h->p = *p;
+  int rc = guarded(nullptr, [&] {
+    int ndev = 0;
+    VG_CUDA(cudaGetDevice(&h->device));
+    VG_CUDA(cudaGetDeviceCount(&ndev));
+    VG_CUDA(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
+    vg::setup_handle(h);
+    vg::compute_mem_norm(h, 0);
+    h->mem_norm = vg::read_mem_norm(h, 0);
+  });
+  if (rc) {
+    delete h;
+    return rc;
+  }
+  *out = h;
+  return 0;
+}
+
+int vg_destroy(vg_handle* h) {
+  if (!h) return 0;
+  if (h->stream) cudaStreamSynchronize(h->stream);
+  if (h->h_sc) cudaFreeHost(h->h_sc);
+  cudaStream_t s = h->stream;
+  delete h;
+  if (s) cudaStreamDestroy(s);
+  return 0;
+}
+
+const char* vg_last_error(const vg_handle* h) { return h ? h->err.c_str() : g_last_error.c_str(); }
+
+int vg_set_reference(vg_handle* h, const double* z_bed_eq, const double* h_ice_eq, const double* h_ice_init) {
+  return guarded(h, [&] {
+    need(h, z_bed_eq && h_ice_eq, "vg_set_reference: z_bed_eq and h_ice_eq are required");
+    const int ng = h->grid.ng;
+    cudaStream_t s = h->stream;
+    h->d_z_bed_eq.upload(z_bed_eq, ng, s);
+    h->d_h_ice_eq.upload(h_ice_eq, ng, s);
+    h->d_h_ice.upload(h_ice_init ? h_ice_init : h_ice_eq, ng, s);
+    VG_CUDA(cudaMemsetAsync(h->d_rsl.p, 0, ng * sizeof(double), s));
+    VG_CUDA(cudaMemcpyAsync(h->d_zbed.p, z_bed_eq, ng * sizeof(double), cudaMemcpyHostToDevice, s));
+    // C0 = ocean_function(z_bed_eq, h_ice_eq); C = C0 (src/vilma_coupling.f90:211-212)
+    VG_CUDA(cudaMemsetAsync(h->d_tmp.p, 0, ng * sizeof(double), s));
+    std::vector<double> c0(ng);
+    for (int i = 0; i < ng; ++i)
+      c0[i] = (z_bed_eq[i] < 0.0 && vg::RHO_ICE * h_ice_eq[i] < -vg::RHO_WATER * z_bed_eq[i]) ? 1.0 : 0.0;
+    h->d_C0.upload(c0.data(), ng, s);
+    h->d_C.upload(c0.data(), ng, s);
+    VG_CUDA(cudaStreamSynchronize(s));
+    h->have_reference = true;
+  });
+}
+
+int vg_enable_visc3d(vg_handle* h, const double* pert) {
+  return guarded(h, [&] {
+    need(h, pert != nullptr, "vg_enable_visc3d: pert is required");
+    vg::visc3d_enable(h, pert);
+  });
+}
+
+int vg_update_device(vg_handle* h, const double* d_h_ice, double dt_yr) {
+  return guarded(h, [&] {
+    need(h, h->have_reference, "vg_update: call vg_set_reference first (solid_earth_init)");
+    need(h, d_h_ice != nullptr, "vg_update: h_ice is required");
+    vg::update_dev(h, d_h_ice, dt_yr);
+    VG_CUDA(cudaStreamSynchronize(h->stream));
+  });
+}
+
+int vg_update(vg_handle* h, const double* h_ice, double dt_yr) {
+  return guarded(h, [&] {
+    need(h, h->have_reference, "vg_update: call vg_set_reference first (solid_earth_init)");
+    need(h, h_ice != nullptr, "vg_update: h_ice is required");
+    h->d_ice1.upload(h_ice, h->grid.ng, h->stream);
+    vg::update_dev(h, h->d_ice1.p, dt_yr);
+    VG_CUDA(cudaStreamSynchronize(h->stream));
+  });
+}
+
+int vg_get_fields(vg_handle* h, double* rsl, double* z_bed, double* C, double* sigma_lm) {
+  return guarded(h, [&] {
+    const int ng = h->grid.ng;
+    cudaStream_t s = h->stream;
+    if (rsl) h->d_rsl.download(rsl, ng, s);
+    if (z_bed) h->d_zbed.download(z_bed, ng, s);
+    if (C) h->d_C.download(C, ng, s);
+    if (sigma_lm) h->d_sigma.download(sigma_lm, 2 * (size_t)h->grid.nlm, s);
+    VG_CUDA(cudaStreamSynchronize(s));
+  });
+}
+
+int vg_rsl_device(vg_handle* h, const double** d_rsl) {
+  return guarded(h, [&] {
+    need(h, d_rsl != nullptr, "vg_rsl_device: null argument");
+    *d_rsl = h->d_rsl.p;
+  });
+}
+
+int vg_get_info(vg_handle* h, vg_info* info) {
+  return guarded(h, [&] {
+    std::memset(info, 0, sizeof(*info));
+    info->lmax = h->grid.lmax;
+    info->nlat = h->grid.nlat;
+    info->nphi = h->grid.nphi;
+    info->nlm = h->grid.nlm;
+    info->nr = h->nr;
+    info->ne = h->ne;
+    info->ndof = h->ndof;
+    info->nk = h->nk;
+    info->ne3d = h->ne3d;
+    info->n_sub_last = h->n_sub_last;
+    info->n_accept = h->n_accept;
+    info->n_reject = h->n_reject;
+    info->n_solve = h->n_solve;
+    info->n_drift_solved = h->n_drift_solved;
+    info->time_yr = h->time_yr;
+    info->worst_mass_resid = h->worst_mass_resid;
+    info->bsl = h->bsl;
+    info->n_outer_last = h->n_outer_last;
+    info->n_inner_last = h->n_inner_last;
+    info->n_coast_flip_last = h->n_flip_last;
+  });
+}
+
+int vg_response_set_dt(vg_handle* h, double dt_s) {
+  return guarded(h, [&] { h->dt = dt_s; });
+}
+
+int vg_response_begin_step(vg_handle* h) {
+  return guarded(h, [&] {
+    vg::launch_drift(h);
+    VG_CUDA(cudaStreamSynchronize(h->stream));
+  });
+}
+
+int vg_response_apply(vg_handle* h, const double* sigma_lm, double* u_lm, double* n_lm) {
+  return guarded(h, [&] {
+    const size_t n2 = 2 * (size_t)h->grid.nlm;
+    h->d_sigma.upload(sigma_lm, n2, h->stream);
+    vg::launch_apply(h, h->d_sigma.p, h->d_ulm.p, h->d_ulm.p + n2);
+    if (u_lm) VG_CUDA(cudaMemcpyAsync(u_lm, h->d_ulm.p, n2 * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    if (n_lm)
+      VG_CUDA(cudaMemcpyAsync(n_lm, h->d_ulm.p + n2, n2 * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    VG_CUDA(cudaStreamSynchronize(h->stream));
+  });
+}
+
+int vg_response_advance(vg_handle* h, const double* sigma_lm) {
+  return guarded(h, [&] {
+    const size_t n2 = 2 * (size_t)h->grid.nlm;
+    h->d_sigma.upload(sigma_lm, n2, h->stream);
+    if (h->lat_visc) vg::visc3d_advance(h, h->d_sigma.p, h->dt);
+    vg::launch_advance_1d(h, h->d_sigma.p, h->dt);
+    h->cur = 1 - h->cur;
+    h->mem_norm = vg::read_mem_norm(h, h->cur);
+    h->time_s += h->dt;
+  });
+}
+
+int vg_get_gains(vg_handle* h, double* gu, double* gn, double* gv) {
+  return guarded(h, [&] {
+    int L = h->grid.lmax + 1;
+    if (gu) h->d_gu.download(gu, L, h->stream);
+    if (gn) h->d_gn.download(gn, L, h->stream);
+    if (gv) h->d_gv.download(gv, L, h->stream);
+    VG_CUDA(cudaStreamSynchronize(h->stream));
+  });
+}
+
+int vg_get_drift(vg_handle* h, double* dUa, double* dFa, double* dVa) {
+  return guarded(h, [&] {
+    const int nk = h->nk;
+    std::vector<double> d((size_t)6 * nk);
+    h->d_drift.download(d.data(), d.size(), h->stream);
+    VG_CUDA(cudaStreamSynchronize(h->stream));
+    double* outs[3] = {dUa, dFa, dVa};
+    for (int q = 0; q < 3; ++q)
+      if (outs[q])
+        for (int k = 0; k < nk; ++k) {
+          outs[q][2 * k] = d[(size_t)(2 * q) * nk + k];
+          outs[q][2 * k + 1] = d[(size_t)(2 * q + 1) * nk + k];
+        }
+  });
+}
+
+// restart layout (NLAM, ne, nk) <-> device [s][ri][e][lam][k]
+int vg_get_state(vg_handle* h, double* Are, double* Aim, double* Bre, double* Bim, double* Cre, double* Cim,
+                 double* time_s) {
+  return guarded(h, [&] {
+    const int ne = h->ne, nk = h->nk;
+    const size_t per = (size_t)ne * 4 * nk;
+    std::vector<double> m(6 * per);
+    h->d_mem[h->cur].download(m.data(), m.size(), h->stream);
+    VG_CUDA(cudaStreamSynchronize(h->stream));
+    double* outs[6] = {Are, Aim, Bre, Bim, Cre, Cim};  // (s, ri) = (0,0),(0,1),(1,0),...
+    for (int q = 0; q < 6; ++q) {
+      if (!outs[q]) continue;
+      const double* src = m.data() + q * per;
+      for (int e = 0; e < ne; ++e)
+        for (int lam = 0; lam < 4; ++lam)
+          for (int k = 0; k < nk; ++k) outs[q][((size_t)k * ne + e) * 4 + lam] = src[((size_t)e * 4 + lam) * nk + k];
+    }
+    if (time_s) *time_s = h->time_s;
+  });
+}
+
+int vg_set_state(vg_handle* h, const double* Are, const double* Aim, const double* Bre, const double* Bim,
+                 const double* Cre, const double* Cim, double time_s) {
+  return guarded(h, [&] {
+    const int ne = h->ne, nk = h->nk;
+    const size_t per = (size_t)ne * 4 * nk;
+    std::vector<double> m(6 * per);
+    const double* ins[6] = {Are, Aim, Bre, Bim, Cre, Cim};
+    for (int q = 0; q < 6; ++q) {
+      need(h, ins[q] != nullptr, "vg_set_state: all six memory arrays are required");
+      double* dst = m.data() + q * per;
+      for (int e = 0; e < ne; ++e)
+        for (int lam = 0; lam < 4; ++lam)
+          for (int k = 0; k < nk; ++k) dst[((size_t)e * 4 + lam) * nk + k] = ins[q][((size_t)k * ne + e) * 4 + lam];
+    }
+    h->d_mem[h->cur].upload(m.data(), m.size(), h->stream);
+    vg::compute_mem_norm(h, h->cur);
+    h->mem_norm = vg::read_mem_norm(h, h->cur);
+    h->time_s = time_s;
+  });
+}
+
+int vg_sht_analysis(vg_handle* h, const double* f, double* q_lm) {
+  return guarded(h, [&] {
+    const int ng = h->grid.ng;
+    const size_t n2 = 2 * (size_t)h->grid.nlm;
+    h->d_tmp.upload(f, ng, h->stream);
+    vg::sht_analysis_dev(h, h->d_tmp.p, h->d_nlm.p, 1);
+    h->d_nlm.download(q_lm, n2, h->stream);
+    VG_CUDA(cudaStreamSynchronize(h->stream));
+  });
+}
+
+int vg_sht_synthesis(vg_handle* h, const double* q_lm, double* f) {
+  return guarded(h, [&] {
+    const int ng = h->grid.ng;
+    const size_t n2 = 2 * (size_t)h->grid.nlm;
+    h->d_nlm.upload(q_lm, n2, h->stream);
+    vg::sht_synthesis_dev(h, h->d_nlm.p, h->d_tmp.p, 1);
+    h->d_tmp.download(f, ng, h->stream);
+    VG_CUDA(cudaStreamSynchronize(h->stream));
+  });
+}
+
+}  // extern "C"

@@ -1,0 +1,142 @@
+// Device helpers shared by the kernels of several translation units.
+#pragma once
+#include <cuda_runtime.h>
+
+namespace vg {
+
+// index of memory element (s, ri, e, lam, k) in one state buffer
+__device__ __forceinline__ size_t mem_idx(int s, int ri, int e, int lam, int k, int ne, int nk) {
+  return ((size_t)((s * 2 + ri) * ne + e) * 4 + lam) * nk + k;
+}
+
+// max that propagates NaN, so a non-finite state never hides from the guard
+__device__ __forceinline__ double nanmax(double a, double b) { return (a != a || b != b) ? (a + b) : fmax(a, b); }
+
+__device__ __forceinline__ void atomic_max_bits(unsigned long long* dst, double v) {
+  // non-negative doubles (and NaN, whose bits sort above +inf) order like their bit patterns
+  atomicMax(dst, (unsigned long long)__double_as_longlong(v));
+}
+
+// src/vilma_viscoelastic.f90:329-359 strain_coeffs: element strain (a, b, c) for
+// lam = 1, 2, 5, 6 from nodal U, V; Z6 has no harmonic below degree 2.
+__device__ __forceinline__ void strain_coeffs(double u1, double u2, double v1, double v2, double Jr, double a[4],
+                                              double b[4], double c[4]) {
+  a[0] = -u1 + u2;
+  b[0] = 0.0;
+  c[0] = 0.0;
+  a[1] = -v1 + v2;
+  b[1] = u1 - v1;
+  c[1] = u2 - v2;
+  a[2] = 0.0;
+  b[2] = -u1 / Jr + 0.5 * v1;
+  c[2] = -u2 / Jr + 0.5 * v2;
+  a[3] = 0.0;
+  b[3] = 0.5 * v1;
+  c[3] = 0.5 * v2;
+  if (Jr <= 2.0) {
+    b[3] = 0.0;
+    c[3] = 0.0;
+  }
+}
+
+// Degree-1 bordered system, dense band storage with kl = ku = nd, solved for
+// up to 4 right-hand sides held in shared memory (xsh[nrhs][ns]); dgbtrs order,
+// CTA-parallel inner loops. ab[(row - 1) * ns + (col - 1)].
+__device__ __forceinline__ void deg1_solve_cta(const double* __restrict__ ab, int ns, int kl, int kv,
+                                               const int* __restrict__ ipiv, double* xsh, int nrhs) {
+  for (int j = 1; j <= ns - 1; ++j) {
+    int lm = min(kl, ns - j);
+    int l = ipiv[j - 1] + 1;
+    if ((int)threadIdx.x < nrhs && l != j) {
+      double* x = xsh + threadIdx.x * ns;
+      double t = x[l - 1];
+      x[l - 1] = x[j - 1];
+      x[j - 1] = t;
+    }
+    __syncthreads();
+    for (int t = threadIdx.x; t < lm * nrhs; t += blockDim.x) {
+      int i = 1 + t / nrhs, rr = t % nrhs;
+      double* x = xsh + rr * ns;
+      x[j + i - 1] -= ab[(size_t)(kv + i) * ns + (j - 1)] * x[j - 1];
+    }
+    __syncthreads();
+  }
+  for (int j = ns; j >= 1; --j) {
+    if ((int)threadIdx.x < nrhs) {
+      double* x = xsh + threadIdx.x * ns;
+      x[j - 1] = x[j - 1] / ab[(size_t)kv * ns + (j - 1)];
+    }
+    __syncthreads();
+    int lm = min(kv, j - 1);
+    for (int t = threadIdx.x; t < lm * nrhs; t += blockDim.x) {
+      int i = 1 + t / nrhs, rr = t % nrhs;
+      double* x = xsh + rr * ns;
+      x[j - i - 1] -= ab[(size_t)(kv - i) * ns + (j - 1)] * x[j - 1];
+    }
+    __syncthreads();
+  }
+}
+
+// --------------------------------------------------------------------------
+// Longitude transforms of one latitude row, CTA-cooperative, twiddles from
+// tables cos/sin(2 pi t / nphi). The real-field convention of the Gauss-grid
+// transforms (src/vilma_sht.f90:11-15): f_i = Re G_0 + 2 Re sum_{m>0} G_m e^{i m phi_i},
+// and F_m = (2 pi / nphi) sum_i f_i e^{-i m phi_i}.
+
+// row (smem, nphi) -> F[m] = (re, im) at F + 2*m*stride, m < M
+__device__ __forceinline__ void row_fourier_analysis(const double* row, int nphi, int M, const double* __restrict__ cs,
+                                                     const double* __restrict__ sn, double* F, size_t stride) {
+  const double sc = 2.0 * 3.14159265358979323846 / (double)nphi;
+  for (int m = threadIdx.x; m < M; m += blockDim.x) {
+    double re = 0.0, im = 0.0;
+    int t = 0;
+    for (int i = 0; i < nphi; ++i) {
+      double f = row[i];
+      re += f * __ldg(&cs[t]);
+      im -= f * __ldg(&sn[t]);
+      t += m;
+      if (t >= nphi) t -= nphi;
+    }
+    F[2 * (size_t)m * stride] = re * sc;
+    F[2 * (size_t)m * stride + 1] = im * sc;
+  }
+}
+
+// G (smem, M complex interleaved) -> f_i for i < nphi (called per thread for its i)
+__device__ __forceinline__ double row_fourier_synth_at(const double* G, int M, int i, int nphi,
+                                                       const double* __restrict__ cs, const double* __restrict__ sn) {
+  double acc = 0.0;
+  int t = i;
+  for (int m = 1; m < M; ++m) {
+    acc += G[2 * m] * __ldg(&cs[t]) - G[2 * m + 1] * __ldg(&sn[t]);
+    t += i;
+    if (t >= nphi) t -= nphi;
+  }
+  return G[0] + 2.0 * acc;
+}
+
+// CTA reductions (fixed order: deterministic for a fixed block size)
+__device__ __forceinline__ double block_sum(double v, double* red) {
+  red[threadIdx.x] = v;
+  __syncthreads();
+  for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+    if ((int)threadIdx.x < o) red[threadIdx.x] += red[threadIdx.x + o];
+    __syncthreads();
+  }
+  double r = red[0];
+  __syncthreads();
+  return r;
+}
+__device__ __forceinline__ double block_max(double v, double* red) {
+  red[threadIdx.x] = v;
+  __syncthreads();
+  for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+    if ((int)threadIdx.x < o) red[threadIdx.x] = nanmax(red[threadIdx.x], red[threadIdx.x + o]);
+    __syncthreads();
+  }
+  double r = red[0];
+  __syncthreads();
+  return r;
+}
+
+}  // namespace vg

@@ -1,0 +1,182 @@
+// Internal declarations of the B200 backend (not part of the C-ABI).
+//
+// Data layout in HBM (one model instance, FP64 throughout unless stated):
+//   memory state   mem[buf][((s*2 + ri)*ne + e)*4 + lam][k]  — shape s in {A,B,C},
+//                  ri in {re,im}, element e, channel lam, slot k FASTEST, so a
+//                  thread per (l,m) slot reads and writes coalesced rows. Two
+//                  buffers: the advance writes the other one, and a rejected
+//                  sub-step is a pointer swap, not a copy.
+//   nodal drift    dUn/dVn[ri][node][k]
+//   band factors   ab[(l*ldab + row)*ndof + col] for l >= 2 (band storage of
+//                  LAPACK dgbtf2, row index kv+1+i-j), degree 1 apart (dense)
+//   grid fields    (nphi, nlat), phi fastest, colatitude north first
+//   Legendre       plm/dplm[lm][j] (j fastest), lm m-major
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "../../include/vilma_gpu.h"
+
+#define VG_CUDA(call)                                                                     \
+  do {                                                                                   \
+    cudaError_t _e = (call);                                                             \
+    if (_e != cudaSuccess)                                                               \
+      throw vg::Error(std::string(#call) + ": " + cudaGetErrorString(_e));              \
+  } while (0)
+
+namespace vg {
+
+struct Error : std::exception {
+  std::string msg;
+  explicit Error(std::string m) : msg(std::move(m)) {}
+  const char* what() const noexcept override { return msg.c_str(); }
+};
+
+constexpr double PI = 3.14159265358979323846;
+constexpr double GRAV_G = 6.67430e-11;       // src/vilma_constants.f90
+constexpr double RHO_ICE = 931.0;
+constexpr double RHO_WATER = 1000.0;
+constexpr double SEC_PER_YEAR = 31556926.0;
+constexpr double KYR = 1000.0 * SEC_PER_YEAR;
+constexpr double TINY = 2.2250738585072014e-308;
+constexpr double HUGE_ = 1.7976931348623157e308;
+
+template <class T>
+struct DArr {
+  T* p = nullptr;
+  size_t n = 0;
+  void alloc(size_t count) {
+    release();
+    n = count;
+    if (count) {
+      VG_CUDA(cudaMalloc(&p, count * sizeof(T)));
+      VG_CUDA(cudaMemset(p, 0, count * sizeof(T)));
+    }
+  }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    n = 0;
+  }
+  void upload(const T* h, size_t count, cudaStream_t s) {
+    VG_CUDA(cudaMemcpyAsync(p, h, count * sizeof(T), cudaMemcpyHostToDevice, s));
+  }
+  void upload(const std::vector<T>& v, cudaStream_t s) {
+    if (v.size() != n) alloc(v.size());
+    upload(v.data(), v.size(), s);
+  }
+  void download(T* h, size_t count, cudaStream_t s) const {
+    VG_CUDA(cudaMemcpyAsync(h, p, count * sizeof(T), cudaMemcpyDeviceToHost, s));
+  }
+  ~DArr() { release(); }
+  DArr() = default;
+  DArr(const DArr&) = delete;
+  DArr& operator=(const DArr&) = delete;
+};
+
+// Scalars the SLE fixed point and the stepper decide on, kept on the device and
+// read back as one small struct when the host needs a decision.
+struct SleScalars {
+  double C_int, ice_int, zeta_int, Cs_int, dphi, dmax, smax, mass_Cs;
+  int flips, pad;
+  unsigned long long mem_norm_bits;  // max |memory| of the state the last advance wrote
+};
+
+struct Grid {
+  int lmax, mmax, M, nlat, nphi, ng, nlm;
+  std::vector<double> x, colat, sint, wts;  // host
+  DArr<double> d_wts, d_sint, d_cott, d_invsin;
+  DArr<double> d_plm, d_dplm;   // (nlm, nlat)
+  DArr<double> d_cos, d_sin;    // (nphi) twiddles cos/sin(2 pi t / nphi)
+  DArr<int> d_lm_m;             // lm -> m
+  DArr<int> d_lm_l;             // lm -> l
+  DArr<int> d_mbeg;             // m -> first lm (size M+1)
+};
+
+}  // namespace vg
+
+struct vg_handle {
+  vg_params p;
+  std::string err;
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  // sizes
+  int nr = 0, ne = 0, ndof = 0, nk = 0, ne3d = 0;
+  int kl = 0, ku = 0, kv = 0, ldab = 0;  // band of degrees >= 2
+  int ns1 = 0, ldab1 = 0, kv1 = 0, kl1 = 0;  // degree-1 bordered system
+  double a = 0, g = 0, dt = 0, time_s = 0, time_yr = 0, max_rate = 0;
+  vg::Grid grid;
+  // host copies of setup data
+  std::vector<double> r, mu, MkPerDt;
+  std::vector<int> elem_layer, kdeg_h, k2lm_h, kbeg_h;
+  std::vector<char> active1d_h;
+  std::vector<int> e3d_h;
+  // operators
+  vg::DArr<double> d_ab, d_dr, d_dc;  // degrees 2..lmax
+  vg::DArr<int> d_ipiv;
+  vg::DArr<double> d_ab1, d_dr1, d_dc1, d_null1;  // degree 1
+  vg::DArr<int> d_ipiv1;
+  // per-element / per-degree constants
+  vg::DArr<double> d_r, d_mu, d_MkPerDt;
+  vg::DArr<char> d_active1d;
+  vg::DArr<double> d_Jr, d_nrmc, d_sa, d_sb, d_sc, d_gu, d_gn, d_gv, d_xUn, d_xVn;
+  vg::DArr<int> d_kdeg, d_k2lm, d_lm2k;
+  // state
+  vg::DArr<double> d_mem[2];
+  int cur = 0;
+  vg::DArr<double> d_dUn, d_dVn, d_drift;  // drift: dUa re,im, dFa re,im, dVa re,im (6*nk)
+  vg::DArr<double> d_mnorm, d_xs;          // per-slot memory norm (2 buffers x nk); band-solve scratch
+  vg::DArr<unsigned long long> d_maxbits;  // max |memory| of each buffer (double bits)
+  vg::DArr<vg::SleScalars> d_sc_;
+  vg::SleScalars* h_sc = nullptr;  // pinned
+  double mem_norm = 0.0;           // ||state cur||_inf (host copy)
+  // 3-D
+  bool lat_visc = false;
+  vg::DArr<double> d_MkPerDt3;  // (ne3d, nlat, nphi)
+  vg::DArr<int> d_e3d;
+  vg::DArr<double> d_G6, d_H6, d_n6;  // spin-2 kernels (nlm, nlat), norms (lmax+1)
+  vg::DArr<double> d_X, d_Y, d_dy;    // 3-D work buffers
+  // sea-level equation fields (ng each unless stated)
+  vg::DArr<double> d_z_bed_eq, d_h_ice_eq, d_h_ice, d_ice1, d_ice_now, d_dice_now, d_rsl, d_rsl_n,
+      d_C, d_C0, d_C_next, d_dig, d_wcorr, d_Sraw, d_zbed, d_tmp;
+  vg::DArr<double> d_F;        // Fourier coefficients (2 * M * nlat * batch)
+  vg::DArr<double> d_Gs;       // Legendre sums (2 * M * nlat * batch)
+  vg::DArr<double> d_sigma, d_ulm, d_nlm;  // spectra (2*nlm)
+  vg::DArr<double> d_rowpart;  // per-row partial sums (8 * nlat)
+  // counters
+  long long n_accept = 0, n_reject = 0, n_solve = 0, n_drift_solved = 0;
+  int n_sub_last = 0, n_outer_last = 0, n_inner_last = 0, n_flip_last = 0;
+  double worst_mass_resid = 0, bsl = 0;
+  bool have_reference = false;
+};
+
+namespace vg {
+// setup (vg_setup.cu)
+void setup_handle(vg_handle* h);
+void build_grid(Grid& G, int lmax, int nlat, int nphi, cudaStream_t s);
+// response kernels (vg_radial.cu)
+void launch_drift(vg_handle* h);
+void launch_advance_1d(vg_handle* h, const double* d_sigma, double dt);
+void launch_apply(vg_handle* h, const double* d_sigma, double* d_u, double* d_n);
+void compute_mem_norm(vg_handle* h, int buf);
+double read_mem_norm(vg_handle* h, int buf);
+// SHT (vg_sht.cu)
+void fourier_analysis_dev(vg_handle* h, const double* d_f, int batch, double* d_F);
+void legendre_analysis_dev(vg_handle* h, const double* d_F, int batch, double* d_q);
+void legendre_synth_dev(vg_handle* h, const double* d_q, int batch, double* d_G);
+void fourier_synth_dev(vg_handle* h, const double* d_G, int batch, double* d_f);
+void sht_analysis_dev(vg_handle* h, const double* d_f, double* d_q, int batch);
+void sht_synthesis_dev(vg_handle* h, const double* d_q, double* d_f, int batch);
+// SLE + stepper (vg_sle.cu)
+void sle_solve_dev(vg_handle* h, double dt, bool report_only);
+void update_dev(vg_handle* h, const double* d_ice1, double dt_yr);
+void update_bsl(vg_handle* h);
+// 3-D (vg_visc3d.cu)
+void visc3d_enable(vg_handle* h, const double* pert_host);
+void visc3d_advance(vg_handle* h, const double* d_sigma, double dt);
+// misc
+void sync_scalars(vg_handle* h);
+}  // namespace vg

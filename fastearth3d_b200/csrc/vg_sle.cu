@@ -1,0 +1,417 @@
+// Sea-level equation on the device (src/vilma_sle.f90:124-425) and the
+// explicit sub-stepping driver with its reactive guard (src/vilma_timestep.f90:
+// 79-227), i.e. one solid_earth_update (src/vilma_coupling.f90:336-437) with
+// every field resident in HBM. The host only takes the scalar decisions the
+// reference takes (coastline, inner convergence, guard), from one small
+// device-to-host read each.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+
+#include "vg_device.cuh"
+#include "vg_internal.cuh"
+
+namespace vg {
+
+enum { RP_C = 0, RP_DIG, RP_ZETA, RP_CS, RP_DMAX, RP_SMAX, RP_FLIP, RP_MASS, RP_N };
+
+__device__ __forceinline__ double ocean(double topo, double ice) {
+  return (topo < 0.0 && RHO_ICE * ice < -RHO_WATER * topo) ? 1.0 : 0.0;
+}
+
+__global__ void k_ice_interp(int ng, double frac, const double* __restrict__ ice0, const double* __restrict__ ice1,
+                             const double* __restrict__ ice_ref, double* __restrict__ ice_now,
+                             double* __restrict__ dice_now) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= ng) return;
+  double v = ice0[i] + frac * (ice1[i] - ice0[i]);
+  ice_now[i] = v;
+  dice_now[i] = v - ice_ref[i];
+}
+
+// C0 = ocean_function(topo0, ice - d_ice)  (src/vilma_sle.f90:212)
+__global__ void k_ocean0(int ng, const double* __restrict__ topo0, const double* __restrict__ ice,
+                         const double* __restrict__ dice, double* __restrict__ C0) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < ng) C0[i] = ocean(topo0[i], ice[i] - dice[i]);
+}
+// C = ocean_function(topo0 - rsl, ice)
+__global__ void k_ocean(int ng, const double* __restrict__ topo0, const double* __restrict__ rsl,
+                        const double* __restrict__ ice, double* __restrict__ C) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < ng) C[i] = ocean(topo0[i] - rsl[i], ice[i]);
+}
+
+// grounded-ice increment and the per-row sums of C, dIg, topo0 (C - C0)
+__global__ void k_pass_setup(int nphi, const double* __restrict__ ice, const double* __restrict__ dice,
+                             const double* __restrict__ C, const double* __restrict__ C0,
+                             const double* __restrict__ topo0, double* __restrict__ dig,
+                             double* __restrict__ rowpart, int nlat) {
+  __shared__ double red[128];
+  int j = blockIdx.x;
+  double sc = 0.0, sd = 0.0, sz = 0.0;
+  for (int i = threadIdx.x; i < nphi; i += blockDim.x) {
+    size_t p = (size_t)j * nphi + i;
+    double d = ice[p] * (1.0 - C[p]) - (ice[p] - dice[p]) * (1.0 - C0[p]);
+    dig[p] = d;
+    sc += C[p];
+    sd += d;
+    sz += topo0[p] * (C[p] - C0[p]);
+  }
+  sc = block_sum(sc, red);
+  sd = block_sum(sd, red);
+  sz = block_sum(sz, red);
+  if (threadIdx.x == 0) {
+    rowpart[RP_C * nlat + j] = sc;
+    rowpart[RP_DIG * nlat + j] = sd;
+    rowpart[RP_ZETA * nlat + j] = sz;
+  }
+}
+
+// surface integral of a row-sum vector: sum_j w_j row_j * 2 pi / nphi (src/vilma_sht.f90:184-202)
+__device__ __forceinline__ double integrate_rows(const double* row, const double* w, int nlat, double dlon) {
+  double total = 0.0;
+  for (int j = 0; j < nlat; ++j) total += w[j] * row[j] * dlon;
+  return total;
+}
+
+__global__ void k_finalize_C(SleScalars* sc, const double* __restrict__ rowpart, const double* __restrict__ w,
+                             int nlat, double dlon) {
+  if (threadIdx.x == 0) sc->C_int = integrate_rows(rowpart + RP_C * nlat, w, nlat, dlon);
+}
+__global__ void k_finalize_pass(SleScalars* sc, const double* __restrict__ rowpart, const double* __restrict__ w,
+                                int nlat, double dlon, int subgrid) {
+  if (threadIdx.x == 0) {
+    sc->ice_int = -(RHO_ICE / RHO_WATER) * integrate_rows(rowpart + RP_DIG * nlat, w, nlat, dlon);
+    sc->zeta_int = subgrid ? integrate_rows(rowpart + RP_ZETA * nlat, w, nlat, dlon) : 0.0;
+  }
+}
+__global__ void k_wcorr(int ng, int subgrid, const double* __restrict__ topo0, const double* __restrict__ C,
+                        const double* __restrict__ C0, double* __restrict__ wcorr) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < ng) wcorr[i] = subgrid ? -RHO_WATER * topo0[i] * (C[i] - C0[i]) : 0.0;
+}
+
+// total surface load (assemble_load, src/vilma_sle.f90:387-403) and its longitude transform
+__global__ void k_load_fourier(int nphi, int nlat, int M, const double* __restrict__ dig,
+                               const double* __restrict__ C, const double* __restrict__ rsl,
+                               const double* __restrict__ wcorr, const double* __restrict__ cs,
+                               const double* __restrict__ sn, double* __restrict__ F) {
+  extern __shared__ double row[];
+  int j = blockIdx.x;
+  for (int i = threadIdx.x; i < nphi; i += blockDim.x) {
+    size_t p = (size_t)j * nphi + i;
+    row[i] = RHO_ICE * dig[p] + RHO_WATER * (C[p] * rsl[p]) + wcorr[p];
+  }
+  __syncthreads();
+  row_fourier_analysis(row, nphi, M, cs, sn, F + (size_t)j * 2, nlat);
+}
+
+// u and N rows from their Legendre sums, Sraw = N - u (+ s_rot), row sum of C Sraw
+__global__ void k_synth_sraw(int nphi, int nlat, int M, const double* __restrict__ G, const double* __restrict__ cs,
+                             const double* __restrict__ sn, const double* __restrict__ C,
+                             const double* __restrict__ srot, double* __restrict__ Sraw,
+                             double* __restrict__ rowpart) {
+  extern __shared__ double sh[];  // Gu[M][2], Gn[M][2]
+  __shared__ double red[128];
+  int j = blockIdx.x;
+  double* Gu = sh;
+  double* Gn = sh + 2 * M;
+  for (int m = threadIdx.x; m < M; m += blockDim.x) {
+    Gu[2 * m] = G[((size_t)m * nlat + j) * 2];
+    Gu[2 * m + 1] = G[((size_t)m * nlat + j) * 2 + 1];
+    Gn[2 * m] = G[(((size_t)M + m) * nlat + j) * 2];
+    Gn[2 * m + 1] = G[(((size_t)M + m) * nlat + j) * 2 + 1];
+  }
+  __syncthreads();
+  double acc = 0.0;
+  for (int i = threadIdx.x; i < nphi; i += blockDim.x) {
+    size_t p = (size_t)j * nphi + i;
+    double u = row_fourier_synth_at(Gu, M, i, nphi, cs, sn);
+    double N = row_fourier_synth_at(Gn, M, i, nphi, cs, sn);
+    double s = N - u;
+    if (srot) s = s + srot[p];
+    Sraw[p] = s;
+    acc += C[p] * s;
+  }
+  acc = block_sum(acc, red);
+  if (threadIdx.x == 0) rowpart[RP_CS * nlat + j] = acc;
+}
+
+__global__ void k_dphi(SleScalars* sc, const double* __restrict__ rowpart, const double* __restrict__ w, int nlat,
+                       double dlon) {
+  if (threadIdx.x == 0) {
+    double Cs = integrate_rows(rowpart + RP_CS * nlat, w, nlat, dlon);
+    sc->Cs_int = Cs;
+    sc->dphi = (sc->ice_int - Cs + sc->zeta_int) / sc->C_int;
+  }
+}
+
+__global__ void k_rsl_update(int nphi, const SleScalars* __restrict__ sc, const double* __restrict__ Sraw,
+                             const double* __restrict__ C, double* __restrict__ rsl, double* __restrict__ rowpart,
+                             int nlat) {
+  __shared__ double red[128];
+  int j = blockIdx.x;
+  double dphi = sc->dphi, dmax = 0.0, smax = 0.0;
+  for (int i = threadIdx.x; i < nphi; i += blockDim.x) {
+    size_t p = (size_t)j * nphi + i;
+    double rn = Sraw[p] + dphi;
+    dmax = nanmax(dmax, fabs(C[p] * (rn - rsl[p])));
+    rsl[p] = rn;
+    smax = nanmax(smax, fabs(C[p] * rn));
+  }
+  dmax = block_max(dmax, red);
+  smax = block_max(smax, red);
+  if (threadIdx.x == 0) {
+    rowpart[RP_DMAX * nlat + j] = dmax;
+    rowpart[RP_SMAX * nlat + j] = smax;
+  }
+}
+
+__global__ void k_conv(SleScalars* sc, const double* __restrict__ rowpart, int nlat) {
+  if (threadIdx.x == 0) {
+    double dmax = 0.0, smax = 0.0;
+    for (int j = 0; j < nlat; ++j) {
+      dmax = nanmax(dmax, rowpart[RP_DMAX * nlat + j]);
+      smax = nanmax(smax, rowpart[RP_SMAX * nlat + j]);
+    }
+    sc->dmax = dmax;
+    sc->smax = smax;
+  }
+}
+
+// migrated coastline and the number of cells that changed state
+__global__ void k_coast(int nphi, const double* __restrict__ topo0, const double* __restrict__ rsl,
+                        const double* __restrict__ ice, const double* __restrict__ C, double* __restrict__ Cn,
+                        double* __restrict__ rowpart, int nlat) {
+  __shared__ double red[128];
+  int j = blockIdx.x;
+  double cnt = 0.0;
+  for (int i = threadIdx.x; i < nphi; i += blockDim.x) {
+    size_t p = (size_t)j * nphi + i;
+    double c = ocean(topo0[p] - rsl[p], ice[p]);
+    Cn[p] = c;
+    cnt += (c != C[p]) ? 1.0 : 0.0;
+  }
+  cnt = block_sum(cnt, red);
+  if (threadIdx.x == 0) rowpart[RP_FLIP * nlat + j] = cnt;
+}
+__global__ void k_flips(SleScalars* sc, const double* __restrict__ rowpart, int nlat) {
+  if (threadIdx.x == 0) {
+    double t = 0.0;
+    for (int j = 0; j < nlat; ++j) t += rowpart[RP_FLIP * nlat + j];
+    sc->flips = (int)t;
+  }
+}
+
+// row sums of a * b (b may be null: sum of a), into rowpart slot
+__global__ void k_rowsum(int nphi, const double* __restrict__ a, const double* __restrict__ b,
+                         double* __restrict__ out) {
+  __shared__ double red[128];
+  int j = blockIdx.x;
+  double s = 0.0;
+  for (int i = threadIdx.x; i < nphi; i += blockDim.x) {
+    size_t p = (size_t)j * nphi + i;
+    s += b ? a[p] * b[p] : a[p];
+  }
+  s = block_sum(s, red);
+  if (threadIdx.x == 0) out[j] = s;
+}
+__global__ void k_mass(SleScalars* sc, const double* __restrict__ rowpart, const double* __restrict__ w, int nlat,
+                       double dlon) {
+  if (threadIdx.x == 0) sc->mass_Cs = integrate_rows(rowpart + RP_MASS * nlat, w, nlat, dlon) - sc->zeta_int;
+}
+
+// z_bed = z_bed_eq - rsl (src/vilma_coupling.f90:428)
+__global__ void k_zbed(int ng, const double* __restrict__ zeq, const double* __restrict__ rsl,
+                       double* __restrict__ zb) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < ng) zb[i] = zeq[i] - rsl[i];
+}
+// row sums of C and of h_ice (1 - C) - h_ice_eq (1 - C0), for update_bsl
+__global__ void k_bsl_rows(int nphi, const double* __restrict__ hi, const double* __restrict__ hq,
+                           const double* __restrict__ C, const double* __restrict__ C0, double* __restrict__ rowpart,
+                           int nlat) {
+  __shared__ double red[128];
+  int j = blockIdx.x;
+  double sc = 0.0, st = 0.0;
+  for (int i = threadIdx.x; i < nphi; i += blockDim.x) {
+    size_t p = (size_t)j * nphi + i;
+    sc += C[p];
+    st += hi[p] * (1.0 - C[p]) - hq[p] * (1.0 - C0[p]);
+  }
+  sc = block_sum(sc, red);
+  st = block_sum(st, red);
+  if (threadIdx.x == 0) {
+    rowpart[RP_C * nlat + j] = sc;
+    rowpart[RP_DIG * nlat + j] = st;
+  }
+}
+
+static void read_scalars(vg_handle* h) {
+  VG_CUDA(cudaMemcpyAsync(h->h_sc, h->d_sc_.p, sizeof(SleScalars), cudaMemcpyDeviceToHost, h->stream));
+  VG_CUDA(cudaStreamSynchronize(h->stream));
+}
+
+void sync_scalars(vg_handle* h) { read_scalars(h); }
+
+// One sea-level solve with the memory advance at its end (FE: a single
+// co-convergence pass), src/vilma_sle.f90:124-405. Writes the advanced memory
+// into the other state buffer; the caller decides to keep or drop it.
+void sle_solve_dev(vg_handle* h, double dt, bool report_only) {
+  const Grid& G = h->grid;
+  const int ng = G.ng, nlat = G.nlat, nphi = G.nphi, M = G.M, nlm = G.nlm;
+  const double dlon = 2.0 * PI / (double)nphi;
+  cudaStream_t s = h->stream;
+  const vg_params& p = h->p;
+  SleScalars* sc = h->d_sc_.p;
+  double* rp = h->d_rowpart.p;
+  const int eb = 256, eg = (ng + eb - 1) / eb;
+  if (!p.sle_warm_start) VG_CUDA(cudaMemsetAsync(h->d_rsl.p, 0, ng * sizeof(double), s));
+  VG_CUDA(cudaMemsetAsync(h->d_wcorr.p, 0, ng * sizeof(double), s));
+  VG_CUDA(cudaMemsetAsync(sc, 0, sizeof(SleScalars), s));
+  k_ocean0<<<eg, eb, 0, s>>>(ng, h->d_z_bed_eq.p, h->d_ice_now.p, h->d_dice_now.p, h->d_C0.p);
+  launch_drift(h);  // response_begin_step
+  h->n_inner_last = 0;
+  h->n_flip_last = 0;
+  for (int io = 1; io <= p.sle_n_outer; ++io) {
+    if (p.sle_fixed_ocean) {
+      if (io == 1) VG_CUDA(cudaMemcpyAsync(h->d_C.p, h->d_C0.p, ng * sizeof(double), cudaMemcpyDeviceToDevice, s));
+    } else if (io == 1) {
+      k_ocean<<<eg, eb, 0, s>>>(ng, h->d_z_bed_eq.p, h->d_rsl.p, h->d_ice_now.p, h->d_C.p);
+    } else {
+      VG_CUDA(cudaMemcpyAsync(h->d_C.p, h->d_C_next.p, ng * sizeof(double), cudaMemcpyDeviceToDevice, s));
+    }
+    k_pass_setup<<<nlat, 128, 0, s>>>(nphi, h->d_ice_now.p, h->d_dice_now.p, h->d_C.p, h->d_C0.p, h->d_z_bed_eq.p,
+                                      h->d_dig.p, rp, nlat);
+    k_finalize_C<<<1, 32, 0, s>>>(sc, rp, G.d_wts.p, nlat, dlon);
+    read_scalars(h);
+    if (h->h_sc->C_int <= 0.0) break;  // no ocean: nothing to redistribute
+    k_finalize_pass<<<1, 32, 0, s>>>(sc, rp, G.d_wts.p, nlat, dlon, p.sle_subgrid);
+    k_wcorr<<<eg, eb, 0, s>>>(ng, p.sle_subgrid, h->d_z_bed_eq.p, h->d_C.p, h->d_C0.p, h->d_wcorr.p);
+    for (int ii = 1; ii <= p.sle_n_inner; ++ii) {
+      k_load_fourier<<<nlat, 128, nphi * sizeof(double), s>>>(nphi, nlat, M, h->d_dig.p, h->d_C.p, h->d_rsl.p,
+                                                              h->d_wcorr.p, G.d_cos.p, G.d_sin.p, h->d_F.p);
+      legendre_analysis_dev(h, h->d_F.p, 1, h->d_sigma.p);
+      launch_apply(h, h->d_sigma.p, h->d_ulm.p, h->d_ulm.p + 2 * (size_t)nlm);
+      legendre_synth_dev(h, h->d_ulm.p, 2, h->d_Gs.p);
+      k_synth_sraw<<<nlat, 128, 4 * M * sizeof(double), s>>>(nphi, nlat, M, h->d_Gs.p, G.d_cos.p, G.d_sin.p,
+                                                             h->d_C.p, nullptr, h->d_Sraw.p, rp);
+      k_dphi<<<1, 32, 0, s>>>(sc, rp, G.d_wts.p, nlat, dlon);
+      k_rsl_update<<<nlat, 128, 0, s>>>(nphi, sc, h->d_Sraw.p, h->d_C.p, h->d_rsl.p, rp, nlat);
+      k_conv<<<1, 32, 0, s>>>(sc, rp, nlat);
+      read_scalars(h);
+      h->n_inner_last = ii;
+      if (h->h_sc->dmax <= p.sle_tol * std::max(h->h_sc->smax, TINY)) break;
+    }
+    h->n_outer_last = io;
+    if (p.sle_fixed_ocean) break;
+    k_coast<<<nlat, 128, 0, s>>>(nphi, h->d_z_bed_eq.p, h->d_rsl.p, h->d_ice_now.p, h->d_C.p, h->d_C_next.p, rp,
+                                 nlat);
+    k_flips<<<1, 32, 0, s>>>(sc, rp, nlat);
+    read_scalars(h);
+    h->n_flip_last = h->h_sc->flips;
+    if (h->h_sc->flips == 0) break;
+  }
+  // closing load, its analysis, and the memory advance (src/vilma_sle.f90:353-358)
+  k_load_fourier<<<nlat, 128, nphi * sizeof(double), s>>>(nphi, nlat, M, h->d_dig.p, h->d_C.p, h->d_rsl.p,
+                                                          h->d_wcorr.p, G.d_cos.p, G.d_sin.p, h->d_F.p);
+  legendre_analysis_dev(h, h->d_F.p, 1, h->d_sigma.p);
+  if (!report_only) {
+    if (h->lat_visc) visc3d_advance(h, h->d_sigma.p, dt);
+    launch_advance_1d(h, h->d_sigma.p, dt);
+  }
+  k_rowsum<<<nlat, 128, 0, s>>>(nphi, h->d_C.p, h->d_rsl.p, rp + RP_MASS * nlat);
+  k_mass<<<1, 32, 0, s>>>(sc, rp, G.d_wts.p, nlat, dlon);
+}
+
+// solid_earth_update without rotation; d_ice1 is the interval-end ice on the device
+void update_dev(vg_handle* h, const double* d_ice1, double dt_yr) {
+  const Grid& G = h->grid;
+  const int ng = G.ng;
+  cudaStream_t s = h->stream;
+  const vg_params& p = h->p;
+  const double dt = dt_yr * SEC_PER_YEAR;
+  const double t0 = h->time_yr * SEC_PER_YEAR, t1 = t0 + dt, span = t1 - t0;
+  const int eb = 256, eg = (ng + eb - 1) / eb;
+  h->worst_mass_resid = 0.0;
+  auto mass_resid = [&]() {
+    read_scalars(h);
+    double ice_int = h->h_sc->ice_int, Cs = h->h_sc->mass_Cs;
+    return std::fabs(ice_int) > 0.0 ? std::fabs(Cs - ice_int) / std::fabs(ice_int) : std::fabs(Cs);
+  };
+  if (span <= 0.0) {
+    k_ice_interp<<<eg, eb, 0, s>>>(ng, 0.0, h->d_h_ice.p, h->d_h_ice.p, h->d_h_ice_eq.p, h->d_ice_now.p,
+                                   h->d_dice_now.p);
+    sle_solve_dev(h, 0.0, true);
+    h->worst_mass_resid = mass_resid();
+  } else {
+    double rate = h->max_rate;
+    double dt_stab = rate > 0.0 ? p.cfl / rate : span;
+    dt_stab = std::min(dt_stab, p.dt_max);
+    if (p.dt_min > 0.0) dt_stab = std::max(dt_stab, p.dt_min);
+    int n_sub = std::max(1, (int)std::ceil(span / dt_stab - 1.0e-9));
+    h->n_sub_last = n_sub;
+    double dtc = span / (double)n_sub, t = t0;
+    double tau_run = h->mem_norm;
+    while (true) {
+      if (t >= t1 - 1.0e-9 * span) break;
+      dtc = std::min(dtc, t1 - t);
+      VG_CUDA(cudaMemcpyAsync(h->d_rsl_n.p, h->d_rsl.p, ng * sizeof(double), cudaMemcpyDeviceToDevice, s));
+      double tau0 = h->mem_norm;
+      double frac = (t + dtc - t0) / span;
+      k_ice_interp<<<eg, eb, 0, s>>>(ng, frac, h->d_h_ice.p, d_ice1, h->d_h_ice_eq.p, h->d_ice_now.p,
+                                     h->d_dice_now.p);
+      VG_CUDA(cudaGetLastError());
+      h->n_solve++;
+      sle_solve_dev(h, dtc, false);
+      h->worst_mass_resid = std::max(h->worst_mass_resid, mass_resid());
+      int nxt = 1 - h->cur;
+      double err_inf = read_mem_norm(h, nxt);
+      bool finite = err_inf <= HUGE_;
+      double scale = std::max(tau0, tau_run);
+      bool accept = scale <= 0.0 ? finite : (finite && err_inf <= p.guard_growth * scale);
+      if (accept) {
+        h->cur = nxt;
+        h->mem_norm = err_inf;
+        h->time_s += dtc;
+        tau_run = std::max(tau_run, err_inf);
+        t = t + dtc;
+        h->n_accept++;
+        dtc = std::min(span / (double)n_sub, 2.0 * dtc);
+      } else {
+        VG_CUDA(cudaMemcpyAsync(h->d_rsl.p, h->d_rsl_n.p, ng * sizeof(double), cudaMemcpyDeviceToDevice, s));
+        h->n_reject++;
+        dtc = 0.5 * dtc;
+        if (dtc <= 1.0e-12 * span)
+          throw Error("vilma_timestep: explicit guard sub-step collapsed (viscosity too stiff for FE)");
+      }
+    }
+  }
+  VG_CUDA(cudaMemcpyAsync(h->d_h_ice.p, d_ice1, ng * sizeof(double), cudaMemcpyDeviceToDevice, s));
+  k_zbed<<<eg, eb, 0, s>>>(ng, h->d_z_bed_eq.p, h->d_rsl.p, h->d_zbed.p);
+  VG_CUDA(cudaGetLastError());
+  h->time_yr += dt_yr;
+  update_bsl(h);
+}
+
+// src/vilma_coupling.f90:572-597 update_bsl
+void update_bsl(vg_handle* h) {
+  const Grid& G = h->grid;
+  const int nlat = G.nlat, nphi = G.nphi;
+  cudaStream_t s = h->stream;
+  double* rp = h->d_rowpart.p;
+  k_bsl_rows<<<nlat, 128, 0, s>>>(nphi, h->d_h_ice.p, h->d_h_ice_eq.p, h->d_C.p, h->d_C0.p, rp, nlat);
+  VG_CUDA(cudaGetLastError());
+  std::vector<double> rows((size_t)RP_N * nlat);
+  VG_CUDA(cudaMemcpyAsync(rows.data(), rp, rows.size() * sizeof(double), cudaMemcpyDeviceToHost, s));
+  VG_CUDA(cudaStreamSynchronize(s));
+  double dlon = 2.0 * PI / (double)nphi, c_int = 0.0, t_int = 0.0;
+  for (int j = 0; j < nlat; ++j) {
+    c_int += G.wts[j] * rows[RP_C * nlat + j] * dlon;
+    t_int += G.wts[j] * rows[RP_DIG * nlat + j] * dlon;
+  }
+  h->bsl = c_int > 0.0 ? -(RHO_ICE / RHO_WATER) * t_int / c_int : 0.0;
+}
+
+}  // namespace vg

@@ -1,0 +1,190 @@
+"""ctypes binding of the CUDA library (libvilma_gpu.so) through its C-ABI.
+
+This is the same binding a Python host would write against include/vilma_gpu.h
+(the Fortran host binds the same symbols through iso_c_binding). There is no
+CPU path: loading fails loudly if the library is missing.
+"""
+import ctypes as C
+import os
+
+import numpy as np
+
+from .abi import VgInfo, VgParams
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libvilma_gpu.so")
+_lib = None
+_P = C.POINTER(C.c_double)
+_VP = C.c_void_p
+
+_SIGS = [
+    ("vg_params_default", [C.POINTER(VgParams)]),
+    ("vg_create", [C.POINTER(VgParams), C.POINTER(_VP)]),
+    ("vg_destroy", [_VP]),
+    ("vg_set_reference", [_VP, _P, _P, _P]),
+    ("vg_enable_visc3d", [_VP, _P]),
+    ("vg_update", [_VP, _P, C.c_double]),
+    ("vg_update_device", [_VP, C.c_void_p, C.c_double]),
+    ("vg_get_fields", [_VP, _P, _P, _P, _P]),
+    ("vg_rsl_device", [_VP, C.POINTER(C.c_void_p)]),
+    ("vg_get_info", [_VP, C.POINTER(VgInfo)]),
+    ("vg_response_set_dt", [_VP, C.c_double]),
+    ("vg_response_begin_step", [_VP]),
+    ("vg_response_apply", [_VP, _P, _P, _P]),
+    ("vg_response_advance", [_VP, _P]),
+    ("vg_get_gains", [_VP, _P, _P, _P]),
+    ("vg_get_drift", [_VP, _P, _P, _P]),
+    ("vg_get_state", [_VP, _P, _P, _P, _P, _P, _P, _P]),
+    ("vg_set_state", [_VP, _P, _P, _P, _P, _P, _P, C.c_double]),
+    ("vg_sht_analysis", [_VP, _P, _P]),
+    ("vg_sht_synthesis", [_VP, _P, _P]),
+]
+EXPORTS = [n for n, _ in _SIGS] + ["vg_last_error"]
+
+
+def lib():
+    """Load libvilma_gpu.so (raises if it was not built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(f"{LIB_PATH} is missing: build it with `python -m fastearth3d_b200.build`")
+        L = C.CDLL(LIB_PATH)
+        for name, args in _SIGS:
+            f = getattr(L, name)
+            f.argtypes = args
+            f.restype = C.c_int
+        L.vg_last_error.argtypes = [_VP]
+        L.vg_last_error.restype = C.c_char_p
+        _lib = L
+    return _lib
+
+
+def ptr(a):
+    if a is None:
+        return None
+    assert a.dtype == np.float64 and a.flags.c_contiguous
+    return a.ctypes.data_as(_P)
+
+
+def default_params():
+    p = VgParams()
+    lib().vg_params_default(C.byref(p))
+    return p
+
+
+class VilmaError(RuntimeError):
+    pass
+
+
+def _pack(z):
+    out = np.zeros(2 * z.size)
+    out[0::2], out[1::2] = z.real, z.imag
+    return out
+
+
+def _unpack(a):
+    return a[0::2] + 1j * a[1::2]
+
+
+class Model:
+    """One model instance on the current CUDA device (vg_create ... vg_destroy)."""
+
+    def __init__(self, p):
+        self.p = p
+        h = _VP()
+        rc = lib().vg_create(C.byref(p), C.byref(h))
+        if rc != 0:
+            raise VilmaError(lib().vg_last_error(None).decode())
+        self.h = h
+        info = self.info()
+        self.nlm, self.nk, self.ne, self.nr = info.nlm, info.nk, info.ne, info.nr
+        self.ng = p.nphi * p.nlat
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().vg_destroy(self.h)
+            self.h = None
+
+    __del__ = close
+
+    def _c(self, rc):
+        if rc != 0:
+            raise VilmaError(lib().vg_last_error(self.h).decode())
+
+    def info(self):
+        i = VgInfo()
+        self._c(lib().vg_get_info(self.h, C.byref(i)))
+        return i
+
+    def set_reference(self, z_bed_eq, h_ice_eq, h_ice_init=None):
+        f = lambda a: None if a is None else np.ascontiguousarray(a, dtype=np.float64)
+        self._c(lib().vg_set_reference(self.h, ptr(f(z_bed_eq)), ptr(f(h_ice_eq)), ptr(f(h_ice_init))))
+
+    def enable_visc3d(self, pert):
+        self._c(lib().vg_enable_visc3d(self.h, ptr(np.ascontiguousarray(pert, dtype=np.float64))))
+
+    def update(self, h_ice, dt_yr):
+        self._c(lib().vg_update(self.h, ptr(np.ascontiguousarray(h_ice, dtype=np.float64)), dt_yr))
+
+    def update_device(self, d_h_ice_ptr, dt_yr):
+        self._c(lib().vg_update_device(self.h, C.c_void_p(d_h_ice_ptr), dt_yr))
+
+    def rsl_device_ptr(self):
+        p = C.c_void_p()
+        self._c(lib().vg_rsl_device(self.h, C.byref(p)))
+        return p.value
+
+    def fields(self):
+        rsl, zb, Cf = np.zeros(self.ng), np.zeros(self.ng), np.zeros(self.ng)
+        sig = np.zeros(2 * self.nlm)
+        self._c(lib().vg_get_fields(self.h, ptr(rsl), ptr(zb), ptr(Cf), ptr(sig)))
+        return rsl, zb, Cf, _unpack(sig)
+
+    def state(self):
+        n = 4 * self.ne * self.nk
+        arrs = [np.zeros(n) for _ in range(6)]
+        t = C.c_double(0)
+        self._c(lib().vg_get_state(self.h, *[ptr(a) for a in arrs], C.byref(t)))
+        return arrs, t.value
+
+    def set_state(self, arrs, t):
+        arrs = [np.ascontiguousarray(a, dtype=np.float64) for a in arrs]
+        self._c(lib().vg_set_state(self.h, *[ptr(a) for a in arrs], t))
+
+    def set_dt(self, dt_s):
+        self._c(lib().vg_response_set_dt(self.h, dt_s))
+
+    def begin_step(self):
+        self._c(lib().vg_response_begin_step(self.h))
+
+    def apply(self, sigma):
+        s = _pack(np.asarray(sigma, dtype=complex))
+        u, n = np.zeros(2 * self.nlm), np.zeros(2 * self.nlm)
+        self._c(lib().vg_response_apply(self.h, ptr(s), ptr(u), ptr(n)))
+        return _unpack(u), _unpack(n)
+
+    def advance(self, sigma):
+        s = _pack(np.asarray(sigma, dtype=complex))
+        self._c(lib().vg_response_advance(self.h, ptr(s)))
+
+    def gains(self):
+        L = self.p.lmax + 1
+        gu, gn, gv = np.zeros(L), np.zeros(L), np.zeros(L)
+        self._c(lib().vg_get_gains(self.h, ptr(gu), ptr(gn), ptr(gv)))
+        return gu, gn, gv
+
+    def drift(self):
+        a = [np.zeros(2 * self.nk) for _ in range(3)]
+        self._c(lib().vg_get_drift(self.h, *[ptr(x) for x in a]))
+        return [_unpack(x) for x in a]
+
+    def analysis(self, f):
+        q = np.zeros(2 * self.nlm)
+        self._c(lib().vg_sht_analysis(self.h, ptr(np.ascontiguousarray(f, dtype=np.float64)), ptr(q)))
+        return _unpack(q)
+
+    def synthesis(self, q):
+        s = _pack(np.asarray(q, dtype=complex))
+        f = np.zeros(self.ng)
+        self._c(lib().vg_sht_synthesis(self.h, ptr(s), ptr(f)))
+        return f

@@ -1,0 +1,59 @@
+"""Extract the golden vectors the tests pin against from the reference tree.
+
+Reads (never copies wholesale) the vendored benchmark tables of the reference
+and writes the few numbers the tests use into tests/golden/*.json:
+
+* love_M3L70V01.json: elastic and fluid loading Love numbers h, l, k of the
+  M3-L70-V01 earth, degrees 1..64, from data/benchmarks/love_M3-L70-V01/
+  mod_M3-L70-V01 (normal-mode table; parsed as tests/test_benchmark_love.f90
+  read_ref does: 5 model lines, then per degree a header `n nmodes k h l`,
+  nmodes mode lines, and the fluid line `n nmodes k h l`).
+* disc_spada2011.json: vertical displacement u and geoid n of the Spada-2011
+  disc load at colatitude 0 and on the 0..20 deg profile, at t = 0, 1, 2, 5,
+  10 kyr (data/benchmarks/disc_spada2011/{u,n}_disc.txt, 201 rows x 6 times).
+
+Run in a container where the reference is mounted:
+    python tests/golden/make_golden.py /root/reference
+"""
+import json
+import os
+import sys
+
+import numpy as np
+
+
+def love(ref):
+    fn = os.path.join(ref, "data/benchmarks/love_M3-L70-V01/mod_M3-L70-V01")
+    lines = open(fn).read().split("\n")[5:]
+    out = {"elastic": {}, "fluid": {}}
+    i = 0
+    while i < len(lines):
+        t = lines[i].split()
+        if len(t) < 5:
+            break
+        n, nm = int(t[0]), int(t[1])
+        k, h, l = map(float, t[2:5])
+        if n <= 64:
+            out["elastic"][n] = {"h": h, "l": l, "k": k}
+        t = lines[i + 1 + nm].split()
+        k, h, l = map(float, t[2:5])
+        if n <= 64:
+            out["fluid"][n] = {"h": h, "l": l, "k": k}
+        i += nm + 2
+    return out
+
+
+def disc(ref):
+    d = os.path.join(ref, "data/benchmarks/disc_spada2011")
+    u = np.loadtxt(os.path.join(d, "u_disc.txt"))
+    n = np.loadtxt(os.path.join(d, "n_disc.txt"))
+    return {"theta_deg": [0.1 * i for i in range(201)], "times_kyr": [0, 1, 2, 5, 10, 100],
+            "u": u[:, :5].tolist(), "n": n[:, :1].tolist()}
+
+
+if __name__ == "__main__":
+    ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    here = os.path.dirname(os.path.abspath(__file__))
+    json.dump(love(ref), open(os.path.join(here, "love_M3L70V01.json"), "w"), indent=1)
+    json.dump(disc(ref), open(os.path.join(here, "disc_spada2011.json"), "w"))
+    print("wrote golden fixtures to", here)

@@ -1,0 +1,220 @@
+"""Parity of the CUDA path (called through the C-ABI) with the CPU oracle on
+the same seeded inputs, plus golden-vector checks of the GPU path itself.
+
+Tolerance: 1e-10 relative to the field's maximum for the FP64 path (the
+target the reference's north star sets for the plain FP64 path); the
+discrete decisions (skip gate, coastline, inner-loop exits) must agree.
+"""
+import json
+import os
+
+import numpy as np
+import pytest
+
+from fastearth3d_b200 import lib as vlib
+from fastearth3d_b200 import synth
+from fastearth3d_b200.abi import M3L70V01, set_layers
+from oracle import orc
+
+pytestmark = pytest.mark.gpu
+GOLD = os.path.join(os.path.dirname(__file__), "golden")
+TOL = 1e-10
+
+
+def rel(a, b):
+    a, b = np.asarray(a), np.asarray(b)
+    d = np.abs(a - b).max()
+    s = np.abs(b).max()
+    return d / s if s > 0 else d
+
+
+def pair(lmax, ne_layer, **kw):
+    ps = []
+    for mk in (vlib.default_params, orc.default_params):
+        p = mk()
+        p.lmax, p.nlat, p.nphi = lmax, lmax + 1, 2 * (lmax + 1)
+        for i, c in enumerate(ne_layer):
+            p.ne_layer[i] = c
+        for k, v in kw.items():
+            setattr(p, k, v)
+        ps.append(p)
+    return vlib.Model(ps[0]), orc.Oracle(ps[1])
+
+
+def rand_sigma(rng, nlm, lmax, scale=1e4):
+    s = (rng.standard_normal(nlm) + 1j * rng.standard_normal(nlm)) * scale
+    s[: lmax + 1] = s[: lmax + 1].real
+    return s
+
+
+@pytest.mark.parametrize("lmax", [16, 128])
+def test_sht_parity(lmax):
+    g, o = pair(lmax, [2, 4, 4, 3])
+    rng = np.random.default_rng(lmax)
+    f = rng.standard_normal(g.ng)
+    assert rel(g.analysis(f), o.analysis(f)) < 1e-12
+    q = rand_sigma(rng, g.nlm, lmax, 1.0)
+    assert rel(g.synthesis(q), o.synthesis(q)) < 1e-12
+    assert rel(g.analysis(g.synthesis(q)), q) < 1e-11
+
+
+def test_gains_parity():
+    g, o = pair(32, [4, 17, 15, 24])
+    for a, b in zip(g.gains(), o.gains()):
+        assert rel(a, b) < TOL
+
+
+def test_gpu_love_numbers_vs_table():
+    """Elastic Love numbers from the device operators (M3-L70-V01, native
+    mesh) against the normal-mode table, 1 % (tests/test_benchmark_love.f90)."""
+    p = vlib.default_params()
+    set_layers(p, M3L70V01)
+    p.lmax, p.nlat, p.nphi = 48, 49, 98
+    m = vlib.Model(p)
+    gu, gn, gv = m.gains()
+    G, a = 6.67430e-11, 6371e3
+    mass = sum(4 / 3 * np.pi * rho * (rt**3 - rb**3) for (rb, rt, rho, *_r) in M3L70V01)
+    g0 = G * mass / a**2
+    ref = json.load(open(os.path.join(GOLD, "love_M3L70V01.json")))["elastic"]
+    for j in range(2, 49):
+        phiL = 4 * np.pi * G * a / (2 * j + 1)
+        h = g0 * gu[j] / phiL
+        k = -(-gn[j] * g0) / phiL - 1.0
+        assert abs(h - ref[str(j)]["h"]) <= 1e-2 * abs(ref[str(j)]["h"])
+        assert abs(k - ref[str(j)]["k"]) <= 1e-2 * abs(ref[str(j)]["k"])
+
+
+def test_drift_parity_random_state():
+    g, o = pair(24, [3, 10, 9, 6], skip_tol=0.0)
+    rng = np.random.default_rng(2)
+    n = 4 * g.ne * g.nk
+    state = [rng.standard_normal(n) * 1e3 for _ in range(6)]
+    g.set_state(state, 0.0)
+    o.set_state(state, 0.0)
+    g.begin_step()
+    o.begin_step()
+    for a, b in zip(g.drift(), o.drift()):
+        assert rel(a, b) < TOL
+
+
+@pytest.mark.parametrize("skip_tol", [0.0, 1e-4])
+def test_response_stepping_parity(skip_tol):
+    g, o = pair(24, [3, 10, 9, 6], skip_tol=skip_tol, dt_init=50 * synth.SEC_PER_YEAR)
+    rng = np.random.default_rng(4)
+    sigma = rand_sigma(rng, g.nlm, 24)
+    for _ in range(6):
+        for mdl in (g, o):
+            mdl.begin_step()
+        ug, ng_ = g.apply(sigma)
+        uo, no = o.apply(sigma)
+        assert rel(ug, uo) < TOL and rel(ng_, no) < TOL
+        g.advance(sigma)
+        o.advance(sigma)
+    sg, _ = g.state()
+    so, _ = o.state()
+    for a, b in zip(sg, so):
+        assert rel(a, b) < TOL
+
+
+def run_workload(w, n_steps, stride=1):
+    pg = w.params(vlib.default_params)
+    po = w.params(orc.default_params)
+    g, o = vlib.Model(pg), orc.Oracle(po)
+    zb, hi = w.reference()
+    g.set_reference(zb, hi)
+    o.set_reference(zb, hi)
+    for step in range(1, n_steps + 1):
+        ice = w.ice_at(step * stride)
+        g.update(ice, w.dt_yr)
+        o.update(ice, w.dt_yr)
+    return g, o
+
+
+def check_models(g, o):
+    rg, zg, cg, sg = g.fields()
+    ro, zo, co, so = o.fields()
+    assert np.array_equal(cg, co), "ocean function differs"
+    assert rel(rg, ro) < TOL
+    assert rel(zg, zo) < TOL
+    assert rel(sg, so) < TOL
+    stg, tg = g.state()
+    sto, to = o.state()
+    for a, b in zip(stg, sto):
+        assert rel(a, b) < TOL
+    ig, io = g.info(), o.info()
+    assert ig.n_accept == io.n_accept and ig.n_reject == io.n_reject and ig.n_sub_last == io.n_sub_last
+    assert abs(ig.bsl - io.bsl) <= 1e-10 * max(1.0, abs(io.bsl))
+
+
+def test_update_parity_with_sea_level():
+    w = synth.Workload("t", 24, 24, 100.0, 6, 3, "sawtooth", sle=True, visc3d=False, seed=3)
+    g, o = run_workload(w, 6, stride=40)
+    check_models(g, o)
+    assert g.info().worst_mass_resid < 1e-10
+
+
+def test_update_parity_land_only():
+    w = synth.Workload("t", 20, 24, 50.0, 6, 3, "ramp", sle=False, visc3d=False, seed=5)
+    g, o = run_workload(w, 6, stride=40)
+    check_models(g, o)
+
+
+def test_update_substeps_parity():
+    """A weak upper mantle forces Maxwell-CFL sub-steps (n_sub > 1)."""
+    w = synth.Workload("t", 16, 20, 200.0, 3, 2, "sawtooth", sle=True, visc3d=False, seed=9)
+    pg = w.params(vlib.default_params)
+    po = w.params(orc.default_params)
+    for p in (pg, po):
+        p.eta[1] = 2e19
+    g, o = vlib.Model(pg), orc.Oracle(po)
+    zb, hi = w.reference()
+    for m in (g, o):
+        m.set_reference(zb, hi)
+    for step in range(1, 4):
+        ice = w.ice_at(step * 100)
+        g.update(ice, w.dt_yr)
+        o.update(ice, w.dt_yr)
+    assert g.info().n_sub_last > 1
+    check_models(g, o)
+
+
+def test_full_size_sea_level_step_properties():
+    """lmax 128, 100 elements (the 1-D + SLE workload): finite, mass-conserving,
+    and equal to the oracle after the first coupling interval."""
+    w = synth.workloads()["c2_1d_sle_l128"]
+    g, o = run_workload(w, 1, stride=200)
+    check_models(g, o)
+    assert g.info().worst_mass_resid < 1e-10
+
+
+def test_disc_benchmark_on_gpu():
+    """Spada-2011 disc centre uplift through the device response operators,
+    1-10 kyr within 3 % (tests/test_benchmark_disc.f90)."""
+    uref = np.array(json.load(open(os.path.join(GOLD, "disc_spada2011.json")))["u"])
+    p = vlib.default_params()
+    set_layers(p, M3L70V01)
+    L = 128
+    p.lmax, p.nlat, p.nphi = L, L + 1, 2 * (L + 1)
+    p.skip_tol = 0.0
+    p.dt_init = 20 * synth.SEC_PER_YEAR
+    m = vlib.Model(p)
+    m.set_dt(p.dt_init)
+    ca = np.cos(np.deg2rad(10.0))
+    sig0 = 931.0 * 1000.0
+    sigma = np.zeros(m.nlm, complex)
+    Pm1, P = 1.0, ca
+    for n in range(1, L + 1):
+        Pp1 = ((2 * n + 1) * ca * P - n * Pm1) / (n + 1)
+        if n >= 2:
+            sigma[n] = 0.5 * sig0 * (Pm1 - Pp1) * np.sqrt(4 * np.pi / (2 * n + 1))
+        Pm1, P = P, Pp1
+    pbar = np.sqrt((2 * np.arange(L + 1) + 1) / (4 * np.pi))
+    out = {}
+    for step in range(501):
+        m.begin_step()
+        u, _ = m.apply(sigma)
+        if step in (50, 100, 250, 500):
+            out[step] = float((u[: L + 1].real * pbar).sum())
+        m.advance(sigma)
+    for it, step in ((1, 50), (2, 100), (3, 250), (4, 500)):
+        assert abs(out[step] - uref[0, it]) <= 3e-2 * abs(uref[0, it])

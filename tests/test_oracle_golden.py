@@ -1,0 +1,217 @@
+"""The CPU oracle pinned against the reference's golden vectors and
+known-answer identities (no GPU).
+
+Mirrors the reference tests: test_benchmark_love.f90 (Love numbers vs the
+normal-mode table, 1 %), test_benchmark_disc.f90 (Spada-2011 disc transient,
+3 %), test_band.f90 (band LU vs dense, 1e-12), test_sht.f90 (round trip,
+integrals, Y10), test_assembly (operator symmetry), test_response_3d.f90
+(3-D path == 1-D path for a laterally uniform viscosity, 1e-9) and
+test_sle.f90 (ocean-mass conservation).
+"""
+import json
+import os
+
+import numpy as np
+import pytest
+
+from fastearth3d_b200.abi import M3L70V01, VG_RHEOL_FLUID, set_layers
+from fastearth3d_b200 import synth
+from oracle import orc
+
+GOLD = os.path.join(os.path.dirname(__file__), "golden")
+
+
+def m3_params():
+    p = orc.default_params()
+    set_layers(p, M3L70V01)
+    return p
+
+
+def test_love_elastic_vs_normal_mode_table():
+    g = json.load(open(os.path.join(GOLD, "love_M3L70V01.json")))["elastic"]
+    h, l, k = orc.love_numbers(m3_params(), 2, 48)
+    for j in range(2, 49):
+        ref = g[str(j)]
+        assert abs(h[j - 2] - ref["h"]) <= 1e-2 * abs(ref["h"])
+        assert abs(k[j - 2] - ref["k"]) <= 1e-2 * abs(ref["k"])
+
+
+def test_love_fluid_limit_vs_table():
+    g = json.load(open(os.path.join(GOLD, "love_M3L70V01.json")))["fluid"]
+    p = orc.default_params()
+    lay = [M3L70V01[0]] + [(a, b, c, 0.0, e, VG_RHEOL_FLUID) for (a, b, c, d, e, f) in M3L70V01[1:4]] + [M3L70V01[4]]
+    set_layers(p, lay)
+    h, l, k = orc.love_numbers(p, 2, 8)
+    for j in range(2, 9):
+        ref = g[str(j)]
+        for ours, key in ((h, "h"), (l, "l"), (k, "k")):
+            assert abs(ours[j - 2] - ref[key]) <= 1e-2 * abs(ref[key])
+
+
+def test_homogeneous_fluid_sphere_limits():
+    # fluid (mu -> 0) homogeneous sphere: h -> -(2j+1)/3, k -> -1 (tests/test_love.f90:36-55)
+    p = orc.default_params()
+    set_layers(p, [(0.0, 6371e3, 5511.0, 1e-3, 0.0, VG_RHEOL_FLUID)])
+    h, l, k = orc.love_numbers(p, 2, 6)
+    for j in range(2, 7):
+        assert abs(h[j - 2] + (2 * j + 1) / 3) < 1e-3
+        assert abs(k[j - 2] + 1.0) < 1e-4
+
+
+def test_band_lu_vs_dense():
+    rng = np.random.default_rng(3)
+    for n, kl, ku in ((40, 6, 6), (31, 3, 5), (17, 16, 16)):
+        A = np.zeros((n, n))
+        for i in range(n):
+            for j in range(max(0, i - kl), min(n, i + ku + 1)):
+                A[i, j] = rng.standard_normal()
+        A[np.arange(0, n, 4), np.arange(0, n, 4)] = 0.0  # zero diagonal entries force pivoting
+        b = rng.standard_normal(n)
+        x = orc.band_dense_solve(A, b)
+        xd = np.linalg.solve(A, b)
+        assert np.abs(x - xd).max() <= 1e-10 * np.abs(xd).max()
+    # saddle point with a zero block (the pressure block of the radial operator)
+    m = 12
+    K = rng.standard_normal((m, m))
+    K = K @ K.T + m * np.eye(m)
+    B = rng.standard_normal((4, m))
+    A = np.block([[K, B.T], [B, np.zeros((4, 4))]])
+    b = rng.standard_normal(m + 4)
+    assert np.abs(orc.band_dense_solve(A, b) - np.linalg.solve(A, b)).max() < 1e-10
+
+
+def test_operator_symmetric():
+    p = orc.default_params()
+    p.ne_layer[:4] = [3, 8, 6, 5]
+    for j in (1, 2, 7):
+        A = orc.dense_operator(p, j, with_uniq=True)
+        assert np.abs(A - A.T).max() <= 1e-12 * np.abs(A).max()
+
+
+@pytest.fixture(scope="module")
+def small_oracle():
+    p = orc.default_params()
+    p.lmax, p.nlat, p.nphi = 24, 25, 50
+    p.ne_layer[:4] = [4, 17, 15, 24]
+    return orc.Oracle(p)
+
+
+def test_sht_identities(small_oracle):
+    o = small_oracle
+    L = o.p.lmax
+    colat, w = o.grid()
+    assert abs(w.sum() - 2.0) < 1e-14
+    assert abs(o.surface_integral(np.ones(o.ng)) - 4 * np.pi) < 1e-12
+    q = np.zeros(o.nlm, complex)
+    q[0] = 1.0
+    f = o.synthesis(q)
+    assert abs(o.surface_integral(f * f) - 1.0) < 1e-12  # int Y00^2 = 1
+    q[0], q[1] = 0.0, 1.0  # Y10
+    y10 = o.synthesis(q).reshape(o.p.nlat, o.p.nphi)
+    assert np.abs(y10[:, 0] - np.sqrt(3 / (4 * np.pi)) * np.cos(colat)).max() < 1e-14
+    rng = np.random.default_rng(5)
+    qq = rng.standard_normal(o.nlm) + 1j * rng.standard_normal(o.nlm)
+    qq[: L + 1] = qq[: L + 1].real
+    assert np.abs(o.analysis(o.synthesis(qq)) - qq).max() < 1e-11
+
+
+def test_tensor_roundtrip_and_completeness(small_oracle):
+    o = small_oracle
+    L = o.p.lmax
+    rng = np.random.default_rng(7)
+    c = rng.standard_normal((4, o.nlm)) + 1j * rng.standard_normal((4, o.nlm))
+    for lm in range(o.nlm):
+        m = next(mm for mm in range(L + 1) if synth.lmidx(L, mm, mm) <= lm < synth.lmidx(L, mm, mm) + L + 1 - mm)
+        l = lm - synth.lmidx(L, m, m) + m
+        if m == 0:
+            c[:, lm] = c[:, lm].real
+        if l == 0:
+            c[1:, lm] = 0.0
+        if l <= 1:
+            c[3, lm] = 0.0
+    back = o.tensor_analysis(o.tensor_synth(c))
+    assert np.abs(back - c).max() < 1e-9 * np.abs(c).max()
+
+
+def test_disc_benchmark_viscoelastic_centre():
+    """Spada-2011 disc (10 deg, 1000 m ice) on M3-L70-V01: centre uplift at
+    1, 2, 5, 10 kyr within 3 % (tests/test_benchmark_disc.f90:34), dt = 20 yr."""
+    g = json.load(open(os.path.join(GOLD, "disc_spada2011.json")))
+    uref = np.array(g["u"])
+    p = m3_params()
+    L = 128  # NMAX_VE of the reference test
+    p.lmax, p.nlat, p.nphi = L, L + 1, 2 * (L + 1)
+    p.skip_tol = 0.0
+    p.dt_init = 20 * synth.SEC_PER_YEAR
+    o = orc.Oracle(p)
+    ca = np.cos(np.deg2rad(10.0))
+    sig0 = 931.0 * 1000.0
+    sig = np.zeros(L + 2)
+    Pm1, P = 1.0, ca
+    for n in range(1, L + 1):
+        Pp1 = ((2 * n + 1) * ca * P - n * Pm1) / (n + 1)
+        sig[n] = 0.5 * sig0 * (Pm1 - Pp1)
+        Pm1, P = P, Pp1
+    sigma = np.zeros(o.nlm, complex)
+    for n in range(2, L + 1):
+        sigma[n] = sig[n] * np.sqrt(4 * np.pi / (2 * n + 1))
+    pbar = np.sqrt((2 * np.arange(L + 1) + 1) / (4 * np.pi))
+    out = {}
+    for step in range(501):
+        o.begin_step()
+        u, _ = o.apply(sigma)
+        if step in (0, 50, 100, 250, 500):
+            out[step] = float((u[: L + 1].real * pbar).sum())
+        o.advance(sigma)
+    for it, step in enumerate((0, 50, 100, 250, 500)):
+        if it == 0:
+            continue
+        assert abs(out[step] - uref[0, it]) <= 3e-2 * abs(uref[0, it]), (step, out[step], uref[0, it])
+
+
+def test_3d_uniform_perturbation_equals_1d():
+    """A laterally uniform log-viscosity perturbation routed through the 3-D
+    pseudo-spectral path reproduces the 1-D path (tests/test_response_3d.f90:
+    218-250), memory and uplift to 1e-9 relative over 5 steps."""
+    p = orc.default_params()
+    p.lmax, p.nlat, p.nphi = 12, 13, 26
+    p.ne_layer[:4] = [2, 5, 4, 3]
+    p.skip_tol = 0.0
+    p.visc3d_tol = -1.0  # every Maxwell element takes the 3-D path
+    p.dt_init = 50 * synth.SEC_PER_YEAR
+    o3, o1 = orc.Oracle(p), orc.Oracle(p)
+    ne = o3.ne
+    pert = np.full((ne, p.nlat, p.nphi), 0.3)
+    o3.enable_visc3d(pert)
+    p1 = p
+    p1.visc3d_tol = 10.0  # spread 0 <= tol: all 1-D with the mean rate
+    o1 = orc.Oracle(p1)
+    o1.enable_visc3d(pert)
+    assert o3.info().ne3d > 0 and o1.info().ne3d == 0
+    rng = np.random.default_rng(11)
+    sigma = rng.standard_normal(o3.nlm) + 1j * rng.standard_normal(o3.nlm)
+    sigma[: p.lmax + 1] = sigma[: p.lmax + 1].real
+    sigma *= 1e4
+    for _ in range(5):
+        for o in (o3, o1):
+            o.begin_step()
+            o.advance(sigma)
+    s3, _ = o3.state()
+    s1, _ = o1.state()
+    mx = max(np.abs(a).max() for a in s1)
+    assert max(np.abs(a - b).max() for a, b in zip(s3, s1)) <= 1e-9 * mx
+    o3.begin_step()
+    o1.begin_step()
+    u3, _ = o3.apply(sigma)
+    u1, _ = o1.apply(sigma)
+    assert np.abs(u3 - u1).max() <= 1e-9 * np.abs(u1).max()
+
+
+def test_sle_mass_conservation():
+    w = synth.Workload("t", 16, 20, 100.0, 5, 2, "sawtooth", sle=True, visc3d=False, seed=7)
+    o = orc.Oracle(w.params(orc.default_params))
+    zb, hi = w.reference()
+    o.set_reference(zb, hi)
+    for step in range(1, 4):
+        o.update(w.ice_at(step * 50), 100.0)
+        assert o.info().worst_mass_resid < 1e-10
