@@ -36,10 +36,16 @@ def _stale(target, deps):
     return any(os.path.getmtime(d) > t for d in deps)
 
 
+# Setup kernels (operator assembly, equilibration, LU factor, unit-load solve)
+# run once per model: compiled without FMA contraction so their arithmetic is
+# the oracle's operation-for-operation (no cost on the time step).
+PER_FILE = {"vg_setup.cu": ["--fmad=false"]}
+
+
 def _compile(src, extra):
     obj = os.path.join(BUILD, os.path.basename(src)[:-3] + ".o")
-    if _stale(obj, [src] + _headers()):
-        cmd = [NVCC, *ARCH, *FLAGS, *extra, "-c", src, "-o", obj]
+    if _stale(obj, [src] + _headers() + [os.path.abspath(__file__)]):
+        cmd = [NVCC, *ARCH, *FLAGS, *PER_FILE.get(os.path.basename(src), []), *extra, "-c", src, "-o", obj]
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError(f"nvcc failed for {src}:\n{r.stdout}\n{r.stderr}")

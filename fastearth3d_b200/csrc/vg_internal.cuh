@@ -53,7 +53,10 @@ struct DArr {
     n = count;
     if (count) {
       VG_CUDA(cudaMalloc(&p, count * sizeof(T)));
+      // The handle's stream is non-blocking, so nothing orders this legacy-stream
+      // memset before later work on it: finish the zeroing here (setup only).
       VG_CUDA(cudaMemset(p, 0, count * sizeof(T)));
+      VG_CUDA(cudaDeviceSynchronize());
     }
   }
   void release() {

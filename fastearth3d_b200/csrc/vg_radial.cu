@@ -97,7 +97,7 @@ __device__ __forceinline__ void band_solve_col(const double* __restrict__ ab, in
 
 // Drift solve for degrees >= 2: one thread per slot k, real and imaginary
 // histories one after the other (src/vilma_response.f90:744-802).
-__global__ void k_drift(DriftArgs A) {
+__global__ void __launch_bounds__(128) k_drift(DriftArgs A) {
   int k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= A.nk) return;
   int l = A.kdeg[k];
@@ -136,7 +136,7 @@ __global__ void k_drift(DriftArgs A) {
 
 // Degree-1 drift (slots k = 0, 1): bordered dense system, CTA-parallel sweeps,
 // CM-frame projection with the stored null mode (src/vilma_response.f90:770-779).
-__global__ void k_drift_deg1(DriftArgs A) {
+__global__ void __launch_bounds__(256) k_drift_deg1(DriftArgs A) {
   extern __shared__ double xsh[];  // [4][ns]
   const int nd = A.nd, ns = nd + 1, nr = A.nr, nk = A.nk;
   const double thr = A.skip_tol * __longlong_as_double((long long)*A.maxbits);
@@ -242,7 +242,7 @@ void launch_drift(vg_handle* h) {
     VG_CUDA(cudaFuncSetAttribute(k_drift_deg1, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
     attr_set = true;
   }
-  k_drift_deg1<<<1, 512, shm, h->stream>>>(A);
+  k_drift_deg1<<<1, 256, shm, h->stream>>>(A);
   VG_CUDA(cudaGetLastError());
 }
 
@@ -279,7 +279,7 @@ void launch_apply(vg_handle* h, const double* d_sigma, double* d_u, double* d_n)
 // Forward-Euler memory advance of the spectrally advanced elements, one thread
 // per slot, out of place (cur -> nxt), with the per-slot norm of the new
 // state over ALL elements (the 3-D elements were written to nxt before).
-__global__ void k_advance_1d(const double* __restrict__ mem, double* __restrict__ nxt, int ne, int nr, int nk,
+__global__ void __launch_bounds__(256) k_advance_1d(const double* __restrict__ mem, double* __restrict__ nxt, int ne, int nr, int nk,
                              double dt, const double* __restrict__ sigma, const int* __restrict__ kdeg,
                              const int* __restrict__ k2lm, const double* __restrict__ Jrv,
                              const double* __restrict__ xUn, const double* __restrict__ xVn,

@@ -327,7 +327,7 @@ __global__ void k_build_band(ElemData ed, int lmax, double* __restrict__ raw, do
 
 // Degree 1: band part plus the KKT border w (E_uniq weight, src/vilma_radial_fe.f90:425-443,
 // 475-477), dense dgbtf2 with kl = ku = nd. Assembly by one thread, factor by the CTA.
-__global__ void k_build_deg1(ElemData ed, double* __restrict__ A /*dense nd x nd col-major scratch*/,
+__global__ void __launch_bounds__(512) k_build_deg1(ElemData ed, double* __restrict__ A /*dense nd x nd col-major scratch*/,
                              double* __restrict__ ab, int ldab, double* __restrict__ dr,
                              double* __restrict__ dc, double* __restrict__ w, int* __restrict__ ipiv,
                              int* __restrict__ status) {
@@ -516,7 +516,7 @@ __global__ void k_unit_load(int lmax, int nr, int n, double r_earth, double g_su
 }
 
 // degree-1 unit-load response (with the CM-frame projection) and null mode
-__global__ void k_unit_load_deg1(int nr, int nd, double r_earth, double g_surf, int deg1_cm,
+__global__ void __launch_bounds__(512) k_unit_load_deg1(int nr, int nd, double r_earth, double g_surf, int deg1_cm,
                                  const double* __restrict__ ab, int kl, int kv, const int* __restrict__ ipiv,
                                  const double* __restrict__ dr, const double* __restrict__ dc,
                                  double* __restrict__ nullmode, double* __restrict__ gu, double* __restrict__ gn,
@@ -674,7 +674,7 @@ void setup_handle(vg_handle* h) {
   h->d_dc1.alloc(nd);
   h->d_ipiv1.alloc(h->ns1);
   h->d_null1.alloc(nd);
-  k_build_deg1<<<1, 1024, 0, s>>>(ed, Adense.p, h->d_ab1.p, h->ldab1, h->d_dr1.p, h->d_dc1.p, w.p, h->d_ipiv1.p,
+  k_build_deg1<<<1, 512, 0, s>>>(ed, Adense.p, h->d_ab1.p, h->ldab1, h->d_dr1.p, h->d_dc1.p, w.p, h->d_ipiv1.p,
                                   status.p);
   VG_CUDA(cudaGetLastError());
   int st = 0;

