@@ -1,0 +1,305 @@
+"""Benchmark of the B200 backend for VILMA v2's viscoelastic time step.
+
+One step = one solid_earth_update interval (dt of the workload, with its
+Maxwell-CFL sub-steps) of the seeded synthetic workload, driven through the
+C-ABI. Prints one JSON line (rank 0).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                  [--workload NAME]
+
+Multi-GPU: instances are independent (no collective on the data path), so N
+ranks run N replicas of the workload ("scaling": "weak"); value = total steps
+of all ranks / max-over-ranks device time.
+
+The reference arm (--impl reference) times the CPU restatement of the
+reference algorithm (the reference itself is Fortran and cannot be built
+here) on the host cores, rank 0 only.
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+from fastearth3d_b200 import synth  # noqa: E402
+
+DEFAULT_WORKLOAD = "c2_1d_sle_l128"
+METRIC = "steps/s @lmax=128 3D visc: batched vs plain GPU, rsl err<=1e-8; grad/fwd"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default=DEFAULT_WORKLOAD)
+    ap.add_argument("--cpu-sample-s", type=float, default=15.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def peaks():
+    try:
+        return json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json"))), "measured"
+    except Exception:
+        return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "bf16_tflops_sustained": 1400.0}, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks/throttle reasons sampled every 200 ms during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index, self.rows, self.proc = index, [], None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([x.strip() for x in line.split(",")])
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in self.rows for i in range(4) if len(r) > 5 + i and r[5 + i] == "Active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.rows)}
+
+
+def algorithmic_bytes(info, phase):
+    """Algorithmic HBM bytes of one call of a phase (the state each must stream)."""
+    ne, nk, nr = info.ne, info.nk, info.nr
+    state = 6 * 4 * ne * nk * 8  # A/B/C re/im memory, (4, ne, nk) doubles each
+    drift_nodal = 2 * 2 * nr * nk * 8  # dUn, dVn re/im
+    if phase == "drift":  # read the state, write the nodal + surface drift
+        return state + drift_nodal + 6 * nk * 8
+    if phase == "advance_1d":  # read state + nodal drift, write state
+        return 2 * state + drift_nodal
+    return None
+
+
+def cpu_baseline(w, budget_s, threads):
+    from oracle import orc  # the CPU restatement: test/baseline infrastructure only
+
+    o = orc.Oracle(w.params(orc.default_params))
+    zb, hi = w.reference()
+    o.set_reference(zb, hi)
+    if w.visc3d:
+        o.enable_visc3d(w.pert(*_layers(o)))
+    o.update(w.ice_at(1), w.dt_yr)  # warm-up step (untimed)
+    t0 = time.perf_counter()
+    n = 0
+    while True:
+        n += 1
+        o.update(w.ice_at(1 + n), w.dt_yr)
+        if time.perf_counter() - t0 >= budget_s:
+            break
+    dt = time.perf_counter() - t0
+    return {"value": n / dt, "unit": "steps/s", "cores": threads, "kind": "port",
+            "sample": f"{n} consecutive steps of {w.name} after 1 warm-up step, {dt:.1f} s, OMP threads={threads}"}
+
+
+def _layers(m):
+    p = m.p
+    lay = []
+    for i in range(p.n_layer):
+        lay.append(p.rheology[i])
+    # element -> layer map from the per-layer counts (surface-first layers, elements bottom-up)
+    counts = [p.ne_layer[i] for i in range(p.n_layer)]
+    el = []
+    for i in range(p.n_layer - 1, -1, -1):
+        el += [i] * counts[i]
+    return el, lay
+
+
+def run_reference(args, w):
+    threads = os.cpu_count() or 1
+    os.environ.setdefault("OMP_NUM_THREADS", str(threads))
+    steps = max(1, args.steps)
+    budget = 150.0
+    from oracle import orc
+
+    o = orc.Oracle(w.params(orc.default_params))
+    zb, hi = w.reference()
+    o.set_reference(zb, hi)
+    if w.visc3d:
+        o.enable_visc3d(w.pert(*_layers(o)))
+    for s in range(1, args.warmup + 1):
+        o.update(w.ice_at(s), w.dt_yr)
+    t0 = time.perf_counter()
+    n = 0
+    for s in range(steps):
+        o.update(w.ice_at(args.warmup + 1 + s), w.dt_yr)
+        n += 1
+        if time.perf_counter() - t0 > budget:
+            break
+    dt = time.perf_counter() - t0
+    v = n / dt
+    sample = f"{n} of {steps} steps of {w.name} after {args.warmup} warm-up steps (bounded at {budget:.0f} s)"
+    out = {"metric": METRIC, "value": v, "unit": "steps/s", "impl": "reference", "n_gpus": args.gpus,
+           "steps": n, "warmup": args.warmup, "ms_per_step": 1e3 * dt / n, "higher_is_better": True,
+           "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+           "config": {"workload": w.name, "lmax": w.lmax, "grid": f"{w.nlat}x{w.nphi}", "radial_elements": w.n_elem,
+                      "dt_yr": w.dt_yr, "visc3d": w.visc3d, "sea_level": w.sle},
+           "cpu_baseline": {"value": v, "unit": "steps/s", "cores": threads, "kind": "port", "sample": sample},
+           "e2e": {"value": v, "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(out))
+
+
+def main():
+    args = parse()
+    w = synth.workloads()[args.workload]
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        if rank == 0:
+            run_reference(args, w)
+        return
+    import torch
+
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    from fastearth3d_b200 import lib as vlib
+
+    m = vlib.Model(w.params(vlib.default_params))
+    zb, hi = w.reference()
+    m.set_reference(zb, hi)
+    if w.visc3d:
+        m.enable_visc3d(w.pert(*_layers(m)))
+    ng = w.nlat * w.nphi
+    total = args.warmup + args.steps
+    n_prof = min(args.steps, 5)
+    n_e2e = min(args.steps, 10)
+    ice_dev = torch.empty((total + n_prof + 1, ng), dtype=torch.float64, device="cuda")
+    for s in range(total + n_prof + 1):
+        ice_dev[s] = torch.from_numpy(w.ice_at(s + 1))
+    stream = torch.cuda.ExternalStream(m.stream_ptr())
+    for s in range(args.warmup):
+        m.update_device(ice_dev[s].data_ptr(), w.dt_yr)
+    launches0 = m.info().n_launch
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clk:
+        with torch.cuda.stream(stream):
+            ev0.record()
+        for s in range(args.warmup, total):
+            m.update_device(ice_dev[s].data_ptr(), w.dt_yr)
+        with torch.cuda.stream(stream):
+            ev1.record()
+        torch.cuda.synchronize()
+    ms = ev0.elapsed_time(ev1)
+    launches = m.info().n_launch - launches0
+    info = m.info()
+    if dist:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+        dist.barrier()
+    # phase timers over a few more steps (separate pass: the timers add events)
+    m.profile_enable(True)
+    for s in range(total, total + n_prof):
+        m.update_device(ice_dev[s].data_ptr(), w.dt_yr)
+    ph_ms, ph_calls = m.profile_read()
+    m.profile_enable(False)
+    # end to end through the public API: host ice in pinned memory, rsl read back each step
+    ice_host = torch.empty((n_e2e, ng), dtype=torch.float64).pin_memory()
+    for s in range(n_e2e):
+        ice_host[s] = torch.from_numpy(w.ice_at(total + n_prof + s + 1))
+    rsl_host = np.zeros(ng)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with torch.cuda.stream(stream):
+        e0.record()
+    for s in range(n_e2e):
+        vlib.lib().vg_update(m.h, vlib.C.cast(ice_host[s].data_ptr(), vlib._P), w.dt_yr)
+        vlib.lib().vg_get_fields(m.h, vlib.ptr(rsl_host), None, None, None)
+    with torch.cuda.stream(stream):
+        e1.record()
+    torch.cuda.synchronize()
+    e2e_ms = e0.elapsed_time(e1) / n_e2e
+    if rank != 0:
+        if dist:
+            dist.destroy_process_group()
+        return
+    pk, pk_kind = peaks()
+    names = ["drift", "advance_1d", "visc3d", "sle"]
+    phases = {names[i]: {"ms_per_call": ph_ms[i] / ph_calls[i] if ph_calls[i] else 0.0, "calls": int(ph_calls[i]),
+                         "ms_total": ph_ms[i]} for i in range(4)}
+    dom = max(["drift", "advance_1d"], key=lambda n: phases[n]["ms_total"])
+    byts = algorithmic_bytes(info, dom)
+    ach = byts / (phases[dom]["ms_per_call"] * 1e-3) / 1e9
+    out = {
+        "metric": METRIC,
+        "value": world * args.steps / (ms * 1e-3),
+        "unit": "steps/s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": ms / args.steps,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f64",
+        "data": "synthetic",
+        "config": {"workload": w.name, "lmax": w.lmax, "grid": f"{w.nlat}x{w.nphi}", "radial_elements": w.n_elem,
+                   "dt_yr": w.dt_yr, "n_sub": info.n_sub_last, "visc3d": w.visc3d, "sea_level": w.sle,
+                   "parallelism": f"replicas{world}",
+                   "l2": "state larger than L2 (%.0f MB streamed per sub-step)" % (6 * 4 * info.ne * info.nk * 8 / 1e6)},
+        "e2e": {"value": 1e3 / e2e_ms, "unit": "steps/s", "h2d_bytes_per_step": ng * 8, "d2h_bytes_per_step": ng * 8},
+        "gpu_launches": int(launches),
+        "roofline": {"bound": "hbm", "kernel": dom, "achieved": ach, "peak": pk["hbm_gbs"], "unit": "GB/s",
+                     "frac": ach / pk["hbm_gbs"], "peak_kind": pk_kind, "traffic": None,
+                     "algorithmic_bytes_per_launch": byts},
+        "phases": phases,
+        "clocks": clk.summary(),
+    }
+    if not args.no_cpu_baseline:
+        out["cpu_baseline"] = cpu_baseline(w, args.cpu_sample_s, os.cpu_count() or 1)
+    print(json.dumps(out))
+    if dist:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -50,7 +50,12 @@ class VgInfo(C.Structure):
         ("worst_mass_resid", C.c_double),
         ("bsl", C.c_double),
         ("n_outer_last", C.c_int), ("n_inner_last", C.c_int), ("n_coast_flip_last", C.c_int),
+        ("n_launch", C.c_longlong),
     ]
+
+
+VG_PH_DRIFT, VG_PH_ADVANCE_1D, VG_PH_VISC3D, VG_PH_SLE, VG_NPHASE = 0, 1, 2, 3, 4
+PHASE_NAMES = ["drift", "advance_1d", "visc3d", "sle"]
 
 
 def set_layers(p, layers):

@@ -31,6 +31,37 @@ static void need(vg_handle* h, bool cond, const char* msg) {
   if (!cond) throw Error(msg);
 }
 
+namespace vg {
+PhaseScope::PhaseScope(vg_handle* hh, int p) : h(hh), ph(p) {
+  if (!h->prof.on) return;
+  cudaEvent_t e;
+  VG_CUDA(cudaEventCreate(&e));
+  VG_CUDA(cudaEventRecord(e, h->stream));
+  h->prof.ev[ph].push_back(e);
+}
+PhaseScope::~PhaseScope() {
+  if (!h->prof.on) return;
+  cudaEvent_t e;
+  if (cudaEventCreate(&e) != cudaSuccess) return;
+  cudaEventRecord(e, h->stream);
+  h->prof.ev[ph].push_back(e);
+  h->prof.calls[ph]++;
+}
+void prof_collect(vg_handle* h) {
+  VG_CUDA(cudaStreamSynchronize(h->stream));
+  for (int ph = 0; ph < VG_NPHASE; ++ph) {
+    auto& v = h->prof.ev[ph];
+    for (size_t i = 0; i + 1 < v.size(); i += 2) {
+      float ms = 0.f;
+      VG_CUDA(cudaEventElapsedTime(&ms, v[i], v[i + 1]));
+      h->prof.ms[ph] += ms;
+    }
+    for (cudaEvent_t e : v) cudaEventDestroy(e);
+    v.clear();
+  }
+}
+}  // namespace vg
+
 extern "C" {
 
 int vg_params_default(vg_params* p) {
@@ -203,6 +234,33 @@ int vg_get_info(vg_handle* h, vg_info* info) {
     info->n_outer_last = h->n_outer_last;
     info->n_inner_last = h->n_inner_last;
     info->n_coast_flip_last = h->n_flip_last;
+    info->n_launch = h->n_launch;
+  });
+}
+
+int vg_stream(vg_handle* h, void** stream) {
+  return guarded(h, [&] {
+    need(h, stream != nullptr, "vg_stream: null argument");
+    *stream = (void*)h->stream;
+  });
+}
+
+int vg_profile_enable(vg_handle* h, int on) {
+  return guarded(h, [&] {
+    if (h->prof.on && !on) vg::prof_collect(h);
+    h->prof.on = on != 0;
+  });
+}
+
+int vg_profile_read(vg_handle* h, double* ms, long long* calls) {
+  return guarded(h, [&] {
+    vg::prof_collect(h);
+    for (int ph = 0; ph < VG_NPHASE; ++ph) {
+      if (ms) ms[ph] = h->prof.ms[ph];
+      if (calls) calls[ph] = h->prof.calls[ph];
+      h->prof.ms[ph] = 0.0;
+      h->prof.calls[ph] = 0;
+    }
   });
 }
 

@@ -88,6 +88,17 @@ struct SleScalars {
   unsigned long long mem_norm_bits;  // max |memory| of the state the last advance wrote
 };
 
+// Phase timers, the device counterpart of the reference's [PROFILE] buckets
+// (t_drift, t_mem, t_sht/t_apply of src/vilma_response.f90:179-186,
+// src/vilma_sle.f90:100-119): CUDA events recorded on the handle's stream
+// around each phase, read and reset by vg_profile_read.
+struct Prof {
+  bool on = false;
+  std::vector<cudaEvent_t> ev[VG_NPHASE];  // start/stop pairs
+  double ms[VG_NPHASE] = {};
+  long long calls[VG_NPHASE] = {};
+};
+
 struct Grid {
   int lmax, mmax, M, nlat, nphi, ng, nlm;
   std::vector<double> x, colat, sint, wts;  // host
@@ -154,6 +165,8 @@ struct vg_handle {
   int n_sub_last = 0, n_outer_last = 0, n_inner_last = 0, n_flip_last = 0;
   double worst_mass_resid = 0, bsl = 0;
   bool have_reference = false;
+  long long n_launch = 0;  // kernels launched by the time step (all phases)
+  vg::Prof prof;
 };
 
 namespace vg {
@@ -182,4 +195,12 @@ void visc3d_enable(vg_handle* h, const double* pert_host);
 void visc3d_advance(vg_handle* h, const double* d_sigma, double dt);
 // misc
 void sync_scalars(vg_handle* h);
+// phase timer scope: records a start event now and a stop event at scope exit
+struct PhaseScope {
+  vg_handle* h;
+  int ph;
+  PhaseScope(vg_handle* hh, int p);
+  ~PhaseScope();
+};
+void prof_collect(vg_handle* h);
 }  // namespace vg

@@ -202,6 +202,7 @@ __global__ void __launch_bounds__(256) k_drift_deg1(DriftArgs A) {
 }
 
 void launch_drift(vg_handle* h) {
+  PhaseScope ps(h, VG_PH_DRIFT);
   DriftArgs A;
   A.mem = h->d_mem[h->cur].p;
   A.mnorm = h->d_mnorm.p + (size_t)h->cur * h->nk;
@@ -234,7 +235,7 @@ void launch_drift(vg_handle* h) {
   A.kl1 = h->kl1;
   A.kv1 = h->kv1;
   A.deg1_cm = h->p.deg1_cm;
-  k_drift<<<(h->nk + 127) / 128, 128, 0, h->stream>>>(A);
+  k_drift<<<(h->nk + 127) / 128, 128, 0, h->stream>>>(A); ++h->n_launch;
   VG_CUDA(cudaGetLastError());
   size_t shm = 4 * (size_t)(h->ndof + 1) * sizeof(double);
   static bool attr_set = false;
@@ -242,7 +243,7 @@ void launch_drift(vg_handle* h) {
     VG_CUDA(cudaFuncSetAttribute(k_drift_deg1, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
     attr_set = true;
   }
-  k_drift_deg1<<<1, 256, shm, h->stream>>>(A);
+  k_drift_deg1<<<1, 256, shm, h->stream>>>(A); ++h->n_launch;
   VG_CUDA(cudaGetLastError());
 }
 
@@ -272,7 +273,7 @@ __global__ void k_apply(int nlm, int nk, double g, const int* __restrict__ lm_l,
 void launch_apply(vg_handle* h, const double* d_sigma, double* d_u, double* d_n) {
   int nlm = h->grid.nlm;
   k_apply<<<(nlm + 255) / 256, 256, 0, h->stream>>>(nlm, h->nk, h->g, h->grid.d_lm_l.p, h->d_lm2k.p, h->d_gu.p,
-                                                    h->d_gn.p, h->d_drift.p, d_sigma, d_u, d_n);
+                                                    h->d_gn.p, h->d_drift.p, d_sigma, d_u, d_n); ++h->n_launch;
   VG_CUDA(cudaGetLastError());
 }
 
@@ -342,12 +343,13 @@ __global__ void __launch_bounds__(256) k_advance_1d(const double* __restrict__ m
 }
 
 void launch_advance_1d(vg_handle* h, const double* d_sigma, double dt) {
+  PhaseScope ps(h, VG_PH_ADVANCE_1D);
   int nxt = 1 - h->cur;
   VG_CUDA(cudaMemsetAsync(h->d_maxbits.p + nxt, 0, sizeof(unsigned long long), h->stream));
   k_advance_1d<<<(h->nk + 255) / 256, 256, 0, h->stream>>>(
       h->d_mem[h->cur].p, h->d_mem[nxt].p, h->ne, h->nr, h->nk, dt, d_sigma, h->d_kdeg.p, h->d_k2lm.p, h->d_Jr.p,
       h->d_xUn.p, h->d_xVn.p, h->d_dUn.p, h->d_dVn.p, h->d_mu.p, h->d_MkPerDt.p, h->d_active1d.p,
-      h->d_mnorm.p + (size_t)nxt * h->nk, h->d_maxbits.p + nxt);
+      h->d_mnorm.p + (size_t)nxt * h->nk, h->d_maxbits.p + nxt); ++h->n_launch;
   VG_CUDA(cudaGetLastError());
 }
 
@@ -373,7 +375,7 @@ __global__ void k_mem_norm(const double* __restrict__ mem, int ne, int nk, doubl
 void compute_mem_norm(vg_handle* h, int buf) {
   VG_CUDA(cudaMemsetAsync(h->d_maxbits.p + buf, 0, sizeof(unsigned long long), h->stream));
   k_mem_norm<<<(h->nk + 255) / 256, 256, 0, h->stream>>>(h->d_mem[buf].p, h->ne, h->nk,
-                                                         h->d_mnorm.p + (size_t)buf * h->nk, h->d_maxbits.p + buf);
+                                                         h->d_mnorm.p + (size_t)buf * h->nk, h->d_maxbits.p + buf); ++h->n_launch;
   VG_CUDA(cudaGetLastError());
 }
 

@@ -81,27 +81,27 @@ void fourier_analysis_dev(vg_handle* h, const double* d_f, int batch, double* d_
   const Grid& G = h->grid;
   dim3 grid(G.nlat, batch);
   k_fourier_analysis<<<grid, 128, G.nphi * sizeof(double), h->stream>>>(d_f, G.nphi, G.nlat, G.M, G.d_cos.p,
-                                                                         G.d_sin.p, d_F);
+                                                                         G.d_sin.p, d_F); ++h->n_launch;
   VG_CUDA(cudaGetLastError());
 }
 void legendre_analysis_dev(vg_handle* h, const double* d_F, int batch, double* d_q) {
   const Grid& G = h->grid;
   long long warps = (long long)G.nlm * batch;
   k_legendre_analysis<<<(unsigned)((warps * 32 + 255) / 256), 256, 0, h->stream>>>(
-      d_F, G.nlat, G.M, G.nlm, batch, G.d_lm_m.p, G.d_plm.p, G.d_wts.p, d_q);
+      d_F, G.nlat, G.M, G.nlm, batch, G.d_lm_m.p, G.d_plm.p, G.d_wts.p, d_q); ++h->n_launch;
   VG_CUDA(cudaGetLastError());
 }
 void legendre_synth_dev(vg_handle* h, const double* d_q, int batch, double* d_G) {
   const Grid& G = h->grid;
   dim3 grid((G.nlat + 63) / 64, G.M, batch);
-  k_legendre_synth<<<grid, 64, 0, h->stream>>>(d_q, G.lmax, G.nlat, G.M, G.nlm, G.d_mbeg.p, G.d_plm.p, d_G);
+  k_legendre_synth<<<grid, 64, 0, h->stream>>>(d_q, G.lmax, G.nlat, G.M, G.nlm, G.d_mbeg.p, G.d_plm.p, d_G); ++h->n_launch;
   VG_CUDA(cudaGetLastError());
 }
 void fourier_synth_dev(vg_handle* h, const double* d_G, int batch, double* d_f) {
   const Grid& G = h->grid;
   dim3 grid(G.nlat, batch);
   k_fourier_synth<<<grid, 128, 2 * G.M * sizeof(double), h->stream>>>(d_G, G.nphi, G.nlat, G.M, G.d_cos.p,
-                                                                       G.d_sin.p, d_f);
+                                                                       G.d_sin.p, d_f); ++h->n_launch;
   VG_CUDA(cudaGetLastError());
 }
 

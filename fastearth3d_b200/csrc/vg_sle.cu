@@ -270,7 +270,7 @@ void sle_solve_dev(vg_handle* h, double dt, bool report_only) {
   if (!p.sle_warm_start) VG_CUDA(cudaMemsetAsync(h->d_rsl.p, 0, ng * sizeof(double), s));
   VG_CUDA(cudaMemsetAsync(h->d_wcorr.p, 0, ng * sizeof(double), s));
   VG_CUDA(cudaMemsetAsync(sc, 0, sizeof(SleScalars), s));
-  k_ocean0<<<eg, eb, 0, s>>>(ng, h->d_z_bed_eq.p, h->d_ice_now.p, h->d_dice_now.p, h->d_C0.p);
+  k_ocean0<<<eg, eb, 0, s>>>(ng, h->d_z_bed_eq.p, h->d_ice_now.p, h->d_dice_now.p, h->d_C0.p); ++h->n_launch;
   launch_drift(h);  // response_begin_step
   h->n_inner_last = 0;
   h->n_flip_last = 0;
@@ -278,28 +278,29 @@ void sle_solve_dev(vg_handle* h, double dt, bool report_only) {
     if (p.sle_fixed_ocean) {
       if (io == 1) VG_CUDA(cudaMemcpyAsync(h->d_C.p, h->d_C0.p, ng * sizeof(double), cudaMemcpyDeviceToDevice, s));
     } else if (io == 1) {
-      k_ocean<<<eg, eb, 0, s>>>(ng, h->d_z_bed_eq.p, h->d_rsl.p, h->d_ice_now.p, h->d_C.p);
+      k_ocean<<<eg, eb, 0, s>>>(ng, h->d_z_bed_eq.p, h->d_rsl.p, h->d_ice_now.p, h->d_C.p); ++h->n_launch;
     } else {
       VG_CUDA(cudaMemcpyAsync(h->d_C.p, h->d_C_next.p, ng * sizeof(double), cudaMemcpyDeviceToDevice, s));
     }
     k_pass_setup<<<nlat, 128, 0, s>>>(nphi, h->d_ice_now.p, h->d_dice_now.p, h->d_C.p, h->d_C0.p, h->d_z_bed_eq.p,
-                                      h->d_dig.p, rp, nlat);
-    k_finalize_C<<<1, 32, 0, s>>>(sc, rp, G.d_wts.p, nlat, dlon);
+                                      h->d_dig.p, rp, nlat); ++h->n_launch;
+    k_finalize_C<<<1, 32, 0, s>>>(sc, rp, G.d_wts.p, nlat, dlon); ++h->n_launch;
     read_scalars(h);
     if (h->h_sc->C_int <= 0.0) break;  // no ocean: nothing to redistribute
-    k_finalize_pass<<<1, 32, 0, s>>>(sc, rp, G.d_wts.p, nlat, dlon, p.sle_subgrid);
-    k_wcorr<<<eg, eb, 0, s>>>(ng, p.sle_subgrid, h->d_z_bed_eq.p, h->d_C.p, h->d_C0.p, h->d_wcorr.p);
+    k_finalize_pass<<<1, 32, 0, s>>>(sc, rp, G.d_wts.p, nlat, dlon, p.sle_subgrid); ++h->n_launch;
+    k_wcorr<<<eg, eb, 0, s>>>(ng, p.sle_subgrid, h->d_z_bed_eq.p, h->d_C.p, h->d_C0.p, h->d_wcorr.p); ++h->n_launch;
     for (int ii = 1; ii <= p.sle_n_inner; ++ii) {
+      PhaseScope ps(h, VG_PH_SLE);
       k_load_fourier<<<nlat, 128, nphi * sizeof(double), s>>>(nphi, nlat, M, h->d_dig.p, h->d_C.p, h->d_rsl.p,
-                                                              h->d_wcorr.p, G.d_cos.p, G.d_sin.p, h->d_F.p);
+                                                              h->d_wcorr.p, G.d_cos.p, G.d_sin.p, h->d_F.p); ++h->n_launch;
       legendre_analysis_dev(h, h->d_F.p, 1, h->d_sigma.p);
       launch_apply(h, h->d_sigma.p, h->d_ulm.p, h->d_ulm.p + 2 * (size_t)nlm);
       legendre_synth_dev(h, h->d_ulm.p, 2, h->d_Gs.p);
       k_synth_sraw<<<nlat, 128, 4 * M * sizeof(double), s>>>(nphi, nlat, M, h->d_Gs.p, G.d_cos.p, G.d_sin.p,
-                                                             h->d_C.p, nullptr, h->d_Sraw.p, rp);
-      k_dphi<<<1, 32, 0, s>>>(sc, rp, G.d_wts.p, nlat, dlon);
-      k_rsl_update<<<nlat, 128, 0, s>>>(nphi, sc, h->d_Sraw.p, h->d_C.p, h->d_rsl.p, rp, nlat);
-      k_conv<<<1, 32, 0, s>>>(sc, rp, nlat);
+                                                             h->d_C.p, nullptr, h->d_Sraw.p, rp); ++h->n_launch;
+      k_dphi<<<1, 32, 0, s>>>(sc, rp, G.d_wts.p, nlat, dlon); ++h->n_launch;
+      k_rsl_update<<<nlat, 128, 0, s>>>(nphi, sc, h->d_Sraw.p, h->d_C.p, h->d_rsl.p, rp, nlat); ++h->n_launch;
+      k_conv<<<1, 32, 0, s>>>(sc, rp, nlat); ++h->n_launch;
       read_scalars(h);
       h->n_inner_last = ii;
       if (h->h_sc->dmax <= p.sle_tol * std::max(h->h_sc->smax, TINY)) break;
@@ -307,22 +308,22 @@ void sle_solve_dev(vg_handle* h, double dt, bool report_only) {
     h->n_outer_last = io;
     if (p.sle_fixed_ocean) break;
     k_coast<<<nlat, 128, 0, s>>>(nphi, h->d_z_bed_eq.p, h->d_rsl.p, h->d_ice_now.p, h->d_C.p, h->d_C_next.p, rp,
-                                 nlat);
-    k_flips<<<1, 32, 0, s>>>(sc, rp, nlat);
+                                 nlat); ++h->n_launch;
+    k_flips<<<1, 32, 0, s>>>(sc, rp, nlat); ++h->n_launch;
     read_scalars(h);
     h->n_flip_last = h->h_sc->flips;
     if (h->h_sc->flips == 0) break;
   }
   // closing load, its analysis, and the memory advance (src/vilma_sle.f90:353-358)
   k_load_fourier<<<nlat, 128, nphi * sizeof(double), s>>>(nphi, nlat, M, h->d_dig.p, h->d_C.p, h->d_rsl.p,
-                                                          h->d_wcorr.p, G.d_cos.p, G.d_sin.p, h->d_F.p);
+                                                          h->d_wcorr.p, G.d_cos.p, G.d_sin.p, h->d_F.p); ++h->n_launch;
   legendre_analysis_dev(h, h->d_F.p, 1, h->d_sigma.p);
   if (!report_only) {
     if (h->lat_visc) visc3d_advance(h, h->d_sigma.p, dt);
     launch_advance_1d(h, h->d_sigma.p, dt);
   }
-  k_rowsum<<<nlat, 128, 0, s>>>(nphi, h->d_C.p, h->d_rsl.p, rp + RP_MASS * nlat);
-  k_mass<<<1, 32, 0, s>>>(sc, rp, G.d_wts.p, nlat, dlon);
+  k_rowsum<<<nlat, 128, 0, s>>>(nphi, h->d_C.p, h->d_rsl.p, rp + RP_MASS * nlat); ++h->n_launch;
+  k_mass<<<1, 32, 0, s>>>(sc, rp, G.d_wts.p, nlat, dlon); ++h->n_launch;
 }
 
 // solid_earth_update without rotation; d_ice1 is the interval-end ice on the device
@@ -342,7 +343,7 @@ void update_dev(vg_handle* h, const double* d_ice1, double dt_yr) {
   };
   if (span <= 0.0) {
     k_ice_interp<<<eg, eb, 0, s>>>(ng, 0.0, h->d_h_ice.p, h->d_h_ice.p, h->d_h_ice_eq.p, h->d_ice_now.p,
-                                   h->d_dice_now.p);
+                                   h->d_dice_now.p); ++h->n_launch;
     sle_solve_dev(h, 0.0, true);
     h->worst_mass_resid = mass_resid();
   } else {
@@ -361,7 +362,7 @@ void update_dev(vg_handle* h, const double* d_ice1, double dt_yr) {
       double tau0 = h->mem_norm;
       double frac = (t + dtc - t0) / span;
       k_ice_interp<<<eg, eb, 0, s>>>(ng, frac, h->d_h_ice.p, d_ice1, h->d_h_ice_eq.p, h->d_ice_now.p,
-                                     h->d_dice_now.p);
+                                     h->d_dice_now.p); ++h->n_launch;
       VG_CUDA(cudaGetLastError());
       h->n_solve++;
       sle_solve_dev(h, dtc, false);
@@ -389,7 +390,7 @@ void update_dev(vg_handle* h, const double* d_ice1, double dt_yr) {
     }
   }
   VG_CUDA(cudaMemcpyAsync(h->d_h_ice.p, d_ice1, ng * sizeof(double), cudaMemcpyDeviceToDevice, s));
-  k_zbed<<<eg, eb, 0, s>>>(ng, h->d_z_bed_eq.p, h->d_rsl.p, h->d_zbed.p);
+  k_zbed<<<eg, eb, 0, s>>>(ng, h->d_z_bed_eq.p, h->d_rsl.p, h->d_zbed.p); ++h->n_launch;
   VG_CUDA(cudaGetLastError());
   h->time_yr += dt_yr;
   update_bsl(h);
@@ -401,7 +402,7 @@ void update_bsl(vg_handle* h) {
   const int nlat = G.nlat, nphi = G.nphi;
   cudaStream_t s = h->stream;
   double* rp = h->d_rowpart.p;
-  k_bsl_rows<<<nlat, 128, 0, s>>>(nphi, h->d_h_ice.p, h->d_h_ice_eq.p, h->d_C.p, h->d_C0.p, rp, nlat);
+  k_bsl_rows<<<nlat, 128, 0, s>>>(nphi, h->d_h_ice.p, h->d_h_ice_eq.p, h->d_C.p, h->d_C0.p, rp, nlat); ++h->n_launch;
   VG_CUDA(cudaGetLastError());
   std::vector<double> rows((size_t)RP_N * nlat);
   VG_CUDA(cudaMemcpyAsync(rows.data(), rp, rows.size() * sizeof(double), cudaMemcpyDeviceToHost, s));

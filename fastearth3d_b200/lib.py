@@ -38,6 +38,9 @@ _SIGS = [
     ("vg_set_state", [_VP, _P, _P, _P, _P, _P, _P, C.c_double]),
     ("vg_sht_analysis", [_VP, _P, _P]),
     ("vg_sht_synthesis", [_VP, _P, _P]),
+    ("vg_stream", [_VP, C.POINTER(C.c_void_p)]),
+    ("vg_profile_enable", [_VP, C.c_int]),
+    ("vg_profile_read", [_VP, _P, C.POINTER(C.c_longlong)]),
 ]
 EXPORTS = [n for n, _ in _SIGS] + ["vg_last_error"]
 
@@ -177,6 +180,21 @@ class Model:
         a = [np.zeros(2 * self.nk) for _ in range(3)]
         self._c(lib().vg_get_drift(self.h, *[ptr(x) for x in a]))
         return [_unpack(x) for x in a]
+
+    def stream_ptr(self):
+        s = C.c_void_p()
+        self._c(lib().vg_stream(self.h, C.byref(s)))
+        return s.value
+
+    def profile_enable(self, on=True):
+        self._c(lib().vg_profile_enable(self.h, int(on)))
+
+    def profile_read(self):
+        """Per-phase (milliseconds, calls) since the last read (and reset)."""
+        ms = np.zeros(4)
+        calls = (C.c_longlong * 4)()
+        self._c(lib().vg_profile_read(self.h, ptr(ms), calls))
+        return ms, np.array(calls[:])
 
     def analysis(self, f):
         q = np.zeros(2 * self.nlm)

@@ -73,6 +73,11 @@ typedef struct vg_params {
   int visc3d_precision;
 } vg_params;
 
+/* Phase timers (the reference's [PROFILE] buckets: drift solve, memory
+ * advance, 3-D advance, sea-level transforms + grid work; src/vilma_drive.f90:
+ * 219-305). */
+enum { VG_PH_DRIFT = 0, VG_PH_ADVANCE_1D = 1, VG_PH_VISC3D = 2, VG_PH_SLE = 3, VG_NPHASE = 4 };
+
 typedef struct vg_info {
   int lmax, nlat, nphi, nlm, nr, ne, ndof, nk, ne3d;
   int n_sub_last;         /* sub-steps taken by the last vg_update */
@@ -81,6 +86,7 @@ typedef struct vg_info {
   double worst_mass_resid;
   double bsl;             /* barystatic sea level diagnostic [m] */
   int n_outer_last, n_inner_last, n_coast_flip_last;
+  long long n_launch;     /* kernels launched by the time step so far */
 } vg_info;
 
 typedef struct vg_handle vg_handle;
@@ -146,6 +152,15 @@ int vg_set_state(vg_handle* h, const double* Are, const double* Aim, const doubl
  * src/vilma_sht.f90:204-226), host arrays in and out. */
 int vg_sht_analysis(vg_handle* h, const double* f, double* q_lm);
 int vg_sht_synthesis(vg_handle* h, const double* q_lm, double* f);
+
+/* The CUDA stream (cudaStream_t) all of the handle's work is ordered on, so a
+ * caller can record events on it. */
+int vg_stream(vg_handle* h, void** stream);
+/* Enable (1) or disable (0) the phase timers; vg_profile_read returns the
+ * accumulated milliseconds and call counts per phase (VG_NPHASE each) since
+ * the last read and resets them. */
+int vg_profile_enable(vg_handle* h, int on);
+int vg_profile_read(vg_handle* h, double* ms, long long* calls);
 
 int vg_destroy(vg_handle* h);
 const char* vg_last_error(const vg_handle* h);
