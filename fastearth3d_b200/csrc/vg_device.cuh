@@ -41,8 +41,8 @@ __device__ __forceinline__ void strain_coeffs(double u1, double u2, double v1, d
 
 // Degree-1 bordered system, dense band storage with kl = ku = nd, solved for
 // up to 4 right-hand sides held in shared memory (xsh[nrhs][ns]); dgbtrs order,
-// CTA-parallel inner loops. ab[(row - 1) * ns + (col - 1)].
-__device__ __forceinline__ void deg1_solve_cta(const double* __restrict__ ab, int ns, int kl, int kv,
+// CTA-parallel inner loops. Column-major band storage ab[(col - 1) * ldab + (row - 1)].
+__device__ __forceinline__ void deg1_solve_cta(const double* __restrict__ ab, int ldab, int ns, int kl, int kv,
                                                const int* __restrict__ ipiv, double* xsh, int nrhs) {
   for (int j = 1; j <= ns - 1; ++j) {
     int lm = min(kl, ns - j);
@@ -57,21 +57,21 @@ __device__ __forceinline__ void deg1_solve_cta(const double* __restrict__ ab, in
     for (int t = threadIdx.x; t < lm * nrhs; t += blockDim.x) {
       int i = 1 + t / nrhs, rr = t % nrhs;
       double* x = xsh + rr * ns;
-      x[j + i - 1] -= ab[(size_t)(kv + i) * ns + (j - 1)] * x[j - 1];
+      x[j + i - 1] -= ab[(size_t)(j - 1) * ldab + (kv + i)] * x[j - 1];
     }
     __syncthreads();
   }
   for (int j = ns; j >= 1; --j) {
     if ((int)threadIdx.x < nrhs) {
       double* x = xsh + threadIdx.x * ns;
-      x[j - 1] = x[j - 1] / ab[(size_t)kv * ns + (j - 1)];
+      x[j - 1] = x[j - 1] / ab[(size_t)(j - 1) * ldab + kv];
     }
     __syncthreads();
     int lm = min(kv, j - 1);
     for (int t = threadIdx.x; t < lm * nrhs; t += blockDim.x) {
       int i = 1 + t / nrhs, rr = t % nrhs;
       double* x = xsh + rr * ns;
-      x[j - i - 1] -= ab[(size_t)(kv - i) * ns + (j - 1)] * x[j - 1];
+      x[j - i - 1] -= ab[(size_t)(j - 1) * ldab + (kv - i)] * x[j - 1];
     }
     __syncthreads();
   }

@@ -20,7 +20,11 @@
 
 #include "../../include/vilma_gpu.h"
 
-#define VG_CUDA(call)                                                                     \
+// leading dimension of the per-column band records of degrees >= 2:
+// rows 0..18 = dgbtf2 band (kl = ku = 6), 19 = 1/pivot, 20 = pivot offset
+#define VG_LDAB 21
+
+#define VG_CUDA(call)                                                                  \
   do {                                                                                   \
     cudaError_t _e = (call);                                                             \
     if (_e != cudaSuccess)                                                               \
@@ -129,9 +133,13 @@ struct vg_handle {
   std::vector<char> active1d_h;
   std::vector<int> e3d_h;
   // operators
-  vg::DArr<double> d_ab, d_dr, d_dc;  // degrees 2..lmax
+  vg::DArr<double> d_ab, d_dr, d_dc, d_rdiag;  // degrees 2..lmax (band, column-major, ldab 19)
   vg::DArr<int> d_ipiv;
-  vg::DArr<double> d_ab1, d_dr1, d_dc1, d_null1;  // degree 1
+  vg::DArr<double> d_ab1, d_dr1, d_dc1, d_null1, d_G1;  // degree 1 (bordered, dense band)
+  vg::DArr<double> d_bh;                        // equilibrated drift RHS (2, 2*nr, nk)
+  vg::DArr<double> d_Krhs;                      // dissipative-forcing coefficients (lmax+1, ne, 48)
+  vg::DArr<int4> d_tasks;                       // drift sweep tasks: (degree, first slot, slots)
+  int ntask = 0;
   vg::DArr<int> d_ipiv1;
   // per-element / per-degree constants
   vg::DArr<double> d_r, d_mu, d_MkPerDt;

@@ -1,8 +1,19 @@
 // Field-driver kernels of the 1-D (spectral) path: the per-(l,m) drift solve
 // with the reference's skip gate, the affine apply, and the forward-Euler
-// memory advance fused with the per-slot memory norm that the next drift gate
-// and the stepper's guard read (src/vilma_response.f90:679-864, 944-992;
+// memory advance with the per-slot memory norm that the next drift gate and
+// the stepper's guard read (src/vilma_response.f90:679-864, 944-992;
 // src/vilma_viscoelastic.f90:329-589).
+//
+// Drift solve (degrees >= 2), two kernels:
+//   k_drift_rhs    one thread per (slot, re/im, node): the dissipative forcing
+//                  -int tau:d eps at the node's U and V dofs from its two
+//                  elements, equilibrated (b = Dr f). Streams the memory state
+//                  with full parallelism.
+//   k_drift_solve  one thread per (slot, re/im): the pivoted band sweeps of
+//                  dgbtrs with the active window in registers (7 values in the
+//                  L sweep, kl = 6; 13 in the U sweep, kv = 12). Only the L-sweep
+//                  output y goes through memory (L2-resident scratch).
+// Degree 1 (bordered, dense): a mat-vec with the precomputed response block G1.
 #include <cstring>
 
 #include "vg_device.cuh"
@@ -11,193 +22,392 @@
 namespace vg {
 
 struct DriftArgs {
-  const double* mem;            // current buffer
-  const double* mnorm;          // per-slot norms of the current buffer
+  const double* mem;                  // current state buffer
+  const double* mnorm;                // per-slot norms of the current buffer
   const unsigned long long* maxbits;  // global max of the current buffer
   double skip_tol;
   const double* r;
   const double *sa, *sb, *sc, *nrmc;
-  const double *ab, *dr, *dc;
+  const double *ab, *dr, *dc, *rdiag;
   const int* ipiv;
   const int* kdeg;
-  double* xs;                   // scratch (2, nd, nk)
+  double* bh;  // equilibrated RHS (2, 2*nr, nk)
+  double* ys;  // L-sweep output (2, nd, nk)
   double *dUn, *dVn, *drift;
-  int ne, nr, nd, nk, lmax;
-  // degree 1
-  const double *ab1, *dr1, *dc1, *null1;
-  const int* ipiv1;
-  int kl1, kv1, deg1_cm;
+  int ne, nr, nd, nk;
+  const double *dr1, *null1, *G1;
+  int deg1_cm;
+  const double* K;     // dissipative-forcing coefficients (lmax+1, ne, 48)
+  const int4* tasks;   // sweep tasks (degree, first slot, slots)
+  int ntask;
 };
 
-// Dissipative forcing -(tau^V : d eps) of one (slot, ri) into a strided column x
-// (src/vilma_viscoelastic.f90:441-480). x must be zero on entry.
-__device__ __forceinline__ void dissipative_rhs_col(const DriftArgs& A, int l, int k, int ri, double* x, size_t st) {
+// Element forcing of one (slot, re/im) at two of its test dofs, from the
+// precomputed linear map K (floc_t = sum_{s,m} K[t][s][m] mem_s[m]).
+__device__ __forceinline__ void element_floc2(const DriftArgs& A, int l, int k, int ri, int e, int t0, int t1,
+                                              double& f0, double& f1) {
+  const double* Kp = A.K + ((size_t)l * A.ne + e) * 48;
+  double a0 = 0.0, a1 = 0.0;
+#pragma unroll
+  for (int s3 = 0; s3 < 3; ++s3)
+#pragma unroll
+    for (int m = 0; m < 4; ++m) {
+      const double v = A.mem[mem_idx(s3, ri, e, m, k, A.ne, A.nk)];
+      a0 += __ldg(&Kp[(t0 * 3 + s3) * 4 + m]) * v;
+      a1 += __ldg(&Kp[(t1 * 3 + s3) * 4 + m]) * v;
+    }
+  f0 = a0;
+  f1 = a1;
+}
+
+__device__ __forceinline__ double skip_threshold(const DriftArgs& A) {
+  return A.skip_tol * __longlong_as_double((long long)*A.maxbits);
+}
+
+// One element's contribution to the four test dofs (U_e, U_e+1, V_e, V_e+1):
+// 2-point radial Gauss quadrature of sum_lam norm_lam tau^lam d eps^lam
+// (src/vilma_viscoelastic.f90:441-480).
+__device__ __forceinline__ void element_floc(const DriftArgs& A, int l, int k, int ri, int e, double floc[4]) {
   const double xg = 0.5773502691896257;
   const double* sa = A.sa + l * 16;
   const double* sb = A.sb + l * 16;
   const double* sc = A.sc + l * 16;
   const double* nrm = A.nrmc + l * 4;
-  for (int e = 0; e < A.ne; ++e) {
-    double rk = A.r[e], rk1 = A.r[e + 1], h = rk1 - rk;
-    double Am[4], Bm[4], Cm[4];
+  double rk = A.r[e], rk1 = A.r[e + 1], h = rk1 - rk;
+  double Am[4], Bm[4], Cm[4];
 #pragma unroll
-    for (int m = 0; m < 4; ++m) {
-      Am[m] = A.mem[mem_idx(0, ri, e, m, k, A.ne, A.nk)];
-      Bm[m] = A.mem[mem_idx(1, ri, e, m, k, A.ne, A.nk)];
-      Cm[m] = A.mem[mem_idx(2, ri, e, m, k, A.ne, A.nk)];
-    }
-    double floc[4] = {0, 0, 0, 0};
+  for (int m = 0; m < 4; ++m) {
+    Am[m] = A.mem[mem_idx(0, ri, e, m, k, A.ne, A.nk)];
+    Bm[m] = A.mem[mem_idx(1, ri, e, m, k, A.ne, A.nk)];
+    Cm[m] = A.mem[mem_idx(2, ri, e, m, k, A.ne, A.nk)];
+  }
 #pragma unroll
-    for (int ig = 0; ig < 2; ++ig) {
-      double ra = 0.5 * (h * (ig ? xg : -xg) + rk + rk1);
-      double psik = (rk1 - ra) / h, psik1 = (ra - rk) / h;
-      double tauV[4];
+  for (int t = 0; t < 4; ++t) floc[t] = 0.0;
 #pragma unroll
-      for (int m = 0; m < 4; ++m) tauV[m] = Am[m] / h + Bm[m] * psik / ra + Cm[m] * psik1 / ra;
+  for (int ig = 0; ig < 2; ++ig) {
+    double ra = 0.5 * (h * (ig ? xg : -xg) + rk + rk1);
+    double psik = (rk1 - ra) / h, psik1 = (ra - rk) / h;
+    double tauV[4];
 #pragma unroll
-      for (int t = 0; t < 4; ++t) {
-        double D = 0.0;
+    for (int m = 0; m < 4; ++m) tauV[m] = Am[m] / h + Bm[m] * psik / ra + Cm[m] * psik1 / ra;
 #pragma unroll
-        for (int m = 0; m < 4; ++m) {
-          double deps = sa[t * 4 + m] / h + sb[t * 4 + m] * psik / ra + sc[t * 4 + m] * psik1 / ra;
-          D = D + nrm[m] * tauV[m] * deps;
-        }
-        floc[t] = floc[t] - D * ra * ra * h * 0.5;
+    for (int t = 0; t < 4; ++t) {
+      double D = 0.0;
+#pragma unroll
+      for (int m = 0; m < 4; ++m) {
+        double deps = __ldg(&sa[t * 4 + m]) / h + __ldg(&sb[t * 4 + m]) * psik / ra + __ldg(&sc[t * 4 + m]) * psik1 / ra;
+        D = D + __ldg(&nrm[m]) * tauV[m] * deps;
       }
+      floc[t] = floc[t] - D * ra * ra * h * 0.5;
     }
-    x[(size_t)(4 * e) * st] += floc[0];
-    x[(size_t)(4 * e + 4) * st] += floc[1];
-    x[(size_t)(4 * e + 1) * st] += floc[2];
-    x[(size_t)(4 * e + 5) * st] += floc[3];
   }
 }
 
-__device__ __forceinline__ void band_solve_col(const double* __restrict__ ab, int n, const int* __restrict__ ipiv,
-                                               double* x, size_t st) {
-  // dgbtrs order, kl = 6, kv = 12; ab[(row - 1) * n + (col - 1)] (band storage row kv + 1 + i - j)
-  constexpr int kl = 6, kv = 12;
-  for (int j = 1; j <= n - 1; ++j) {
-    int lm = min(kl, n - j);
-    int l = __ldg(&ipiv[j - 1]) + 1;
-    if (l != j) {
-      double t = x[(size_t)(l - 1) * st];
-      x[(size_t)(l - 1) * st] = x[(size_t)(j - 1) * st];
-      x[(size_t)(j - 1) * st] = t;
-    }
-    double t = x[(size_t)(j - 1) * st];
-    for (int i = 1; i <= lm; ++i) x[(size_t)(j + i - 1) * st] -= __ldg(&ab[(size_t)(kv + i) * n + (j - 1)]) * t;
-  }
-  for (int j = n; j >= 1; --j) {
-    double xj = x[(size_t)(j - 1) * st] / __ldg(&ab[(size_t)kv * n + (j - 1)]);
-    x[(size_t)(j - 1) * st] = xj;
-    int lm = min(kv, j - 1);
-    for (int i = 1; i <= lm; ++i) x[(size_t)(j - i - 1) * st] -= __ldg(&ab[(size_t)(kv - i) * n + (j - 1)]) * xj;
-  }
-}
-
-// Drift solve for degrees >= 2: one thread per slot k, real and imaginary
-// histories one after the other (src/vilma_response.f90:744-802).
-__global__ void __launch_bounds__(128) k_drift(DriftArgs A) {
-  int k = blockIdx.x * blockDim.x + threadIdx.x;
-  if (k >= A.nk) return;
+// b(U_node) = dr * (floc1(e = node-1) + floc0(e = node)), likewise V with floc3/floc2:
+// the reference's accumulation order (element e adds to nodes e, e+1 in turn).
+__global__ void __launch_bounds__(128) k_drift_rhs(DriftArgs A) {
+  int k = blockIdx.x * 32 + threadIdx.x, node = blockIdx.y * 4 + threadIdx.y, ri = blockIdx.z;
+  if (k >= A.nk || node >= A.nr) return;
+  if (A.mnorm[k] <= skip_threshold(A)) return;
   int l = A.kdeg[k];
-  if (l < 2) return;
-  const double thr = A.skip_tol * __longlong_as_double((long long)*A.maxbits);
-  const int nr = A.nr, nd = A.nd, nk = A.nk;
-  if (A.mnorm[k] <= thr) {
-    for (int q = 0; q < 6; ++q) A.drift[(size_t)q * nk + k] = 0.0;
-    for (int ri = 0; ri < 2; ++ri)
-      for (int node = 0; node < nr; ++node) {
-        A.dUn[((size_t)ri * nr + node) * nk + k] = 0.0;
-        A.dVn[((size_t)ri * nr + node) * nk + k] = 0.0;
-      }
-    return;
+  double fU = 0.0, fV = 0.0, a, b2;
+  if (node >= 1) {  // element node-1: its second node's U, V (test dofs 1, 3)
+    element_floc2(A, l, k, ri, node - 1, 1, 3, a, b2);
+    fU = a;
+    fV = b2;
   }
-  const double* ab = A.ab + (size_t)(l - 2) * 19 * nd;
-  const double* dr = A.dr + (size_t)(l - 2) * nd;
-  const double* dc = A.dc + (size_t)(l - 2) * nd;
-  const int* ipiv = A.ipiv + (size_t)(l - 2) * nd;
-  for (int ri = 0; ri < 2; ++ri) {
-    double* x = A.xs + (size_t)ri * nd * nk + k;
-    for (int i = 0; i < nd; ++i) x[(size_t)i * nk] = 0.0;
-    dissipative_rhs_col(A, l, k, ri, x, nk);
-    for (int i = 0; i < nd; ++i) x[(size_t)i * nk] = __ldg(&dr[i]) * x[(size_t)i * nk];
-    band_solve_col(ab, nd, ipiv, x, nk);
-    for (int node = 0; node < nr; ++node) {
-      A.dUn[((size_t)ri * nr + node) * nk + k] = __ldg(&dc[4 * node]) * x[(size_t)(4 * node) * nk];
-      A.dVn[((size_t)ri * nr + node) * nk + k] = __ldg(&dc[4 * node + 1]) * x[(size_t)(4 * node + 1) * nk];
-    }
-    int us = 4 * (nr - 1);
-    A.drift[(size_t)(0 + ri) * nk + k] = dc[us] * x[(size_t)us * nk];            // dUa
-    A.drift[(size_t)(2 + ri) * nk + k] = dc[us + 2] * x[(size_t)(us + 2) * nk];  // dFa
-    A.drift[(size_t)(4 + ri) * nk + k] = dc[us + 1] * x[(size_t)(us + 1) * nk];  // dVa
+  if (node < A.ne) {  // element node: its first node's U, V (test dofs 0, 2)
+    element_floc2(A, l, k, ri, node, 0, 2, a, b2);
+    fU = fU + a;
+    fV = fV + b2;
+  }
+  const double* dr = (l == 1) ? A.dr1 : A.dr + (size_t)(l - 2) * A.nd;
+  double* b = A.bh + ((size_t)ri * 2 * A.nr + 2 * node) * A.nk + k;
+  b[0] = __ldg(&dr[4 * node]) * fU;
+  b[A.nk] = __ldg(&dr[4 * node + 1]) * fV;
+}
+
+// ---- shared-memory staging of the sweeps (cp.async, double-buffered) ----
+constexpr int SW_CH = 32;                            // band columns (sweep steps) per chunk
+constexpr int SW_BAND = 2 * SW_CH * VG_LDAB;         // two band chunks
+constexpr int SW_AUX = 2 * SW_CH * 32;               // two chunks of per-lane values (b or y)
+constexpr int SW_WARP = SW_BAND + SW_AUX;            // doubles of shared memory per warp
+constexpr int SW_WARPS = 4;                          // warps (tasks) per block
+
+__device__ __forceinline__ void cp8(double* s, const double* g) {
+  unsigned sa = (unsigned)__cvta_generic_to_shared(s);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(sa), "l"(g) : "memory");
+}
+__device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+
+// band records of columns [c0, c0 + SW_CH) of one degree; zero outside [0, nd)
+__device__ __forceinline__ void stage_band(double* dst, const double* ab, int c0, int nd, int lane) {
+  for (int t = lane; t < SW_CH * VG_LDAB; t += 32) {
+    int col = c0 + t / VG_LDAB;
+    if (col >= 0 && col < nd)
+      cp8(dst + t, ab + (size_t)col * VG_LDAB + (t % VG_LDAB));
+    else
+      dst[t] = 0.0;
   }
 }
 
-// Degree-1 drift (slots k = 0, 1): bordered dense system, CTA-parallel sweeps,
+// Drift sweeps, one warp per task: up to 16 slots of one degree x (re, im).
+// The degree's band columns stream through shared memory in chunks of 32 so
+// that every load on the recurrence is a shared-memory load; the per-lane
+// entering values (RHS in the L sweep, y in the U sweep) are staged the same
+// way one chunk ahead.
+__global__ void __launch_bounds__(128) k_drift_solve(DriftArgs A) {
+  extern __shared__ double smem[];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int tix = blockIdx.x * SW_WARPS + warp;
+  if (tix >= A.ntask) return;  // whole warp
+  const int4 T = A.tasks[tix];
+  const int l = T.x, k0 = T.y, nsl = T.z;
+  const int sl = lane & 15, ri = lane >> 4;
+  const bool valid = sl < nsl;
+  const int k = k0 + (valid ? sl : 0);
+  const int nr = A.nr, nd = A.nd;
+  const size_t nk = A.nk;
+  double* dUn = A.dUn + (size_t)ri * nr * nk + k;
+  double* dVn = A.dVn + (size_t)ri * nr * nk + k;
+  const bool active = valid && !(A.mnorm[k] <= skip_threshold(A));
+  if (valid && !active) {  // negligible memory => zero drift
+    for (int node = 0; node < nr; ++node) {
+      dUn[node * nk] = 0.0;
+      dVn[node * nk] = 0.0;
+    }
+    A.drift[(0 + ri) * nk + k] = 0.0;
+    A.drift[(2 + ri) * nk + k] = 0.0;
+    A.drift[(4 + ri) * nk + k] = 0.0;
+  }
+  if (!__any_sync(0xffffffffu, active)) return;
+  double* sband = smem + (size_t)warp * SW_WARP;
+  double* saux = sband + SW_BAND;
+  const double* ab = A.ab + (size_t)(l - 2) * VG_LDAB * nd;
+  const double* dc = A.dc + (size_t)(l - 2) * nd;
+  const double* b = A.bh + ((size_t)ri * 2 * nr) * nk + k;  // b[(2 node + {0,1}) nk]
+  double* y = A.ys + (size_t)ri * nd * nk + k;
+  // entering RHS values of chunk c: U, V of nodes 8c+2 .. 8c+9, slot (2 kbi + uv)
+  auto stage_b = [&](double* dst, int c) {
+#pragma unroll
+    for (int q = 0; q < 16; ++q) {
+      int node = 8 * c + (q >> 1) + 2;
+      if (node < nr)
+        cp8(dst + q * 32 + lane, b + (size_t)(2 * node + (q & 1)) * nk);
+      else
+        dst[q * 32 + lane] = 0.0;
+    }
+  };
+  // ---- L sweep (P and L): window w0..w6 = x(j .. j+6) ----
+  const int nchf = (nd - 1 + SW_CH - 1) / SW_CH;  // steps j = 0 .. nd-2
+  stage_band(sband, ab, 0, nd, lane);
+  stage_b(saux, 0);
+  cp_commit();
+  double w0 = b[0], w1 = b[nk], w2 = 0.0, w3 = 0.0, w4 = b[2 * nk], w5 = b[3 * nk], w6;
+  for (int c = 0; c < nchf; ++c) {
+    const int cur = c & 1;
+    if (c + 1 < nchf) {
+      stage_band(sband + (cur ^ 1) * SW_CH * VG_LDAB, ab, SW_CH * (c + 1), nd, lane);
+      stage_b(saux + (cur ^ 1) * SW_CH * 32, c + 1);
+      cp_commit();
+      cp_wait<1>();
+    } else {
+      cp_wait<0>();
+    }
+    __syncwarp();
+    const double* bandc = sband + cur * SW_CH * VG_LDAB;
+    const double* bin = saux + cur * SW_CH * 32;
+#pragma unroll 4
+    for (int jj = 0; jj < SW_CH; ++jj) {
+      const int j = SW_CH * c + jj, t = jj & 3;
+      if (j > nd - 2) break;
+      // dof j + 6 enters: F_{kb+1}, P_{kb+1} (no forcing), U_{kb+2}, V_{kb+2}
+      w6 = (t < 2) ? 0.0 : bin[(2 * (jj >> 2) + (t - 2)) * 32 + lane];
+      const double* col = bandc + jj * VG_LDAB;
+      const int jp = (int)col[20];
+      const double x0 = w0;
+      double s = w0;
+      s = (jp == 1) ? w1 : s;
+      s = (jp == 2) ? w2 : s;
+      s = (jp == 3) ? w3 : s;
+      s = (jp == 4) ? w4 : s;
+      s = (jp == 5) ? w5 : s;
+      s = (jp == 6) ? w6 : s;
+      w1 = (jp == 1) ? x0 : w1;
+      w2 = (jp == 2) ? x0 : w2;
+      w3 = (jp == 3) ? x0 : w3;
+      w4 = (jp == 4) ? x0 : w4;
+      w5 = (jp == 5) ? x0 : w5;
+      w6 = (jp == 6) ? x0 : w6;
+      w0 = s;
+      if (valid) y[(size_t)j * nk] = w0;
+      w1 -= col[13] * w0;
+      w2 -= col[14] * w0;
+      w3 -= col[15] * w0;
+      w4 -= col[16] * w0;
+      w5 -= col[17] * w0;
+      w6 -= col[18] * w0;
+      w0 = w1;
+      w1 = w2;
+      w2 = w3;
+      w3 = w4;
+      w4 = w5;
+      w5 = w6;
+    }
+    __syncwarp();  // the buffer just read is refilled by the next prefetch
+  }
+  if (valid) y[(size_t)(nd - 1) * nk] = w0;
+  __threadfence_block();  // y stores before this lane's own cp.async reads of them
+  // ---- U sweep: window v0..v12 = x(j-12 .. j), j descending ----
+  // entering y(j - 13) of chunk c (steps j = J0-31 .. J0, J0 = nd-1-32c) at slot j - (J0 - 31)
+  auto stage_y = [&](double* dst, int c) {
+    const int jlo = nd - 1 - SW_CH * c - (SW_CH - 1);
+#pragma unroll 4
+    for (int q = 0; q < SW_CH; ++q) {
+      int src = jlo + q - 13;
+      if (src >= 0 && valid)
+        cp8(dst + q * 32 + lane, y + (size_t)src * nk);
+      else
+        dst[q * 32 + lane] = 0.0;
+    }
+  };
+  const int nchb = (nd + SW_CH - 1) / SW_CH;
+  stage_band(sband, ab, nd - SW_CH, nd, lane);
+  stage_y(saux, 0);
+  cp_commit();
+  double v0, v1, v2, v3, v4, v5, v6, v7, v8, v9, v10, v11, v12;
+#define YAT(i) (((i) >= 0 && valid) ? y[(size_t)(i) * nk] : 0.0)
+  v0 = YAT(nd - 13);
+  v1 = YAT(nd - 12);
+  v2 = YAT(nd - 11);
+  v3 = YAT(nd - 10);
+  v4 = YAT(nd - 9);
+  v5 = YAT(nd - 8);
+  v6 = YAT(nd - 7);
+  v7 = YAT(nd - 6);
+  v8 = YAT(nd - 5);
+  v9 = YAT(nd - 4);
+  v10 = YAT(nd - 3);
+  v11 = YAT(nd - 2);
+  v12 = YAT(nd - 1);
+#undef YAT
+  const int us = 4 * (nr - 1);
+  for (int c = 0; c < nchb; ++c) {
+    const int cur = c & 1, J0 = nd - 1 - SW_CH * c, jlo = J0 - (SW_CH - 1);
+    if (c + 1 < nchb) {
+      stage_band(sband + (cur ^ 1) * SW_CH * VG_LDAB, ab, jlo - SW_CH, nd, lane);
+      stage_y(saux + (cur ^ 1) * SW_CH * 32, c + 1);
+      cp_commit();
+      cp_wait<1>();
+    } else {
+      cp_wait<0>();
+    }
+    __syncwarp();
+    const double* bandc = sband + cur * SW_CH * VG_LDAB;
+    const double* yin = saux + cur * SW_CH * 32;
+#pragma unroll 4
+    for (int jj = SW_CH - 1; jj >= 0; --jj) {
+      const int j = jlo + jj;
+      if (j < 0) break;
+      const double* col = bandc + jj * VG_LDAB;
+      const double xj = v12 * col[19];
+      const int node = j >> 2, typ = j & 3;
+      if (active) {
+        if (typ == 0) dUn[node * nk] = __ldg(&dc[j]) * xj;
+        if (typ == 1) dVn[node * nk] = __ldg(&dc[j]) * xj;
+        if (j >= us) {
+          if (typ == 0) A.drift[(0 + ri) * nk + k] = dc[j] * xj;
+          if (typ == 2) A.drift[(2 + ri) * nk + k] = dc[j] * xj;
+          if (typ == 1) A.drift[(4 + ri) * nk + k] = dc[j] * xj;
+        }
+      }
+      v11 -= col[11] * xj;
+      v10 -= col[10] * xj;
+      v9 -= col[9] * xj;
+      v8 -= col[8] * xj;
+      v7 -= col[7] * xj;
+      v6 -= col[6] * xj;
+      v5 -= col[5] * xj;
+      v4 -= col[4] * xj;
+      v3 -= col[3] * xj;
+      v2 -= col[2] * xj;
+      v1 -= col[1] * xj;
+      v0 -= col[0] * xj;
+      v12 = v11;
+      v11 = v10;
+      v10 = v9;
+      v9 = v8;
+      v8 = v7;
+      v7 = v6;
+      v6 = v5;
+      v5 = v4;
+      v4 = v3;
+      v3 = v2;
+      v2 = v1;
+      v1 = v0;
+      v0 = yin[jj * 32 + lane];
+    }
+    __syncwarp();
+  }
+}
+
+// Degree-1 drift (slots k = 0, 1; 4 right-hand sides): x = G1 b, then the
 // CM-frame projection with the stored null mode (src/vilma_response.f90:770-779).
 __global__ void __launch_bounds__(256) k_drift_deg1(DriftArgs A) {
-  extern __shared__ double xsh[];  // [4][ns]
-  const int nd = A.nd, ns = nd + 1, nr = A.nr, nk = A.nk;
-  const double thr = A.skip_tol * __longlong_as_double((long long)*A.maxbits);
-  __shared__ int s_active[2];
-  if (threadIdx.x < 2) s_active[threadIdx.x] = !(A.mnorm[threadIdx.x] <= thr);
-  for (int i = threadIdx.x; i < 4 * ns; i += blockDim.x) xsh[i] = 0.0;
+  extern __shared__ double sh[];
+  const int nr = A.nr, ncol = 2 * nr, nrow = 2 * nr + 1;
+  const size_t nk = A.nk;
+  double* f = sh;             // [4][ncol]
+  double* x = sh + 4 * ncol;  // [4][nrow]
+  __shared__ int s_act[2];
+  __shared__ double s_c[4];
+  const double thr = skip_threshold(A);
+  if (threadIdx.x < 2) s_act[threadIdx.x] = !(A.mnorm[threadIdx.x] <= thr);
   __syncthreads();
-  if (!s_active[0] && !s_active[1]) {
-    for (int t = threadIdx.x; t < 2; t += blockDim.x) {
-      int k = t;
-      for (int q = 0; q < 6; ++q) A.drift[(size_t)q * nk + k] = 0.0;
-    }
-    for (int t = threadIdx.x; t < 2 * 2 * nr; t += blockDim.x) {
-      int k = t % 2, rest = t / 2, ri = rest % 2, node = rest / 2;
-      A.dUn[((size_t)ri * nr + node) * nk + k] = 0.0;
-      A.dVn[((size_t)ri * nr + node) * nk + k] = 0.0;
-    }
-    return;
-  }
-  if (threadIdx.x < 4) {  // rhs index q = k*2 + ri
-    int k = threadIdx.x / 2, ri = threadIdx.x % 2;
-    if (s_active[k]) {
-      dissipative_rhs_col(A, 1, k, ri, xsh + threadIdx.x * ns, 1);
-      for (int i = 0; i < nd; ++i) xsh[threadIdx.x * ns + i] = A.dr1[i] * xsh[threadIdx.x * ns + i];
-    }
+  for (int t = threadIdx.x; t < 4 * ncol; t += blockDim.x) {
+    int q = t / ncol, c = t % ncol, kk = q >> 1, ri = q & 1;
+    f[t] = s_act[kk] ? A.bh[((size_t)ri * 2 * nr + c) * nk + kk] : 0.0;
   }
   __syncthreads();
-  deg1_solve_cta(A.ab1, ns, A.kl1, A.kv1, A.ipiv1, xsh, 4);
-  for (int t = threadIdx.x; t < 4 * nd; t += blockDim.x) {
-    int q = t / nd, i = t % nd;
-    xsh[q * ns + i] = A.dc1[i] * xsh[q * ns + i];
+  for (int t = threadIdx.x; t < 4 * nrow; t += blockDim.x) {
+    int q = t / nrow, r = t % nrow;
+    const double* G = A.G1 + (size_t)r * ncol;
+    const double* fq = f + q * ncol;
+    double acc = 0.0;
+    for (int c = 0; c < ncol; ++c) acc += __ldg(&G[c]) * fq[c];
+    x[q * nrow + r] = acc;
   }
   __syncthreads();
-  if (A.deg1_cm) {
-    int fs = 4 * (nr - 1) + 2;
-    double fa_n = A.null1[fs];
-    if (fa_n != 0.0) {
-      __shared__ double s_c[4];
-      if (threadIdx.x < 4) s_c[threadIdx.x] = -xsh[threadIdx.x * ns + fs] / fa_n;
-      __syncthreads();
-      for (int t = threadIdx.x; t < 4 * nd; t += blockDim.x) {
-        int q = t / nd, i = t % nd;
-        xsh[q * ns + i] = xsh[q * ns + i] + s_c[q] * A.null1[i];
-      }
-      __syncthreads();
+  const int fs = 4 * (nr - 1) + 2;
+  const double fa_n = A.null1[fs];
+  const bool proj = A.deg1_cm && fa_n != 0.0;
+  if (proj) {
+    if (threadIdx.x < 4) s_c[threadIdx.x] = -x[threadIdx.x * nrow + 2 * nr] / fa_n;
+    __syncthreads();
+    for (int t = threadIdx.x; t < 4 * nrow; t += blockDim.x) {
+      int q = t / nrow, r = t % nrow;
+      int dof = (r < 2 * nr) ? 4 * (r >> 1) + (r & 1) : fs;
+      x[t] = x[t] + s_c[q] * A.null1[dof];
     }
+    __syncthreads();
   }
   for (int t = threadIdx.x; t < 4 * nr; t += blockDim.x) {
-    int q = t / nr, node = t % nr, k = q / 2, ri = q % 2;
-    double u = s_active[k] ? xsh[q * ns + 4 * node] : 0.0;
-    double v = s_active[k] ? xsh[q * ns + 4 * node + 1] : 0.0;
-    A.dUn[((size_t)ri * nr + node) * nk + k] = u;
-    A.dVn[((size_t)ri * nr + node) * nk + k] = v;
+    int q = t / nr, node = t % nr, kk = q >> 1, ri = q & 1;
+    bool act = s_act[kk];
+    A.dUn[((size_t)ri * nr + node) * nk + kk] = act ? x[q * nrow + 2 * node] : 0.0;
+    A.dVn[((size_t)ri * nr + node) * nk + kk] = act ? x[q * nrow + 2 * node + 1] : 0.0;
   }
   if (threadIdx.x < 4) {
-    int q = threadIdx.x, k = q / 2, ri = q % 2, us = 4 * (nr - 1);
-    bool act = s_active[k];
-    A.drift[(size_t)(0 + ri) * nk + k] = act ? xsh[q * ns + us] : 0.0;
+    int q = threadIdx.x, kk = q >> 1, ri = q & 1;
+    bool act = s_act[kk];
+    A.drift[(0 + ri) * nk + kk] = act ? x[q * nrow + 2 * (nr - 1)] : 0.0;
     // N_1 == 0 in the "cf" frame (src/vilma_response.f90:779)
-    A.drift[(size_t)(2 + ri) * nk + k] = (act && A.deg1_cm) ? xsh[q * ns + us + 2] : 0.0;
-    A.drift[(size_t)(4 + ri) * nk + k] = act ? xsh[q * ns + us + 1] : 0.0;
+    A.drift[(2 + ri) * nk + kk] = (act && A.deg1_cm) ? x[q * nrow + 2 * nr] : 0.0;
+    A.drift[(4 + ri) * nk + kk] = act ? x[q * nrow + 2 * (nr - 1) + 1] : 0.0;
   }
 }
 
@@ -216,9 +426,11 @@ void launch_drift(vg_handle* h) {
   A.ab = h->d_ab.p;
   A.dr = h->d_dr.p;
   A.dc = h->d_dc.p;
+  A.rdiag = h->d_rdiag.p;
   A.ipiv = h->d_ipiv.p;
   A.kdeg = h->d_kdeg.p;
-  A.xs = h->d_xs.p;
+  A.bh = h->d_bh.p;
+  A.ys = h->d_xs.p;
   A.dUn = h->d_dUn.p;
   A.dVn = h->d_dVn.p;
   A.drift = h->d_drift.p;
@@ -226,24 +438,29 @@ void launch_drift(vg_handle* h) {
   A.nr = h->nr;
   A.nd = h->ndof;
   A.nk = h->nk;
-  A.lmax = h->p.lmax;
-  A.ab1 = h->d_ab1.p;
   A.dr1 = h->d_dr1.p;
-  A.dc1 = h->d_dc1.p;
   A.null1 = h->d_null1.p;
-  A.ipiv1 = h->d_ipiv1.p;
-  A.kl1 = h->kl1;
-  A.kv1 = h->kv1;
+  A.G1 = h->d_G1.p;
   A.deg1_cm = h->p.deg1_cm;
-  k_drift<<<(h->nk + 127) / 128, 128, 0, h->stream>>>(A); ++h->n_launch;
+  A.K = h->d_Krhs.p;
+  A.tasks = h->d_tasks.p;
+  A.ntask = h->ntask;
+  dim3 rgrid((h->nk + 31) / 32, (h->nr + 3) / 4, 2);
+  k_drift_rhs<<<rgrid, dim3(32, 4), 0, h->stream>>>(A);
+  ++h->n_launch;
   VG_CUDA(cudaGetLastError());
-  size_t shm = 4 * (size_t)(h->ndof + 1) * sizeof(double);
-  static bool attr_set = false;
-  if (!attr_set && shm > 48 * 1024) {
-    VG_CUDA(cudaFuncSetAttribute(k_drift_deg1, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
-    attr_set = true;
+  const size_t sw_smem = (size_t)SW_WARPS * SW_WARP * sizeof(double);
+  static bool sw_attr = false;
+  if (!sw_attr) {
+    VG_CUDA(cudaFuncSetAttribute(k_drift_solve, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sw_smem));
+    sw_attr = true;
   }
-  k_drift_deg1<<<1, 256, shm, h->stream>>>(A); ++h->n_launch;
+  k_drift_solve<<<(h->ntask + SW_WARPS - 1) / SW_WARPS, 32 * SW_WARPS, sw_smem, h->stream>>>(A);
+  ++h->n_launch;
+  VG_CUDA(cudaGetLastError());
+  size_t shm = (size_t)(4 * 2 * h->nr + 4 * (2 * h->nr + 1)) * sizeof(double);
+  k_drift_deg1<<<1, 256, shm, h->stream>>>(A);
+  ++h->n_launch;
   VG_CUDA(cudaGetLastError());
 }
 
@@ -273,109 +490,110 @@ __global__ void k_apply(int nlm, int nk, double g, const int* __restrict__ lm_l,
 void launch_apply(vg_handle* h, const double* d_sigma, double* d_u, double* d_n) {
   int nlm = h->grid.nlm;
   k_apply<<<(nlm + 255) / 256, 256, 0, h->stream>>>(nlm, h->nk, h->g, h->grid.d_lm_l.p, h->d_lm2k.p, h->d_gu.p,
-                                                    h->d_gn.p, h->d_drift.p, d_sigma, d_u, d_n); ++h->n_launch;
+                                                    h->d_gn.p, h->d_drift.p, d_sigma, d_u, d_n);
+  ++h->n_launch;
   VG_CUDA(cudaGetLastError());
 }
 
-// Forward-Euler memory advance of the spectrally advanced elements, one thread
-// per slot, out of place (cur -> nxt), with the per-slot norm of the new
-// state over ALL elements (the 3-D elements were written to nxt before).
-__global__ void __launch_bounds__(256) k_advance_1d(const double* __restrict__ mem, double* __restrict__ nxt, int ne, int nr, int nk,
-                             double dt, const double* __restrict__ sigma, const int* __restrict__ kdeg,
-                             const int* __restrict__ k2lm, const double* __restrict__ Jrv,
-                             const double* __restrict__ xUn, const double* __restrict__ xVn,
-                             const double* __restrict__ dUn, const double* __restrict__ dVn,
-                             const double* __restrict__ mu, const double* __restrict__ MkPerDt,
-                             const char* __restrict__ active, double* __restrict__ mnorm,
-                             unsigned long long* __restrict__ maxbits) {
-  int k = blockIdx.x * blockDim.x + threadIdx.x;
+// Forward-Euler memory advance (src/vilma_viscoelastic.f90:577-584) of the
+// spectrally advanced elements, out of place (cur -> nxt): one thread per
+// (slot, element, re/im). Each thread also folds |new memory| of its element
+// (or of the 3-D element the pseudo-spectral pass already wrote) into the
+// per-slot norm.
+__global__ void __launch_bounds__(256) k_advance_1d(const double* __restrict__ mem, double* __restrict__ nxt, int ne,
+                                                    int nr, int nk, double dt, const double* __restrict__ sigma,
+                                                    const int* __restrict__ kdeg, const int* __restrict__ k2lm,
+                                                    const double* __restrict__ Jrv, const double* __restrict__ xUn,
+                                                    const double* __restrict__ xVn, const double* __restrict__ dUn,
+                                                    const double* __restrict__ dVn, const double* __restrict__ mu,
+                                                    const double* __restrict__ MkPerDt,
+                                                    const char* __restrict__ active, double* __restrict__ mnorm) {
+  const int k = blockIdx.x * 32 + threadIdx.x, e = blockIdx.y * 8 + threadIdx.y, ri = blockIdx.z;
   double amax = 0.0;
-  if (k < nk) {
-    int l = kdeg[k], lm = k2lm[k];
-    double Jr = Jrv[l];
-    const double* xu = xUn + (size_t)l * nr;
-    const double* xv = xVn + (size_t)l * nr;
-    for (int ri = 0; ri < 2; ++ri) {
-      double s = sigma[2 * lm + ri];
-      double U0 = s * xu[0] + dUn[((size_t)ri * nr + 0) * nk + k];
-      double V0 = s * xv[0] + dVn[((size_t)ri * nr + 0) * nk + k];
-      for (int e = 0; e < ne; ++e) {
-        double U1 = s * xu[e + 1] + dUn[((size_t)ri * nr + e + 1) * nk + k];
-        double V1 = s * xv[e + 1] + dVn[((size_t)ri * nr + e + 1) * nk + k];
-        if (active[e]) {
-          double a[4], b[4], c[4];
-          strain_coeffs(U0, U1, V0, V1, Jr, a, b, c);
-          double Me = MkPerDt[e] * dt;
-          double om = 1.0 - Me, two_muM = 2.0 * mu[e] * Me;
+  if (k < nk && e < ne) {
+    if (active[e]) {
+      const int l = kdeg[k], lm = k2lm[k];
+      const double s = sigma[2 * lm + ri];
+      const double* xu = xUn + (size_t)l * nr;
+      const double* xv = xVn + (size_t)l * nr;
+      const double U0 = s * __ldg(&xu[e]) + dUn[((size_t)ri * nr + e) * nk + k];
+      const double V0 = s * __ldg(&xv[e]) + dVn[((size_t)ri * nr + e) * nk + k];
+      const double U1 = s * __ldg(&xu[e + 1]) + dUn[((size_t)ri * nr + e + 1) * nk + k];
+      const double V1 = s * __ldg(&xv[e + 1]) + dVn[((size_t)ri * nr + e + 1) * nk + k];
+      double a[4], b[4], c[4];
+      strain_coeffs(U0, U1, V0, V1, Jrv[l], a, b, c);
+      const double Me = MkPerDt[e] * dt;
+      const double om = 1.0 - Me, two_muM = 2.0 * mu[e] * Me;
 #pragma unroll
-          for (int m = 0; m < 4; ++m) {
-            size_t iA = mem_idx(0, ri, e, m, k, ne, nk), iB = mem_idx(1, ri, e, m, k, ne, nk),
-                   iC = mem_idx(2, ri, e, m, k, ne, nk);
-            double An = om * mem[iA] - two_muM * a[m];
-            double Bn = om * mem[iB] - two_muM * b[m];
-            double Cn = om * mem[iC] - two_muM * c[m];
-            nxt[iA] = An;
-            nxt[iB] = Bn;
-            nxt[iC] = Cn;
-            amax = nanmax(amax, nanmax(fabs(An), nanmax(fabs(Bn), fabs(Cn))));
-          }
-        } else {
-#pragma unroll
-          for (int m = 0; m < 4; ++m)
-#pragma unroll
-            for (int s3 = 0; s3 < 3; ++s3) amax = nanmax(amax, fabs(nxt[mem_idx(s3, ri, e, m, k, ne, nk)]));
-        }
-        U0 = U1;
-        V0 = V1;
+      for (int m = 0; m < 4; ++m) {
+        size_t iA = mem_idx(0, ri, e, m, k, ne, nk), iB = mem_idx(1, ri, e, m, k, ne, nk),
+               iC = mem_idx(2, ri, e, m, k, ne, nk);
+        double An = om * mem[iA] - two_muM * a[m];
+        double Bn = om * mem[iB] - two_muM * b[m];
+        double Cn = om * mem[iC] - two_muM * c[m];
+        nxt[iA] = An;
+        nxt[iB] = Bn;
+        nxt[iC] = Cn;
+        amax = nanmax(amax, nanmax(fabs(An), nanmax(fabs(Bn), fabs(Cn))));
       }
+    } else {
+#pragma unroll
+      for (int m = 0; m < 4; ++m)
+#pragma unroll
+        for (int s3 = 0; s3 < 3; ++s3) amax = nanmax(amax, fabs(nxt[mem_idx(s3, ri, e, m, k, ne, nk)]));
     }
-    mnorm[k] = amax;
   }
-  // block max, then one atomic per block
-  __shared__ double red[256];
-  red[threadIdx.x] = amax;
+  __shared__ double red[8][33];
+  red[threadIdx.y][threadIdx.x] = amax;
   __syncthreads();
-  for (int o = blockDim.x / 2; o > 0; o >>= 1) {
-    if (threadIdx.x < o) red[threadIdx.x] = nanmax(red[threadIdx.x], red[threadIdx.x + o]);
-    __syncthreads();
+  if (threadIdx.y == 0 && k < nk) {
+    double v = red[0][threadIdx.x];
+#pragma unroll
+    for (int t = 1; t < 8; ++t) v = nanmax(v, red[t][threadIdx.x]);
+    atomic_max_bits(reinterpret_cast<unsigned long long*>(mnorm) + k, v);
   }
-  if (threadIdx.x == 0) atomic_max_bits(maxbits, red[0]);
+}
+
+// global max of the per-slot norms of one buffer
+__global__ void k_norm_max(const double* __restrict__ mnorm, int nk, unsigned long long* __restrict__ maxbits) {
+  __shared__ double red[1024];
+  double v = 0.0;
+  for (int k = threadIdx.x; k < nk; k += blockDim.x) v = nanmax(v, mnorm[k]);
+  v = block_max(v, red);
+  if (threadIdx.x == 0) *maxbits = (unsigned long long)__double_as_longlong(v);
 }
 
 void launch_advance_1d(vg_handle* h, const double* d_sigma, double dt) {
   PhaseScope ps(h, VG_PH_ADVANCE_1D);
   int nxt = 1 - h->cur;
-  VG_CUDA(cudaMemsetAsync(h->d_maxbits.p + nxt, 0, sizeof(unsigned long long), h->stream));
-  k_advance_1d<<<(h->nk + 255) / 256, 256, 0, h->stream>>>(
-      h->d_mem[h->cur].p, h->d_mem[nxt].p, h->ne, h->nr, h->nk, dt, d_sigma, h->d_kdeg.p, h->d_k2lm.p, h->d_Jr.p,
-      h->d_xUn.p, h->d_xVn.p, h->d_dUn.p, h->d_dVn.p, h->d_mu.p, h->d_MkPerDt.p, h->d_active1d.p,
-      h->d_mnorm.p + (size_t)nxt * h->nk, h->d_maxbits.p + nxt); ++h->n_launch;
+  double* mn = h->d_mnorm.p + (size_t)nxt * h->nk;
+  VG_CUDA(cudaMemsetAsync(mn, 0, h->nk * sizeof(double), h->stream));
+  dim3 grid((h->nk + 31) / 32, (h->ne + 7) / 8, 2);
+  k_advance_1d<<<grid, dim3(32, 8), 0, h->stream>>>(h->d_mem[h->cur].p, h->d_mem[nxt].p, h->ne, h->nr, h->nk, dt,
+                                                    d_sigma, h->d_kdeg.p, h->d_k2lm.p, h->d_Jr.p, h->d_xUn.p,
+                                                    h->d_xVn.p, h->d_dUn.p, h->d_dVn.p, h->d_mu.p, h->d_MkPerDt.p,
+                                                    h->d_active1d.p, mn);
+  ++h->n_launch;
+  VG_CUDA(cudaGetLastError());
+  k_norm_max<<<1, 1024, 0, h->stream>>>(mn, h->nk, h->d_maxbits.p + nxt);
+  ++h->n_launch;
   VG_CUDA(cudaGetLastError());
 }
 
 // per-slot norm and global max of one buffer (after vg_set_state / reset)
-__global__ void k_mem_norm(const double* __restrict__ mem, int ne, int nk, double* __restrict__ mnorm,
-                           unsigned long long* __restrict__ maxbits) {
+__global__ void k_mem_norm(const double* __restrict__ mem, int ne, int nk, double* __restrict__ mnorm) {
   int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= nk) return;
   double amax = 0.0;
-  if (k < nk) {
-    for (int q = 0; q < 6 * ne * 4; ++q) amax = nanmax(amax, fabs(mem[(size_t)q * nk + k]));
-    mnorm[k] = amax;
-  }
-  __shared__ double red[256];
-  red[threadIdx.x] = amax;
-  __syncthreads();
-  for (int o = blockDim.x / 2; o > 0; o >>= 1) {
-    if (threadIdx.x < o) red[threadIdx.x] = nanmax(red[threadIdx.x], red[threadIdx.x + o]);
-    __syncthreads();
-  }
-  if (threadIdx.x == 0) atomic_max_bits(maxbits, red[0]);
+  for (int q = 0; q < 6 * ne * 4; ++q) amax = nanmax(amax, fabs(mem[(size_t)q * nk + k]));
+  mnorm[k] = amax;
 }
 
 void compute_mem_norm(vg_handle* h, int buf) {
-  VG_CUDA(cudaMemsetAsync(h->d_maxbits.p + buf, 0, sizeof(unsigned long long), h->stream));
-  k_mem_norm<<<(h->nk + 255) / 256, 256, 0, h->stream>>>(h->d_mem[buf].p, h->ne, h->nk,
-                                                         h->d_mnorm.p + (size_t)buf * h->nk, h->d_maxbits.p + buf); ++h->n_launch;
+  double* mn = h->d_mnorm.p + (size_t)buf * h->nk;
+  k_mem_norm<<<(h->nk + 255) / 256, 256, 0, h->stream>>>(h->d_mem[buf].p, h->ne, h->nk, mn);
+  VG_CUDA(cudaGetLastError());
+  k_norm_max<<<1, 1024, 0, h->stream>>>(mn, h->nk, h->d_maxbits.p + buf);
   VG_CUDA(cudaGetLastError());
 }
 

@@ -238,7 +238,7 @@ struct ElemData {
 // arithmetic order matches the reference's serial assembly.
 __device__ void band_factor_dev(double* ab, int ldab, int n, int kl, int ku, int* ipiv, int* ok) {
   const int kv = kl + ku;
-#define AB(row1, col1) ab[(size_t)((row1)-1) * n + ((col1)-1)]
+#define AB(row1, col1) ab[(size_t)((col1)-1) * ldab + ((row1)-1)]
   int ju = 1;
   *ok = 1;
   for (int j = 1; j <= n; ++j) {
@@ -279,7 +279,7 @@ __device__ void band_factor_dev(double* ab, int ldab, int n, int kl, int ku, int
 
 __global__ void k_build_band(ElemData ed, int lmax, double* __restrict__ raw, double* __restrict__ ab,
                              double* __restrict__ drv, double* __restrict__ dcv, int* __restrict__ ipiv,
-                             int* __restrict__ status) {
+                             double* __restrict__ rdg, int* __restrict__ status) {
   int l = blockIdx.x * blockDim.x + threadIdx.x + 2;
   if (l > lmax) return;
   const int n = ed.nd, KL = 6, NB = 13;
@@ -312,17 +312,27 @@ __global__ void k_build_band(ElemData ed, int lmax, double* __restrict__ raw, do
     dr[i] = m > 0.0 ? 1.0 / sqrt(m) : 1.0;
   }
   // dgbtf2 storage: ldab = 2 kl + ku + 1 = 19, A(i,j) at row kv + i - j (0-based), kv = 12
-  const int ldab = 19, kv = 12;
+  const int ldab = VG_LDAB, kv = 12;
   double* A = ab + (size_t)(l - 2) * ldab * n;
   for (size_t t = 0; t < (size_t)ldab * n; ++t) A[t] = 0.0;
   for (int k = 0; k < n; ++k)
     for (int i = max(0, k - KL); i <= min(n - 1, k + KL); ++i) {
       double v = R[(size_t)(KL + i - k) * n + k];
-      if (v != 0.0) A[(size_t)(kv + i - k) * n + k] = dr[i] * v * dc[k];
+      if (v != 0.0) A[(size_t)k * ldab + (kv + i - k)] = dr[i] * v * dc[k];
     }
   int ok;
   band_factor_dev(A, ldab, n, KL, KL, ipiv + (size_t)(l - 2) * n, &ok);
-  if (!ok) atomicExch(status, l);
+  if (!ok) {
+    atomicExch(status, l);
+    return;
+  }
+  // Two extra rows per column for the drift sweeps, so one column is one
+  // contiguous record: row 19 = reciprocal pivot, row 20 = pivot offset jp.
+  for (int j = 0; j < n; ++j) {
+    A[(size_t)j * ldab + 19] = 1.0 / A[(size_t)j * ldab + kv];
+    A[(size_t)j * ldab + 20] = (double)(ipiv[(size_t)(l - 2) * n + j] - j);
+    rdg[(size_t)(l - 2) * n + j] = A[(size_t)j * ldab + 19];
+  }
 }
 
 // Degree 1: band part plus the KKT border w (E_uniq weight, src/vilma_radial_fe.f90:425-443,
@@ -385,12 +395,12 @@ __global__ void __launch_bounds__(512) k_build_deg1(ElemData ed, double* __restr
   for (size_t t = threadIdx.x; t < (size_t)nd * nd; t += blockDim.x) {
     int i = (int)(t % nd), k = (int)(t / nd);
     double v = A[t];
-    if (v != 0.0) ab[(size_t)(kv + i - k) * ns + k] = dr[i] * v * dc[k];
+    if (v != 0.0) ab[(size_t)k * ldab + (kv + i - k)] = dr[i] * v * dc[k];
   }
   for (int i = threadIdx.x; i < nd; i += blockDim.x) {
     if (w[i] != 0.0) {
-      ab[(size_t)(kv + i - nd) * ns + nd] = dr[i] * w[i] * s_dcb;   // border column
-      ab[(size_t)(kv + nd - i) * ns + i] = s_drb * w[i] * dc[i];    // border row
+      ab[(size_t)nd * ldab + (kv + i - nd)] = dr[i] * w[i] * s_dcb;   // border column
+      ab[(size_t)i * ldab + (kv + nd - i)] = s_drb * w[i] * dc[i];    // border row
     }
   }
   __syncthreads();
@@ -403,7 +413,7 @@ __global__ void __launch_bounds__(512) k_build_deg1(ElemData ed, double* __restr
     s_fail = 0;
   }
   __syncthreads();
-#define AB(row1, col1) ab[(size_t)((row1)-1) * ns + ((col1)-1)]
+#define AB(row1, col1) ab[(size_t)((col1)-1) * ldab + ((row1)-1)]
   for (int j = 1; j <= ns; ++j) {
     if (j + kv <= ns)
       for (int i = 1 + threadIdx.x; i <= kl; i += blockDim.x) AB(i, j + kv) = 0.0;
@@ -467,9 +477,9 @@ __global__ void __launch_bounds__(512) k_build_deg1(ElemData ed, double* __restr
 }
 
 // Solve with one factored band system (dgbtrs order) for a column x with stride.
-__device__ __forceinline__ void band_solve_strided(const double* __restrict__ ab, int n, int kl, int kv,
+__device__ __forceinline__ void band_solve_strided(const double* __restrict__ ab, int ldab, int n, int kl, int kv,
                                                    const int* __restrict__ ipiv, double* x, size_t st) {
-#define AB(row1, col1) ab[(size_t)((row1)-1) * n + ((col1)-1)]
+#define AB(row1, col1) ab[(size_t)((col1)-1) * ldab + ((row1)-1)]
   for (int j = 1; j <= n - 1; ++j) {
     int lm = min(kl, n - j);
     int l = ipiv[j - 1] + 1;
@@ -504,7 +514,7 @@ __global__ void k_unit_load(int lmax, int nr, int n, double r_earth, double g_su
   for (int i = 0; i < n; ++i) x[i] = 0.0;
   x[4 * (nr - 1)] = dr[4 * (nr - 1)] * (-r_earth * r_earth * 1.0 * g_surf);
   x[4 * (nr - 1) + 2] = dr[4 * (nr - 1) + 2] * (-r_earth * r_earth * 1.0);
-  band_solve_strided(ab + (size_t)(l - 2) * 19 * n, n, 6, 12, ipiv + (size_t)(l - 2) * n, x, 1);
+  band_solve_strided(ab + (size_t)(l - 2) * VG_LDAB * n, VG_LDAB, n, 6, 12, ipiv + (size_t)(l - 2) * n, x, 1);
   for (int i = 0; i < n; ++i) x[i] = dc[i] * x[i];
   gu[l] = x[4 * (nr - 1)];
   gn[l] = -x[4 * (nr - 1) + 2] / g_surf;
@@ -517,7 +527,7 @@ __global__ void k_unit_load(int lmax, int nr, int n, double r_earth, double g_su
 
 // degree-1 unit-load response (with the CM-frame projection) and null mode
 __global__ void __launch_bounds__(512) k_unit_load_deg1(int nr, int nd, double r_earth, double g_surf, int deg1_cm,
-                                 const double* __restrict__ ab, int kl, int kv, const int* __restrict__ ipiv,
+                                 const double* __restrict__ ab, int ldab, int kl, int kv, const int* __restrict__ ipiv,
                                  const double* __restrict__ dr, const double* __restrict__ dc,
                                  double* __restrict__ nullmode, double* __restrict__ gu, double* __restrict__ gn,
                                  double* __restrict__ gv, double* __restrict__ xUn, double* __restrict__ xVn) {
@@ -531,7 +541,7 @@ __global__ void __launch_bounds__(512) k_unit_load_deg1(int nr, int nd, double r
     xsh[ns + nd] = 1.0;  // null mode: zero physical RHS, border value 1
   }
   __syncthreads();
-  deg1_solve_cta(ab, ns, kl, kv, ipiv, xsh, 2);
+  deg1_solve_cta(ab, ldab, ns, kl, kv, ipiv, xsh, 2);
   for (int i = threadIdx.x; i < nd; i += blockDim.x) {
     xsh[i] = dc[i] * xsh[i];
     xsh[ns + i] = dc[i] * xsh[ns + i];
@@ -557,6 +567,80 @@ __global__ void __launch_bounds__(512) k_unit_load_deg1(int nr, int nd, double r
     xUn[(size_t)nr + node] = xsh[4 * node];
     xVn[(size_t)nr + node] = xsh[4 * node + 1];
   }
+}
+
+// Degree-1 response block G1 = Dc Ahat^-1 restricted to the rows the drift
+// needs (U and V of every node, then F at the surface: r = 2 node + {0,1},
+// r = 2 nr) and to the columns the dissipative forcing can reach (U and V of
+// every node: c = 2 node + {0,1}), in the equilibrated-RHS space. One thread
+// per column solves the bordered system (dgbtrs order) for a unit RHS.
+__global__ void k_deg1_green(int nr, int nd, const double* __restrict__ ab, int ldab, int kl, int kv,
+                             const int* __restrict__ ipiv, const double* __restrict__ dc,
+                             double* __restrict__ scratch, double* __restrict__ G1) {
+  int c = blockIdx.x * blockDim.x + threadIdx.x;
+  const int ncol = 2 * nr, ns = nd + 1;
+  if (c >= ncol) return;
+  double* x = scratch + (size_t)c * ns;
+  for (int i = 0; i < ns; ++i) x[i] = 0.0;
+  x[4 * (c / 2) + (c % 2)] = 1.0;
+#define AB(row1, col1) ab[(size_t)((col1)-1) * ldab + ((row1)-1)]
+  for (int j = 1; j <= ns - 1; ++j) {
+    int lm = min(kl, ns - j);
+    int l = ipiv[j - 1] + 1;
+    if (l != j) {
+      double t = x[l - 1];
+      x[l - 1] = x[j - 1];
+      x[j - 1] = t;
+    }
+    double t = x[j - 1];
+    if (t != 0.0)
+      for (int i = 1; i <= lm; ++i) x[j + i - 1] -= AB(kv + 1 + i, j) * t;
+  }
+  for (int j = ns; j >= 1; --j) {
+    double xj = x[j - 1] / AB(kv + 1, j);
+    x[j - 1] = xj;
+    int lm = min(kv, j - 1);
+    if (xj != 0.0)
+      for (int i = 1; i <= lm; ++i) x[j - i - 1] -= AB(kv + 1 - i, j) * xj;
+  }
+#undef AB
+  for (int node = 0; node < nr; ++node) {
+    G1[(size_t)(2 * node) * ncol + c] = dc[4 * node] * x[4 * node];
+    G1[(size_t)(2 * node + 1) * ncol + c] = dc[4 * node + 1] * x[4 * node + 1];
+  }
+  int fs = 4 * (nr - 1) + 2;
+  G1[(size_t)(2 * nr) * ncol + c] = dc[fs] * x[fs];
+}
+
+// Dissipative forcing as a linear map of one element's memory: the 2-point
+// Gauss quadrature of dissipative_rhs (src/vilma_viscoelastic.f90:441-480)
+// folded into K[t][s][m] with floc_t = sum_{s,m} K[t][s][m] mem_s[m] for the
+// test dofs t = (U_e, U_e+1, V_e, V_e+1), shape coefficients s = (A, B, C) and
+// channels m. One thread per (degree, element).
+__global__ void k_rhs_coeffs(int lmax, int ne, const double* __restrict__ r, const double* __restrict__ sa,
+                             const double* __restrict__ sb, const double* __restrict__ sc,
+                             const double* __restrict__ nrmc, double* __restrict__ K) {
+  int e = blockIdx.x * blockDim.x + threadIdx.x, l = blockIdx.y + 1;
+  if (e >= ne || l > lmax) return;
+  const double xg = 0.5773502691896257;
+  double rk = r[e], rk1 = r[e + 1], h = rk1 - rk;
+  double acc[4][3][4] = {};
+  for (int ig = 0; ig < 2; ++ig) {
+    double ra = 0.5 * (h * (ig ? xg : -xg) + rk + rk1);
+    double psik = (rk1 - ra) / h, psik1 = (ra - rk) / h;
+    double w = ra * ra * h * 0.5;
+    double basis[3] = {1.0 / h, psik / ra, psik1 / ra};
+    for (int t = 0; t < 4; ++t)
+      for (int m = 0; m < 4; ++m) {
+        double deps = sa[l * 16 + t * 4 + m] / h + sb[l * 16 + t * 4 + m] * psik / ra + sc[l * 16 + t * 4 + m] * psik1 / ra;
+        double c = w * nrmc[l * 4 + m] * deps;
+        for (int s3 = 0; s3 < 3; ++s3) acc[t][s3][m] -= c * basis[s3];
+      }
+  }
+  double* out = K + ((size_t)l * ne + e) * 48;
+  for (int t = 0; t < 4; ++t)
+    for (int s3 = 0; s3 < 3; ++s3)
+      for (int m = 0; m < 4; ++m) out[(t * 3 + s3) * 4 + m] = acc[t][s3][m];
 }
 
 // ----------------------------------------------------------------- setup
@@ -649,17 +733,18 @@ void setup_handle(vg_handle* h) {
   // band operators for l >= 2
   h->kl = h->ku = 6;
   h->kv = 12;
-  h->ldab = 19;
+  h->ldab = VG_LDAB;
   DArr<double> raw;
   DArr<int> status;
   raw.alloc((size_t)(lmax - 1) * 13 * nd);
   status.alloc(1);
-  h->d_ab.alloc((size_t)(lmax - 1) * 19 * nd);
+  h->d_ab.alloc((size_t)(lmax - 1) * VG_LDAB * nd);
   h->d_dr.alloc((size_t)(lmax - 1) * nd);
   h->d_dc.alloc((size_t)(lmax - 1) * nd);
   h->d_ipiv.alloc((size_t)(lmax - 1) * nd);
+  h->d_rdiag.alloc((size_t)(lmax - 1) * nd);
   k_build_band<<<(lmax - 1 + 31) / 32, 32, 0, s>>>(ed, lmax, raw.p, h->d_ab.p, h->d_dr.p, h->d_dc.p, h->d_ipiv.p,
-                                                    status.p);
+                                                    h->d_rdiag.p, status.p);
   VG_CUDA(cudaGetLastError());
   // degree 1 (bordered, dense)
   h->ns1 = nd + 1;
@@ -718,6 +803,12 @@ void setup_handle(vg_handle* h) {
   h->d_sa.upload(sa, s);
   h->d_sb.upload(sb, s);
   h->d_sc.upload(sc, s);
+  h->d_Krhs.alloc((size_t)(lmax + 1) * ne * 48);
+  {
+    dim3 g((ne + 63) / 64, lmax);
+    k_rhs_coeffs<<<g, 64, 0, s>>>(lmax, ne, h->d_r.p, h->d_sa.p, h->d_sb.p, h->d_sc.p, h->d_nrmc.p, h->d_Krhs.p);
+    VG_CUDA(cudaGetLastError());
+  }
   // unit-load response
   h->d_gu.alloc(lmax + 1);
   h->d_gn.alloc(lmax + 1);
@@ -733,10 +824,19 @@ void setup_handle(vg_handle* h) {
   size_t shm = 2 * (size_t)h->ns1 * sizeof(double);
   if (shm > 48 * 1024)
     VG_CUDA(cudaFuncSetAttribute(k_unit_load_deg1, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm));
-  k_unit_load_deg1<<<1, 512, shm, s>>>(nr, nd, p.r_earth, h->g, p.deg1_cm, h->d_ab1.p, h->kl1, h->kv1,
+  k_unit_load_deg1<<<1, 512, shm, s>>>(nr, nd, p.r_earth, h->g, p.deg1_cm, h->d_ab1.p, h->ldab1, h->kl1, h->kv1,
                                        h->d_ipiv1.p, h->d_dr1.p, h->d_dc1.p, h->d_null1.p, h->d_gu.p, h->d_gn.p,
                                        h->d_gv.p, h->d_xUn.p, h->d_xVn.p);
   VG_CUDA(cudaGetLastError());
+  {  // degree-1 response block for the drift
+    DArr<double> scratch;
+    scratch.alloc((size_t)2 * nr * h->ns1);
+    h->d_G1.alloc((size_t)(2 * nr + 1) * 2 * nr);
+    k_deg1_green<<<(2 * nr + 63) / 64, 64, 0, s>>>(nr, nd, h->d_ab1.p, h->ldab1, h->kl1, h->kv1, h->d_ipiv1.p,
+                                                  h->d_dc1.p, scratch.p, h->d_G1.p);
+    VG_CUDA(cudaGetLastError());
+    VG_CUDA(cudaStreamSynchronize(s));
+  }
   // degree 0: monopole geoid (src/vilma_response.f90:603-605)
   double gn0 = 4.0 * PI * GRAV_G * h->a / h->g, zero = 0.0;
   VG_CUDA(cudaMemcpyAsync(h->d_gn.p, &gn0, sizeof(double), cudaMemcpyHostToDevice, s));
@@ -765,6 +865,13 @@ void setup_handle(vg_handle* h) {
   h->d_kdeg.upload(h->kdeg_h, s);
   h->d_k2lm.upload(h->k2lm_h, s);
   h->d_lm2k.upload(lm2k, s);
+  {  // drift sweep tasks: one warp = up to 16 slots of ONE degree (x re/im = 32 lanes)
+    std::vector<int4> tasks;
+    for (int l = 2; l <= lmax; ++l)
+      for (int s0 = 0; s0 < l + 1; s0 += 16) tasks.push_back(make_int4(l, h->kbeg_h[l] + s0, std::min(16, l + 1 - s0), 0));
+    h->ntask = (int)tasks.size();
+    h->d_tasks.upload(tasks, s);
+  }
   // state and work buffers
   const size_t nmem = (size_t)6 * ne * 4 * nk;
   h->d_mem[0].alloc(nmem);
@@ -776,6 +883,7 @@ void setup_handle(vg_handle* h) {
   h->d_mnorm.alloc((size_t)2 * nk);
   h->d_maxbits.alloc(2);
   h->d_xs.alloc((size_t)2 * nd * nk);
+  h->d_bh.alloc((size_t)2 * 2 * nr * nk);
   h->d_sc_.alloc(1);
   VG_CUDA(cudaMallocHost(&h->h_sc, sizeof(SleScalars)));
   std::memset(h->h_sc, 0, sizeof(SleScalars));
