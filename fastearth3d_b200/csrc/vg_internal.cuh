@@ -160,7 +160,9 @@ struct vg_handle {
   vg::DArr<double> d_MkPerDt3;  // (ne3d, nlat, nphi)
   vg::DArr<int> d_e3d;
   vg::DArr<double> d_G6, d_H6, d_n6;  // spin-2 kernels (nlm, nlat), norms (lmax+1)
-  vg::DArr<double> d_X, d_Y, d_dy;    // 3-D work buffers
+  vg::DArr<double> d_wP, d_wD, d_wG, d_wH;  // quadrature-weighted analysis kernels (nlm, nlat)
+  vg::DArr<int> d_kbeg;               // first slot of each degree (lmax + 2)
+  vg::DArr<double> d_X, d_Y, d_dy;    // 3-D work buffers: synthesis input, Fourier products, increments
   // sea-level equation fields (ng each unless stated)
   vg::DArr<double> d_z_bed_eq, d_h_ice_eq, d_h_ice, d_ice1, d_ice_now, d_dice_now, d_rsl, d_rsl_n,
       d_C, d_C0, d_C_next, d_dig, d_wcorr, d_Sraw, d_zbed, d_tmp;

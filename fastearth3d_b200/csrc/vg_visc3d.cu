@@ -1,5 +1,24 @@
 // Laterally varying viscosity: the pseudo-spectral Maxwell memory advance of
-// the genuinely 3-D elements (src/vilma_response.f90:994-1053, 1171-1319).
+// the genuinely 3-D elements (response_enable_lateral_visc and
+// advance_memory_3d, src/vilma_response.f90:994-1053, 1171-1319; the dyadic
+// tensor transforms of src/vilma_tensor_sh.f90:168-387).
+//
+// All 3-D elements and their three radial shape coefficients are batched as
+// nf = 3 * ne3d tensor fields f = (element, shape). Per sub-step:
+//   gather    X[k][ch][f][ri] = memory + 2 mu strain (the combined synthesis
+//             input of tau + 2 mu eps), channel 3 pre-scaled by -l(l+1)
+//   synth     per order m, six products over l: P.X0, D.X1, P.X1, P.X2, G.X3,
+//             H.X3 -> S[m][j][p][f][ri] (Fourier coefficients at latitude j)
+//   lon       per latitude: dyadic Fourier coefficients (rr, rt, rp, tt, pp, tp),
+//             inverse DFT to the grid, times -M(theta, phi), forward DFT, the
+//             six analysis inputs (RR, RT, m/sin RP, TT+PP, TT-PP, TP)
+//   analysis  per order m, the quadrature adjoints: wP, wD, wP, wP, wG, wH
+//   scatter   channel normalisations (1, 1/J, -1/(2J), 1/n6) and the increment
+//             c += Delta into the next state buffer
+// G and H are the spin-2 kernels of Z6 written through P and dP/dtheta:
+//   G = -2 cot dP - l(l+1) P + 2 m^2/sin^2 P,   H = (m/sin)(dP - cot P)
+// so that Sg = sum c G e^{im phi} and Sh = i sum c H e^{im phi}
+// (the grid identities of src/vilma_tensor_sh.f90:244-266).
 #include <algorithm>
 #include <cmath>
 
@@ -8,17 +27,468 @@
 
 namespace vg {
 
+// ------------------------------------------------------------------ tables
+
+// spin-2 synthesis kernels and the quadrature-weighted analysis kernels, [lm][j]
+__global__ void k_visc3d_tables(int nlm, int nlat, const int* __restrict__ lm_l, const int* __restrict__ lm_m,
+                                const double* __restrict__ plm, const double* __restrict__ dplm,
+                                const double* __restrict__ wts, const double* __restrict__ cott,
+                                const double* __restrict__ invsin, double* __restrict__ G, double* __restrict__ H,
+                                double* __restrict__ wP, double* __restrict__ wD, double* __restrict__ wG,
+                                double* __restrict__ wH) {
+  int j = blockIdx.x * blockDim.x + threadIdx.x, lm = blockIdx.y;
+  if (j >= nlat || lm >= nlm) return;
+  double l = lm_l[lm], m = lm_m[lm];
+  size_t o = (size_t)lm * nlat + j;
+  double P = plm[o], D = dplm[o], ct = cott[j], is = invsin[j], w = wts[j];
+  double g = -2.0 * ct * D - l * (l + 1.0) * P + 2.0 * m * m * is * is * P;
+  double hh = m * is * (D - ct * P);
+  G[o] = g;
+  H[o] = hh;
+  wP[o] = w * P;
+  wD[o] = w * D;
+  wG[o] = w * g;
+  wH[o] = w * hh;
+}
+
+// spin-2 norm per degree: n6(l) = 4 pi sum_j w_j (G^2 + 4 H^2) at the sectoral
+// order m = l — the quadrature value of the synthesis-then-adjoint calibration
+// of src/vilma_tensor_sh.f90:99-133 (which also uses m = l).
+__global__ void k_visc3d_n6(int lmax, int nlat, const int* __restrict__ mbeg, const double* __restrict__ G,
+                            const double* __restrict__ H, const double* __restrict__ wts, double* __restrict__ n6) {
+  int l = blockIdx.x * blockDim.x + threadIdx.x;
+  if (l > lmax) return;
+  if (l < 2) {
+    n6[l] = 0.0;
+    return;
+  }
+  int lm = mbeg[l];  // (l, m = l)
+  double s = 0.0;
+  for (int j = 0; j < nlat; ++j) {
+    double g = G[(size_t)lm * nlat + j], hh = H[(size_t)lm * nlat + j];
+    s += wts[j] * (g * g + 4.0 * hh * hh);
+  }
+  n6[l] = 4.0 * PI * s;
+}
+
+// ------------------------------------------------------------------ gather
+
+struct V3Args {
+  const double* mem;
+  double* nxt;
+  const double* sigma;
+  const int *kdeg, *k2lm, *e3d;
+  const double *Jr, *xUn, *xVn, *dUn, *dVn, *mu;
+  int ne, nr, nk, ne3d, nf, ncf;  // ncf = 2 nf
+  double* X;                      // (nk + 1) rows x (4 * ncf)
+};
+
+// one thread per (slot k, 3-D element): strain of both histories, 24 values
+__global__ void __launch_bounds__(256) k_v3_gather(V3Args A) {
+  const int k = blockIdx.x * 32 + threadIdx.x, ei = blockIdx.y * 8 + threadIdx.y;
+  if (k >= A.nk || ei >= A.ne3d) return;
+  const int e = A.e3d[ei], l = A.kdeg[k], lm = A.k2lm[k];
+  const double Jr = A.Jr[l], twoMu = 2.0 * A.mu[e];
+  const double* xu = A.xUn + (size_t)l * A.nr;
+  const double* xv = A.xVn + (size_t)l * A.nr;
+  double* row = A.X + (size_t)k * 4 * A.ncf;
+  for (int ri = 0; ri < 2; ++ri) {
+    const double s = A.sigma[2 * lm + ri];
+    const double U0 = s * xu[e] + A.dUn[((size_t)ri * A.nr + e) * A.nk + k];
+    const double U1 = s * xu[e + 1] + A.dUn[((size_t)ri * A.nr + e + 1) * A.nk + k];
+    const double V0 = s * xv[e] + A.dVn[((size_t)ri * A.nr + e) * A.nk + k];
+    const double V1 = s * xv[e + 1] + A.dVn[((size_t)ri * A.nr + e + 1) * A.nk + k];
+    double eps[3][4];
+    strain_coeffs(U0, U1, V0, V1, Jr, eps[0], eps[1], eps[2]);
+#pragma unroll
+    for (int s3 = 0; s3 < 3; ++s3)
+#pragma unroll
+      for (int lam = 0; lam < 4; ++lam) {
+        double v = A.mem[mem_idx(s3, ri, e, lam, k, A.ne, A.nk)] + twoMu * eps[s3][lam];
+        if (lam == 2) v = -Jr * v;  // trace channel enters the synthesis as -l(l+1) c
+        row[(size_t)lam * A.ncf + (3 * ei + s3) * 2 + ri] = v;
+      }
+  }
+}
+
+// ------------------------------------------------------------------ GEMMs
+
+// Per-order batched FP64 products (the Legendre stage of the tensor transforms).
+//   mode 0 (synthesis): C[j][n] = sum_{kk < K_m} T_p[mbeg + kk][j] * X[row(m + kk, m)][col_p + n]
+//                       -> S[((m * nlat + j) * 6 + p) * ncf + n]
+//   mode 1 (analysis):  C[i][n] = sum_{j} T_p[mbeg + i][j] * S[((m * nlat + j) * 6 + p) * ncf + n]
+//                       -> R[(row(m + i, m) * 6 + p) * ncf + n]
+// row(l, m) = kbeg[l] + m for l >= 1, the zero row nk for l = 0.
+struct GemmArgs {
+  int mode, lmax, nlat, nk, ncf;
+  const int *mbeg, *kbeg;
+  const double* T[6];  // per product: table [lm][j]
+  int chan[6];         // synthesis: input channel per product
+  const double* in;
+  double* out;
+};
+
+constexpr int GB_M = 64, GB_N = 64, GB_K = 8;
+
+__device__ __forceinline__ int slot_row(const int* kbeg, int l, int m, int nk) { return l >= 1 ? kbeg[l] + m : nk; }
+
+__global__ void __launch_bounds__(256) k_v3_gemm(GemmArgs A) {
+  __shared__ double As[GB_K][GB_M + 1];
+  __shared__ double Bs[GB_K][GB_N];
+  const int m = blockIdx.z / 6, p = blockIdx.z % 6;
+  const int Km = A.lmax - m + 1;
+  const int rows = (A.mode == 0) ? A.nlat : Km;
+  const int kdim = (A.mode == 0) ? Km : A.nlat;
+  const int r0 = blockIdx.y * GB_M, n0 = blockIdx.x * GB_N;
+  if (r0 >= rows) return;
+  const double* T = A.T[p];
+  const int mb = A.mbeg[m];
+  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;  // 16 x 16 threads, 4 x 4 outputs each
+  double acc[4][4];
+#pragma unroll
+  for (int a = 0; a < 4; ++a)
+#pragma unroll
+    for (int b = 0; b < 4; ++b) acc[a][b] = 0.0;
+  for (int k0 = 0; k0 < kdim; k0 += GB_K) {
+    // A tile (rows r0.., k k0..): synthesis T[mb + kk][j = r]; analysis T[mb + r][j = kk]
+    for (int t = threadIdx.x; t < GB_K * GB_M; t += 256) {
+      int kk = t / GB_M, r = t % GB_M;
+      int gr = r0 + r, gk = k0 + kk;
+      double v = 0.0;
+      if (gr < rows && gk < kdim)
+        v = (A.mode == 0) ? T[(size_t)(mb + gk) * A.nlat + gr] : T[(size_t)(mb + gr) * A.nlat + gk];
+      As[kk][r] = v;
+    }
+    for (int t = threadIdx.x; t < GB_K * GB_N; t += 256) {
+      int kk = t / GB_N, n = t % GB_N;
+      int gk = k0 + kk, gn = n0 + n;
+      double v = 0.0;
+      if (gk < kdim && gn < A.ncf) {
+        if (A.mode == 0) {
+          int row = slot_row(A.kbeg, m + gk, m, A.nk);
+          v = A.in[(size_t)row * 4 * A.ncf + (size_t)A.chan[p] * A.ncf + gn];
+        } else {
+          v = A.in[(((size_t)m * A.nlat + gk) * 6 + p) * A.ncf + gn];
+        }
+      }
+      Bs[kk][n] = v;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int kk = 0; kk < GB_K; ++kk) {
+      double a[4], b[4];
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        a[q] = As[kk][ty + 16 * q];
+        b[q] = Bs[kk][tx + 16 * q];
+      }
+#pragma unroll
+      for (int q = 0; q < 4; ++q)
+#pragma unroll
+        for (int u = 0; u < 4; ++u) acc[q][u] += a[q] * b[u];
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    int gr = r0 + ty + 16 * q;
+    if (gr >= rows) continue;
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      int gn = n0 + tx + 16 * u;
+      if (gn >= A.ncf) continue;
+      if (A.mode == 0)
+        A.out[(((size_t)m * A.nlat + gr) * 6 + p) * A.ncf + gn] = acc[q][u];
+      else
+        A.out[((size_t)slot_row(A.kbeg, m + gr, m, A.nk) * 6 + p) * A.ncf + gn] = acc[q][u];
+    }
+  }
+}
+
+// ------------------------------------------------------------------ longitude
+
+// One CTA per (latitude j, tile of FT fields). Dyadic Fourier coefficients from
+// the six synthesis products, inverse DFT (half-period split: phi + pi flips
+// odd m), times -M(theta_j, phi_i) of the field's element, forward DFT, and the
+// six analysis inputs, written in place over the synthesis products.
+constexpr int LON_FT = 4;
+
+__global__ void __launch_bounds__(256) k_v3_lon(double* __restrict__ S, int nlat, int nphi, int M, int nf,
+                                                double dt, const double* __restrict__ Mk3rate,
+                                                const double* __restrict__ cs, const double* __restrict__ sn,
+                                                const double* __restrict__ invsin) {
+  extern __shared__ double sm[];
+  const int j = blockIdx.x, f0 = blockIdx.y * LON_FT;
+  const int nft = min(LON_FT, nf - f0);
+  const int ncf = 2 * nf, half = nphi / 2;
+  double* C = sm;                               // [6 comp][FT][M][2]
+  double* Gr = sm + 6 * LON_FT * M * 2;          // [6 comp][FT][nphi]
+  const double is = invsin[j];
+  // 1. dyadic coefficients rr, rt, rp, tt, pp, tp
+  for (int t = threadIdx.x; t < LON_FT * M; t += blockDim.x) {
+    int fl = t / M, m = t % M;
+    double pr[6][2];
+    for (int p = 0; p < 6; ++p)
+      for (int ri = 0; ri < 2; ++ri)
+        pr[p][ri] = (fl < nft) ? S[(((size_t)m * nlat + j) * 6 + p) * ncf + (f0 + fl) * 2 + ri] : 0.0;
+    double ms = m * is;
+    double rr[2] = {pr[0][0], pr[0][1]};
+    double rt[2] = {pr[1][0], pr[1][1]};
+    double rp[2] = {-ms * pr[2][1], ms * pr[2][0]};  // i (m / sin) P.X1
+    double tr[2] = {pr[3][0], pr[3][1]};
+    double sg[2] = {pr[4][0], pr[4][1]};
+    double sh[2] = {-pr[5][1], pr[5][0]};  // i H.X3
+    double comp[6][2] = {{rr[0], rr[1]},
+                         {rt[0], rt[1]},
+                         {rp[0], rp[1]},
+                         {tr[0] + sg[0], tr[1] + sg[1]},
+                         {tr[0] - sg[0], tr[1] - sg[1]},
+                         {4.0 * sh[0], 4.0 * sh[1]}};
+    for (int c = 0; c < 6; ++c) {
+      C[((c * LON_FT + fl) * M + m) * 2] = comp[c][0];
+      C[((c * LON_FT + fl) * M + m) * 2 + 1] = comp[c][1];
+    }
+  }
+  __syncthreads();
+  // 2. inverse DFT (f_i = Re C0 + 2 Re sum_m C_m e^{i m phi_i}), times -M
+  for (int t = threadIdx.x; t < 6 * LON_FT * half; t += blockDim.x) {
+    int row = t / half, i = t % half, fl = row % LON_FT;
+    const double* c = C + (size_t)row * M * 2;
+    double ev = 0.0, od = 0.0;
+    int tw = i;
+    for (int m = 1; m < M; ++m) {
+      double v = c[2 * m] * __ldg(&cs[tw]) - c[2 * m + 1] * __ldg(&sn[tw]);
+      if (m & 1)
+        od += v;
+      else
+        ev += v;
+      tw += i;
+      if (tw >= nphi) tw -= nphi;
+    }
+    double a = c[0] + 2.0 * ev, b = 2.0 * od;
+    double m1 = 0.0, m2 = 0.0;
+    if (fl < nft) {
+      int e = (f0 + fl) / 3;
+      const double* Mr = Mk3rate + ((size_t)e * nlat + j) * nphi;
+      m1 = Mr[i] * dt;
+      m2 = Mr[i + half] * dt;
+    }
+    Gr[(size_t)row * nphi + i] = -m1 * (a + b);
+    Gr[(size_t)row * nphi + i + half] = -m2 * (a - b);
+  }
+  __syncthreads();
+  // 3. forward DFT (F_m = 2 pi / nphi sum_i f_i e^{-i m phi_i}) and analysis inputs
+  const double scl = 2.0 * PI / (double)nphi;
+  for (int t = threadIdx.x; t < LON_FT * M; t += blockDim.x) {
+    int fl = t / M, m = t % M;
+    double F[6][2];
+    for (int c = 0; c < 6; ++c) {
+      const double* g = Gr + (size_t)(c * LON_FT + fl) * nphi;
+      double re = 0.0, im = 0.0;
+      int tw = 0;
+      double sgn = (m & 1) ? -1.0 : 1.0;
+      for (int i = 0; i < half; ++i) {
+        double v = g[i] + sgn * g[i + half];
+        re += v * __ldg(&cs[tw]);
+        im -= v * __ldg(&sn[tw]);
+        tw += m;
+        if (tw >= nphi) tw -= nphi;
+      }
+      F[c][0] = re * scl;
+      F[c][1] = im * scl;
+    }
+    if (fl >= nft) continue;
+    double ms = m * is;
+    double out[6][2] = {{F[0][0], F[0][1]},
+                        {F[1][0], F[1][1]},
+                        {ms * F[2][0], ms * F[2][1]},
+                        {F[3][0] + F[4][0], F[3][1] + F[4][1]},
+                        {F[3][0] - F[4][0], F[3][1] - F[4][1]},
+                        {F[5][0], F[5][1]}};
+    for (int q = 0; q < 6; ++q)
+      for (int ri = 0; ri < 2; ++ri) S[(((size_t)m * nlat + j) * 6 + q) * ncf + (f0 + fl) * 2 + ri] = out[q][ri];
+  }
+}
+
+// ------------------------------------------------------------------ scatter
+
+// Channel normalisations and the increment form c += Delta
+// (src/vilma_response.f90:1281-1318): one thread per (slot, 3-D element).
+__global__ void __launch_bounds__(256) k_v3_scatter(V3Args A, const double* __restrict__ R,
+                                                    const double* __restrict__ n6) {
+  const int k = blockIdx.x * 32 + threadIdx.x, ei = blockIdx.y * 8 + threadIdx.y;
+  if (k >= A.nk || ei >= A.ne3d) return;
+  const int e = A.e3d[ei], l = A.kdeg[k];
+  const double J = A.Jr[l], nn = n6[l];
+  const double* row = R + (size_t)k * 6 * A.ncf;
+  for (int s3 = 0; s3 < 3; ++s3) {
+    const int f = 3 * ei + s3;
+    double q[6][2];
+    for (int p = 0; p < 6; ++p)
+      for (int ri = 0; ri < 2; ++ri) q[p][ri] = row[(size_t)p * A.ncf + 2 * f + ri];
+    double d[4][2];
+    d[0][0] = q[0][0];
+    d[0][1] = q[0][1];
+    d[1][0] = (q[1][0] + q[2][1]) / J;  // (wD.RT - i wP.(m/sin RP)) / J
+    d[1][1] = (q[1][1] - q[2][0]) / J;
+    d[2][0] = q[3][0] / (-2.0 * J);
+    d[2][1] = q[3][1] / (-2.0 * J);
+    d[3][0] = nn != 0.0 ? (q[4][0] + 2.0 * q[5][1]) / nn : 0.0;  // (wG.(TT-PP) - 2i wH.TP) / n6
+    d[3][1] = nn != 0.0 ? (q[4][1] - 2.0 * q[5][0]) / nn : 0.0;
+    for (int ri = 0; ri < 2; ++ri)
+      for (int lam = 0; lam < 4; ++lam) {
+        size_t idx = mem_idx(s3, ri, e, lam, k, A.ne, A.nk);
+        A.nxt[idx] = A.mem[idx] + d[lam][ri];
+      }
+  }
+}
+
+// ------------------------------------------------------------------ host
+
 void visc3d_enable(vg_handle* h, const double* pert) {
-  (void)h;
-  (void)pert;
-  throw Error("vg_enable_visc3d: lateral viscosity is not built yet");
+  const Grid& G = h->grid;
+  const int ne = h->ne, ng = G.ng;
+  cudaStream_t s = h->stream;
+  if (G.nphi % 2 != 0) throw Error("vg_enable_visc3d: the longitude pass needs an even nphi");
+  if (h->lat_visc) throw Error("vg_enable_visc3d: lateral viscosity is already enabled for this handle");
+  // Maxwell-CFL rate: the grid maximum of mu/eta_eff over every Maxwell element
+  // (src/vilma_response.f90:1783-1793, MkPerDt3 covers all elements)
+  double rate_max = 0.0;
+  for (int e = 0; e < ne; ++e) {
+    if (h->MkPerDt[e] == 0.0) continue;
+    const double* pe = pert + (size_t)e * ng;
+    for (int g = 0; g < ng; ++g) rate_max = std::max(rate_max, h->MkPerDt[e] * std::pow(10.0, -pe[g]));
+  }
+  // classification (src/vilma_response.f90:1024-1046), on the host: setup only
+  std::vector<double> rate3;
+  h->e3d_h.clear();
+  for (int e = 0; e < ne; ++e) {
+    h->active1d_h[e] = 1;
+    if (h->MkPerDt[e] == 0.0) continue;
+    const double* pe = pert + (size_t)e * ng;
+    double mx = -1e300, mn = 1e300;
+    for (int g = 0; g < ng; ++g) {
+      mx = std::max(mx, pe[g]);
+      mn = std::min(mn, pe[g]);
+    }
+    if (mx - mn > h->p.visc3d_tol) {
+      h->active1d_h[e] = 0;
+      h->e3d_h.push_back(e);
+      for (int g = 0; g < ng; ++g) rate3.push_back(h->MkPerDt[e] * std::pow(10.0, -pe[g]));
+    } else {
+      double sum = 0.0;
+      for (int g = 0; g < ng; ++g) sum += pe[g];
+      h->MkPerDt[e] = h->MkPerDt[e] * std::pow(10.0, -(sum / (double)ng));
+    }
+  }
+  h->ne3d = (int)h->e3d_h.size();
+  h->max_rate = rate_max;
+  for (double v : h->MkPerDt) h->max_rate = std::max(h->max_rate, v);
+  h->d_MkPerDt.upload(h->MkPerDt, s);
+  h->d_active1d.upload(h->active1d_h, s);
+  h->lat_visc = true;
+  if (h->ne3d == 0) return;
+  h->d_e3d.upload(h->e3d_h, s);
+  h->d_MkPerDt3.upload(rate3, s);
+  // tables
+  const size_t tab = (size_t)G.nlm * G.nlat;
+  for (DArr<double>* a : {&h->d_G6, &h->d_H6, &h->d_wP, &h->d_wD, &h->d_wG, &h->d_wH}) a->alloc(tab);
+  dim3 tg((G.nlat + 63) / 64, G.nlm);
+  k_visc3d_tables<<<tg, 64, 0, s>>>(G.nlm, G.nlat, G.d_lm_l.p, G.d_lm_m.p, G.d_plm.p, G.d_dplm.p, G.d_wts.p,
+                                    G.d_cott.p, G.d_invsin.p, h->d_G6.p, h->d_H6.p, h->d_wP.p, h->d_wD.p, h->d_wG.p,
+                                    h->d_wH.p);
+  VG_CUDA(cudaGetLastError());
+  h->d_n6.alloc(G.lmax + 1);
+  k_visc3d_n6<<<(G.lmax + 64) / 64, 64, 0, s>>>(G.lmax, G.nlat, G.d_mbeg.p, h->d_G6.p, h->d_H6.p, G.d_wts.p,
+                                               h->d_n6.p);
+  VG_CUDA(cudaGetLastError());
+  h->d_kbeg.upload(h->kbeg_h, s);
+  // work buffers
+  const int nf = 3 * h->ne3d, ncf = 2 * nf;
+  h->d_X.alloc((size_t)(h->nk + 1) * 4 * ncf);
+  h->d_Y.alloc((size_t)G.M * G.nlat * 6 * ncf);
+  h->d_dy.alloc((size_t)(h->nk + 1) * 6 * ncf);
+  VG_CUDA(cudaStreamSynchronize(s));
 }
 
 void visc3d_advance(vg_handle* h, const double* d_sigma, double dt) {
-  (void)h;
-  (void)d_sigma;
-  (void)dt;
-  throw Error("visc3d_advance: lateral viscosity is not built yet");
+  if (h->ne3d == 0) return;
+  PhaseScope ps(h, VG_PH_VISC3D);
+  const Grid& G = h->grid;
+  cudaStream_t s = h->stream;
+  const int nf = 3 * h->ne3d, ncf = 2 * nf;
+  V3Args A;
+  A.mem = h->d_mem[h->cur].p;
+  A.nxt = h->d_mem[1 - h->cur].p;
+  A.sigma = d_sigma;
+  A.kdeg = h->d_kdeg.p;
+  A.k2lm = h->d_k2lm.p;
+  A.e3d = h->d_e3d.p;
+  A.Jr = h->d_Jr.p;
+  A.xUn = h->d_xUn.p;
+  A.xVn = h->d_xVn.p;
+  A.dUn = h->d_dUn.p;
+  A.dVn = h->d_dVn.p;
+  A.mu = h->d_mu.p;
+  A.ne = h->ne;
+  A.nr = h->nr;
+  A.nk = h->nk;
+  A.ne3d = h->ne3d;
+  A.nf = nf;
+  A.ncf = ncf;
+  A.X = h->d_X.p;
+  dim3 gg((h->nk + 31) / 32, (h->ne3d + 7) / 8);
+  k_v3_gather<<<gg, dim3(32, 8), 0, s>>>(A);
+  ++h->n_launch;
+  VG_CUDA(cudaGetLastError());
+  // synthesis
+  GemmArgs S;
+  S.mode = 0;
+  S.lmax = G.lmax;
+  S.nlat = G.nlat;
+  S.nk = h->nk;
+  S.ncf = ncf;
+  S.mbeg = G.d_mbeg.p;
+  S.kbeg = h->d_kbeg.p;
+  const double* st[6] = {G.d_plm.p, G.d_dplm.p, G.d_plm.p, G.d_plm.p, h->d_G6.p, h->d_H6.p};
+  const int sc[6] = {0, 1, 1, 2, 3, 3};
+  for (int p = 0; p < 6; ++p) {
+    S.T[p] = st[p];
+    S.chan[p] = sc[p];
+  }
+  S.in = h->d_X.p;
+  S.out = h->d_Y.p;
+  dim3 sg((ncf + GB_N - 1) / GB_N, (G.nlat + GB_M - 1) / GB_M, G.M * 6);
+  k_v3_gemm<<<sg, 256, 0, s>>>(S);
+  ++h->n_launch;
+  VG_CUDA(cudaGetLastError());
+  // longitude pass
+  size_t lsm = (size_t)(6 * LON_FT * G.M * 2 + 6 * LON_FT * G.nphi) * sizeof(double);
+  static bool lon_attr = false;
+  if (!lon_attr) {
+    VG_CUDA(cudaFuncSetAttribute(k_v3_lon, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+    lon_attr = true;
+  }
+  if (lsm > 200 * 1024) throw Error("visc3d: grid too large for the longitude pass");
+  dim3 lg(G.nlat, (nf + LON_FT - 1) / LON_FT);
+  k_v3_lon<<<lg, 256, lsm, s>>>(h->d_Y.p, G.nlat, G.nphi, G.M, nf, dt, h->d_MkPerDt3.p, G.d_cos.p, G.d_sin.p,
+                                G.d_invsin.p);
+  ++h->n_launch;
+  VG_CUDA(cudaGetLastError());
+  // analysis
+  GemmArgs Aa = S;
+  Aa.mode = 1;
+  const double* at[6] = {h->d_wP.p, h->d_wD.p, h->d_wP.p, h->d_wP.p, h->d_wG.p, h->d_wH.p};
+  for (int p = 0; p < 6; ++p) Aa.T[p] = at[p];
+  Aa.in = h->d_Y.p;
+  Aa.out = h->d_dy.p;
+  dim3 ag((ncf + GB_N - 1) / GB_N, (G.M + GB_M - 1) / GB_M, G.M * 6);
+  k_v3_gemm<<<ag, 256, 0, s>>>(Aa);
+  ++h->n_launch;
+  VG_CUDA(cudaGetLastError());
+  k_v3_scatter<<<gg, dim3(32, 8), 0, s>>>(A, h->d_dy.p, h->d_n6.p);
+  ++h->n_launch;
+  VG_CUDA(cudaGetLastError());
 }
 
 }  // namespace vg

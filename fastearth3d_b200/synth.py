@@ -95,6 +95,7 @@ def random_sh_field(seed, lmax_field, lmax, nlat, nphi, std, mean):
     rng = np.random.default_rng(seed)
     nlm = (lmax + 1) * (lmax + 2) // 2
     q = np.zeros(nlm, complex)
+    lmax_field = min(lmax_field, lmax)
     for m in range(lmax_field + 1):
         for l in range(max(m, 1), lmax_field + 1):
             s = l ** -1.0  # amplitude ~ l^-1 -> variance ~ l^-2
@@ -166,12 +167,17 @@ class Workload:
         zb = np.ascontiguousarray(self.topo.reshape(-1))
         return zb, np.zeros(self.nlat * self.nphi)
 
-    def pert(self, elem_layers, rheology):
-        """(ne, nlat, nphi) perturbation: the lateral pattern in Maxwell elements."""
-        ne = len(elem_layers)
-        out = np.zeros((ne, self.nlat, self.nphi))
+    def pert(self, p):
+        """(ne, nlat, nphi) log10-viscosity perturbation for the params `p`
+        (explicit per-layer element counts): the lateral pattern in every
+        Maxwell element, zero elsewhere. Elements run bottom-up, layers are
+        surface-first."""
+        elem_layers = []
+        for i in range(p.n_layer - 1, -1, -1):
+            elem_layers += [i] * p.ne_layer[i]
+        out = np.zeros((len(elem_layers), self.nlat, self.nphi))
         for e, L in enumerate(elem_layers):
-            if rheology[L] == VG_RHEOL_MAXWELL:
+            if p.rheology[L] == VG_RHEOL_MAXWELL:
                 out[e] = self.pert2d
         return out
 

@@ -223,3 +223,84 @@ def test_disc_benchmark_on_gpu():
         m.advance(sigma)
     for it, step in ((1, 50), (2, 100), (3, 250), (4, 500)):
         assert abs(out[step] - uref[0, it]) <= 3e-2 * abs(uref[0, it])
+
+
+# ----------------------------------------------------------------- 3-D viscosity
+
+def _pert_for(model, seed, amp=0.3, lmax_field=6):
+    """Random smooth lateral log10-viscosity perturbation in every Maxwell element."""
+    p = model.p
+    f = synth.random_sh_field(seed, lmax_field, p.lmax, p.nlat, p.nphi, amp, 0.0)
+    elem_layers = []
+    for i in range(p.n_layer - 1, -1, -1):
+        elem_layers += [i] * p.ne_layer[i]
+    out = np.zeros((len(elem_layers), p.nlat, p.nphi))
+    for e, L in enumerate(elem_layers):
+        if p.rheology[L] == 1:
+            out[e] = f * (1.0 + 0.1 * e)
+    return out
+
+
+def test_visc3d_response_parity():
+    """Pseudo-spectral 3-D advance (FP64 GPU) vs the oracle's tensor-SH advance,
+    held load, 6 steps (src/vilma_response.f90:1171-1319)."""
+    g, o = pair(16, [2, 6, 5, 3], skip_tol=0.0, dt_init=50 * synth.SEC_PER_YEAR)
+    pert = _pert_for(g, 21)
+    g.enable_visc3d(pert)
+    o.enable_visc3d(pert)
+    assert g.info().ne3d == o.info().ne3d > 0
+    rng = np.random.default_rng(8)
+    sigma = rand_sigma(rng, g.nlm, 16)
+    for _ in range(6):
+        for mdl in (g, o):
+            mdl.begin_step()
+        ug, ng_ = g.apply(sigma)
+        uo, no = o.apply(sigma)
+        assert rel(ug, uo) < TOL and rel(ng_, no) < TOL
+        g.advance(sigma)
+        o.advance(sigma)
+    sg, _ = g.state()
+    so, _ = o.state()
+    for a, b in zip(sg, so):
+        assert rel(a, b) < TOL_STATE
+
+
+def test_visc3d_uniform_equals_1d_on_gpu():
+    """A laterally uniform perturbation through the 3-D path reproduces the
+    1-D path (tests/test_response_3d.f90:218-250), 1e-9 relative."""
+    kw = dict(skip_tol=0.0, dt_init=50 * synth.SEC_PER_YEAR)
+    g3, _ = pair(12, [2, 5, 4, 3], visc3d_tol=-1.0, **kw)
+    g1, _ = pair(12, [2, 5, 4, 3], visc3d_tol=10.0, **kw)
+    pert = np.full((g3.ne, 13, 26), 0.3)
+    g3.enable_visc3d(pert)
+    g1.enable_visc3d(pert)
+    assert g3.info().ne3d > 0 and g1.info().ne3d == 0
+    rng = np.random.default_rng(11)
+    sigma = rand_sigma(rng, g3.nlm, 12)
+    for _ in range(5):
+        for m in (g3, g1):
+            m.begin_step()
+            m.advance(sigma)
+    s3, _ = g3.state()
+    s1, _ = g1.state()
+    mx = max(np.abs(a).max() for a in s1)
+    assert max(np.abs(a - b).max() for a, b in zip(s3, s1)) <= 1e-9 * mx
+
+
+def test_visc3d_update_parity_with_sea_level():
+    w = synth.Workload("t", 16, 20, 50.0, 3, 2, "sawtooth", sle=True, visc3d=True, seed=13)
+    pg = w.params(vlib.default_params)
+    po = w.params(orc.default_params)
+    g, o = vlib.Model(pg), orc.Oracle(po)
+    pert = w.pert(pg)
+    g.enable_visc3d(pert)
+    o.enable_visc3d(pert)
+    zb, hi = w.reference()
+    for m in (g, o):
+        m.set_reference(zb, hi)
+    for step in range(1, 4):
+        ice = w.ice_at(step * 200)
+        g.update(ice, w.dt_yr)
+        o.update(ice, w.dt_yr)
+    assert g.info().n_sub_last == o.info().n_sub_last >= 1
+    check_models(g, o)
