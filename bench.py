@@ -43,6 +43,8 @@ def parse():
     ap.add_argument("--workload", default=DEFAULT_WORKLOAD)
     ap.add_argument("--cpu-sample-s", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--precision", default="split_tc", choices=["split_tc", "fp64"],
+                    help="3-D stress products of the timed arm (a plain FP64 arm is always timed beside split_tc)")
     return ap.parse_args()
 
 
@@ -112,19 +114,6 @@ def algorithmic_bytes(info, phase):
 FP64_NOMINAL_TFLOPS = 37.0  # B200 dense FP64 (vector and tensor), datasheet figure
 
 
-def visc3d_flops(w, info):
-    """Algorithmic FLOPs of one pseudo-spectral 3-D advance (one sub-step):
-    6 Legendre products each way (2 flops per multiply-add over nlat x nlm x
-    2 nf columns) and the longitude pass (inverse + forward DFT of 6 dyadic
-    components of nf fields at every latitude, half-period split)."""
-    nf = 3 * info.ne3d
-    ncf = 2 * nf
-    nlat, nphi, M = w.nlat, w.nphi, w.lmax + 1
-    legendre = 2 * 6 * 2 * nlat * info.nlm * ncf
-    lon = 6 * nf * nlat * (nphi // 2) * M * 9
-    return float(legendre + lon)
-
-
 def cpu_baseline(w, budget_s, threads):
     from oracle import orc  # the CPU restatement: test/baseline infrastructure only
 
@@ -180,6 +169,139 @@ def run_reference(args, w):
     print(json.dumps(out))
 
 
+def stage_work(w, info):
+    """Algorithmic work of one call of each fine-grained phase.
+
+    Tensor-core stages of the split path: the MMA flops the decomposition
+    needs (2 x rows x N x K per sub-GEMM, three split products), summed over
+    the stage's sub-GEMMs (parity / half-period halves, no padding). The gather
+    and scatter stream the Maxwell-element state and the FP32 operand rows.
+    Returned as {phase: (kind, amount)} with kind "flop" or "byte".
+    """
+    L, nlat, nphi = w.lmax, w.nlat, w.nphi
+    nh, half = (nlat + 1) // 2, nphi // 2
+    F = 3 * info.ne3d
+    NC, NCOL = 2 * F, 6 * F
+    kev, kod = 2 * (L // 2), 2 * ((L + 1) // 2)
+    legendre = 3 * 2.0 * NC * nh * info.nlm * 6  # sum over m of (K_E + K_O) = nlm, 6 products
+    inv = 3 * 2.0 * NCOL * (half - 1) * (kev + kod) * nlat
+    fwd = 3 * 2.0 * NCOL * (kev + kod) * half * nlat
+    ne3d, nk = info.ne3d, info.nk
+    state3 = 6 * 4 * ne3d * nk * 8  # memory of the 3-D elements, one buffer
+    drift = 2 * 2 * (ne3d + 1) * nk * 8
+    gather = state3 + drift + (nk + 1) * 4 * NC * 4
+    scatter = 2 * state3 + (nk + 1) * 6 * NC * 4
+    return {"v3_synth": ("flop", legendre), "v3_analysis": ("flop", legendre), "v3_lon_inv": ("flop", inv),
+            "v3_lon_fwd": ("flop", fwd), "v3_gather": ("byte", gather), "v3_scatter": ("byte", scatter),
+            "drift": ("byte", algorithmic_bytes(info, "drift")),
+            "advance_1d": ("byte", algorithmic_bytes(info, "advance_1d"))}
+
+
+def run_arm(w, precision, args, ice_dev, local, dist, want_e2e):
+    """Warm-up, device-timed region, phase-timer pass and end-to-end pass of one
+    model instance of the workload; returns the measurements."""
+    import torch
+
+    from fastearth3d_b200 import lib as vlib
+
+    p = w.params(vlib.default_params)
+    p.visc3d_precision = precision
+    m = vlib.Model(p)
+    zb, hi = w.reference()
+    m.set_reference(zb, hi)
+    if w.visc3d:
+        m.enable_visc3d(w.pert(m.p))
+    ng = w.nlat * w.nphi
+    total = args.warmup + args.steps
+    stream = torch.cuda.ExternalStream(m.stream_ptr())
+    for s in range(args.warmup):
+        m.update_device(ice_dev[s].data_ptr(), w.dt_yr)
+    launches0 = m.info().n_launch
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clk:
+        with torch.cuda.stream(stream):
+            ev0.record()
+        for s in range(args.warmup, total):
+            m.update_device(ice_dev[s].data_ptr(), w.dt_yr)
+        with torch.cuda.stream(stream):
+            ev1.record()
+        torch.cuda.synchronize()
+    ms = ev0.elapsed_time(ev1)
+    out = {"ms": ms, "launches": m.info().n_launch - launches0, "info": m.info(), "clocks": clk.summary()}
+    out["rsl"], out["zbed"] = m.fields()[:2]
+    if dist:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        out["ms"] = float(t.item())
+        dist.barrier()
+    # phase timers over a few more steps (separate pass: the timers add events)
+    n_prof = min(args.steps, 5)
+    m.profile_enable(True)
+    for s in range(total, total + n_prof):
+        m.update_device(ice_dev[s].data_ptr(), w.dt_yr)
+    out["ph_ms"], out["ph_calls"] = m.profile_read()
+    m.profile_enable(False)
+    if want_e2e:
+        # end to end through the public C-ABI: host ice in pinned memory, rsl read back every step
+        n_e2e = min(args.steps, 10)
+        ice_host = torch.empty((n_e2e, ng), dtype=torch.float64).pin_memory()
+        for s in range(n_e2e):
+            ice_host[s] = torch.from_numpy(w.ice_at(total + n_prof + s + 1))
+        rsl_host = np.zeros(ng)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        with torch.cuda.stream(stream):
+            e0.record()
+        for s in range(n_e2e):
+            vlib.lib().vg_update(m.h, vlib.C.cast(ice_host[s].data_ptr(), vlib._P), w.dt_yr)
+            vlib.lib().vg_get_fields(m.h, vlib.ptr(rsl_host), None, None, None)
+        with torch.cuda.stream(stream):
+            e1.record()
+        torch.cuda.synchronize()
+        out["e2e_ms"] = e0.elapsed_time(e1) / n_e2e
+    del m
+    torch.cuda.synchronize()
+    return out
+
+
+def phases_of(arm):
+    from fastearth3d_b200.abi import PHASE_NAMES
+
+    return {n: {"ms_per_call": arm["ph_ms"][i] / arm["ph_calls"][i] if arm["ph_calls"][i] else 0.0,
+                "calls": int(arm["ph_calls"][i]), "ms_total": float(arm["ph_ms"][i])}
+            for i, n in enumerate(PHASE_NAMES)}
+
+
+def roofline(w, arm, pk, pk_kind, split):
+    """Roofline of the dominant kernel (the fine-grained phase with the most
+    time; each such phase is one kernel launch)."""
+    info = arm["info"]
+    ph = phases_of(arm)
+    work = stage_work(w, info)
+    cands = [n for n in work if ph.get(n, {}).get("calls")]
+    dom = max(cands, key=lambda n: ph[n]["ms_total"])
+    kind, amount = work[dom]
+    t = ph[dom]["ms_per_call"] * 1e-3
+    if kind == "byte":
+        ach = amount / t / 1e9
+        return {"bound": "hbm", "kernel": dom, "achieved": ach, "peak": pk["hbm_gbs"], "unit": "GB/s",
+                "frac": ach / pk["hbm_gbs"], "peak_kind": pk_kind + " copy bandwidth", "traffic": None,
+                "algorithmic_bytes_per_launch": amount}
+    ach = amount / t / 1e12
+    if split:
+        peak = 0.5 * pk["bf16_tflops_sustained"]
+        return {"bound": "tensor", "kernel": dom, "achieved": ach, "peak": peak, "unit": "TFLOP/s",
+                "frac": ach / peak, "peak_kind": pk_kind + " sustained dense bf16 x 0.5 (tf32 rate)",
+                "traffic": None, "algorithmic_flops_per_launch": amount}
+    fp64 = amount / 3.0 / t / 1e12  # FP64 path: one product per multiply-add instead of three
+    return {"bound": "fp64", "kernel": dom, "achieved": fp64, "peak": FP64_NOMINAL_TFLOPS, "unit": "TFLOP/s",
+            "frac": fp64 / FP64_NOMINAL_TFLOPS, "peak_kind": "nominal FP64 (no measured FP64 peak)",
+            "traffic": None, "algorithmic_flops_per_launch": amount / 3.0}
+
+
 def main():
     args = parse()
     w = synth.workloads()[args.workload]
@@ -200,94 +322,22 @@ def main():
         import torch.distributed as dist
 
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
-    from fastearth3d_b200 import lib as vlib
-
-    m = vlib.Model(w.params(vlib.default_params))
-    zb, hi = w.reference()
-    m.set_reference(zb, hi)
-    if w.visc3d:
-        m.enable_visc3d(w.pert(m.p))
     ng = w.nlat * w.nphi
     total = args.warmup + args.steps
     n_prof = min(args.steps, 5)
-    n_e2e = min(args.steps, 10)
     ice_dev = torch.empty((total + n_prof + 1, ng), dtype=torch.float64, device="cuda")
     for s in range(total + n_prof + 1):
         ice_dev[s] = torch.from_numpy(w.ice_at(s + 1))
-    stream = torch.cuda.ExternalStream(m.stream_ptr())
-    for s in range(args.warmup):
-        m.update_device(ice_dev[s].data_ptr(), w.dt_yr)
-    launches0 = m.info().n_launch
-    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    if dist:
-        dist.barrier()
-    torch.cuda.synchronize()
-    with ClockSampler(local) as clk:
-        with torch.cuda.stream(stream):
-            ev0.record()
-        for s in range(args.warmup, total):
-            m.update_device(ice_dev[s].data_ptr(), w.dt_yr)
-        with torch.cuda.stream(stream):
-            ev1.record()
-        torch.cuda.synchronize()
-    ms = ev0.elapsed_time(ev1)
-    launches = m.info().n_launch - launches0
-    info = m.info()
-    if dist:
-        t = torch.tensor([ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
-        dist.barrier()
-    # phase timers over a few more steps (separate pass: the timers add events)
-    m.profile_enable(True)
-    for s in range(total, total + n_prof):
-        m.update_device(ice_dev[s].data_ptr(), w.dt_yr)
-    ph_ms, ph_calls = m.profile_read()
-    m.profile_enable(False)
-    # end to end through the public API: host ice in pinned memory, rsl read back each step
-    ice_host = torch.empty((n_e2e, ng), dtype=torch.float64).pin_memory()
-    for s in range(n_e2e):
-        ice_host[s] = torch.from_numpy(w.ice_at(total + n_prof + s + 1))
-    rsl_host = np.zeros(ng)
-    torch.cuda.synchronize()
-    t0 = time.perf_counter()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    with torch.cuda.stream(stream):
-        e0.record()
-    for s in range(n_e2e):
-        vlib.lib().vg_update(m.h, vlib.C.cast(ice_host[s].data_ptr(), vlib._P), w.dt_yr)
-        vlib.lib().vg_get_fields(m.h, vlib.ptr(rsl_host), None, None, None)
-    with torch.cuda.stream(stream):
-        e1.record()
-    torch.cuda.synchronize()
-    e2e_ms = e0.elapsed_time(e1) / n_e2e
+    split = w.visc3d and args.precision == "split_tc"
+    main_arm = run_arm(w, 1 if split else 0, args, ice_dev, local, dist, True)
+    plain = run_arm(w, 0, args, ice_dev, local, dist, False) if split else None
     if rank != 0:
         if dist:
             dist.destroy_process_group()
         return
     pk, pk_kind = peaks()
-    names = ["drift", "advance_1d", "visc3d", "sle"]
-    phases = {names[i]: {"ms_per_call": ph_ms[i] / ph_calls[i] if ph_calls[i] else 0.0, "calls": int(ph_calls[i]),
-                         "ms_total": ph_ms[i]} for i in range(4)}
-    dom = max(["drift", "advance_1d", "visc3d"], key=lambda n: phases[n]["ms_total"])
-    if dom == "visc3d":
-        fl = visc3d_flops(w, info)
-        ach = fl / (phases[dom]["ms_per_call"] * 1e-3) / 1e12
-        if m.p.visc3d_precision == 0:
-            roof = {"bound": "fp64", "kernel": "visc3d (Legendre GEMMs + longitude DFT, FP64)", "achieved": ach,
-                    "peak": FP64_NOMINAL_TFLOPS, "unit": "TFLOP/s", "frac": ach / FP64_NOMINAL_TFLOPS,
-                    "peak_kind": "nominal FP64 (no measured FP64 peak)", "traffic": None,
-                    "algorithmic_flops_per_launch": fl}
-        else:
-            roof = {"bound": "tensor", "kernel": "visc3d", "achieved": ach, "peak": pk["bf16_tflops_sustained"],
-                    "unit": "TFLOP/s", "frac": ach / pk["bf16_tflops_sustained"], "peak_kind": pk_kind + " sustained",
-                    "traffic": None, "algorithmic_flops_per_launch": fl}
-    else:
-        byts = algorithmic_bytes(info, dom)
-        ach = byts / (phases[dom]["ms_per_call"] * 1e-3) / 1e9
-        roof = {"bound": "hbm", "kernel": dom, "achieved": ach, "peak": pk["hbm_gbs"], "unit": "GB/s",
-                "frac": ach / pk["hbm_gbs"], "peak_kind": pk_kind, "traffic": None,
-                "algorithmic_bytes_per_launch": byts}
+    info = main_arm["info"]
+    ms = main_arm["ms"]
     out = {
         "metric": METRIC,
         "value": world * args.steps / (ms * 1e-3),
@@ -299,18 +349,31 @@ def main():
         "higher_is_better": True,
         "scaling": "weak",
         "vs_baseline": None,
-        "dtype": "f64",
+        "dtype": "tf32x3 3-D stress products, f64 elsewhere" if split else "f64",
         "data": "synthetic",
         "config": {"workload": w.name, "lmax": w.lmax, "grid": f"{w.nlat}x{w.nphi}", "radial_elements": w.n_elem,
                    "dt_yr": w.dt_yr, "n_sub": info.n_sub_last, "visc3d": w.visc3d, "sea_level": w.sle,
-                   "parallelism": f"replicas{world}",
+                   "visc3d_precision": "split_tc" if split else "fp64", "parallelism": f"replicas{world}",
                    "l2": "state larger than L2 (%.0f MB streamed per sub-step)" % (6 * 4 * info.ne * info.nk * 8 / 1e6)},
-        "e2e": {"value": 1e3 / e2e_ms, "unit": "steps/s", "h2d_bytes_per_step": ng * 8, "d2h_bytes_per_step": ng * 8},
-        "gpu_launches": int(launches),
-        "roofline": roof,
-        "phases": phases,
-        "clocks": clk.summary(),
+        "e2e": {"value": 1e3 / main_arm["e2e_ms"], "unit": "steps/s", "h2d_bytes_per_step": ng * 8,
+                "d2h_bytes_per_step": ng * 8},
+        "gpu_launches": int(main_arm["launches"]),
+        "roofline": roofline(w, main_arm, pk, pk_kind, split),
+        "phases": phases_of(main_arm),
+        "clocks": main_arm["clocks"],
     }
+    if plain is not None:
+        r0, r1 = plain["rsl"], main_arm["rsl"]
+        z0, z1 = plain["zbed"], main_arm["zbed"]
+        out["plain_fp64"] = {
+            "value": world * args.steps / (plain["ms"] * 1e-3), "unit": "steps/s",
+            "ms_per_step": plain["ms"] / args.steps, "speedup_split_over_plain": plain["ms"] / ms,
+            "gpu_launches": int(plain["launches"]), "phases": phases_of(plain), "clocks": plain["clocks"],
+            "roofline": roofline(w, plain, pk, pk_kind, False)}
+        out["split_error_vs_fp64"] = {
+            "after_steps": total, "rsl": float(np.abs(r1 - r0).max() / np.abs(r0).max()),
+            "z_bed": float(np.abs(z1 - z0).max() / np.abs(z0).max()), "norm": "max abs diff / max abs (FP64 GPU)",
+            "rsl_target": 1e-8}
     if not args.no_cpu_baseline:
         out["cpu_baseline"] = cpu_baseline(w, args.cpu_sample_s, os.cpu_count() or 1)
     print(json.dumps(out))

@@ -55,7 +55,9 @@ class VgInfo(C.Structure):
 
 
 VG_PH_DRIFT, VG_PH_ADVANCE_1D, VG_PH_VISC3D, VG_PH_SLE, VG_NPHASE = 0, 1, 2, 3, 4
-PHASE_NAMES = ["drift", "advance_1d", "visc3d", "sle"]
+PHASE_NAMES = ["drift", "advance_1d", "visc3d", "sle", "v3_gather", "v3_synth", "v3_lon_inv", "v3_lon_fwd",
+               "v3_analysis", "v3_scatter"]
+VG_NPHASE = len(PHASE_NAMES)
 
 
 def set_layers(p, layers):

@@ -151,7 +151,7 @@ struct vg_handle {
   int cur = 0;
   vg::DArr<double> d_dUn, d_dVn, d_drift;  // drift: dUa re,im, dFa re,im, dVa re,im (6*nk)
   vg::DArr<double> d_mnorm, d_xs;          // per-slot memory norm (2 buffers x nk); band-solve scratch
-  vg::DArr<unsigned long long> d_maxbits;  // max |memory| of each buffer (double bits)
+  vg::DArr<unsigned long long> d_maxbits;  // max |memory| of each buffer (double bits); [2] kernel status bits
   vg::DArr<vg::SleScalars> d_sc_;
   vg::SleScalars* h_sc = nullptr;  // pinned
   double mem_norm = 0.0;           // ||state cur||_inf (host copy)
@@ -177,6 +177,12 @@ struct vg_handle {
   bool have_reference = false;
   long long n_launch = 0;  // kernels launched by the time step (all phases)
   vg::Prof prof;
+  // split-precision tensor-core plan of the 3-D advance (owned, opaque here)
+  void* tc_plan = nullptr;
+  void (*tc_plan_release)(void*) = nullptr;
+  ~vg_handle() {
+    if (tc_plan_release) tc_plan_release(tc_plan);
+  }
 };
 
 namespace vg {
@@ -203,6 +209,10 @@ void update_bsl(vg_handle* h);
 // 3-D (vg_visc3d.cu)
 void visc3d_enable(vg_handle* h, const double* pert_host);
 void visc3d_advance(vg_handle* h, const double* d_sigma, double dt);
+// 3-D split-precision tensor-core stages (vg_tc.cu)
+void visc3d_tc_enable(vg_handle* h);
+void visc3d_tc_buffers(vg_handle* h, float** X, float** dy);
+void visc3d_tc_run(vg_handle* h, double dt);
 // misc
 void sync_scalars(vg_handle* h);
 // phase timer scope: records a start event now and a stop event at scope exit

@@ -14,6 +14,7 @@
 //                  L sweep, kl = 6; 13 in the U sweep, kv = 12). Only the L-sweep
 //                  output y goes through memory (L2-resident scratch).
 // Degree 1 (bordered, dense): a mat-vec with the precomputed response block G1.
+#include <cstdio>
 #include <cstring>
 
 #include "vg_device.cuh"
@@ -598,11 +599,17 @@ void compute_mem_norm(vg_handle* h, int buf) {
 }
 
 double read_mem_norm(vg_handle* h, int buf) {
-  unsigned long long bits = 0;
-  VG_CUDA(cudaMemcpyAsync(&bits, h->d_maxbits.p + buf, sizeof(bits), cudaMemcpyDeviceToHost, h->stream));
+  unsigned long long bits[3] = {0, 0, 0};
+  VG_CUDA(cudaMemcpyAsync(bits, h->d_maxbits.p, sizeof(bits), cudaMemcpyDeviceToHost, h->stream));
   VG_CUDA(cudaStreamSynchronize(h->stream));
+  if (bits[2] != 0) {
+    char msg[160];
+    std::snprintf(msg, sizeof(msg), "tensor-core stage wait timed out (status bits 0x%llx); results are invalid",
+                  bits[2]);
+    throw Error(msg);
+  }
   double v;
-  std::memcpy(&v, &bits, sizeof(v));
+  std::memcpy(&v, &bits[buf], sizeof(v));
   return v;
 }
 

@@ -881,7 +881,7 @@ void setup_handle(vg_handle* h) {
   h->d_dVn.alloc((size_t)2 * nr * nk);
   h->d_drift.alloc((size_t)6 * nk);
   h->d_mnorm.alloc((size_t)2 * nk);
-  h->d_maxbits.alloc(2);
+  h->d_maxbits.alloc(3);  // two buffer norms + kernel status bits
   h->d_xs.alloc((size_t)2 * nd * nk);
   h->d_bh.alloc((size_t)2 * 2 * nr * nk);
   h->d_sc_.alloc(1);

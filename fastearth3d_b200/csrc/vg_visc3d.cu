@@ -80,18 +80,19 @@ struct V3Args {
   const int *kdeg, *k2lm, *e3d;
   const double *Jr, *xUn, *xVn, *dUn, *dVn, *mu;
   int ne, nr, nk, ne3d, nf, ncf;  // ncf = 2 nf
-  double* X;                      // (nk + 1) rows x (4 * ncf)
 };
 
-// one thread per (slot k, 3-D element): strain of both histories, 24 values
-__global__ void __launch_bounds__(256) k_v3_gather(V3Args A) {
+// one thread per (slot k, 3-D element): strain of both histories, 24 values,
+// written as X[k][ch][f][ri] (FP64, or FP32 for the tensor-core stages)
+template <class T>
+__global__ void __launch_bounds__(256) k_v3_gather(V3Args A, T* __restrict__ X) {
   const int k = blockIdx.x * 32 + threadIdx.x, ei = blockIdx.y * 8 + threadIdx.y;
   if (k >= A.nk || ei >= A.ne3d) return;
   const int e = A.e3d[ei], l = A.kdeg[k], lm = A.k2lm[k];
   const double Jr = A.Jr[l], twoMu = 2.0 * A.mu[e];
   const double* xu = A.xUn + (size_t)l * A.nr;
   const double* xv = A.xVn + (size_t)l * A.nr;
-  double* row = A.X + (size_t)k * 4 * A.ncf;
+  T* row = X + (size_t)k * 4 * A.ncf;
   for (int ri = 0; ri < 2; ++ri) {
     const double s = A.sigma[2 * lm + ri];
     const double U0 = s * xu[e] + A.dUn[((size_t)ri * A.nr + e) * A.nk + k];
@@ -106,7 +107,7 @@ __global__ void __launch_bounds__(256) k_v3_gather(V3Args A) {
       for (int lam = 0; lam < 4; ++lam) {
         double v = A.mem[mem_idx(s3, ri, e, lam, k, A.ne, A.nk)] + twoMu * eps[s3][lam];
         if (lam == 2) v = -Jr * v;  // trace channel enters the synthesis as -l(l+1) c
-        row[(size_t)lam * A.ncf + (3 * ei + s3) * 2 + ri] = v;
+        row[(size_t)lam * A.ncf + (3 * ei + s3) * 2 + ri] = (T)v;
       }
   }
 }
@@ -314,18 +315,19 @@ __global__ void __launch_bounds__(256) k_v3_lon(double* __restrict__ S, int nlat
 
 // Channel normalisations and the increment form c += Delta
 // (src/vilma_response.f90:1281-1318): one thread per (slot, 3-D element).
-__global__ void __launch_bounds__(256) k_v3_scatter(V3Args A, const double* __restrict__ R,
+template <class T>
+__global__ void __launch_bounds__(256) k_v3_scatter(V3Args A, const T* __restrict__ R,
                                                     const double* __restrict__ n6) {
   const int k = blockIdx.x * 32 + threadIdx.x, ei = blockIdx.y * 8 + threadIdx.y;
   if (k >= A.nk || ei >= A.ne3d) return;
   const int e = A.e3d[ei], l = A.kdeg[k];
   const double J = A.Jr[l], nn = n6[l];
-  const double* row = R + (size_t)k * 6 * A.ncf;
+  const T* row = R + (size_t)k * 6 * A.ncf;
   for (int s3 = 0; s3 < 3; ++s3) {
     const int f = 3 * ei + s3;
     double q[6][2];
     for (int p = 0; p < 6; ++p)
-      for (int ri = 0; ri < 2; ++ri) q[p][ri] = row[(size_t)p * A.ncf + 2 * f + ri];
+      for (int ri = 0; ri < 2; ++ri) q[p][ri] = (double)row[(size_t)p * A.ncf + 2 * f + ri];
     double d[4][2];
     d[0][0] = q[0][0];
     d[0][1] = q[0][1];
@@ -403,7 +405,12 @@ void visc3d_enable(vg_handle* h, const double* pert) {
                                                h->d_n6.p);
   VG_CUDA(cudaGetLastError());
   h->d_kbeg.upload(h->kbeg_h, s);
-  // work buffers
+  VG_CUDA(cudaStreamSynchronize(s));
+  if (h->p.visc3d_precision == VG_VISC3D_SPLIT_TC) {
+    visc3d_tc_enable(h);
+    return;
+  }
+  // work buffers of the FP64 path
   const int nf = 3 * h->ne3d, ncf = 2 * nf;
   h->d_X.alloc((size_t)(h->nk + 1) * 4 * ncf);
   h->d_Y.alloc((size_t)G.M * G.nlat * 6 * ncf);
@@ -436,11 +443,29 @@ void visc3d_advance(vg_handle* h, const double* d_sigma, double dt) {
   A.ne3d = h->ne3d;
   A.nf = nf;
   A.ncf = ncf;
-  A.X = h->d_X.p;
   dim3 gg((h->nk + 31) / 32, (h->ne3d + 7) / 8);
-  k_v3_gather<<<gg, dim3(32, 8), 0, s>>>(A);
-  ++h->n_launch;
-  VG_CUDA(cudaGetLastError());
+  if (h->p.visc3d_precision == VG_VISC3D_SPLIT_TC) {
+    float *X32 = nullptr, *dy32 = nullptr;
+    visc3d_tc_buffers(h, &X32, &dy32);
+    {
+      PhaseScope pg(h, VG_PH_V3_GATHER);
+      k_v3_gather<float><<<gg, dim3(32, 8), 0, s>>>(A, X32);
+      ++h->n_launch;
+      VG_CUDA(cudaGetLastError());
+    }
+    visc3d_tc_run(h, dt);
+    PhaseScope pc(h, VG_PH_V3_SCATTER);
+    k_v3_scatter<float><<<gg, dim3(32, 8), 0, s>>>(A, dy32, h->d_n6.p);
+    ++h->n_launch;
+    VG_CUDA(cudaGetLastError());
+    return;
+  }
+  {
+    PhaseScope pg(h, VG_PH_V3_GATHER);
+    k_v3_gather<double><<<gg, dim3(32, 8), 0, s>>>(A, h->d_X.p);
+    ++h->n_launch;
+    VG_CUDA(cudaGetLastError());
+  }
   // synthesis
   GemmArgs S;
   S.mode = 0;
@@ -459,9 +484,12 @@ void visc3d_advance(vg_handle* h, const double* d_sigma, double dt) {
   S.in = h->d_X.p;
   S.out = h->d_Y.p;
   dim3 sg((ncf + GB_N - 1) / GB_N, (G.nlat + GB_M - 1) / GB_M, G.M * 6);
-  k_v3_gemm<<<sg, 256, 0, s>>>(S);
-  ++h->n_launch;
-  VG_CUDA(cudaGetLastError());
+  {
+    PhaseScope pp(h, VG_PH_V3_SYNTH);
+    k_v3_gemm<<<sg, 256, 0, s>>>(S);
+    ++h->n_launch;
+    VG_CUDA(cudaGetLastError());
+  }
   // longitude pass
   size_t lsm = (size_t)(6 * LON_FT * G.M * 2 + 6 * LON_FT * G.nphi) * sizeof(double);
   static bool lon_attr = false;
@@ -471,10 +499,13 @@ void visc3d_advance(vg_handle* h, const double* d_sigma, double dt) {
   }
   if (lsm > 200 * 1024) throw Error("visc3d: grid too large for the longitude pass");
   dim3 lg(G.nlat, (nf + LON_FT - 1) / LON_FT);
-  k_v3_lon<<<lg, 256, lsm, s>>>(h->d_Y.p, G.nlat, G.nphi, G.M, nf, dt, h->d_MkPerDt3.p, G.d_cos.p, G.d_sin.p,
-                                G.d_invsin.p);
-  ++h->n_launch;
-  VG_CUDA(cudaGetLastError());
+  {
+    PhaseScope pp(h, VG_PH_V3_LON_INV);
+    k_v3_lon<<<lg, 256, lsm, s>>>(h->d_Y.p, G.nlat, G.nphi, G.M, nf, dt, h->d_MkPerDt3.p, G.d_cos.p, G.d_sin.p,
+                                  G.d_invsin.p);
+    ++h->n_launch;
+    VG_CUDA(cudaGetLastError());
+  }
   // analysis
   GemmArgs Aa = S;
   Aa.mode = 1;
@@ -483,10 +514,14 @@ void visc3d_advance(vg_handle* h, const double* d_sigma, double dt) {
   Aa.in = h->d_Y.p;
   Aa.out = h->d_dy.p;
   dim3 ag((ncf + GB_N - 1) / GB_N, (G.M + GB_M - 1) / GB_M, G.M * 6);
-  k_v3_gemm<<<ag, 256, 0, s>>>(Aa);
-  ++h->n_launch;
-  VG_CUDA(cudaGetLastError());
-  k_v3_scatter<<<gg, dim3(32, 8), 0, s>>>(A, h->d_dy.p, h->d_n6.p);
+  {
+    PhaseScope pp(h, VG_PH_V3_ANALYSIS);
+    k_v3_gemm<<<ag, 256, 0, s>>>(Aa);
+    ++h->n_launch;
+    VG_CUDA(cudaGetLastError());
+  }
+  PhaseScope pc(h, VG_PH_V3_SCATTER);
+  k_v3_scatter<double><<<gg, dim3(32, 8), 0, s>>>(A, h->d_dy.p, h->d_n6.p);
   ++h->n_launch;
   VG_CUDA(cudaGetLastError());
 }

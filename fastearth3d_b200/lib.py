@@ -9,7 +9,7 @@ import os
 
 import numpy as np
 
-from .abi import VgInfo, VgParams
+from .abi import VG_NPHASE, VgInfo, VgParams
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "libvilma_gpu.so")
@@ -191,8 +191,8 @@ class Model:
 
     def profile_read(self):
         """Per-phase (milliseconds, calls) since the last read (and reset)."""
-        ms = np.zeros(4)
-        calls = (C.c_longlong * 4)()
+        ms = np.zeros(VG_NPHASE)
+        calls = (C.c_longlong * VG_NPHASE)()
         self._c(lib().vg_profile_read(self.h, ptr(ms), calls))
         return ms, np.array(calls[:])
 

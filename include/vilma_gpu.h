@@ -76,7 +76,20 @@ typedef struct vg_params {
 /* Phase timers (the reference's [PROFILE] buckets: drift solve, memory
  * advance, 3-D advance, sea-level transforms + grid work; src/vilma_drive.f90:
  * 219-305). */
-enum { VG_PH_DRIFT = 0, VG_PH_ADVANCE_1D = 1, VG_PH_VISC3D = 2, VG_PH_SLE = 3, VG_NPHASE = 4 };
+enum {
+  VG_PH_DRIFT = 0,
+  VG_PH_ADVANCE_1D = 1,
+  VG_PH_VISC3D = 2,
+  VG_PH_SLE = 3,
+  /* stages inside VG_PH_VISC3D (FP64 path: the whole longitude pass is V3_LON_INV) */
+  VG_PH_V3_GATHER = 4,
+  VG_PH_V3_SYNTH = 5,
+  VG_PH_V3_LON_INV = 6,
+  VG_PH_V3_LON_FWD = 7,
+  VG_PH_V3_ANALYSIS = 8,
+  VG_PH_V3_SCATTER = 9,
+  VG_NPHASE = 10
+};
 
 typedef struct vg_info {
   int lmax, nlat, nphi, nlm, nr, ne, ndof, nk, ne3d;
