@@ -38,6 +38,7 @@ _SIGS = [
     ("vg_set_state", [_VP, _P, _P, _P, _P, _P, _P, C.c_double]),
     ("vg_sht_analysis", [_VP, _P, _P]),
     ("vg_sht_synthesis", [_VP, _P, _P]),
+    ("vg_sht_analysis_noalloc", [_VP, C.c_void_p, C.c_void_p, C.c_int]),
     ("vg_stream", [_VP, C.POINTER(C.c_void_p)]),
     ("vg_profile_enable", [_VP, C.c_int]),
     ("vg_profile_read", [_VP, _P, C.POINTER(C.c_longlong)]),

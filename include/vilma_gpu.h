@@ -166,6 +166,24 @@ int vg_set_state(vg_handle* h, const double* Are, const double* Aim, const doubl
 int vg_sht_analysis(vg_handle* h, const double* f, double* q_lm);
 int vg_sht_synthesis(vg_handle* h, const double* q_lm, double* f);
 
+/* vg_sht_analysis on device buffers, allocating nothing (no counterpart in the
+ * reference). d_f holds `batch` grid fields ((nphi, nlat) each, phi fastest),
+ * d_q_lm receives `batch` spectra (nlm complex each, interleaved re/im). The
+ * work is queued on the handle's stream and not waited for.
+ * For callers that may not allocate device memory at the point of the call:
+ * hosts that reserve all device memory up front (a climate coupler with its
+ * own pool), code that runs while memory is exhausted, and callers that
+ * cannot tolerate the implicit synchronisation an allocation brings. The
+ * Fourier scratch is a file-scope device array of VG_NOALLOC_SCRATCH_DOUBLES
+ * doubles per device, so 2 * (mmax + 1) * nlat * batch must not exceed it
+ * (larger requests return an error); its address is looked up once per
+ * device, with the handle's device current (make the first call before any
+ * stream capture). The scratch carries nothing between calls. Calls that
+ * overlap in time on one device share that array and race: order them on
+ * one stream. */
+#define VG_NOALLOC_SCRATCH_DOUBLES (1 << 19)
+int vg_sht_analysis_noalloc(vg_handle* h, const double* d_f, double* d_q_lm, int batch);
+
 /* The CUDA stream (cudaStream_t) all of the handle's work is ordered on, so a
  * caller can record events on it. */
 int vg_stream(vg_handle* h, void** stream);
