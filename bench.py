@@ -44,7 +44,9 @@ def parse():
     ap.add_argument("--cpu-sample-s", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--precision", default="split_tc", choices=["split_tc", "fp64"],
-                    help="3-D stress products of the timed arm (a plain FP64 arm is always timed beside split_tc)")
+                    help="3-D stress products of the timed arm")
+    ap.add_argument("--plain", default="on", choices=["on", "off"],
+                    help="also time the plain FP64 arm beside split_tc (and report the rsl error between them)")
     return ap.parse_args()
 
 
@@ -330,7 +332,7 @@ def main():
         ice_dev[s] = torch.from_numpy(w.ice_at(s + 1))
     split = w.visc3d and args.precision == "split_tc"
     main_arm = run_arm(w, 1 if split else 0, args, ice_dev, local, dist, True)
-    plain = run_arm(w, 0, args, ice_dev, local, dist, False) if split else None
+    plain = run_arm(w, 0, args, ice_dev, local, dist, False) if split and args.plain == "on" else None
     if rank != 0:
         if dist:
             dist.destroy_process_group()

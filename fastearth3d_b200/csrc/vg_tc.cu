@@ -48,7 +48,8 @@ constexpr int A_WORDS = TM * KC;  // one split term of the A chunk (32-bit words
 constexpr int B_WORDS = TN * KC;
 constexpr int STAGE_WORDS = 2 * A_WORDS + 2 * B_WORDS;
 constexpr int TMEM_COLS = 256;
-constexpr size_t SMEM_BYTES = (size_t)NSTAGE * STAGE_WORDS * 4 + 1024 + 256 + 4 * TM * 8;
+constexpr int MAX_L = 511;  // synthesis slot table in shared memory: lmax + 1 entries
+constexpr size_t SMEM_BYTES = (size_t)NSTAGE * STAGE_WORDS * 4 + 1024 + 256 + 4 * TM * 8 + (MAX_L + 1) * 4;
 constexpr unsigned long long WAIT_NS = 2000000000ull;  // 2 s bound on any wait
 
 enum { ST_SYNTH = 0, ST_INV = 1, ST_FWD = 2, ST_ANA = 3 };
@@ -220,71 +221,149 @@ __device__ __forceinline__ Cta cta_info(const Args& A) {
   return c;
 }
 
-// Four consecutive K values of one A row (raw FP32, split later). `sum`
-// accumulates the CUDA-core side terms (DFT column i = 0 / order m = 0).
+// Loader context of one thread: the tile row it stages and that row's
+// constant base address (computed once per CTA).
+struct RowCtx {
+  bool live;
+  const float* base;
+  int p;
+  double is_j;  // 1 / sin(theta_j) for the inverse stage's p = 2 rows
+};
+
 template <int STAGE>
-__device__ __forceinline__ float4 load_a(const Args& A, const Cta& c, int sub, int r, int k0, double& sum) {
-  float v[4] = {0.f, 0.f, 0.f, 0.f};
+__device__ __forceinline__ RowCtx row_ctx(const Args& A, const Cta& c, int r) {
+  RowCtx rc;
   const int row = c.row0 + r;
-  if (r < c.rows) {
-    if (STAGE == ST_SYNTH) {
-      // X[slot(l, m)][chan_p][n], l = m + par + 2 kk
-      const int m = c.batch_m;
-      const int chan = (c.p == 0) ? 0 : (c.p <= 2 ? 1 : (c.p == 3 ? 2 : 3));
+  rc.live = r < c.rows;
+  rc.p = 0;
+  rc.is_j = 0.0;
+  if (STAGE == ST_SYNTH) {
+    const int chan = (c.p == 0) ? 0 : (c.p <= 2 ? 1 : (c.p == 3 ? 2 : 3));
+    rc.base = A.X + (size_t)chan * A.NC + row;  // + slot * 4 NC
+  } else if (STAGE == ST_INV) {
+    rc.p = row / A.F;
+    const int f = row % A.F;
+    rc.base = A.S + ((size_t)c.j * 6 + rc.p) * A.NC + 2 * f;  // + m nlat 6 NC
+    rc.is_j = A.invsin[c.j];
+  } else if (STAGE == ST_FWD) {
+    rc.base = A.Gs + (size_t)c.j * 2 * A.half * A.NCOL + row;  // + (sub half + i) NCOL
+  } else {
+    rc.base = A.S + (size_t)c.batch_m * A.nlat * 6 * A.NC + (size_t)c.p * A.NC + row;  // + j 6 NC
+  }
+  if (!rc.live) rc.base = nullptr;
+  return rc;
+}
+
+// raw values of one quad (four consecutive K of one row; the analysis also
+// holds the mirrored latitude's four values)
+struct Quad {
+  float v[8];
+};
+
+// Issue the global loads of one quad (zeros outside the valid K range).
+template <int STAGE>
+__device__ __forceinline__ void fetch(const Args& A, const Cta& c, const RowCtx& rc, const int* slot_sm, int sub,
+                                      int k0, Quad& Q) {
 #pragma unroll
-      for (int q = 0; q < 4; ++q) {
-        const int l = m + sub + 2 * (k0 + q);
-        if (l <= A.L) v[q] = A.X[((size_t)slot_row(A.kbeg, l, m, A.nk) * 4 + chan) * A.NC + row];
+  for (int i = 0; i < 8; ++i) Q.v[i] = 0.f;
+  if (!rc.live) return;
+  if (STAGE == ST_SYNTH) {
+    // X[slot(l, m)][chan_p][n], l = m + par + 2 kk
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const int dl = sub + 2 * (k0 + q);
+      if (c.batch_m + dl <= A.L) Q.v[q] = rc.base[(size_t)slot_sm[dl] * 4 * A.NC];
+    }
+  } else if (STAGE == ST_INV) {
+    // (m, re), (m, im), (m + 2, re), (m + 2, im), m = (sub ? 1 : 2) + 2 (k / 2)
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const int m = (sub ? 1 : 2) + 2 * ((k0 >> 1) + h);
+      if (m <= A.L) {
+        const float2 z = *reinterpret_cast<const float2*>(rc.base + (size_t)m * A.nlat * 6 * A.NC);
+        Q.v[2 * h] = z.x;
+        Q.v[2 * h + 1] = z.y;
       }
-    } else if (STAGE == ST_INV) {
-      // (m, re), (m, im), (m + 2, re), (m + 2, im) of the row's complex order-m
-      // coefficient z, m = (sub ? 1 : 2) + 2 (k / 2); p = 2 and p = 5 enter as i z
-      // (p = 2 also times m / sin theta)
-      const int p = row / A.F, f = row % A.F;
+    }
+  } else if (STAGE == ST_FWD) {
+    // s_i (sub 0) or d_i (sub 1), i = k
 #pragma unroll
-      for (int h = 0; h < 2; ++h) {
-        const int m = (sub ? 1 : 2) + 2 * ((k0 >> 1) + h);
-        if (m <= A.L) {
-          const float2 z = *reinterpret_cast<const float2*>(A.S + (((size_t)m * A.nlat + c.j) * 6 + p) * A.NC + 2 * f);
-          float re = z.x, im = z.y;
-          if (p == 2) {
-            const float a = (float)((double)m * A.invsin[c.j]);
-            re = -a * z.y;
-            im = a * z.x;
-          } else if (p == 5) {
-            re = -z.y;
-            im = z.x;
-          }
-          v[2 * h] = re;
-          v[2 * h + 1] = im;
-          sum += 2.0 * (double)re;  // column i = 0: sum_m 2 Re z_m
-        }
-      }
-    } else if (STAGE == ST_FWD) {
-      // s_i (sub 0) or d_i (sub 1), i = k
-      const float* g = A.Gs + ((size_t)c.j * 2 + sub) * A.half * A.NCOL + row;
+    for (int q = 0; q < 4; ++q) {
+      const int i = k0 + q;
+      if (i < A.half) Q.v[q] = rc.base[((size_t)sub * A.half + i) * A.NCOL];
+    }
+  } else {
+    // analysis: R_j and R_mirror over the northern rows j = k
 #pragma unroll
-      for (int q = 0; q < 4; ++q) {
-        const int i = k0 + q;
-        if (i < A.half) v[q] = g[(size_t)i * A.NCOL];
-        if (sub == 0) sum += (double)v[q];  // order m = 0: sum_i s_i
-      }
-    } else {
-      // analysis: R_j +- sigma R_mirror over the northern rows j = k
-      const int m = c.batch_m;
-      const float sg = table_sigma(c.p) * (sub ? -1.0f : 1.0f);
-#pragma unroll
-      for (int q = 0; q < 4; ++q) {
-        const int j = k0 + q;
-        if (j < A.nh) {
-          const int jm = A.nlat - 1 - j;
-          const float a = A.S[(((size_t)m * A.nlat + j) * 6 + c.p) * A.NC + row];
-          v[q] = (jm == j) ? a : a + sg * A.S[(((size_t)m * A.nlat + jm) * 6 + c.p) * A.NC + row];
-        }
+    for (int q = 0; q < 4; ++q) {
+      const int j = k0 + q, jm = A.nlat - 1 - j;
+      if (j < A.nh) {
+        Q.v[q] = rc.base[(size_t)j * 6 * A.NC];
+        if (jm != j) Q.v[4 + q] = rc.base[(size_t)jm * 6 * A.NC];
       }
     }
   }
-  return make_float4(v[0], v[1], v[2], v[3]);
+}
+
+// The quad's four A values from its raw loads. `sum` accumulates the CUDA-core
+// side terms (inverse: column i = 0, sum_m 2 Re z_m; forward: order 0, sum_i s_i).
+template <int STAGE>
+__device__ __forceinline__ float4 finish(const Cta& c, const RowCtx& rc, int sub, int k0, const Quad& Q,
+                                         double& sum) {
+  if (STAGE == ST_INV) {
+    float v[4];
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      float re = Q.v[2 * h], im = Q.v[2 * h + 1];
+      if (rc.p == 2) {  // i (m / sin theta) z
+        const int m = (sub ? 1 : 2) + 2 * ((k0 >> 1) + h);
+        const float a = (float)((double)m * rc.is_j);
+        const float t = re;
+        re = -a * im;
+        im = a * t;
+      } else if (rc.p == 5) {  // i z
+        const float t = re;
+        re = -im;
+        im = t;
+      }
+      v[2 * h] = re;
+      v[2 * h + 1] = im;
+      sum += 2.0 * (double)re;
+    }
+    return make_float4(v[0], v[1], v[2], v[3]);
+  }
+  if (STAGE == ST_FWD) {
+    if (sub == 0) sum += (double)Q.v[0] + (double)Q.v[1] + (double)Q.v[2] + (double)Q.v[3];
+    return make_float4(Q.v[0], Q.v[1], Q.v[2], Q.v[3]);
+  }
+  if (STAGE == ST_ANA) {  // E: R_j + sigma R_mirror; O: R_j - sigma R_mirror
+    const float sg = table_sigma(c.p) * (sub ? -1.0f : 1.0f);
+    return make_float4(Q.v[0] + sg * Q.v[4], Q.v[1] + sg * Q.v[5], Q.v[2] + sg * Q.v[6], Q.v[3] + sg * Q.v[7]);
+  }
+  return make_float4(Q.v[0], Q.v[1], Q.v[2], Q.v[3]);
+}
+
+__device__ __forceinline__ void cp16(void* dst, const void* src) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(saddr(dst)), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_wait() {
+  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
+__device__ __forceinline__ void store_split(uint32_t* hi_plane, uint32_t* lo_plane, size_t at, float4 v) {
+  uint4 hi, lo;
+  hi.x = to_tf32(v.x);
+  lo.x = to_tf32(v.x - __uint_as_float(hi.x));
+  hi.y = to_tf32(v.y);
+  lo.y = to_tf32(v.y - __uint_as_float(hi.y));
+  hi.z = to_tf32(v.z);
+  lo.z = to_tf32(v.z - __uint_as_float(hi.z));
+  hi.w = to_tf32(v.w);
+  lo.w = to_tf32(v.w - __uint_as_float(hi.w));
+  *reinterpret_cast<uint4*>(hi_plane + at) = hi;
+  *reinterpret_cast<uint4*>(lo_plane + at) = lo;
 }
 
 // ------------------------------------------------------------------ kernel
@@ -298,6 +377,7 @@ __global__ void __launch_bounds__(NTHR, 1) k_tc_stage(Args A) {
   uint32_t* tslot = (uint32_t*)(bars + NSTAGE + 1);
   volatile int* abort_flag = (volatile int*)(tslot + 1);
   double* rsum = (double*)(sm + (size_t)NSTAGE * STAGE_WORDS * 4 + 256);  // [2 subs][2 halves][TM]
+  int* slot_sm = (int*)(rsum + 4 * TM);                                     // synthesis: slot(m + dl, m)
 
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const Cta c = cta_info<STAGE>(A);
@@ -310,6 +390,8 @@ __global__ void __launch_bounds__(NTHR, 1) k_tc_stage(Args A) {
   }
   if (warp == 0) tmem_alloc(tslot, TMEM_COLS);
   for (int i = tid; i < 4 * TM; i += NTHR) rsum[i] = 0.0;
+  if (STAGE == ST_SYNTH)
+    for (int dl = tid; dl <= A.L - c.batch_m; dl += NTHR) slot_sm[dl] = slot_row(A.kbeg, c.batch_m + dl, c.batch_m, A.nk);
   tc_fence_before();
   __syncthreads();
   tc_fence_after();
@@ -318,54 +400,74 @@ __global__ void __launch_bounds__(NTHR, 1) k_tc_stage(Args A) {
   const int nch0 = c.sub[0].kpad / KC, nch1 = c.sub[1].kpad / KC, nch = nch0 + nch1;
   // loader mapping: thread serves row r = tid % TM, quads q = tid / TM + 2 * qq
   const int lr = tid % TM, lh = tid / TM;
-  double sums[2] = {0.0, 0.0};
+  const RowCtx rc = row_ctx<STAGE>(A, c, lr);
+  double sum0 = 0.0, sum1 = 0.0;  // loader side sums of the two sub-GEMMs
+  constexpr int QPT = (TM * KC / 4) / NTHR;  // quads per thread per chunk
+  Quad cur[QPT], nxt[QPT];
+  // B chunk of image `I` (chunk kc) into stage buffer `b`, 16-byte cp.async
+  auto copy_b = [&](int b, const ImgInfo& I, int kc) {
+    uint32_t* Bhi = stage_base + (size_t)b * STAGE_WORDS + 2 * A_WORDS;
+    uint32_t* Blo = Bhi + B_WORDS;
+    const int nvec = I.npad * (KC / 4);
+    const float* src_hi = A.img + I.off + (size_t)kc * KC * I.npad;
+    const float* src_lo = src_hi + (size_t)I.kpad * I.npad;
+    for (int t = tid; t < nvec; t += NTHR) {
+      cp16(Bhi + 4 * t, src_hi + 4 * t);
+      cp16(Blo + 4 * t, src_lo + 4 * t);
+    }
+    cp_commit();
+  };
+  auto fetch_chunk = [&](int ch, Quad* Q) {
+    const int sub = ch < nch0 ? 0 : 1, kc = sub ? ch - nch0 : ch;
+#pragma unroll
+    for (int qq = 0; qq < QPT; ++qq) fetch<STAGE>(A, c, rc, slot_sm, sub, kc * KC + 4 * (lh + 2 * qq), Q[qq]);
+  };
+  if (nch > 0) {
+    copy_b(0, c.sub[0].kpad > 0 ? c.sub[0] : c.sub[1], 0);
+    fetch_chunk(0, cur);
+  }
   int issued = 0;
   for (int ch = 0; ch < nch; ++ch) {
     const int buf = ch % NSTAGE;
     const int sub = ch < nch0 ? 0 : 1, kc = sub ? ch - nch0 : ch;
     const ImgInfo& I = c.sub[sub];
-    if (ch >= NSTAGE) {
-      if (!mbar_wait(&bars[buf], (uint32_t)((ch / NSTAGE - 1) & 1))) {
+    const bool more = ch + 1 < nch;
+    if (more) {
+      // stage buffer of chunk ch + 1 was last read by the MMAs of chunk ch + 1 - NSTAGE
+      const int nb = (ch + 1) % NSTAGE;
+      if (ch + 1 >= NSTAGE && !mbar_wait(&bars[nb], (uint32_t)(((ch + 1) / NSTAGE - 1) & 1))) {
         *abort_flag = 1;
         atomicOr(A.status, 1ull << STAGE);
       }
+      const int sub1 = (ch + 1) < nch0 ? 0 : 1, kc1 = sub1 ? ch + 1 - nch0 : ch + 1;
+      copy_b(nb, c.sub[sub1], kc1);
+      fetch_chunk(ch + 1, nxt);
     }
+    // A of chunk ch: finish the loads issued one chunk earlier, split, store
     uint32_t* Ahi = stage_base + (size_t)buf * STAGE_WORDS;
     uint32_t* Alo = Ahi + A_WORDS;
-    uint32_t* Bhi = Alo + A_WORDS;
-    uint32_t* Blo = Bhi + B_WORDS;
-    // A: raw values -> tf32 hi/lo, 16-byte rows of the canonical layout
 #pragma unroll
-    for (int qq = 0; qq < (TM * KC / 4) / NTHR; ++qq) {
+    for (int qq = 0; qq < QPT; ++qq) {
       const int q = lh + 2 * qq;
-      const float4 v = load_a<STAGE>(A, c, sub, lr, kc * KC + 4 * q, sums[sub]);
-      uint4 hi, lo;
-      hi.x = to_tf32(v.x);
-      lo.x = to_tf32(v.x - __uint_as_float(hi.x));
-      hi.y = to_tf32(v.y);
-      lo.y = to_tf32(v.y - __uint_as_float(hi.y));
-      hi.z = to_tf32(v.z);
-      lo.z = to_tf32(v.z - __uint_as_float(hi.z));
-      hi.w = to_tf32(v.w);
-      lo.w = to_tf32(v.w - __uint_as_float(hi.w));
-      *reinterpret_cast<uint4*>(Ahi + ((size_t)q * TM + lr) * 4) = hi;
-      *reinterpret_cast<uint4*>(Alo + ((size_t)q * TM + lr) * 4) = lo;
+      double part = 0.0;
+      const float4 v = finish<STAGE>(c, rc, sub, kc * KC + 4 * q, cur[qq], part);
+      if (sub)
+        sum1 += part;
+      else
+        sum0 += part;
+      store_split(Ahi, Alo, ((size_t)q * TM + lr) * 4, v);
     }
-    // B: straight copy of the pre-split image chunk
-    {
-      const int nvec = I.npad * (KC / 4);
-      const uint4* src_hi = reinterpret_cast<const uint4*>(A.img + I.off + (size_t)kc * KC * I.npad);
-      const uint4* src_lo = reinterpret_cast<const uint4*>(A.img + I.off + (size_t)I.kpad * I.npad + (size_t)kc * KC * I.npad);
-      for (int t = tid; t < nvec; t += NTHR) {
-        reinterpret_cast<uint4*>(Bhi)[t] = __ldg(src_hi + t);
-        reinterpret_cast<uint4*>(Blo)[t] = __ldg(src_lo + t);
-      }
-    }
+    if (more)
+      cp_wait<1>();
+    else
+      cp_wait<0>();
     fence_async_smem();
     __syncthreads();
     if (*abort_flag) break;
     if (tid == 0) {
       tc_fence_after();
+      uint32_t* Bhi = Alo + A_WORDS;
+      uint32_t* Blo = Bhi + B_WORDS;
       const uint32_t idesc = idesc_tf32(TM, I.npad);
       const uint32_t d = tmem + (uint32_t)(sub * TN);
 #pragma unroll
@@ -382,7 +484,12 @@ __global__ void __launch_bounds__(NTHR, 1) k_tc_stage(Args A) {
       mma_commit(&bars[buf]);
     }
     ++issued;
+    if (more) {
+#pragma unroll
+      for (int qq = 0; qq < QPT; ++qq) cur[qq] = nxt[qq];
+    }
   }
+  cp_wait<0>();
   // drain: one more commit tracks every MMA this thread issued
   bool ok = (*abort_flag == 0);
   if (tid == 0 && issued > 0) mma_commit(&bars[NSTAGE]);
@@ -391,8 +498,8 @@ __global__ void __launch_bounds__(NTHR, 1) k_tc_stage(Args A) {
     atomicOr(A.status, 1ull << (8 + STAGE));
   }
   // per-row side sums of the two loader threads
-  rsum[(0 * 2 + lh) * TM + lr] = sums[0];
-  rsum[(1 * 2 + lh) * TM + lr] = sums[1];
+  rsum[(0 * 2 + lh) * TM + lr] = sum0;
+  rsum[(1 * 2 + lh) * TM + lr] = sum1;
   __syncthreads();
   tc_fence_after();
 
@@ -581,6 +688,7 @@ void visc3d_tc_enable(vg_handle* h) {
   cudaStream_t s = h->stream;
   const int L = G.lmax, nlat = G.nlat, nphi = G.nphi, half = nphi / 2;
   if (G.mmax != L) throw Error("vg_enable_visc3d: the tensor-core path needs mmax = lmax");
+  if (L > tc::MAX_L) throw Error("vg_enable_visc3d: the tensor-core path supports lmax <= 511");
   const int nh = (nlat + 1) / 2;
   const int F = 3 * h->ne3d, NC = 2 * F, NCOL = 6 * F;
   auto* P = new TcPlan();
