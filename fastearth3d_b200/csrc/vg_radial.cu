@@ -358,7 +358,7 @@ __global__ void __launch_bounds__(128) k_drift_solve(DriftArgs A) {
 
 // Degree-1 drift (slots k = 0, 1; 4 right-hand sides): x = G1 b, then the
 // CM-frame projection with the stored null mode (src/vilma_response.f90:770-779).
-__global__ void __launch_bounds__(256) k_drift_deg1(DriftArgs A) {
+__global__ void __launch_bounds__(512) k_drift_deg1(DriftArgs A) {
   extern __shared__ double sh[];
   const int nr = A.nr, ncol = 2 * nr, nrow = 2 * nr + 1;
   const size_t nk = A.nk;
@@ -374,13 +374,33 @@ __global__ void __launch_bounds__(256) k_drift_deg1(DriftArgs A) {
     f[t] = s_act[kk] ? A.bh[((size_t)ri * 2 * nr + c) * nk + kk] : 0.0;
   }
   __syncthreads();
-  for (int t = threadIdx.x; t < 4 * nrow; t += blockDim.x) {
-    int q = t / nrow, r = t % nrow;
-    const double* G = A.G1 + (size_t)r * ncol;
-    const double* fq = f + q * ncol;
-    double acc = 0.0;
-    for (int c = 0; c < ncol; ++c) acc += __ldg(&G[c]) * fq[c];
-    x[q * nrow + r] = acc;
+  // x = G1 f: a warp per row, lanes over the columns (coalesced rows of G1),
+  // the four right-hand sides at once
+  {
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    for (int r = wid; r < nrow; r += nw) {
+      const double* G = A.G1 + (size_t)r * ncol;
+      double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
+      for (int c = lane; c < ncol; c += 32) {
+        const double g = __ldg(&G[c]);
+        a0 += g * f[c];
+        a1 += g * f[ncol + c];
+        a2 += g * f[2 * ncol + c];
+        a3 += g * f[3 * ncol + c];
+      }
+      for (int o = 16; o > 0; o >>= 1) {
+        a0 += __shfl_xor_sync(0xffffffffu, a0, o);
+        a1 += __shfl_xor_sync(0xffffffffu, a1, o);
+        a2 += __shfl_xor_sync(0xffffffffu, a2, o);
+        a3 += __shfl_xor_sync(0xffffffffu, a3, o);
+      }
+      if (lane == 0) {
+        x[r] = a0;
+        x[nrow + r] = a1;
+        x[2 * nrow + r] = a2;
+        x[3 * nrow + r] = a3;
+      }
+    }
   }
   __syncthreads();
   const int fs = 4 * (nr - 1) + 2;
@@ -460,7 +480,7 @@ void launch_drift(vg_handle* h) {
   ++h->n_launch;
   VG_CUDA(cudaGetLastError());
   size_t shm = (size_t)(4 * 2 * h->nr + 4 * (2 * h->nr + 1)) * sizeof(double);
-  k_drift_deg1<<<1, 256, shm, h->stream>>>(A);
+  k_drift_deg1<<<1, 512, shm, h->stream>>>(A);
   ++h->n_launch;
   VG_CUDA(cudaGetLastError());
 }

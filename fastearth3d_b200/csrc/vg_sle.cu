@@ -68,22 +68,38 @@ __global__ void k_pass_setup(int nphi, const double* __restrict__ ice, const dou
   }
 }
 
-// surface integral of a row-sum vector: sum_j w_j row_j * 2 pi / nphi (src/vilma_sht.f90:184-202)
-__device__ __forceinline__ double integrate_rows(const double* row, const double* w, int nlat, double dlon) {
+// Surface integral of a row-sum vector, sum_j w_j row_j 2 pi / nphi
+// (src/vilma_sht.f90:184-202), summed in row order like the reference. The
+// finalizer kernels run one block: every thread stages a slice of the terms
+// in shared memory (one coalesced pass), then thread 0 adds them in order.
+// The result is valid in thread 0.
+constexpr int FIN_THREADS = 128, FIN_SEG = 1024;
+__device__ double integrate_rows(const double* row, const double* w, int nlat, double dlon) {
+  __shared__ double term[FIN_SEG];
   double total = 0.0;
-  for (int j = 0; j < nlat; ++j) total += w[j] * row[j] * dlon;
+  for (int j0 = 0; j0 < nlat; j0 += FIN_SEG) {
+    const int n = min(FIN_SEG, nlat - j0);
+    __syncthreads();
+    for (int j = threadIdx.x; j < n; j += blockDim.x) term[j] = w[j0 + j] * row[j0 + j] * dlon;
+    __syncthreads();
+    if (threadIdx.x == 0)
+      for (int j = 0; j < n; ++j) total += term[j];
+  }
   return total;
 }
 
 __global__ void k_finalize_C(SleScalars* sc, const double* __restrict__ rowpart, const double* __restrict__ w,
                              int nlat, double dlon) {
-  if (threadIdx.x == 0) sc->C_int = integrate_rows(rowpart + RP_C * nlat, w, nlat, dlon);
+  const double c = integrate_rows(rowpart + RP_C * nlat, w, nlat, dlon);
+  if (threadIdx.x == 0) sc->C_int = c;
 }
 __global__ void k_finalize_pass(SleScalars* sc, const double* __restrict__ rowpart, const double* __restrict__ w,
                                 int nlat, double dlon, int subgrid) {
+  const double d = integrate_rows(rowpart + RP_DIG * nlat, w, nlat, dlon);
+  const double z = subgrid ? integrate_rows(rowpart + RP_ZETA * nlat, w, nlat, dlon) : 0.0;
   if (threadIdx.x == 0) {
-    sc->ice_int = -(RHO_ICE / RHO_WATER) * integrate_rows(rowpart + RP_DIG * nlat, w, nlat, dlon);
-    sc->zeta_int = subgrid ? integrate_rows(rowpart + RP_ZETA * nlat, w, nlat, dlon) : 0.0;
+    sc->ice_int = -(RHO_ICE / RHO_WATER) * d;
+    sc->zeta_int = z;
   }
 }
 __global__ void k_wcorr(int ng, int subgrid, const double* __restrict__ topo0, const double* __restrict__ C,
@@ -140,8 +156,8 @@ __global__ void k_synth_sraw(int nphi, int nlat, int M, const double* __restrict
 
 __global__ void k_dphi(SleScalars* sc, const double* __restrict__ rowpart, const double* __restrict__ w, int nlat,
                        double dlon) {
+  const double Cs = integrate_rows(rowpart + RP_CS * nlat, w, nlat, dlon);
   if (threadIdx.x == 0) {
-    double Cs = integrate_rows(rowpart + RP_CS * nlat, w, nlat, dlon);
     sc->Cs_int = Cs;
     sc->dphi = (sc->ice_int - Cs + sc->zeta_int) / sc->C_int;
   }
@@ -169,12 +185,15 @@ __global__ void k_rsl_update(int nphi, const SleScalars* __restrict__ sc, const 
 }
 
 __global__ void k_conv(SleScalars* sc, const double* __restrict__ rowpart, int nlat) {
+  __shared__ double red[FIN_THREADS];
+  double dmax = 0.0, smax = 0.0;
+  for (int j = threadIdx.x; j < nlat; j += blockDim.x) {
+    dmax = nanmax(dmax, rowpart[RP_DMAX * nlat + j]);
+    smax = nanmax(smax, rowpart[RP_SMAX * nlat + j]);
+  }
+  dmax = block_max(dmax, red);
+  smax = block_max(smax, red);
   if (threadIdx.x == 0) {
-    double dmax = 0.0, smax = 0.0;
-    for (int j = 0; j < nlat; ++j) {
-      dmax = nanmax(dmax, rowpart[RP_DMAX * nlat + j]);
-      smax = nanmax(smax, rowpart[RP_SMAX * nlat + j]);
-    }
     sc->dmax = dmax;
     sc->smax = smax;
   }
@@ -197,11 +216,11 @@ __global__ void k_coast(int nphi, const double* __restrict__ topo0, const double
   if (threadIdx.x == 0) rowpart[RP_FLIP * nlat + j] = cnt;
 }
 __global__ void k_flips(SleScalars* sc, const double* __restrict__ rowpart, int nlat) {
-  if (threadIdx.x == 0) {
-    double t = 0.0;
-    for (int j = 0; j < nlat; ++j) t += rowpart[RP_FLIP * nlat + j];
-    sc->flips = (int)t;
-  }
+  __shared__ double red[FIN_THREADS];
+  double t = 0.0;  // integer-valued row counts: exact in any order
+  for (int j = threadIdx.x; j < nlat; j += blockDim.x) t += rowpart[RP_FLIP * nlat + j];
+  t = block_sum(t, red);
+  if (threadIdx.x == 0) sc->flips = (int)t;
 }
 
 // row sums of a * b (b may be null: sum of a), into rowpart slot
@@ -219,7 +238,8 @@ __global__ void k_rowsum(int nphi, const double* __restrict__ a, const double* _
 }
 __global__ void k_mass(SleScalars* sc, const double* __restrict__ rowpart, const double* __restrict__ w, int nlat,
                        double dlon) {
-  if (threadIdx.x == 0) sc->mass_Cs = integrate_rows(rowpart + RP_MASS * nlat, w, nlat, dlon) - sc->zeta_int;
+  const double m = integrate_rows(rowpart + RP_MASS * nlat, w, nlat, dlon);
+  if (threadIdx.x == 0) sc->mass_Cs = m - sc->zeta_int;
 }
 
 // z_bed = z_bed_eq - rsl (src/vilma_coupling.f90:428)
@@ -284,10 +304,10 @@ void sle_solve_dev(vg_handle* h, double dt, bool report_only) {
     }
     k_pass_setup<<<nlat, 128, 0, s>>>(nphi, h->d_ice_now.p, h->d_dice_now.p, h->d_C.p, h->d_C0.p, h->d_z_bed_eq.p,
                                       h->d_dig.p, rp, nlat); ++h->n_launch;
-    k_finalize_C<<<1, 32, 0, s>>>(sc, rp, G.d_wts.p, nlat, dlon); ++h->n_launch;
+    k_finalize_C<<<1, FIN_THREADS, 0, s>>>(sc, rp, G.d_wts.p, nlat, dlon); ++h->n_launch;
     read_scalars(h);
     if (h->h_sc->C_int <= 0.0) break;  // no ocean: nothing to redistribute
-    k_finalize_pass<<<1, 32, 0, s>>>(sc, rp, G.d_wts.p, nlat, dlon, p.sle_subgrid); ++h->n_launch;
+    k_finalize_pass<<<1, FIN_THREADS, 0, s>>>(sc, rp, G.d_wts.p, nlat, dlon, p.sle_subgrid); ++h->n_launch;
     k_wcorr<<<eg, eb, 0, s>>>(ng, p.sle_subgrid, h->d_z_bed_eq.p, h->d_C.p, h->d_C0.p, h->d_wcorr.p); ++h->n_launch;
     for (int ii = 1; ii <= p.sle_n_inner; ++ii) {
       PhaseScope ps(h, VG_PH_SLE);
@@ -298,9 +318,9 @@ void sle_solve_dev(vg_handle* h, double dt, bool report_only) {
       legendre_synth_dev(h, h->d_ulm.p, 2, h->d_Gs.p);
       k_synth_sraw<<<nlat, 128, 4 * M * sizeof(double), s>>>(nphi, nlat, M, h->d_Gs.p, G.d_cos.p, G.d_sin.p,
                                                              h->d_C.p, nullptr, h->d_Sraw.p, rp); ++h->n_launch;
-      k_dphi<<<1, 32, 0, s>>>(sc, rp, G.d_wts.p, nlat, dlon); ++h->n_launch;
+      k_dphi<<<1, FIN_THREADS, 0, s>>>(sc, rp, G.d_wts.p, nlat, dlon); ++h->n_launch;
       k_rsl_update<<<nlat, 128, 0, s>>>(nphi, sc, h->d_Sraw.p, h->d_C.p, h->d_rsl.p, rp, nlat); ++h->n_launch;
-      k_conv<<<1, 32, 0, s>>>(sc, rp, nlat); ++h->n_launch;
+      k_conv<<<1, FIN_THREADS, 0, s>>>(sc, rp, nlat); ++h->n_launch;
       read_scalars(h);
       h->n_inner_last = ii;
       if (h->h_sc->dmax <= p.sle_tol * std::max(h->h_sc->smax, TINY)) break;
@@ -309,7 +329,7 @@ void sle_solve_dev(vg_handle* h, double dt, bool report_only) {
     if (p.sle_fixed_ocean) break;
     k_coast<<<nlat, 128, 0, s>>>(nphi, h->d_z_bed_eq.p, h->d_rsl.p, h->d_ice_now.p, h->d_C.p, h->d_C_next.p, rp,
                                  nlat); ++h->n_launch;
-    k_flips<<<1, 32, 0, s>>>(sc, rp, nlat); ++h->n_launch;
+    k_flips<<<1, FIN_THREADS, 0, s>>>(sc, rp, nlat); ++h->n_launch;
     read_scalars(h);
     h->n_flip_last = h->h_sc->flips;
     if (h->h_sc->flips == 0) break;
@@ -323,7 +343,7 @@ void sle_solve_dev(vg_handle* h, double dt, bool report_only) {
     launch_advance_1d(h, h->d_sigma.p, dt);
   }
   k_rowsum<<<nlat, 128, 0, s>>>(nphi, h->d_C.p, h->d_rsl.p, rp + RP_MASS * nlat); ++h->n_launch;
-  k_mass<<<1, 32, 0, s>>>(sc, rp, G.d_wts.p, nlat, dlon); ++h->n_launch;
+  k_mass<<<1, FIN_THREADS, 0, s>>>(sc, rp, G.d_wts.p, nlat, dlon); ++h->n_launch;
 }
 
 // solid_earth_update without rotation; d_ice1 is the interval-end ice on the device
