@@ -69,7 +69,10 @@ typedef struct vg_params {
   int sle_fixed_ocean, sle_subgrid, sle_warm_start;
   /* rotational feedback (src/vilma_params.f90:96); not implemented: must be 0 */
   int rotation;
-  /* precision of the 3-D Legendre contractions (no reference counterpart) */
+  /* arithmetic of the 3-D stress products (no reference counterpart):
+   * VG_VISC3D_FP64 (default) or VG_VISC3D_SPLIT_TC, the Legendre and longitude
+   * contractions on the tensor cores with two-term TF32 operands and FP32
+   * accumulation (rsl within ~2e-6 of the FP64 path on the lmax-128 workload) */
   int visc3d_precision;
 } vg_params;
 
