@@ -188,4 +188,39 @@ int stepper_advance(Stepper& st, const Sht& s, Response& R, SleSolver& sle, cons
                     const double* ice0, const double* ice1, const double* ice_ref, double t0,
                     double t1, double* rsl, double* C, const double* s_rot, cplx* sigma_out);
 
+// ---------------------------------------------------------------- rotation
+// vilma_rotation.f90: two degree-2 viscoelastic channels (load, tidal) carrying
+// Maxwell memory, and the algebraic (Chandler-neglected) Liouville equation.
+struct Deg2Channel {
+  bool tidal = false;
+  int nr = 0, ne = 0, ndof = 0;
+  double Jr = 6.0, dt = 0.0;
+  RadialOp op;
+  std::vector<double> r, mu, Mk, MkPerDt;
+  double norm[4] = {0, 0, 0, 0}, sa[16] = {}, sb[16] = {}, sc[16] = {};
+  double Fe = 0.0, Ue = 0.0;
+  std::vector<double> xUn, xVn;
+  std::vector<double> Are, Aim, Bre, Bim, Cre, Cim;  // (NLAM, ne): [e][lam]
+  cplx dF = 0.0, dU = 0.0;
+  std::vector<double> dUn_re, dUn_im, dVn_re, dVn_im;
+};
+struct Rotation {
+  bool enabled = false;
+  cplx m = 0.0;
+  double time = 0.0;
+  double a = 6.371e6, g = 9.81, CminusA = 2.63e35, Omega = 7.292115e-5;
+  double k_s = 0.0, k_s_fluid = 0.0, k_s_flat = 0.0, kTe = 0.0, hTe = 0.0;
+  double dt_fe_max = 1.7976931348623157e308;
+  cplx cload = 0.0;
+  Deg2Channel load_ch, tidal_ch;
+};
+void radial_operator_tidal_rhs(const RadialOp& op, double phi_t, double* b);
+void rotation_init(Rotation& rt, const Earth& e, const Mesh& m, double dt);
+void rotation_begin_step(Rotation& rt, double dt);
+void rotation_solve_m(Rotation& rt, const Sht& s, const double* load);
+void rotation_s_rot(const Rotation& rt, const Sht& s, double* srot);
+void rotation_commit(Rotation& rt);
+void rotation_update(Rotation& rt, const Sht& s, const double* load, double dt);
+cplx inertia21(const Sht& s, const double* load, double a);
+
 }  // namespace orc

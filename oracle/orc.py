@@ -38,6 +38,9 @@ def lib():
             ("orc_enable_visc3d", [_VP, _P]),
             ("orc_update", [_VP, _P, C.c_double]),
             ("orc_get_fields", [_VP, _P, _P, _P, _P]),
+            ("orc_get_rotation", [_VP, _P, _P]),
+            ("orc_rotation_update", [_VP, _P, C.c_double]),
+            ("orc_rotation_inertia", [_VP, _P, _P]),
             ("orc_get_info", [_VP, C.POINTER(VgInfo)]),
             ("orc_response_set_dt", [_VP, C.c_double]),
             ("orc_response_begin_step", [_VP]),
@@ -149,6 +152,20 @@ class Oracle:
         sig = np.zeros(2 * self.nlm)
         self._c(lib().orc_get_fields(self.h, ptr(rsl), ptr(zb), ptr(Cf), ptr(sig)))
         return rsl, zb, Cf, sig[0::2] + 1j * sig[1::2]
+
+    def rotation(self):
+        """Polar motion m (complex) and (kTe, hTe, k_s fluid, k_s flattening)."""
+        m, love = np.zeros(2), np.zeros(4)
+        self._c(lib().orc_get_rotation(self.h, ptr(m), ptr(love)))
+        return m[0] + 1j * m[1], love
+
+    def rotation_update(self, load, dt_s):
+        self._c(lib().orc_rotation_update(self.h, ptr(np.ascontiguousarray(load, dtype=np.float64)), dt_s))
+
+    def rotation_inertia(self, load):
+        out = np.zeros(2)
+        self._c(lib().orc_rotation_inertia(self.h, ptr(np.ascontiguousarray(load, dtype=np.float64)), ptr(out)))
+        return out[0] + 1j * out[1]
 
     def state(self):
         n = 4 * self.ne * self.nk

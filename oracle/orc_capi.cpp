@@ -26,6 +26,7 @@ struct OrcHandle {
   std::vector<cplx> sigma_lm;
   double time_yr = 0.0, bsl = 0.0;
   SleResult last;
+  Rotation rot;
   std::string err;
 };
 
@@ -77,7 +78,6 @@ int orc_params_default(vg_params* p) {
 
 int orc_create(const vg_params* p, OrcHandle** out) {
   try {
-    if (p->rotation) throw std::runtime_error("rotation is not part of the oracle");
     OrcHandle* h = new OrcHandle();
     h->p = *p;
     h->earth.r_earth = p->r_earth;
@@ -109,6 +109,8 @@ int orc_create(const vg_params* p, OrcHandle** out) {
     h->st.dt_min = p->dt_min;
     h->st.dt_max = p->dt_max;
     h->sigma_lm.assign(h->sht.nlm, 0.0);
+    // rotational feedback (src/vilma_coupling.f90:310-316)
+    if (p->rotation) rotation_init(h->rot, h->earth, h->mesh, dt0);
     *out = h;
     return 0;
   } catch (const std::exception& ex) {
@@ -156,22 +158,68 @@ static void update_bsl(OrcHandle* h) {
   }
 }
 
-// vilma_coupling.f90:336-437 solid_earth_update (rotation off)
+// vilma_coupling.f90:336-437 solid_earth_update; with rotation the feedback is
+// coupled at the interval level (:399-424): s_rot from the entering polar motion
+// is held across the interval, then the polar motion is advanced under the
+// interval-end load, sub-stepped to the channels' stability ceiling.
 int orc_update(OrcHandle* h, const double* h_ice, double dt_yr) {
   const int ng = h->sht.nphi * h->sht.nlat;
   double dt = dt_yr * SEC_PER_YEAR;
   double t0 = h->time_yr * SEC_PER_YEAR, t1 = t0 + dt;
   std::vector<double> ice_new(h_ice, h_ice + ng);
+  std::vector<double> s_rot;
+  if (h->rot.enabled) {
+    rotation_begin_step(h->rot, dt);
+    s_rot.resize(ng);
+    rotation_s_rot(h->rot, h->sht, s_rot.data());
+  }
   int rc = stepper_advance(h->st, h->sht, h->R, h->sle, h->z_bed_eq.data(), h->h_ice.data(), ice_new.data(),
-                           h->h_ice_eq.data(), t0, t1, h->rsl.data(), h->C.data(), nullptr, h->sigma_lm.data());
+                           h->h_ice_eq.data(), t0, t1, h->rsl.data(), h->C.data(),
+                           h->rot.enabled ? s_rot.data() : nullptr, h->sigma_lm.data());
   if (rc) {
     h->err = "vilma_timestep: explicit guard sub-step collapsed (viscosity too stiff for FE)";
     return rc;
+  }
+  if (h->rot.enabled) {
+    std::vector<double> load(ng);
+    sht_synth(h->sht, h->sigma_lm.data(), load.data());
+    const int n_sub = std::max(1, (int)std::ceil(dt / h->rot.dt_fe_max));
+    const double dt_sub = dt / (double)n_sub;
+    for (int k = 0; k < n_sub; ++k) rotation_update(h->rot, h->sht, load.data(), dt_sub);
   }
   h->h_ice = ice_new;
   for (int i = 0; i < ng; ++i) h->z_bed[i] = h->z_bed_eq[i] - h->rsl[i];
   h->time_yr += dt_yr;
   update_bsl(h);
+  return 0;
+}
+
+// polar motion m (re, im) and the degree-2 constants kTe, hTe, k_s (fluid), k_s (flattening)
+int orc_get_rotation(OrcHandle* h, double* m, double* love) {
+  if (m) {
+    m[0] = h->rot.m.real();
+    m[1] = h->rot.m.imag();
+  }
+  if (love) {
+    love[0] = h->rot.kTe;
+    love[1] = h->rot.hTe;
+    love[2] = h->rot.k_s_fluid;
+    love[3] = h->rot.k_s_flat;
+  }
+  return h->rot.enabled ? 0 : 1;
+}
+
+// rotation_update under a held load (the standalone polar-motion step of
+// tests/test_rotation.f90) and the rigid (2,1) inertia of a load
+int orc_rotation_update(OrcHandle* h, const double* load, double dt_s) {
+  if (!h->rot.enabled) return 1;
+  rotation_update(h->rot, h->sht, load, dt_s);
+  return 0;
+}
+int orc_rotation_inertia(OrcHandle* h, const double* load, double* I21) {
+  cplx v = inertia21(h->sht, load, h->earth.r_earth);
+  I21[0] = v.real();
+  I21[1] = v.imag();
   return 0;
 }
 

@@ -471,6 +471,13 @@ void radial_operator_load_rhs(const RadialOp& op, double sigma, double* b) {
   b[idx_f(op.nr - 1)] = -op.r_earth * op.r_earth * sigma;
 }
 
+// vilma_radial_fe.f90:627-645 radial_operator_tidal_rhs: external degree-j
+// potential phi_t couples to F(a) like the load's own potential, no traction on U(a)
+void radial_operator_tidal_rhs(const RadialOp& op, double phi_t, double* b) {
+  for (int i = 0; i < op.ndof; ++i) b[i] = 0.0;
+  b[idx_f(op.nr - 1)] = -op.r_earth / (4.0 * PI * GRAV_G) * (double)(2 * op.j + 1) * phi_t;
+}
+
 // vilma_radial_fe.f90:837-866
 void loading_love(const Earth& e, int j, double sigma, double Ua, double Va, double Fa, double& h,
                   double& l, double& k) {

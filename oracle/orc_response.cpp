@@ -457,3 +457,203 @@ void response_enable_lateral_visc(Response& R, const Sht& s, const double* pert)
 }
 
 }  // namespace orc
+
+// ================================================================ rotation
+// vilma_rotation.f90 (CPU restatement). JROT = 2 throughout.
+
+namespace orc {
+
+// vilma_rotation.f90:375-433 channel_init
+static void channel_init(Deg2Channel& c, const Earth& e, const Mesh& m, double dt, bool tidal) {
+  c = Deg2Channel();
+  c.tidal = tidal;
+  c.nr = m.nr;
+  c.ne = m.ne;
+  c.ndof = ndof_of(m.nr);
+  c.Jr = 6.0;
+  c.dt = dt;
+  c.r = m.r;
+  c.mu.assign(c.ne, 0.0);
+  c.MkPerDt.assign(c.ne, 0.0);
+  c.Mk.assign(c.ne, 0.0);
+  for (int k = 0; k < c.ne; ++k) {
+    const Layer& L = e.layers[m.elem_layer[k]];
+    c.mu[k] = L.mu;
+    c.MkPerDt[k] = L.eta > 0.0 ? c.mu[k] / L.eta : 0.0;
+    c.Mk[k] = c.MkPerDt[k] * dt;
+  }
+  ve_strain_constants(c.Jr, c.norm, c.sa, c.sb, c.sc);
+  radial_operator_assemble(c.op, e, m, 2);
+  std::vector<double> b(c.ndof), x(c.ndof);
+  if (tidal)
+    radial_operator_tidal_rhs(c.op, 1.0, b.data());
+  else
+    radial_operator_load_rhs(c.op, 1.0, b.data());
+  radial_operator_solve_vec(c.op, b.data(), x.data(), nullptr);
+  c.Fe = x[idx_f(c.nr - 1)];
+  c.Ue = x[idx_u(c.nr - 1)];
+  c.xUn.resize(c.nr);
+  c.xVn.resize(c.nr);
+  for (int k = 0; k < c.nr; ++k) {
+    c.xUn[k] = x[idx_u(k)];
+    c.xVn[k] = x[idx_v(k)];
+  }
+  for (auto* v : {&c.Are, &c.Aim, &c.Bre, &c.Bim, &c.Cre, &c.Cim}) v->assign((size_t)NLAM * c.ne, 0.0);
+  for (auto* v : {&c.dUn_re, &c.dUn_im, &c.dVn_re, &c.dVn_im}) v->assign(c.nr, 0.0);
+  c.dF = 0.0;
+  c.dU = 0.0;
+}
+
+// vilma_rotation.f90:435-440
+static void channel_set_dt(Deg2Channel& c, double dt) {
+  c.dt = dt;
+  for (int k = 0; k < c.ne; ++k) c.Mk[k] = c.MkPerDt[k] * dt;
+}
+
+// vilma_rotation.f90:442-463 channel_begin: drift frozen from the entering memory
+static void channel_begin(Deg2Channel& c) {
+  std::vector<double> fre(c.ndof, 0.0), fim(c.ndof, 0.0), xre(c.ndof), xim(c.ndof);
+  dissipative_rhs(c.ne, c.r.data(), c.sa, c.sb, c.sc, c.norm, c.Are.data(), c.Bre.data(), c.Cre.data(), fre.data());
+  dissipative_rhs(c.ne, c.r.data(), c.sa, c.sb, c.sc, c.norm, c.Aim.data(), c.Bim.data(), c.Cim.data(), fim.data());
+  radial_operator_solve_vec(c.op, fre.data(), xre.data(), nullptr);
+  radial_operator_solve_vec(c.op, fim.data(), xim.data(), nullptr);
+  c.dF = cplx(xre[idx_f(c.nr - 1)], xim[idx_f(c.nr - 1)]);
+  c.dU = cplx(xre[idx_u(c.nr - 1)], xim[idx_u(c.nr - 1)]);
+  for (int k = 0; k < c.nr; ++k) {
+    c.dUn_re[k] = xre[idx_u(k)];
+    c.dUn_im[k] = xim[idx_u(k)];
+    c.dVn_re[k] = xre[idx_v(k)];
+    c.dVn_im[k] = xim[idx_v(k)];
+  }
+}
+
+// vilma_rotation.f90:465-485 channel_commit: forward-Euler memory with the converged forcing
+static void channel_commit(Deg2Channel& c, cplx coeff) {
+  std::vector<double> Ure(c.nr), Uim(c.nr), Vre(c.nr), Vim(c.nr);
+  const double cr = coeff.real(), ci = coeff.imag();
+  for (int k = 0; k < c.nr; ++k) {
+    Ure[k] = cr * c.xUn[k] + c.dUn_re[k];
+    Uim[k] = ci * c.xUn[k] + c.dUn_im[k];
+    Vre[k] = cr * c.xVn[k] + c.dVn_re[k];
+    Vim[k] = ci * c.xVn[k] + c.dVn_im[k];
+  }
+  advance_memory_fe(c.ne, c.mu.data(), c.Mk.data(), Ure.data(), Vre.data(), c.Jr, c.Are.data(), c.Bre.data(),
+                    c.Cre.data(), nullptr);
+  advance_memory_fe(c.ne, c.mu.data(), c.Mk.data(), Uim.data(), Vim.data(), c.Jr, c.Aim.data(), c.Bim.data(),
+                    c.Cim.data(), nullptr);
+}
+
+// vilma_rotation.f90:342-371 fluid_tidal_k: elastic tidal solve with every Maxwell
+// layer fluidised (elastic lithosphere and fluid core unchanged)
+static double fluid_tidal_k(const Earth& e, const Mesh& m) {
+  Earth ef = e;
+  for (auto& L : ef.layers)
+    if (L.rheology == RHEOL_MAXWELL) {
+      L.mu = 0.0;
+      L.rheology = RHEOL_FLUID;
+    }
+  RadialOp op;
+  radial_operator_assemble(op, ef, m, 2);
+  std::vector<double> b(op.ndof), x(op.ndof);
+  radial_operator_tidal_rhs(op, 1.0, b.data());
+  radial_operator_solve_vec(op, b.data(), x.data(), nullptr);
+  return -x[idx_f(m.nr - 1)] / 1.0 - 1.0;  // tidal_love, vilma_radial_fe.f90:868-893
+}
+
+// vilma_rotation.f90:114-152 rotation_init
+void rotation_init(Rotation& rt, const Earth& e, const Mesh& m, double dt) {
+  rt = Rotation();
+  rt.a = e.r_earth;
+  rt.g = earth_gravity_at(e, e.r_earth);
+  channel_init(rt.load_ch, e, m, dt, false);
+  channel_init(rt.tidal_ch, e, m, dt, true);
+  rt.kTe = -rt.tidal_ch.Fe - 1.0;
+  rt.hTe = earth_gravity_at(e, e.r_earth) * rt.tidal_ch.Ue;
+  rt.k_s_fluid = fluid_tidal_k(e, m);
+  rt.k_s_flat = 3.0 * GRAV_G * rt.CminusA / (std::pow(rt.a, 5) * rt.Omega * rt.Omega);
+  double mx = 0.0;
+  for (double v : rt.load_ch.MkPerDt) mx = std::max(mx, v);
+  if (mx > 0.0) rt.dt_fe_max = 1.0 / mx;
+  rt.k_s = rt.k_s_fluid;
+  rt.m = 0.0;
+  rt.time = 0.0;
+  rt.enabled = true;
+}
+
+// vilma_rotation.f90:154-168
+void rotation_begin_step(Rotation& rt, double dt) {
+  if (!rt.enabled) return;
+  if (dt != rt.load_ch.dt) {
+    channel_set_dt(rt.load_ch, dt);
+    channel_set_dt(rt.tidal_ch, dt);
+  }
+  channel_begin(rt.load_ch);
+  channel_begin(rt.tidal_ch);
+}
+
+// vilma_rotation.f90:315-338 inertia21: I13 + i I23 of a surface load by Gauss-grid quadrature
+cplx inertia21(const Sht& s, const double* load, double a) {
+  const int np = s.nphi, nl = s.nlat;
+  std::vector<double> w13((size_t)np * nl), w23((size_t)np * nl);
+  for (int j = 0; j < nl; ++j) {
+    const double st = std::sin(s.colat[j]), ct = std::cos(s.colat[j]), sc2 = st * ct;
+    for (int i = 0; i < np; ++i) {
+      const double lon = 2.0 * PI * (double)i / (double)np;
+      w13[(size_t)j * np + i] = load[(size_t)j * np + i] * sc2 * std::cos(lon);
+      w23[(size_t)j * np + i] = load[(size_t)j * np + i] * sc2 * std::sin(lon);
+    }
+  }
+  const double a4 = std::pow(a, 4);
+  return cplx(-a4 * sht_surface_integral(s, w13.data()), -a4 * sht_surface_integral(s, w23.data()));
+}
+
+// vilma_rotation.f90:170-190 rotation_solve_m
+void rotation_solve_m(Rotation& rt, const Sht& s, const double* load) {
+  if (!rt.enabled) return;
+  const cplx Irig = inertia21(s, load, rt.a);
+  const double scl = 5.0 / (4.0 * PI * GRAV_G * rt.a);
+  rt.cload = Irig * scl;
+  const cplx Itot = -(rt.load_ch.Fe * rt.cload + rt.load_ch.dF);
+  const cplx psiL = Itot / rt.CminusA;
+  rt.m = (psiL - rt.tidal_ch.dF / rt.k_s) / (1.0 - rt.kTe / rt.k_s);
+}
+
+// vilma_rotation.f90:192-222 rotation_s_rot: s_rot = N_rot - u_rot on the Gauss grid
+void rotation_s_rot(const Rotation& rt, const Sht& s, double* srot) {
+  const int np = s.nphi, nl = s.nlat;
+  if (!rt.enabled) {
+    for (size_t i = 0; i < (size_t)np * nl; ++i) srot[i] = 0.0;
+    return;
+  }
+  const cplx cN = rt.m + (rt.kTe * rt.m - rt.tidal_ch.dF);
+  const cplx cU = rt.tidal_ch.Ue * rt.m + rt.tidal_ch.dU;
+  const double kN = rt.Omega * rt.Omega * rt.a * rt.a / rt.g;
+  const double ku = rt.Omega * rt.Omega * rt.a * rt.a;
+  for (int j = 0; j < nl; ++j) {
+    const double gam = std::sin(s.colat[j]) * std::cos(s.colat[j]);
+    for (int i = 0; i < np; ++i) {
+      const double lon = 2.0 * PI * (double)i / (double)np;
+      const double cphi = std::cos(lon), sphi = std::sin(lon);
+      srot[(size_t)j * np + i] = gam * (kN * (cN.real() * cphi + cN.imag() * sphi) -
+                                        ku * (cU.real() * cphi + cU.imag() * sphi));
+    }
+  }
+}
+
+// vilma_rotation.f90:224-233
+void rotation_commit(Rotation& rt) {
+  if (!rt.enabled) return;
+  channel_commit(rt.load_ch, rt.cload);
+  channel_commit(rt.tidal_ch, rt.m);
+  rt.time += rt.load_ch.dt;
+}
+
+// vilma_rotation.f90:235-249
+void rotation_update(Rotation& rt, const Sht& s, const double* load, double dt) {
+  if (!rt.enabled) return;
+  rotation_begin_step(rt, dt);
+  rotation_solve_m(rt, s, load);
+  rotation_commit(rt);
+}
+
+}  // namespace orc

@@ -12,6 +12,13 @@ and writes the few numbers the tests use into tests/golden/*.json:
   disc load at colatitude 0 and on the 0..20 deg profile, at t = 0, 1, 2, 5,
   10 kyr (data/benchmarks/disc_spada2011/{u,n}_disc.txt, 201 rows x 6 times).
 
+* rotation_spada2011.json: Spada-2011 Test 3/2 polar motion |m| [deg] of the
+  cap and disc Heaviside loads, Chandler wobble excluded (the quasi-static
+  column a time-domain solver targets, TABOO "Gs" values), at t = 0, 1, 2, 5,
+  10, 20 kyr, and the published rigid (2,1) geometrical factors G, from
+  data/benchmarks/rotation_spada2011/polar_motion_test3-2.txt (rows
+  `load cw t m_Vb m_Gs ...`, G in the header comment).
+
 Run in a container where the reference is mounted:
     python tests/golden/make_golden.py /root/reference
 """
@@ -51,9 +58,29 @@ def disc(ref):
             "u": u[:, :5].tolist(), "n": n[:, :1].tolist()}
 
 
+def rotation(ref):
+    import re
+
+    fn = os.path.join(ref, "data/benchmarks/rotation_spada2011/polar_motion_test3-2.txt")
+    out = {"t_kyr": [], "m_deg": {"cap": [], "disc": []}, "G": {}}
+    for line in open(fn):
+        if line.startswith("#"):
+            g = re.match(r"#\s+(cap|disc)\s*:\s*-\(([0-9.e+-]+)\s*\+\s*i\s*([0-9.e+-]+)\)", line)
+            if g:
+                out["G"][g.group(1)] = [-float(g.group(2)), -float(g.group(3))]
+            continue
+        t = line.split()
+        if len(t) >= 5 and t[0] in ("cap", "disc") and t[1] == "excl":
+            out["m_deg"][t[0]].append(float(t[4]))
+            if t[0] == "cap":
+                out["t_kyr"].append(float(t[2]))
+    return out
+
+
 if __name__ == "__main__":
     ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
     here = os.path.dirname(os.path.abspath(__file__))
     json.dump(love(ref), open(os.path.join(here, "love_M3L70V01.json"), "w"), indent=1)
     json.dump(disc(ref), open(os.path.join(here, "disc_spada2011.json"), "w"))
+    json.dump(rotation(ref), open(os.path.join(here, "rotation_spada2011.json"), "w"), indent=1)
     print("wrote golden fixtures to", here)

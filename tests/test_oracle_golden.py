@@ -14,7 +14,7 @@ import os
 import numpy as np
 import pytest
 
-from fastearth3d_b200.abi import M3L70V01, VG_RHEOL_FLUID, set_layers
+from fastearth3d_b200.abi import M3L70V01, VG_RHEOL_ELASTIC, VG_RHEOL_FLUID, VG_RHEOL_MAXWELL, set_layers
 from fastearth3d_b200 import synth
 from oracle import orc
 
@@ -215,3 +215,66 @@ def test_sle_mass_conservation():
     for step in range(1, 4):
         o.update(w.ice_at(step * 50), 100.0)
         assert o.info().worst_mass_resid < 1e-10
+
+
+def _spada_load(o, name, h):
+    """Cap (parabolic) or disc load of tests/test_rotation.f90 build_load:
+    alpha 10 deg, centroid colatitude 25 deg, longitude 75 deg, rho_ice 931."""
+    colat, _ = o.grid()
+    nphi = o.p.nphi
+    lon = 2 * np.pi * np.arange(nphi) / nphi
+    a, tc, lc = np.deg2rad(10.0), np.deg2rad(25.0), np.deg2rad(75.0)
+    cg = np.cos(tc) * np.cos(colat)[:, None] + np.sin(tc) * np.sin(colat)[:, None] * np.cos(lon[None, :] - lc)
+    inside = cg >= np.cos(a)
+    if name == "cap":
+        frac = (cg - np.cos(a)) / (1 - np.cos(a))
+        load = np.where(inside, 931.0 * h * np.sqrt(np.maximum(frac, 0.0)), 0.0)
+    else:
+        load = np.where(inside, 931.0 * h, 0.0)
+    return np.ascontiguousarray(load.reshape(-1))
+
+
+def test_rotation_tidal_love_homogeneous_sphere():
+    """Degree-2 tidal Love numbers of a homogeneous incompressible sphere
+    (Munk & MacDonald; src/vilma_radial_fe.f90:868-893): elastic
+    k = 1.5/(1+mu~), h = 2.5/(1+mu~), mu~ = 19 mu/(2 rho g a); fluid k = 3/2."""
+    a, rho, mu = 6371e3, 5511.0, 1.4e11
+    p = orc.default_params()
+    p.lmax, p.nlat, p.nphi, p.rotation = 4, 5, 10, 1
+    set_layers(p, [(0.0, a, rho, mu, 1e300, VG_RHEOL_ELASTIC)])
+    p.ne_layer[0] = 200
+    _, love = orc.Oracle(p).rotation()
+    g = 6.67430e-11 * rho * 4.0 / 3.0 * np.pi * a
+    mt = 19 * mu / (2 * rho * g * a)
+    assert abs(love[0] - 1.5 / (1 + mt)) < 1e-4 * love[0]
+    assert abs(love[1] - 2.5 / (1 + mt)) < 1e-4 * love[1]
+    set_layers(p, [(0.0, a, rho, mu, 1e21, VG_RHEOL_MAXWELL)])
+    _, love = orc.Oracle(p).rotation()
+    assert abs(love[2] - 1.5) < 1e-4
+
+
+def test_rotation_polar_motion_spada2011():
+    """Spada et al. 2011 Test 3/2 (tests/test_rotation.f90): rigid (2,1)
+    inertia of the cap and disc loads vs the published G (2 %), and the
+    quasi-static polar motion |m(t)| under a Heaviside load vs Table 14
+    (Chandler wobble excluded) at 0..20 kyr (3 %). M3-L70-V01, native mesh,
+    Gauss grid 256 x 512, dt 25 yr."""
+    g = json.load(open(os.path.join(GOLD, "rotation_spada2011.json")))
+    p = m3_params()
+    p.lmax, p.nlat, p.nphi, p.rotation = 4, 256, 512, 1
+    yr = 3.15576e7
+    p.dt_init = 25.0 * yr
+    for name, h in (("cap", 1.5e3), ("disc", 1.0e3)):
+        o = orc.Oracle(p)
+        load = _spada_load(o, name, h)
+        G = o.rotation_inertia(load) / 2.63e35
+        Gref = complex(*g["G"][name])
+        assert abs(G - Gref) <= 0.02 * abs(Gref)
+        want = dict(zip(g["t_kyr"], g["m_deg"][name]))
+        dt = 25.0 * yr
+        for step in range(801):
+            t_kyr = step * 25.0 / 1e3
+            o.rotation_update(load, dt)
+            if t_kyr in want:
+                m_deg = abs(o.rotation()[0]) * 180.0 / np.pi
+                assert abs(m_deg - want[t_kyr]) <= 0.03 * want[t_kyr], (name, t_kyr, m_deg, want[t_kyr])
