@@ -121,6 +121,7 @@ int vg_create(const vg_params* p, vg_handle** out) {
     VG_CUDA(cudaGetDeviceCount(&ndev));
     VG_CUDA(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
     vg::setup_handle(h);
+    if (h->p.rotation) vg::rotation_setup(h);
     vg::compute_mem_norm(h, 0);
     h->mem_norm = vg::read_mem_norm(h, 0);
   });
@@ -208,6 +209,25 @@ int vg_rsl_device(vg_handle* h, const double** d_rsl) {
   return guarded(h, [&] {
     need(h, d_rsl != nullptr, "vg_rsl_device: null argument");
     *d_rsl = h->d_rsl.p;
+  });
+}
+
+int vg_get_rotation(vg_handle* h, double* m, double* love) {
+  return guarded(h, [&] {
+    if (!h->rot_on) throw vg::Error("vg_get_rotation: rotational feedback is off for this handle");
+    double sc[2] = {0.0, 0.0};
+    VG_CUDA(cudaMemcpyAsync(sc, h->d_rot_sc.p + 8, sizeof(sc), cudaMemcpyDeviceToHost, h->stream));
+    VG_CUDA(cudaStreamSynchronize(h->stream));
+    if (m) {
+      m[0] = sc[0];
+      m[1] = sc[1];
+    }
+    if (love) {
+      love[0] = h->rot_kTe;
+      love[1] = h->rot_hTe;
+      love[2] = h->rot_ks_fluid;
+      love[3] = h->rot_ks_flat;
+    }
   });
 }
 

@@ -139,4 +139,29 @@ __device__ __forceinline__ double block_max(double v, double* red) {
   return r;
 }
 
+// dgbtrs-style solve with the factor of band_factor_dev (column-major band
+// storage, leading dimension ldab), right-hand side with element stride st
+__device__ __forceinline__ void band_solve_strided(const double* __restrict__ ab, int ldab, int n, int kl, int kv,
+                                                   const int* __restrict__ ipiv, double* x, size_t st) {
+#define AB(row1, col1) ab[(size_t)((col1)-1) * ldab + ((row1)-1)]
+  for (int j = 1; j <= n - 1; ++j) {
+    int lm = min(kl, n - j);
+    int l = ipiv[j - 1] + 1;
+    if (l != j) {
+      double t = x[(size_t)(l - 1) * st];
+      x[(size_t)(l - 1) * st] = x[(size_t)(j - 1) * st];
+      x[(size_t)(j - 1) * st] = t;
+    }
+    double t = x[(size_t)(j - 1) * st];
+    for (int i = 1; i <= lm; ++i) x[(size_t)(j + i - 1) * st] -= AB(kv + 1 + i, j) * t;
+  }
+  for (int j = n; j >= 1; --j) {
+    double xj = x[(size_t)(j - 1) * st] / AB(kv + 1, j);
+    x[(size_t)(j - 1) * st] = xj;
+    int lm = min(kv, j - 1);
+    for (int i = 1; i <= lm; ++i) x[(size_t)(j - i - 1) * st] -= AB(kv + 1 - i, j) * xj;
+  }
+#undef AB
+}
+
 }  // namespace vg

@@ -14,6 +14,7 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include <cmath>
 #include <cstdint>
 #include <string>
 #include <vector>
@@ -177,6 +178,20 @@ struct vg_handle {
   bool have_reference = false;
   long long n_launch = 0;  // kernels launched by the time step (all phases)
   vg::Prof prof;
+  // rotational feedback (two degree-2 channels and the polar motion)
+  bool rot_on = false;
+  double rot_kTe = 0, rot_hTe = 0, rot_ks = 0, rot_ks_fluid = 0, rot_ks_flat = 0;
+  double rot_Fe[2] = {0, 0}, rot_Ue[2] = {0, 0};  // unit responses: load, tidal channel
+  double rot_a = 0, rot_g = 0, rot_CminusA = 2.63e35, rot_Omega = 7.292115e-5, rot_dt_fe_max = HUGE_VAL;
+  vg::DArr<double> d_rot_mkdt;  // channel mu/eta per element (ne)
+  vg::DArr<double> d_rot_x;     // unit nodal responses [ch][U, V][nr]
+  vg::DArr<double> d_rot_mem;   // memory [ch][A re, A im, B re, B im, C re, C im][ne][4]
+  vg::DArr<double> d_rot_dn;    // nodal drift [ch][dUn re, dUn im, dVn re, dVn im][nr]
+  vg::DArr<double> d_rot_sc;    // scalars (see vg_rotation.cu)
+  vg::DArr<double> d_rot_f;     // channel solve work (4 x ndof)
+  vg::DArr<double> d_rot_rows;  // per-row partial inertia sums (2 x nlat)
+  vg::DArr<double> d_rot_geo;   // sin(theta)cos(theta) [nlat], cos(lon), sin(lon) [nphi each]
+  vg::DArr<double> d_srot, d_rot_load;  // grid fields
   // split-precision tensor-core plan of the 3-D advance (owned, opaque here)
   void* tc_plan = nullptr;
   void (*tc_plan_release)(void*) = nullptr;
@@ -209,6 +224,12 @@ void update_bsl(vg_handle* h);
 // 3-D (vg_visc3d.cu)
 void visc3d_enable(vg_handle* h, const double* pert_host);
 void visc3d_advance(vg_handle* h, const double* d_sigma, double dt);
+// rotational feedback (vg_rotation.cu)
+void build_fluid_deg2_band(vg_handle* h, DArr<double>& ab, DArr<double>& dr, DArr<double>& dc, DArr<int>& ipiv);
+void rotation_setup(vg_handle* h);
+void rotation_begin(vg_handle* h);
+void rotation_s_rot(vg_handle* h);
+void rotation_advance(vg_handle* h, const double* d_sigma, double dt);
 // 3-D split-precision tensor-core stages (vg_tc.cu)
 void visc3d_tc_enable(vg_handle* h);
 void visc3d_tc_buffers(vg_handle* h, float** X, float** dy);

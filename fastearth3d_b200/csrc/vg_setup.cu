@@ -477,28 +477,6 @@ __global__ void __launch_bounds__(512) k_build_deg1(ElemData ed, double* __restr
 }
 
 // Solve with one factored band system (dgbtrs order) for a column x with stride.
-__device__ __forceinline__ void band_solve_strided(const double* __restrict__ ab, int ldab, int n, int kl, int kv,
-                                                   const int* __restrict__ ipiv, double* x, size_t st) {
-#define AB(row1, col1) ab[(size_t)((col1)-1) * ldab + ((row1)-1)]
-  for (int j = 1; j <= n - 1; ++j) {
-    int lm = min(kl, n - j);
-    int l = ipiv[j - 1] + 1;
-    if (l != j) {
-      double t = x[(size_t)(l - 1) * st];
-      x[(size_t)(l - 1) * st] = x[(size_t)(j - 1) * st];
-      x[(size_t)(j - 1) * st] = t;
-    }
-    double t = x[(size_t)(j - 1) * st];
-    for (int i = 1; i <= lm; ++i) x[(size_t)(j + i - 1) * st] -= AB(kv + 1 + i, j) * t;
-  }
-  for (int j = n; j >= 1; --j) {
-    double xj = x[(size_t)(j - 1) * st] / AB(kv + 1, j);
-    x[(size_t)(j - 1) * st] = xj;
-    int lm = min(kv, j - 1);
-    for (int i = 1; i <= lm; ++i) x[(size_t)(j - i - 1) * st] -= AB(kv + 1 - i, j) * xj;
-  }
-#undef AB
-}
 
 // unit surface load (sigma = 1) response for degrees >= 2, one thread per degree
 __global__ void k_unit_load(int lmax, int nr, int n, double r_earth, double g_surf, const double* __restrict__ ab,
@@ -694,10 +672,45 @@ static void build_mesh(vg_handle* h) {
   h->r[h->nr - 1] = p.r_earth;
 }
 
+// Degree-2 band operator of the handle's earth with every Maxwell element
+// fluidised (mu = 0; elastic and fluid elements unchanged), factored like the
+// response's own bands: the relaxed tidal limit k^T_f of the rotational
+// feedback (fluid_tidal_k, src/vilma_rotation.f90:342-371). Setup only.
+void build_fluid_deg2_band(vg_handle* h, DArr<double>& ab, DArr<double>& dr, DArr<double>& dc, DArr<int>& ipiv) {
+  const vg_params& p = h->p;
+  cudaStream_t s = h->stream;
+  const int ne = h->ne, nr = h->nr, nd = h->ndof;
+  std::vector<double> mu(ne), rho(ne), Rk(ne, 0.0);
+  for (int e = 0; e < ne; ++e) {
+    int L = h->elem_layer[e];
+    mu[e] = p.rheology[L] == VG_RHEOL_MAXWELL ? 0.0 : p.mu[L];
+    rho[e] = p.rho[L];
+  }
+  for (int k = 1; k < ne; ++k) Rk[k] = Rk[k - 1] + (rho[k - 1] - rho[k]) * std::pow(h->r[k], 3);
+  DArr<double> d_mu, d_rho, d_Rk, raw, rdg;
+  DArr<int> status;
+  d_mu.upload(mu, s);
+  d_rho.upload(rho, s);
+  d_Rk.upload(Rk, s);
+  ElemData ed{h->d_r.p, d_mu.p, d_rho.p, d_Rk.p, ne, nr, nd, p.r_earth};
+  raw.alloc((size_t)13 * nd);
+  rdg.alloc(nd);
+  status.alloc(1);
+  ab.alloc((size_t)VG_LDAB * nd);
+  dr.alloc(nd);
+  dc.alloc(nd);
+  ipiv.alloc(nd);
+  k_build_band<<<1, 32, 0, s>>>(ed, 2, raw.p, ab.p, dr.p, dc.p, ipiv.p, rdg.p, status.p);
+  VG_CUDA(cudaGetLastError());
+  int st = 0;
+  status.download(&st, 1, s);
+  VG_CUDA(cudaStreamSynchronize(s));
+  if (st) throw Error("rotation_init: fluid-limit degree-2 factorization failed (zero pivot)");
+}
+
 void setup_handle(vg_handle* h) {
   const vg_params& p = h->p;
   if (p.scheme != VG_SCHEME_FE) throw Error("vg_create: only the forward-Euler memory scheme (\"fe\") is supported");
-  if (p.rotation) throw Error("vg_create: rotational feedback is not implemented in this backend (set rotation = 0)");
   if (p.lmax < 2) throw Error("vg_create: lmax must be >= 2");
   cudaStream_t s = h->stream;
   build_grid(h->grid, p.lmax, p.nlat, p.nphi, s);

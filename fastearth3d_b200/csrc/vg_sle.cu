@@ -317,7 +317,7 @@ void sle_solve_dev(vg_handle* h, double dt, bool report_only) {
       launch_apply(h, h->d_sigma.p, h->d_ulm.p, h->d_ulm.p + 2 * (size_t)nlm);
       legendre_synth_dev(h, h->d_ulm.p, 2, h->d_Gs.p);
       k_synth_sraw<<<nlat, 128, 4 * M * sizeof(double), s>>>(nphi, nlat, M, h->d_Gs.p, G.d_cos.p, G.d_sin.p,
-                                                             h->d_C.p, nullptr, h->d_Sraw.p, rp); ++h->n_launch;
+                                                             h->d_C.p, h->rot_on ? h->d_srot.p : nullptr, h->d_Sraw.p, rp); ++h->n_launch;
       k_dphi<<<1, FIN_THREADS, 0, s>>>(sc, rp, G.d_wts.p, nlat, dlon); ++h->n_launch;
       k_rsl_update<<<nlat, 128, 0, s>>>(nphi, sc, h->d_Sraw.p, h->d_C.p, h->d_rsl.p, rp, nlat); ++h->n_launch;
       k_conv<<<1, FIN_THREADS, 0, s>>>(sc, rp, nlat); ++h->n_launch;
@@ -356,6 +356,12 @@ void update_dev(vg_handle* h, const double* d_ice1, double dt_yr) {
   const double t0 = h->time_yr * SEC_PER_YEAR, t1 = t0 + dt, span = t1 - t0;
   const int eb = 256, eg = (ng + eb - 1) / eb;
   h->worst_mass_resid = 0.0;
+  // rotational feedback: drift frozen at the interval start, s_rot held across
+  // the interval from the entering polar motion (src/vilma_coupling.f90:399-405)
+  if (h->rot_on) {
+    rotation_begin(h);
+    rotation_s_rot(h);
+  }
   auto mass_resid = [&]() {
     read_scalars(h);
     double ice_int = h->h_sc->ice_int, Cs = h->h_sc->mass_Cs;
@@ -409,6 +415,8 @@ void update_dev(vg_handle* h, const double* d_ice1, double dt_yr) {
       }
     }
   }
+  // polar motion to the interval end under the converged load (:411-421)
+  if (h->rot_on) rotation_advance(h, h->d_sigma.p, span);
   VG_CUDA(cudaMemcpyAsync(h->d_h_ice.p, d_ice1, ng * sizeof(double), cudaMemcpyDeviceToDevice, s));
   k_zbed<<<eg, eb, 0, s>>>(ng, h->d_z_bed_eq.p, h->d_rsl.p, h->d_zbed.p); ++h->n_launch;
   VG_CUDA(cudaGetLastError());

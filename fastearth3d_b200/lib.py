@@ -28,6 +28,7 @@ _SIGS = [
     ("vg_get_fields", [_VP, _P, _P, _P, _P]),
     ("vg_rsl_device", [_VP, C.POINTER(C.c_void_p)]),
     ("vg_get_info", [_VP, C.POINTER(VgInfo)]),
+    ("vg_get_rotation", [_VP, _P, _P]),
     ("vg_response_set_dt", [_VP, C.c_double]),
     ("vg_response_begin_step", [_VP]),
     ("vg_response_apply", [_VP, _P, _P, _P]),
@@ -143,6 +144,12 @@ class Model:
         sig = np.zeros(2 * self.nlm)
         self._c(lib().vg_get_fields(self.h, ptr(rsl), ptr(zb), ptr(Cf), ptr(sig)))
         return rsl, zb, Cf, _unpack(sig)
+
+    def rotation(self):
+        """Polar motion m (complex, rad) and (kTe, hTe, k_s fluid, k_s flattening)."""
+        m, love = np.zeros(2), np.zeros(4)
+        self._c(lib().vg_get_rotation(self.h, ptr(m), ptr(love)))
+        return m[0] + 1j * m[1], love
 
     def state(self):
         n = 4 * self.ne * self.nk

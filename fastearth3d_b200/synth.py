@@ -134,8 +134,9 @@ def sawtooth(t_yr, period=100000.0, grow=90000.0):
 class Workload:
     """One benchmark configuration: params, reference fields, ice history."""
 
-    def __init__(self, name, lmax, n_elem, dt_yr, n_steps, n_caps, history, sle, visc3d, seed=1234):
+    def __init__(self, name, lmax, n_elem, dt_yr, n_steps, n_caps, history, sle, visc3d, seed=1234, rotation=False):
         self.name, self.lmax, self.n_elem = name, lmax, n_elem
+        self.rotation = rotation
         self.nlat, self.nphi = lmax + 1, 2 * (lmax + 1)
         self.dt_yr, self.n_steps, self.history, self.sle, self.visc3d = dt_yr, n_steps, history, sle, visc3d
         self.seed = seed
@@ -156,6 +157,7 @@ class Workload:
         set_layers(p, EARTH4)
         for i, c in enumerate(element_counts(self.n_elem)):
             p.ne_layer[i] = c
+        p.rotation = 1 if self.rotation else 0
         return p
 
     def ice_at(self, step):
@@ -185,6 +187,7 @@ class Workload:
 def workloads():
     return {
         "c1_1d_l64": Workload("c1_1d_l64", 64, 60, 50.0, 400, 3, "ramp", sle=False, visc3d=False),
-        "c2_1d_sle_l128": Workload("c2_1d_sle_l128", 128, 100, 100.0, 1000, 6, "sawtooth", sle=True, visc3d=False),
+        "c2_1d_sle_l128": Workload("c2_1d_sle_l128", 128, 100, 100.0, 1000, 6, "sawtooth", sle=True, visc3d=False,
+                                   rotation=True),
         "c3_3d_l128": Workload("c3_3d_l128", 128, 100, 50.0, 2000, 6, "sawtooth", sle=True, visc3d=True),
     }

@@ -67,7 +67,9 @@ typedef struct vg_params {
   int sle_n_outer, sle_n_inner;
   double sle_tol;
   int sle_fixed_ocean, sle_subgrid, sle_warm_start;
-  /* rotational feedback (src/vilma_params.f90:96); not implemented: must be 0 */
+  /* rotational feedback / polar wander (src/vilma_params.f90:96,
+   * src/vilma_rotation.f90), coupled per interval like
+   * src/vilma_coupling.f90:399-424 */
   int rotation;
   /* arithmetic of the 3-D stress products (no reference counterpart):
    * VG_VISC3D_FP64 (default) or VG_VISC3D_SPLIT_TC, the Legendre and longitude
@@ -128,7 +130,7 @@ int vg_set_reference(vg_handle* h, const double* z_bed_eq, const double* h_ice_e
  * src/vilma_response.f90:994-1053). */
 int vg_enable_visc3d(vg_handle* h, const double* pert);
 
-/* solid_earth_update (src/vilma_coupling.f90:336-437) without rotation:
+/* solid_earth_update (src/vilma_coupling.f90:336-437):
  * advance by dt_yr years with the ice linearly interpolated from the carried
  * ice to h_ice (stepper_advance, src/vilma_timestep.f90:79-227). h_ice is a
  * host array. */
@@ -142,6 +144,11 @@ int vg_get_fields(vg_handle* h, double* rsl, double* z_bed, double* C, double* s
 /* Device pointer of the rsl field (read-only, valid until vg_destroy). */
 int vg_rsl_device(vg_handle* h, const double** d_rsl);
 int vg_get_info(vg_handle* h, vg_info* info);
+/* Rotational feedback (rotation = 1; src/vilma_rotation.f90): polar motion
+ * m = m1 + i m2 [rad] as (re, im), and the degree-2 constants (k^T_e, h^T_e,
+ * k^T_f the secular k_s used, k_s from the observed flattening). Either
+ * pointer may be NULL. Fails when rotation is off. */
+int vg_get_rotation(vg_handle* h, double* m, double* love);
 
 /* Response-level operators (src/vilma_response.f90:43-52, 266-319) for a run
  * without the sea-level equation (bench_visc3d style): begin_step freezes the
