@@ -89,7 +89,7 @@ struct DArr {
 // read back as one small struct when the host needs a decision.
 struct SleScalars {
   double C_int, ice_int, zeta_int, Cs_int, dphi, dmax, smax, mass_Cs;
-  int flips, pad;
+  int flips, n_inner;  // coastline flips; inner iterations done by the fused loop
   unsigned long long mem_norm_bits;  // max |memory| of the state the last advance wrote
 };
 
@@ -171,6 +171,8 @@ struct vg_handle {
   vg::DArr<double> d_Gs;       // Legendre sums (2 * M * nlat * batch)
   vg::DArr<double> d_sigma, d_ulm, d_nlm;  // spectra (2*nlm)
   vg::DArr<double> d_rowpart;  // per-row partial sums (8 * nlat)
+  vg::DArr<unsigned int> d_gbar;  // grid barrier of the fused inner loop: count, generation, error
+  int sle_grid = 0;               // CTAs of the cooperative inner-loop launch (one per SM)
   // counters
   long long n_accept = 0, n_reject = 0, n_solve = 0, n_drift_solved = 0;
   int n_sub_last = 0, n_outer_last = 0, n_inner_last = 0, n_flip_last = 0;

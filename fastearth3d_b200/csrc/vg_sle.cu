@@ -268,12 +268,303 @@ __global__ void k_bsl_rows(int nphi, const double* __restrict__ hi, const double
   }
 }
 
+// ------------------------------------------------------------------ fused inner loop
+// The inner load fixed point of sle_solve (src/vilma_sle.f90:280-340) as one
+// cooperative persistent kernel: one CTA per SM, phases separated by a grid
+// barrier, the convergence test on the device, so no host round trip per
+// iteration. Each phase keeps the arithmetic (and the per-thread summation
+// order) of the separate kernels it replaces:
+//   1 load + longitude analysis per row     (k_load_fourier)
+//   2 Legendre analysis + apply, warp per lm (k_legendre_analysis, k_apply)
+//   3 Legendre synthesis of u and N          (k_legendre_synth)
+//   4 longitude synthesis, Sraw, row sums    (k_synth_sraw)
+//   5 mass-conserving dphi                   (k_dphi)
+//   6 rsl update, row maxima                 (k_rsl_update)
+//   7 convergence                            (k_conv)
+struct InnerArgs {
+  int nphi, nlat, M, nlm, nk, lmax, n_inner;
+  double tol, dlon, g;
+  const double *dig, *C, *wcorr, *cs, *sn, *plm, *wts, *gu, *gn, *drift, *srot;
+  const int *lm_m, *lm_l, *lm2k, *mbeg;
+  double *rsl, *F, *sigma, *ulm, *Gs, *Sraw, *rowpart;
+  SleScalars* sc;
+  unsigned int* bar;  // count, generation, error
+};
+
+constexpr unsigned long long BAR_WAIT_NS = 2000000000ull;  // 2 s bound on a grid barrier
+
+__device__ __forceinline__ unsigned long long gtimer_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+// Sense-counting grid barrier with a bounded wait. Returns false (in every
+// thread of the CTA) if it timed out or another CTA reported a timeout.
+__device__ bool grid_barrier(unsigned int* bar, unsigned int& gen) {
+  __shared__ int s_ok;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int ok = 1;
+    volatile unsigned int* vgen = bar + 1;
+    __threadfence();
+    const unsigned int arrived = atomicAdd(bar, 1u);
+    if (arrived == gridDim.x - 1) {
+      bar[0] = 0u;
+      __threadfence();
+      atomicExch(bar + 1, gen + 1u);
+    } else {
+      const unsigned long long t0 = gtimer_ns();
+      while (*vgen == gen) {
+        if (gtimer_ns() - t0 > BAR_WAIT_NS) {
+          atomicExch(bar + 2, 1u);
+          ok = 0;
+          break;
+        }
+        __nanosleep(64);
+      }
+    }
+    __threadfence();
+    if (*(volatile unsigned int*)(bar + 2)) ok = 0;
+    s_ok = ok;
+  }
+  ++gen;
+  __syncthreads();
+  return s_ok != 0;
+}
+
+__global__ void __launch_bounds__(512) k_sle_inner(InnerArgs A) {
+  extern __shared__ double sm[];  // max(nphi, 4 M) doubles
+  __shared__ double red[512];
+  __shared__ int s_stop;
+  const int tid = threadIdx.x, nthr = blockDim.x;
+  const int lane = tid & 31, wid = tid >> 5, nw = nthr >> 5;
+  const int nphi = A.nphi, nlat = A.nlat, M = A.M, nlm = A.nlm;
+  const double sc_f = 2.0 * PI / (double)nphi;
+  unsigned int gen = 0;
+  int it = 0;
+  for (it = 1; it <= A.n_inner; ++it) {
+    // 1. total surface load of each row and its longitude analysis
+    for (int j = blockIdx.x; j < nlat; j += gridDim.x) {
+      __syncthreads();
+      for (int i = tid; i < nphi; i += nthr) {
+        const size_t p = (size_t)j * nphi + i;
+        sm[i] = RHO_ICE * A.dig[p] + RHO_WATER * (A.C[p] * A.rsl[p]) + A.wcorr[p];
+      }
+      __syncthreads();
+      for (int m = tid; m < M; m += nthr) {
+        double re = 0.0, im = 0.0;
+        int t = 0;
+        for (int i = 0; i < nphi; ++i) {
+          const double f = sm[i];
+          re += f * __ldg(&A.cs[t]);
+          im -= f * __ldg(&A.sn[t]);
+          t += m;
+          if (t >= nphi) t -= nphi;
+        }
+        A.F[((size_t)m * nlat + j) * 2] = re * sc_f;
+        A.F[((size_t)m * nlat + j) * 2 + 1] = im * sc_f;
+      }
+    }
+    if (!grid_barrier(A.bar, gen)) return;
+    // 2. Legendre analysis (warp per lm) and the affine response u, N
+    for (int lm = blockIdx.x * nw + wid; lm < nlm; lm += gridDim.x * nw) {
+      const int m = A.lm_m[lm];
+      const double* Fm = A.F + ((size_t)m * nlat) * 2;
+      const double* P = A.plm + (size_t)lm * nlat;
+      double re = 0.0, im = 0.0;
+      for (int j = lane; j < nlat; j += 32) {
+        const double wp = A.wts[j] * P[j];
+        re += wp * Fm[2 * j];
+        im += wp * Fm[2 * j + 1];
+      }
+      for (int o = 16; o > 0; o >>= 1) {
+        re += __shfl_down_sync(0xffffffffu, re, o);
+        im += __shfl_down_sync(0xffffffffu, im, o);
+      }
+      if (lane == 0) {
+        A.sigma[2 * lm] = re;
+        A.sigma[2 * lm + 1] = im;
+        const int l = A.lm_l[lm];
+        double* u = A.ulm;
+        double* n = A.ulm + 2 * (size_t)nlm;
+        if (l == 0) {
+          u[2 * lm] = A.gu[0] * re;
+          u[2 * lm + 1] = A.gu[0] * im;
+          n[2 * lm] = A.gn[0] * re;
+          n[2 * lm + 1] = A.gn[0] * im;
+        } else {
+          const int k = A.lm2k[lm];
+          u[2 * lm] = A.gu[l] * re + A.drift[(size_t)0 * A.nk + k];
+          u[2 * lm + 1] = A.gu[l] * im + A.drift[(size_t)1 * A.nk + k];
+          n[2 * lm] = A.gn[l] * re - A.drift[(size_t)2 * A.nk + k] / A.g;
+          n[2 * lm + 1] = A.gn[l] * im - A.drift[(size_t)3 * A.nk + k] / A.g;
+        }
+      }
+    }
+    if (!grid_barrier(A.bar, gen)) return;
+    // 3. Legendre synthesis of u (b = 0) and N (b = 1): a thread per (b, m, j)
+    for (int t = blockIdx.x * nthr + tid; t < 2 * M * nlat; t += gridDim.x * nthr) {
+      const int j = t % nlat, m = (t / nlat) % M, b = t / (nlat * M);
+      const int lm0 = A.mbeg[m];
+      const double* qb = A.ulm + (size_t)b * nlm * 2;
+      double re = 0.0, im = 0.0;
+      for (int l = m; l <= A.lmax; ++l) {
+        const double p = A.plm[(size_t)(lm0 + l - m) * nlat + j];
+        re += qb[2 * (lm0 + l - m)] * p;
+        im += qb[2 * (lm0 + l - m) + 1] * p;
+      }
+      A.Gs[(((size_t)b * M + m) * nlat + j) * 2] = re;
+      A.Gs[(((size_t)b * M + m) * nlat + j) * 2 + 1] = im;
+    }
+    if (!grid_barrier(A.bar, gen)) return;
+    // 4. longitude synthesis, Sraw = N - u (+ s_rot), row sums of C Sraw
+    for (int j = blockIdx.x; j < nlat; j += gridDim.x) {
+      double* Gu = sm;
+      double* Gn = sm + 2 * M;
+      __syncthreads();
+      for (int m = tid; m < M; m += nthr) {
+        Gu[2 * m] = A.Gs[((size_t)m * nlat + j) * 2];
+        Gu[2 * m + 1] = A.Gs[((size_t)m * nlat + j) * 2 + 1];
+        Gn[2 * m] = A.Gs[(((size_t)M + m) * nlat + j) * 2];
+        Gn[2 * m + 1] = A.Gs[(((size_t)M + m) * nlat + j) * 2 + 1];
+      }
+      __syncthreads();
+      double acc = 0.0;
+      for (int i = tid; i < nphi; i += nthr) {
+        const size_t p = (size_t)j * nphi + i;
+        const double u = row_fourier_synth_at(Gu, M, i, nphi, A.cs, A.sn);
+        const double N = row_fourier_synth_at(Gn, M, i, nphi, A.cs, A.sn);
+        double sv = N - u;
+        if (A.srot) sv = sv + A.srot[p];
+        A.Sraw[p] = sv;
+        acc += A.C[p] * sv;
+      }
+      acc = block_sum(acc, red);
+      if (tid == 0) A.rowpart[RP_CS * nlat + j] = acc;
+    }
+    if (!grid_barrier(A.bar, gen)) return;
+    // 5. dphi (one CTA, rows in order)
+    if (blockIdx.x == 0) {
+      const double Cs = integrate_rows(A.rowpart + RP_CS * nlat, A.wts, nlat, A.dlon);
+      if (tid == 0) {
+        A.sc->Cs_int = Cs;
+        A.sc->dphi = (A.sc->ice_int - Cs + A.sc->zeta_int) / A.sc->C_int;
+      }
+    }
+    if (!grid_barrier(A.bar, gen)) return;
+    // 6. rsl update and the row maxima of the change
+    const double dphi = *(volatile double*)&A.sc->dphi;
+    for (int j = blockIdx.x; j < nlat; j += gridDim.x) {
+      double dmax = 0.0, smax = 0.0;
+      for (int i = tid; i < nphi; i += nthr) {
+        const size_t p = (size_t)j * nphi + i;
+        const double rn = A.Sraw[p] + dphi;
+        dmax = nanmax(dmax, fabs(A.C[p] * (rn - A.rsl[p])));
+        A.rsl[p] = rn;
+        smax = nanmax(smax, fabs(A.C[p] * rn));
+      }
+      dmax = block_max(dmax, red);
+      smax = block_max(smax, red);
+      if (tid == 0) {
+        A.rowpart[RP_DMAX * nlat + j] = dmax;
+        A.rowpart[RP_SMAX * nlat + j] = smax;
+      }
+    }
+    if (!grid_barrier(A.bar, gen)) return;
+    // 7. convergence (src/vilma_sle.f90:330-338), decided by CTA 0
+    if (blockIdx.x == 0) {
+      double dmax = 0.0, smax = 0.0;
+      for (int j = tid; j < nlat; j += nthr) {
+        dmax = nanmax(dmax, A.rowpart[RP_DMAX * nlat + j]);
+        smax = nanmax(smax, A.rowpart[RP_SMAX * nlat + j]);
+      }
+      dmax = block_max(dmax, red);
+      smax = block_max(smax, red);
+      if (tid == 0) {
+        A.sc->dmax = dmax;
+        A.sc->smax = smax;
+        A.sc->n_inner = it;
+        A.bar[3] = (dmax <= A.tol * fmax(smax, TINY)) ? 1u : 0u;
+      }
+    }
+    if (!grid_barrier(A.bar, gen)) return;
+    if (tid == 0) s_stop = (int)*(volatile unsigned int*)(A.bar + 3);
+    __syncthreads();
+    if (s_stop) break;
+  }
+}
+
+static void launch_inner_loop(vg_handle* h) {
+  const Grid& G = h->grid;
+  cudaStream_t s = h->stream;
+  if (h->sle_grid == 0) {
+    int dev = 0, nsm = 0, per_sm = 0;
+    VG_CUDA(cudaGetDevice(&dev));
+    VG_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+    const size_t shm = (size_t)std::max(G.nphi, 4 * G.M) * sizeof(double);
+    if (shm > 48 * 1024)
+      VG_CUDA(cudaFuncSetAttribute(k_sle_inner, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm));
+    VG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_sle_inner, 512, shm));
+    if (per_sm < 1) throw Error("sle_solve: the fused inner loop does not fit on an SM");
+    h->sle_grid = nsm;
+    h->d_gbar.alloc(4);
+  }
+  InnerArgs A;
+  A.nphi = G.nphi;
+  A.nlat = G.nlat;
+  A.M = G.M;
+  A.nlm = G.nlm;
+  A.nk = h->nk;
+  A.lmax = G.lmax;
+  A.n_inner = h->p.sle_n_inner;
+  A.tol = h->p.sle_tol;
+  A.dlon = 2.0 * PI / (double)G.nphi;
+  A.g = h->g;
+  A.dig = h->d_dig.p;
+  A.C = h->d_C.p;
+  A.wcorr = h->d_wcorr.p;
+  A.cs = G.d_cos.p;
+  A.sn = G.d_sin.p;
+  A.plm = G.d_plm.p;
+  A.wts = G.d_wts.p;
+  A.gu = h->d_gu.p;
+  A.gn = h->d_gn.p;
+  A.drift = h->d_drift.p;
+  A.srot = h->rot_on ? h->d_srot.p : nullptr;
+  A.lm_m = G.d_lm_m.p;
+  A.lm_l = G.d_lm_l.p;
+  A.lm2k = h->d_lm2k.p;
+  A.mbeg = G.d_mbeg.p;
+  A.rsl = h->d_rsl.p;
+  A.F = h->d_F.p;
+  A.sigma = h->d_sigma.p;
+  A.ulm = h->d_ulm.p;
+  A.Gs = h->d_Gs.p;
+  A.Sraw = h->d_Sraw.p;
+  A.rowpart = h->d_rowpart.p;
+  A.sc = h->d_sc_.p;
+  A.bar = h->d_gbar.p;
+  VG_CUDA(cudaMemsetAsync(h->d_gbar.p, 0, 4 * sizeof(unsigned int), s));
+  const size_t shm = (size_t)std::max(G.nphi, 4 * G.M) * sizeof(double);
+  void* args[] = {&A};
+  VG_CUDA(cudaLaunchCooperativeKernel((const void*)k_sle_inner, dim3(h->sle_grid), dim3(512), args, shm, s));
+  ++h->n_launch;
+}
+
 static void read_scalars(vg_handle* h) {
   VG_CUDA(cudaMemcpyAsync(h->h_sc, h->d_sc_.p, sizeof(SleScalars), cudaMemcpyDeviceToHost, h->stream));
   VG_CUDA(cudaStreamSynchronize(h->stream));
 }
 
 void sync_scalars(vg_handle* h) { read_scalars(h); }
+
+// error word of the fused loop's grid barrier (read after read_scalars synchronised)
+static bool h_bar_error(vg_handle* h) {
+  unsigned int e = 0;
+  VG_CUDA(cudaMemcpy(&e, h->d_gbar.p + 2, sizeof(e), cudaMemcpyDeviceToHost));
+  return e != 0;
+}
 
 // One sea-level solve with the memory advance at its end (FE: a single
 // co-convergence pass), src/vilma_sle.f90:124-405. Writes the advanced memory
@@ -309,22 +600,13 @@ void sle_solve_dev(vg_handle* h, double dt, bool report_only) {
     if (h->h_sc->C_int <= 0.0) break;  // no ocean: nothing to redistribute
     k_finalize_pass<<<1, FIN_THREADS, 0, s>>>(sc, rp, G.d_wts.p, nlat, dlon, p.sle_subgrid); ++h->n_launch;
     k_wcorr<<<eg, eb, 0, s>>>(ng, p.sle_subgrid, h->d_z_bed_eq.p, h->d_C.p, h->d_C0.p, h->d_wcorr.p); ++h->n_launch;
-    for (int ii = 1; ii <= p.sle_n_inner; ++ii) {
+    {
       PhaseScope ps(h, VG_PH_SLE);
-      k_load_fourier<<<nlat, 128, nphi * sizeof(double), s>>>(nphi, nlat, M, h->d_dig.p, h->d_C.p, h->d_rsl.p,
-                                                              h->d_wcorr.p, G.d_cos.p, G.d_sin.p, h->d_F.p); ++h->n_launch;
-      legendre_analysis_dev(h, h->d_F.p, 1, h->d_sigma.p);
-      launch_apply(h, h->d_sigma.p, h->d_ulm.p, h->d_ulm.p + 2 * (size_t)nlm);
-      legendre_synth_dev(h, h->d_ulm.p, 2, h->d_Gs.p);
-      k_synth_sraw<<<nlat, 128, 4 * M * sizeof(double), s>>>(nphi, nlat, M, h->d_Gs.p, G.d_cos.p, G.d_sin.p,
-                                                             h->d_C.p, h->rot_on ? h->d_srot.p : nullptr, h->d_Sraw.p, rp); ++h->n_launch;
-      k_dphi<<<1, FIN_THREADS, 0, s>>>(sc, rp, G.d_wts.p, nlat, dlon); ++h->n_launch;
-      k_rsl_update<<<nlat, 128, 0, s>>>(nphi, sc, h->d_Sraw.p, h->d_C.p, h->d_rsl.p, rp, nlat); ++h->n_launch;
-      k_conv<<<1, FIN_THREADS, 0, s>>>(sc, rp, nlat); ++h->n_launch;
-      read_scalars(h);
-      h->n_inner_last = ii;
-      if (h->h_sc->dmax <= p.sle_tol * std::max(h->h_sc->smax, TINY)) break;
+      launch_inner_loop(h);
     }
+    read_scalars(h);
+    if (h_bar_error(h)) throw Error("sle_solve: grid barrier of the fused inner loop timed out");
+    h->n_inner_last = h->h_sc->n_inner;
     h->n_outer_last = io;
     if (p.sle_fixed_ocean) break;
     k_coast<<<nlat, 128, 0, s>>>(nphi, h->d_z_bed_eq.p, h->d_rsl.p, h->d_ice_now.p, h->d_C.p, h->d_C_next.p, rp,
