@@ -384,6 +384,46 @@ int vg_set_state(vg_handle* h, const double* Are, const double* Aim, const doubl
     vg::compute_mem_norm(h, h->cur);
     h->mem_norm = vg::read_mem_norm(h, h->cur);
     h->time_s = time_s;
+    h->time_yr = time_s / vg::SEC_PER_YEAR;
+  });
+}
+
+int vg_set_fields(vg_handle* h, const double* h_ice, const double* rsl, const double* z_bed, const double* C) {
+  return guarded(h, [&] {
+    need(h, h->have_reference, "vg_set_fields: vg_set_reference must come first");
+    const int ng = h->grid.ng;
+    cudaStream_t s = h->stream;
+    if (h_ice) h->d_h_ice.upload(h_ice, ng, s);
+    if (rsl) h->d_rsl.upload(rsl, ng, s);
+    if (z_bed) h->d_zbed.upload(z_bed, ng, s);
+    if (C) h->d_C.upload(C, ng, s);
+    vg::update_bsl(h);
+  });
+}
+
+int vg_get_rotation_state(vg_handle* h, double* m, double* load_mem, double* tidal_mem) {
+  return guarded(h, [&] {
+    need(h, h->rot_on, "vg_get_rotation_state: rotational feedback is off for this handle");
+    const size_t per = (size_t)6 * h->ne * 4;
+    cudaStream_t s = h->stream;
+    if (m) VG_CUDA(cudaMemcpyAsync(m, h->d_rot_sc.p + 8, 2 * sizeof(double), cudaMemcpyDeviceToHost, s));
+    if (load_mem) VG_CUDA(cudaMemcpyAsync(load_mem, h->d_rot_mem.p, per * sizeof(double), cudaMemcpyDeviceToHost, s));
+    if (tidal_mem)
+      VG_CUDA(cudaMemcpyAsync(tidal_mem, h->d_rot_mem.p + per, per * sizeof(double), cudaMemcpyDeviceToHost, s));
+    VG_CUDA(cudaStreamSynchronize(s));
+  });
+}
+
+int vg_set_rotation_state(vg_handle* h, const double* m, const double* load_mem, const double* tidal_mem) {
+  return guarded(h, [&] {
+    need(h, h->rot_on, "vg_set_rotation_state: rotational feedback is off for this handle");
+    need(h, m && load_mem && tidal_mem, "vg_set_rotation_state: m and both channel memories are required");
+    const size_t per = (size_t)6 * h->ne * 4;
+    cudaStream_t s = h->stream;
+    VG_CUDA(cudaMemcpyAsync(h->d_rot_sc.p + 8, m, 2 * sizeof(double), cudaMemcpyHostToDevice, s));
+    VG_CUDA(cudaMemcpyAsync(h->d_rot_mem.p, load_mem, per * sizeof(double), cudaMemcpyHostToDevice, s));
+    VG_CUDA(cudaMemcpyAsync(h->d_rot_mem.p + per, tidal_mem, per * sizeof(double), cudaMemcpyHostToDevice, s));
+    VG_CUDA(cudaStreamSynchronize(s));
   });
 }
 

@@ -37,6 +37,9 @@ _SIGS = [
     ("vg_get_drift", [_VP, _P, _P, _P]),
     ("vg_get_state", [_VP, _P, _P, _P, _P, _P, _P, _P]),
     ("vg_set_state", [_VP, _P, _P, _P, _P, _P, _P, C.c_double]),
+    ("vg_set_fields", [_VP, _P, _P, _P, _P]),
+    ("vg_get_rotation_state", [_VP, _P, _P, _P]),
+    ("vg_set_rotation_state", [_VP, _P, _P, _P]),
     ("vg_sht_analysis", [_VP, _P, _P]),
     ("vg_sht_synthesis", [_VP, _P, _P]),
     ("vg_sht_analysis_noalloc", [_VP, C.c_void_p, C.c_void_p, C.c_int]),
@@ -144,6 +147,21 @@ class Model:
         sig = np.zeros(2 * self.nlm)
         self._c(lib().vg_get_fields(self.h, ptr(rsl), ptr(zb), ptr(Cf), ptr(sig)))
         return rsl, zb, Cf, _unpack(sig)
+
+    def set_fields(self, h_ice=None, rsl=None, z_bed=None, C_ocean=None):
+        self._c(lib().vg_set_fields(self.h, *[ptr(None if a is None else np.ascontiguousarray(a, dtype=np.float64))
+                                              for a in (h_ice, rsl, z_bed, C_ocean)]))
+
+    def rotation_state(self):
+        n = 6 * self.ne * 4
+        m, lm, tm = np.zeros(2), np.zeros(n), np.zeros(n)
+        self._c(lib().vg_get_rotation_state(self.h, ptr(m), ptr(lm), ptr(tm)))
+        return m, lm, tm
+
+    def set_rotation_state(self, m, load_mem, tidal_mem):
+        self._c(lib().vg_set_rotation_state(self.h, ptr(np.ascontiguousarray(m, dtype=np.float64)),
+                                            ptr(np.ascontiguousarray(load_mem, dtype=np.float64)),
+                                            ptr(np.ascontiguousarray(tidal_mem, dtype=np.float64))))
 
     def rotation(self):
         """Polar motion m (complex, rad) and (kTe, hTe, k_s fluid, k_s flattening)."""

@@ -170,6 +170,18 @@ int vg_get_state(vg_handle* h, double* Are, double* Aim, double* Bre, double* Bi
                  double* Cre, double* Cim, double* time_s);
 int vg_set_state(vg_handle* h, const double* Are, const double* Aim, const double* Bre,
                  const double* Bim, const double* Cre, const double* Cim, double time_s);
+/* The restart's diagnostic fields, restored when present (vilma_restart_read,
+ * src/vilma_io.f90:414-468, 587-597): carried ice h_ice, rsl (the sea-level
+ * warm start), z_bed, ocean function C, all (nphi, nlat). NULL skips a field.
+ * After vg_set_reference. */
+int vg_set_fields(vg_handle* h, const double* h_ice, const double* rsl, const double* z_bed,
+                  const double* C);
+/* Rotation restart state (rotation_get_memory / rotation_set_memory,
+ * src/vilma_rotation.f90:275-295): polar motion m as (re, im) and the load and
+ * tidal channels' memory stress, each (NLAM=4, ne, 6) Fortran order with the
+ * last axis [A re, A im, B re, B im, C re, C im]. */
+int vg_get_rotation_state(vg_handle* h, double* m, double* load_mem, double* tidal_mem);
+int vg_set_rotation_state(vg_handle* h, const double* m, const double* load_mem, const double* tidal_mem);
 
 /* Gauss-grid transforms on the device (sht_grid_synthesis / _analysis,
  * src/vilma_sht.f90:204-226), host arrays in and out. */
