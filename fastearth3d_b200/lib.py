@@ -40,6 +40,8 @@ _SIGS = [
     ("vg_set_fields", [_VP, _P, _P, _P, _P]),
     ("vg_get_rotation_state", [_VP, _P, _P, _P]),
     ("vg_set_rotation_state", [_VP, _P, _P, _P]),
+    ("vg_misfit", [_VP, C.c_int, C.c_double, _P, C.c_int, C.POINTER(C.c_int), _P, _P]),
+    ("vg_misfit_grad", [_VP, C.c_int, C.c_double, _P, C.c_int, C.POINTER(C.c_int), _P, C.c_int, _P, _P]),
     ("vg_sht_analysis", [_VP, _P, _P]),
     ("vg_sht_synthesis", [_VP, _P, _P]),
     ("vg_sht_analysis_noalloc", [_VP, C.c_void_p, C.c_void_p, C.c_int]),
@@ -162,6 +164,31 @@ class Model:
         self._c(lib().vg_set_rotation_state(self.h, ptr(np.ascontiguousarray(m, dtype=np.float64)),
                                             ptr(np.ascontiguousarray(load_mem, dtype=np.float64)),
                                             ptr(np.ascontiguousarray(tidal_mem, dtype=np.float64))))
+
+    def _misfit_args(self, sigma, sites, obs):
+        sig = np.ascontiguousarray(np.stack([np.asarray(sigma).real, np.asarray(sigma).imag], axis=-1).reshape(-1),
+                                   dtype=np.float64)
+        st = np.ascontiguousarray(sites, dtype=np.int32)
+        ob = np.ascontiguousarray(obs, dtype=np.float64).reshape(-1)
+        return sig, st, ob
+
+    def misfit(self, sigma, dt_s, sites, obs):
+        """J of the response-level run (sigma: (nsteps, nlm) complex; obs: (nsteps, nsite))."""
+        sig, st, ob = self._misfit_args(sigma, sites, obs)
+        J = C.c_double(0)
+        self._c(lib().vg_misfit(self.h, len(sigma), dt_s, ptr(sig), len(st),
+                                st.ctypes.data_as(C.POINTER(C.c_int)), ptr(ob), C.byref(J)))
+        return J.value
+
+    def misfit_grad(self, sigma, dt_s, sites, obs, ckpt_every=50):
+        """(J, dJ/dsigma) with dJ/dsigma shaped like sigma: d/dRe + 1j d/dIm."""
+        sig, st, ob = self._misfit_args(sigma, sites, obs)
+        J = C.c_double(0)
+        g = np.zeros_like(sig)
+        self._c(lib().vg_misfit_grad(self.h, len(sigma), dt_s, ptr(sig), len(st),
+                                     st.ctypes.data_as(C.POINTER(C.c_int)), ptr(ob), ckpt_every, C.byref(J), ptr(g)))
+        g = g.reshape(len(sigma), -1, 2)
+        return J.value, g[..., 0] + 1j * g[..., 1]
 
     def rotation(self):
         """Polar motion m (complex, rad) and (kTe, hTe, k_s fluid, k_s flattening)."""

@@ -183,6 +183,23 @@ int vg_set_fields(vg_handle* h, const double* h_ice, const double* rsl, const do
 int vg_get_rotation_state(vg_handle* h, double* m, double* load_mem, double* tidal_mem);
 int vg_set_rotation_state(vg_handle* h, const double* m, const double* load_mem, const double* tidal_mem);
 
+/* Relative-sea-level misfit of a response-level run and its gradient
+ * (hand-written discrete adjoint; the reference has no counterpart). From the
+ * handle's current memory, nsteps steps of length dt_s: begin_step, apply and
+ * advance (src/vilma_response.f90:228-319) with the load sigma_lm[n] (nlm
+ * complex per step, interleaved) held over step n, no sea-level equation:
+ *   J = sum_n sum_s (rsl_n(site[s]) - obs[n * nsite + s])^2,  rsl = N - u
+ * at the Gauss-grid points site[s] (land sites, no ocean). vg_misfit_grad also
+ * returns dJ/dsigma (same layout as sigma_lm; NULL skips it) from a reverse
+ * sweep, keeping the memory every ckpt_every steps for recomputation. The
+ * handle's memory is left as it was. The drift skip gate is off inside these
+ * calls. Elements with lateral viscosity are not yet differentiated
+ * (vg_misfit_grad fails for them; vg_misfit supports them). */
+int vg_misfit(vg_handle* h, int nsteps, double dt_s, const double* sigma_lm, int nsite, const int* site,
+              const double* obs, double* J);
+int vg_misfit_grad(vg_handle* h, int nsteps, double dt_s, const double* sigma_lm, int nsite, const int* site,
+                   const double* obs, int ckpt_every, double* J, double* grad_sigma);
+
 /* Gauss-grid transforms on the device (sht_grid_synthesis / _analysis,
  * src/vilma_sht.f90:204-226), host arrays in and out. */
 int vg_sht_analysis(vg_handle* h, const double* f, double* q_lm);

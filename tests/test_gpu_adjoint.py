@@ -1,0 +1,68 @@
+"""The hand-written adjoint of the response-level time step (vg_misfit_grad):
+its gradient of the rsl misfit with respect to the load history against
+central finite differences of the FP64 GPU forward (vg_misfit) along seeded
+random directions, and its independence of the checkpoint interval. The
+forward is linear in the load, so central differences are exact up to
+rounding; the stated tolerance is 1e-6 relative."""
+import numpy as np
+import pytest
+
+from fastearth3d_b200 import lib as vlib
+from fastearth3d_b200 import synth
+
+pytestmark = pytest.mark.gpu
+
+
+def setup(lmax=12, nsteps=10, nsite=40, seed=3):
+    p = vlib.default_params()
+    p.lmax, p.nlat, p.nphi = lmax, lmax + 1, 2 * (lmax + 1)
+    for i, c in enumerate([2, 6, 5, 3]):
+        p.ne_layer[i] = c
+    m = vlib.Model(p)
+    rng = np.random.default_rng(seed)
+    nlm = m.nlm
+
+    def load_history(scale):
+        s = (rng.standard_normal((nsteps, nlm)) + 1j * rng.standard_normal((nsteps, nlm))) * scale
+        s[:, : lmax + 1] = s[:, : lmax + 1].real  # m = 0 coefficients of a real field
+        return s
+
+    sigma = load_history(1e3)
+    truth = load_history(1e3)
+    sites = rng.choice(m.ng, size=nsite, replace=False)
+    dt = 100.0 * synth.SEC_PER_YEAR
+    obs = np.zeros((nsteps, nsite))
+    # observations: the forward's rsl for the truth history (misfit of zero obs gives -rsl)
+    J0 = m.misfit(truth, dt, sites, obs)
+    assert J0 > 0
+    return m, sigma, truth, sites, dt, rng
+
+
+def test_adjoint_gradient_vs_central_differences():
+    m, sigma, truth, sites, dt, rng = setup()
+    obs = 0.01 * rng.standard_normal((len(sigma), len(sites)))
+    J, g = m.misfit_grad(sigma, dt, sites, obs, ckpt_every=4)
+    assert abs(J - m.misfit(sigma, dt, sites, obs)) <= 1e-12 * J
+    for _ in range(8):
+        d = rng.standard_normal(sigma.shape) + 1j * rng.standard_normal(sigma.shape)
+        d[:, : m.p.lmax + 1] = d[:, : m.p.lmax + 1].real
+        h = 1e-3 * np.abs(sigma).max() / np.abs(d).max()
+        jp = m.misfit(sigma + h * d, dt, sites, obs)
+        jm = m.misfit(sigma - h * d, dt, sites, obs)
+        fd = (jp - jm) / (2 * h)
+        ad = np.sum(g.real * d.real + g.imag * d.imag)
+        assert abs(fd - ad) <= 1e-6 * max(abs(fd), 1e-300), (fd, ad)
+
+
+def test_adjoint_checkpoint_interval_and_state_kept():
+    m, sigma, truth, sites, dt, rng = setup(nsteps=7)
+    obs = np.zeros((len(sigma), len(sites)))
+    s0, _ = m.state()
+    J1, g1 = m.misfit_grad(sigma, dt, sites, obs, ckpt_every=1)
+    J3, g3 = m.misfit_grad(sigma, dt, sites, obs, ckpt_every=3)
+    J7, g7 = m.misfit_grad(sigma, dt, sites, obs, ckpt_every=7)
+    assert J1 == J3 == J7
+    assert np.array_equal(g1, g3) and np.array_equal(g1, g7)
+    s1, _ = m.state()
+    for a, b in zip(s0, s1):
+        assert np.array_equal(a, b)
