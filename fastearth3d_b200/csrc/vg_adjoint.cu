@@ -52,24 +52,32 @@ __global__ void k_site_synth(int nsite, const int* __restrict__ site, int nlm, i
   if (threadIdx.x == 0) resid[s] = acc - obs[s];
 }
 
-// q_bar = (site synthesis)^T (2 r): one thread per lm, sites in order
-__global__ void k_site_synth_T(int nsite, const int* __restrict__ site, int nlm, int nlat, int nphi,
-                               const int* __restrict__ lm_m, const double* __restrict__ plm,
-                               const double* __restrict__ cs, const double* __restrict__ sn,
-                               const double* __restrict__ resid, double* __restrict__ qbar) {
-  const int lm = blockIdx.x * blockDim.x + threadIdx.x;
+// q_bar = (site synthesis)^T (2 r): a warp per lm, lanes over the sites
+__global__ void __launch_bounds__(256) k_site_synth_T(int nsite, const int* __restrict__ site, int nlm, int nlat,
+                                                      int nphi, const int* __restrict__ lm_m,
+                                                      const double* __restrict__ plm, const double* __restrict__ cs,
+                                                      const double* __restrict__ sn, const double* __restrict__ resid,
+                                                      double* __restrict__ qbar) {
+  const int lm = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
   if (lm >= nlm) return;
   const int m = lm_m[lm];
+  const double* P = plm + (size_t)lm * nlat;
   double br = 0.0, bi = 0.0;
-  for (int s = 0; s < nsite; ++s) {
+  for (int s = lane; s < nsite; s += 32) {
     const int g = site[s], j = g / nphi, i = g % nphi;
     const int t = (int)(((long long)m * i) % nphi);
-    const double c = (m == 0 ? 1.0 : 2.0) * plm[(size_t)lm * nlat + j] * 2.0 * resid[s];
+    const double c = (m == 0 ? 1.0 : 2.0) * P[j] * 2.0 * resid[s];
     br += c * cs[t];
     bi -= c * sn[t];
   }
-  qbar[2 * lm] = br;
-  qbar[2 * lm + 1] = (m == 0) ? 0.0 : bi;
+  for (int o = 16; o > 0; o >>= 1) {
+    br += __shfl_down_sync(0xffffffffu, br, o);
+    bi += __shfl_down_sync(0xffffffffu, bi, o);
+  }
+  if (lane == 0) {
+    qbar[2 * lm] = br;
+    qbar[2 * lm + 1] = (m == 0) ? 0.0 : bi;
+  }
 }
 
 // apply^T: sigma_bar += (gn - gu) q_bar; surface drift adjoints dUa_bar = -q_bar,
@@ -101,81 +109,77 @@ __device__ __forceinline__ void strain_T(const double ab[4], const double bb[4],
   v1 = ab[1] - cb[1] + 0.5 * cb[2] + 0.5 * c3;
 }
 
-// advance^T of the spectrally advanced (1-D) elements, one thread per (slot,
-// re/im), elements in order: lam_new = (1 - M) lam; the strain adjoint
-// -2 mu M lam goes to the nodal drift adjoints (this thread owns the column)
-// and to sigma_bar through the unit-load response.
-__global__ void k_adv1d_T(int ne, int nr, int nk, double dt, const int* __restrict__ kdeg,
-                          const int* __restrict__ k2lm, const double* __restrict__ Jrv,
-                          const double* __restrict__ xUn, const double* __restrict__ xVn,
-                          const double* __restrict__ mu, const double* __restrict__ MkPerDt,
-                          const char* __restrict__ active, const double* __restrict__ lam,
-                          double* __restrict__ lam_new, double* __restrict__ dUn_bar, double* __restrict__ dVn_bar,
-                          double* __restrict__ sbar) {
-  const int k = blockIdx.x * blockDim.x + threadIdx.x, ri = blockIdx.y;
-  if (k >= nk) return;
-  const int l = kdeg[k], lm = k2lm[k];
+// advance^T of the spectrally advanced (1-D) elements, a thread per (slot,
+// element, re/im): lam_new = (1 - M) lam; the strain adjoint -2 mu M lam,
+// transposed through the strain coefficients, kept per element as
+// E[c][ri][e][k] (c: U0, U1, V0, V1 and the element's sigma_bar share)
+__global__ void __launch_bounds__(256) k_adv1d_T_elem(int ne, int nr, int nk, double dt,
+                                                      const int* __restrict__ kdeg, const double* __restrict__ Jrv,
+                                                      const double* __restrict__ xUn, const double* __restrict__ xVn,
+                                                      const double* __restrict__ mu,
+                                                      const double* __restrict__ MkPerDt,
+                                                      const char* __restrict__ active,
+                                                      const double* __restrict__ lam, double* __restrict__ lam_new,
+                                                      double* __restrict__ E) {
+  const int k = blockIdx.x * 32 + threadIdx.x, e = blockIdx.y * 8 + threadIdx.y, ri = blockIdx.z;
+  if (k >= nk || e >= ne) return;
+  const size_t plane = (size_t)2 * ne * nk, at = ((size_t)ri * ne + e) * nk + k;
+  if (!active[e]) {
+    for (int c = 0; c < 5; ++c) E[c * plane + at] = 0.0;
+    return;
+  }
+  const int l = kdeg[k];
   const double J = Jrv[l];
+  const double Me = MkPerDt[e] * dt, om = 1.0 - Me, two_muM = 2.0 * mu[e] * Me;
+  double ab[4], bb[4], cb[4];
+#pragma unroll
+  for (int m = 0; m < 4; ++m) {
+    const size_t iA = mem_idx(0, ri, e, m, k, ne, nk), iB = mem_idx(1, ri, e, m, k, ne, nk),
+                 iC = mem_idx(2, ri, e, m, k, ne, nk);
+    const double la = lam[iA], lb = lam[iB], lc = lam[iC];
+    lam_new[iA] = om * la;
+    lam_new[iB] = om * lb;
+    lam_new[iC] = om * lc;
+    ab[m] = -two_muM * la;
+    bb[m] = -two_muM * lb;
+    cb[m] = -two_muM * lc;
+  }
+  double u0, u1, v0, v1;
+  strain_T(ab, bb, cb, J, u0, u1, v0, v1);
   const double* xu = xUn + (size_t)l * nr;
   const double* xv = xVn + (size_t)l * nr;
-  double* ub = dUn_bar + (size_t)ri * nr * nk + k;
-  double* vb = dVn_bar + (size_t)ri * nr * nk + k;
-  for (int node = 0; node < nr; ++node) {
-    ub[(size_t)node * nk] = 0.0;
-    vb[(size_t)node * nk] = 0.0;
-  }
-  double s_acc = 0.0;
-  for (int e = 0; e < ne; ++e) {
-    if (!active[e]) continue;
-    const double Me = MkPerDt[e] * dt, om = 1.0 - Me, two_muM = 2.0 * mu[e] * Me;
-    double ab[4], bb[4], cb[4];
-#pragma unroll
-    for (int m = 0; m < 4; ++m) {
-      const size_t iA = mem_idx(0, ri, e, m, k, ne, nk), iB = mem_idx(1, ri, e, m, k, ne, nk),
-                   iC = mem_idx(2, ri, e, m, k, ne, nk);
-      const double la = lam[iA], lb = lam[iB], lc = lam[iC];
-      lam_new[iA] = om * la;
-      lam_new[iB] = om * lb;
-      lam_new[iC] = om * lc;
-      ab[m] = -two_muM * la;
-      bb[m] = -two_muM * lb;
-      cb[m] = -two_muM * lc;
-    }
-    double u0, u1, v0, v1;
-    strain_T(ab, bb, cb, J, u0, u1, v0, v1);
-    ub[(size_t)e * nk] += u0;
-    ub[(size_t)(e + 1) * nk] += u1;
-    vb[(size_t)e * nk] += v0;
-    vb[(size_t)(e + 1) * nk] += v1;
-    s_acc += u0 * xu[e] + u1 * xu[e + 1] + v0 * xv[e] + v1 * xv[e + 1];
-  }
-  sbar[2 * lm + ri] += s_acc;
+  E[0 * plane + at] = u0;
+  E[1 * plane + at] = u1;
+  E[2 * plane + at] = v0;
+  E[3 * plane + at] = v1;
+  E[4 * plane + at] = u0 * xu[e] + u1 * xu[e + 1] + v0 * xv[e] + v1 * xv[e + 1];
 }
 
-// transposed band solve with the dgbtf2 factor (A = P L U): U^T, then L^T with
-// the row interchanges applied in reverse; right-hand side stride st
-__device__ void band_solve_T_strided(const double* __restrict__ ab, int ldab, int n, int kl, int kv,
-                                     const int* __restrict__ ipiv, double* x, size_t st) {
-#define AB(row1, col1) ab[(size_t)((col1)-1) * ldab + ((row1)-1)]
-  for (int j = 1; j <= n; ++j) {
-    double t = x[(size_t)(j - 1) * st];
-    const int lm = min(kv, j - 1);
-    for (int i = 1; i <= lm; ++i) t -= AB(kv + 1 - i, j) * x[(size_t)(j - i - 1) * st];
-    x[(size_t)(j - 1) * st] = t / AB(kv + 1, j);
+// nodal drift adjoints from the two elements that share each node; the node-0
+// thread of each slot also adds the slot's sigma_bar (elements in order)
+__global__ void __launch_bounds__(256) k_adv1d_T_node(int ne, int nr, int nk, const int* __restrict__ k2lm,
+                                                      const double* __restrict__ E, double* __restrict__ dUn_bar,
+                                                      double* __restrict__ dVn_bar, double* __restrict__ sbar) {
+  const int k = blockIdx.x * 32 + threadIdx.x, node = blockIdx.y * 8 + threadIdx.y, ri = blockIdx.z;
+  if (k >= nk || node >= nr) return;
+  const size_t plane = (size_t)2 * ne * nk;
+  const double* Er = E + (size_t)ri * ne * nk + k;
+  double u = 0.0, v = 0.0;
+  if (node < ne) {
+    u += Er[0 * plane + (size_t)node * nk];
+    v += Er[2 * plane + (size_t)node * nk];
   }
-  for (int j = n - 1; j >= 1; --j) {
-    const int lm = min(kl, n - j);
-    double t = x[(size_t)(j - 1) * st];
-    for (int i = 1; i <= lm; ++i) t -= AB(kv + 1 + i, j) * x[(size_t)(j + i - 1) * st];
-    x[(size_t)(j - 1) * st] = t;
-    const int p = ipiv[j - 1] + 1;
-    if (p != j) {
-      const double tmp = x[(size_t)(p - 1) * st];
-      x[(size_t)(p - 1) * st] = x[(size_t)(j - 1) * st];
-      x[(size_t)(j - 1) * st] = tmp;
-    }
+  if (node >= 1) {
+    u += Er[1 * plane + (size_t)(node - 1) * nk];
+    v += Er[3 * plane + (size_t)(node - 1) * nk];
   }
-#undef AB
+  dUn_bar[((size_t)ri * nr + node) * nk + k] = u;
+  dVn_bar[((size_t)ri * nr + node) * nk + k] = v;
+  if (node == 0) {
+    double acc = 0.0;
+    for (int e = 0; e < ne; ++e) acc += Er[4 * plane + (size_t)e * nk];
+    sbar[2 * k2lm[k] + ri] += acc;
+  }
 }
 
 // K^T: f_bar at an element's four test dofs (U_e, U_e+1, V_e, V_e+1) into the
@@ -193,34 +197,135 @@ __device__ __forceinline__ void rhs_T(const double* __restrict__ Kp, const doubl
     }
 }
 
-// drift^T for degrees >= 2, one thread per (slot, re/im)
-__global__ void k_drift_T(int ne, int nr, int nd, int nk, const int* __restrict__ kdeg, const double* __restrict__ ab,
-                          const double* __restrict__ drv, const double* __restrict__ dcv, const int* __restrict__ ipiv,
-                          const double* __restrict__ K, const double* __restrict__ dUn_bar,
-                          const double* __restrict__ dVn_bar, const double* __restrict__ surf_bar,
-                          double* __restrict__ w, double* __restrict__ lam_new) {
+// Transposed solve of one right-hand side with the degree's dgbtf2 factor
+// (A = P L U; kl = 6, kv = 12), x with element stride st, sliding windows in
+// registers. U^T sweep (forward): x_j = (z_j - sum_{i<=12} U(j-i, j) x_{j-i}) /
+// U(j, j), the 12 previous values held in w[]. L^T sweep (backward, pivots
+// undone): x_j -= sum_{i<=6} L(j+i, j) x_{j+i}, then swap x_j and x_{ipiv_j};
+// a value leaves the 7-value window v[] once no later swap can reach it.
+__device__ __forceinline__ void band_solve_T_window(const double* __restrict__ ab, int n,
+                                                    const int* __restrict__ ipiv, double* x, size_t st) {
+  constexpr int KL = 6, KV = 12, LD = VG_LDAB;
+  double w[KV], cu[KV + 1], cn[KV + 1];
+#pragma unroll
+  for (int i = 0; i < KV; ++i) w[i] = 0.0;
+#pragma unroll
+  for (int r = 0; r <= KV; ++r) cn[r] = __ldg(&ab[r]);  // column 0: rows 0..KV (U part and diagonal)
+  double xn = x[0];
+  for (int j = 0; j < n; ++j) {  // 0-based column j; the next column is loaded one step ahead
+#pragma unroll
+    for (int r = 0; r <= KV; ++r) cu[r] = cn[r];
+    const double xj = xn;
+    if (j + 1 < n) {
+      const double* nc = ab + (size_t)(j + 1) * LD;
+#pragma unroll
+      for (int r = 0; r <= KV; ++r) cn[r] = __ldg(&nc[r]);
+      xn = x[(size_t)(j + 1) * st];
+    }
+    double t = xj;
+#pragma unroll
+    for (int i = 1; i <= KV; ++i)
+      if (i <= j) t -= cu[KV - i] * w[i - 1];
+    t = t / cu[KV];
+    x[(size_t)j * st] = t;
+#pragma unroll
+    for (int i = KV - 1; i > 0; --i) w[i] = w[i - 1];
+    w[0] = t;
+  }
+  double v[KL + 1];  // v[i] = x_{j+i}, starting at j = n - 1 (nothing beyond it)
+  v[0] = x[(size_t)(n - 1) * st];
+#pragma unroll
+  for (int i = 1; i <= KL; ++i) v[i] = 0.0;
+  double ln[KL], lc[KL];
+  int pn = 0;
+  if (n >= 2) {
+    const double* c0 = ab + (size_t)(n - 2) * LD;
+#pragma unroll
+    for (int i = 0; i < KL; ++i) ln[i] = __ldg(&c0[KV + 1 + i]);
+    pn = ipiv[n - 2];
+  }
+  double xl = (n >= 2) ? x[(size_t)(n - 2) * st] : 0.0;
+  for (int j = n - 2; j >= 0; --j) {
+#pragma unroll
+    for (int i = 0; i < KL; ++i) lc[i] = ln[i];
+    const int pj = pn;
+    const double xj = xl;
+    if (j >= 1) {
+      const double* c1 = ab + (size_t)(j - 1) * LD;
+#pragma unroll
+      for (int i = 0; i < KL; ++i) ln[i] = __ldg(&c1[KV + 1 + i]);
+      pn = ipiv[j - 1];
+      xl = x[(size_t)(j - 1) * st];
+    }
+    // shift the window down by one: v[i] = x_{j+i}; x_{j+1+KL} is final
+    const double out = v[KL];
+    if (j + 1 + KL <= n - 1) x[(size_t)(j + 1 + KL) * st] = out;
+#pragma unroll
+    for (int i = KL; i > 0; --i) v[i] = v[i - 1];
+    double t = xj;
+#pragma unroll
+    for (int i = 1; i <= KL; ++i)
+      if (j + i <= n - 1) t -= lc[i - 1] * v[i];
+    v[0] = t;
+    const int d = pj - j;  // 0 .. KL
+    if (d != 0) {
+      double vd = v[0];
+#pragma unroll
+      for (int i = 1; i <= KL; ++i)
+        if (i == d) {
+          vd = v[i];
+          v[i] = v[0];
+        }
+      v[0] = vd;
+    }
+  }
+#pragma unroll
+  for (int i = 0; i <= KL; ++i)
+    if (i <= n - 1) x[(size_t)i * st] = v[i];
+}
+
+// transposed solves of the drift (degrees >= 2), one thread per (slot, re/im)
+__global__ void __launch_bounds__(32) k_drift_T(int nr, int nd, int nk, const int* __restrict__ kdeg,
+                                                const double* __restrict__ ab, const double* __restrict__ dcv,
+                                                const int* __restrict__ ipiv, const double* __restrict__ dUn_bar,
+                                                const double* __restrict__ dVn_bar,
+                                                const double* __restrict__ surf_bar, double* __restrict__ w) {
   const int k = blockIdx.x * blockDim.x + threadIdx.x, ri = blockIdx.y;
   if (k >= nk) return;
   const int l = kdeg[k];
   if (l < 2) return;
-  const double* dr = drv + (size_t)(l - 2) * nd;
   const double* dc = dcv + (size_t)(l - 2) * nd;
   double* x = w + (size_t)ri * nd * nk + k;
-  for (int i = 0; i < nd; ++i) x[(size_t)i * nk] = 0.0;
   for (int node = 0; node < nr; ++node) {
-    x[(size_t)(4 * node) * nk] = dUn_bar[((size_t)ri * nr + node) * nk + k];
-    x[(size_t)(4 * node + 1) * nk] = dVn_bar[((size_t)ri * nr + node) * nk + k];
+    double xu = dUn_bar[((size_t)ri * nr + node) * nk + k], xv = dVn_bar[((size_t)ri * nr + node) * nk + k];
+    double xf = 0.0;
+    if (node == nr - 1) {
+      xu += surf_bar[(size_t)(0 + ri) * nk + k];
+      xf = surf_bar[(size_t)(2 + ri) * nk + k];
+    }
+    x[(size_t)(4 * node) * nk] = dc[4 * node] * xu;
+    x[(size_t)(4 * node + 1) * nk] = dc[4 * node + 1] * xv;
+    x[(size_t)(4 * node + 2) * nk] = dc[4 * node + 2] * xf;
+    if (node < nr - 1) x[(size_t)(4 * node + 3) * nk] = 0.0;
   }
-  x[(size_t)(4 * (nr - 1)) * nk] += surf_bar[(size_t)(0 + ri) * nk + k];
-  x[(size_t)(4 * (nr - 1) + 2) * nk] += surf_bar[(size_t)(2 + ri) * nk + k];
-  for (int i = 0; i < nd; ++i) x[(size_t)i * nk] *= dc[i];
-  band_solve_T_strided(ab + (size_t)(l - 2) * VG_LDAB * nd, VG_LDAB, nd, 6, 12, ipiv + (size_t)(l - 2) * nd, x, nk);
-  for (int e = 0; e < ne; ++e) {
-    const double fb[4] = {dr[4 * e] * x[(size_t)(4 * e) * nk], dr[4 * (e + 1)] * x[(size_t)(4 * (e + 1)) * nk],
-                          dr[4 * e + 1] * x[(size_t)(4 * e + 1) * nk],
-                          dr[4 * (e + 1) + 1] * x[(size_t)(4 * (e + 1) + 1) * nk]};
-    rhs_T(K + ((size_t)l * ne + e) * 48, fb, lam_new, ri, e, k, ne, nk);
-  }
+  band_solve_T_window(ab + (size_t)(l - 2) * VG_LDAB * nd, nd, ipiv + (size_t)(l - 2) * nd, x, nk);
+}
+
+// K^T after the transposed solves (degrees >= 2): a thread per (slot,
+// element, re/im), f_bar = dr x at the element's four test dofs
+__global__ void __launch_bounds__(256) k_rhs_T(int ne, int nd, int nk, const int* __restrict__ kdeg,
+                                               const double* __restrict__ drv, const double* __restrict__ K,
+                                               const double* __restrict__ w, double* __restrict__ lam_new) {
+  const int k = blockIdx.x * 32 + threadIdx.x, e = blockIdx.y * 8 + threadIdx.y, ri = blockIdx.z;
+  if (k >= nk || e >= ne) return;
+  const int l = kdeg[k];
+  if (l < 2) return;
+  const double* dr = drv + (size_t)(l - 2) * nd;
+  const double* x = w + (size_t)ri * nd * nk + k;
+  const double fb[4] = {dr[4 * e] * x[(size_t)(4 * e) * nk], dr[4 * (e + 1)] * x[(size_t)(4 * (e + 1)) * nk],
+                        dr[4 * e + 1] * x[(size_t)(4 * e + 1) * nk],
+                        dr[4 * (e + 1) + 1] * x[(size_t)(4 * (e + 1) + 1) * nk]};
+  rhs_T(K + ((size_t)l * ne + e) * 48, fb, lam_new, ri, e, k, ne, nk);
 }
 
 // drift^T for degree 1 (slots 0, 1; four right-hand sides): the CM projection
@@ -228,7 +333,7 @@ __global__ void k_drift_T(int ne, int nr, int nd, int nk, const int* __restrict_
 __global__ void __launch_bounds__(512) k_drift_T_deg1(int ne, int nr, int nk, int deg1_cm,
                                                       const double* __restrict__ dr1,
                                                       const double* __restrict__ null1,
-                                                      const double* __restrict__ G1, const double* __restrict__ K,
+                                                      const double* __restrict__ G1T, const double* __restrict__ K,
                                                       const double* __restrict__ dUn_bar,
                                                       const double* __restrict__ dVn_bar,
                                                       const double* __restrict__ surf_bar,
@@ -267,12 +372,32 @@ __global__ void __launch_bounds__(512) k_drift_T_deg1(int ne, int nr, int nk, in
     if (threadIdx.x < 4) xb[threadIdx.x * nrow + 2 * nr] -= s_c[threadIdx.x] / fa_n;
     __syncthreads();
   }
-  for (int t = threadIdx.x; t < 4 * ncol; t += blockDim.x) {
-    const int q = t / ncol, c = t % ncol;
-    double acc = 0.0;
-    for (int r = 0; r < nrow; ++r) acc += G1[(size_t)r * ncol + c] * xb[q * nrow + r];
-    const int node = c >> 1;
-    fb[t] = dr1[4 * node + (c & 1)] * acc;  // bh row c = dr1 * f at (node, U or V)
+  {  // f_bar = G1^T x_bar: a warp per column c (rows of G1T contiguous), lanes over r
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    for (int c = wid; c < ncol; c += nw) {
+      const double* gc = G1T + (size_t)c * nrow;
+      double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
+      for (int r = lane; r < nrow; r += 32) {
+        const double gv = gc[r];
+        a0 += gv * xb[r];
+        a1 += gv * xb[nrow + r];
+        a2 += gv * xb[2 * nrow + r];
+        a3 += gv * xb[3 * nrow + r];
+      }
+      for (int o = 16; o > 0; o >>= 1) {
+        a0 += __shfl_xor_sync(0xffffffffu, a0, o);
+        a1 += __shfl_xor_sync(0xffffffffu, a1, o);
+        a2 += __shfl_xor_sync(0xffffffffu, a2, o);
+        a3 += __shfl_xor_sync(0xffffffffu, a3, o);
+      }
+      if (lane == 0) {
+        const double sc = dr1[4 * (c >> 1) + (c & 1)];  // bh row c = dr1 * f at (node, U or V)
+        fb[c] = sc * a0;
+        fb[ncol + c] = sc * a1;
+        fb[2 * ncol + c] = sc * a2;
+        fb[3 * ncol + c] = sc * a3;
+      }
+    }
   }
   __syncthreads();
   for (int t = threadIdx.x; t < 4 * ne; t += blockDim.x) {
@@ -283,14 +408,38 @@ __global__ void __launch_bounds__(512) k_drift_T_deg1(int ne, int nr, int nk, in
   }
 }
 
+// G1T[c][r] = G1[r][c] (degree-1 Green's block, rows r < nrow, columns c < ncol)
+__global__ void k_transpose(int nrow, int ncol, const double* __restrict__ A, double* __restrict__ AT) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= nrow * ncol) return;
+  const int r = t / ncol, c = t % ncol;
+  AT[(size_t)c * nrow + r] = A[t];
+}
+
 // ------------------------------------------------------------------ host
 
 namespace {
 
 struct AdjWork {
-  DArr<double> sig, obs, resid, lam, lam_new, dUn_bar, dVn_bar, surf_bar, qbar, w, gsig, ckpt;
+  DArr<double> sig, obs, resid, lam, lam_new, dUn_bar, dVn_bar, surf_bar, qbar, w, gsig, ckpt, E, G1T;
   DArr<int> site;
 };
+
+void adj_release(void* p) { delete static_cast<AdjWork*>(p); }
+
+// the handle's work buffers, kept across calls (grown when a call needs more)
+AdjWork& work_of(vg_handle* h) {
+  if (!h->adj_work) {
+    h->adj_work = new AdjWork();
+    h->adj_release = adj_release;
+  }
+  return *static_cast<AdjWork*>(h->adj_work);
+}
+
+template <class T>
+void ensure(DArr<T>& a, size_t count) {
+  if (a.n < count) a.alloc(count);
+}
 
 struct SkipOff {  // the drift skip gate is off inside the misfit entry points
   vg_handle* h;
@@ -311,12 +460,12 @@ void upload_inputs(vg_handle* h, AdjWork& W, int nsteps, const double* sigma, in
                    const double* obs) {
   const size_t n2 = 2 * (size_t)h->grid.nlm;
   cudaStream_t s = h->stream;
-  W.sig.alloc((size_t)nsteps * n2);
+  ensure(W.sig, (size_t)nsteps * n2);
   W.sig.upload(sigma, (size_t)nsteps * n2, s);
-  W.obs.alloc((size_t)nsteps * nsite);
+  ensure(W.obs, (size_t)nsteps * nsite);
   W.obs.upload(obs, (size_t)nsteps * nsite, s);
-  W.resid.alloc((size_t)nsteps * nsite);
-  W.site.alloc(nsite);
+  ensure(W.resid, (size_t)nsteps * nsite);
+  ensure(W.site, (size_t)nsite);
   W.site.upload(site, nsite, s);
 }
 
@@ -349,17 +498,17 @@ double sum_squares(vg_handle* h, const AdjWork& W, size_t count) {
 // the handle's memory at entry, put back at exit
 struct StateGuard {
   vg_handle* h;
-  DArr<double> saved;
+  DArr<double>& saved;
   int cur;
-  explicit StateGuard(vg_handle* hh) : h(hh), cur(hh->cur) {
+  StateGuard(vg_handle* hh, DArr<double>& buf) : h(hh), saved(buf), cur(hh->cur) {
     const size_t S = h->d_mem[h->cur].n;
-    saved.alloc(S);
+    ensure(saved, S);
     VG_CUDA(cudaMemcpyAsync(saved.p, h->d_mem[h->cur].p, S * sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
   }
   void restore() {
     h->cur = cur;
-    VG_CUDA(cudaMemcpyAsync(h->d_mem[h->cur].p, saved.p, saved.n * sizeof(double), cudaMemcpyDeviceToDevice,
-                            h->stream));
+    VG_CUDA(cudaMemcpyAsync(h->d_mem[h->cur].p, saved.p, h->d_mem[h->cur].n * sizeof(double),
+                            cudaMemcpyDeviceToDevice, h->stream));
     compute_mem_norm(h, h->cur);
     h->mem_norm = read_mem_norm(h, h->cur);
   }
@@ -371,8 +520,8 @@ double misfit_dev(vg_handle* h, int nsteps, double dt, const double* sigma, int 
                   const double* obs) {
   check_args(h, nsteps, dt, nsite, site);
   SkipOff skip(h);
-  StateGuard guard(h);
-  AdjWork W;
+  AdjWork& W = work_of(h);
+  StateGuard guard(h, W.lam_new);
   upload_inputs(h, W, nsteps, sigma, nsite, site, obs);
   compute_mem_norm(h, h->cur);
   for (int n = 0; n < nsteps; ++n) fwd_step(h, W, n, nsite, dt);
@@ -388,18 +537,18 @@ double misfit_grad_dev(vg_handle* h, int nsteps, double dt, const double* sigma,
     throw Error("vg_misfit_grad: elements with lateral viscosity are not differentiated yet");
   if (ckpt < 1) throw Error("vg_misfit_grad: ckpt_every must be >= 1");
   SkipOff skip(h);
-  StateGuard guard(h);
   const Grid& G = h->grid;
   cudaStream_t s = h->stream;
   const size_t n2 = 2 * (size_t)G.nlm, S = h->d_mem[0].n;
   const int nk = h->nk, nr = h->nr, ne = h->ne, nd = h->ndof;
-  AdjWork W;
+  AdjWork& W = work_of(h);
+  const int cur0 = h->cur;  // the entry state is checkpoint 0, put back at the end
   upload_inputs(h, W, nsteps, sigma, nsite, site, obs);
   // forward sweep with checkpoints of the memory every `ckpt` steps (the
   // reverse sweep recomputes a segment from its checkpoint when it needs the
   // states; the transposes of the 1-D step do not depend on them)
   const int nck = (nsteps + ckpt - 1) / ckpt;
-  W.ckpt.alloc((size_t)nck * S);
+  ensure(W.ckpt, (size_t)nck * S);
   compute_mem_norm(h, h->cur);
   for (int n = 0; n < nsteps; ++n) {
     if (n % ckpt == 0)
@@ -409,37 +558,53 @@ double misfit_grad_dev(vg_handle* h, int nsteps, double dt, const double* sigma,
   }
   const double J = sum_squares(h, W, (size_t)nsteps * nsite);
   // reverse sweep
-  W.lam.alloc(S);
-  W.lam_new.alloc(S);
-  W.dUn_bar.alloc((size_t)2 * nr * nk);
-  W.dVn_bar.alloc((size_t)2 * nr * nk);
-  W.surf_bar.alloc((size_t)4 * nk);
-  W.qbar.alloc(n2);
-  W.w.alloc((size_t)2 * nd * nk);
-  W.gsig.alloc((size_t)nsteps * n2);
-  const dim3 kg((nk + 127) / 128, 2);
+  ensure(W.lam, S);
+  ensure(W.lam_new, S);
+  ensure(W.dUn_bar, (size_t)2 * nr * nk);
+  ensure(W.dVn_bar, (size_t)2 * nr * nk);
+  ensure(W.surf_bar, (size_t)4 * nk);
+  ensure(W.qbar, n2);
+  ensure(W.w, (size_t)2 * nd * nk);
+  ensure(W.gsig, (size_t)nsteps * n2);
+  VG_CUDA(cudaMemsetAsync(W.lam.p, 0, S * sizeof(double), s));  // no terminal cost: lam_N = 0
+  VG_CUDA(cudaMemsetAsync(W.gsig.p, 0, (size_t)nsteps * n2 * sizeof(double), s));
+  const dim3 kg((nk + 31) / 32, 2);
+  const dim3 eg((nk + 31) / 32, (ne + 7) / 8, 2), ng_((nk + 31) / 32, (nr + 7) / 8, 2);
+  ensure(W.E, (size_t)5 * 2 * ne * nk);
+  {
+    const int nrow = 2 * nr + 1, ncol = 2 * nr;
+    if (W.G1T.n != (size_t)nrow * ncol) {
+      W.G1T.alloc((size_t)nrow * ncol);
+      k_transpose<<<(nrow * ncol + 255) / 256, 256, 0, s>>>(nrow, ncol, h->d_G1.p, W.G1T.p);
+      VG_CUDA(cudaGetLastError());
+    }
+  }
   const size_t shm1 = (size_t)(4 * (2 * nr + 1) + 4 * 2 * nr) * sizeof(double);
   for (int n = nsteps - 1; n >= 0; --n) {
     double* sbar = W.gsig.p + (size_t)n * n2;
-    k_site_synth_T<<<(G.nlm + 127) / 128, 128, 0, s>>>(nsite, W.site.p, G.nlm, G.nlat, G.nphi, G.d_lm_m.p, G.d_plm.p,
+    k_site_synth_T<<<(G.nlm * 32 + 255) / 256, 256, 0, s>>>(nsite, W.site.p, G.nlm, G.nlat, G.nphi, G.d_lm_m.p, G.d_plm.p,
                                                       G.d_cos.p, G.d_sin.p, W.resid.p + (size_t)n * nsite, W.qbar.p);
     VG_CUDA(cudaMemsetAsync(W.surf_bar.p, 0, W.surf_bar.n * sizeof(double), s));
     k_apply_T<<<(G.nlm + 255) / 256, 256, 0, s>>>(G.nlm, nk, h->g, G.d_lm_l.p, h->d_lm2k.p, h->d_gu.p, h->d_gn.p,
                                                  W.qbar.p, sbar, W.surf_bar.p);
-    k_adv1d_T<<<kg, 128, 0, s>>>(ne, nr, nk, dt, h->d_kdeg.p, h->d_k2lm.p, h->d_Jr.p, h->d_xUn.p, h->d_xVn.p,
-                                 h->d_mu.p, h->d_MkPerDt.p, h->d_active1d.p, W.lam.p, W.lam_new.p, W.dUn_bar.p,
-                                 W.dVn_bar.p, sbar);
-    k_drift_T<<<kg, 128, 0, s>>>(ne, nr, nd, nk, h->d_kdeg.p, h->d_ab.p, h->d_dr.p, h->d_dc.p, h->d_ipiv.p,
-                                 h->d_Krhs.p, W.dUn_bar.p, W.dVn_bar.p, W.surf_bar.p, W.w.p, W.lam_new.p);
-    k_drift_T_deg1<<<1, 512, shm1, s>>>(ne, nr, nk, h->p.deg1_cm, h->d_dr1.p, h->d_null1.p, h->d_G1.p, h->d_Krhs.p,
+    k_adv1d_T_elem<<<eg, dim3(32, 8), 0, s>>>(ne, nr, nk, dt, h->d_kdeg.p, h->d_Jr.p, h->d_xUn.p, h->d_xVn.p,
+                                               h->d_mu.p, h->d_MkPerDt.p, h->d_active1d.p, W.lam.p, W.lam_new.p,
+                                               W.E.p);
+    k_adv1d_T_node<<<ng_, dim3(32, 8), 0, s>>>(ne, nr, nk, h->d_k2lm.p, W.E.p, W.dUn_bar.p, W.dVn_bar.p, sbar);
+    k_drift_T<<<kg, 32, 0, s>>>(nr, nd, nk, h->d_kdeg.p, h->d_ab.p, h->d_dc.p, h->d_ipiv.p, W.dUn_bar.p,
+                                W.dVn_bar.p, W.surf_bar.p, W.w.p);
+    k_rhs_T<<<eg, dim3(32, 8), 0, s>>>(ne, nd, nk, h->d_kdeg.p, h->d_dr.p, h->d_Krhs.p, W.w.p, W.lam_new.p);
+    k_drift_T_deg1<<<1, 512, shm1, s>>>(ne, nr, nk, h->p.deg1_cm, h->d_dr1.p, h->d_null1.p, W.G1T.p, h->d_Krhs.p,
                                         W.dUn_bar.p, W.dVn_bar.p, W.surf_bar.p, W.lam_new.p);
-    h->n_launch += 5;
+    h->n_launch += 7;
     VG_CUDA(cudaGetLastError());
     std::swap(W.lam.p, W.lam_new.p);
   }
   if (grad_sigma) W.gsig.download(grad_sigma, (size_t)nsteps * n2, s);
-  VG_CUDA(cudaStreamSynchronize(s));
-  guard.restore();
+  h->cur = cur0;
+  VG_CUDA(cudaMemcpyAsync(h->d_mem[h->cur].p, W.ckpt.p, S * sizeof(double), cudaMemcpyDeviceToDevice, s));
+  compute_mem_norm(h, h->cur);
+  h->mem_norm = read_mem_norm(h, h->cur);
   return J;
 }
 

@@ -197,8 +197,12 @@ struct vg_handle {
   // split-precision tensor-core plan of the 3-D advance (owned, opaque here)
   void* tc_plan = nullptr;
   void (*tc_plan_release)(void*) = nullptr;
+  // work buffers of the misfit / adjoint entry points (owned, opaque here)
+  void* adj_work = nullptr;
+  void (*adj_release)(void*) = nullptr;
   ~vg_handle() {
     if (tc_plan_release) tc_plan_release(tc_plan);
+    if (adj_release) adj_release(adj_work);
   }
 };
 
