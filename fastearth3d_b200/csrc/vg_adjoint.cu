@@ -16,6 +16,11 @@
 //   strain of -2 mu M), drift^T (the dissipative map's transpose after an
 //   equilibrated transposed band solve, U^T then L^T with the pivots undone;
 //   degree 1 through the transposed Green's block and CM projection).
+// With 3-D elements (FP64 path) the reverse sweep also runs the transposed
+// pseudo-spectral advance (vg_visc3d.cu: scatter^T, analysis^T, longitude^T,
+// synthesis^T, gather^T), which needs each step's state: a segment is
+// recomputed from its checkpoint, and d J / d(M dt) on the grid gives the
+// gradient with respect to the lateral log10-viscosity.
 // All in FP64. The drift skip gate is off inside these entry points: with a
 // zero threshold it only skips slots whose memory is exactly zero, whose drift
 // is zero anyway, so the forward stays exactly linear.
@@ -422,6 +427,7 @@ namespace {
 
 struct AdjWork {
   DArr<double> sig, obs, resid, lam, lam_new, dUn_bar, dVn_bar, surf_bar, qbar, w, gsig, ckpt, E, G1T;
+  DArr<double> ckpt_norm, seg, seg_norm, gradMdt;  // checkpoint norms, segment states, d J / d (M dt)
   DArr<int> site;
 };
 
@@ -531,10 +537,11 @@ double misfit_dev(vg_handle* h, int nsteps, double dt, const double* sigma, int 
 }
 
 double misfit_grad_dev(vg_handle* h, int nsteps, double dt, const double* sigma, int nsite, const int* site,
-                       const double* obs, int ckpt, double* grad_sigma) {
+                       const double* obs, int ckpt, double* grad_sigma, double* grad_pert) {
   check_args(h, nsteps, dt, nsite, site);
-  if (h->lat_visc && h->ne3d > 0)
-    throw Error("vg_misfit_grad: elements with lateral viscosity are not differentiated yet");
+  const bool v3 = h->lat_visc && h->ne3d > 0;
+  if (v3 && h->p.visc3d_precision != VG_VISC3D_FP64)
+    throw Error("vg_misfit_grad: the 3-D adjoint follows the FP64 path (visc3d_precision = FP64)");
   if (ckpt < 1) throw Error("vg_misfit_grad: ckpt_every must be >= 1");
   SkipOff skip(h);
   const Grid& G = h->grid;
@@ -549,11 +556,28 @@ double misfit_grad_dev(vg_handle* h, int nsteps, double dt, const double* sigma,
   // states; the transposes of the 1-D step do not depend on them)
   const int nck = (nsteps + ckpt - 1) / ckpt;
   ensure(W.ckpt, (size_t)nck * S);
+  ensure(W.ckpt_norm, (size_t)nck * nk);
   compute_mem_norm(h, h->cur);
+  auto snapshot = [&](double* st, double* nm) {  // the state and its per-slot norms (the drift's gate)
+    VG_CUDA(cudaMemcpyAsync(st, h->d_mem[h->cur].p, S * sizeof(double), cudaMemcpyDeviceToDevice, s));
+    VG_CUDA(cudaMemcpyAsync(nm, h->d_mnorm.p + (size_t)h->cur * nk, nk * sizeof(double), cudaMemcpyDeviceToDevice,
+                            s));
+  };
+  auto restore = [&](const double* st, const double* nm) {
+    VG_CUDA(cudaMemcpyAsync(h->d_mem[h->cur].p, st, S * sizeof(double), cudaMemcpyDeviceToDevice, s));
+    VG_CUDA(cudaMemcpyAsync(h->d_mnorm.p + (size_t)h->cur * nk, nm, nk * sizeof(double), cudaMemcpyDeviceToDevice,
+                            s));
+  };
+  // with 3-D elements the reverse sweep needs every state; the last segment's
+  // are kept from this sweep, the others are recomputed from their checkpoints
+  const int last0 = ((nsteps - 1) / ckpt) * ckpt;
+  if (v3) {
+    ensure(W.seg, (size_t)ckpt * S);
+    ensure(W.seg_norm, (size_t)ckpt * nk);
+  }
   for (int n = 0; n < nsteps; ++n) {
-    if (n % ckpt == 0)
-      VG_CUDA(cudaMemcpyAsync(W.ckpt.p + (size_t)(n / ckpt) * S, h->d_mem[h->cur].p, S * sizeof(double),
-                              cudaMemcpyDeviceToDevice, s));
+    if (n % ckpt == 0) snapshot(W.ckpt.p + (size_t)(n / ckpt) * S, W.ckpt_norm.p + (size_t)(n / ckpt) * nk);
+    if (v3 && n >= last0) snapshot(W.seg.p + (size_t)(n - last0) * S, W.seg_norm.p + (size_t)(n - last0) * nk);
     fwd_step(h, W, n, nsite, dt);
   }
   const double J = sum_squares(h, W, (size_t)nsteps * nsite);
@@ -580,8 +604,26 @@ double misfit_grad_dev(vg_handle* h, int nsteps, double dt, const double* sigma,
     }
   }
   const size_t shm1 = (size_t)(4 * (2 * nr + 1) + 4 * 2 * nr) * sizeof(double);
+  if (v3) {
+    const size_t ngm = (size_t)h->ne3d * G.ng;
+    ensure(W.gradMdt, ngm);
+    VG_CUDA(cudaMemsetAsync(W.gradMdt.p, 0, ngm * sizeof(double), s));
+  }
   for (int n = nsteps - 1; n >= 0; --n) {
     double* sbar = W.gsig.p + (size_t)n * n2;
+    if (v3) {
+      // the states of this step's segment, recomputed from its checkpoint
+      const int c = n / ckpt, n0 = c * ckpt;
+      if (n < last0 && n % ckpt == ckpt - 1) {
+        restore(W.ckpt.p + (size_t)c * S, W.ckpt_norm.p + (size_t)c * nk);
+        for (int q = n0; q <= n; ++q) {
+          snapshot(W.seg.p + (size_t)(q - n0) * S, W.seg_norm.p + (size_t)(q - n0) * nk);
+          fwd_step(h, W, q, nsite, dt);
+        }
+      }
+      restore(W.seg.p + (size_t)(n - n0) * S, W.seg_norm.p + (size_t)(n - n0) * nk);
+      launch_drift(h);  // drift of tau_n, the gather's strain
+    }
     k_site_synth_T<<<(G.nlm * 32 + 255) / 256, 256, 0, s>>>(nsite, W.site.p, G.nlm, G.nlat, G.nphi, G.d_lm_m.p, G.d_plm.p,
                                                       G.d_cos.p, G.d_sin.p, W.resid.p + (size_t)n * nsite, W.qbar.p);
     VG_CUDA(cudaMemsetAsync(W.surf_bar.p, 0, W.surf_bar.n * sizeof(double), s));
@@ -590,6 +632,7 @@ double misfit_grad_dev(vg_handle* h, int nsteps, double dt, const double* sigma,
     k_adv1d_T_elem<<<eg, dim3(32, 8), 0, s>>>(ne, nr, nk, dt, h->d_kdeg.p, h->d_Jr.p, h->d_xUn.p, h->d_xVn.p,
                                                h->d_mu.p, h->d_MkPerDt.p, h->d_active1d.p, W.lam.p, W.lam_new.p,
                                                W.E.p);
+    if (v3) visc3d_adjoint(h, W.sig.p + (size_t)n * n2, dt, W.lam.p, W.lam_new.p, W.E.p, W.gradMdt.p);
     k_adv1d_T_node<<<ng_, dim3(32, 8), 0, s>>>(ne, nr, nk, h->d_k2lm.p, W.E.p, W.dUn_bar.p, W.dVn_bar.p, sbar);
     k_drift_T<<<kg, 32, 0, s>>>(nr, nd, nk, h->d_kdeg.p, h->d_ab.p, h->d_dc.p, h->d_ipiv.p, W.dUn_bar.p,
                                 W.dVn_bar.p, W.surf_bar.p, W.w.p);
@@ -601,6 +644,23 @@ double misfit_grad_dev(vg_handle* h, int nsteps, double dt, const double* sigma,
     std::swap(W.lam.p, W.lam_new.p);
   }
   if (grad_sigma) W.gsig.download(grad_sigma, (size_t)nsteps * n2, s);
+  if (grad_pert) {
+    // d J / d pert = d J / d(M dt) * (-ln 10) M dt on the 3-D elements' grid,
+    // (nphi, nlat, ne) like vg_enable_visc3d's input; zero elsewhere
+    const size_t ng = G.ng;
+    std::fill(grad_pert, grad_pert + (size_t)ne * ng, 0.0);
+    if (v3) {
+      std::vector<double> gm((size_t)h->ne3d * ng), rate((size_t)h->ne3d * ng);
+      W.gradMdt.download(gm.data(), gm.size(), s);
+      h->d_MkPerDt3.download(rate.data(), rate.size(), s);
+      VG_CUDA(cudaStreamSynchronize(s));
+      for (int ei = 0; ei < h->ne3d; ++ei)
+        for (size_t g = 0; g < ng; ++g) {
+          const size_t q = (size_t)ei * ng + g;
+          grad_pert[(size_t)h->e3d_h[ei] * ng + g] = -std::log(10.0) * rate[q] * dt * gm[q];
+        }
+    }
+  }
   h->cur = cur0;
   VG_CUDA(cudaMemcpyAsync(h->d_mem[h->cur].p, W.ckpt.p, S * sizeof(double), cudaMemcpyDeviceToDevice, s));
   compute_mem_norm(h, h->cur);
@@ -624,11 +684,12 @@ extern "C" int vg_misfit(vg_handle* h, int nsteps, double dt_s, const double* si
 }
 
 extern "C" int vg_misfit_grad(vg_handle* h, int nsteps, double dt_s, const double* sigma_lm, int nsite,
-                              const int* site, const double* obs, int ckpt_every, double* J, double* grad_sigma) {
+                              const int* site, const double* obs, int ckpt_every, double* J, double* grad_sigma,
+                              double* grad_pert) {
   if (!h) return 1;
   try {
     if (!sigma_lm || !obs || !J) throw vg::Error("vg_misfit_grad: null argument");
-    *J = vg::misfit_grad_dev(h, nsteps, dt_s, sigma_lm, nsite, site, obs, ckpt_every, grad_sigma);
+    *J = vg::misfit_grad_dev(h, nsteps, dt_s, sigma_lm, nsite, site, obs, ckpt_every, grad_sigma, grad_pert);
     return 0;
   } catch (const std::exception& ex) {
     h->err = ex.what();

@@ -122,6 +122,7 @@ __global__ void __launch_bounds__(256) k_v3_gather(V3Args A, T* __restrict__ X) 
 // row(l, m) = kbeg[l] + m for l >= 1, the zero row nk for l = 0.
 struct GemmArgs {
   int mode, lmax, nlat, nk, ncf;
+  int nin;  // synthesis input channels per slot row (4: the gathered channels; 6: per product)
   const int *mbeg, *kbeg;
   const double* T[6];  // per product: table [lm][j]
   int chan[6];         // synthesis: input channel per product
@@ -167,7 +168,7 @@ __global__ void __launch_bounds__(256) k_v3_gemm(GemmArgs A) {
       if (gk < kdim && gn < A.ncf) {
         if (A.mode == 0) {
           int row = slot_row(A.kbeg, m + gk, m, A.nk);
-          v = A.in[(size_t)row * 4 * A.ncf + (size_t)A.chan[p] * A.ncf + gn];
+          v = A.in[(size_t)row * A.nin * A.ncf + (size_t)A.chan[p] * A.ncf + gn];
         } else {
           v = A.in[(((size_t)m * A.nlat + gk) * 6 + p) * A.ncf + gn];
         }
@@ -473,6 +474,7 @@ void visc3d_advance(vg_handle* h, const double* d_sigma, double dt) {
   S.nlat = G.nlat;
   S.nk = h->nk;
   S.ncf = ncf;
+  S.nin = 4;
   S.mbeg = G.d_mbeg.p;
   S.kbeg = h->d_kbeg.p;
   const double* st[6] = {G.d_plm.p, G.d_dplm.p, G.d_plm.p, G.d_plm.p, h->d_G6.p, h->d_H6.p};
@@ -523,6 +525,309 @@ void visc3d_advance(vg_handle* h, const double* d_sigma, double dt) {
   PhaseScope pc(h, VG_PH_V3_SCATTER);
   k_v3_scatter<double><<<gg, dim3(32, 8), 0, s>>>(A, h->d_dy.p, h->d_n6.p);
   ++h->n_launch;
+  VG_CUDA(cudaGetLastError());
+}
+
+// ------------------------------------------------------------------ adjoint
+
+// scatter^T: the memory adjoint of a 3-D element's increment back to the six
+// products' analysis outputs (the normalisations of k_v3_scatter transposed)
+__global__ void __launch_bounds__(256) k_v3_scatter_T(V3Args A, const double* __restrict__ lam,
+                                                      const double* __restrict__ n6, double* __restrict__ dyb) {
+  const int k = blockIdx.x * 32 + threadIdx.x, ei = blockIdx.y * 8 + threadIdx.y;
+  if (k >= A.nk || ei >= A.ne3d) return;
+  const int e = A.e3d[ei], l = A.kdeg[k];
+  const double J = A.Jr[l], nn = n6[l];
+  double* row = dyb + (size_t)k * 6 * A.ncf;
+  for (int s3 = 0; s3 < 3; ++s3) {
+    const int f = 3 * ei + s3;
+    double L[4][2];
+    for (int ri = 0; ri < 2; ++ri)
+      for (int lam_ = 0; lam_ < 4; ++lam_) L[lam_][ri] = lam[mem_idx(s3, ri, e, lam_, k, A.ne, A.nk)];
+    double q[6][2];
+    q[0][0] = L[0][0];
+    q[0][1] = L[0][1];
+    q[1][0] = L[1][0] / J;
+    q[1][1] = L[1][1] / J;
+    q[2][0] = -L[1][1] / J;
+    q[2][1] = L[1][0] / J;
+    q[3][0] = L[2][0] / (-2.0 * J);
+    q[3][1] = L[2][1] / (-2.0 * J);
+    q[4][0] = nn != 0.0 ? L[3][0] / nn : 0.0;
+    q[4][1] = nn != 0.0 ? L[3][1] / nn : 0.0;
+    q[5][0] = nn != 0.0 ? -2.0 * L[3][1] / nn : 0.0;
+    q[5][1] = nn != 0.0 ? 2.0 * L[3][0] / nn : 0.0;
+    for (int p = 0; p < 6; ++p)
+      for (int ri = 0; ri < 2; ++ri) row[(size_t)p * A.ncf + 2 * f + ri] = q[p][ri];
+  }
+}
+
+// longitude pass transposed, one CTA per (latitude j, 3-D element): the three
+// shape fields' forward grid values g (from the forward products Yf) and the
+// adjoint chain on Yb in place: analysis-input scales^T, forward DFT^T,
+// times -M dt, inverse DFT^T, dyadic components^T; and
+// d J / d (M dt)(j, i) += -sum over components and shapes of G_bar g
+__global__ void __launch_bounds__(256) k_v3_lon_T(const double* __restrict__ Yf, double* __restrict__ Yb, int nlat,
+                                                  int nphi, int M, int nf, double dt,
+                                                  const double* __restrict__ Mk3rate,
+                                                  const double* __restrict__ cs, const double* __restrict__ sn,
+                                                  const double* __restrict__ invsin, double* __restrict__ gradMdt) {
+  extern __shared__ double sm[];
+  constexpr int FT = 3;
+  const int j = blockIdx.x, ei = blockIdx.y, f0 = 3 * ei;
+  const int ncf = 2 * nf, half = nphi / 2, R = 6 * FT;
+  double* Cc = sm;                        // [R][M][2] component coefficients (forward, then adjoint)
+  double* gf = sm + (size_t)R * M * 2;    // [R][nphi] forward grid
+  double* Gb = gf + (size_t)R * nphi;     // [R][nphi] adjoint grid
+  const double is = invsin[j];
+  const double scl = 2.0 * PI / (double)nphi;
+  // 1. forward dyadic coefficients from the forward products
+  for (int t = threadIdx.x; t < FT * M; t += blockDim.x) {
+    const int fl = t / M, m = t % M;
+    double pr[6][2];
+    for (int p = 0; p < 6; ++p)
+      for (int ri = 0; ri < 2; ++ri) pr[p][ri] = Yf[(((size_t)m * nlat + j) * 6 + p) * ncf + (f0 + fl) * 2 + ri];
+    const double ms = m * is;
+    const double comp[6][2] = {{pr[0][0], pr[0][1]},
+                               {pr[1][0], pr[1][1]},
+                               {-ms * pr[2][1], ms * pr[2][0]},
+                               {pr[3][0] + pr[4][0], pr[3][1] + pr[4][1]},
+                               {pr[3][0] - pr[4][0], pr[3][1] - pr[4][1]},
+                               {-4.0 * pr[5][1], 4.0 * pr[5][0]}};
+    for (int c = 0; c < 6; ++c) {
+      Cc[((c * FT + fl) * M + m) * 2] = comp[c][0];
+      Cc[((c * FT + fl) * M + m) * 2 + 1] = comp[c][1];
+    }
+  }
+  __syncthreads();
+  // 2. forward inverse DFT (g, before the factor -M dt)
+  for (int t = threadIdx.x; t < R * half; t += blockDim.x) {
+    const int row = t / half, i = t % half;
+    const double* c = Cc + (size_t)row * M * 2;
+    double ev = 0.0, od = 0.0;
+    int tw = i;
+    for (int m = 1; m < M; ++m) {
+      const double v = c[2 * m] * __ldg(&cs[tw]) - c[2 * m + 1] * __ldg(&sn[tw]);
+      if (m & 1)
+        od += v;
+      else
+        ev += v;
+      tw += i;
+      if (tw >= nphi) tw -= nphi;
+    }
+    const double a = c[0] + 2.0 * ev, b = 2.0 * od;
+    gf[(size_t)row * nphi + i] = a + b;
+    gf[(size_t)row * nphi + i + half] = a - b;
+  }
+  __syncthreads();
+  // 3. adjoint dyadic Fourier coefficients from the analysis-input adjoints
+  for (int t = threadIdx.x; t < FT * M; t += blockDim.x) {
+    const int fl = t / M, m = t % M;
+    double o[6][2];
+    for (int q = 0; q < 6; ++q)
+      for (int ri = 0; ri < 2; ++ri) o[q][ri] = Yb[(((size_t)m * nlat + j) * 6 + q) * ncf + (f0 + fl) * 2 + ri];
+    const double ms = m * is;
+    const double Fb[6][2] = {{o[0][0], o[0][1]},
+                             {o[1][0], o[1][1]},
+                             {ms * o[2][0], ms * o[2][1]},
+                             {o[3][0] + o[4][0], o[3][1] + o[4][1]},
+                             {o[3][0] - o[4][0], o[3][1] - o[4][1]},
+                             {o[5][0], o[5][1]}};
+    for (int c = 0; c < 6; ++c) {
+      Cc[((c * FT + fl) * M + m) * 2] = Fb[c][0];
+      Cc[((c * FT + fl) * M + m) * 2 + 1] = Fb[c][1];
+    }
+  }
+  __syncthreads();
+  // 4. forward DFT^T: G_bar(i) = scl sum_m (Fre cos(m phi_i) - Fim sin(m phi_i))
+  for (int t = threadIdx.x; t < R * half; t += blockDim.x) {
+    const int row = t / half, i = t % half;
+    const double* c = Cc + (size_t)row * M * 2;
+    double ev = c[0], od = 0.0;  // m = 0: Fre only
+    int tw = i;
+    for (int m = 1; m < M; ++m) {
+      const double v = c[2 * m] * __ldg(&cs[tw]) - c[2 * m + 1] * __ldg(&sn[tw]);
+      if (m & 1)
+        od += v;
+      else
+        ev += v;
+      tw += i;
+      if (tw >= nphi) tw -= nphi;
+    }
+    Gb[(size_t)row * nphi + i] = scl * (ev + od);
+    Gb[(size_t)row * nphi + i + half] = scl * (ev - od);
+  }
+  __syncthreads();
+  // 5. d J / d(M dt) and g_bar = -M dt G_bar (in place in Gb)
+  const double* Mr = Mk3rate + ((size_t)ei * nlat + j) * nphi;
+  for (int i = threadIdx.x; i < nphi; i += blockDim.x) {
+    double acc = 0.0;
+    for (int row = 0; row < R; ++row) acc += Gb[(size_t)row * nphi + i] * gf[(size_t)row * nphi + i];
+    gradMdt[((size_t)ei * nlat + j) * nphi + i] -= acc;
+    const double mdt = Mr[i] * dt;
+    for (int row = 0; row < R; ++row) Gb[(size_t)row * nphi + i] *= -mdt;
+  }
+  __syncthreads();
+  // 6. inverse DFT^T: c_bar(m) = w_m sum_i g_bar(i) (cos, -sin)(m phi_i), then
+  //    the dyadic components^T into the product adjoints (written over Yb)
+  for (int t = threadIdx.x; t < FT * M; t += blockDim.x) {
+    const int fl = t / M, m = t % M;
+    const double w = (m == 0) ? 1.0 : 2.0;
+    double cb[6][2];
+    for (int c = 0; c < 6; ++c) {
+      const double* g = Gb + (size_t)(c * FT + fl) * nphi;
+      double re = 0.0, im = 0.0;
+      int tw = 0;
+      const double sgn = (m & 1) ? -1.0 : 1.0;
+      for (int i = 0; i < half; ++i) {
+        const double v = g[i] + sgn * g[i + half];
+        re += v * __ldg(&cs[tw]);
+        im -= v * __ldg(&sn[tw]);
+        tw += m;
+        if (tw >= nphi) tw -= nphi;
+      }
+      cb[c][0] = w * re;
+      cb[c][1] = (m == 0) ? 0.0 : w * im;
+    }
+    const double ms = m * is;
+    const double Sb[6][2] = {{cb[0][0], cb[0][1]},
+                             {cb[1][0], cb[1][1]},
+                             {ms * cb[2][1], -ms * cb[2][0]},
+                             {cb[3][0] + cb[4][0], cb[3][1] + cb[4][1]},
+                             {cb[3][0] - cb[4][0], cb[3][1] - cb[4][1]},
+                             {4.0 * cb[5][1], -4.0 * cb[5][0]}};
+    for (int q = 0; q < 6; ++q)
+      for (int ri = 0; ri < 2; ++ri) Yb[(((size_t)m * nlat + j) * 6 + q) * ncf + (f0 + fl) * 2 + ri] = Sb[q][ri];
+  }
+}
+
+// gather^T: the synthesis-input adjoint (per product, combined into the four
+// channels) back to the memory (identity of tau + Delta plus G) and to the
+// strain, whose transposed coefficients go to the nodal drift adjoints per
+// element (E planes: U0, U1, V0, V1, sigma_bar share)
+__global__ void __launch_bounds__(256) k_v3_gather_T(V3Args A, const double* __restrict__ Rb,
+                                                     const double* __restrict__ lam, double* __restrict__ lam_new,
+                                                     double* __restrict__ E) {
+  const int k = blockIdx.x * 32 + threadIdx.x, ei = blockIdx.y * 8 + threadIdx.y;
+  if (k >= A.nk || ei >= A.ne3d) return;
+  const int e = A.e3d[ei], l = A.kdeg[k];
+  const double Jr = A.Jr[l], twoMu = 2.0 * A.mu[e];
+  const double* xu = A.xUn + (size_t)l * A.nr;
+  const double* xv = A.xVn + (size_t)l * A.nr;
+  const double* row = Rb + (size_t)k * 6 * A.ncf;
+  const size_t plane = (size_t)2 * A.ne * A.nk;
+  for (int ri = 0; ri < 2; ++ri) {
+    double eb[3][4];
+    for (int s3 = 0; s3 < 3; ++s3) {
+      const int n = (3 * ei + s3) * 2 + ri;
+      const double x[4] = {row[(size_t)0 * A.ncf + n], row[(size_t)1 * A.ncf + n] + row[(size_t)2 * A.ncf + n],
+                           row[(size_t)3 * A.ncf + n], row[(size_t)4 * A.ncf + n] + row[(size_t)5 * A.ncf + n]};
+      for (int lam_ = 0; lam_ < 4; ++lam_) {
+        const double y = (lam_ == 2) ? -Jr * x[lam_] : x[lam_];
+        const size_t idx = mem_idx(s3, ri, e, lam_, k, A.ne, A.nk);
+        lam_new[idx] = lam[idx] + y;
+        eb[s3][lam_] = twoMu * y;
+      }
+    }
+    const double b3 = (Jr <= 2.0) ? 0.0 : eb[1][3], c3 = (Jr <= 2.0) ? 0.0 : eb[2][3];
+    const double u0 = -eb[0][0] + eb[1][1] - eb[1][2] / Jr;
+    const double u1 = eb[0][0] + eb[2][1] - eb[2][2] / Jr;
+    const double v0 = -eb[0][1] - eb[1][1] + 0.5 * eb[1][2] + 0.5 * b3;
+    const double v1 = eb[0][1] - eb[2][1] + 0.5 * eb[2][2] + 0.5 * c3;
+    const size_t at = ((size_t)ri * A.ne + e) * A.nk + k;
+    E[0 * plane + at] = u0;
+    E[1 * plane + at] = u1;
+    E[2 * plane + at] = v0;
+    E[3 * plane + at] = v1;
+    E[4 * plane + at] = u0 * xu[e] + u1 * xu[e + 1] + v0 * xv[e] + v1 * xv[e + 1];
+  }
+}
+
+void visc3d_adjoint(vg_handle* h, const double* d_sigma, double dt, const double* lam, double* lam_new, double* E,
+                    double* gradMdt) {
+  if (h->ne3d == 0) return;
+  if (h->p.visc3d_precision != VG_VISC3D_FP64)
+    throw Error("vg_misfit_grad: the 3-D adjoint follows the FP64 path (visc3d_precision = FP64)");
+  const Grid& G = h->grid;
+  cudaStream_t s = h->stream;
+  const int nf = 3 * h->ne3d, ncf = 2 * nf;
+  const size_t ny = (size_t)G.M * G.nlat * 6 * ncf, nr6 = (size_t)(h->nk + 1) * 6 * ncf;
+  if (h->d_v3a_Yf.n != ny) {
+    h->d_v3a_Yf.alloc(ny);
+    h->d_v3a_Yb.alloc(ny);
+    h->d_v3a_dyb.alloc(nr6);  // slot row nk (degree 0) stays zero
+    h->d_v3a_Rb.alloc(nr6);
+  }
+  V3Args A;
+  A.mem = h->d_mem[h->cur].p;
+  A.nxt = nullptr;
+  A.sigma = d_sigma;
+  A.kdeg = h->d_kdeg.p;
+  A.k2lm = h->d_k2lm.p;
+  A.e3d = h->d_e3d.p;
+  A.Jr = h->d_Jr.p;
+  A.xUn = h->d_xUn.p;
+  A.xVn = h->d_xVn.p;
+  A.dUn = h->d_dUn.p;
+  A.dVn = h->d_dVn.p;
+  A.mu = h->d_mu.p;
+  A.ne = h->ne;
+  A.nr = h->nr;
+  A.nk = h->nk;
+  A.ne3d = h->ne3d;
+  A.nf = nf;
+  A.ncf = ncf;
+  dim3 gg((h->nk + 31) / 32, (h->ne3d + 7) / 8);
+  // forward products of this step (recomputed from its state and drift)
+  k_v3_gather<double><<<gg, dim3(32, 8), 0, s>>>(A, h->d_X.p);
+  GemmArgs S;
+  S.mode = 0;
+  S.lmax = G.lmax;
+  S.nlat = G.nlat;
+  S.nk = h->nk;
+  S.ncf = ncf;
+  S.nin = 4;
+  S.mbeg = G.d_mbeg.p;
+  S.kbeg = h->d_kbeg.p;
+  const double* st[6] = {G.d_plm.p, G.d_dplm.p, G.d_plm.p, G.d_plm.p, h->d_G6.p, h->d_H6.p};
+  const double* at[6] = {h->d_wP.p, h->d_wD.p, h->d_wP.p, h->d_wP.p, h->d_wG.p, h->d_wH.p};
+  const int sc[6] = {0, 1, 1, 2, 3, 3};
+  for (int p = 0; p < 6; ++p) {
+    S.T[p] = st[p];
+    S.chan[p] = sc[p];
+  }
+  S.in = h->d_X.p;
+  S.out = h->d_v3a_Yf.p;
+  dim3 sgrid((ncf + GB_N - 1) / GB_N, (G.nlat + GB_M - 1) / GB_M, G.M * 6);
+  k_v3_gemm<<<sgrid, 256, 0, s>>>(S);
+  // adjoint chain
+  k_v3_scatter_T<<<gg, dim3(32, 8), 0, s>>>(A, lam, h->d_n6.p, h->d_v3a_dyb.p);
+  GemmArgs Ab = S;  // analysis^T: the weighted tables, per-product input rows
+  Ab.nin = 6;
+  for (int p = 0; p < 6; ++p) {
+    Ab.T[p] = at[p];
+    Ab.chan[p] = p;
+  }
+  Ab.in = h->d_v3a_dyb.p;
+  Ab.out = h->d_v3a_Yb.p;
+  k_v3_gemm<<<sgrid, 256, 0, s>>>(Ab);
+  const size_t lsm = (size_t)(18 * G.M * 2 + 2 * 18 * G.nphi) * sizeof(double);
+  static bool lon_attr = false;
+  if (!lon_attr) {
+    VG_CUDA(cudaFuncSetAttribute(k_v3_lon_T, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+    lon_attr = true;
+  }
+  if (lsm > 200 * 1024) throw Error("vg_misfit_grad: grid too large for the transposed longitude pass");
+  k_v3_lon_T<<<dim3(G.nlat, h->ne3d), 256, lsm, s>>>(h->d_v3a_Yf.p, h->d_v3a_Yb.p, G.nlat, G.nphi, G.M, nf, dt,
+                                                       h->d_MkPerDt3.p, G.d_cos.p, G.d_sin.p, G.d_invsin.p, gradMdt);
+  GemmArgs Sb = S;  // synthesis^T: the unweighted tables, per product out
+  Sb.mode = 1;
+  Sb.in = h->d_v3a_Yb.p;
+  Sb.out = h->d_v3a_Rb.p;
+  dim3 agrid((ncf + GB_N - 1) / GB_N, (G.M + GB_M - 1) / GB_M, G.M * 6);
+  k_v3_gemm<<<agrid, 256, 0, s>>>(Sb);
+  k_v3_gather_T<<<gg, dim3(32, 8), 0, s>>>(A, h->d_v3a_Rb.p, lam, lam_new, E);
+  h->n_launch += 7;
   VG_CUDA(cudaGetLastError());
 }
 

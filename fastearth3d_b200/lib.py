@@ -41,7 +41,7 @@ _SIGS = [
     ("vg_get_rotation_state", [_VP, _P, _P, _P]),
     ("vg_set_rotation_state", [_VP, _P, _P, _P]),
     ("vg_misfit", [_VP, C.c_int, C.c_double, _P, C.c_int, C.POINTER(C.c_int), _P, _P]),
-    ("vg_misfit_grad", [_VP, C.c_int, C.c_double, _P, C.c_int, C.POINTER(C.c_int), _P, C.c_int, _P, _P]),
+    ("vg_misfit_grad", [_VP, C.c_int, C.c_double, _P, C.c_int, C.POINTER(C.c_int), _P, C.c_int, _P, _P, _P]),
     ("vg_sht_analysis", [_VP, _P, _P]),
     ("vg_sht_synthesis", [_VP, _P, _P]),
     ("vg_sht_analysis_noalloc", [_VP, C.c_void_p, C.c_void_p, C.c_int]),
@@ -180,15 +180,21 @@ class Model:
                                 st.ctypes.data_as(C.POINTER(C.c_int)), ptr(ob), C.byref(J)))
         return J.value
 
-    def misfit_grad(self, sigma, dt_s, sites, obs, ckpt_every=50):
-        """(J, dJ/dsigma) with dJ/dsigma shaped like sigma: d/dRe + 1j d/dIm."""
+    def misfit_grad(self, sigma, dt_s, sites, obs, ckpt_every=50, want_pert=False):
+        """(J, dJ/dsigma[, dJ/dpert]): dJ/dsigma shaped like sigma (d/dRe + 1j d/dIm),
+        dJ/dpert shaped (ne, nlat, nphi) like the vg_enable_visc3d input."""
         sig, st, ob = self._misfit_args(sigma, sites, obs)
         J = C.c_double(0)
         g = np.zeros_like(sig)
+        gp = np.zeros(self.ne * self.ng) if want_pert else None
         self._c(lib().vg_misfit_grad(self.h, len(sigma), dt_s, ptr(sig), len(st),
-                                     st.ctypes.data_as(C.POINTER(C.c_int)), ptr(ob), ckpt_every, C.byref(J), ptr(g)))
+                                     st.ctypes.data_as(C.POINTER(C.c_int)), ptr(ob), ckpt_every, C.byref(J), ptr(g),
+                                     ptr(gp)))
         g = g.reshape(len(sigma), -1, 2)
-        return J.value, g[..., 0] + 1j * g[..., 1]
+        out = (J.value, g[..., 0] + 1j * g[..., 1])
+        if want_pert:
+            out = out + (gp.reshape(self.ne, self.p.nlat, self.p.nphi),)
+        return out
 
     def rotation(self):
         """Polar motion m (complex, rad) and (kTe, hTe, k_s fluid, k_s flattening)."""

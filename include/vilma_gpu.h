@@ -190,15 +190,16 @@ int vg_set_rotation_state(vg_handle* h, const double* m, const double* load_mem,
  * complex per step, interleaved) held over step n, no sea-level equation:
  *   J = sum_n sum_s (rsl_n(site[s]) - obs[n * nsite + s])^2,  rsl = N - u
  * at the Gauss-grid points site[s] (land sites, no ocean). vg_misfit_grad also
- * returns dJ/dsigma (same layout as sigma_lm; NULL skips it) from a reverse
- * sweep, keeping the memory every ckpt_every steps for recomputation. The
- * handle's memory is left as it was. The drift skip gate is off inside these
- * calls. Elements with lateral viscosity are not yet differentiated
- * (vg_misfit_grad fails for them; vg_misfit supports them). */
+ * returns dJ/dsigma (same layout as sigma_lm; NULL skips it) and, with
+ * lateral viscosity (FP64 path), dJ/dpert with respect to the log10-viscosity
+ * perturbation of vg_enable_visc3d ((nphi, nlat, ne); zero on elements that
+ * are not 3-D; NULL skips it), from a reverse sweep that keeps the memory every
+ * ckpt_every steps and recomputes each segment from it. The handle's memory
+ * is left as it was. The drift skip gate is off inside these calls. */
 int vg_misfit(vg_handle* h, int nsteps, double dt_s, const double* sigma_lm, int nsite, const int* site,
               const double* obs, double* J);
 int vg_misfit_grad(vg_handle* h, int nsteps, double dt_s, const double* sigma_lm, int nsite, const int* site,
-                   const double* obs, int ckpt_every, double* J, double* grad_sigma);
+                   const double* obs, int ckpt_every, double* J, double* grad_sigma, double* grad_pert);
 
 /* Gauss-grid transforms on the device (sht_grid_synthesis / _analysis,
  * src/vilma_sht.f90:204-226), host arrays in and out. */

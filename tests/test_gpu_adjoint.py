@@ -66,3 +66,53 @@ def test_adjoint_checkpoint_interval_and_state_kept():
     s1, _ = m.state()
     for a, b in zip(s0, s1):
         assert np.array_equal(a, b)
+
+
+def setup_3d(lmax=10, nsteps=5, nsite=30, seed=5):
+    """A model whose Maxwell elements are all carried as 3-D, with a seeded
+    lateral log-viscosity field; returns a factory so finite differences can
+    rebuild the model with a perturbed field."""
+    rng = np.random.default_rng(seed)
+
+    def make(pert):
+        p = vlib.default_params()
+        p.lmax, p.nlat, p.nphi = lmax, lmax + 1, 2 * (lmax + 1)
+        for i, c in enumerate([2, 4, 3, 3]):
+            p.ne_layer[i] = c
+        p.visc3d_tol = -1.0  # every Maxwell element 3-D
+        m = vlib.Model(p)
+        m.enable_visc3d(pert)
+        return m
+
+    m0 = make(np.zeros((12, lmax + 1, 2 * (lmax + 1))))
+    th = np.linspace(0.1, 3.0, lmax + 1)[:, None]
+    ph = np.linspace(0, 2 * np.pi, 2 * (lmax + 1), endpoint=False)[None, :]
+    base = 0.3 * np.sin(2 * th) * np.cos(2 * ph) + 0.1 * rng.standard_normal((lmax + 1, 2 * (lmax + 1)))
+    pert = np.stack([base * (1 + 0.05 * e) for e in range(m0.ne)])
+    sig = (rng.standard_normal((nsteps, m0.nlm)) + 1j * rng.standard_normal((nsteps, m0.nlm))) * 1e3
+    sig[:, : lmax + 1] = sig[:, : lmax + 1].real
+    sites = rng.choice(m0.ng, size=nsite, replace=False)
+    obs = 0.01 * rng.standard_normal((nsteps, nsite))
+    return make, pert, sig, sites, obs, 50.0 * synth.SEC_PER_YEAR, rng
+
+
+def test_adjoint_3d_log_viscosity_gradient_vs_central_differences():
+    make, pert, sig, sites, obs, dt, rng = setup_3d()
+    m = make(pert)
+    assert m.info().ne3d > 0
+    J, gs, gp = m.misfit_grad(sig, dt, sites, obs, ckpt_every=2, want_pert=True)
+    assert abs(J - m.misfit(sig, dt, sites, obs)) <= 1e-12 * J
+    h = 1e-4
+    for _ in range(4):
+        d = rng.standard_normal(pert.shape)
+        fd = (make(pert + h * d).misfit(sig, dt, sites, obs) - make(pert - h * d).misfit(sig, dt, sites, obs)) / (2 * h)
+        ad = np.sum(gp * d)
+        assert abs(fd - ad) <= 1e-6 * abs(fd), (fd, ad)
+    # the load gradient through the 3-D transposes
+    for _ in range(3):
+        d = rng.standard_normal(sig.shape) + 1j * rng.standard_normal(sig.shape)
+        d[:, : m.p.lmax + 1] = d[:, : m.p.lmax + 1].real
+        hs = 1e-3 * np.abs(sig).max() / np.abs(d).max()
+        fd = (m.misfit(sig + hs * d, dt, sites, obs) - m.misfit(sig - hs * d, dt, sites, obs)) / (2 * hs)
+        ad = np.sum(gs.real * d.real + gs.imag * d.imag)
+        assert abs(fd - ad) <= 1e-6 * abs(fd), (fd, ad)
