@@ -289,6 +289,45 @@ def run_arm(w, precision, args, ice_dev, local, dist, want_e2e):
     return out
 
 
+def measure_grad_fwd(w, nsteps=10, ckpt=5, nsite=200, seed=7):
+    """Cost of the adjoint gradient against the forward it differentiates: a
+    response-level run of the workload's earth (lateral viscosity on, FP64)
+    with a seeded load per step and rsl observations at land-grid sites;
+    J = vg_misfit, (J, dJ/dload, dJ/dlog10 eta) = vg_misfit_grad with
+    checkpoints every `ckpt` steps (the rest recomputed). Each timed twice
+    after a warm-up call, best of two, wall clock around the synchronous calls."""
+    from fastearth3d_b200 import lib as vlib
+
+    p = w.params(vlib.default_params)
+    p.rotation = 0
+    p.visc3d_precision = 0
+    m = vlib.Model(p)
+    if w.visc3d:
+        m.enable_visc3d(w.pert(m.p))
+    rng = np.random.default_rng(seed)
+    sig = (rng.standard_normal((nsteps, m.nlm)) + 1j * rng.standard_normal((nsteps, m.nlm))) * 1e3
+    sig[:, : w.lmax + 1] = sig[:, : w.lmax + 1].real
+    land = np.flatnonzero(w.topo.reshape(-1) > 0)
+    sites = rng.choice(land if land.size >= nsite else np.arange(m.ng), nsite, replace=False)
+    obs = 0.01 * rng.standard_normal((nsteps, nsite))
+    dt = w.dt_yr * synth.SEC_PER_YEAR
+    m.misfit(sig, dt, sites, obs)
+    m.misfit_grad(sig, dt, sites, obs, ckpt, want_pert=w.visc3d)
+    tf, tg = [], []
+    for _ in range(2):
+        t0 = time.perf_counter()
+        m.misfit(sig, dt, sites, obs)
+        t1 = time.perf_counter()
+        m.misfit_grad(sig, dt, sites, obs, ckpt, want_pert=w.visc3d)
+        t2 = time.perf_counter()
+        tf.append(t1 - t0)
+        tg.append(t2 - t1)
+    return {"value": min(tg) / min(tf), "unit": "gradient cost / forward cost", "steps": nsteps, "ckpt_every": ckpt,
+            "sites": nsite, "fwd_ms_per_step": 1e3 * min(tf) / nsteps, "grad_ms_per_step": 1e3 * min(tg) / nsteps,
+            "gradient": "dJ/dload and dJ/dlog10(eta) of the 3-D elements" if w.visc3d else "dJ/dload",
+            "model": "response-level steps (no sea-level equation), FP64", "target": 3.0}
+
+
 def phases_of(arm):
     from fastearth3d_b200.abi import PHASE_NAMES
 
@@ -401,6 +440,7 @@ def main():
             "after_steps": total, "rsl": float(np.abs(r1 - r0).max() / np.abs(r0).max()),
             "z_bed": float(np.abs(z1 - z0).max() / np.abs(z0).max()), "norm": "max abs diff / max abs (FP64 GPU)",
             "rsl_target": 1e-8}
+    out["grad_fwd"] = measure_grad_fwd(w)
     if not args.no_cpu_baseline:
         out["cpu_baseline"] = cpu_baseline(w, args.cpu_sample_s, os.cpu_count() or 1)
     print(json.dumps(out))

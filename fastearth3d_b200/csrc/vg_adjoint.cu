@@ -18,9 +18,11 @@
 //   degree 1 through the transposed Green's block and CM projection).
 // With 3-D elements (FP64 path) the reverse sweep also runs the transposed
 // pseudo-spectral advance (vg_visc3d.cu: scatter^T, analysis^T, longitude^T,
-// synthesis^T, gather^T), which needs each step's state: a segment is
-// recomputed from its checkpoint, and d J / d(M dt) on the grid gives the
-// gradient with respect to the lateral log10-viscosity.
+// synthesis^T, gather^T). Of the forward it needs only each step's grid of
+// dyadic components before the factor -M dt (the longitude pass stores it,
+// nlat x 3 ne3d x 6 x nphi doubles a step), for d J / d(M dt) and so the
+// gradient with respect to the lateral log10-viscosity: a segment's grids are
+// recomputed from its checkpoint, the last segment's kept from the forward.
 // All in FP64. The drift skip gate is off inside these entry points: with a
 // zero threshold it only skips slots whose memory is exactly zero, whose drift
 // is zero anyway, so the forward stays exactly linear.
@@ -427,7 +429,7 @@ namespace {
 
 struct AdjWork {
   DArr<double> sig, obs, resid, lam, lam_new, dUn_bar, dVn_bar, surf_bar, qbar, w, gsig, ckpt, E, G1T;
-  DArr<double> ckpt_norm, seg, seg_norm, gradMdt;  // checkpoint norms, segment states, d J / d (M dt)
+  DArr<double> ckpt_norm, gseg, gradMdt;  // checkpoint norms, a segment's longitude grids, d J / d (M dt)
   DArr<int> site;
 };
 
@@ -568,18 +570,22 @@ double misfit_grad_dev(vg_handle* h, int nsteps, double dt, const double* sigma,
     VG_CUDA(cudaMemcpyAsync(h->d_mnorm.p + (size_t)h->cur * nk, nm, nk * sizeof(double), cudaMemcpyDeviceToDevice,
                             s));
   };
-  // with 3-D elements the reverse sweep needs every state; the last segment's
-  // are kept from this sweep, the others are recomputed from their checkpoints
+  // with 3-D elements the reverse sweep needs every step's longitude grid; the
+  // last segment's are kept from this sweep, the others recomputed from their
+  // checkpoints
   const int last0 = ((nsteps - 1) / ckpt) * ckpt;
-  if (v3) {
-    ensure(W.seg, (size_t)ckpt * S);
-    ensure(W.seg_norm, (size_t)ckpt * nk);
-  }
+  const size_t gsz = (size_t)G.nlat * 3 * h->ne3d * 6 * G.nphi;
+  if (v3) ensure(W.gseg, (size_t)std::min(ckpt, nsteps) * gsz);
+  struct GridStore {  // the longitude pass stores its grid while set
+    vg_handle* h;
+    ~GridStore() { h->v3_gstore = nullptr; }
+  } gstore_off{h};
   for (int n = 0; n < nsteps; ++n) {
     if (n % ckpt == 0) snapshot(W.ckpt.p + (size_t)(n / ckpt) * S, W.ckpt_norm.p + (size_t)(n / ckpt) * nk);
-    if (v3 && n >= last0) snapshot(W.seg.p + (size_t)(n - last0) * S, W.seg_norm.p + (size_t)(n - last0) * nk);
+    h->v3_gstore = (v3 && n >= last0) ? W.gseg.p + (size_t)(n - last0) * gsz : nullptr;
     fwd_step(h, W, n, nsite, dt);
   }
+  h->v3_gstore = nullptr;
   const double J = sum_squares(h, W, (size_t)nsteps * nsite);
   // reverse sweep
   ensure(W.lam, S);
@@ -611,18 +617,15 @@ double misfit_grad_dev(vg_handle* h, int nsteps, double dt, const double* sigma,
   }
   for (int n = nsteps - 1; n >= 0; --n) {
     double* sbar = W.gsig.p + (size_t)n * n2;
-    if (v3) {
-      // the states of this step's segment, recomputed from its checkpoint
-      const int c = n / ckpt, n0 = c * ckpt;
-      if (n < last0 && n % ckpt == ckpt - 1) {
-        restore(W.ckpt.p + (size_t)c * S, W.ckpt_norm.p + (size_t)c * nk);
-        for (int q = n0; q <= n; ++q) {
-          snapshot(W.seg.p + (size_t)(q - n0) * S, W.seg_norm.p + (size_t)(q - n0) * nk);
-          fwd_step(h, W, q, nsite, dt);
-        }
+    const int n0 = (n / ckpt) * ckpt;
+    if (v3 && n < last0 && n % ckpt == ckpt - 1) {
+      // this segment's longitude grids, recomputed from its checkpoint
+      restore(W.ckpt.p + (size_t)(n / ckpt) * S, W.ckpt_norm.p + (size_t)(n / ckpt) * nk);
+      for (int q = n0; q <= n; ++q) {
+        h->v3_gstore = W.gseg.p + (size_t)(q - n0) * gsz;
+        fwd_step(h, W, q, nsite, dt);
       }
-      restore(W.seg.p + (size_t)(n - n0) * S, W.seg_norm.p + (size_t)(n - n0) * nk);
-      launch_drift(h);  // drift of tau_n, the gather's strain
+      h->v3_gstore = nullptr;
     }
     k_site_synth_T<<<(G.nlm * 32 + 255) / 256, 256, 0, s>>>(nsite, W.site.p, G.nlm, G.nlat, G.nphi, G.d_lm_m.p, G.d_plm.p,
                                                       G.d_cos.p, G.d_sin.p, W.resid.p + (size_t)n * nsite, W.qbar.p);
@@ -632,7 +635,7 @@ double misfit_grad_dev(vg_handle* h, int nsteps, double dt, const double* sigma,
     k_adv1d_T_elem<<<eg, dim3(32, 8), 0, s>>>(ne, nr, nk, dt, h->d_kdeg.p, h->d_Jr.p, h->d_xUn.p, h->d_xVn.p,
                                                h->d_mu.p, h->d_MkPerDt.p, h->d_active1d.p, W.lam.p, W.lam_new.p,
                                                W.E.p);
-    if (v3) visc3d_adjoint(h, W.sig.p + (size_t)n * n2, dt, W.lam.p, W.lam_new.p, W.E.p, W.gradMdt.p);
+    if (v3) visc3d_adjoint(h, W.gseg.p + (size_t)(n - n0) * gsz, dt, W.lam.p, W.lam_new.p, W.E.p, W.gradMdt.p);
     k_adv1d_T_node<<<ng_, dim3(32, 8), 0, s>>>(ne, nr, nk, h->d_k2lm.p, W.E.p, W.dUn_bar.p, W.dVn_bar.p, sbar);
     k_drift_T<<<kg, 32, 0, s>>>(nr, nd, nk, h->d_kdeg.p, h->d_ab.p, h->d_dc.p, h->d_ipiv.p, W.dUn_bar.p,
                                 W.dVn_bar.p, W.surf_bar.p, W.w.p);

@@ -164,7 +164,8 @@ struct vg_handle {
   vg::DArr<double> d_wP, d_wD, d_wG, d_wH;  // quadrature-weighted analysis kernels (nlm, nlat)
   vg::DArr<int> d_kbeg;               // first slot of each degree (lmax + 2)
   vg::DArr<double> d_X, d_Y, d_dy;    // 3-D work buffers: synthesis input, Fourier products, increments
-  vg::DArr<double> d_v3a_Yf, d_v3a_Yb, d_v3a_dyb, d_v3a_Rb;  // 3-D adjoint: forward products, their adjoints
+  vg::DArr<double> d_v3a_Yb, d_v3a_dyb, d_v3a_Rb;  // 3-D adjoint: product adjoints
+  double* v3_gstore = nullptr;  // when set, the FP64 longitude pass also stores its grid there (adjoint sweeps)
   // sea-level equation fields (ng each unless stated)
   vg::DArr<double> d_z_bed_eq, d_h_ice_eq, d_h_ice, d_ice1, d_ice_now, d_dice_now, d_rsl, d_rsl_n,
       d_C, d_C0, d_C_next, d_dig, d_wcorr, d_Sraw, d_zbed, d_tmp;
@@ -231,10 +232,11 @@ void update_bsl(vg_handle* h);
 // 3-D (vg_visc3d.cu)
 void visc3d_enable(vg_handle* h, const double* pert_host);
 void visc3d_advance(vg_handle* h, const double* d_sigma, double dt);
-// transposed 3-D advance (FP64 path) at the current state and drift: lam_new
-// (3-D entries) = lam + gather^T, E (3-D elements) = strain adjoints, and
-// d J / d (M dt) accumulated into gradMdt (ne3d, nlat, nphi)
-void visc3d_adjoint(vg_handle* h, const double* d_sigma, double dt, const double* lam, double* lam_new, double* E,
+// transposed 3-D advance (FP64 path) of one step whose longitude-pass grid the
+// forward stored in gstore: lam_new (3-D entries) = lam + gather^T, E (3-D
+// elements) = strain adjoints, d J / d (M dt) accumulated into gradMdt
+// (ne3d, nlat, nphi)
+void visc3d_adjoint(vg_handle* h, const double* gstore, double dt, const double* lam, double* lam_new, double* E,
                     double* gradMdt);
 // rotational feedback (vg_rotation.cu)
 void build_fluid_deg2_band(vg_handle* h, DArr<double>& ab, DArr<double>& dr, DArr<double>& dc, DArr<int>& ipiv);

@@ -218,7 +218,7 @@ constexpr int LON_FT = 4;
 __global__ void __launch_bounds__(256) k_v3_lon(double* __restrict__ S, int nlat, int nphi, int M, int nf,
                                                 double dt, const double* __restrict__ Mk3rate,
                                                 const double* __restrict__ cs, const double* __restrict__ sn,
-                                                const double* __restrict__ invsin) {
+                                                const double* __restrict__ invsin, double* __restrict__ gstore) {
   extern __shared__ double sm[];
   const int j = blockIdx.x, f0 = blockIdx.y * LON_FT;
   const int nft = min(LON_FT, nf - f0);
@@ -277,6 +277,12 @@ __global__ void __launch_bounds__(256) k_v3_lon(double* __restrict__ S, int nlat
     }
     Gr[(size_t)row * nphi + i] = -m1 * (a + b);
     Gr[(size_t)row * nphi + i + half] = -m2 * (a - b);
+    if (gstore && fl < nft) {  // the grid before -M dt, [j][field][component][i], for the adjoint
+      const int c = row / LON_FT;
+      double* gs = gstore + (((size_t)j * nf + f0 + fl) * 6 + c) * nphi;
+      gs[i] = a + b;
+      gs[i + half] = a - b;
+    }
   }
   __syncthreads();
   // 3. forward DFT (F_m = 2 pi / nphi sum_i f_i e^{-i m phi_i}) and analysis inputs
@@ -504,7 +510,7 @@ void visc3d_advance(vg_handle* h, const double* d_sigma, double dt) {
   {
     PhaseScope pp(h, VG_PH_V3_LON_INV);
     k_v3_lon<<<lg, 256, lsm, s>>>(h->d_Y.p, G.nlat, G.nphi, G.M, nf, dt, h->d_MkPerDt3.p, G.d_cos.p, G.d_sin.p,
-                                  G.d_invsin.p);
+                                  G.d_invsin.p, h->v3_gstore);
     ++h->n_launch;
     VG_CUDA(cudaGetLastError());
   }
@@ -567,8 +573,8 @@ __global__ void __launch_bounds__(256) k_v3_scatter_T(V3Args A, const double* __
 // adjoint chain on Yb in place: analysis-input scales^T, forward DFT^T,
 // times -M dt, inverse DFT^T, dyadic components^T; and
 // d J / d (M dt)(j, i) += -sum over components and shapes of G_bar g
-__global__ void __launch_bounds__(256) k_v3_lon_T(const double* __restrict__ Yf, double* __restrict__ Yb, int nlat,
-                                                  int nphi, int M, int nf, double dt,
+__global__ void __launch_bounds__(256) k_v3_lon_T(const double* __restrict__ gstore, double* __restrict__ Yb,
+                                                  int nlat, int nphi, int M, int nf, double dt,
                                                   const double* __restrict__ Mk3rate,
                                                   const double* __restrict__ cs, const double* __restrict__ sn,
                                                   const double* __restrict__ invsin, double* __restrict__ gradMdt) {
@@ -576,48 +582,15 @@ __global__ void __launch_bounds__(256) k_v3_lon_T(const double* __restrict__ Yf,
   constexpr int FT = 3;
   const int j = blockIdx.x, ei = blockIdx.y, f0 = 3 * ei;
   const int ncf = 2 * nf, half = nphi / 2, R = 6 * FT;
-  double* Cc = sm;                        // [R][M][2] component coefficients (forward, then adjoint)
-  double* gf = sm + (size_t)R * M * 2;    // [R][nphi] forward grid
+  double* Cc = sm;                        // [R][M][2] adjoint component coefficients
+  double* gf = sm + (size_t)R * M * 2;    // [R][nphi] forward grid (stored by the forward pass)
   double* Gb = gf + (size_t)R * nphi;     // [R][nphi] adjoint grid
   const double is = invsin[j];
   const double scl = 2.0 * PI / (double)nphi;
-  // 1. forward dyadic coefficients from the forward products
-  for (int t = threadIdx.x; t < FT * M; t += blockDim.x) {
-    const int fl = t / M, m = t % M;
-    double pr[6][2];
-    for (int p = 0; p < 6; ++p)
-      for (int ri = 0; ri < 2; ++ri) pr[p][ri] = Yf[(((size_t)m * nlat + j) * 6 + p) * ncf + (f0 + fl) * 2 + ri];
-    const double ms = m * is;
-    const double comp[6][2] = {{pr[0][0], pr[0][1]},
-                               {pr[1][0], pr[1][1]},
-                               {-ms * pr[2][1], ms * pr[2][0]},
-                               {pr[3][0] + pr[4][0], pr[3][1] + pr[4][1]},
-                               {pr[3][0] - pr[4][0], pr[3][1] - pr[4][1]},
-                               {-4.0 * pr[5][1], 4.0 * pr[5][0]}};
-    for (int c = 0; c < 6; ++c) {
-      Cc[((c * FT + fl) * M + m) * 2] = comp[c][0];
-      Cc[((c * FT + fl) * M + m) * 2 + 1] = comp[c][1];
-    }
-  }
-  __syncthreads();
-  // 2. forward inverse DFT (g, before the factor -M dt)
-  for (int t = threadIdx.x; t < R * half; t += blockDim.x) {
-    const int row = t / half, i = t % half;
-    const double* c = Cc + (size_t)row * M * 2;
-    double ev = 0.0, od = 0.0;
-    int tw = i;
-    for (int m = 1; m < M; ++m) {
-      const double v = c[2 * m] * __ldg(&cs[tw]) - c[2 * m + 1] * __ldg(&sn[tw]);
-      if (m & 1)
-        od += v;
-      else
-        ev += v;
-      tw += i;
-      if (tw >= nphi) tw -= nphi;
-    }
-    const double a = c[0] + 2.0 * ev, b = 2.0 * od;
-    gf[(size_t)row * nphi + i] = a + b;
-    gf[(size_t)row * nphi + i + half] = a - b;
+  // 1-2. the forward grid g of the element's three fields (row = c FT + fl)
+  for (int t = threadIdx.x; t < R * nphi; t += blockDim.x) {
+    const int row = t / nphi, i = t % nphi, c = row / FT, fl = row % FT;
+    gf[t] = gstore[(((size_t)j * nf + f0 + fl) * 6 + c) * nphi + i];
   }
   __syncthreads();
   // 3. adjoint dyadic Fourier coefficients from the analysis-input adjoints
@@ -743,7 +716,7 @@ __global__ void __launch_bounds__(256) k_v3_gather_T(V3Args A, const double* __r
   }
 }
 
-void visc3d_adjoint(vg_handle* h, const double* d_sigma, double dt, const double* lam, double* lam_new, double* E,
+void visc3d_adjoint(vg_handle* h, const double* gstore, double dt, const double* lam, double* lam_new, double* E,
                     double* gradMdt) {
   if (h->ne3d == 0) return;
   if (h->p.visc3d_precision != VG_VISC3D_FP64)
@@ -752,8 +725,7 @@ void visc3d_adjoint(vg_handle* h, const double* d_sigma, double dt, const double
   cudaStream_t s = h->stream;
   const int nf = 3 * h->ne3d, ncf = 2 * nf;
   const size_t ny = (size_t)G.M * G.nlat * 6 * ncf, nr6 = (size_t)(h->nk + 1) * 6 * ncf;
-  if (h->d_v3a_Yf.n != ny) {
-    h->d_v3a_Yf.alloc(ny);
+  if (h->d_v3a_Yb.n != ny) {
     h->d_v3a_Yb.alloc(ny);
     h->d_v3a_dyb.alloc(nr6);  // slot row nk (degree 0) stays zero
     h->d_v3a_Rb.alloc(nr6);
@@ -761,7 +733,7 @@ void visc3d_adjoint(vg_handle* h, const double* d_sigma, double dt, const double
   V3Args A;
   A.mem = h->d_mem[h->cur].p;
   A.nxt = nullptr;
-  A.sigma = d_sigma;
+  A.sigma = nullptr;
   A.kdeg = h->d_kdeg.p;
   A.k2lm = h->d_k2lm.p;
   A.e3d = h->d_e3d.p;
@@ -778,8 +750,6 @@ void visc3d_adjoint(vg_handle* h, const double* d_sigma, double dt, const double
   A.nf = nf;
   A.ncf = ncf;
   dim3 gg((h->nk + 31) / 32, (h->ne3d + 7) / 8);
-  // forward products of this step (recomputed from its state and drift)
-  k_v3_gather<double><<<gg, dim3(32, 8), 0, s>>>(A, h->d_X.p);
   GemmArgs S;
   S.mode = 0;
   S.lmax = G.lmax;
@@ -796,10 +766,7 @@ void visc3d_adjoint(vg_handle* h, const double* d_sigma, double dt, const double
     S.T[p] = st[p];
     S.chan[p] = sc[p];
   }
-  S.in = h->d_X.p;
-  S.out = h->d_v3a_Yf.p;
   dim3 sgrid((ncf + GB_N - 1) / GB_N, (G.nlat + GB_M - 1) / GB_M, G.M * 6);
-  k_v3_gemm<<<sgrid, 256, 0, s>>>(S);
   // adjoint chain
   k_v3_scatter_T<<<gg, dim3(32, 8), 0, s>>>(A, lam, h->d_n6.p, h->d_v3a_dyb.p);
   GemmArgs Ab = S;  // analysis^T: the weighted tables, per-product input rows
@@ -818,7 +785,7 @@ void visc3d_adjoint(vg_handle* h, const double* d_sigma, double dt, const double
     lon_attr = true;
   }
   if (lsm > 200 * 1024) throw Error("vg_misfit_grad: grid too large for the transposed longitude pass");
-  k_v3_lon_T<<<dim3(G.nlat, h->ne3d), 256, lsm, s>>>(h->d_v3a_Yf.p, h->d_v3a_Yb.p, G.nlat, G.nphi, G.M, nf, dt,
+  k_v3_lon_T<<<dim3(G.nlat, h->ne3d), 256, lsm, s>>>(gstore, h->d_v3a_Yb.p, G.nlat, G.nphi, G.M, nf, dt,
                                                        h->d_MkPerDt3.p, G.d_cos.p, G.d_sin.p, G.d_invsin.p, gradMdt);
   GemmArgs Sb = S;  // synthesis^T: the unweighted tables, per product out
   Sb.mode = 1;
@@ -827,7 +794,7 @@ void visc3d_adjoint(vg_handle* h, const double* d_sigma, double dt, const double
   dim3 agrid((ncf + GB_N - 1) / GB_N, (G.M + GB_M - 1) / GB_M, G.M * 6);
   k_v3_gemm<<<agrid, 256, 0, s>>>(Sb);
   k_v3_gather_T<<<gg, dim3(32, 8), 0, s>>>(A, h->d_v3a_Rb.p, lam, lam_new, E);
-  h->n_launch += 7;
+  h->n_launch += 5;
   VG_CUDA(cudaGetLastError());
 }
 

@@ -194,8 +194,11 @@ int vg_set_rotation_state(vg_handle* h, const double* m, const double* load_mem,
  * lateral viscosity (FP64 path), dJ/dpert with respect to the log10-viscosity
  * perturbation of vg_enable_visc3d ((nphi, nlat, ne); zero on elements that
  * are not 3-D; NULL skips it), from a reverse sweep that keeps the memory every
- * ckpt_every steps and recomputes each segment from it. The handle's memory
- * is left as it was. The drift skip gate is off inside these calls. */
+ * ckpt_every steps and recomputes each segment from it. With 3-D elements a
+ * segment's longitude grids are held on the device: min(ckpt_every, nsteps) x
+ * nlat x 18 ne3d x nphi doubles (about 0.26 GB a step at lmax 128 with 54
+ * 3-D elements). The handle's memory is left as it was. The drift skip gate
+ * is off inside these calls. */
 int vg_misfit(vg_handle* h, int nsteps, double dt_s, const double* sigma_lm, int nsite, const int* site,
               const double* obs, double* J);
 int vg_misfit_grad(vg_handle* h, int nsteps, double dt_s, const double* sigma_lm, int nsite, const int* site,
