@@ -166,6 +166,7 @@ struct vg_handle {
   vg::DArr<double> d_X, d_Y, d_dy;    // 3-D work buffers: synthesis input, Fourier products, increments
   vg::DArr<double> d_v3a_Yb, d_v3a_dyb, d_v3a_Rb;  // 3-D adjoint: product adjoints
   double* v3_gstore = nullptr;  // when set, the FP64 longitude pass also stores its grid there (adjoint sweeps)
+  vg::DArr<double> d_lon_tw, d_lon_twt;  // FP64 longitude pass: dense twiddle tables (by order, by longitude)
   // sea-level equation fields (ng each unless stated)
   vg::DArr<double> d_z_bed_eq, d_h_ice_eq, d_h_ice, d_ice1, d_ice_now, d_dice_now, d_rsl, d_rsl_n,
       d_C, d_C0, d_C_next, d_dig, d_wcorr, d_Sraw, d_zbed, d_tmp;

@@ -209,113 +209,293 @@ __global__ void __launch_bounds__(256) k_v3_gemm(GemmArgs A) {
 
 // ------------------------------------------------------------------ longitude
 
-// One CTA per (latitude j, tile of FT fields). Dyadic Fourier coefficients from
-// the six synthesis products, inverse DFT (half-period split: phi + pi flips
-// odd m), times -M(theta_j, phi_i) of the field's element, forward DFT, and the
-// six analysis inputs, written in place over the synthesis products.
-constexpr int LON_FT = 4;
+// The longitude transforms of the FP64 path as register-tiled real DFT
+// contractions over dense twiddle tables, split by the parity of m
+// (phi_{i + half} = phi_i + pi flips the odd orders):
+//   synthesis  E(r, i) = sum_{m even} A(r, 2m) cos(m phi_i) - A(r, 2m+1) sin(m phi_i),
+//              O(r, i) the same over odd m; g(i) = E + O, g(i + half) = E - O
+//   analysis   F(r, m) = sum_{i < half} X_p(r, i) (cos, -sin)(m phi_i) with
+//              X_0 = g(i) + g(i + half) for even m, X_1 = g(i) - g(i + half) for odd m
+// A thread owns the six dyadic components (rows) of one field at LON_TC
+// longitudes or orders, spaced so that a warp's twiddle loads are contiguous.
+// Tables: tw[2m + ri][ncg TC] = (cos, -sin)(m phi_i) (zero past half and M),
+// twt[p][i][Mq][2] = (cos, -sin)(m phi_i) at m = p + 2 mq (zero past M).
+constexpr int LON_TC = 3;
 
-__global__ void __launch_bounds__(256) k_v3_lon(double* __restrict__ S, int nlat, int nphi, int M, int nf,
-                                                double dt, const double* __restrict__ Mk3rate,
-                                                const double* __restrict__ cs, const double* __restrict__ sn,
-                                                const double* __restrict__ invsin, double* __restrict__ gstore) {
+struct LonTables {
+  const double* tw;
+  const double* twt;
+  int M, M2, half, ncg, nmg0, nmg1, Mq;
+};
+
+static LonTables lon_tables(const vg_handle* h) {
+  const Grid& G = h->grid;
+  LonTables T;
+  T.tw = h->d_lon_tw.p;
+  T.twt = h->d_lon_twt.p;
+  T.M = G.M;
+  T.M2 = (G.M + 1) & ~1;
+  T.half = G.nphi / 2;
+  T.ncg = (T.half + LON_TC - 1) / LON_TC;
+  T.nmg0 = ((G.M + 1) / 2 + LON_TC - 1) / LON_TC;
+  T.nmg1 = (G.M / 2 + LON_TC - 1) / LON_TC;
+  T.Mq = std::max(T.nmg0, T.nmg1) * LON_TC;
+  return T;
+}
+
+static void lon_tables_build(vg_handle* h) {
+  const Grid& G = h->grid;
+  const LonTables T = lon_tables(h);
+  const int nphi = G.nphi, wT = T.ncg * LON_TC;
+  std::vector<double> cs(nphi), sn(nphi);
+  for (int t = 0; t < nphi; ++t) {  // the grid's twiddles cos/sin(2 pi t / nphi)
+    cs[t] = std::cos(2.0 * PI * (double)t / (double)nphi);
+    sn[t] = std::sin(2.0 * PI * (double)t / (double)nphi);
+  }
+  std::vector<double> tw((size_t)2 * T.M2 * wT, 0.0), twt((size_t)2 * T.half * T.Mq * 2, 0.0);
+  for (int m = 0; m < G.M; ++m)
+    for (int i = 0; i < T.half; ++i) {
+      const int t = (int)(((long long)m * i) % nphi);
+      tw[(size_t)(2 * m) * wT + i] = cs[t];
+      tw[(size_t)(2 * m + 1) * wT + i] = -sn[t];
+      const int p = m & 1, mq = m >> 1;
+      twt[(((size_t)p * T.half + i) * T.Mq + mq) * 2] = cs[t];
+      twt[(((size_t)p * T.half + i) * T.Mq + mq) * 2 + 1] = -sn[t];
+    }
+  h->d_lon_tw.upload(tw, h->stream);
+  h->d_lon_twt.upload(twt, h->stream);
+}
+
+__device__ __forceinline__ void lon_cp16(void* dst, const void* src) {
+  const unsigned sa = (unsigned)__cvta_generic_to_shared(dst);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(src) : "memory");
+}
+__device__ __forceinline__ void lon_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void lon_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+
+// synthesis tiles over A (shared, [6 nfl][2 M2], row 6 fl + c): for each
+// (field fl, longitude i < half) calls epi(fl, i, g(i), g(i + half)) with the
+// six components' values
+template <class Epi>
+__device__ __forceinline__ void lon_synth(const double* __restrict__ A, int nfl, const LonTables& T, Epi epi) {
+  const int wA = 2 * T.M2, wT = T.ncg * LON_TC, ntile = nfl * T.ncg;
+  for (int tile = threadIdx.x; tile < ntile; tile += blockDim.x) {
+    const int fl = tile / T.ncg, cg = tile % T.ncg;
+    const double* a = A + (size_t)fl * 6 * wA;
+    double e[6][LON_TC], o[6][LON_TC];
+#pragma unroll
+    for (int c = 0; c < 6; ++c)
+#pragma unroll
+      for (int t = 0; t < LON_TC; ++t) e[c][t] = o[c][t] = 0.0;
+    const double* tp = T.tw + cg;
+    for (int m = 0; m < T.M2; m += 2) {
+      double tr[LON_TC], ti[LON_TC], ur[LON_TC], ui[LON_TC];
+#pragma unroll
+      for (int t = 0; t < LON_TC; ++t) {
+        tr[t] = __ldg(tp + (size_t)(2 * m) * wT + t * T.ncg);
+        ti[t] = __ldg(tp + (size_t)(2 * m + 1) * wT + t * T.ncg);
+        ur[t] = __ldg(tp + (size_t)(2 * m + 2) * wT + t * T.ncg);
+        ui[t] = __ldg(tp + (size_t)(2 * m + 3) * wT + t * T.ncg);
+      }
+#pragma unroll
+      for (int c = 0; c < 6; ++c) {
+        const double2 v = *reinterpret_cast<const double2*>(a + (size_t)c * wA + 2 * m);
+        const double2 u = *reinterpret_cast<const double2*>(a + (size_t)c * wA + 2 * m + 2);
+#pragma unroll
+        for (int t = 0; t < LON_TC; ++t) {
+          e[c][t] = fma(v.x, tr[t], fma(v.y, ti[t], e[c][t]));
+          o[c][t] = fma(u.x, ur[t], fma(u.y, ui[t], o[c][t]));
+        }
+      }
+    }
+#pragma unroll
+    for (int t = 0; t < LON_TC; ++t) {
+      const int i = cg + T.ncg * t;
+      if (i >= T.half) continue;
+      double g1[6], g2[6];
+#pragma unroll
+      for (int c = 0; c < 6; ++c) {
+        g1[c] = e[c][t] + o[c][t];
+        g2[c] = e[c][t] - o[c][t];
+      }
+      epi(fl, i, g1, g2);
+    }
+  }
+}
+
+// analysis tiles over X (shared, [6 nfl][nphi]: X_0 in [0, half), X_1 in
+// [half, nphi)): for each (field fl, order m < M) calls epi(fl, m, re, im)
+// with the six components' sums
+template <class Epi>
+__device__ __forceinline__ void lon_anal(const double* __restrict__ X, int nfl, int nphi, const LonTables& T,
+                                         Epi epi) {
+  const int n0 = nfl * T.nmg0, ntile = n0 + nfl * T.nmg1;
+  for (int tile = threadIdx.x; tile < ntile; tile += blockDim.x) {
+    const int p = tile < n0 ? 0 : 1, nmg = p ? T.nmg1 : T.nmg0, tl = p ? tile - n0 : tile;
+    const int fl = tl / nmg, mg = tl % nmg;
+    const double* x = X + (size_t)fl * 6 * nphi + p * T.half;
+    const double2* tp = reinterpret_cast<const double2*>(T.twt) + (size_t)p * T.half * T.Mq + mg;
+    double re[6][LON_TC], im[6][LON_TC];
+#pragma unroll
+    for (int c = 0; c < 6; ++c)
+#pragma unroll
+      for (int t = 0; t < LON_TC; ++t) re[c][t] = im[c][t] = 0.0;
+    for (int i = 0; i < T.half; ++i) {
+      double2 w[LON_TC];
+#pragma unroll
+      for (int t = 0; t < LON_TC; ++t) w[t] = __ldg(tp + (size_t)i * T.Mq + t * nmg);
+#pragma unroll
+      for (int c = 0; c < 6; ++c) {
+        const double v = x[(size_t)c * nphi + i];
+#pragma unroll
+        for (int t = 0; t < LON_TC; ++t) {
+          re[c][t] = fma(v, w[t].x, re[c][t]);
+          im[c][t] = fma(v, w[t].y, im[c][t]);
+        }
+      }
+    }
+#pragma unroll
+    for (int t = 0; t < LON_TC; ++t) {
+      const int m = p + 2 * (mg + nmg * t);
+      if (m >= T.M) continue;
+      double r6[6], i6[6];
+#pragma unroll
+      for (int c = 0; c < 6; ++c) {
+        r6[c] = re[c][t];
+        i6[c] = im[c][t];
+      }
+      epi(fl, m, r6, i6);
+    }
+  }
+}
+
+constexpr int LON_THREADS = 384;
+constexpr int LON_LF = 3;  // fields per CTA: one element's three shape coefficients (two CTAs per SM)
+
+// the CTA's slice of the products S[m][j][q][f][ri] (fields f0 .. f0 + nft - 1,
+// a contiguous run of 2 nft doubles per (m, q)) to and from shared [m][q][2 nft]
+// (16-byte cp.async pieces, all in flight together; ncf and 2 f0 are even)
+__device__ __forceinline__ void stage_in(const double* __restrict__ S, double* __restrict__ X, int nlat, int ncf,
+                                         int j, int f0, int nft, int M) {
+  const int n = M * 6 * nft;
+  for (int t = threadIdx.x; t < n; t += blockDim.x) {
+    const int mq = t / nft, c = t % nft;
+    lon_cp16(X + (size_t)mq * 2 * nft + 2 * c,
+             S + ((size_t)(mq / 6) * nlat + j) * 6 * ncf + (size_t)(mq % 6) * ncf + 2 * f0 + 2 * c);
+  }
+  lon_commit();
+  lon_wait<0>();
+}
+
+__device__ __forceinline__ void stage_out(const double* __restrict__ X, double* __restrict__ S, int nlat, int ncf,
+                                          int j, int f0, int nft, int M) {
+  const int w = 2 * nft, n = M * 6 * w;
+  for (int t = threadIdx.x; t < n; t += blockDim.x) {
+    const int mq = t / w, c = t % w;
+    S[((size_t)(mq / 6) * nlat + j) * 6 * ncf + (size_t)(mq % 6) * ncf + 2 * f0 + c] = X[t];
+  }
+}
+
+// One CTA per (latitude j, LF fields). Dyadic Fourier coefficients from the
+// six synthesis products, synthesis to the grid, times -M(theta_j, phi_i) of
+// the field's element, analysis, and the six analysis inputs, written in place
+// over the synthesis products. With gstore set, the grid before -M dt is also
+// stored, [j][field][component][i], for the adjoint.
+template <int LF>
+__global__ void __launch_bounds__(LON_THREADS, 1)
+    k_v3_lon(double* __restrict__ S, int nlat, int nphi, int nf, double dt, const double* __restrict__ Mk3rate,
+             LonTables T, const double* __restrict__ invsin, double* __restrict__ gstore) {
   extern __shared__ double sm[];
-  const int j = blockIdx.x, f0 = blockIdx.y * LON_FT;
-  const int nft = min(LON_FT, nf - f0);
-  const int ncf = 2 * nf, half = nphi / 2;
-  double* C = sm;                               // [6 comp][FT][M][2]
-  double* Gr = sm + 6 * LON_FT * M * 2;          // [6 comp][FT][nphi]
+  const int j = blockIdx.x, f0 = blockIdx.y * LF;
+  const int nft = min(LF, nf - f0);
+  const int ncf = 2 * nf, half = T.half, wA = 2 * T.M2;
+  double* A = sm;                          // [6 LF][2 M2]
+  double* X = sm + (size_t)6 * LF * wA;    // [6 LF][nphi]
   const double is = invsin[j];
-  // 1. dyadic coefficients rr, rt, rp, tt, pp, tp
-  for (int t = threadIdx.x; t < LON_FT * M; t += blockDim.x) {
-    int fl = t / M, m = t % M;
+  // 1. the CTA's synthesis products, staged in X as [m][q][2 nft] (contiguous
+  //    runs of 2 nft doubles in S), then the dyadic coefficients rr, rt, rp,
+  //    tt, pp, tp with the synthesis weights (1 at m = 0, 2 above), zero past M
+  stage_in(S, X, nlat, ncf, j, f0, nft, T.M);
+  __syncthreads();
+  for (int t = threadIdx.x; t < nft * T.M2; t += blockDim.x) {
+    const int fl = t / T.M2, m = t % T.M2;
     double pr[6][2];
-    for (int p = 0; p < 6; ++p)
-      for (int ri = 0; ri < 2; ++ri)
-        pr[p][ri] = (fl < nft) ? S[(((size_t)m * nlat + j) * 6 + p) * ncf + (f0 + fl) * 2 + ri] : 0.0;
-    double ms = m * is;
-    double rr[2] = {pr[0][0], pr[0][1]};
-    double rt[2] = {pr[1][0], pr[1][1]};
-    double rp[2] = {-ms * pr[2][1], ms * pr[2][0]};  // i (m / sin) P.X1
-    double tr[2] = {pr[3][0], pr[3][1]};
-    double sg[2] = {pr[4][0], pr[4][1]};
-    double sh[2] = {-pr[5][1], pr[5][0]};  // i H.X3
-    double comp[6][2] = {{rr[0], rr[1]},
-                         {rt[0], rt[1]},
-                         {rp[0], rp[1]},
-                         {tr[0] + sg[0], tr[1] + sg[1]},
-                         {tr[0] - sg[0], tr[1] - sg[1]},
-                         {4.0 * sh[0], 4.0 * sh[1]}};
+    for (int q = 0; q < 6; ++q)
+      for (int ri = 0; ri < 2; ++ri) pr[q][ri] = (m < T.M) ? X[((size_t)m * 6 + q) * 2 * nft + 2 * fl + ri] : 0.0;
+    const double ms = m * is, w = (m == 0) ? 1.0 : 2.0;
+    const double comp[6][2] = {{pr[0][0], pr[0][1]},
+                               {pr[1][0], pr[1][1]},
+                               {-ms * pr[2][1], ms * pr[2][0]},           // i (m / sin) P.X1
+                               {pr[3][0] + pr[4][0], pr[3][1] + pr[4][1]},  // TT + PP
+                               {pr[3][0] - pr[4][0], pr[3][1] - pr[4][1]},  // TT - PP
+                               {-4.0 * pr[5][1], 4.0 * pr[5][0]}};          // 4 i H.X3
     for (int c = 0; c < 6; ++c) {
-      C[((c * LON_FT + fl) * M + m) * 2] = comp[c][0];
-      C[((c * LON_FT + fl) * M + m) * 2 + 1] = comp[c][1];
+      A[(size_t)(fl * 6 + c) * wA + 2 * m] = w * comp[c][0];
+      A[(size_t)(fl * 6 + c) * wA + 2 * m + 1] = w * comp[c][1];
     }
   }
   __syncthreads();
-  // 2. inverse DFT (f_i = Re C0 + 2 Re sum_m C_m e^{i m phi_i}), times -M
-  for (int t = threadIdx.x; t < 6 * LON_FT * half; t += blockDim.x) {
-    int row = t / half, i = t % half, fl = row % LON_FT;
-    const double* c = C + (size_t)row * M * 2;
-    double ev = 0.0, od = 0.0;
-    int tw = i;
-    for (int m = 1; m < M; ++m) {
-      double v = c[2 * m] * __ldg(&cs[tw]) - c[2 * m + 1] * __ldg(&sn[tw]);
-      if (m & 1)
-        od += v;
-      else
-        ev += v;
-      tw += i;
-      if (tw >= nphi) tw -= nphi;
+  // 2. synthesis, times -M dt, and the parity combinations of the analysis
+  lon_synth(A, nft, T, [&](int fl, int i, const double* g1, const double* g2) {
+    const int f = f0 + fl;
+    const double* Mr = Mk3rate + ((size_t)(f / 3) * nlat + j) * nphi;
+    const double m1 = Mr[i] * dt, m2 = Mr[i + half] * dt;
+    for (int c = 0; c < 6; ++c) {
+      if (gstore) {
+        double* gs = gstore + (((size_t)j * nf + f) * 6 + c) * nphi;
+        gs[i] = g1[c];
+        gs[i + half] = g2[c];
+      }
+      const double a = -m1 * g1[c], b = -m2 * g2[c];
+      X[(size_t)(fl * 6 + c) * nphi + i] = a + b;
+      X[(size_t)(fl * 6 + c) * nphi + half + i] = a - b;
     }
-    double a = c[0] + 2.0 * ev, b = 2.0 * od;
-    double m1 = 0.0, m2 = 0.0;
-    if (fl < nft) {
-      int e = (f0 + fl) / 3;
-      const double* Mr = Mk3rate + ((size_t)e * nlat + j) * nphi;
-      m1 = Mr[i] * dt;
-      m2 = Mr[i + half] * dt;
-    }
-    Gr[(size_t)row * nphi + i] = -m1 * (a + b);
-    Gr[(size_t)row * nphi + i + half] = -m2 * (a - b);
-    if (gstore && fl < nft) {  // the grid before -M dt, [j][field][component][i], for the adjoint
-      const int c = row / LON_FT;
-      double* gs = gstore + (((size_t)j * nf + f0 + fl) * 6 + c) * nphi;
-      gs[i] = a + b;
-      gs[i + half] = a - b;
-    }
-  }
+  });
   __syncthreads();
-  // 3. forward DFT (F_m = 2 pi / nphi sum_i f_i e^{-i m phi_i}) and analysis inputs
+  // 3. analysis (F_m = 2 pi / nphi sum_i f_i e^{-i m phi_i}) and the analysis
+  //    inputs RR, RT, m/sin RP, TT + PP, TT - PP, TP
   const double scl = 2.0 * PI / (double)nphi;
-  for (int t = threadIdx.x; t < LON_FT * M; t += blockDim.x) {
-    int fl = t / M, m = t % M;
+  lon_anal(X, nft, nphi, T, [&](int fl, int m, const double* re, const double* im) {
     double F[6][2];
     for (int c = 0; c < 6; ++c) {
-      const double* g = Gr + (size_t)(c * LON_FT + fl) * nphi;
-      double re = 0.0, im = 0.0;
-      int tw = 0;
-      double sgn = (m & 1) ? -1.0 : 1.0;
-      for (int i = 0; i < half; ++i) {
-        double v = g[i] + sgn * g[i + half];
-        re += v * __ldg(&cs[tw]);
-        im -= v * __ldg(&sn[tw]);
-        tw += m;
-        if (tw >= nphi) tw -= nphi;
-      }
-      F[c][0] = re * scl;
-      F[c][1] = im * scl;
+      F[c][0] = scl * re[c];
+      F[c][1] = scl * im[c];
     }
-    if (fl >= nft) continue;
-    double ms = m * is;
-    double out[6][2] = {{F[0][0], F[0][1]},
-                        {F[1][0], F[1][1]},
-                        {ms * F[2][0], ms * F[2][1]},
-                        {F[3][0] + F[4][0], F[3][1] + F[4][1]},
-                        {F[3][0] - F[4][0], F[3][1] - F[4][1]},
-                        {F[5][0], F[5][1]}};
+    const double ms = m * is;
+    const double out[6][2] = {{F[0][0], F[0][1]},
+                              {F[1][0], F[1][1]},
+                              {ms * F[2][0], ms * F[2][1]},
+                              {F[3][0] + F[4][0], F[3][1] + F[4][1]},
+                              {F[3][0] - F[4][0], F[3][1] - F[4][1]},
+                              {F[5][0], F[5][1]}};
     for (int q = 0; q < 6; ++q)
-      for (int ri = 0; ri < 2; ++ri) S[(((size_t)m * nlat + j) * 6 + q) * ncf + (f0 + fl) * 2 + ri] = out[q][ri];
-  }
+      for (int ri = 0; ri < 2; ++ri) A[((size_t)m * 6 + q) * 2 * nft + 2 * fl + ri] = out[q][ri];
+  });
+  __syncthreads();
+  stage_out(A, S, nlat, ncf, j, f0, nft, T.M);
+}
+
+// shared memory of the longitude pass (forward: adj = 0) and its transpose
+static size_t lon_smem(const vg_handle* h, int LF, bool adj) {
+  const LonTables T = lon_tables(h);
+  const int nphi = h->grid.nphi;
+  return (size_t)(6 * LF * 2 * T.M2 + 6 * LF * nphi + (adj ? LF * nphi : 0)) * sizeof(double);
+}
+
+static int lon_threads(const vg_handle* h, int LF) {
+  const LonTables T = lon_tables(h);
+  const int tiles = std::max(LF * T.ncg, LF * (T.nmg0 + T.nmg1));
+  return std::min(LON_THREADS, (tiles + 31) / 32 * 32);
+}
+
+constexpr size_t LON_SMEM_MAX = 220 * 1024;
+static void lon_attributes();  // the longitude kernels' shared-memory limit (defined after the transpose)
+
+static void lon_check(const vg_handle* h) {
+  if (lon_smem(h, LON_LF, true) > LON_SMEM_MAX) throw Error("visc3d: grid too large for the FP64 longitude pass");
 }
 
 // ------------------------------------------------------------------ scatter
@@ -417,11 +597,14 @@ void visc3d_enable(vg_handle* h, const double* pert) {
     visc3d_tc_enable(h);
     return;
   }
-  // work buffers of the FP64 path
+  // work buffers and longitude tables of the FP64 path
   const int nf = 3 * h->ne3d, ncf = 2 * nf;
   h->d_X.alloc((size_t)(h->nk + 1) * 4 * ncf);
   h->d_Y.alloc((size_t)G.M * G.nlat * 6 * ncf);
   h->d_dy.alloc((size_t)(h->nk + 1) * 6 * ncf);
+  lon_tables_build(h);
+  lon_check(h);  // the grid fits the longitude pass (throws otherwise)
+  lon_attributes();
   VG_CUDA(cudaStreamSynchronize(s));
 }
 
@@ -499,18 +682,11 @@ void visc3d_advance(vg_handle* h, const double* d_sigma, double dt) {
     VG_CUDA(cudaGetLastError());
   }
   // longitude pass
-  size_t lsm = (size_t)(6 * LON_FT * G.M * 2 + 6 * LON_FT * G.nphi) * sizeof(double);
-  static bool lon_attr = false;
-  if (!lon_attr) {
-    VG_CUDA(cudaFuncSetAttribute(k_v3_lon, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
-    lon_attr = true;
-  }
-  if (lsm > 200 * 1024) throw Error("visc3d: grid too large for the longitude pass");
-  dim3 lg(G.nlat, (nf + LON_FT - 1) / LON_FT);
   {
     PhaseScope pp(h, VG_PH_V3_LON_INV);
-    k_v3_lon<<<lg, 256, lsm, s>>>(h->d_Y.p, G.nlat, G.nphi, G.M, nf, dt, h->d_MkPerDt3.p, G.d_cos.p, G.d_sin.p,
-                                  G.d_invsin.p, h->v3_gstore);
+    const dim3 lg(G.nlat, (nf + LON_LF - 1) / LON_LF);
+    k_v3_lon<LON_LF><<<lg, lon_threads(h, LON_LF), lon_smem(h, LON_LF, false), s>>>(
+        h->d_Y.p, G.nlat, G.nphi, nf, dt, h->d_MkPerDt3.p, lon_tables(h), G.d_invsin.p, h->v3_gstore);
     ++h->n_launch;
     VG_CUDA(cudaGetLastError());
   }
@@ -568,37 +744,35 @@ __global__ void __launch_bounds__(256) k_v3_scatter_T(V3Args A, const double* __
   }
 }
 
-// longitude pass transposed, one CTA per (latitude j, 3-D element): the three
-// shape fields' forward grid values g (from the forward products Yf) and the
-// adjoint chain on Yb in place: analysis-input scales^T, forward DFT^T,
-// times -M dt, inverse DFT^T, dyadic components^T; and
-// d J / d (M dt)(j, i) += -sum over components and shapes of G_bar g
-__global__ void __launch_bounds__(256) k_v3_lon_T(const double* __restrict__ gstore, double* __restrict__ Yb,
-                                                  int nlat, int nphi, int M, int nf, double dt,
-                                                  const double* __restrict__ Mk3rate,
-                                                  const double* __restrict__ cs, const double* __restrict__ sn,
-                                                  const double* __restrict__ invsin, double* __restrict__ gradMdt) {
+// longitude pass transposed, one CTA per (latitude j, LF fields): the adjoint
+// chain on Yb in place: analysis-input combinations^T, analysis^T (a
+// synthesis with weights 2 pi / nphi), times -M dt, synthesis^T (an analysis
+// with weights 1 at m = 0, 2 above), dyadic components^T; and
+// d J / d (M dt)(j, i) += -sum over components and shapes of G_bar g, g the
+// forward grid that the forward pass stored in gstore
+template <int LF>
+__global__ void __launch_bounds__(LON_THREADS, 1)
+    k_v3_lon_T(const double* __restrict__ gstore, double* __restrict__ Yb, int nlat, int nphi, int nf, double dt,
+               const double* __restrict__ Mk3rate, LonTables T, const double* __restrict__ invsin,
+               double* __restrict__ gradMdt) {
   extern __shared__ double sm[];
-  constexpr int FT = 3;
-  const int j = blockIdx.x, ei = blockIdx.y, f0 = 3 * ei;
-  const int ncf = 2 * nf, half = nphi / 2, R = 6 * FT;
-  double* Cc = sm;                        // [R][M][2] adjoint component coefficients
-  double* gf = sm + (size_t)R * M * 2;    // [R][nphi] forward grid (stored by the forward pass)
-  double* Gb = gf + (size_t)R * nphi;     // [R][nphi] adjoint grid
+  const int j = blockIdx.x, f0 = blockIdx.y * LF;
+  const int nft = min(LF, nf - f0);
+  const int ncf = 2 * nf, half = T.half, wA = 2 * T.M2;
+  double* A = sm;                          // [6 LF][2 M2] adjoint Fourier coefficients
+  double* X = A + (size_t)6 * LF * wA;     // [6 LF][nphi] adjoint grid, parity combinations
+  double* P = X + (size_t)6 * LF * nphi;   // [LF][nphi] per-field G_bar . g
   const double is = invsin[j];
   const double scl = 2.0 * PI / (double)nphi;
-  // 1-2. the forward grid g of the element's three fields (row = c FT + fl)
-  for (int t = threadIdx.x; t < R * nphi; t += blockDim.x) {
-    const int row = t / nphi, i = t % nphi, c = row / FT, fl = row % FT;
-    gf[t] = gstore[(((size_t)j * nf + f0 + fl) * 6 + c) * nphi + i];
-  }
+  // 1. adjoint dyadic Fourier coefficients from the analysis-input adjoints
+  //    (staged in X as [m][q][2 nft])
+  stage_in(Yb, X, nlat, ncf, j, f0, nft, T.M);
   __syncthreads();
-  // 3. adjoint dyadic Fourier coefficients from the analysis-input adjoints
-  for (int t = threadIdx.x; t < FT * M; t += blockDim.x) {
-    const int fl = t / M, m = t % M;
+  for (int t = threadIdx.x; t < nft * T.M2; t += blockDim.x) {
+    const int fl = t / T.M2, m = t % T.M2;
     double o[6][2];
     for (int q = 0; q < 6; ++q)
-      for (int ri = 0; ri < 2; ++ri) o[q][ri] = Yb[(((size_t)m * nlat + j) * 6 + q) * ncf + (f0 + fl) * 2 + ri];
+      for (int ri = 0; ri < 2; ++ri) o[q][ri] = (m < T.M) ? X[((size_t)m * 6 + q) * 2 * nft + 2 * fl + ri] : 0.0;
     const double ms = m * is;
     const double Fb[6][2] = {{o[0][0], o[0][1]},
                              {o[1][0], o[1][1]},
@@ -607,60 +781,45 @@ __global__ void __launch_bounds__(256) k_v3_lon_T(const double* __restrict__ gst
                              {o[3][0] - o[4][0], o[3][1] - o[4][1]},
                              {o[5][0], o[5][1]}};
     for (int c = 0; c < 6; ++c) {
-      Cc[((c * FT + fl) * M + m) * 2] = Fb[c][0];
-      Cc[((c * FT + fl) * M + m) * 2 + 1] = Fb[c][1];
+      A[(size_t)(fl * 6 + c) * wA + 2 * m] = scl * Fb[c][0];
+      A[(size_t)(fl * 6 + c) * wA + 2 * m + 1] = scl * Fb[c][1];
     }
   }
   __syncthreads();
-  // 4. forward DFT^T: G_bar(i) = scl sum_m (Fre cos(m phi_i) - Fim sin(m phi_i))
-  for (int t = threadIdx.x; t < R * half; t += blockDim.x) {
-    const int row = t / half, i = t % half;
-    const double* c = Cc + (size_t)row * M * 2;
-    double ev = c[0], od = 0.0;  // m = 0: Fre only
-    int tw = i;
-    for (int m = 1; m < M; ++m) {
-      const double v = c[2 * m] * __ldg(&cs[tw]) - c[2 * m + 1] * __ldg(&sn[tw]);
-      if (m & 1)
-        od += v;
-      else
-        ev += v;
-      tw += i;
-      if (tw >= nphi) tw -= nphi;
+  // 2. analysis^T: G_bar(i) = scl sum_m (Fre cos(m phi_i) - Fim sin(m phi_i));
+  //    the per-field G_bar . g and g_bar = -M dt G_bar in parity form
+  lon_synth(A, nft, T, [&](int fl, int i, const double* b1, const double* b2) {
+    const int f = f0 + fl;
+    const double* Mr = Mk3rate + ((size_t)(f / 3) * nlat + j) * nphi;
+    const double m1 = Mr[i] * dt, m2 = Mr[i + half] * dt;
+    double p1 = 0.0, p2 = 0.0;
+    for (int c = 0; c < 6; ++c) {
+      const double* gs = gstore + (((size_t)j * nf + f) * 6 + c) * nphi;
+      p1 += b1[c] * gs[i];
+      p2 += b2[c] * gs[i + half];
+      const double a = -m1 * b1[c], b = -m2 * b2[c];
+      X[(size_t)(fl * 6 + c) * nphi + i] = a + b;
+      X[(size_t)(fl * 6 + c) * nphi + half + i] = a - b;
     }
-    Gb[(size_t)row * nphi + i] = scl * (ev + od);
-    Gb[(size_t)row * nphi + i + half] = scl * (ev - od);
-  }
+    P[(size_t)fl * nphi + i] = p1;
+    P[(size_t)fl * nphi + i + half] = p2;
+  });
   __syncthreads();
-  // 5. d J / d(M dt) and g_bar = -M dt G_bar (in place in Gb)
-  const double* Mr = Mk3rate + ((size_t)ei * nlat + j) * nphi;
-  for (int i = threadIdx.x; i < nphi; i += blockDim.x) {
-    double acc = 0.0;
-    for (int row = 0; row < R; ++row) acc += Gb[(size_t)row * nphi + i] * gf[(size_t)row * nphi + i];
-    gradMdt[((size_t)ei * nlat + j) * nphi + i] -= acc;
-    const double mdt = Mr[i] * dt;
-    for (int row = 0; row < R; ++row) Gb[(size_t)row * nphi + i] *= -mdt;
+  // 3. d J / d (M dt) of each element (three shape fields), one CTA per (j, element)
+  for (int t = threadIdx.x; t < (nft / 3) * nphi; t += blockDim.x) {
+    const int el = t / nphi, i = t % nphi;
+    const double acc = P[(size_t)(3 * el) * nphi + i] + P[(size_t)(3 * el + 1) * nphi + i] +
+                       P[(size_t)(3 * el + 2) * nphi + i];
+    gradMdt[((size_t)(f0 / 3 + el) * nlat + j) * nphi + i] -= acc;
   }
-  __syncthreads();
-  // 6. inverse DFT^T: c_bar(m) = w_m sum_i g_bar(i) (cos, -sin)(m phi_i), then
+  // 4. synthesis^T: c_bar(m) = w_m sum_i g_bar(i) (cos, -sin)(m phi_i), then
   //    the dyadic components^T into the product adjoints (written over Yb)
-  for (int t = threadIdx.x; t < FT * M; t += blockDim.x) {
-    const int fl = t / M, m = t % M;
+  lon_anal(X, nft, nphi, T, [&](int fl, int m, const double* re, const double* im) {
     const double w = (m == 0) ? 1.0 : 2.0;
     double cb[6][2];
     for (int c = 0; c < 6; ++c) {
-      const double* g = Gb + (size_t)(c * FT + fl) * nphi;
-      double re = 0.0, im = 0.0;
-      int tw = 0;
-      const double sgn = (m & 1) ? -1.0 : 1.0;
-      for (int i = 0; i < half; ++i) {
-        const double v = g[i] + sgn * g[i + half];
-        re += v * __ldg(&cs[tw]);
-        im -= v * __ldg(&sn[tw]);
-        tw += m;
-        if (tw >= nphi) tw -= nphi;
-      }
-      cb[c][0] = w * re;
-      cb[c][1] = (m == 0) ? 0.0 : w * im;
+      cb[c][0] = w * re[c];
+      cb[c][1] = (m == 0) ? 0.0 : w * im[c];
     }
     const double ms = m * is;
     const double Sb[6][2] = {{cb[0][0], cb[0][1]},
@@ -670,8 +829,10 @@ __global__ void __launch_bounds__(256) k_v3_lon_T(const double* __restrict__ gst
                              {cb[3][0] - cb[4][0], cb[3][1] - cb[4][1]},
                              {4.0 * cb[5][1], -4.0 * cb[5][0]}};
     for (int q = 0; q < 6; ++q)
-      for (int ri = 0; ri < 2; ++ri) Yb[(((size_t)m * nlat + j) * 6 + q) * ncf + (f0 + fl) * 2 + ri] = Sb[q][ri];
-  }
+      for (int ri = 0; ri < 2; ++ri) A[((size_t)m * 6 + q) * 2 * nft + 2 * fl + ri] = Sb[q][ri];
+  });
+  __syncthreads();
+  stage_out(A, Yb, nlat, ncf, j, f0, nft, T.M);
 }
 
 // gather^T: the synthesis-input adjoint (per product, combined into the four
@@ -714,6 +875,11 @@ __global__ void __launch_bounds__(256) k_v3_gather_T(V3Args A, const double* __r
     E[3 * plane + at] = v1;
     E[4 * plane + at] = u0 * xu[e] + u1 * xu[e + 1] + v0 * xv[e] + v1 * xv[e + 1];
   }
+}
+
+static void lon_attributes() {
+  for (const void* k : {(const void*)k_v3_lon<LON_LF>, (const void*)k_v3_lon_T<LON_LF>})
+    VG_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)LON_SMEM_MAX));
 }
 
 void visc3d_adjoint(vg_handle* h, const double* gstore, double dt, const double* lam, double* lam_new, double* E,
@@ -778,15 +944,11 @@ void visc3d_adjoint(vg_handle* h, const double* gstore, double dt, const double*
   Ab.in = h->d_v3a_dyb.p;
   Ab.out = h->d_v3a_Yb.p;
   k_v3_gemm<<<sgrid, 256, 0, s>>>(Ab);
-  const size_t lsm = (size_t)(18 * G.M * 2 + 2 * 18 * G.nphi) * sizeof(double);
-  static bool lon_attr = false;
-  if (!lon_attr) {
-    VG_CUDA(cudaFuncSetAttribute(k_v3_lon_T, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
-    lon_attr = true;
+  {
+    const dim3 lg(G.nlat, (nf + LON_LF - 1) / LON_LF);
+    k_v3_lon_T<LON_LF><<<lg, lon_threads(h, LON_LF), lon_smem(h, LON_LF, true), s>>>(
+        gstore, h->d_v3a_Yb.p, G.nlat, G.nphi, nf, dt, h->d_MkPerDt3.p, lon_tables(h), G.d_invsin.p, gradMdt);
   }
-  if (lsm > 200 * 1024) throw Error("vg_misfit_grad: grid too large for the transposed longitude pass");
-  k_v3_lon_T<<<dim3(G.nlat, h->ne3d), 256, lsm, s>>>(gstore, h->d_v3a_Yb.p, G.nlat, G.nphi, G.M, nf, dt,
-                                                       h->d_MkPerDt3.p, G.d_cos.p, G.d_sin.p, G.d_invsin.p, gradMdt);
   GemmArgs Sb = S;  // synthesis^T: the unweighted tables, per product out
   Sb.mode = 1;
   Sb.in = h->d_v3a_Yb.p;
