@@ -416,6 +416,12 @@ __global__ void __launch_bounds__(512) k_drift_T_deg1(int ne, int nr, int nk, in
 }
 
 // G1T[c][r] = G1[r][c] (degree-1 Green's block, rows r < nrow, columns c < ncol)
+// d J / d pert = scale * rate * d J / d (M dt), in place (scale = -ln 10 dt)
+__global__ void k_grad_pert(size_t n, double scale, const double* __restrict__ rate, double* __restrict__ g) {
+  const size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t < n) g[t] *= scale * rate[t];
+}
+
 __global__ void k_transpose(int nrow, int ncol, const double* __restrict__ A, double* __restrict__ AT) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= nrow * ncol) return;
@@ -649,19 +655,25 @@ double misfit_grad_dev(vg_handle* h, int nsteps, double dt, const double* sigma,
   if (grad_sigma) W.gsig.download(grad_sigma, (size_t)nsteps * n2, s);
   if (grad_pert) {
     // d J / d pert = d J / d(M dt) * (-ln 10) M dt on the 3-D elements' grid,
-    // (nphi, nlat, ne) like vg_enable_visc3d's input; zero elsewhere
+    // (nphi, nlat, ne) like vg_enable_visc3d's input; zero elsewhere. Formed
+    // on the device; each 3-D element's slab is copied into place.
     const size_t ng = G.ng;
-    std::fill(grad_pert, grad_pert + (size_t)ne * ng, 0.0);
     if (v3) {
-      std::vector<double> gm((size_t)h->ne3d * ng), rate((size_t)h->ne3d * ng);
-      W.gradMdt.download(gm.data(), gm.size(), s);
-      h->d_MkPerDt3.download(rate.data(), rate.size(), s);
-      VG_CUDA(cudaStreamSynchronize(s));
-      for (int ei = 0; ei < h->ne3d; ++ei)
-        for (size_t g = 0; g < ng; ++g) {
-          const size_t q = (size_t)ei * ng + g;
-          grad_pert[(size_t)h->e3d_h[ei] * ng + g] = -std::log(10.0) * rate[q] * dt * gm[q];
-        }
+      const size_t n3 = (size_t)h->ne3d * ng;
+      k_grad_pert<<<(unsigned)((n3 + 255) / 256), 256, 0, s>>>(n3, -std::log(10.0) * dt, h->d_MkPerDt3.p,
+                                                              W.gradMdt.p);
+      ++h->n_launch;
+      VG_CUDA(cudaGetLastError());
+    }
+    int e3 = 0;
+    for (int e = 0; e < ne; ++e) {
+      if (e3 < h->ne3d && h->e3d_h[e3] == e) {
+        VG_CUDA(cudaMemcpyAsync(grad_pert + (size_t)e * ng, W.gradMdt.p + (size_t)e3 * ng, ng * sizeof(double),
+                                cudaMemcpyDeviceToHost, s));
+        ++e3;
+      } else {
+        std::fill(grad_pert + (size_t)e * ng, grad_pert + (size_t)(e + 1) * ng, 0.0);
+      }
     }
   }
   h->cur = cur0;
