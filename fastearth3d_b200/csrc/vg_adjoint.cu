@@ -204,118 +204,197 @@ __device__ __forceinline__ void rhs_T(const double* __restrict__ Kp, const doubl
     }
 }
 
-// Transposed solve of one right-hand side with the degree's dgbtf2 factor
-// (A = P L U; kl = 6, kv = 12), x with element stride st, sliding windows in
-// registers. U^T sweep (forward): x_j = (z_j - sum_{i<=12} U(j-i, j) x_{j-i}) /
-// U(j, j), the 12 previous values held in w[]. L^T sweep (backward, pivots
-// undone): x_j -= sum_{i<=6} L(j+i, j) x_{j+i}, then swap x_j and x_{ipiv_j};
-// a value leaves the 7-value window v[] once no later swap can reach it.
-__device__ __forceinline__ void band_solve_T_window(const double* __restrict__ ab, int n,
-                                                    const int* __restrict__ ipiv, double* x, size_t st) {
-  constexpr int KL = 6, KV = 12, LD = VG_LDAB;
-  double w[KV], cu[KV + 1], cn[KV + 1];
-#pragma unroll
-  for (int i = 0; i < KV; ++i) w[i] = 0.0;
-#pragma unroll
-  for (int r = 0; r <= KV; ++r) cn[r] = __ldg(&ab[r]);  // column 0: rows 0..KV (U part and diagonal)
-  double xn = x[0];
-  for (int j = 0; j < n; ++j) {  // 0-based column j; the next column is loaded one step ahead
-#pragma unroll
-    for (int r = 0; r <= KV; ++r) cu[r] = cn[r];
-    const double xj = xn;
-    if (j + 1 < n) {
-      const double* nc = ab + (size_t)(j + 1) * LD;
-#pragma unroll
-      for (int r = 0; r <= KV; ++r) cn[r] = __ldg(&nc[r]);
-      xn = x[(size_t)(j + 1) * st];
-    }
-    double t = xj;
-#pragma unroll
-    for (int i = 1; i <= KV; ++i)
-      if (i <= j) t -= cu[KV - i] * w[i - 1];
-    t = t / cu[KV];
-    x[(size_t)j * st] = t;
-#pragma unroll
-    for (int i = KV - 1; i > 0; --i) w[i] = w[i - 1];
-    w[0] = t;
-  }
-  double v[KL + 1];  // v[i] = x_{j+i}, starting at j = n - 1 (nothing beyond it)
-  v[0] = x[(size_t)(n - 1) * st];
-#pragma unroll
-  for (int i = 1; i <= KL; ++i) v[i] = 0.0;
-  double ln[KL], lc[KL];
-  int pn = 0;
-  if (n >= 2) {
-    const double* c0 = ab + (size_t)(n - 2) * LD;
-#pragma unroll
-    for (int i = 0; i < KL; ++i) ln[i] = __ldg(&c0[KV + 1 + i]);
-    pn = ipiv[n - 2];
-  }
-  double xl = (n >= 2) ? x[(size_t)(n - 2) * st] : 0.0;
-  for (int j = n - 2; j >= 0; --j) {
-#pragma unroll
-    for (int i = 0; i < KL; ++i) lc[i] = ln[i];
-    const int pj = pn;
-    const double xj = xl;
-    if (j >= 1) {
-      const double* c1 = ab + (size_t)(j - 1) * LD;
-#pragma unroll
-      for (int i = 0; i < KL; ++i) ln[i] = __ldg(&c1[KV + 1 + i]);
-      pn = ipiv[j - 1];
-      xl = x[(size_t)(j - 1) * st];
-    }
-    // shift the window down by one: v[i] = x_{j+i}; x_{j+1+KL} is final
-    const double out = v[KL];
-    if (j + 1 + KL <= n - 1) x[(size_t)(j + 1 + KL) * st] = out;
-#pragma unroll
-    for (int i = KL; i > 0; --i) v[i] = v[i - 1];
-    double t = xj;
-#pragma unroll
-    for (int i = 1; i <= KL; ++i)
-      if (j + i <= n - 1) t -= lc[i - 1] * v[i];
-    v[0] = t;
-    const int d = pj - j;  // 0 .. KL
-    if (d != 0) {
-      double vd = v[0];
-#pragma unroll
-      for (int i = 1; i <= KL; ++i)
-        if (i == d) {
-          vd = v[i];
-          v[i] = v[0];
-        }
-      v[0] = vd;
-    }
-  }
-#pragma unroll
-  for (int i = 0; i <= KL; ++i)
-    if (i <= n - 1) x[(size_t)i * st] = v[i];
+// ---- shared-memory staging of the transposed sweeps (cp.async, double-buffered) ----
+constexpr int TS_CH = 32;                     // band columns (sweep steps) per chunk
+constexpr int TS_BAND = 2 * TS_CH * VG_LDAB;  // two band chunks
+constexpr int TS_AUX = 2 * TS_CH * 32;        // two chunks of per-lane entering values
+constexpr int TS_WARP = TS_BAND + TS_AUX;     // doubles of shared memory per warp
+constexpr int TS_WARPS = 4;                   // warps (tasks) per block
+
+__device__ __forceinline__ void ts_cp8(double* s, const double* g) {
+  const unsigned sa = (unsigned)__cvta_generic_to_shared(s);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(sa), "l"(g) : "memory");
+}
+__device__ __forceinline__ void ts_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void ts_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
 }
 
-// transposed solves of the drift (degrees >= 2), one thread per (slot, re/im)
-__global__ void __launch_bounds__(32) k_drift_T(int nr, int nd, int nk, const int* __restrict__ kdeg,
-                                                const double* __restrict__ ab, const double* __restrict__ dcv,
-                                                const int* __restrict__ ipiv, const double* __restrict__ dUn_bar,
-                                                const double* __restrict__ dVn_bar,
-                                                const double* __restrict__ surf_bar, double* __restrict__ w) {
-  const int k = blockIdx.x * blockDim.x + threadIdx.x, ri = blockIdx.y;
-  if (k >= nk) return;
-  const int l = kdeg[k];
-  if (l < 2) return;
-  const double* dc = dcv + (size_t)(l - 2) * nd;
-  double* x = w + (size_t)ri * nd * nk + k;
-  for (int node = 0; node < nr; ++node) {
-    double xu = dUn_bar[((size_t)ri * nr + node) * nk + k], xv = dVn_bar[((size_t)ri * nr + node) * nk + k];
-    double xf = 0.0;
-    if (node == nr - 1) {
-      xu += surf_bar[(size_t)(0 + ri) * nk + k];
-      xf = surf_bar[(size_t)(2 + ri) * nk + k];
-    }
-    x[(size_t)(4 * node) * nk] = dc[4 * node] * xu;
-    x[(size_t)(4 * node + 1) * nk] = dc[4 * node + 1] * xv;
-    x[(size_t)(4 * node + 2) * nk] = dc[4 * node + 2] * xf;
-    if (node < nr - 1) x[(size_t)(4 * node + 3) * nk] = 0.0;
+// band records of columns [c0, c0 + TS_CH) of one degree; zero outside [0, nd)
+__device__ __forceinline__ void ts_stage_band(double* dst, const double* ab, int c0, int nd, int lane) {
+  for (int t = lane; t < TS_CH * VG_LDAB; t += 32) {
+    const int col = c0 + t / VG_LDAB;
+    if (col >= 0 && col < nd)
+      ts_cp8(dst + t, ab + (size_t)col * VG_LDAB + (t % VG_LDAB));
+    else
+      dst[t] = 0.0;
   }
-  band_solve_T_window(ab + (size_t)(l - 2) * VG_LDAB * nd, nd, ipiv + (size_t)(l - 2) * nd, x, nk);
+}
+
+// Transposed drift solves (degrees >= 2), one warp per task: up to 16 slots of
+// one degree x (re, im), the forward sweeps' task list. With A = P L U the
+// dgbtf2 factor (kl = 6, kv = 12) and the drift's right-hand side scaled by
+// the column equilibration dc:
+//   U^T sweep (ascending): x_j = (z_j - sum_{i<=12} U(j-i, j) x_{j-i}) / U(j, j),
+//     z_j = dc_j (U-bar, V-bar, F-bar at the dofs of node j/4; surface terms at
+//     the last node), the 12 previous values in registers;
+//   L^T sweep (descending, pivots undone): x_j -= sum_{i<=6} L(j+i, j) x_{j+i},
+//     then swap x_j and x_{j + jp_j}; a value leaves the 7-value window once
+//     no later swap can reach it.
+// The degree's band columns stream through shared memory in chunks of 32 so
+// that every load on the recurrences is a shared-memory load; the per-lane
+// entering values (U-bar / V-bar in the U^T sweep, its output in the L^T
+// sweep) are staged the same way one chunk ahead.
+__global__ void __launch_bounds__(32 * TS_WARPS) k_drift_T(int nr, int nd, int nk, const int4* __restrict__ tasks,
+                                                           int ntask, const double* __restrict__ ab_all,
+                                                           const double* __restrict__ dcv,
+                                                           const double* __restrict__ dUn_bar,
+                                                           const double* __restrict__ dVn_bar,
+                                                           const double* __restrict__ surf_bar,
+                                                           double* __restrict__ w) {
+  constexpr int KL = 6, KV = 12;
+  extern __shared__ double smem[];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int tix = blockIdx.x * TS_WARPS + warp;
+  if (tix >= ntask) return;  // whole warp
+  const int4 T = tasks[tix];
+  const int l = T.x, k0 = T.y, nsl = T.z;
+  const int sl = lane & 15, ri = lane >> 4;
+  const bool valid = sl < nsl;
+  const int k = k0 + (valid ? sl : 0);
+  double* sband = smem + (size_t)warp * TS_WARP;
+  double* saux = sband + TS_BAND;
+  const double* ab = ab_all + (size_t)(l - 2) * VG_LDAB * nd;
+  const double* dc = dcv + (size_t)(l - 2) * nd;
+  const double* ub = dUn_bar + (size_t)ri * nr * nk + k;
+  const double* vb = dVn_bar + (size_t)ri * nr * nk + k;
+  double* x = w + (size_t)ri * nd * nk + k;
+  const double sU = surf_bar[(size_t)(0 + ri) * nk + k], sF = surf_bar[(size_t)(2 + ri) * nk + k];
+  // ---- U^T sweep ----
+  // entering U-bar, V-bar of chunk c (columns 32c .. 32c+31 = nodes 8c .. 8c+7) at slot (2 node' + uv)
+  auto stage_z = [&](double* dst, int c) {
+#pragma unroll
+    for (int q = 0; q < 16; ++q) {
+      const int node = 8 * c + (q >> 1);
+      if (node < nr)
+        ts_cp8(dst + q * 32 + lane, ((q & 1) ? vb : ub) + (size_t)node * nk);
+      else
+        dst[q * 32 + lane] = 0.0;
+    }
+  };
+  const int nch = (nd + TS_CH - 1) / TS_CH;
+  ts_stage_band(sband, ab, 0, nd, lane);
+  stage_z(saux, 0);
+  ts_commit();
+  double wv[KV];  // wv[i] = x_{j-1-i}
+#pragma unroll
+  for (int i = 0; i < KV; ++i) wv[i] = 0.0;
+  for (int c = 0; c < nch; ++c) {
+    const int cur = c & 1;
+    if (c + 1 < nch) {
+      ts_stage_band(sband + (cur ^ 1) * TS_CH * VG_LDAB, ab, TS_CH * (c + 1), nd, lane);
+      stage_z(saux + (cur ^ 1) * TS_CH * 32, c + 1);
+      ts_commit();
+      ts_wait<1>();
+    } else {
+      ts_wait<0>();
+    }
+    __syncwarp();
+    const double* bandc = sband + cur * TS_CH * VG_LDAB;
+    const double* zin = saux + cur * TS_CH * 32;
+#pragma unroll 4
+    for (int jj = 0; jj < TS_CH; ++jj) {
+      const int j = TS_CH * c + jj;
+      if (j >= nd) break;
+      const int node = j >> 2, typ = j & 3;
+      double raw = (typ == 0) ? zin[(2 * (jj >> 2)) * 32 + lane] : (typ == 1) ? zin[(2 * (jj >> 2) + 1) * 32 + lane] : 0.0;
+      if (node == nr - 1) {
+        if (typ == 0) raw += sU;
+        if (typ == 2) raw = sF;
+      }
+      const double* col = bandc + jj * VG_LDAB;
+      double t = __ldg(&dc[j]) * raw;
+#pragma unroll
+      for (int i = 1; i <= KV; ++i)
+        if (i <= j) t -= col[KV - i] * wv[i - 1];
+      t = t / col[KV];
+      if (valid) x[(size_t)j * nk] = t;
+#pragma unroll
+      for (int i = KV - 1; i > 0; --i) wv[i] = wv[i - 1];
+      wv[0] = t;
+    }
+    __syncwarp();  // the buffer just read is refilled by the next prefetch
+  }
+  __threadfence_block();  // x stores before this lane's own cp.async reads of them
+  // ---- L^T sweep: steps j = nd-2 .. 0; chunk c covers j = jhi-31 .. jhi, jhi = nd-2-32c ----
+  auto stage_x = [&](double* dst, int c) {
+    const int jlo = nd - 2 - TS_CH * c - (TS_CH - 1);
+#pragma unroll 4
+    for (int q = 0; q < TS_CH; ++q) {
+      const int j = jlo + q;
+      if (j >= 0 && valid)
+        ts_cp8(dst + q * 32 + lane, x + (size_t)j * nk);
+      else
+        dst[q * 32 + lane] = 0.0;
+    }
+  };
+  double v[KL + 1];  // v[i] = x_{j+i}, starting at j = nd - 1 (nothing beyond it)
+  v[0] = valid ? x[(size_t)(nd - 1) * nk] : 0.0;
+#pragma unroll
+  for (int i = 1; i <= KL; ++i) v[i] = 0.0;
+  const int nchl = (nd - 1 + TS_CH - 1) / TS_CH;
+  if (nchl > 0) {
+    ts_stage_band(sband, ab, nd - 2 - (TS_CH - 1), nd, lane);
+    stage_x(saux, 0);
+    ts_commit();
+  }
+  for (int c = 0; c < nchl; ++c) {
+    const int cur = c & 1, jlo = nd - 2 - TS_CH * c - (TS_CH - 1);
+    if (c + 1 < nchl) {
+      ts_stage_band(sband + (cur ^ 1) * TS_CH * VG_LDAB, ab, jlo - TS_CH, nd, lane);
+      stage_x(saux + (cur ^ 1) * TS_CH * 32, c + 1);
+      ts_commit();
+      ts_wait<1>();
+    } else {
+      ts_wait<0>();
+    }
+    __syncwarp();
+    const double* bandc = sband + cur * TS_CH * VG_LDAB;
+    const double* xin = saux + cur * TS_CH * 32;
+#pragma unroll 4
+    for (int jj = TS_CH - 1; jj >= 0; --jj) {
+      const int j = jlo + jj;
+      if (j < 0) break;
+      const double out = v[KL];  // x_{j+1+KL} is final
+      if (valid && j + 1 + KL <= nd - 1) x[(size_t)(j + 1 + KL) * nk] = out;
+#pragma unroll
+      for (int i = KL; i > 0; --i) v[i] = v[i - 1];
+      const double* col = bandc + jj * VG_LDAB;
+      double t = xin[jj * 32 + lane];
+#pragma unroll
+      for (int i = 1; i <= KL; ++i)
+        if (j + i <= nd - 1) t -= col[KV + i] * v[i];
+      v[0] = t;
+      const int d = (int)col[20];  // jp_j = ipiv_j - j, 0 .. KL
+      if (d != 0) {
+        double vd = v[0];
+#pragma unroll
+        for (int i = 1; i <= KL; ++i)
+          if (i == d) {
+            vd = v[i];
+            v[i] = v[0];
+          }
+        v[0] = vd;
+      }
+    }
+    __syncwarp();
+  }
+  if (valid) {
+#pragma unroll
+    for (int i = 0; i <= KL; ++i)
+      if (i <= nd - 1) x[(size_t)i * nk] = v[i];
+  }
 }
 
 // K^T after the transposed solves (degrees >= 2): a thread per (slot,
@@ -604,7 +683,6 @@ double misfit_grad_dev(vg_handle* h, int nsteps, double dt, const double* sigma,
   ensure(W.gsig, (size_t)nsteps * n2);
   VG_CUDA(cudaMemsetAsync(W.lam.p, 0, S * sizeof(double), s));  // no terminal cost: lam_N = 0
   VG_CUDA(cudaMemsetAsync(W.gsig.p, 0, (size_t)nsteps * n2 * sizeof(double), s));
-  const dim3 kg((nk + 31) / 32, 2);
   const dim3 eg((nk + 31) / 32, (ne + 7) / 8, 2), ng_((nk + 31) / 32, (nr + 7) / 8, 2);
   ensure(W.E, (size_t)5 * 2 * ne * nk);
   {
@@ -616,6 +694,12 @@ double misfit_grad_dev(vg_handle* h, int nsteps, double dt, const double* sigma,
     }
   }
   const size_t shm1 = (size_t)(4 * (2 * nr + 1) + 4 * 2 * nr) * sizeof(double);
+  const size_t ts_smem = (size_t)TS_WARPS * TS_WARP * sizeof(double);
+  static bool ts_attr = false;
+  if (!ts_attr) {
+    VG_CUDA(cudaFuncSetAttribute(k_drift_T, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ts_smem));
+    ts_attr = true;
+  }
   if (v3) {
     const size_t ngm = (size_t)h->ne3d * G.ng;
     ensure(W.gradMdt, ngm);
@@ -643,8 +727,8 @@ double misfit_grad_dev(vg_handle* h, int nsteps, double dt, const double* sigma,
                                                W.E.p);
     if (v3) visc3d_adjoint(h, W.gseg.p + (size_t)(n - n0) * gsz, dt, W.lam.p, W.lam_new.p, W.E.p, W.gradMdt.p);
     k_adv1d_T_node<<<ng_, dim3(32, 8), 0, s>>>(ne, nr, nk, h->d_k2lm.p, W.E.p, W.dUn_bar.p, W.dVn_bar.p, sbar);
-    k_drift_T<<<kg, 32, 0, s>>>(nr, nd, nk, h->d_kdeg.p, h->d_ab.p, h->d_dc.p, h->d_ipiv.p, W.dUn_bar.p,
-                                W.dVn_bar.p, W.surf_bar.p, W.w.p);
+    k_drift_T<<<(h->ntask + TS_WARPS - 1) / TS_WARPS, 32 * TS_WARPS, ts_smem, s>>>(
+        nr, nd, nk, h->d_tasks.p, h->ntask, h->d_ab.p, h->d_dc.p, W.dUn_bar.p, W.dVn_bar.p, W.surf_bar.p, W.w.p);
     k_rhs_T<<<eg, dim3(32, 8), 0, s>>>(ne, nd, nk, h->d_kdeg.p, h->d_dr.p, h->d_Krhs.p, W.w.p, W.lam_new.p);
     k_drift_T_deg1<<<1, 512, shm1, s>>>(ne, nr, nk, h->p.deg1_cm, h->d_dr1.p, h->d_null1.p, W.G1T.p, h->d_Krhs.p,
                                         W.dUn_bar.p, W.dVn_bar.p, W.surf_bar.p, W.lam_new.p);
