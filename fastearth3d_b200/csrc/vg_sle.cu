@@ -270,23 +270,32 @@ __global__ void k_bsl_rows(int nphi, const double* __restrict__ hi, const double
 
 // ------------------------------------------------------------------ fused inner loop
 // The inner load fixed point of sle_solve (src/vilma_sle.f90:280-340) as one
-// cooperative persistent kernel: one CTA per SM, phases separated by a grid
-// barrier, the convergence test on the device, so no host round trip per
-// iteration. Each phase keeps the arithmetic (and the per-thread summation
-// order) of the separate kernels it replaces:
-//   1 load + longitude analysis per row     (k_load_fourier)
-//   2 Legendre analysis + apply, warp per lm (k_legendre_analysis, k_apply)
-//   3 Legendre synthesis of u and N          (k_legendre_synth)
-//   4 longitude synthesis, Sraw, row sums    (k_synth_sraw)
-//   5 mass-conserving dphi                   (k_dphi)
-//   6 rsl update, row maxima                 (k_rsl_update)
-//   7 convergence                            (k_conv)
+// cooperative persistent kernel: one CTA per SM, the convergence test on the
+// device, so no host round trip per iteration. Four grid barriers an
+// iteration:
+//   L  total load of each row and its longitude analysis (the CTA that owns
+//      the row; for the next iteration it runs right after U, on the rows the
+//      CTA has just updated)
+//   A  Legendre analysis + apply, warp per lm                 | barrier
+//   S  Legendre synthesis of u and N, thread per (b, m, j)    | barrier
+//   R  longitude synthesis, Sraw = N - u (+ s_rot), row sums  | barrier
+//   U  mass-conserving dphi (every CTA, rows summed in order by one thread,
+//      so all CTAs agree), rsl update, row maxima, then L     | barrier
+//   convergence (every CTA from the row maxima, the same decision everywhere)
+// The longitude transforms split the half periods (phi + pi flips odd m) and
+// spread each output's sum over several threads, so no thread runs a loop of
+// more than about nphi / 6 terms.
+constexpr int SLE_LCH = 16;  // degrees per Legendre synthesis chunk
+
 struct InnerArgs {
   int nphi, nlat, M, nlm, nk, lmax, n_inner;
   double tol, dlon, g;
   const double *dig, *C, *wcorr, *cs, *sn, *plm, *wts, *gu, *gn, *drift, *srot;
   const int *lm_m, *lm_l, *lm2k, *mbeg;
-  double *rsl, *F, *sigma, *ulm, *Gs, *Sraw, *rowpart;
+  const int2* chunk;  // Legendre synthesis chunks: (m, first l - m), at most SLE_LCH degrees each
+  const int* cbeg;    // first chunk of each order (M + 1)
+  int nchunk;
+  double *rsl, *F, *sigma, *ulm, *Gp, *Sraw, *rowpart;
   SleScalars* sc;
   unsigned int* bar;  // count, generation, error
 };
@@ -333,128 +342,255 @@ __device__ bool grid_barrier(unsigned int* bar, unsigned int& gen) {
   return s_ok != 0;
 }
 
+// L for row j: the total surface load and its longitude analysis into F
+// (F_m = 2 pi / nphi sum_i f_i e^{-i m phi_i}; even m read f_i + f_{i+half},
+// odd m f_i - f_{i+half}); tpm threads per order, partial sums in part[2][nthr]
+__device__ __forceinline__ void sle_row_load(const InnerArgs& A, int j, double* sm, double* part) {
+  const int tid = threadIdx.x, nthr = blockDim.x, nphi = A.nphi, M = A.M, half = nphi / 2;
+  const double sc_f = 2.0 * PI / (double)nphi;
+  __syncthreads();
+  for (int i = tid; i < nphi; i += nthr) {
+    const size_t p = (size_t)j * nphi + i;
+    sm[i] = RHO_ICE * A.dig[p] + RHO_WATER * (A.C[p] * A.rsl[p]) + A.wcorr[p];
+  }
+  __syncthreads();
+  const int tpm = max(1, min(8, nthr / M));
+  for (int base = 0; base < M * tpm; base += nthr) {
+    const int u = base + tid, m = u / tpm, q = u % tpm;
+    const bool act = u < M * tpm;
+    double re = 0.0, im = 0.0;
+    if (act) {
+      const double sg = (m & 1) ? -1.0 : 1.0;
+      const int step = (m * tpm) % nphi;
+      int t = (m * q) % nphi;
+      for (int i = q; i < half; i += tpm) {
+        const double v = sm[i] + sg * sm[i + half];
+        re += v * __ldg(&A.cs[t]);
+        im -= v * __ldg(&A.sn[t]);
+        t += step;
+        if (t >= nphi) t -= nphi;
+      }
+    }
+    part[tid] = re;
+    part[nthr + tid] = im;
+    __syncthreads();
+    if (act && q == 0) {
+      double r = 0.0, s2 = 0.0;
+      for (int c = 0; c < tpm; ++c) {
+        r += part[tid + c];
+        s2 += part[nthr + tid + c];
+      }
+      A.F[((size_t)m * A.nlat + j) * 2] = r * sc_f;
+      A.F[((size_t)m * A.nlat + j) * 2 + 1] = s2 * sc_f;
+    }
+    __syncthreads();
+  }
+}
+
 __global__ void __launch_bounds__(512) k_sle_inner(InnerArgs A) {
-  extern __shared__ double sm[];  // max(nphi, 4 M) doubles
+  extern __shared__ double sm[];  // max(nphi, 4 M + 4 nchunk) doubles
   __shared__ double red[512];
+  __shared__ double part[4 * 512];
+  __shared__ double s_val;
   __shared__ int s_stop;
   const int tid = threadIdx.x, nthr = blockDim.x;
   const int lane = tid & 31, wid = tid >> 5, nw = nthr >> 5;
-  const int nphi = A.nphi, nlat = A.nlat, M = A.M, nlm = A.nlm;
-  const double sc_f = 2.0 * PI / (double)nphi;
+  const int nphi = A.nphi, nlat = A.nlat, M = A.M, nlm = A.nlm, half = nphi / 2;
   unsigned int gen = 0;
-  int it = 0;
-  for (it = 1; it <= A.n_inner; ++it) {
-    // 1. total surface load of each row and its longitude analysis
-    for (int j = blockIdx.x; j < nlat; j += gridDim.x) {
-      __syncthreads();
-      for (int i = tid; i < nphi; i += nthr) {
-        const size_t p = (size_t)j * nphi + i;
-        sm[i] = RHO_ICE * A.dig[p] + RHO_WATER * (A.C[p] * A.rsl[p]) + A.wcorr[p];
+  // L of the first iteration
+  for (int j = blockIdx.x; j < nlat; j += gridDim.x) sle_row_load(A, j, sm, part);
+  if (!grid_barrier(A.bar, gen)) return;
+  for (int it = 1; it <= A.n_inner; ++it) {
+    // A. Legendre analysis (warp per lm, four lm of a warp at once) and the
+    //    affine response u, N
+    for (int lm0 = blockIdx.x * nw + wid; lm0 < nlm; lm0 += 4 * gridDim.x * nw) {
+      constexpr int U4 = 4;
+      double re[U4], im[U4];
+      int lmv[U4];
+      const double* Fm[U4];
+      const double* P[U4];
+#pragma unroll
+      for (int u = 0; u < U4; ++u) {
+        lmv[u] = lm0 + u * gridDim.x * nw;
+        const int lmc = min(lmv[u], nlm - 1);  // past the end: a valid row, result unused
+        Fm[u] = A.F + ((size_t)A.lm_m[lmc] * nlat) * 2;
+        P[u] = A.plm + (size_t)lmc * nlat;
+        re[u] = 0.0;
+        im[u] = 0.0;
       }
-      __syncthreads();
-      for (int m = tid; m < M; m += nthr) {
-        double re = 0.0, im = 0.0;
-        int t = 0;
-        for (int i = 0; i < nphi; ++i) {
-          const double f = sm[i];
-          re += f * __ldg(&A.cs[t]);
-          im -= f * __ldg(&A.sn[t]);
-          t += m;
-          if (t >= nphi) t -= nphi;
-        }
-        A.F[((size_t)m * nlat + j) * 2] = re * sc_f;
-        A.F[((size_t)m * nlat + j) * 2 + 1] = im * sc_f;
-      }
-    }
-    if (!grid_barrier(A.bar, gen)) return;
-    // 2. Legendre analysis (warp per lm) and the affine response u, N
-    for (int lm = blockIdx.x * nw + wid; lm < nlm; lm += gridDim.x * nw) {
-      const int m = A.lm_m[lm];
-      const double* Fm = A.F + ((size_t)m * nlat) * 2;
-      const double* P = A.plm + (size_t)lm * nlat;
-      double re = 0.0, im = 0.0;
       for (int j = lane; j < nlat; j += 32) {
-        const double wp = A.wts[j] * P[j];
-        re += wp * Fm[2 * j];
-        im += wp * Fm[2 * j + 1];
+        const double w = A.wts[j];
+#pragma unroll
+        for (int u = 0; u < U4; ++u) {
+          const double wp = w * P[u][j];
+          re[u] += wp * Fm[u][2 * j];
+          im[u] += wp * Fm[u][2 * j + 1];
+        }
       }
-      for (int o = 16; o > 0; o >>= 1) {
-        re += __shfl_down_sync(0xffffffffu, re, o);
-        im += __shfl_down_sync(0xffffffffu, im, o);
+#pragma unroll
+      for (int u = 0; u < U4; ++u)
+        for (int o = 16; o > 0; o >>= 1) {
+          re[u] += __shfl_down_sync(0xffffffffu, re[u], o);
+          im[u] += __shfl_down_sync(0xffffffffu, im[u], o);
+        }
+      // lanes 0..3 write lm u (the sums are in lane 0; broadcast them)
+#pragma unroll
+      for (int u = 0; u < U4; ++u) {
+        re[u] = __shfl_sync(0xffffffffu, re[u], 0);
+        im[u] = __shfl_sync(0xffffffffu, im[u], 0);
       }
-      if (lane == 0) {
-        A.sigma[2 * lm] = re;
-        A.sigma[2 * lm + 1] = im;
-        const int l = A.lm_l[lm];
-        double* u = A.ulm;
-        double* n = A.ulm + 2 * (size_t)nlm;
-        if (l == 0) {
-          u[2 * lm] = A.gu[0] * re;
-          u[2 * lm + 1] = A.gu[0] * im;
-          n[2 * lm] = A.gn[0] * re;
-          n[2 * lm + 1] = A.gn[0] * im;
-        } else {
-          const int k = A.lm2k[lm];
-          u[2 * lm] = A.gu[l] * re + A.drift[(size_t)0 * A.nk + k];
-          u[2 * lm + 1] = A.gu[l] * im + A.drift[(size_t)1 * A.nk + k];
-          n[2 * lm] = A.gn[l] * re - A.drift[(size_t)2 * A.nk + k] / A.g;
-          n[2 * lm + 1] = A.gn[l] * im - A.drift[(size_t)3 * A.nk + k] / A.g;
+      if (lane < U4) {
+        double r = re[0], i2 = im[0];
+#pragma unroll
+        for (int u = 1; u < U4; ++u)
+          if (lane == u) {
+            r = re[u];
+            i2 = im[u];
+          }
+        const int lm = lmv[lane];
+        if (lm < nlm) {
+          A.sigma[2 * lm] = r;
+          A.sigma[2 * lm + 1] = i2;
+          const int l = A.lm_l[lm];
+          double* uu = A.ulm;
+          double* n = A.ulm + 2 * (size_t)nlm;
+          if (l == 0) {
+            uu[2 * lm] = A.gu[0] * r;
+            uu[2 * lm + 1] = A.gu[0] * i2;
+            n[2 * lm] = A.gn[0] * r;
+            n[2 * lm + 1] = A.gn[0] * i2;
+          } else {
+            const int k = A.lm2k[lm];
+            uu[2 * lm] = A.gu[l] * r + A.drift[(size_t)0 * A.nk + k];
+            uu[2 * lm + 1] = A.gu[l] * i2 + A.drift[(size_t)1 * A.nk + k];
+            n[2 * lm] = A.gn[l] * r - A.drift[(size_t)2 * A.nk + k] / A.g;
+            n[2 * lm + 1] = A.gn[l] * i2 - A.drift[(size_t)3 * A.nk + k] / A.g;
+          }
         }
       }
     }
     if (!grid_barrier(A.bar, gen)) return;
-    // 3. Legendre synthesis of u (b = 0) and N (b = 1): a thread per (b, m, j)
-    for (int t = blockIdx.x * nthr + tid; t < 2 * M * nlat; t += gridDim.x * nthr) {
-      const int j = t % nlat, m = (t / nlat) % M, b = t / (nlat * M);
-      const int lm0 = A.mbeg[m];
-      const double* qb = A.ulm + (size_t)b * nlm * 2;
-      double re = 0.0, im = 0.0;
-      for (int l = m; l <= A.lmax; ++l) {
-        const double p = A.plm[(size_t)(lm0 + l - m) * nlat + j];
-        re += qb[2 * (lm0 + l - m)] * p;
-        im += qb[2 * (lm0 + l - m) + 1] * p;
+    // S. Legendre synthesis of u and N in chunks of at most SLE_LCH degrees: a
+    //    thread per (chunk, j), partial sums Gp[j][chunk][u re, u im, N re, N im]
+    //    (one 32-byte sector per thread; a row's partials contiguous)
+    for (int t = blockIdx.x * nthr + tid; t < A.nchunk * nlat; t += gridDim.x * nthr) {
+      const int c = t / nlat, j = t % nlat;
+      const int2 ch = A.chunk[c];
+      const int n = min(SLE_LCH, A.lmax - ch.x + 1 - ch.y);
+      const int lm = A.mbeg[ch.x] + ch.y;
+      const double* pc = A.plm + (size_t)lm * nlat + j;
+      const double* qu = A.ulm + 2 * (size_t)lm;
+      const double* qn = A.ulm + 2 * ((size_t)nlm + lm);
+      double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
+#pragma unroll 4
+      for (int q = 0; q < n; ++q) {
+        const double p = pc[(size_t)q * nlat];
+        a0 += qu[2 * q] * p;
+        a1 += qu[2 * q + 1] * p;
+        a2 += qn[2 * q] * p;
+        a3 += qn[2 * q + 1] * p;
       }
-      A.Gs[(((size_t)b * M + m) * nlat + j) * 2] = re;
-      A.Gs[(((size_t)b * M + m) * nlat + j) * 2 + 1] = im;
+      double* o = A.Gp + ((size_t)j * A.nchunk + c) * 4;
+      o[0] = a0;
+      o[1] = a1;
+      o[2] = a2;
+      o[3] = a3;
     }
     if (!grid_barrier(A.bar, gen)) return;
-    // 4. longitude synthesis, Sraw = N - u (+ s_rot), row sums of C Sraw
+    // R. longitude synthesis (g(i) = G_0 + 2 sum_m Re G_m e^{i m phi_i}, even and
+    //    odd m apart, tpi threads per longitude pair (i, i + half)),
+    //    Sraw = N - u (+ s_rot), row sums of C Sraw
     for (int j = blockIdx.x; j < nlat; j += gridDim.x) {
       double* Gu = sm;
       double* Gn = sm + 2 * M;
+      double* gp = sm + 4 * M;  // the row's partial sums, staged
       __syncthreads();
-      for (int m = tid; m < M; m += nthr) {
-        Gu[2 * m] = A.Gs[((size_t)m * nlat + j) * 2];
-        Gu[2 * m + 1] = A.Gs[((size_t)m * nlat + j) * 2 + 1];
-        Gn[2 * m] = A.Gs[(((size_t)M + m) * nlat + j) * 2];
-        Gn[2 * m + 1] = A.Gs[(((size_t)M + m) * nlat + j) * 2 + 1];
+      for (int t = tid; t < 4 * A.nchunk; t += nthr) gp[t] = A.Gp[(size_t)j * A.nchunk * 4 + t];
+      __syncthreads();
+      for (int m = tid; m < M; m += nthr) {  // the order's chunks summed in order
+        double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
+        for (int c = A.cbeg[m]; c < A.cbeg[m + 1]; ++c) {
+          const double* o = gp + 4 * c;
+          a0 += o[0];
+          a1 += o[1];
+          a2 += o[2];
+          a3 += o[3];
+        }
+        Gu[2 * m] = a0;
+        Gu[2 * m + 1] = a1;
+        Gn[2 * m] = a2;
+        Gn[2 * m + 1] = a3;
       }
       __syncthreads();
+      const int tpi = max(1, min(8, nthr / half));
       double acc = 0.0;
-      for (int i = tid; i < nphi; i += nthr) {
-        const size_t p = (size_t)j * nphi + i;
-        const double u = row_fourier_synth_at(Gu, M, i, nphi, A.cs, A.sn);
-        const double N = row_fourier_synth_at(Gn, M, i, nphi, A.cs, A.sn);
-        double sv = N - u;
-        if (A.srot) sv = sv + A.srot[p];
-        A.Sraw[p] = sv;
-        acc += A.C[p] * sv;
+      for (int base = 0; base < half * tpi; base += nthr) {
+        const int u = base + tid, i = u / tpi, q = u % tpi;
+        const bool act = u < half * tpi;
+        double ue = 0.0, uo = 0.0, ne = 0.0, no = 0.0;
+        if (act) {
+          int t = (i * (1 + q)) % nphi;
+          const int step = (i * tpi) % nphi;
+          for (int m = 1 + q; m < M; m += tpi) {
+            const double c = __ldg(&A.cs[t]), sn = __ldg(&A.sn[t]);
+            const double vu = Gu[2 * m] * c - Gu[2 * m + 1] * sn;
+            const double vn = Gn[2 * m] * c - Gn[2 * m + 1] * sn;
+            if (m & 1) {
+              uo += vu;
+              no += vn;
+            } else {
+              ue += vu;
+              ne += vn;
+            }
+            t += step;
+            if (t >= nphi) t -= nphi;
+          }
+        }
+        part[tid] = ue;
+        part[nthr + tid] = uo;
+        part[2 * nthr + tid] = ne;
+        part[3 * nthr + tid] = no;
+        __syncthreads();
+        if (act && q == 0) {
+          double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
+          for (int c = 0; c < tpi; ++c) {
+            a0 += part[tid + c];
+            a1 += part[nthr + tid + c];
+            a2 += part[2 * nthr + tid + c];
+            a3 += part[3 * nthr + tid + c];
+          }
+          const double u1 = Gu[0] + 2.0 * (a0 + a1), u2 = Gu[0] + 2.0 * (a0 - a1);
+          const double n1 = Gn[0] + 2.0 * (a2 + a3), n2 = Gn[0] + 2.0 * (a2 - a3);
+          const size_t p1 = (size_t)j * nphi + i, p2 = p1 + half;
+          double s1 = n1 - u1, s2 = n2 - u2;
+          if (A.srot) {
+            s1 = s1 + A.srot[p1];
+            s2 = s2 + A.srot[p2];
+          }
+          A.Sraw[p1] = s1;
+          A.Sraw[p2] = s2;
+          acc += A.C[p1] * s1 + A.C[p2] * s2;
+        }
+        __syncthreads();
       }
       acc = block_sum(acc, red);
       if (tid == 0) A.rowpart[RP_CS * nlat + j] = acc;
     }
     if (!grid_barrier(A.bar, gen)) return;
-    // 5. dphi (one CTA, rows in order)
-    if (blockIdx.x == 0) {
+    // U. dphi in every CTA (rows in order by thread 0: the same value everywhere)
+    {
       const double Cs = integrate_rows(A.rowpart + RP_CS * nlat, A.wts, nlat, A.dlon);
       if (tid == 0) {
-        A.sc->Cs_int = Cs;
-        A.sc->dphi = (A.sc->ice_int - Cs + A.sc->zeta_int) / A.sc->C_int;
+        const double dphi = (A.sc->ice_int - Cs + A.sc->zeta_int) / A.sc->C_int;
+        s_val = dphi;
+        if (blockIdx.x == 0) {
+          A.sc->Cs_int = Cs;
+          A.sc->dphi = dphi;
+        }
       }
+      __syncthreads();
     }
-    if (!grid_barrier(A.bar, gen)) return;
-    // 6. rsl update and the row maxima of the change
-    const double dphi = *(volatile double*)&A.sc->dphi;
+    const double dphi = s_val;
     for (int j = blockIdx.x; j < nlat; j += gridDim.x) {
       double dmax = 0.0, smax = 0.0;
       for (int i = tid; i < nphi; i += nthr) {
@@ -470,10 +606,11 @@ __global__ void __launch_bounds__(512) k_sle_inner(InnerArgs A) {
         A.rowpart[RP_DMAX * nlat + j] = dmax;
         A.rowpart[RP_SMAX * nlat + j] = smax;
       }
+      sle_row_load(A, j, sm, part);  // L of the next iteration (unused if this one converged)
     }
     if (!grid_barrier(A.bar, gen)) return;
-    // 7. convergence (src/vilma_sle.f90:330-338), decided by CTA 0
-    if (blockIdx.x == 0) {
+    // convergence (src/vilma_sle.f90:330-338), the same decision in every CTA
+    {
       double dmax = 0.0, smax = 0.0;
       for (int j = tid; j < nlat; j += nthr) {
         dmax = nanmax(dmax, A.rowpart[RP_DMAX * nlat + j]);
@@ -482,17 +619,26 @@ __global__ void __launch_bounds__(512) k_sle_inner(InnerArgs A) {
       dmax = block_max(dmax, red);
       smax = block_max(smax, red);
       if (tid == 0) {
-        A.sc->dmax = dmax;
-        A.sc->smax = smax;
-        A.sc->n_inner = it;
-        A.bar[3] = (dmax <= A.tol * fmax(smax, TINY)) ? 1u : 0u;
+        s_stop = (dmax <= A.tol * fmax(smax, TINY)) ? 1 : 0;
+        if (blockIdx.x == 0) {
+          A.sc->dmax = dmax;
+          A.sc->smax = smax;
+          A.sc->n_inner = it;
+        }
       }
+      __syncthreads();
+      if (s_stop) break;
     }
-    if (!grid_barrier(A.bar, gen)) return;
-    if (tid == 0) s_stop = (int)*(volatile unsigned int*)(A.bar + 3);
-    __syncthreads();
-    if (s_stop) break;
   }
+}
+
+// dynamic shared memory of the fused loop: the row (nphi) or, in R, the
+// Fourier sums (4 M) and the row's staged partial sums (4 chunks)
+static size_t sle_inner_smem(const vg_handle* h) {
+  const Grid& G = h->grid;
+  int nch = 0;
+  for (int m = 0; m < G.M; ++m) nch += (G.lmax - m + SLE_LCH) / SLE_LCH;
+  return (size_t)std::max(G.nphi, 4 * G.M + 4 * nch) * sizeof(double);
 }
 
 static void launch_inner_loop(vg_handle* h) {
@@ -502,13 +648,23 @@ static void launch_inner_loop(vg_handle* h) {
     int dev = 0, nsm = 0, per_sm = 0;
     VG_CUDA(cudaGetDevice(&dev));
     VG_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
-    const size_t shm = (size_t)std::max(G.nphi, 4 * G.M) * sizeof(double);
-    if (shm > 48 * 1024)
-      VG_CUDA(cudaFuncSetAttribute(k_sle_inner, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm));
+    const size_t shm = sle_inner_smem(h);
+    VG_CUDA(cudaFuncSetAttribute(k_sle_inner, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm));
     VG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_sle_inner, 512, shm));
     if (per_sm < 1) throw Error("sle_solve: the fused inner loop does not fit on an SM");
     h->sle_grid = nsm;
     h->d_gbar.alloc(4);
+    std::vector<int2> chunk;
+    std::vector<int> cbeg(G.M + 1);
+    for (int m = 0; m < G.M; ++m) {
+      cbeg[m] = (int)chunk.size();
+      for (int l0 = 0; l0 < G.lmax - m + 1; l0 += SLE_LCH) chunk.push_back(make_int2(m, l0));
+    }
+    cbeg[G.M] = (int)chunk.size();
+    h->sle_nchunk = (int)chunk.size();
+    h->d_sle_chunk.upload(chunk, s);
+    h->d_sle_cbeg.upload(cbeg, s);
+    h->d_sle_Gp.alloc((size_t)h->sle_nchunk * G.nlat * 4);
   }
   InnerArgs A;
   A.nphi = G.nphi;
@@ -540,13 +696,16 @@ static void launch_inner_loop(vg_handle* h) {
   A.F = h->d_F.p;
   A.sigma = h->d_sigma.p;
   A.ulm = h->d_ulm.p;
-  A.Gs = h->d_Gs.p;
+  A.chunk = h->d_sle_chunk.p;
+  A.cbeg = h->d_sle_cbeg.p;
+  A.nchunk = h->sle_nchunk;
+  A.Gp = h->d_sle_Gp.p;
   A.Sraw = h->d_Sraw.p;
   A.rowpart = h->d_rowpart.p;
   A.sc = h->d_sc_.p;
   A.bar = h->d_gbar.p;
   VG_CUDA(cudaMemsetAsync(h->d_gbar.p, 0, 4 * sizeof(unsigned int), s));
-  const size_t shm = (size_t)std::max(G.nphi, 4 * G.M) * sizeof(double);
+  const size_t shm = sle_inner_smem(h);
   void* args[] = {&A};
   VG_CUDA(cudaLaunchCooperativeKernel((const void*)k_sle_inner, dim3(h->sle_grid), dim3(512), args, shm, s));
   ++h->n_launch;
