@@ -47,8 +47,8 @@ def parse():
                     help="3-D stress products of the timed arm")
     ap.add_argument("--plain", default="on", choices=["on", "off"],
                     help="also time the plain FP64 arm beside split_tc (and report the rsl error between them)")
-    ap.add_argument("--grad-fwd", default="on", choices=["on", "off"],
-                    help="also time the adjoint gradient against its forward (grad/fwd)")
+    ap.add_argument("--grad-fwd", default="on", choices=["on", "off", "only"],
+                    help="also time the adjoint gradient against its forward (grad/fwd); 'only' prints that alone")
     return ap.parse_args()
 
 
@@ -385,6 +385,10 @@ def main():
     import torch
 
     torch.cuda.set_device(local)
+    if args.grad_fwd == "only":
+        if rank == 0:
+            print(json.dumps({"workload": w.name, "grad_fwd": measure_grad_fwd(w)}), flush=True)
+        return
     dist = None
     if world > 1:
         import datetime
