@@ -36,6 +36,10 @@ class VgParams(C.Structure):
         ("sle_fixed_ocean", C.c_int), ("sle_subgrid", C.c_int), ("sle_warm_start", C.c_int),
         ("rotation", C.c_int),
         ("visc3d_precision", C.c_int),
+        ("rtol", C.c_double), ("atol", C.c_double), ("safety", C.c_double),
+        ("grow_max", C.c_double), ("shrink_min", C.c_double),
+        ("sle_max_mem_iter", C.c_int),
+        ("couple_tol", C.c_double),
     ]
 
 

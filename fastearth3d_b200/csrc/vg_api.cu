@@ -104,6 +104,13 @@ int vg_params_default(vg_params* p) {
   p->sle_warm_start = 1;
   p->rotation = 0;
   p->visc3d_precision = VG_VISC3D_FP64;
+  p->rtol = 1e-4;
+  p->atol = 1e-3;
+  p->safety = 0.9;
+  p->grow_max = 5.0;
+  p->shrink_min = 0.2;
+  p->sle_max_mem_iter = 20;
+  p->couple_tol = 1e-6;
   return 0;
 }
 

@@ -38,7 +38,7 @@ extern "C" {
 #define VG_MAX_LAYER 16
 
 enum { VG_RHEOL_ELASTIC = 0, VG_RHEOL_MAXWELL = 1, VG_RHEOL_FLUID = 2 };
-enum { VG_SCHEME_FE = 0 };
+enum { VG_SCHEME_FE = 0, VG_SCHEME_TRAP = 2 };  /* "fe" | "trap" (SCHEME_* of src/vilma_viscoelastic.f90:60-64) */
 enum { VG_VISC3D_FP64 = 0, VG_VISC3D_SPLIT_TC = 1 };
 
 /* The &vilma namelist record restricted to what the time step reads
@@ -56,7 +56,7 @@ typedef struct vg_params {
    * (src/vilma_radial_fe.f90:43-50, 140-224). No reference counterpart. */
   int ne_layer[VG_MAX_LAYER];
   /* response (src/vilma_params.f90:65-70, 135-158) */
-  int scheme;        /* VG_SCHEME_FE ("fe") */
+  int scheme;        /* VG_SCHEME_FE ("fe") or VG_SCHEME_TRAP ("trap") */
   int deg1_cm;       /* 1: deg1_frame = "cm", 0: "cf" */
   double skip_tol;   /* drift-solve skip gate, src/vilma_response.f90:88-93 */
   double visc3d_tol; /* 1-D/3-D element split [dex] */
@@ -76,6 +76,14 @@ typedef struct vg_params {
    * contractions on the tensor cores with two-term TF32 operands and FP32
    * accumulation (rsl within ~2e-6 of the FP64 path on the lmax-128 workload) */
   int visc3d_precision;
+  /* trapezoidal scheme (scheme = VG_SCHEME_TRAP): the step-doubling controller
+   * (src/vilma_timestep.f90:40-53, 229-307; rtol, atol, safety, grow_max,
+   * shrink_min of src/vilma_params.f90:86-92), the sea-level <-> memory
+   * co-convergence cap (sle_max_mem_iter, src/vilma_params.f90:76) and its
+   * tolerance on the surface drift (couple_tol, src/vilma_response.f90:177) */
+  double rtol, atol, safety, grow_max, shrink_min;
+  int sle_max_mem_iter;
+  double couple_tol;
 } vg_params;
 
 /* Phase timers (the reference's [PROFILE] buckets: drift solve, memory

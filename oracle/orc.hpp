@@ -123,6 +123,8 @@ void sht_calibrate_n6(Sht& s);
 
 // ---------------------------------------------------------------- response
 constexpr int NLAM = 4;
+// vilma_viscoelastic.f90:60-64 memory-scheme codes (forward Euler, trapezoidal)
+enum Scheme { SCHEME_FE = 0, SCHEME_TRAP = 2 };
 
 struct Response {
   int lmax = 0, nr = 0, ne = 0, ndof = 0, nlm = 0, nk = 0;
@@ -148,6 +150,23 @@ struct Response {
   int ne3d = 0;
   std::vector<int> e3d;
   std::vector<double> Mk3, MkPerDt3;  // [e][j][i] (nphi fastest)
+  // memory scheme and the sea-level <-> memory co-convergence
+  // (vilma_response.f90:176-223, 1480-1663)
+  int scheme = SCHEME_FE;
+  double couple_tol = 1e-6;
+  int couple_pass = 0, couple_iters_last = 0;
+  bool couple_done = false;
+  std::vector<cplx> sigma_n, sigma_next;  // start-of-step load, staged endpoint load
+  bool sigma_primed = false;
+  std::vector<double> edUn_re, edUn_im, edVn_re, edVn_im;  // endpoint drift [k][node]
+  std::vector<cplx> dUa_prev;
+  std::vector<double> Are0, Aim0, Bre0, Bim0, Cre0, Cim0;  // tau_n snapshot
+  // step-doubling buffers: A = tau_n (+ time, sigma_n), B = tau_coarse
+  std::vector<double> Are_s, Aim_s, Bre_s, Bim_s, Cre_s, Cim_s;
+  std::vector<double> Are_c, Aim_c, Bre_c, Bim_c, Cre_c, Cim_c;
+  double time_s = 0;
+  std::vector<cplx> sigma_n_s;
+  bool sigma_primed_s = false;
   // profile counters
   double t_drift = 0, t_mem = 0;
   long n_drift = 0, n_mem = 0, n_solved = 0;
@@ -160,16 +179,25 @@ void response_set_dt(Response& R, double dt);
 double response_max_rate(const Response& R);
 double response_memory_norm(const Response& R);
 void response_enable_lateral_visc(Response& R, const Sht& s, const double* pert /*[e][j][i]*/);
+void response_prepare_endpoint(Response& R);
+void response_advance_endpoint(Response& R, const Sht& s, const cplx* sigma);
+bool response_endpoint_converged(const Response& R);
+void response_finalize_step(Response& R);
+void response_prime_sigma(Response& R, const cplx* sig0);
+void response_save_state(Response& R);
+void response_restore_state(Response& R);
+void response_stash_coarse(Response& R);
+void response_coarse_fine_error(const Response& R, double& err_inf, double& tau_inf);
 
 // ---------------------------------------------------------------- SLE / stepper / coupling
 struct SleSolver {
-  int n_outer = 3, n_inner = 20;
+  int n_outer = 3, n_inner = 20, max_mem_iter = 20;
   double tol = 1e-7;
   bool fixed_ocean = false, subgrid = true, warm_start = false;
   long n_solve = 0, n_outer_tot = 0, n_inner_tot = 0;
 };
 struct SleResult {
-  int n_outer_done = 0, n_inner_last = 0, n_coast_flip = 0;
+  int n_outer_done = 0, n_inner_last = 0, n_coast_flip = 0, n_couple_done = 0;
   double resid = 0, mass_resid = 0, ocean_frac = 0, esl = 0;
 };
 void ocean_function(int n, const double* topo, const double* ice, double* C);
@@ -179,7 +207,9 @@ void sle_solve(SleSolver& sle, const Sht& s, Response& R, const double* d_ice, c
 
 struct Stepper {
   double cfl = 1.0, guard_growth = 1e3, dt_min = 0, dt_max = 1e300;
-  long n_accept = 0, n_reject = 0, n_solve = 0;
+  // trapezoidal step-doubling controller (vilma_timestep.f90:40-53)
+  double rtol = 1e-4, atol = 1e-3, safety = 0.9, grow_max = 5.0, shrink_min = 0.2, dt_try = 0.0;
+  long n_accept = 0, n_reject = 0, n_solve = 0, n_floor = 0;
   int n_sub_last = 0;
   double worst_mass_resid = 0;
 };

@@ -73,6 +73,13 @@ int orc_params_default(vg_params* p) {
   p->sle_warm_start = 1;
   p->rotation = 0;
   p->visc3d_precision = VG_VISC3D_FP64;
+  p->rtol = 1e-4;
+  p->atol = 1e-3;
+  p->safety = 0.9;
+  p->grow_max = 5.0;
+  p->shrink_min = 0.2;
+  p->sle_max_mem_iter = 20;
+  p->couple_tol = 1e-6;
   return 0;
 }
 
@@ -97,7 +104,17 @@ int orc_create(const vg_params* p, OrcHandle** out) {
     h->R.deg1_cm = p->deg1_cm != 0;
     h->R.skip_tol = p->skip_tol;
     h->R.visc3d_tol = p->visc3d_tol;
+    if (p->scheme != SCHEME_FE && p->scheme != SCHEME_TRAP)
+      throw std::runtime_error("vilma_params: scheme must be \"fe\" or \"trap\"");
     response_init_ve(h->R, h->earth, h->mesh, h->sht, dt0);
+    h->R.scheme = p->scheme;
+    h->R.couple_tol = p->couple_tol;
+    h->sle.max_mem_iter = p->sle_max_mem_iter;
+    h->st.rtol = p->rtol;
+    h->st.atol = p->atol;
+    h->st.safety = p->safety;
+    h->st.grow_max = p->grow_max;
+    h->st.shrink_min = p->shrink_min;
     h->sle.n_outer = p->sle_n_outer;
     h->sle.n_inner = p->sle_n_inner;
     h->sle.tol = p->sle_tol;
@@ -177,7 +194,9 @@ int orc_update(OrcHandle* h, const double* h_ice, double dt_yr) {
                            h->h_ice_eq.data(), t0, t1, h->rsl.data(), h->C.data(),
                            h->rot.enabled ? s_rot.data() : nullptr, h->sigma_lm.data());
   if (rc) {
-    h->err = "vilma_timestep: explicit guard sub-step collapsed (viscosity too stiff for FE)";
+    h->err = rc == 1   ? "vilma_timestep: explicit guard sub-step collapsed (viscosity too stiff for FE)"
+             : rc == 2 ? "vilma_timestep: implicit local-error estimate went non-finite"
+                       : "vilma_timestep: implicit adaptive step collapsed (tolerance unreachable)";
     return rc;
   }
   if (h->rot.enabled) {

@@ -90,6 +90,27 @@ static void advance_memory_fe(int ne, const double* mu, const double* Mk, const 
   }
 }
 
+// vilma_viscoelastic.f90:482-589 advance_memory, trapezoidal branch (:556-569):
+// tau_{n+1} = [(1 - M/2) tau_n - mu M (eps_n + eps_{n+1})] / (1 + M/2) with
+// eps_{n+1} from (Un, Vn) and eps_n from (Un_prev, Vn_prev)
+static void advance_memory_trap(int ne, const double* mu, const double* Mk, const double* Un, const double* Vn,
+                                const double* Un_prev, const double* Vn_prev, double Jr, double* A, double* B,
+                                double* C, const char* active) {
+  for (int e = 0; e < ne; ++e) {
+    if (!active[e]) continue;
+    double a[4], b[4], c[4], ap[4], bp[4], cp[4];
+    strain_coeffs(Un[e], Un[e + 1], Vn[e], Vn[e + 1], Jr, a, b, c);
+    strain_coeffs(Un_prev[e], Un_prev[e + 1], Vn_prev[e], Vn_prev[e + 1], Jr, ap, bp, cp);
+    const double Me = Mk[e], denom = 1.0 + 0.5 * Me;
+    const double c_old = (1.0 - 0.5 * Me) / denom, w_eps = mu[e] * Me / denom;
+    for (int m = 0; m < 4; ++m) {
+      A[e * 4 + m] = c_old * A[e * 4 + m] - w_eps * (a[m] + ap[m]);
+      B[e * 4 + m] = c_old * B[e * 4 + m] - w_eps * (b[m] + bp[m]);
+      C[e * 4 + m] = c_old * C[e * 4 + m] - w_eps * (c[m] + cp[m]);
+    }
+  }
+}
+
 // vilma_response.f90:386-420 response_deg1_to_cm
 static void deg1_to_cm(const RadialOp& op, double* x) {
   if (op.nullmode.empty()) return;
@@ -205,9 +226,11 @@ static double absmax6(int n, const double* x1, const double* x2, const double* x
   return amax;
 }
 
-// vilma_response.f90:679-809 ve_response_begin -> solve_drift
-void response_begin_step(Response& R, const Sht& s) {
-  (void)s;
+// vilma_response.f90:679-809 solve_drift: the nodal drift into the given
+// targets (begin_step: dUn, the endpoint pass: edUn) and the surface drift
+// dUa, dFa, dVa (the report drift the sea-level iteration applies)
+static void solve_drift(Response& R, std::vector<double>& dUn_re, std::vector<double>& dUn_im,
+                        std::vector<double>& dVn_re, std::vector<double>& dVn_im) {
   const int nb = 4 * R.ne, nr = R.nr;
 #pragma omp parallel for schedule(static)
   for (int k = 0; k < R.nk; ++k) {
@@ -229,10 +252,10 @@ void response_begin_step(Response& R, const Sht& s) {
           R.dFa[k] = 0.0;
           R.dVa[k] = 0.0;
           for (int node = 0; node < nr; ++node) {
-            R.dUn_re[(size_t)k * nr + node] = 0.0;
-            R.dUn_im[(size_t)k * nr + node] = 0.0;
-            R.dVn_re[(size_t)k * nr + node] = 0.0;
-            R.dVn_im[(size_t)k * nr + node] = 0.0;
+            dUn_re[(size_t)k * nr + node] = 0.0;
+            dUn_im[(size_t)k * nr + node] = 0.0;
+            dVn_re[(size_t)k * nr + node] = 0.0;
+            dVn_im[(size_t)k * nr + node] = 0.0;
           }
           continue;
         }
@@ -255,16 +278,22 @@ void response_begin_step(Response& R, const Sht& s) {
         R.dVa[k] = cplx(xre[idx_v(nr - 1)], xim[idx_v(nr - 1)]);
         if (l == 1 && !R.deg1_cm) R.dFa[k] = 0.0;
         for (int node = 0; node < nr; ++node) {
-          R.dUn_re[(size_t)k * nr + node] = xre[idx_u(node)];
-          R.dUn_im[(size_t)k * nr + node] = xim[idx_u(node)];
-          R.dVn_re[(size_t)k * nr + node] = xre[idx_v(node)];
-          R.dVn_im[(size_t)k * nr + node] = xim[idx_v(node)];
+          dUn_re[(size_t)k * nr + node] = xre[idx_u(node)];
+          dUn_im[(size_t)k * nr + node] = xim[idx_u(node)];
+          dVn_re[(size_t)k * nr + node] = xre[idx_v(node)];
+          dVn_im[(size_t)k * nr + node] = xim[idx_v(node)];
         }
       }
     }
   }
   R.n_solved += solved;
   R.n_drift++;
+}
+
+// vilma_response.f90:679-809 ve_response_begin: the drift of the entering memory
+void response_begin_step(Response& R, const Sht& s) {
+  (void)s;
+  solve_drift(R, R.dUn_re, R.dUn_im, R.dVn_re, R.dVn_im);
 }
 
 // vilma_response.f90:842-864 ve_response_apply
@@ -391,6 +420,254 @@ void response_advance(Response& R, const Sht& s, const cplx* sigma) {
     }
   }
   R.n_mem++;
+}
+
+// ------------------------------------------------------------- trapezoidal scheme
+// vilma_response.f90:1371-1445 gather_tensor_coeffs_trap: tau_n (the *0
+// snapshot), eps_n (sigma_n x_Un + dUn) and eps_{n+1} (sigma_{n+1} x_Un + edUn)
+// of element e as (4, nlm) channel-major blocks
+static void gather_strain_block(const Response& R, const cplx* sigma, const std::vector<double>& dUr,
+                                const std::vector<double>& dUi, const std::vector<double>& dVr,
+                                const std::vector<double>& dVi, int e, cplx* ca, cplx* cb, cplx* cc, int nlm) {
+  const int nr = R.nr;
+  for (int t = 0; t < 4 * nlm; ++t) ca[t] = cb[t] = cc[t] = 0.0;
+  for (int k = 0; k < R.nk; ++k) {
+    int l = R.kdeg[k], lm = R.k2lm[k];
+    double sre = sigma[lm].real(), sim = sigma[lm].imag();
+    const double* xu = &R.xUn[(size_t)l * nr];
+    const double* xv = &R.xVn[(size_t)l * nr];
+    size_t kn = (size_t)k * nr;
+    double Ur = sre * xu[e] + dUr[kn + e], Ui = sim * xu[e] + dUi[kn + e];
+    double Ur1 = sre * xu[e + 1] + dUr[kn + e + 1], Ui1 = sim * xu[e + 1] + dUi[kn + e + 1];
+    double Vr = sre * xv[e] + dVr[kn + e], Vi = sim * xv[e] + dVi[kn + e];
+    double Vr1 = sre * xv[e + 1] + dVr[kn + e + 1], Vi1 = sim * xv[e + 1] + dVi[kn + e + 1];
+    double ar[4], br[4], cr[4], ai[4], bi[4], ci[4];
+    strain_coeffs(Ur, Ur1, Vr, Vr1, R.Jr[l], ar, br, cr);
+    strain_coeffs(Ui, Ui1, Vi, Vi1, R.Jr[l], ai, bi, ci);
+    for (int lam = 0; lam < 4; ++lam) {
+      ca[lam * nlm + lm] = cplx(ar[lam], ai[lam]);
+      cb[lam * nlm + lm] = cplx(br[lam], bi[lam]);
+      cc[lam * nlm + lm] = cplx(cr[lam], ci[lam]);
+    }
+  }
+}
+
+// vilma_response.f90:1447-1478 advance_shape_tensor_trap (increment form):
+// tau+ - tau_n = -M [tau_n + mu (eps_n + eps_{n+1})] / (1 + M/2) on the grid
+static void advance_shape_tensor_trap(const Response& R, const Sht& s, int e, cplx* c0, const cplx* eps_n,
+                                      const cplx* eps_1, double* dt0, double* den, double* de1, cplx* cdel) {
+  const size_t ng = (size_t)s.nphi * s.nlat;
+  tensor_synth(s, c0, dt0);
+  tensor_synth(s, eps_n, den);
+  tensor_synth(s, eps_1, de1);
+  const double* M = &R.Mk3[(size_t)e * ng];
+  for (size_t g = 0; g < ng; ++g) {
+    const double wtau = M[g] / (1.0 + 0.5 * M[g]), weps = R.mu[e] * M[g] / (1.0 + 0.5 * M[g]);
+    for (int p = 0; p < 6; ++p)
+      dt0[p * ng + g] = -wtau * dt0[p * ng + g] - weps * (den[p * ng + g] + de1[p * ng + g]);
+  }
+  tensor_analysis(s, dt0, cdel);
+  for (int t = 0; t < 4 * s.nlm; ++t) c0[t] = c0[t] + cdel[t];
+}
+
+// vilma_response.f90:1321-1369 advance_memory_3d_trap
+static void advance_memory_3d_trap(Response& R, const Sht& s, const cplx* sigma) {
+  if (R.ne3d == 0) return;
+  const int nlm = s.nlm;
+  const size_t ng = (size_t)s.nphi * s.nlat;
+  const cplx* sig_n = R.sigma_primed ? R.sigma_n.data() : sigma;  // first step: sigma_{n+1} (:1398-1403)
+#pragma omp parallel
+  {
+    std::vector<cplx> c0[3], cn[3], c1[3];
+    for (int q = 0; q < 3; ++q) {
+      c0[q].assign(4 * nlm, 0.0);
+      cn[q].assign(4 * nlm, 0.0);
+      c1[q].assign(4 * nlm, 0.0);
+    }
+    std::vector<cplx> cdel(4 * nlm);
+    std::vector<double> dt0(6 * ng), den(6 * ng), de1(6 * ng);
+#pragma omp for schedule(dynamic)
+    for (int ei = 0; ei < R.ne3d; ++ei) {
+      const int e = R.e3d[ei];
+      for (int q = 0; q < 3; ++q) std::fill(c0[q].begin(), c0[q].end(), cplx(0.0));
+      for (int k = 0; k < R.nk; ++k) {
+        const int lm = R.k2lm[k];
+        const size_t o = ((size_t)k * R.ne + e) * 4;
+        for (int lam = 0; lam < 4; ++lam) {
+          c0[0][lam * nlm + lm] = cplx(R.Are0[o + lam], R.Aim0[o + lam]);
+          c0[1][lam * nlm + lm] = cplx(R.Bre0[o + lam], R.Bim0[o + lam]);
+          c0[2][lam * nlm + lm] = cplx(R.Cre0[o + lam], R.Cim0[o + lam]);
+        }
+      }
+      gather_strain_block(R, sig_n, R.dUn_re, R.dUn_im, R.dVn_re, R.dVn_im, e, cn[0].data(), cn[1].data(),
+                          cn[2].data(), nlm);
+      gather_strain_block(R, sigma, R.edUn_re, R.edUn_im, R.edVn_re, R.edVn_im, e, c1[0].data(), c1[1].data(),
+                          c1[2].data(), nlm);
+      for (int q = 0; q < 3; ++q)
+        advance_shape_tensor_trap(R, s, e, c0[q].data(), cn[q].data(), c1[q].data(), dt0.data(), den.data(),
+                                  de1.data(), cdel.data());
+      for (int k = 0; k < R.nk; ++k) {
+        const int lm = R.k2lm[k];
+        const size_t o = ((size_t)k * R.ne + e) * 4;
+        for (int lam = 0; lam < 4; ++lam) {
+          R.Are[o + lam] = c0[0][lam * nlm + lm].real();
+          R.Aim[o + lam] = c0[0][lam * nlm + lm].imag();
+          R.Bre[o + lam] = c0[1][lam * nlm + lm].real();
+          R.Bim[o + lam] = c0[1][lam * nlm + lm].imag();
+          R.Cre[o + lam] = c0[2][lam * nlm + lm].real();
+          R.Cim[o + lam] = c0[2][lam * nlm + lm].imag();
+        }
+      }
+    }
+  }
+}
+
+// vilma_response.f90:1524-1596 trapezoid_advance_all: reset to tau_n, advance
+// the 1-D-effective elements with (eps_n, eps_{n+1}), then the 3-D ones
+static void trapezoid_advance_all(Response& R, const Sht& s, const cplx* sigma) {
+  const int nr = R.nr;
+#pragma omp parallel
+  {
+    std::vector<double> Ure(nr), Uim(nr), Vre(nr), Vim(nr), Urn(nr), Uin(nr), Vrn(nr), Vin(nr);
+#pragma omp for schedule(static)
+    for (int k = 0; k < R.nk; ++k) {
+      const int l = R.kdeg[k], lm = R.k2lm[k];
+      const double sre = sigma[lm].real(), sim = sigma[lm].imag();
+      const double srn = R.sigma_primed ? R.sigma_n[lm].real() : sre;
+      const double sin_ = R.sigma_primed ? R.sigma_n[lm].imag() : sim;
+      const double* xu = &R.xUn[(size_t)l * nr];
+      const double* xv = &R.xVn[(size_t)l * nr];
+      const size_t kn = (size_t)k * nr;
+      for (int node = 0; node < nr; ++node) {
+        Urn[node] = srn * xu[node] + R.dUn_re[kn + node];
+        Vrn[node] = srn * xv[node] + R.dVn_re[kn + node];
+        Uin[node] = sin_ * xu[node] + R.dUn_im[kn + node];
+        Vin[node] = sin_ * xv[node] + R.dVn_im[kn + node];
+        Ure[node] = sre * xu[node] + R.edUn_re[kn + node];
+        Vre[node] = sre * xv[node] + R.edVn_re[kn + node];
+        Uim[node] = sim * xu[node] + R.edUn_im[kn + node];
+        Vim[node] = sim * xv[node] + R.edVn_im[kn + node];
+      }
+      const size_t o = (size_t)k * R.ne * 4, n4 = (size_t)R.ne * 4;
+      std::copy(&R.Are0[o], &R.Are0[o] + n4, &R.Are[o]);
+      std::copy(&R.Bre0[o], &R.Bre0[o] + n4, &R.Bre[o]);
+      std::copy(&R.Cre0[o], &R.Cre0[o] + n4, &R.Cre[o]);
+      std::copy(&R.Aim0[o], &R.Aim0[o] + n4, &R.Aim[o]);
+      std::copy(&R.Bim0[o], &R.Bim0[o] + n4, &R.Bim[o]);
+      std::copy(&R.Cim0[o], &R.Cim0[o] + n4, &R.Cim[o]);
+      advance_memory_trap(R.ne, R.mu.data(), R.Mk.data(), Ure.data(), Vre.data(), Urn.data(), Vrn.data(), R.Jr[l],
+                          &R.Are[o], &R.Bre[o], &R.Cre[o], R.active1d.data());
+      advance_memory_trap(R.ne, R.mu.data(), R.Mk.data(), Uim.data(), Vim.data(), Uin.data(), Vin.data(), R.Jr[l],
+                          &R.Aim[o], &R.Bim[o], &R.Cim[o], R.active1d.data());
+    }
+  }
+  if (R.lat_visc) advance_memory_3d_trap(R, s, sigma);
+  R.n_mem++;
+}
+
+// vilma_response.f90:1598-1616 ve_response_prepare_endpoint
+void response_prepare_endpoint(Response& R) {
+  R.couple_pass = 0;
+  R.couple_done = false;
+  if (R.scheme != SCHEME_TRAP) return;
+  R.Are0 = R.Are;  // snapshot_taun (:1514-1522)
+  R.Aim0 = R.Aim;
+  R.Bre0 = R.Bre;
+  R.Bim0 = R.Bim;
+  R.Cre0 = R.Cre;
+  R.Cim0 = R.Cim;
+  R.edUn_re = R.dUn_re;
+  R.edUn_im = R.dUn_im;
+  R.edVn_re = R.dVn_re;
+  R.edVn_im = R.dVn_im;
+  R.dUa_prev = R.dUa;  // keep_drift (:1492-1497)
+}
+
+// vilma_response.f90:1618-1646 ve_response_advance_endpoint
+void response_advance_endpoint(Response& R, const Sht& s, const cplx* sigma) {
+  if (R.scheme != SCHEME_TRAP) {
+    response_advance(R, s, sigma);
+    R.couple_pass = 1;
+    R.couple_done = true;
+    return;
+  }
+  trapezoid_advance_all(R, s, sigma);
+  R.sigma_next.assign(sigma, sigma + R.nlm);
+  solve_drift(R, R.edUn_re, R.edUn_im, R.edVn_re, R.edVn_im);  // solve_endpoint_drift (:1480-1490)
+  R.couple_pass++;
+  double cnorm = 0.0, snorm = 0.0;  // drift_change (:1499-1512)
+  for (int k = 0; k < R.nk; ++k) {
+    cnorm = std::max(cnorm, std::abs(R.dUa[k] - R.dUa_prev[k]));
+    snorm = std::max(snorm, std::abs(R.dUa[k]));
+  }
+  R.dUa_prev = R.dUa;
+  R.couple_done = (R.couple_pass >= 2 && cnorm <= R.couple_tol * std::max(snorm, 2.2250738585072014e-308));
+}
+
+// vilma_response.f90:1648-1651
+bool response_endpoint_converged(const Response& R) { return R.couple_done; }
+
+// vilma_response.f90:1653-1663 ve_response_finalize_step
+void response_finalize_step(Response& R) {
+  R.couple_iters_last = R.couple_pass;
+  if (!R.sigma_next.empty()) {
+    R.sigma_n = R.sigma_next;
+    R.sigma_primed = true;
+  }
+  R.time += R.dt;
+}
+
+// response_prime_sigma: the start-of-step load sigma_n
+void response_prime_sigma(Response& R, const cplx* sig0) {
+  R.sigma_n.assign(sig0, sig0 + R.nlm);
+  R.sigma_primed = true;
+}
+
+// vilma_response.f90:1695-1740 response_save_state / response_restore_state
+void response_save_state(Response& R) {
+  R.Are_s = R.Are;
+  R.Aim_s = R.Aim;
+  R.Bre_s = R.Bre;
+  R.Bim_s = R.Bim;
+  R.Cre_s = R.Cre;
+  R.Cim_s = R.Cim;
+  R.time_s = R.time;
+  R.sigma_n_s = R.sigma_n;
+  R.sigma_primed_s = R.sigma_primed;
+}
+void response_restore_state(Response& R) {
+  R.Are = R.Are_s;
+  R.Aim = R.Aim_s;
+  R.Bre = R.Bre_s;
+  R.Bim = R.Bim_s;
+  R.Cre = R.Cre_s;
+  R.Cim = R.Cim_s;
+  R.time = R.time_s;
+  R.sigma_n = R.sigma_n_s;
+  R.sigma_primed = R.sigma_primed_s;
+}
+
+// vilma_response.f90:1742-1758 response_stash_coarse
+void response_stash_coarse(Response& R) {
+  R.Are_c = R.Are;
+  R.Aim_c = R.Aim;
+  R.Bre_c = R.Bre;
+  R.Bim_c = R.Bim;
+  R.Cre_c = R.Cre;
+  R.Cim_c = R.Cim;
+}
+
+// vilma_response.f90:1760-1781 response_coarse_fine_error: max |tau_fine - tau_coarse|, max |tau_fine|
+void response_coarse_fine_error(const Response& R, double& err_inf, double& tau_inf) {
+  err_inf = 0.0;
+  tau_inf = 0.0;
+  const std::vector<double>* f[6] = {&R.Are, &R.Aim, &R.Bre, &R.Bim, &R.Cre, &R.Cim};
+  const std::vector<double>* c[6] = {&R.Are_c, &R.Aim_c, &R.Bre_c, &R.Bim_c, &R.Cre_c, &R.Cim_c};
+  for (int q = 0; q < 6; ++q)
+    for (size_t i = 0; i < f[q]->size(); ++i) {
+      err_inf = std::max(err_inf, std::fabs((*f[q])[i] - (*c[q])[i]));
+      tau_inf = std::max(tau_inf, std::fabs((*f[q])[i]));
+    }
 }
 
 // vilma_response.f90:1665-1680 response_set_dt

@@ -14,7 +14,9 @@ void ocean_function(int n, const double* topo, const double* ice, double* C) {
   for (int i = 0; i < n; ++i) C[i] = (topo[i] < 0.0 && RHO_ICE * ice[i] < -RHO_WATER * topo[i]) ? 1.0 : 0.0;
 }
 
-// vilma_sle.f90:124-405 sle_solve (FE / first-order response: one memory pass)
+// vilma_sle.f90:124-405 sle_solve; the im loop is the sea-level <-> memory
+// co-convergence (:218-365): one pass for forward Euler, repeated trapezoid
+// endpoint passes until the surface drift settles for the trapezoidal scheme
 void sle_solve(SleSolver& sle, const Sht& s, Response& R, const double* d_ice, const double* ice,
                const double* topo0, double* rsl, double* C, SleResult& res, bool report_only,
                cplx* sigma_out, const double* s_rot) {
@@ -34,9 +36,13 @@ void sle_solve(SleSolver& sle, const Sht& s, Response& R, const double* d_ice, c
   for (int i = 0; i < ng; ++i) ice_ref[i] = ice[i] - d_ice[i];
   ocean_function(ng, topo0, ice_ref.data(), C0.data());
   response_begin_step(R, s);
+  if (!report_only) response_prepare_endpoint(R);
   auto assemble_load = [&]() {
     for (int i = 0; i < ng; ++i) load[i] = RHO_ICE * d_ice_g[i] + RHO_WATER * (C[i] * rsl[i]) + wcorr[i];
   };
+  const int n_mem = report_only ? 1 : sle.max_mem_iter;
+  res.n_couple_done = 0;
+  for (int im = 1; im <= n_mem; ++im) {
   for (int io = 1; io <= sle.n_outer; ++io) {
     if (sle.fixed_ocean) {
       if (io == 1)
@@ -100,10 +106,12 @@ void sle_solve(SleSolver& sle, const Sht& s, Response& R, const double* d_ice, c
   }
   assemble_load();
   sht_analysis(s, load.data(), load_lm.data());
-  if (!report_only) {
-    response_advance(R, s, load_lm.data());
-    R.time += R.dt;
+  if (report_only) break;
+  response_advance_endpoint(R, s, load_lm.data());
+  res.n_couple_done = im;
+  if (response_endpoint_converged(R)) break;
   }
+  if (!report_only) response_finalize_step(R);
   if (sigma_out)
     for (int lm = 0; lm < nlm; ++lm) sigma_out[lm] = load_lm[lm];
   for (int i = 0; i < ng; ++i) tmp[i] = C[i] * rsl[i];
@@ -134,6 +142,71 @@ int stepper_advance(Stepper& st, const Sht& s, Response& R, SleSolver& sle, cons
     }
     sle_solve(sle, s, R, dice_now.data(), ice_now.data(), topo0, rsl, C, res, true, sig_last.data(), s_rot);
     st.worst_mass_resid = res.mass_resid;
+    if (sigma_out) std::copy(sig_last.begin(), sig_last.end(), sigma_out);
+    return 0;
+  }
+  if (R.scheme == SCHEME_TRAP) {
+    // vilma_timestep.f90:229-307 implicit branch: step doubling around each
+    // trial step, accept / reject against rtol, atol; dt_try carried across calls
+    auto solve_at = [&](double t_eval) {
+      const double frac = (t_eval - t0) / span;
+      for (int i = 0; i < ng; ++i) {
+        ice_now[i] = ice0[i] + frac * (ice1[i] - ice0[i]);
+        dice_now[i] = ice_now[i] - ice_ref[i];
+      }
+      st.n_solve++;
+      sle_solve(sle, s, R, dice_now.data(), ice_now.data(), topo0, rsl, C, res, false, sig_last.data(), s_rot);
+      st.worst_mass_resid = std::max(st.worst_mass_resid, res.mass_resid);
+    };
+    if (!R.sigma_primed) {  // seed sigma_n with a report-only solve at t0 (:234-241)
+      std::vector<cplx> sig0(s.nlm);
+      for (int i = 0; i < ng; ++i) {
+        ice_now[i] = ice0[i];
+        dice_now[i] = ice0[i] - ice_ref[i];
+      }
+      sle_solve(sle, s, R, dice_now.data(), ice_now.data(), topo0, rsl, C, res, true, sig0.data(), s_rot);
+      response_prime_sigma(R, sig0.data());
+    }
+    const double ricfac = 3.0, expo = 1.0 / 3.0;  // order p = 2: 2^p - 1, 1 / (p + 1)
+    double t = t0;
+    if (st.dt_try <= 0.0) st.dt_try = span;
+    int n_acc = 0;
+    while (true) {
+      if (t >= t1 - 1.0e-9 * span) break;
+      const double dt = std::min(st.dt_try, t1 - t);
+      const bool at_floor = (st.dt_min > 0.0 && dt <= st.dt_min * (1.0 + 1.0e-9));
+      rsl_n.assign(rsl, rsl + ng);
+      response_save_state(R);
+      response_set_dt(R, dt);
+      solve_at(t + dt);  // coarse
+      response_stash_coarse(R);
+      response_restore_state(R);
+      std::copy(rsl_n.begin(), rsl_n.end(), rsl);
+      response_set_dt(R, 0.5 * dt);
+      solve_at(t + 0.5 * dt);  // fine
+      solve_at(t + dt);
+      double err_inf = 0.0, tau_inf = 0.0;
+      response_coarse_fine_error(R, err_inf, tau_inf);
+      response_set_dt(R, dt);
+      const double errsc = (err_inf / ricfac) / (st.atol + st.rtol * tau_inf);
+      if (!(errsc <= 1.7976931348623157e308)) return 2;  // non-finite estimate (:268-274)
+      const bool accept = (errsc <= 1.0) || at_floor;
+      if (accept) {
+        t = t + dt;
+        st.n_accept++;
+        ++n_acc;
+        if (at_floor && errsc > 1.0) st.n_floor++;
+      } else {
+        response_restore_state(R);
+        std::copy(rsl_n.begin(), rsl_n.end(), rsl);
+        st.n_reject++;
+      }
+      double fac = (errsc <= 0.0) ? st.grow_max : st.safety * std::pow(errsc, -expo);
+      fac = std::min(st.grow_max, std::max(st.shrink_min, fac));
+      st.dt_try = std::min(st.dt_max, std::max(st.dt_min, dt * fac));
+      if (st.dt_try <= 1.0e-12 * span) return 3;  // step collapsed (:302-303)
+    }
+    st.n_sub_last = n_acc;
     if (sigma_out) std::copy(sig_last.begin(), sig_last.end(), sigma_out);
     return 0;
   }
