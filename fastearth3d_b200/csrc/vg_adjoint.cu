@@ -612,6 +612,7 @@ struct StateGuard {
 double misfit_dev(vg_handle* h, int nsteps, double dt, const double* sigma, int nsite, const int* site,
                   const double* obs) {
   check_args(h, nsteps, dt, nsite, site);
+  if (h->p.scheme != VG_SCHEME_FE) throw Error("vg_misfit: the response-level run follows the forward-Euler scheme");
   SkipOff skip(h);
   AdjWork& W = work_of(h);
   StateGuard guard(h, W.lam_new);
@@ -630,6 +631,7 @@ double misfit_grad_dev(vg_handle* h, int nsteps, double dt, const double* sigma,
   if (v3 && h->p.visc3d_precision != VG_VISC3D_FP64)
     throw Error("vg_misfit_grad: the 3-D adjoint follows the FP64 path (visc3d_precision = FP64)");
   if (ckpt < 1) throw Error("vg_misfit_grad: ckpt_every must be >= 1");
+  if (h->p.scheme != VG_SCHEME_FE) throw Error("vg_misfit_grad: the adjoint follows the forward-Euler scheme");
   SkipOff skip(h);
   const Grid& G = h->grid;
   cudaStream_t s = h->stream;

@@ -129,6 +129,7 @@ int vg_create(const vg_params* p, vg_handle** out) {
     VG_CUDA(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
     vg::setup_handle(h);
     if (h->p.rotation) vg::rotation_setup(h);
+    if (h->p.scheme == VG_SCHEME_TRAP) vg::trap_setup(h);
     vg::compute_mem_norm(h, 0);
     h->mem_norm = vg::read_mem_norm(h, 0);
   });
@@ -392,6 +393,7 @@ int vg_set_state(vg_handle* h, const double* Are, const double* Aim, const doubl
     h->mem_norm = vg::read_mem_norm(h, h->cur);
     h->time_s = time_s;
     h->time_yr = time_s / vg::SEC_PER_YEAR;
+    h->sigma_primed = false;  // trapezoidal scheme: the next update seeds sigma_n from this state
   });
 }
 

@@ -167,6 +167,17 @@ struct vg_handle {
   vg::DArr<double> d_v3a_Yb, d_v3a_dyb, d_v3a_Rb;  // 3-D adjoint: product adjoints
   double* v3_gstore = nullptr;  // when set, the FP64 longitude pass also stores its grid there (adjoint sweeps)
   vg::DArr<double> d_lon_tw, d_lon_twt;  // FP64 longitude pass: dense twiddle tables (by order, by longitude)
+  // trapezoidal scheme (scheme = VG_SCHEME_TRAP; vg_trap.cu)
+  vg::DArr<double> d_edUn, d_edVn;      // endpoint nodal drift (2 nr nk each)
+  vg::DArr<double> d_dU_avg, d_dV_avg;  // mean of the entering and endpoint nodal drift
+  vg::DArr<double> d_sigma_n, d_sigma_next, d_sigma_avg, d_sigma_n_s;  // loads (2 nlm each)
+  vg::DArr<double> d_dUa_prev;          // surface U drift of the previous endpoint pass (2 nk)
+  vg::DArr<double> d_mem_s, d_mem_c;    // step doubling: tau_n and tau_coarse
+  vg::DArr<unsigned long long> d_trap_red;  // max reductions (err, tau, drift change, drift)
+  bool sigma_primed = false, sigma_primed_s = false;
+  double time_s_saved = 0.0, dt_try = 0.0;  // dt_try carried across intervals [s]
+  int couple_pass = 0, couple_iters_last = 0;
+  long long n_floor = 0;
   // sea-level equation fields (ng each unless stated)
   vg::DArr<double> d_z_bed_eq, d_h_ice_eq, d_h_ice, d_ice1, d_ice_now, d_dice_now, d_rsl, d_rsl_n,
       d_C, d_C0, d_C_next, d_dig, d_wcorr, d_Sraw, d_zbed, d_tmp;
@@ -218,8 +229,14 @@ namespace vg {
 void setup_handle(vg_handle* h);
 void build_grid(Grid& G, int lmax, int nlat, int nphi, cudaStream_t s);
 // response kernels (vg_radial.cu)
-void launch_drift(vg_handle* h);
-void launch_advance_1d(vg_handle* h, const double* d_sigma, double dt);
+// drift of memory buffer buf (-1: the current one) into the nodal targets
+// (nullptr: the handle's dUn, dVn) and the surface drift
+void launch_drift(vg_handle* h, int buf = -1, double* dUn = nullptr, double* dVn = nullptr);
+// 1-D memory advance, current buffer -> the other one, with the strain of
+// (sigma, dUn, dVn) (nullptr: the handle's drift); trap: the trapezoidal rule
+// with sigma, dUn, dVn the means of the step's two ends
+void launch_advance_1d(vg_handle* h, const double* d_sigma, double dt, const double* dUn = nullptr,
+                       const double* dVn = nullptr, bool trap = false);
 void launch_apply(vg_handle* h, const double* d_sigma, double* d_u, double* d_n);
 void compute_mem_norm(vg_handle* h, int buf);
 double read_mem_norm(vg_handle* h, int buf);
@@ -236,7 +253,10 @@ void update_dev(vg_handle* h, const double* d_ice1, double dt_yr);
 void update_bsl(vg_handle* h);
 // 3-D (vg_visc3d.cu)
 void visc3d_enable(vg_handle* h, const double* pert_host);
-void visc3d_advance(vg_handle* h, const double* d_sigma, double dt);
+// 3-D memory advance (current buffer -> the other one); dUn, dVn and trap as
+// for launch_advance_1d (the pointwise factor M / (1 + M/2) when trap)
+void visc3d_advance(vg_handle* h, const double* d_sigma, double dt, const double* dUn = nullptr,
+                    const double* dVn = nullptr, bool trap = false);
 // transposed 3-D advance (FP64 path) of one step whose longitude-pass grid the
 // forward stored in gstore: lam_new (3-D entries) = lam + gather^T, E (3-D
 // elements) = strain adjoints, d J / d (M dt) accumulated into gradMdt
@@ -252,7 +272,17 @@ void rotation_advance(vg_handle* h, const double* d_sigma, double dt);
 // 3-D split-precision tensor-core stages (vg_tc.cu)
 void visc3d_tc_enable(vg_handle* h);
 void visc3d_tc_buffers(vg_handle* h, float** X, float** dy);
-void visc3d_tc_run(vg_handle* h, double dt);
+void visc3d_tc_run(vg_handle* h, double dt, bool trap = false);
+// trapezoidal scheme (vg_trap.cu)
+void trap_setup(vg_handle* h);
+void trap_prepare(vg_handle* h);
+bool trap_endpoint_pass(vg_handle* h, double dt);
+void trap_finalize(vg_handle* h, double dt);
+void trap_save(vg_handle* h);
+void trap_restore(vg_handle* h);
+void trap_stash_coarse(vg_handle* h);
+void trap_coarse_fine_error(vg_handle* h, double& err_inf, double& tau_inf);
+void trap_prime(vg_handle* h);
 // misc
 void sync_scalars(vg_handle* h);
 // phase timer scope: records a start event now and a stop event at scope exit

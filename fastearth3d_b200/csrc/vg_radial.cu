@@ -432,12 +432,13 @@ __global__ void __launch_bounds__(512) k_drift_deg1(DriftArgs A) {
   }
 }
 
-void launch_drift(vg_handle* h) {
+void launch_drift(vg_handle* h, int buf, double* dUn, double* dVn) {
   PhaseScope ps(h, VG_PH_DRIFT);
+  if (buf < 0) buf = h->cur;
   DriftArgs A;
-  A.mem = h->d_mem[h->cur].p;
-  A.mnorm = h->d_mnorm.p + (size_t)h->cur * h->nk;
-  A.maxbits = h->d_maxbits.p + h->cur;
+  A.mem = h->d_mem[buf].p;
+  A.mnorm = h->d_mnorm.p + (size_t)buf * h->nk;
+  A.maxbits = h->d_maxbits.p + buf;
   A.skip_tol = h->p.skip_tol;
   A.r = h->d_r.p;
   A.sa = h->d_sa.p;
@@ -452,8 +453,8 @@ void launch_drift(vg_handle* h) {
   A.kdeg = h->d_kdeg.p;
   A.bh = h->d_bh.p;
   A.ys = h->d_xs.p;
-  A.dUn = h->d_dUn.p;
-  A.dVn = h->d_dVn.p;
+  A.dUn = dUn ? dUn : h->d_dUn.p;
+  A.dVn = dVn ? dVn : h->d_dVn.p;
   A.drift = h->d_drift.p;
   A.ne = h->ne;
   A.nr = h->nr;
@@ -528,7 +529,8 @@ __global__ void __launch_bounds__(256) k_advance_1d(const double* __restrict__ m
                                                     const double* __restrict__ xVn, const double* __restrict__ dUn,
                                                     const double* __restrict__ dVn, const double* __restrict__ mu,
                                                     const double* __restrict__ MkPerDt,
-                                                    const char* __restrict__ active, double* __restrict__ mnorm) {
+                                                    const char* __restrict__ active, double* __restrict__ mnorm,
+                                                    int trap) {
   const int k = blockIdx.x * 32 + threadIdx.x, e = blockIdx.y * 8 + threadIdx.y, ri = blockIdx.z;
   double amax = 0.0;
   if (k < nk && e < ne) {
@@ -544,7 +546,15 @@ __global__ void __launch_bounds__(256) k_advance_1d(const double* __restrict__ m
       double a[4], b[4], c[4];
       strain_coeffs(U0, U1, V0, V1, Jrv[l], a, b, c);
       const double Me = MkPerDt[e] * dt;
-      const double om = 1.0 - Me, two_muM = 2.0 * mu[e] * Me;
+      // forward Euler: (1 - M) tau - 2 mu M eps; trapezoidal with eps the mean of
+      // eps_n and eps_{n+1}: [(1 - M/2) tau_n - 2 mu M eps] / (1 + M/2)
+      // (src/vilma_viscoelastic.f90:556-569, 577-584)
+      double om = 1.0 - Me, two_muM = 2.0 * mu[e] * Me;
+      if (trap) {
+        const double denom = 1.0 + 0.5 * Me;
+        om = (1.0 - 0.5 * Me) / denom;
+        two_muM = 2.0 * (mu[e] * Me / denom);
+      }
 #pragma unroll
       for (int m = 0; m < 4; ++m) {
         size_t iA = mem_idx(0, ri, e, m, k, ne, nk), iB = mem_idx(1, ri, e, m, k, ne, nk),
@@ -584,7 +594,8 @@ __global__ void k_norm_max(const double* __restrict__ mnorm, int nk, unsigned lo
   if (threadIdx.x == 0) *maxbits = (unsigned long long)__double_as_longlong(v);
 }
 
-void launch_advance_1d(vg_handle* h, const double* d_sigma, double dt) {
+void launch_advance_1d(vg_handle* h, const double* d_sigma, double dt, const double* dUn, const double* dVn,
+                       bool trap) {
   PhaseScope ps(h, VG_PH_ADVANCE_1D);
   int nxt = 1 - h->cur;
   double* mn = h->d_mnorm.p + (size_t)nxt * h->nk;
@@ -592,8 +603,8 @@ void launch_advance_1d(vg_handle* h, const double* d_sigma, double dt) {
   dim3 grid((h->nk + 31) / 32, (h->ne + 7) / 8, 2);
   k_advance_1d<<<grid, dim3(32, 8), 0, h->stream>>>(h->d_mem[h->cur].p, h->d_mem[nxt].p, h->ne, h->nr, h->nk, dt,
                                                     d_sigma, h->d_kdeg.p, h->d_k2lm.p, h->d_Jr.p, h->d_xUn.p,
-                                                    h->d_xVn.p, h->d_dUn.p, h->d_dVn.p, h->d_mu.p, h->d_MkPerDt.p,
-                                                    h->d_active1d.p, mn);
+                                                    h->d_xVn.p, dUn ? dUn : h->d_dUn.p, dVn ? dVn : h->d_dVn.p,
+                                                    h->d_mu.p, h->d_MkPerDt.p, h->d_active1d.p, mn, trap ? 1 : 0);
   ++h->n_launch;
   VG_CUDA(cudaGetLastError());
   k_norm_max<<<1, 1024, 0, h->stream>>>(mn, h->nk, h->d_maxbits.p + nxt);

@@ -710,7 +710,8 @@ void build_fluid_deg2_band(vg_handle* h, DArr<double>& ab, DArr<double>& dr, DAr
 
 void setup_handle(vg_handle* h) {
   const vg_params& p = h->p;
-  if (p.scheme != VG_SCHEME_FE) throw Error("vg_create: only the forward-Euler memory scheme (\"fe\") is supported");
+  if (p.scheme != VG_SCHEME_FE && p.scheme != VG_SCHEME_TRAP)
+    throw Error("vg_create: the memory scheme must be \"fe\" (VG_SCHEME_FE) or \"trap\" (VG_SCHEME_TRAP)");
   if (p.lmax < 2) throw Error("vg_create: lmax must be >= 2");
   cudaStream_t s = h->stream;
   build_grid(h->grid, p.lmax, p.nlat, p.nphi, s);

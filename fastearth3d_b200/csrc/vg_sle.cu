@@ -742,8 +742,15 @@ void sle_solve_dev(vg_handle* h, double dt, bool report_only) {
   VG_CUDA(cudaMemsetAsync(sc, 0, sizeof(SleScalars), s));
   k_ocean0<<<eg, eb, 0, s>>>(ng, h->d_z_bed_eq.p, h->d_ice_now.p, h->d_dice_now.p, h->d_C0.p); ++h->n_launch;
   launch_drift(h);  // response_begin_step
+  // the sea-level <-> memory co-convergence (src/vilma_sle.f90:218-365): one
+  // pass for forward Euler; trapezoid endpoint passes until the surface drift
+  // settles for the trapezoidal scheme
+  const bool trap = p.scheme == VG_SCHEME_TRAP && !report_only;
+  if (trap) trap_prepare(h);
+  const int n_mem = trap ? std::max(1, p.sle_max_mem_iter) : 1;
   h->n_inner_last = 0;
   h->n_flip_last = 0;
+  for (int im = 1; im <= n_mem; ++im) {
   for (int io = 1; io <= p.sle_n_outer; ++io) {
     if (p.sle_fixed_ocean) {
       if (io == 1) VG_CUDA(cudaMemcpyAsync(h->d_C.p, h->d_C0.p, ng * sizeof(double), cudaMemcpyDeviceToDevice, s));
@@ -779,10 +786,15 @@ void sle_solve_dev(vg_handle* h, double dt, bool report_only) {
   k_load_fourier<<<nlat, 128, nphi * sizeof(double), s>>>(nphi, nlat, M, h->d_dig.p, h->d_C.p, h->d_rsl.p,
                                                           h->d_wcorr.p, G.d_cos.p, G.d_sin.p, h->d_F.p); ++h->n_launch;
   legendre_analysis_dev(h, h->d_F.p, 1, h->d_sigma.p);
-  if (!report_only) {
+  if (report_only) break;
+  if (!trap) {
     if (h->lat_visc) visc3d_advance(h, h->d_sigma.p, dt);
     launch_advance_1d(h, h->d_sigma.p, dt);
+    break;
   }
+  if (trap_endpoint_pass(h, dt)) break;
+  }
+  if (trap) trap_finalize(h, dt);
   k_rowsum<<<nlat, 128, 0, s>>>(nphi, h->d_C.p, h->d_rsl.p, rp + RP_MASS * nlat); ++h->n_launch;
   k_mass<<<1, FIN_THREADS, 0, s>>>(sc, rp, G.d_wts.p, nlat, dlon); ++h->n_launch;
 }
@@ -813,6 +825,65 @@ void update_dev(vg_handle* h, const double* d_ice1, double dt_yr) {
                                    h->d_dice_now.p); ++h->n_launch;
     sle_solve_dev(h, 0.0, true);
     h->worst_mass_resid = mass_resid();
+  } else if (p.scheme == VG_SCHEME_TRAP) {
+    // implicit branch (src/vilma_timestep.f90:229-307): step doubling around
+    // each trial step, accept / reject against rtol, atol; dt_try carried
+    // across intervals
+    auto solve_at = [&](double t_eval, double dts) {
+      k_ice_interp<<<eg, eb, 0, s>>>(ng, (t_eval - t0) / span, h->d_h_ice.p, d_ice1, h->d_h_ice_eq.p,
+                                     h->d_ice_now.p, h->d_dice_now.p); ++h->n_launch;
+      VG_CUDA(cudaGetLastError());
+      h->n_solve++;
+      sle_solve_dev(h, dts, false);
+      h->worst_mass_resid = std::max(h->worst_mass_resid, mass_resid());
+    };
+    if (!h->sigma_primed) {  // seed sigma_n: a report-only solve at t0 (:234-241)
+      k_ice_interp<<<eg, eb, 0, s>>>(ng, 0.0, h->d_h_ice.p, h->d_h_ice.p, h->d_h_ice_eq.p, h->d_ice_now.p,
+                                     h->d_dice_now.p); ++h->n_launch;
+      sle_solve_dev(h, 0.0, true);
+      trap_prime(h);
+    }
+    const double ricfac = 3.0, expo = 1.0 / 3.0;  // order 2: 2^p - 1, 1 / (p + 1)
+    if (h->dt_try <= 0.0) h->dt_try = span;
+    double t = t0;
+    int n_acc = 0;
+    while (true) {
+      if (t >= t1 - 1.0e-9 * span) break;
+      const double dts = std::min(h->dt_try, t1 - t);
+      const bool at_floor = p.dt_min > 0.0 && dts <= p.dt_min * (1.0 + 1.0e-9);
+      VG_CUDA(cudaMemcpyAsync(h->d_rsl_n.p, h->d_rsl.p, ng * sizeof(double), cudaMemcpyDeviceToDevice, s));
+      trap_save(h);
+      solve_at(t + dts, dts);  // coarse
+      trap_stash_coarse(h);
+      trap_restore(h);
+      VG_CUDA(cudaMemcpyAsync(h->d_rsl.p, h->d_rsl_n.p, ng * sizeof(double), cudaMemcpyDeviceToDevice, s));
+      solve_at(t + 0.5 * dts, 0.5 * dts);  // fine
+      solve_at(t + dts, 0.5 * dts);
+      double err_inf = 0.0, tau_inf = 0.0;
+      trap_coarse_fine_error(h, err_inf, tau_inf);
+      const double errsc = (err_inf / ricfac) / (p.atol + p.rtol * tau_inf);
+      if (!(errsc <= HUGE_))
+        throw Error("vilma_timestep: implicit local-error estimate went non-finite (viscosity too stiff, or the "
+                    "state has already diverged)");
+      const bool accept = errsc <= 1.0 || at_floor;
+      if (accept) {
+        t = t + dts;
+        h->n_accept++;
+        ++n_acc;
+        if (at_floor && errsc > 1.0) h->n_floor++;
+      } else {
+        trap_restore(h);
+        VG_CUDA(cudaMemcpyAsync(h->d_rsl.p, h->d_rsl_n.p, ng * sizeof(double), cudaMemcpyDeviceToDevice, s));
+        h->n_reject++;
+      }
+      double fac = errsc <= 0.0 ? p.grow_max : p.safety * std::pow(errsc, -expo);
+      fac = std::min(p.grow_max, std::max(p.shrink_min, fac));
+      h->dt_try = std::min(p.dt_max, std::max(p.dt_min, dts * fac));
+      if (h->dt_try <= 1.0e-12 * span)
+        throw Error("vilma_timestep: implicit adaptive step collapsed (tolerance unreachable)");
+    }
+    h->n_sub_last = n_acc;
+    h->mem_norm = read_mem_norm(h, h->cur);
   } else {
     double rate = h->max_rate;
     double dt_stab = rate > 0.0 ? p.cfl / rate : span;

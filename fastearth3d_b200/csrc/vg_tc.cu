@@ -70,6 +70,7 @@ struct Args {
   float* dy;          // [(nk + 1)][6][NC]
   const float* rate;  // [nlat][nphi][ne3d]  mu / eta_eff
   float dt;
+  int trap;  // trapezoidal scheme: the factor M / (1 + M/2) instead of M
   const double* invsin;
   const float* img;
   const ImgInfo* info;
@@ -539,7 +540,11 @@ __global__ void __launch_bounds__(NTHR, 1) k_tc_stage(Args A) {
       float* gs = A.Gs + (size_t)c.j * 2 * A.half * A.NCOL + row;
       float* gd = gs + (size_t)A.half * A.NCOL;
       auto emit = [&](int i, float ev, float od) {
-        const float m1 = rate_j[(size_t)i * A.ne3d] * A.dt, m2 = rate_j[(size_t)(i + A.half) * A.ne3d] * A.dt;
+        float m1 = rate_j[(size_t)i * A.ne3d] * A.dt, m2 = rate_j[(size_t)(i + A.half) * A.ne3d] * A.dt;
+        if (A.trap) {
+          m1 = m1 / (1.0f + 0.5f * m1);
+          m2 = m2 / (1.0f + 0.5f * m2);
+        }
         const float g1 = -m1 * (ev + od), g2 = -m2 * (ev - od);
         gs[(size_t)i * A.NCOL] = g1 + g2;
         gd[(size_t)i * A.NCOL] = g1 - g2;
@@ -812,12 +817,13 @@ void visc3d_tc_buffers(vg_handle* h, float** X, float** dy) {
 }
 
 // The four tensor-core stages between the FP32 gather and the scatter.
-void visc3d_tc_run(vg_handle* h, double dt) {
+void visc3d_tc_run(vg_handle* h, double dt, bool trap) {
   TcPlan* P = static_cast<TcPlan*>(h->tc_plan);
   const Grid& G = h->grid;
   cudaStream_t s = h->stream;
   tc::Args a = P->a;
   a.dt = (float)dt;
+  a.trap = trap ? 1 : 0;
   auto launch = [&](auto kernel, int phase, const tc::ImgInfo* info, dim3 grid) {
     PhaseScope ps(h, phase);
     a.info = info;

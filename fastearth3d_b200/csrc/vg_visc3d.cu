@@ -407,7 +407,7 @@ __device__ __forceinline__ void stage_out(const double* __restrict__ X, double* 
 template <int LF>
 __global__ void __launch_bounds__(LON_THREADS, 1)
     k_v3_lon(double* __restrict__ S, int nlat, int nphi, int nf, double dt, const double* __restrict__ Mk3rate,
-             LonTables T, const double* __restrict__ invsin, double* __restrict__ gstore) {
+             LonTables T, const double* __restrict__ invsin, double* __restrict__ gstore, int trap) {
   extern __shared__ double sm[];
   const int j = blockIdx.x, f0 = blockIdx.y * LF;
   const int nft = min(LF, nf - f0);
@@ -442,7 +442,11 @@ __global__ void __launch_bounds__(LON_THREADS, 1)
   lon_synth(A, nft, T, [&](int fl, int i, const double* g1, const double* g2) {
     const int f = f0 + fl;
     const double* Mr = Mk3rate + ((size_t)(f / 3) * nlat + j) * nphi;
-    const double m1 = Mr[i] * dt, m2 = Mr[i + half] * dt;
+    double m1 = Mr[i] * dt, m2 = Mr[i + half] * dt;
+    if (trap) {  // trapezoidal: M / (1 + M/2) (src/vilma_response.f90:1468-1473)
+      m1 = m1 / (1.0 + 0.5 * m1);
+      m2 = m2 / (1.0 + 0.5 * m2);
+    }
     for (int c = 0; c < 6; ++c) {
       if (gstore) {
         double* gs = gstore + (((size_t)j * nf + f) * 6 + c) * nphi;
@@ -608,7 +612,8 @@ void visc3d_enable(vg_handle* h, const double* pert) {
   VG_CUDA(cudaStreamSynchronize(s));
 }
 
-void visc3d_advance(vg_handle* h, const double* d_sigma, double dt) {
+void visc3d_advance(vg_handle* h, const double* d_sigma, double dt, const double* dUn, const double* dVn,
+                    bool trap) {
   if (h->ne3d == 0) return;
   PhaseScope ps(h, VG_PH_VISC3D);
   const Grid& G = h->grid;
@@ -624,8 +629,8 @@ void visc3d_advance(vg_handle* h, const double* d_sigma, double dt) {
   A.Jr = h->d_Jr.p;
   A.xUn = h->d_xUn.p;
   A.xVn = h->d_xVn.p;
-  A.dUn = h->d_dUn.p;
-  A.dVn = h->d_dVn.p;
+  A.dUn = dUn ? dUn : h->d_dUn.p;
+  A.dVn = dVn ? dVn : h->d_dVn.p;
   A.mu = h->d_mu.p;
   A.ne = h->ne;
   A.nr = h->nr;
@@ -643,7 +648,7 @@ void visc3d_advance(vg_handle* h, const double* d_sigma, double dt) {
       ++h->n_launch;
       VG_CUDA(cudaGetLastError());
     }
-    visc3d_tc_run(h, dt);
+    visc3d_tc_run(h, dt, trap);
     PhaseScope pc(h, VG_PH_V3_SCATTER);
     k_v3_scatter<float><<<gg, dim3(32, 8), 0, s>>>(A, dy32, h->d_n6.p);
     ++h->n_launch;
@@ -686,7 +691,7 @@ void visc3d_advance(vg_handle* h, const double* d_sigma, double dt) {
     PhaseScope pp(h, VG_PH_V3_LON_INV);
     const dim3 lg(G.nlat, (nf + LON_LF - 1) / LON_LF);
     k_v3_lon<LON_LF><<<lg, lon_threads(h, LON_LF), lon_smem(h, LON_LF, false), s>>>(
-        h->d_Y.p, G.nlat, G.nphi, nf, dt, h->d_MkPerDt3.p, lon_tables(h), G.d_invsin.p, h->v3_gstore);
+        h->d_Y.p, G.nlat, G.nphi, nf, dt, h->d_MkPerDt3.p, lon_tables(h), G.d_invsin.p, h->v3_gstore, trap ? 1 : 0);
     ++h->n_launch;
     VG_CUDA(cudaGetLastError());
   }
