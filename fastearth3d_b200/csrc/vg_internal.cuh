@@ -90,6 +90,7 @@ struct DArr {
 struct SleScalars {
   double C_int, ice_int, zeta_int, Cs_int, dphi, dmax, smax, mass_Cs;
   int flips, n_inner;  // coastline flips; inner iterations done by the fused loop
+  int bar_error;       // a grid barrier of the fused loop gave up
   unsigned long long mem_norm_bits;  // max |memory| of the state the last advance wrote
 };
 

@@ -95,6 +95,7 @@ __global__ void k_finalize_C(SleScalars* sc, const double* __restrict__ rowpart,
 }
 __global__ void k_finalize_pass(SleScalars* sc, const double* __restrict__ rowpart, const double* __restrict__ w,
                                 int nlat, double dlon, int subgrid) {
+  if (!(sc->C_int > 0.0)) return;  // no ocean: the pass ends here (src/vilma_sle.f90:273-274)
   const double d = integrate_rows(rowpart + RP_DIG * nlat, w, nlat, dlon);
   const double z = subgrid ? integrate_rows(rowpart + RP_ZETA * nlat, w, nlat, dlon) : 0.0;
   if (threadIdx.x == 0) {
@@ -102,8 +103,9 @@ __global__ void k_finalize_pass(SleScalars* sc, const double* __restrict__ rowpa
     sc->zeta_int = z;
   }
 }
-__global__ void k_wcorr(int ng, int subgrid, const double* __restrict__ topo0, const double* __restrict__ C,
-                        const double* __restrict__ C0, double* __restrict__ wcorr) {
+__global__ void k_wcorr(const SleScalars* sc, int ng, int subgrid, const double* __restrict__ topo0,
+                        const double* __restrict__ C, const double* __restrict__ C0, double* __restrict__ wcorr) {
+  if (!(sc->C_int > 0.0)) return;  // no ocean
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i < ng) wcorr[i] = subgrid ? -RHO_WATER * topo0[i] * (C[i] - C0[i]) : 0.0;
 }
@@ -387,6 +389,11 @@ __device__ __forceinline__ void sle_row_load(const InnerArgs& A, int j, double* 
   }
 }
 
+// a grid barrier gave up: record it where the host reads the loop's scalars
+__device__ __forceinline__ void bar_fail(const InnerArgs& A) {
+  if (threadIdx.x == 0) A.sc->bar_error = 1;
+}
+
 __global__ void __launch_bounds__(512) k_sle_inner(InnerArgs A) {
   extern __shared__ double sm[];  // max(nphi, 4 M + 4 nchunk) doubles
   __shared__ double red[512];
@@ -397,9 +404,10 @@ __global__ void __launch_bounds__(512) k_sle_inner(InnerArgs A) {
   const int lane = tid & 31, wid = tid >> 5, nw = nthr >> 5;
   const int nphi = A.nphi, nlat = A.nlat, M = A.M, nlm = A.nlm, half = nphi / 2;
   unsigned int gen = 0;
+  if (!(A.sc->C_int > 0.0)) return;  // no ocean: nothing to redistribute (every CTA reads the same value)
   // L of the first iteration
   for (int j = blockIdx.x; j < nlat; j += gridDim.x) sle_row_load(A, j, sm, part);
-  if (!grid_barrier(A.bar, gen)) return;
+  if (!grid_barrier(A.bar, gen)) return bar_fail(A);
   for (int it = 1; it <= A.n_inner; ++it) {
     // A. Legendre analysis (warp per lm, four lm of a warp at once) and the
     //    affine response u, N
@@ -469,7 +477,7 @@ __global__ void __launch_bounds__(512) k_sle_inner(InnerArgs A) {
         }
       }
     }
-    if (!grid_barrier(A.bar, gen)) return;
+    if (!grid_barrier(A.bar, gen)) return bar_fail(A);
     // S. Legendre synthesis of u and N in chunks of at most SLE_LCH degrees: a
     //    thread per (chunk, j), partial sums Gp[j][chunk][u re, u im, N re, N im]
     //    (one 32-byte sector per thread; a row's partials contiguous)
@@ -496,7 +504,7 @@ __global__ void __launch_bounds__(512) k_sle_inner(InnerArgs A) {
       o[2] = a2;
       o[3] = a3;
     }
-    if (!grid_barrier(A.bar, gen)) return;
+    if (!grid_barrier(A.bar, gen)) return bar_fail(A);
     // R. longitude synthesis (g(i) = G_0 + 2 sum_m Re G_m e^{i m phi_i}, even and
     //    odd m apart, tpi threads per longitude pair (i, i + half)),
     //    Sraw = N - u (+ s_rot), row sums of C Sraw
@@ -576,7 +584,7 @@ __global__ void __launch_bounds__(512) k_sle_inner(InnerArgs A) {
       acc = block_sum(acc, red);
       if (tid == 0) A.rowpart[RP_CS * nlat + j] = acc;
     }
-    if (!grid_barrier(A.bar, gen)) return;
+    if (!grid_barrier(A.bar, gen)) return bar_fail(A);
     // U. dphi in every CTA (rows in order by thread 0: the same value everywhere)
     {
       const double Cs = integrate_rows(A.rowpart + RP_CS * nlat, A.wts, nlat, A.dlon);
@@ -608,7 +616,7 @@ __global__ void __launch_bounds__(512) k_sle_inner(InnerArgs A) {
       }
       sle_row_load(A, j, sm, part);  // L of the next iteration (unused if this one converged)
     }
-    if (!grid_barrier(A.bar, gen)) return;
+    if (!grid_barrier(A.bar, gen)) return bar_fail(A);
     // convergence (src/vilma_sle.f90:330-338), the same decision in every CTA
     {
       double dmax = 0.0, smax = 0.0;
@@ -718,12 +726,6 @@ static void read_scalars(vg_handle* h) {
 
 void sync_scalars(vg_handle* h) { read_scalars(h); }
 
-// error word of the fused loop's grid barrier (read after read_scalars synchronised)
-static bool h_bar_error(vg_handle* h) {
-  unsigned int e = 0;
-  VG_CUDA(cudaMemcpy(&e, h->d_gbar.p + 2, sizeof(e), cudaMemcpyDeviceToHost));
-  return e != 0;
-}
 
 // One sea-level solve with the memory advance at its end (FE: a single
 // co-convergence pass), src/vilma_sle.f90:124-405. Writes the advanced memory
@@ -762,23 +764,26 @@ void sle_solve_dev(vg_handle* h, double dt, bool report_only) {
     k_pass_setup<<<nlat, 128, 0, s>>>(nphi, h->d_ice_now.p, h->d_dice_now.p, h->d_C.p, h->d_C0.p, h->d_z_bed_eq.p,
                                       h->d_dig.p, rp, nlat); ++h->n_launch;
     k_finalize_C<<<1, FIN_THREADS, 0, s>>>(sc, rp, G.d_wts.p, nlat, dlon); ++h->n_launch;
-    read_scalars(h);
-    if (h->h_sc->C_int <= 0.0) break;  // no ocean: nothing to redistribute
+    // no host round trip before the inner loop: with no ocean (C_int <= 0) the
+    // kernels below return at once and the pass ends after the one read
     k_finalize_pass<<<1, FIN_THREADS, 0, s>>>(sc, rp, G.d_wts.p, nlat, dlon, p.sle_subgrid); ++h->n_launch;
-    k_wcorr<<<eg, eb, 0, s>>>(ng, p.sle_subgrid, h->d_z_bed_eq.p, h->d_C.p, h->d_C0.p, h->d_wcorr.p); ++h->n_launch;
+    k_wcorr<<<eg, eb, 0, s>>>(sc, ng, p.sle_subgrid, h->d_z_bed_eq.p, h->d_C.p, h->d_C0.p, h->d_wcorr.p);
+    ++h->n_launch;
     {
       PhaseScope ps(h, VG_PH_SLE);
       launch_inner_loop(h);
     }
+    if (!p.sle_fixed_ocean) {  // the coastline test of this pass, read with the loop's scalars
+      k_coast<<<nlat, 128, 0, s>>>(nphi, h->d_z_bed_eq.p, h->d_rsl.p, h->d_ice_now.p, h->d_C.p, h->d_C_next.p,
+                                   rp, nlat); ++h->n_launch;
+      k_flips<<<1, FIN_THREADS, 0, s>>>(sc, rp, nlat); ++h->n_launch;
+    }
     read_scalars(h);
-    if (h_bar_error(h)) throw Error("sle_solve: grid barrier of the fused inner loop timed out");
+    if (h->h_sc->C_int <= 0.0) break;  // no ocean: nothing to redistribute
+    if (h->h_sc->bar_error) throw Error("sle_solve: grid barrier of the fused inner loop timed out");
     h->n_inner_last = h->h_sc->n_inner;
     h->n_outer_last = io;
     if (p.sle_fixed_ocean) break;
-    k_coast<<<nlat, 128, 0, s>>>(nphi, h->d_z_bed_eq.p, h->d_rsl.p, h->d_ice_now.p, h->d_C.p, h->d_C_next.p, rp,
-                                 nlat); ++h->n_launch;
-    k_flips<<<1, FIN_THREADS, 0, s>>>(sc, rp, nlat); ++h->n_launch;
-    read_scalars(h);
     h->n_flip_last = h->h_sc->flips;
     if (h->h_sc->flips == 0) break;
   }
@@ -815,10 +820,13 @@ void update_dev(vg_handle* h, const double* d_ice1, double dt_yr) {
     rotation_begin(h);
     rotation_s_rot(h);
   }
-  auto mass_resid = [&]() {
-    read_scalars(h);
+  auto mass_resid_read = [&]() {  // from scalars already read
     double ice_int = h->h_sc->ice_int, Cs = h->h_sc->mass_Cs;
     return std::fabs(ice_int) > 0.0 ? std::fabs(Cs - ice_int) / std::fabs(ice_int) : std::fabs(Cs);
+  };
+  auto mass_resid = [&]() {
+    read_scalars(h);
+    return mass_resid_read();
   };
   if (span <= 0.0) {
     k_ice_interp<<<eg, eb, 0, s>>>(ng, 0.0, h->d_h_ice.p, h->d_h_ice.p, h->d_h_ice_eq.p, h->d_ice_now.p,
@@ -904,9 +912,10 @@ void update_dev(vg_handle* h, const double* d_ice1, double dt_yr) {
       VG_CUDA(cudaGetLastError());
       h->n_solve++;
       sle_solve_dev(h, dtc, false);
-      h->worst_mass_resid = std::max(h->worst_mass_resid, mass_resid());
       int nxt = 1 - h->cur;
-      double err_inf = read_mem_norm(h, nxt);
+      VG_CUDA(cudaMemcpyAsync(h->h_sc, h->d_sc_.p, sizeof(SleScalars), cudaMemcpyDeviceToHost, s));
+      double err_inf = read_mem_norm(h, nxt);  // synchronises: the scalars are in as well
+      h->worst_mass_resid = std::max(h->worst_mass_resid, mass_resid_read());
       bool finite = err_inf <= HUGE_;
       double scale = std::max(tau0, tau_run);
       bool accept = scale <= 0.0 ? finite : (finite && err_inf <= p.guard_growth * scale);

@@ -23,12 +23,15 @@
 // Every CTA computes one 128-row tile against two sub-GEMMs (E/O or even/odd),
 // each N <= 128 wide, accumulating into 2 x 128 TMEM columns. Operands are
 // staged through shared memory in the canonical no-swizzle K-major layout
-// (16-byte core-matrix rows): A (the data) is loaded from HBM, split into
-// hi/lo on the fly; B (Legendre tables and DFT twiddles) is constant and kept
-// pre-split in HBM in exactly the shared-memory image, copied with 16-byte
-// vector loads. One elected thread issues the MMAs; tcgen05.commit arrives on
-// a per-stage mbarrier that releases the stage buffer. All waits are bounded
-// by the global timer and raise a status bit instead of hanging.
+// (16-byte core-matrix rows): A (the data) is loaded from HBM two chunks
+// ahead into registers and split into hi/lo on the fly; B (Legendre tables
+// and DFT twiddles) is constant and kept pre-split in HBM in exactly the
+// shared-memory image, copied per chunk by two TMA bulk copies (cp.async.bulk
+// completing on an mbarrier). One elected thread issues the MMAs;
+// tcgen05.commit arrives on a per-stage mbarrier that releases the stage
+// buffer. The inverse stage's epilogue stages its latitude's viscosity rates
+// in the (then idle) stage ring. All waits are bounded by the global timer and
+// raise a status bit instead of hanging.
 #include <algorithm>
 #include <cmath>
 #include <cstdint>
@@ -159,6 +162,18 @@ __device__ __forceinline__ void mma_tf32(uint32_t tmem_d, uint64_t da, uint64_t 
       : "memory");
 }
 
+// TMA bulk copy (no tensor map, no multicast): global -> this CTA's shared
+// memory, completing `bytes` on the mbarrier's transaction count
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(saddr(bar)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                   saddr(dst)),
+               "l"(src), "r"(bytes), "r"(saddr(bar))
+               : "memory");
+}
+
 __device__ __forceinline__ void mma_commit(uint64_t* bar) {
   asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(saddr(bar))
                : "memory");
@@ -179,7 +194,9 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float* v) {
 
 // ------------------------------------------------------------------ per-stage geometry
 
-__device__ __forceinline__ int slot_row(const int* kbeg, int l, int m, int nk) { return l >= 1 ? kbeg[l] + m : nk; }
+__device__ __forceinline__ int slot_row(const int* kbeg, int l, int m, int nk) {
+  return l >= 1 ? __ldg(&kbeg[l]) + m : nk;  // read-only: not ordered behind the epilogue's stores
+}
 
 // table sign under theta -> pi - theta (times (-1)^(l+m)): P, G even; dP, H odd
 __device__ __forceinline__ float table_sigma(int p) { return (p == 1 || p == 5) ? -1.0f : 1.0f; }
@@ -344,15 +361,6 @@ __device__ __forceinline__ float4 finish(const Cta& c, const RowCtx& rc, int sub
   return make_float4(Q.v[0], Q.v[1], Q.v[2], Q.v[3]);
 }
 
-__device__ __forceinline__ void cp16(void* dst, const void* src) {
-  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(saddr(dst)), "l"(src) : "memory");
-}
-__device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
-template <int N>
-__device__ __forceinline__ void cp_wait() {
-  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
-}
-
 __device__ __forceinline__ void store_split(uint32_t* hi_plane, uint32_t* lo_plane, size_t at, float4 v) {
   uint4 hi, lo;
   hi.x = to_tf32(v.x);
@@ -374,8 +382,9 @@ __global__ void __launch_bounds__(NTHR, 1) k_tc_stage(Args A) {
   extern __shared__ unsigned char smraw[];
   unsigned char* sm = (unsigned char*)(((uintptr_t)smraw + 1023) & ~(uintptr_t)1023);
   uint32_t* stage_base = (uint32_t*)sm;
-  uint64_t* bars = (uint64_t*)(sm + (size_t)NSTAGE * STAGE_WORDS * 4);  // NSTAGE + 1
-  uint32_t* tslot = (uint32_t*)(bars + NSTAGE + 1);
+  uint64_t* bars = (uint64_t*)(sm + (size_t)NSTAGE * STAGE_WORDS * 4);  // NSTAGE + 1: MMA done per stage, drain
+  uint64_t* bfull = bars + NSTAGE + 1;                                      // NSTAGE: B bulk copy landed
+  uint32_t* tslot = (uint32_t*)(bfull + NSTAGE);
   volatile int* abort_flag = (volatile int*)(tslot + 1);
   double* rsum = (double*)(sm + (size_t)NSTAGE * STAGE_WORDS * 4 + 256);  // [2 subs][2 halves][TM]
   int* slot_sm = (int*)(rsum + 4 * TM);                                     // synthesis: slot(m + dl, m)
@@ -386,6 +395,7 @@ __global__ void __launch_bounds__(NTHR, 1) k_tc_stage(Args A) {
 
   if (tid == 0) {
     for (int i = 0; i <= NSTAGE; ++i) mbar_init(&bars[i], 1);
+    for (int i = 0; i < NSTAGE; ++i) mbar_init(&bfull[i], 1);
     fence_mbar_init();
     *abort_flag = 0;
   }
@@ -404,19 +414,23 @@ __global__ void __launch_bounds__(NTHR, 1) k_tc_stage(Args A) {
   const RowCtx rc = row_ctx<STAGE>(A, c, lr);
   double sum0 = 0.0, sum1 = 0.0;  // loader side sums of the two sub-GEMMs
   constexpr int QPT = (TM * KC / 4) / NTHR;  // quads per thread per chunk
-  Quad cur[QPT], nxt[QPT];
-  // B chunk of image `I` (chunk kc) into stage buffer `b`, 16-byte cp.async
+  Quad cur[QPT], nxt[QPT], nx2[QPT];  // A raw loads of chunks ch, ch + 1, ch + 2 (two chunks in flight)
+  // B chunk of image `I` (chunk kc) into stage buffer `b`: its hi and lo planes
+  // are contiguous runs of npad * KC words in the image (offsets multiples of
+  // 64 words), two TMA bulk copies issued by one thread onto bfull[b]
+  int b_issued = 0, b_done = 0;  // B copies issued; waited for with success (thread 0)
   auto copy_b = [&](int b, const ImgInfo& I, int kc) {
-    uint32_t* Bhi = stage_base + (size_t)b * STAGE_WORDS + 2 * A_WORDS;
-    uint32_t* Blo = Bhi + B_WORDS;
-    const int nvec = I.npad * (KC / 4);
-    const float* src_hi = A.img + I.off + (size_t)kc * KC * I.npad;
-    const float* src_lo = src_hi + (size_t)I.kpad * I.npad;
-    for (int t = tid; t < nvec; t += NTHR) {
-      cp16(Bhi + 4 * t, src_hi + 4 * t);
-      cp16(Blo + 4 * t, src_lo + 4 * t);
+    if (tid == 0) {
+      uint32_t* Bhi = stage_base + (size_t)b * STAGE_WORDS + 2 * A_WORDS;
+      uint32_t* Blo = Bhi + B_WORDS;
+      const uint32_t bytes = (uint32_t)(I.npad * KC * 4);
+      const float* src_hi = A.img + I.off + (size_t)kc * KC * I.npad;
+      const float* src_lo = src_hi + (size_t)I.kpad * I.npad;
+      mbar_expect_tx(&bfull[b], 2 * bytes);
+      bulk_g2s(Bhi, src_hi, bytes, &bfull[b]);
+      bulk_g2s(Blo, src_lo, bytes, &bfull[b]);
     }
-    cp_commit();
+    ++b_issued;
   };
   auto fetch_chunk = [&](int ch, Quad* Q) {
     const int sub = ch < nch0 ? 0 : 1, kc = sub ? ch - nch0 : ch;
@@ -427,6 +441,7 @@ __global__ void __launch_bounds__(NTHR, 1) k_tc_stage(Args A) {
     copy_b(0, c.sub[0].kpad > 0 ? c.sub[0] : c.sub[1], 0);
     fetch_chunk(0, cur);
   }
+  if (nch > 1) fetch_chunk(1, nxt);
   int issued = 0;
   for (int ch = 0; ch < nch; ++ch) {
     const int buf = ch % NSTAGE;
@@ -442,9 +457,9 @@ __global__ void __launch_bounds__(NTHR, 1) k_tc_stage(Args A) {
       }
       const int sub1 = (ch + 1) < nch0 ? 0 : 1, kc1 = sub1 ? ch + 1 - nch0 : ch + 1;
       copy_b(nb, c.sub[sub1], kc1);
-      fetch_chunk(ch + 1, nxt);
     }
-    // A of chunk ch: finish the loads issued one chunk earlier, split, store
+    if (ch + 2 < nch) fetch_chunk(ch + 2, nx2);
+    // A of chunk ch: finish the loads issued two chunks earlier, split, store
     uint32_t* Ahi = stage_base + (size_t)buf * STAGE_WORDS;
     uint32_t* Alo = Ahi + A_WORDS;
 #pragma unroll
@@ -458,14 +473,18 @@ __global__ void __launch_bounds__(NTHR, 1) k_tc_stage(Args A) {
         sum0 += part;
       store_split(Ahi, Alo, ((size_t)q * TM + lr) * 4, v);
     }
-    if (more)
-      cp_wait<1>();
-    else
-      cp_wait<0>();
     fence_async_smem();
     __syncthreads();
     if (*abort_flag) break;
     if (tid == 0) {
+      if (mbar_wait(&bfull[buf], (uint32_t)((ch / NSTAGE) & 1))) {
+        ++b_done;
+      } else {
+        *abort_flag = 1;
+        atomicOr(A.status, 1ull << (4 + STAGE));
+      }
+    }
+    if (tid == 0 && !*abort_flag) {
       tc_fence_after();
       uint32_t* Bhi = Alo + A_WORDS;
       uint32_t* Blo = Bhi + B_WORDS;
@@ -487,10 +506,17 @@ __global__ void __launch_bounds__(NTHR, 1) k_tc_stage(Args A) {
     ++issued;
     if (more) {
 #pragma unroll
-      for (int qq = 0; qq < QPT; ++qq) cur[qq] = nxt[qq];
+      for (int qq = 0; qq < QPT; ++qq) {
+        cur[qq] = nxt[qq];
+        nxt[qq] = nx2[qq];
+      }
     }
   }
-  cp_wait<0>();
+  // B copies still in flight after an abort: wait for them (bounded) before
+  // the stage ring is reused or the CTA exits
+  if (tid == 0)
+    for (int q = b_done; q < b_issued; ++q)
+      if (!mbar_wait(&bfull[q % NSTAGE], (uint32_t)((q / NSTAGE) & 1))) atomicOr(A.status, 1ull << (4 + STAGE));
   // drain: one more commit tracks every MMA this thread issued
   bool ok = (*abort_flag == 0);
   if (tid == 0 && issued > 0) mma_commit(&bars[NSTAGE]);
@@ -501,7 +527,7 @@ __global__ void __launch_bounds__(NTHR, 1) k_tc_stage(Args A) {
   // per-row side sums of the two loader threads
   rsum[(0 * 2 + lh) * TM + lr] = sum0;
   rsum[(1 * 2 + lh) * TM + lr] = sum1;
-  __syncthreads();
+  ok = __syncthreads_and(ok) != 0;  // the same epilogue decision in every thread
   tc_fence_after();
 
   if (ok && !*abort_flag) {
@@ -536,7 +562,16 @@ __global__ void __launch_bounds__(NTHR, 1) k_tc_stage(Args A) {
         const float2 z = *reinterpret_cast<const float2*>(A.S + (((size_t)0 * A.nlat + c.j) * 6 + p) * A.NC + 2 * f);
         c0 = (p == 5) ? -z.y : z.x;
       }
-      const float* rate_j = A.rate + (size_t)c.j * A.nphi * A.ne3d + e3;
+      // the latitude's rates mu / eta (nphi x ne3d floats) staged once in the
+      // stage ring, free after the main loop (all MMAs have completed)
+      const float* rate_g = A.rate + (size_t)c.j * A.nphi * A.ne3d;
+      const float* rate_j = rate_g + e3;
+      if (A.nphi * A.ne3d <= NSTAGE * STAGE_WORDS) {  // uniform: fits the ring (always at lmax 128)
+        float* rate_s = reinterpret_cast<float*>(stage_base);
+        for (int t = tid; t < A.nphi * A.ne3d; t += NTHR) rate_s[t] = __ldg(&rate_g[t]);
+        __syncthreads();
+        rate_j = rate_s + e3;
+      }
       float* gs = A.Gs + (size_t)c.j * 2 * A.half * A.NCOL + row;
       float* gd = gs + (size_t)A.half * A.NCOL;
       auto emit = [&](int i, float ev, float od) {
