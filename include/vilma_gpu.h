@@ -191,6 +191,18 @@ int vg_set_fields(vg_handle* h, const double* h_ice, const double* rsl, const do
 int vg_get_rotation_state(vg_handle* h, double* m, double* load_mem, double* tidal_mem);
 int vg_set_rotation_state(vg_handle* h, const double* m, const double* load_mem, const double* tidal_mem);
 
+/* LGM-memory spin-up, the relaxation of solid_earth_spinup (relax_hold,
+ * src/vilma_coupling.f90:453-570): a zero-length update seeds the entering ice
+ * with h_ice_lgm (nphi, nlat), then h_ice_lgm is held over passes of 200 yr
+ * growing by 1.6 per pass (at most 60, at most t_max_yr in total) until the
+ * mean bed velocity int |z_bed - z_prev| dOmega / (4 pi) / pass falls below
+ * rate_tol [m/yr] (equil_rate_tol). t_max_yr <= 0 does nothing
+ * (equil_time_max = 0). The 1-D pre-equilibration (pre_spinup_1d) is not
+ * provided. Outputs (any may be NULL): the model time spent [yr], the passes,
+ * 1 if the bed came to rest before the cap. */
+int vg_spinup(vg_handle* h, const double* h_ice_lgm, double t_max_yr, double rate_tol, double* t_done_yr,
+              int* passes, int* converged);
+
 /* Relative-sea-level misfit of a response-level run and its gradient
  * (hand-written discrete adjoint; the reference has no counterpart). From the
  * handle's current memory, nsteps steps of length dt_s: begin_step, apply and

@@ -213,6 +213,40 @@ int orc_update(OrcHandle* h, const double* h_ice, double dt_yr) {
   return 0;
 }
 
+// vilma_coupling.f90:453-570 solid_earth_spinup's relaxation (relax_hold):
+// seed the entering ice with a zero-length update, then hold h_ice_lgm over
+// passes of 200 yr growing by 1.6 (at most 60, capped at t_cap) until the mean
+// bed velocity int |dz_bed| dOmega / (4 pi) / pass falls below tol [m/yr]
+int orc_spinup(OrcHandle* h, const double* h_ice_lgm, double t_cap, double tol, double* t_done, int* passes,
+               int* converged) {
+  const int ng = h->sht.nphi * h->sht.nlat;
+  *t_done = 0.0;
+  *passes = 0;
+  *converged = 0;
+  if (!(t_cap > 0.0)) return 0;
+  int rc = orc_update(h, h_ice_lgm, 0.0);
+  if (rc) return rc;
+  std::vector<double> prev = h->z_bed, d(ng);
+  double pass_dt = 200.0;
+  for (int it = 1; it <= 60; ++it) {
+    pass_dt = std::min(pass_dt, t_cap - *t_done);
+    if (pass_dt <= 0.0) break;
+    rc = orc_update(h, h_ice_lgm, pass_dt);
+    if (rc) return rc;
+    *t_done += pass_dt;
+    *passes = it;
+    for (int i = 0; i < ng; ++i) d[i] = std::fabs(h->z_bed[i] - prev[i]);
+    const double rate = sht_surface_integral(h->sht, d.data()) / (4.0 * PI) / pass_dt;
+    if (rate < tol) {
+      *converged = 1;
+      break;
+    }
+    prev = h->z_bed;
+    pass_dt = pass_dt * 1.6;
+  }
+  return 0;
+}
+
 // polar motion m (re, im) and the degree-2 constants kTe, hTe, k_s (fluid), k_s (flattening)
 int orc_get_rotation(OrcHandle* h, double* m, double* love) {
   if (m) {
