@@ -84,32 +84,53 @@ struct V3Args {
 
 // one thread per (slot k, 3-D element): strain of both histories, 24 values,
 // written as X[k][ch][f][ri] (FP64, or FP32 for the tensor-core stages)
+// Blocks of 32 slots x 8 3-D elements. The memory and drift are read along
+// the slot index (coalesced); the operand rows X[k][ch][f][ri] are written
+// through a shared tile [ch][f in block][slot] so that each (slot, channel)
+// row's 6 x 8 entries go out as one contiguous run.
+constexpr int V3_TK = 32, V3_TE = 8, V3_TC = 6 * V3_TE, V3_TP = V3_TK + 1;  // tile: columns per row, padded slots
+
 template <class T>
 __global__ void __launch_bounds__(256) k_v3_gather(V3Args A, T* __restrict__ X) {
-  const int k = blockIdx.x * 32 + threadIdx.x, ei = blockIdx.y * 8 + threadIdx.y;
-  if (k >= A.nk || ei >= A.ne3d) return;
-  const int e = A.e3d[ei], l = A.kdeg[k], lm = A.k2lm[k];
-  const double Jr = A.Jr[l], twoMu = 2.0 * A.mu[e];
-  const double* xu = A.xUn + (size_t)l * A.nr;
-  const double* xv = A.xVn + (size_t)l * A.nr;
-  T* row = X + (size_t)k * 4 * A.ncf;
-  for (int ri = 0; ri < 2; ++ri) {
-    const double s = A.sigma[2 * lm + ri];
-    const double U0 = s * xu[e] + A.dUn[((size_t)ri * A.nr + e) * A.nk + k];
-    const double U1 = s * xu[e + 1] + A.dUn[((size_t)ri * A.nr + e + 1) * A.nk + k];
-    const double V0 = s * xv[e] + A.dVn[((size_t)ri * A.nr + e) * A.nk + k];
-    const double V1 = s * xv[e + 1] + A.dVn[((size_t)ri * A.nr + e + 1) * A.nk + k];
-    double eps[3][4];
-    strain_coeffs(U0, U1, V0, V1, Jr, eps[0], eps[1], eps[2]);
+  extern __shared__ unsigned char v3_sm[];
+  T* tile = reinterpret_cast<T*>(v3_sm);  // [4 ch][V3_TC][V3_TP]
+  const int kx = threadIdx.x, ey = threadIdx.y;
+  const int k0 = blockIdx.x * V3_TK, e0 = blockIdx.y * V3_TE;
+  const int k = k0 + kx, ei = e0 + ey;
+  if (k < A.nk && ei < A.ne3d) {
+    const int e = A.e3d[ei], l = A.kdeg[k], lm = A.k2lm[k];
+    const double Jr = A.Jr[l], twoMu = 2.0 * A.mu[e];
+    const double* xu = A.xUn + (size_t)l * A.nr;
+    const double* xv = A.xVn + (size_t)l * A.nr;
+    for (int ri = 0; ri < 2; ++ri) {
+      const double s = A.sigma[2 * lm + ri];
+      const double U0 = s * xu[e] + A.dUn[((size_t)ri * A.nr + e) * A.nk + k];
+      const double U1 = s * xu[e + 1] + A.dUn[((size_t)ri * A.nr + e + 1) * A.nk + k];
+      const double V0 = s * xv[e] + A.dVn[((size_t)ri * A.nr + e) * A.nk + k];
+      const double V1 = s * xv[e + 1] + A.dVn[((size_t)ri * A.nr + e + 1) * A.nk + k];
+      double eps[3][4];
+      strain_coeffs(U0, U1, V0, V1, Jr, eps[0], eps[1], eps[2]);
 #pragma unroll
-    for (int s3 = 0; s3 < 3; ++s3)
+      for (int s3 = 0; s3 < 3; ++s3)
 #pragma unroll
-      for (int lam = 0; lam < 4; ++lam) {
-        double v = A.mem[mem_idx(s3, ri, e, lam, k, A.ne, A.nk)] + twoMu * eps[s3][lam];
-        if (lam == 2) v = -Jr * v;  // trace channel enters the synthesis as -l(l+1) c
-        row[(size_t)lam * A.ncf + (3 * ei + s3) * 2 + ri] = (T)v;
-      }
+        for (int lam = 0; lam < 4; ++lam) {
+          double v = A.mem[mem_idx(s3, ri, e, lam, k, A.ne, A.nk)] + twoMu * eps[s3][lam];
+          if (lam == 2) v = -Jr * v;  // trace channel enters the synthesis as -l(l+1) c
+          tile[((size_t)lam * V3_TC + ey * 6 + s3 * 2 + ri) * V3_TP + kx] = (T)v;
+        }
+    }
   }
+  __syncthreads();
+  const int nkb = min(V3_TK, A.nk - k0), w = 6 * min(V3_TE, A.ne3d - e0);
+  for (int t = threadIdx.y * V3_TK + threadIdx.x; t < nkb * 4 * w; t += V3_TK * V3_TE) {
+    const int kl = t / (4 * w), rem = t % (4 * w), lam = rem / w, c = rem % w;
+    X[((size_t)(k0 + kl) * 4 + lam) * A.ncf + 6 * e0 + c] = tile[((size_t)lam * V3_TC + c) * V3_TP + kl];
+  }
+}
+
+template <class T>
+constexpr size_t v3_gather_smem() {
+  return (size_t)4 * V3_TC * V3_TP * sizeof(T);
 }
 
 // ------------------------------------------------------------------ GEMMs
@@ -536,6 +557,17 @@ __global__ void __launch_bounds__(256) k_v3_scatter(V3Args A, const T* __restric
   }
 }
 
+// the gather tile (the FP64 one is above the default 48 KB)
+static void v3_tile_attributes() {
+  static bool done = false;
+  if (done) return;
+  VG_CUDA(cudaFuncSetAttribute(k_v3_gather<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)v3_gather_smem<double>()));
+  VG_CUDA(cudaFuncSetAttribute(k_v3_gather<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)v3_gather_smem<float>()));
+  done = true;
+}
+
 // ------------------------------------------------------------------ host
 
 void visc3d_enable(vg_handle* h, const double* pert) {
@@ -639,12 +671,13 @@ void visc3d_advance(vg_handle* h, const double* d_sigma, double dt, const double
   A.nf = nf;
   A.ncf = ncf;
   dim3 gg((h->nk + 31) / 32, (h->ne3d + 7) / 8);
+  v3_tile_attributes();
   if (h->p.visc3d_precision == VG_VISC3D_SPLIT_TC) {
     float *X32 = nullptr, *dy32 = nullptr;
     visc3d_tc_buffers(h, &X32, &dy32);
     {
       PhaseScope pg(h, VG_PH_V3_GATHER);
-      k_v3_gather<float><<<gg, dim3(32, 8), 0, s>>>(A, X32);
+      k_v3_gather<float><<<gg, dim3(32, 8), v3_gather_smem<float>(), s>>>(A, X32);
       ++h->n_launch;
       VG_CUDA(cudaGetLastError());
     }
@@ -657,7 +690,7 @@ void visc3d_advance(vg_handle* h, const double* d_sigma, double dt, const double
   }
   {
     PhaseScope pg(h, VG_PH_V3_GATHER);
-    k_v3_gather<double><<<gg, dim3(32, 8), 0, s>>>(A, h->d_X.p);
+    k_v3_gather<double><<<gg, dim3(32, 8), v3_gather_smem<double>(), s>>>(A, h->d_X.p);
     ++h->n_launch;
     VG_CUDA(cudaGetLastError());
   }
