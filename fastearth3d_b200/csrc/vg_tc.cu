@@ -46,7 +46,9 @@ constexpr int TM = 128;           // tile rows (MMA M)
 constexpr int TN = 128;           // max columns of one sub-GEMM (MMA N)
 constexpr int KC = 16;            // K per pipeline chunk = two tf32 k-steps
 constexpr int NSTAGE = 3;         // shared-memory ring depth
-constexpr int NTHR = 256;
+constexpr int NTHR = 256;             // loader threads (A operand: fetch, split, store)
+constexpr int MMA_WARP = NTHR / 32;   // the warp after them issues the MMAs
+constexpr int NTHR_ALL = NTHR + 32;
 constexpr int A_WORDS = TM * KC;  // one split term of the A chunk (32-bit words)
 constexpr int B_WORDS = TN * KC;
 constexpr int STAGE_WORDS = 2 * A_WORDS + 2 * B_WORDS;
@@ -120,6 +122,21 @@ __device__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
     if (mbar_try(bar, parity)) return true;
     if (gtimer() - t0 > WAIT_NS) return false;
   }
+}
+
+// bounded wait that also gives up once `abort_flag` is raised (the other side
+// of a producer / consumer handoff stopped)
+__device__ bool mbar_wait_or_abort(uint64_t* bar, uint32_t parity, volatile int* abort_flag) {
+  if (mbar_try(bar, parity)) return true;
+  const unsigned long long t0 = gtimer();
+  while (true) {
+    if (mbar_try(bar, parity)) return true;
+    if (*abort_flag || gtimer() - t0 > WAIT_NS) return false;
+  }
+}
+
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(saddr(bar)) : "memory");
 }
 
 __device__ __forceinline__ void tmem_alloc(uint32_t* slot, uint32_t ncols) {
@@ -378,13 +395,14 @@ __device__ __forceinline__ void store_split(uint32_t* hi_plane, uint32_t* lo_pla
 // ------------------------------------------------------------------ kernel
 
 template <int STAGE>
-__global__ void __launch_bounds__(NTHR, 1) k_tc_stage(Args A) {
+__global__ void __launch_bounds__(NTHR_ALL, 2) k_tc_stage(Args A) {
   extern __shared__ unsigned char smraw[];
   unsigned char* sm = (unsigned char*)(((uintptr_t)smraw + 1023) & ~(uintptr_t)1023);
   uint32_t* stage_base = (uint32_t*)sm;
   uint64_t* bars = (uint64_t*)(sm + (size_t)NSTAGE * STAGE_WORDS * 4);  // NSTAGE + 1: MMA done per stage, drain
   uint64_t* bfull = bars + NSTAGE + 1;                                      // NSTAGE: B bulk copy landed
-  uint32_t* tslot = (uint32_t*)(bfull + NSTAGE);
+  uint64_t* afull = bfull + NSTAGE;                                         // NSTAGE: A stored by all loaders
+  uint32_t* tslot = (uint32_t*)(afull + NSTAGE);
   volatile int* abort_flag = (volatile int*)(tslot + 1);
   double* rsum = (double*)(sm + (size_t)NSTAGE * STAGE_WORDS * 4 + 256);  // [2 subs][2 halves][TM]
   int* slot_sm = (int*)(rsum + 4 * TM);                                     // synthesis: slot(m + dl, m)
@@ -396,13 +414,15 @@ __global__ void __launch_bounds__(NTHR, 1) k_tc_stage(Args A) {
   if (tid == 0) {
     for (int i = 0; i <= NSTAGE; ++i) mbar_init(&bars[i], 1);
     for (int i = 0; i < NSTAGE; ++i) mbar_init(&bfull[i], 1);
+    for (int i = 0; i < NSTAGE; ++i) mbar_init(&afull[i], NTHR);
     fence_mbar_init();
     *abort_flag = 0;
   }
   if (warp == 0) tmem_alloc(tslot, TMEM_COLS);
-  for (int i = tid; i < 4 * TM; i += NTHR) rsum[i] = 0.0;
+  for (int i = tid; i < 4 * TM; i += NTHR_ALL) rsum[i] = 0.0;
   if (STAGE == ST_SYNTH)
-    for (int dl = tid; dl <= A.L - c.batch_m; dl += NTHR) slot_sm[dl] = slot_row(A.kbeg, c.batch_m + dl, c.batch_m, A.nk);
+    for (int dl = tid; dl <= A.L - c.batch_m; dl += NTHR_ALL)
+      slot_sm[dl] = slot_row(A.kbeg, c.batch_m + dl, c.batch_m, A.nk);
   tc_fence_before();
   __syncthreads();
   tc_fence_after();
@@ -418,7 +438,7 @@ __global__ void __launch_bounds__(NTHR, 1) k_tc_stage(Args A) {
   // B chunk of image `I` (chunk kc) into stage buffer `b`: its hi and lo planes
   // are contiguous runs of npad * KC words in the image (offsets multiples of
   // 64 words), two TMA bulk copies issued by one thread onto bfull[b]
-  int b_issued = 0, b_done = 0;  // B copies issued; waited for with success (thread 0)
+  int b_issued = 0;  // B copies issued (loader thread 0 issues them)
   auto copy_b = [&](int b, const ImgInfo& I, int kc) {
     if (tid == 0) {
       uint32_t* Bhi = stage_base + (size_t)b * STAGE_WORDS + 2 * A_WORDS;
@@ -437,100 +457,123 @@ __global__ void __launch_bounds__(NTHR, 1) k_tc_stage(Args A) {
 #pragma unroll
     for (int qq = 0; qq < QPT; ++qq) fetch<STAGE>(A, c, rc, slot_sm, sub, kc * KC + 4 * (lh + 2 * qq), Q[qq]);
   };
-  if (nch > 0) {
-    copy_b(0, c.sub[0].kpad > 0 ? c.sub[0] : c.sub[1], 0);
-    fetch_chunk(0, cur);
-  }
-  if (nch > 1) fetch_chunk(1, nxt);
+  __shared__ int s_b_issued, s_mma_issued;
   int issued = 0;
-  for (int ch = 0; ch < nch; ++ch) {
-    const int buf = ch % NSTAGE;
-    const int sub = ch < nch0 ? 0 : 1, kc = sub ? ch - nch0 : ch;
-    const ImgInfo& I = c.sub[sub];
-    const bool more = ch + 1 < nch;
-    if (more) {
-      // stage buffer of chunk ch + 1 was last read by the MMAs of chunk ch + 1 - NSTAGE
-      const int nb = (ch + 1) % NSTAGE;
-      if (ch + 1 >= NSTAGE && !mbar_wait(&bars[nb], (uint32_t)(((ch + 1) / NSTAGE - 1) & 1))) {
-        *abort_flag = 1;
-        atomicOr(A.status, 1ull << STAGE);
-      }
-      const int sub1 = (ch + 1) < nch0 ? 0 : 1, kc1 = sub1 ? ch + 1 - nch0 : ch + 1;
-      copy_b(nb, c.sub[sub1], kc1);
-    }
-    if (ch + 2 < nch) fetch_chunk(ch + 2, nx2);
-    // A of chunk ch: finish the loads issued two chunks earlier, split, store
-    uint32_t* Ahi = stage_base + (size_t)buf * STAGE_WORDS;
-    uint32_t* Alo = Ahi + A_WORDS;
-#pragma unroll
-    for (int qq = 0; qq < QPT; ++qq) {
-      const int q = lh + 2 * qq;
-      double part = 0.0;
-      const float4 v = finish<STAGE>(c, rc, sub, kc * KC + 4 * q, cur[qq], part);
-      if (sub)
-        sum1 += part;
-      else
-        sum0 += part;
-      store_split(Ahi, Alo, ((size_t)q * TM + lr) * 4, v);
-    }
-    fence_async_smem();
-    __syncthreads();
-    if (*abort_flag) break;
-    if (tid == 0) {
-      if (mbar_wait(&bfull[buf], (uint32_t)((ch / NSTAGE) & 1))) {
+  if (warp == MMA_WARP) {
+    // ---- MMA issuer: chunk ch once its A (all loaders) and B (bulk copy) landed
+    if (lane == 0) {
+      int b_done = 0;
+      for (int ch = 0; ch < nch; ++ch) {
+        const int buf = ch % NSTAGE;
+        const uint32_t ph = (uint32_t)((ch / NSTAGE) & 1);
+        if (!mbar_wait_or_abort(&afull[buf], ph, abort_flag)) {
+          *abort_flag = 1;
+          atomicOr(A.status, 1ull << (12 + STAGE));
+          break;
+        }
+        if (!mbar_wait(&bfull[buf], ph)) {
+          *abort_flag = 1;
+          atomicOr(A.status, 1ull << (4 + STAGE));
+          break;
+        }
         ++b_done;
-      } else {
-        *abort_flag = 1;
-        atomicOr(A.status, 1ull << (4 + STAGE));
-      }
-    }
-    if (tid == 0 && !*abort_flag) {
-      tc_fence_after();
-      uint32_t* Bhi = Alo + A_WORDS;
-      uint32_t* Blo = Bhi + B_WORDS;
-      const uint32_t idesc = idesc_tf32(TM, I.npad);
-      const uint32_t d = tmem + (uint32_t)(sub * TN);
+        tc_fence_after();
+        const int sub = ch < nch0 ? 0 : 1, kc = sub ? ch - nch0 : ch;
+        const ImgInfo& I = c.sub[sub];
+        uint32_t* Ahi = stage_base + (size_t)buf * STAGE_WORDS;
+        uint32_t* Alo = Ahi + A_WORDS;
+        uint32_t* Bhi = Alo + A_WORDS;
+        uint32_t* Blo = Bhi + B_WORDS;
+        const uint32_t idesc = idesc_tf32(TM, I.npad);
+        const uint32_t d = tmem + (uint32_t)(sub * TN);
 #pragma unroll
-      for (int ks = 0; ks < KC / 8; ++ks) {
-        const uint32_t aoff = (uint32_t)ks * 2 * TM * 16, boff = (uint32_t)ks * 2 * I.npad * 16;
-        const uint64_t dah = sdesc(saddr(Ahi) + aoff, TM * 16, 128);
-        const uint64_t dal = sdesc(saddr(Alo) + aoff, TM * 16, 128);
-        const uint64_t dbh = sdesc(saddr(Bhi) + boff, I.npad * 16, 128);
-        const uint64_t dbl = sdesc(saddr(Blo) + boff, I.npad * 16, 128);
-        mma_tf32(d, dah, dbh, idesc, (kc > 0 || ks > 0) ? 1u : 0u);
-        mma_tf32(d, dah, dbl, idesc, 1u);
-        mma_tf32(d, dal, dbh, idesc, 1u);
+        for (int ks = 0; ks < KC / 8; ++ks) {
+          const uint32_t aoff = (uint32_t)ks * 2 * TM * 16, boff = (uint32_t)ks * 2 * I.npad * 16;
+          const uint64_t dah = sdesc(saddr(Ahi) + aoff, TM * 16, 128);
+          const uint64_t dal = sdesc(saddr(Alo) + aoff, TM * 16, 128);
+          const uint64_t dbh = sdesc(saddr(Bhi) + boff, I.npad * 16, 128);
+          const uint64_t dbl = sdesc(saddr(Blo) + boff, I.npad * 16, 128);
+          mma_tf32(d, dah, dbh, idesc, (kc > 0 || ks > 0) ? 1u : 0u);
+          mma_tf32(d, dah, dbl, idesc, 1u);
+          mma_tf32(d, dal, dbh, idesc, 1u);
+        }
+        mma_commit(&bars[buf]);
+        ++issued;
       }
-      mma_commit(&bars[buf]);
+      if (issued > 0) mma_commit(&bars[NSTAGE]);  // drain: tracks every MMA this thread issued
+      s_b_issued = b_done;  // the B copies this side has seen land
+      s_mma_issued = issued;
     }
-    ++issued;
-    if (more) {
+    __syncwarp();
+  } else {
+    // ---- loaders: A of chunk ch into stage buffer ch % NSTAGE, B bulk copies one chunk ahead
+    if (nch > 0) {
+      copy_b(0, c.sub[0].kpad > 0 ? c.sub[0] : c.sub[1], 0);
+      fetch_chunk(0, cur);
+    }
+    if (nch > 1) fetch_chunk(1, nxt);
+    for (int ch = 0; ch < nch; ++ch) {
+      const int buf = ch % NSTAGE;
+      const int sub = ch < nch0 ? 0 : 1, kc = sub ? ch - nch0 : ch;
+      const bool more = ch + 1 < nch;
+      if (more) {
+        // stage buffer of chunk ch + 1 was last read by the MMAs of chunk ch + 1 - NSTAGE
+        const int nb = (ch + 1) % NSTAGE;
+        if (ch + 1 >= NSTAGE && !mbar_wait_or_abort(&bars[nb], (uint32_t)(((ch + 1) / NSTAGE - 1) & 1), abort_flag)) {
+          *abort_flag = 1;
+          atomicOr(A.status, 1ull << STAGE);
+        }
+        if (*abort_flag) break;
+        const int sub1 = (ch + 1) < nch0 ? 0 : 1, kc1 = sub1 ? ch + 1 - nch0 : ch + 1;
+        copy_b(nb, c.sub[sub1], kc1);
+      }
+      if (ch + 2 < nch) fetch_chunk(ch + 2, nx2);
+      // A of chunk ch: finish the loads issued two chunks earlier, split, store
+      uint32_t* Ahi = stage_base + (size_t)buf * STAGE_WORDS;
+      uint32_t* Alo = Ahi + A_WORDS;
 #pragma unroll
       for (int qq = 0; qq < QPT; ++qq) {
-        cur[qq] = nxt[qq];
-        nxt[qq] = nx2[qq];
+        const int q = lh + 2 * qq;
+        double part = 0.0;
+        const float4 v = finish<STAGE>(c, rc, sub, kc * KC + 4 * q, cur[qq], part);
+        if (sub)
+          sum1 += part;
+        else
+          sum0 += part;
+        store_split(Ahi, Alo, ((size_t)q * TM + lr) * 4, v);
+      }
+      fence_async_smem();  // this thread's A stores, visible to the tensor cores
+      mbar_arrive(&afull[buf]);
+      if (more) {
+#pragma unroll
+        for (int qq = 0; qq < QPT; ++qq) {
+          cur[qq] = nxt[qq];
+          nxt[qq] = nx2[qq];
+        }
       }
     }
   }
+  __syncthreads();
   // B copies still in flight after an abort: wait for them (bounded) before
   // the stage ring is reused or the CTA exits
   if (tid == 0)
-    for (int q = b_done; q < b_issued; ++q)
+    for (int q = s_b_issued; q < b_issued; ++q)
       if (!mbar_wait(&bfull[q % NSTAGE], (uint32_t)((q / NSTAGE) & 1))) atomicOr(A.status, 1ull << (4 + STAGE));
-  // drain: one more commit tracks every MMA this thread issued
+  // drain: the issuer's last commit completes once every MMA has
   bool ok = (*abort_flag == 0);
-  if (tid == 0 && issued > 0) mma_commit(&bars[NSTAGE]);
-  if (issued > 0 && !mbar_wait(&bars[NSTAGE], 0)) {
+  if (s_mma_issued > 0 && !mbar_wait(&bars[NSTAGE], 0)) {
     ok = false;
     atomicOr(A.status, 1ull << (8 + STAGE));
   }
   // per-row side sums of the two loader threads
-  rsum[(0 * 2 + lh) * TM + lr] = sum0;
-  rsum[(1 * 2 + lh) * TM + lr] = sum1;
+  if (tid < NTHR) {
+    rsum[(0 * 2 + lh) * TM + lr] = sum0;
+    rsum[(1 * 2 + lh) * TM + lr] = sum1;
+  }
   ok = __syncthreads_and(ok) != 0;  // the same epilogue decision in every thread
   tc_fence_after();
 
-  if (ok && !*abort_flag) {
+  if (ok && !*abort_flag) {  // the MMA warp (chalf 2) finds no columns below and only joins the barriers
     const int quad = warp & 3, chalf = warp >> 2;
     const int r = quad * 32 + lane;  // tile row of this thread
     const int row = c.row0 + r;
@@ -568,7 +611,7 @@ __global__ void __launch_bounds__(NTHR, 1) k_tc_stage(Args A) {
       const float* rate_j = rate_g + e3;
       if (A.nphi * A.ne3d <= NSTAGE * STAGE_WORDS) {  // uniform: fits the ring (always at lmax 128)
         float* rate_s = reinterpret_cast<float*>(stage_base);
-        for (int t = tid; t < A.nphi * A.ne3d; t += NTHR) rate_s[t] = __ldg(&rate_g[t]);
+        for (int t = tid; t < A.nphi * A.ne3d; t += NTHR_ALL) rate_s[t] = __ldg(&rate_g[t]);
         __syncthreads();
         rate_j = rate_s + e3;
       }
@@ -862,7 +905,7 @@ void visc3d_tc_run(vg_handle* h, double dt, bool trap) {
   auto launch = [&](auto kernel, int phase, const tc::ImgInfo* info, dim3 grid) {
     PhaseScope ps(h, phase);
     a.info = info;
-    kernel<<<grid, tc::NTHR, tc::SMEM_BYTES, s>>>(a);
+    kernel<<<grid, tc::NTHR_ALL, tc::SMEM_BYTES, s>>>(a);
     ++h->n_launch;
     VG_CUDA(cudaGetLastError());
   };
