@@ -203,9 +203,9 @@ def stage_work(w, info):
 
 # DRAM bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum) of the
 # split-path stages, from one `ncu --set full` capture of the lmax-128 3-D
-# workload (second sub-step of `bench.py --steps 2 --warmup 1 --plain off`)
-NCU_TRAFFIC = {("c3_3d_l128", "v3_synth"): 146.96e6, ("c3_3d_l128", "v3_lon_inv"): 224.46e6,
-               ("c3_3d_l128", "v3_lon_fwd"): 219.99e6, ("c3_3d_l128", "v3_analysis"): 206.34e6}
+# workload (second sub-step of `bench.py --steps 2 --warmup 1 --plain off --grad-fwd off`)
+NCU_TRAFFIC = {("c3_3d_l128", "v3_synth"): 150.75e6, ("c3_3d_l128", "v3_lon_inv"): 227.35e6,
+               ("c3_3d_l128", "v3_lon_fwd"): 223.56e6, ("c3_3d_l128", "v3_analysis"): 209.04e6}
 
 
 def max_over_ranks(ms, dist, device):
