@@ -374,6 +374,38 @@ int vg_get_state(vg_handle* h, double* Are, double* Aim, double* Bre, double* Bi
   });
 }
 
+int vg_get_step_state(vg_handle* h, double* dt_try_yr, double* sigma_n, int* sigma_primed) {
+  return guarded(h, [&] {
+    if (dt_try_yr) *dt_try_yr = h->dt_try / vg::SEC_PER_YEAR;
+    const bool tracked = h->sigma_primed && h->d_sigma_n.p != nullptr;
+    if (sigma_primed) *sigma_primed = tracked ? 1 : 0;
+    if (sigma_n) {
+      const size_t n2 = 2 * (size_t)h->grid.nlm;
+      if (tracked) {
+        h->d_sigma_n.download(sigma_n, n2, h->stream);
+        VG_CUDA(cudaStreamSynchronize(h->stream));
+      } else {
+        for (size_t i = 0; i < n2; ++i) sigma_n[i] = 0.0;
+      }
+    }
+  });
+}
+
+int vg_set_step_state(vg_handle* h, double dt_try_yr, const double* sigma_n, int sigma_primed) {
+  return guarded(h, [&] {
+    need(h, !(sigma_primed && !sigma_n), "vg_set_step_state: a primed sigma_n is required");
+    need(h, !(sigma_primed && h->p.scheme != VG_SCHEME_TRAP),
+         "vg_set_step_state: sigma_n is tracked by the trapezoidal scheme only");
+    h->dt_try = dt_try_yr * vg::SEC_PER_YEAR;
+    h->sigma_primed = false;
+    if (sigma_primed) {
+      h->d_sigma_n.upload(sigma_n, 2 * (size_t)h->grid.nlm, h->stream);
+      VG_CUDA(cudaStreamSynchronize(h->stream));
+      h->sigma_primed = true;
+    }
+  });
+}
+
 int vg_set_state(vg_handle* h, const double* Are, const double* Aim, const double* Bre, const double* Bim,
                  const double* Cre, const double* Cim, double time_s) {
   return guarded(h, [&] {

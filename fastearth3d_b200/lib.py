@@ -39,6 +39,8 @@ _SIGS = [
     ("vg_set_state", [_VP, _P, _P, _P, _P, _P, _P, C.c_double]),
     ("vg_set_fields", [_VP, _P, _P, _P, _P]),
     ("vg_get_rotation_state", [_VP, _P, _P, _P]),
+    ("vg_get_step_state", [_VP, _P, _P, C.POINTER(C.c_int)]),
+    ("vg_set_step_state", [_VP, C.c_double, _P, C.c_int]),
     ("vg_set_rotation_state", [_VP, _P, _P, _P]),
     ("vg_spinup", [_VP, _P, C.c_double, C.c_double, _P, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
     ("vg_misfit", [_VP, C.c_int, C.c_double, _P, C.c_int, C.POINTER(C.c_int), _P, _P]),
@@ -163,6 +165,19 @@ class Model:
     def set_fields(self, h_ice=None, rsl=None, z_bed=None, C_ocean=None):
         self._c(lib().vg_set_fields(self.h, *[ptr(None if a is None else np.ascontiguousarray(a, dtype=np.float64))
                                               for a in (h_ice, rsl, z_bed, C_ocean)]))
+
+    def step_state(self):
+        """(dt_try [yr], sigma_n as nlm complex, primed) of the time stepper."""
+        dt = C.c_double(0.0)
+        pr = C.c_int(0)
+        q = np.zeros(2 * self.nlm)
+        self._c(lib().vg_get_step_state(self.h, C.byref(dt), ptr(q), C.byref(pr)))
+        return dt.value, q[0::2] + 1j * q[1::2], bool(pr.value)
+
+    def set_step_state(self, dt_try_yr, sigma_n, primed):
+        q = np.zeros(2 * self.nlm)
+        q[0::2], q[1::2] = np.real(sigma_n), np.imag(sigma_n)
+        self._c(lib().vg_set_step_state(self.h, dt_try_yr, ptr(q), 1 if primed else 0))
 
     def rotation_state(self):
         n = 6 * self.ne * 4

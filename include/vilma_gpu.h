@@ -184,6 +184,16 @@ int vg_set_state(vg_handle* h, const double* Are, const double* Aim, const doubl
  * After vg_set_reference. */
 int vg_set_fields(vg_handle* h, const double* h_ice, const double* rsl, const double* z_bed,
                   const double* C);
+/* Time-stepping restart state (the restart variables "dt_try", "sigma_n_re",
+ * "sigma_n_im", "sigma_primed" of src/vilma_io.f90:38-46, 329-334, 457-458,
+ * 599-615): the adaptive controller's next-step suggestion dt_try [yr] (used by
+ * the trapezoidal scheme, carried by every scheme) and the trapezoidal
+ * scheme's start-of-step load sigma_n (nlm complex, interleaved) with its
+ * primed flag (0: not tracked; the next update seeds it with a report-only
+ * solve). vg_set_state clears the flag, so restore with vg_set_step_state
+ * after it. sigma_n may be NULL (get: not returned; set: only with primed = 0). */
+int vg_get_step_state(vg_handle* h, double* dt_try_yr, double* sigma_n, int* sigma_primed);
+int vg_set_step_state(vg_handle* h, double dt_try_yr, const double* sigma_n, int sigma_primed);
 /* Rotation restart state (rotation_get_memory / rotation_set_memory,
  * src/vilma_rotation.f90:275-295): polar motion m as (re, im) and the load and
  * tidal channels' memory stress, each (NLAM=4, ne, 6) Fortran order with the
