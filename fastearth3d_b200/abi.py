@@ -40,6 +40,7 @@ class VgParams(C.Structure):
         ("grow_max", C.c_double), ("shrink_min", C.c_double),
         ("sle_max_mem_iter", C.c_int),
         ("couple_tol", C.c_double),
+        ("toroidal", C.c_int),
     ]
 
 

@@ -84,6 +84,10 @@ typedef struct vg_params {
   double rtol, atol, safety, grow_max, shrink_min;
   int sle_max_mem_iter;
   double couple_tol;
+  /* l_toroidal (src/vilma_params.f90:156, default 0): carry the toroidal
+   * degree of freedom (W and the lambda 3, 4 memory) once a genuinely 3-D
+   * element exists (src/vilma_response.f90:1048-1118) */
+  int toroidal;
 } vg_params;
 
 /* Phase timers (the reference's [PROFILE] buckets: drift solve, memory

@@ -96,6 +96,23 @@ void radial_operator_solve_vec(const RadialOp& op, const double* b, double* x, c
 void radial_operator_load_rhs(const RadialOp& op, double sigma, double* b);
 void loading_love(const Earth& e, int j, double sigma, double Ua, double Va, double Fa,
                   double& h, double& l, double& k);
+// w: (nd, nb) column-major border columns, nb = 0 for none
+void bordered_band_factor(BorderedBand& sys, const std::vector<double>& A, int nd, const std::vector<double>& w,
+                          int nb);
+void bordered_band_solve(const BorderedBand& sys, const double* b, double* x, const double* border);
+
+// vilma_radial_fe.f90:699-817: the per-degree toroidal W operator (nr x nr,
+// tridiagonal; dead nodes pinned; degree 1 bordered by per-shell net-rotation
+// constraints)
+struct TorOp {
+  int j = -1, nr = 0, ne = 0;
+  BorderedBand sys;
+  std::vector<char> pinned;  // per node
+};
+std::vector<double> build_toroidal_operator(const std::vector<double>& r, const std::vector<double>& mu, int j);
+std::vector<double> rotation_weights(const std::vector<double>& r, const std::vector<double>& mu, int& nshell);
+void toroidal_operator_assemble(TorOp& op, const std::vector<double>& r, const std::vector<double>& mu, int j);
+void toroidal_operator_solve_vec(const TorOp& op, const double* b, double* x);
 
 // ---------------------------------------------------------------- SHT grid
 struct Sht {
@@ -106,6 +123,7 @@ struct Sht {
   std::vector<int> ldeg, mord;              // nlm
   std::vector<double> llp1;                 // nlm
   std::vector<double> n6;                   // 0..lmax, spin-2 norm
+  std::vector<double> n4;                   // 0..lmax, toroidal spin-2 norm
   // FFT plan (mixed radix over nphi)
   std::vector<int> fft_factors;
   std::vector<cplx> tw;  // exp(-2 pi i k / nphi)
@@ -117,12 +135,17 @@ void sht_synth(const Sht& s, const cplx* q, double* f);
 void sht_analysis(const Sht& s, const double* f, cplx* q);
 void sht_sph_synth(const Sht& s, const cplx* sl, double* vt, double* vp);
 void sht_sph_analysis(const Sht& s, const double* vt, const double* vp, cplx* sl);
-void tensor_synth(const Sht& s, const cplx* c /*4*nlm, channel-major*/, double* dyad /*6*np*nl*/);
-void tensor_analysis(const Sht& s, const double* dyad, cplx* c);
+// c: (nch, nlm) channel-major, nch = 4 (lambda 1,2,5,6) or 6 (+ lambda 3,4)
+void tensor_synth(const Sht& s, const cplx* c, double* dyad /*6*np*nl*/, int nch = 4);
+void tensor_analysis(const Sht& s, const double* dyad, cplx* c, int nch = 4);
+// e_r x grad_1 T = (-F, E) (vilma_sht.f90:258-277) and its analysis
+void sht_tor_synth(const Sht& s, const cplx* tl, double* vt, double* vp);
+void sht_tor_analysis(const Sht& s, const double* vt, const double* vp, cplx* tl);
 void sht_calibrate_n6(Sht& s);
 
 // ---------------------------------------------------------------- response
 constexpr int NLAM = 4;
+constexpr int NLAM_TOR = 2;  // vilma_viscoelastic.f90: lambda 3, 4
 // vilma_viscoelastic.f90:60-64 memory-scheme codes (forward Euler, trapezoidal)
 enum Scheme { SCHEME_FE = 0, SCHEME_TRAP = 2 };
 
@@ -167,6 +190,19 @@ struct Response {
   double time_s = 0;
   std::vector<cplx> sigma_n_s;
   bool sigma_primed_s = false;
+  // toroidal channels (vilma_response.f90:126-146, 1055-1118): carried once a
+  // 3-D element exists and `toroidal` is set. Memory (NLAM_TOR, ne, nk):
+  // [k][e][lam], lam 0 = lambda 3, 1 = lambda 4.
+  bool toroidal = false;
+  int nlam = NLAM;
+  std::vector<TorOp> tops;                       // index l (0 unused)
+  std::vector<double> nrmt, sat, sbt, sct;       // l*2 + lam; l*4 + t*2 + lam
+  std::vector<double> Atre, Atim, Btre, Btim, Ctre, Ctim;
+  std::vector<cplx> dWa, dWa_prev;               // surface W drift (nk)
+  std::vector<double> dWn_re, dWn_im, edWn_re, edWn_im;  // [k][node]
+  std::vector<double> Atre0, Atim0, Btre0, Btim0, Ctre0, Ctim0;
+  std::vector<double> Atre_s, Atim_s, Btre_s, Btim_s, Ctre_s, Ctim_s;
+  std::vector<double> Atre_c, Atim_c, Btre_c, Btim_c, Ctre_c, Ctim_c;
   // profile counters
   double t_drift = 0, t_mem = 0;
   long n_drift = 0, n_mem = 0, n_solved = 0;
@@ -179,6 +215,7 @@ void response_set_dt(Response& R, double dt);
 double response_max_rate(const Response& R);
 double response_memory_norm(const Response& R);
 void response_enable_lateral_visc(Response& R, const Sht& s, const double* pert /*[e][j][i]*/);
+void response_enable_toroidal(Response& R);
 void response_prepare_endpoint(Response& R);
 void response_advance_endpoint(Response& R, const Sht& s, const cplx* sigma);
 bool response_endpoint_converged(const Response& R);

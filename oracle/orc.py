@@ -56,8 +56,11 @@ def lib():
             ("orc_love_numbers", [C.POINTER(VgParams), C.c_int, C.c_int, _P, _P, _P]),
             ("orc_band_dense_solve", [C.c_int, _P, _P, _P]),
             ("orc_dense_operator", [C.POINTER(VgParams), C.c_int, C.c_int, _P, C.POINTER(C.c_int)]),
-            ("orc_tensor_synth", [_VP, _P, _P]),
-            ("orc_tensor_analysis", [_VP, _P, _P]),
+            ("orc_tensor_synth", [_VP, _P, _P, C.c_int]),
+            ("orc_tensor_analysis", [_VP, _P, _P, C.c_int]),
+            ("orc_get_toroidal", [_VP, _P]),
+            ("orc_get_state_tor", [_VP, _P, _P, _P, _P, _P, _P, C.POINTER(C.c_int)]),
+            ("orc_toroidal_operator", [C.POINTER(VgParams), C.c_int, _P, C.POINTER(C.c_int)]),
             ("orc_grid", [_VP, _P, _P]),
             ("orc_mesh", [_VP, _P, C.POINTER(C.c_int)]),
         ]:
@@ -104,6 +107,15 @@ def band_dense_solve(A, b):
     x = np.zeros(n)
     _check(lib().orc_band_dense_solve(n, ptr(flat), ptr(np.ascontiguousarray(b, dtype=np.float64)), ptr(x)))
     return x
+
+
+def toroidal_operator(p, j):
+    """Dense toroidal W operator of degree j (nr x nr), nothing pinned."""
+    nr = C.c_int(0)
+    _check(lib().orc_toroidal_operator(C.byref(p), j, None, C.byref(nr)))
+    A = np.zeros(nr.value * nr.value)
+    _check(lib().orc_toroidal_operator(C.byref(p), j, ptr(A), C.byref(nr)))
+    return A.reshape(nr.value, nr.value).T.copy()
 
 
 def dense_operator(p, j, with_uniq=True):
@@ -228,18 +240,34 @@ class Oracle:
         return f
 
     def tensor_synth(self, c):
-        """c: (4, nlm) complex -> dyad (6, ng)"""
-        s = np.zeros(2 * 4 * self.nlm)
+        """c: (4 or 6, nlm) complex -> dyad (6, ng) (rr, rt, rp, tt, tp, pp)"""
+        nch = c.shape[0]
+        s = np.zeros(2 * nch * self.nlm)
         cf = np.ascontiguousarray(c).reshape(-1)
         s[0::2], s[1::2] = cf.real, cf.imag
         d = np.zeros(6 * self.ng)
-        self._c(lib().orc_tensor_synth(self.h, ptr(s), ptr(d)))
+        self._c(lib().orc_tensor_synth(self.h, ptr(s), ptr(d), nch))
         return d.reshape(6, self.ng)
 
-    def tensor_analysis(self, dyad):
-        c = np.zeros(2 * 4 * self.nlm)
-        self._c(lib().orc_tensor_analysis(self.h, ptr(np.ascontiguousarray(dyad, dtype=np.float64).reshape(-1)), ptr(c)))
-        return (c[0::2] + 1j * c[1::2]).reshape(4, self.nlm)
+    def tensor_analysis(self, dyad, nch=4):
+        c = np.zeros(2 * nch * self.nlm)
+        d = np.ascontiguousarray(dyad, dtype=np.float64).reshape(-1)
+        self._c(lib().orc_tensor_analysis(self.h, ptr(d), ptr(c), nch))
+        return (c[0::2] + 1j * c[1::2]).reshape(nch, self.nlm)
+
+    def toroidal(self):
+        """Surface toroidal drift W(a) as t_lm (lm order); zero while not carried."""
+        t = np.zeros(2 * self.nlm)
+        self._c(lib().orc_get_toroidal(self.h, ptr(t)))
+        return t[0::2] + 1j * t[1::2]
+
+    def state_tor(self):
+        """Toroidal memory (NLAM_TOR, ne, nk) x 6, or None while not carried."""
+        n = 2 * self.ne * self.nk
+        arrs = [np.zeros(n) for _ in range(6)]
+        c = C.c_int(0)
+        self._c(lib().orc_get_state_tor(self.h, *[ptr(a) for a in arrs], C.byref(c)))
+        return arrs if c.value else None
 
     def grid(self):
         colat, w = np.zeros(self.p.nlat), np.zeros(self.p.nlat)

@@ -80,6 +80,7 @@ int orc_params_default(vg_params* p) {
   p->shrink_min = 0.2;
   p->sle_max_mem_iter = 20;
   p->couple_tol = 1e-6;
+  p->toroidal = 0;
   return 0;
 }
 
@@ -109,6 +110,7 @@ int orc_create(const vg_params* p, OrcHandle** out) {
     response_init_ve(h->R, h->earth, h->mesh, h->sht, dt0);
     h->R.scheme = p->scheme;
     h->R.couple_tol = p->couple_tol;
+    h->R.toroidal = p->toroidal != 0;
     h->sle.max_mem_iter = p->sle_max_mem_iter;
     h->st.rtol = p->rtol;
     h->st.atol = p->atol;
@@ -389,6 +391,56 @@ int orc_set_state(OrcHandle* h, const double* Are, const double* Aim, const doub
   h->R.time = time_s;
   return 0;
 }
+// response_horizontal_toroidal (vilma_response.f90:884-900): t_lm of the
+// surface W(a) of the last drift solve, in lm order; zero while no toroidal
+// field is carried
+int orc_get_toroidal(OrcHandle* h, double* t_lm) {
+  for (int lm = 0; lm < 2 * h->sht.nlm; ++lm) t_lm[lm] = 0.0;
+  if (h->R.nlam == NLAM) return 0;
+  for (int k = 0; k < h->R.nk; ++k) {
+    t_lm[2 * h->R.k2lm[k]] = h->R.dWa[k].real();
+    t_lm[2 * h->R.k2lm[k] + 1] = h->R.dWa[k].imag();
+  }
+  return 0;
+}
+// toroidal memory in the (NLAM_TOR, ne, nk) layout; *carried = 0 (and
+// nothing written) while only the spheroidal channels exist
+int orc_get_state_tor(OrcHandle* h, double* Are, double* Aim, double* Bre, double* Bim, double* Cre, double* Cim,
+                      int* carried) {
+  *carried = h->R.nlam > NLAM ? 1 : 0;
+  if (!*carried) return 0;
+  std::copy(h->R.Atre.begin(), h->R.Atre.end(), Are);
+  std::copy(h->R.Atim.begin(), h->R.Atim.end(), Aim);
+  std::copy(h->R.Btre.begin(), h->R.Btre.end(), Bre);
+  std::copy(h->R.Btim.begin(), h->R.Btim.end(), Bim);
+  std::copy(h->R.Ctre.begin(), h->R.Ctre.end(), Cre);
+  std::copy(h->R.Ctim.begin(), h->R.Ctim.end(), Cim);
+  return 0;
+}
+// dense toroidal operator of degree j on the params' mesh (nr x nr, column-major)
+int orc_toroidal_operator(const vg_params* p, int j, double* A, int* nr_out) {
+  Earth e;
+  e.r_earth = p->r_earth;
+  for (int i = 0; i < p->n_layer; ++i) {
+    Layer L;
+    L.r_bot = p->r_bot[i];
+    L.r_top = p->r_top[i];
+    L.rho = p->rho[i];
+    L.mu = p->mu[i];
+    L.eta = p->eta[i];
+    L.rheology = p->rheology[i];
+    e.layers.push_back(L);
+  }
+  Mesh m = radial_mesh_build(e, p->ne_layer);
+  *nr_out = m.nr;
+  if (A) {
+    std::vector<double> mu(m.ne);
+    for (int k = 0; k < m.ne; ++k) mu[k] = e.layers[m.elem_layer[k]].mu;  // as response_init_ve
+    std::vector<double> D = build_toroidal_operator(m.r, mu, j);
+    std::copy(D.begin(), D.end(), A);
+  }
+  return 0;
+}
 int orc_sht_analysis(OrcHandle* h, const double* f, double* q) {
   std::vector<cplx> c(h->sht.nlm);
   sht_analysis(h->sht, f, c.data());
@@ -486,18 +538,21 @@ int orc_dense_operator(const vg_params* p, int j, int with_uniq, double* A, int*
   return 0;
 }
 
-// tensor synth/analysis round trip on the handle's grid (test_tensor_sh path)
-int orc_tensor_synth(OrcHandle* h, const double* c /* 4*nlm complex, channel-major */, double* dyad) {
+// tensor synth/analysis round trip on the handle's grid (test_tensor_sh path);
+// nch = 4 (spheroidal) or 6 (with the toroidal lambda 3, 4)
+int orc_tensor_synth(OrcHandle* h, const double* c /* nch*nlm complex, channel-major */, double* dyad, int nch) {
+  if (nch != 4 && nch != 6) return 2;
   sht_calibrate_n6(h->sht);
-  std::vector<cplx> cc((size_t)4 * h->sht.nlm);
+  std::vector<cplx> cc((size_t)nch * h->sht.nlm);
   for (size_t t = 0; t < cc.size(); ++t) cc[t] = cplx(c[2 * t], c[2 * t + 1]);
-  tensor_synth(h->sht, cc.data(), dyad);
+  tensor_synth(h->sht, cc.data(), dyad, nch);
   return 0;
 }
-int orc_tensor_analysis(OrcHandle* h, const double* dyad, double* c) {
+int orc_tensor_analysis(OrcHandle* h, const double* dyad, double* c, int nch) {
+  if (nch != 4 && nch != 6) return 2;
   sht_calibrate_n6(h->sht);
-  std::vector<cplx> cc((size_t)4 * h->sht.nlm);
-  tensor_analysis(h->sht, dyad, cc.data());
+  std::vector<cplx> cc((size_t)nch * h->sht.nlm);
+  tensor_analysis(h->sht, dyad, cc.data(), nch);
   for (size_t t = 0; t < cc.size(); ++t) {
     c[2 * t] = cc[t].real();
     c[2 * t + 1] = cc[t].imag();

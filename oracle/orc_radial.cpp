@@ -360,14 +360,13 @@ static double colnorm_of(const double* col, int n, int stride) {
 }
 
 // vilma_radial_fe.f90:497-576 bordered_band_factor
-static void bordered_band_factor(BorderedBand& sys, const std::vector<double>& A, int nd,
-                                 const std::vector<double>* w) {
-  int nb = w ? 1 : 0;
+void bordered_band_factor(BorderedBand& sys, const std::vector<double>& A, int nd, const std::vector<double>& w,
+                          int nb) {
   sys.nd = nd;
   sys.nb = nb;
   sys.ns = nd + nb;
   sys.w.assign((size_t)nd * nb, 0.0);
-  if (nb) sys.w = *w;
+  if (nb) sys.w.assign(w.begin(), w.begin() + (size_t)nd * nb);
   sys.dc.assign(nd, 1.0);
   sys.dr.assign(nd, 1.0);
   std::vector<double> dc_b(nb), dr_b(nb);
@@ -421,8 +420,7 @@ static void bordered_band_factor(BorderedBand& sys, const std::vector<double>& A
 }
 
 // vilma_radial_fe.f90:578-605 bordered_band_solve
-static void bordered_band_solve(const BorderedBand& sys, const double* b, double* x,
-                                const double* border) {
+void bordered_band_solve(const BorderedBand& sys, const double* b, double* x, const double* border) {
   std::vector<double> bs(sys.ns, 0.0);
   for (int i = 0; i < sys.nd; ++i) bs[i] = sys.dr[i] * b[i];
   if (border)
@@ -443,9 +441,9 @@ void radial_operator_assemble(RadialOp& op, const Earth& e, const Mesh& m, int j
   op.g_surf = earth_gravity_at(e, e.r_earth);
   if (j == 1) {
     std::vector<double> w = uniq_weight(m);
-    bordered_band_factor(op.sys, A, nd, &w);
+    bordered_band_factor(op.sys, A, nd, w, 1);
   } else {
-    bordered_band_factor(op.sys, A, nd, nullptr);
+    bordered_band_factor(op.sys, A, nd, {}, 0);
   }
   op.nullmode.clear();
   if (op.sys.nb > 0) {
@@ -486,6 +484,90 @@ void loading_love(const Earth& e, int j, double sigma, double Ua, double Va, dou
   h = g * Ua / phiL;
   l = g * Va / phiL;
   k = -Fa / phiL - 1.0;
+}
+
+}  // namespace orc
+
+namespace orc {
+
+// vilma_radial_integrals.f90:117-126 elem_k4: int psi_a r^3 dr
+static void K4(double rk, double rk1, double v[2]) {
+  double h = rk1 - rk;
+  v[0] = h / 20.0 * (rk1 * rk1 * rk1 + 2.0 * rk1 * rk1 * rk + 3.0 * rk1 * rk * rk + 4.0 * rk * rk * rk);
+  v[1] = h / 20.0 * (4.0 * rk1 * rk1 * rk1 + 3.0 * rk1 * rk1 * rk + 2.0 * rk1 * rk * rk + rk * rk * rk);
+}
+
+// vilma_radial_fe.f90:699-729 build_toroidal_operator: per element
+// mu_k { J [I1 - I3(b,a) - I3(a,b) + I6] + J(J-2) I6 } W^a dW^b; column-major
+std::vector<double> build_toroidal_operator(const std::vector<double>& r, const std::vector<double>& mu, int j) {
+  const int nr = (int)r.size(), ne = (int)mu.size();
+  const double Jr = (double)j * (double)(j + 1);
+  std::vector<double> A((size_t)nr * nr, 0.0);
+  for (int e = 0; e < ne; ++e) {
+    if (mu[e] == 0.0) continue;
+    M2 i1 = I1(r[e], r[e + 1]), i3 = I3(r[e], r[e + 1]), i6 = I6(r[e], r[e + 1]);
+    for (int ia = 0; ia < 2; ++ia)      // trial node
+      for (int ib = 0; ib < 2; ++ib) {  // test node: row
+        A[(size_t)(e + ia) * nr + (e + ib)] +=
+            mu[e] * (Jr * (i1.v[ia][ib] - i3.v[ib][ia] - i3.v[ia][ib] + i6.v[ia][ib]) + Jr * (Jr - 2.0) * i6.v[ia][ib]);
+      }
+  }
+  return A;
+}
+
+// vilma_radial_fe.f90:745-773 rotation_weights: one column per solid shell
+// (a maximal run of mu > 0 elements), w_s(k) = sum_{e in s} int psi_k r^3 dr
+std::vector<double> rotation_weights(const std::vector<double>& r, const std::vector<double>& mu, int& nshell) {
+  const int nr = (int)r.size(), ne = (int)mu.size();
+  std::vector<int> shell(ne, -1);
+  int ns = 0;
+  bool prev = false;
+  for (int e = 0; e < ne; ++e) {
+    bool solid = mu[e] > 0.0;
+    if (solid && !prev) ++ns;
+    if (solid) shell[e] = ns - 1;
+    prev = solid;
+  }
+  std::vector<double> w((size_t)nr * ns, 0.0);
+  for (int e = 0; e < ne; ++e) {
+    if (shell[e] < 0) continue;
+    double k4[2];
+    K4(r[e], r[e + 1], k4);
+    w[(size_t)shell[e] * nr + e] += k4[0];
+    w[(size_t)shell[e] * nr + e + 1] += k4[1];
+  }
+  nshell = ns;
+  return w;
+}
+
+// vilma_radial_fe.f90:775-799 toroidal_operator_assemble (with
+// toroidal_dead_nodes, :731-743)
+void toroidal_operator_assemble(TorOp& op, const std::vector<double>& r, const std::vector<double>& mu, int j) {
+  if (j < 1) throw std::runtime_error("toroidal_operator_assemble: toroidal fields start at degree 1");
+  const int nr = (int)r.size(), ne = (int)mu.size();
+  op.j = j;
+  op.nr = nr;
+  op.ne = ne;
+  std::vector<double> A = build_toroidal_operator(r, mu, j);
+  op.pinned.assign(nr, 1);
+  for (int e = 0; e < ne; ++e)
+    if (mu[e] > 0.0) op.pinned[e] = op.pinned[e + 1] = 0;
+  for (int k = 0; k < nr; ++k)
+    if (op.pinned[k]) A[(size_t)k * nr + k] = 1.0;
+  if (j == 1) {
+    int ns = 0;
+    std::vector<double> w = rotation_weights(r, mu, ns);
+    bordered_band_factor(op.sys, A, nr, w, ns);
+  } else {
+    bordered_band_factor(op.sys, A, nr, {}, 0);
+  }
+}
+
+// vilma_radial_fe.f90:801-810 toroidal_operator_solve_vec
+void toroidal_operator_solve_vec(const TorOp& op, const double* b, double* x) {
+  std::vector<double> bd(op.nr);
+  for (int k = 0; k < op.nr; ++k) bd[k] = op.pinned[k] ? 0.0 : b[k];
+  bordered_band_solve(op.sys, bd.data(), x, nullptr);
 }
 
 }  // namespace orc

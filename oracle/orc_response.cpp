@@ -111,6 +111,89 @@ static void advance_memory_trap(int ne, const double* mu, const double* Mk, cons
   }
 }
 
+// ------------------------------------------------------------- toroidal kernels
+// vilma_viscoelastic.f90:373-390 strain_coeffs_tor: lam 0 = lambda 3, 1 = lambda 4
+static inline void strain_coeffs_tor(double w1, double w2, double Jr, double a[2], double b[2], double c[2]) {
+  a[0] = -w1 + w2;
+  b[0] = -w1;
+  c[0] = -w2;
+  a[1] = 0.0;
+  b[1] = w1;
+  c[1] = w2;
+  if (Jr <= 2.0) {
+    b[1] = 0.0;
+    c[1] = 0.0;
+  }
+}
+
+// vilma_viscoelastic.f90:392-401 ve_strain_constants_tor
+static void ve_strain_constants_tor(double Jr, double norm[2], double sa[4], double sb[4], double sc[4]) {
+  norm[0] = 0.5 * Jr;
+  norm[1] = 0.5 * Jr * (Jr - 2.0);
+  strain_coeffs_tor(1.0, 0.0, Jr, &sa[0], &sb[0], &sc[0]);
+  strain_coeffs_tor(0.0, 1.0, Jr, &sa[2], &sb[2], &sc[2]);
+}
+
+// vilma_viscoelastic.f90:403-439 dissipative_rhs_tor; A/B/C are (2, ne) [e][lam],
+// f per node
+static void dissipative_rhs_tor(int ne, const double* r, const double* sa, const double* sb, const double* sc,
+                                const double* norm, const double* Am, const double* Bm, const double* Cm,
+                                double* f) {
+  const double xg = 0.5773502691896257;
+  const double gp[2] = {-xg, xg};
+  for (int e = 0; e < ne; ++e) {
+    double rk = r[e], rk1 = r[e + 1], h = rk1 - rk;
+    double floc[2] = {0, 0};
+    for (int ig = 0; ig < 2; ++ig) {
+      double ra = 0.5 * (h * gp[ig] + rk + rk1);
+      double psik = (rk1 - ra) / h, psik1 = (ra - rk) / h;
+      double tauV[2];
+      for (int m = 0; m < 2; ++m)
+        tauV[m] = Am[e * 2 + m] / h + Bm[e * 2 + m] * psik / ra + Cm[e * 2 + m] * psik1 / ra;
+      for (int t = 0; t < 2; ++t) {
+        double D = 0.0;
+        for (int m = 0; m < 2; ++m) {
+          double deps = sa[t * 2 + m] / h + sb[t * 2 + m] * psik / ra + sc[t * 2 + m] * psik1 / ra;
+          D = D + norm[m] * tauV[m] * deps;
+        }
+        floc[t] = floc[t] - D * ra * ra * h * 0.5;
+      }
+    }
+    f[e] += floc[0];
+    f[e + 1] += floc[1];
+  }
+}
+
+// vilma_viscoelastic.f90:591-629 advance_memory_tor with maxwell_fe (:640-654)
+// or, given Wn_prev, maxwell_trap (:683-700)
+static void advance_memory_tor(int ne, const double* mu, const double* Mk, const double* Wn, const double* Wn_prev,
+                               double Jr, double* A, double* B, double* C, const char* active) {
+  for (int e = 0; e < ne; ++e) {
+    if (active && !active[e]) continue;
+    double a[2], b[2], c[2];
+    strain_coeffs_tor(Wn[e], Wn[e + 1], Jr, a, b, c);
+    const double Me = Mk[e];
+    if (Wn_prev) {
+      double ap[2], bp[2], cp[2];
+      strain_coeffs_tor(Wn_prev[e], Wn_prev[e + 1], Jr, ap, bp, cp);
+      const double denom = 1.0 + 0.5 * Me;
+      const double c_old = (1.0 - 0.5 * Me) / denom, w_eps = mu[e] * Me / denom;
+      for (int m = 0; m < 2; ++m) {
+        A[e * 2 + m] = c_old * A[e * 2 + m] - w_eps * (a[m] + ap[m]);
+        B[e * 2 + m] = c_old * B[e * 2 + m] - w_eps * (b[m] + bp[m]);
+        C[e * 2 + m] = c_old * C[e * 2 + m] - w_eps * (c[m] + cp[m]);
+      }
+    } else {
+      const double om = 1.0 - Me, two_muM = 2.0 * mu[e] * Me;
+      for (int m = 0; m < 2; ++m) {
+        A[e * 2 + m] = om * A[e * 2 + m] - two_muM * a[m];
+        B[e * 2 + m] = om * B[e * 2 + m] - two_muM * b[m];
+        C[e * 2 + m] = om * C[e * 2 + m] - two_muM * c[m];
+      }
+    }
+  }
+}
+
 // vilma_response.f90:386-420 response_deg1_to_cm
 static void deg1_to_cm(const RadialOp& op, double* x) {
   if (op.nullmode.empty()) return;
@@ -230,12 +313,21 @@ static double absmax6(int n, const double* x1, const double* x2, const double* x
 // targets (begin_step: dUn, the endpoint pass: edUn) and the surface drift
 // dUa, dFa, dVa (the report drift the sea-level iteration applies)
 static void solve_drift(Response& R, std::vector<double>& dUn_re, std::vector<double>& dUn_im,
-                        std::vector<double>& dVn_re, std::vector<double>& dVn_im) {
-  const int nb = 4 * R.ne, nr = R.nr;
+                        std::vector<double>& dVn_re, std::vector<double>& dVn_im, std::vector<double>* dWn_re,
+                        std::vector<double>* dWn_im) {
+  const int nb = 4 * R.ne, nr = R.nr, nbt = 2 * R.ne;
+  const bool tor = R.nlam > NLAM;
+  if (tor && !(dWn_re && dWn_im))
+    throw std::runtime_error("solve_drift: the toroidal channels are carried, so W targets are required");
 #pragma omp parallel for schedule(static)
   for (int k = 0; k < R.nk; ++k) {
     size_t o = (size_t)k * nb;
     R.mnorm[k] = absmax6(nb, &R.Are[o], &R.Bre[o], &R.Cre[o], &R.Aim[o], &R.Bim[o], &R.Cim[o]);
+    if (tor) {  // the (nlam, ne) slot block scanned flat includes lambda 3, 4
+      size_t ot = (size_t)k * nbt;
+      R.mnorm[k] = std::max(R.mnorm[k], absmax6(nbt, &R.Atre[ot], &R.Btre[ot], &R.Ctre[ot], &R.Atim[ot],
+                                                &R.Btim[ot], &R.Ctim[ot]));
+    }
   }
   double mx = 0.0;
   for (int k = 0; k < R.nk; ++k) mx = std::max(mx, R.mnorm[k]);
@@ -244,6 +336,7 @@ static void solve_drift(Response& R, std::vector<double>& dUn_re, std::vector<do
 #pragma omp parallel reduction(+ : solved)
   {
     std::vector<double> fre(R.ndof), fim(R.ndof), xre(R.ndof), xim(R.ndof);
+    std::vector<double> gre(nr), gim(nr), wre(nr), wim(nr);
 #pragma omp for schedule(dynamic)
     for (int l = 1; l <= R.lmax; ++l) {
       for (int k = R.kbeg[l]; k < R.kbeg[l + 1]; ++k) {
@@ -256,6 +349,13 @@ static void solve_drift(Response& R, std::vector<double>& dUn_re, std::vector<do
             dUn_im[(size_t)k * nr + node] = 0.0;
             dVn_re[(size_t)k * nr + node] = 0.0;
             dVn_im[(size_t)k * nr + node] = 0.0;
+          }
+          if (tor) {
+            R.dWa[k] = 0.0;
+            for (int node = 0; node < nr; ++node) {
+              (*dWn_re)[(size_t)k * nr + node] = 0.0;
+              (*dWn_im)[(size_t)k * nr + node] = 0.0;
+            }
           }
           continue;
         }
@@ -283,6 +383,22 @@ static void solve_drift(Response& R, std::vector<double>& dUn_re, std::vector<do
           dVn_re[(size_t)k * nr + node] = xre[idx_v(node)];
           dVn_im[(size_t)k * nr + node] = xim[idx_v(node)];
         }
+        if (tor) {  // its own forcing, its own operator; no frame projection at l = 1
+          std::fill(gre.begin(), gre.end(), 0.0);
+          std::fill(gim.begin(), gim.end(), 0.0);
+          size_t ot = (size_t)k * nbt;
+          dissipative_rhs_tor(R.ne, R.r.data(), &R.sat[l * 4], &R.sbt[l * 4], &R.sct[l * 4], &R.nrmt[l * 2],
+                              &R.Atre[ot], &R.Btre[ot], &R.Ctre[ot], gre.data());
+          dissipative_rhs_tor(R.ne, R.r.data(), &R.sat[l * 4], &R.sbt[l * 4], &R.sct[l * 4], &R.nrmt[l * 2],
+                              &R.Atim[ot], &R.Btim[ot], &R.Ctim[ot], gim.data());
+          toroidal_operator_solve_vec(R.tops[l], gre.data(), wre.data());
+          toroidal_operator_solve_vec(R.tops[l], gim.data(), wim.data());
+          for (int node = 0; node < nr; ++node) {
+            (*dWn_re)[(size_t)k * nr + node] = wre[node];
+            (*dWn_im)[(size_t)k * nr + node] = wim[node];
+          }
+          R.dWa[k] = cplx(wre[nr - 1], wim[nr - 1]);
+        }
       }
     }
   }
@@ -293,7 +409,10 @@ static void solve_drift(Response& R, std::vector<double>& dUn_re, std::vector<do
 // vilma_response.f90:679-809 ve_response_begin: the drift of the entering memory
 void response_begin_step(Response& R, const Sht& s) {
   (void)s;
-  solve_drift(R, R.dUn_re, R.dUn_im, R.dVn_re, R.dVn_im);
+  if (R.nlam > NLAM)
+    solve_drift(R, R.dUn_re, R.dUn_im, R.dVn_re, R.dVn_im, &R.dWn_re, &R.dWn_im);
+  else
+    solve_drift(R, R.dUn_re, R.dUn_im, R.dVn_re, R.dVn_im, nullptr, nullptr);
 }
 
 // vilma_response.f90:842-864 ve_response_apply
@@ -318,7 +437,7 @@ void response_apply(const Response& R, const Sht& s, const cplx* sigma, cplx* u,
 static void gather_tensor_coeffs(const Response& R, const Sht& s, const cplx* sigma, int e, cplx* cma,
                                  cplx* cmb, cplx* cmc, cplx* cea, cplx* ceb, cplx* cec) {
   const int nlm = s.nlm, nr = R.nr;
-  for (int t = 0; t < 4 * nlm; ++t) cma[t] = cmb[t] = cmc[t] = cea[t] = ceb[t] = cec[t] = 0.0;
+  for (int t = 0; t < R.nlam * nlm; ++t) cma[t] = cmb[t] = cmc[t] = cea[t] = ceb[t] = cec[t] = 0.0;
   for (int k = 0; k < R.nk; ++k) {
     int l = R.kdeg[k], lm = R.k2lm[k];
     double sre = sigma[lm].real(), sim = sigma[lm].imag();
@@ -341,6 +460,22 @@ static void gather_tensor_coeffs(const Response& R, const Sht& s, const cplx* si
       cmb[lam * nlm + lm] = cplx(R.Bre[o + lam], R.Bim[o + lam]);
       cmc[lam * nlm + lm] = cplx(R.Cre[o + lam], R.Cim[o + lam]);
     }
+    if (R.nlam == NLAM) continue;
+    // channels 4, 5: the lambda 3, 4 memory and the strain of the nodal W drift
+    // (no load term: eq 84 does not force W)
+    double at[2], bt[2], ct[2], ati[2], bti[2], cti[2];
+    strain_coeffs_tor(R.dWn_re[kn + e], R.dWn_re[kn + e + 1], R.Jr[l], at, bt, ct);
+    strain_coeffs_tor(R.dWn_im[kn + e], R.dWn_im[kn + e + 1], R.Jr[l], ati, bti, cti);
+    size_t ot = ((size_t)k * R.ne + e) * 2;
+    for (int lam = 0; lam < 2; ++lam) {
+      const size_t c = (size_t)(NLAM + lam) * nlm + lm;
+      cea[c] = cplx(at[lam], ati[lam]);
+      ceb[c] = cplx(bt[lam], bti[lam]);
+      cec[c] = cplx(ct[lam], cti[lam]);
+      cma[c] = cplx(R.Atre[ot + lam], R.Atim[ot + lam]);
+      cmb[c] = cplx(R.Btre[ot + lam], R.Btim[ot + lam]);
+      cmc[c] = cplx(R.Ctre[ot + lam], R.Ctim[ot + lam]);
+    }
   }
 }
 
@@ -349,13 +484,13 @@ static void advance_shape_tensor(const Response& R, const Sht& s, int e, cplx* c
                                  double* dtau, double* deps, cplx* cdel) {
   const size_t ng = (size_t)s.nphi * s.nlat;
   double twoMu = 2.0 * R.mu[e];
-  tensor_synth(s, c, dtau);
-  tensor_synth(s, eps, deps);
+  tensor_synth(s, c, dtau, R.nlam);
+  tensor_synth(s, eps, deps, R.nlam);
   const double* M = &R.Mk3[(size_t)e * ng];
   for (int p = 0; p < 6; ++p)
     for (size_t g = 0; g < ng; ++g) dtau[p * ng + g] = -M[g] * (dtau[p * ng + g] + twoMu * deps[p * ng + g]);
-  tensor_analysis(s, dtau, cdel);
-  for (int t = 0; t < 4 * s.nlm; ++t) c[t] = c[t] + cdel[t];
+  tensor_analysis(s, dtau, cdel, R.nlam);
+  for (int t = 0; t < R.nlam * s.nlm; ++t) c[t] = c[t] + cdel[t];
 }
 
 // vilma_response.f90:1171-1225 advance_memory_3d
@@ -365,8 +500,8 @@ static void advance_memory_3d(Response& R, const Sht& s, const cplx* sigma) {
   const size_t ng = (size_t)s.nphi * s.nlat;
 #pragma omp parallel
   {
-    std::vector<cplx> cma(4 * nlm), cmb(4 * nlm), cmc(4 * nlm), cea(4 * nlm), ceb(4 * nlm),
-        cec(4 * nlm), cdel(4 * nlm);
+    const int nc = R.nlam * nlm;
+    std::vector<cplx> cma(nc), cmb(nc), cmc(nc), cea(nc), ceb(nc), cec(nc), cdel(nc);
     std::vector<double> dtau(6 * ng), deps(6 * ng);
 #pragma omp for schedule(dynamic)
     for (int ei = 0; ei < R.ne3d; ++ei) {
@@ -386,6 +521,17 @@ static void advance_memory_3d(Response& R, const Sht& s, const cplx* sigma) {
           R.Bim[o + lam] = cmb[lam * nlm + lm].imag();
           R.Cre[o + lam] = cmc[lam * nlm + lm].real();
           R.Cim[o + lam] = cmc[lam * nlm + lm].imag();
+        }
+        if (R.nlam == NLAM) continue;
+        size_t ot = ((size_t)k * R.ne + e) * 2;
+        for (int lam = 0; lam < 2; ++lam) {
+          const size_t c = (size_t)(NLAM + lam) * nlm + lm;
+          R.Atre[ot + lam] = cma[c].real();
+          R.Atim[ot + lam] = cma[c].imag();
+          R.Btre[ot + lam] = cmb[c].real();
+          R.Btim[ot + lam] = cmb[c].imag();
+          R.Ctre[ot + lam] = cmc[c].real();
+          R.Ctim[ot + lam] = cmc[c].imag();
         }
       }
     }
@@ -417,6 +563,13 @@ void response_advance(Response& R, const Sht& s, const cplx* sigma) {
                         &R.Cre[o], R.active1d.data());
       advance_memory_fe(R.ne, R.mu.data(), R.Mk.data(), Uim.data(), Vim.data(), R.Jr[l], &R.Aim[o], &R.Bim[o],
                         &R.Cim[o], R.active1d.data());
+      if (R.nlam > NLAM) {  // W is pure drift: no sigma x_Wn term
+        size_t ot = (size_t)k * R.ne * 2;
+        advance_memory_tor(R.ne, R.mu.data(), R.Mk.data(), &R.dWn_re[kn], nullptr, R.Jr[l], &R.Atre[ot],
+                           &R.Btre[ot], &R.Ctre[ot], R.active1d.data());
+        advance_memory_tor(R.ne, R.mu.data(), R.Mk.data(), &R.dWn_im[kn], nullptr, R.Jr[l], &R.Atim[ot],
+                           &R.Btim[ot], &R.Ctim[ot], R.active1d.data());
+      }
     }
   }
   R.n_mem++;
@@ -428,9 +581,10 @@ void response_advance(Response& R, const Sht& s, const cplx* sigma) {
 // of element e as (4, nlm) channel-major blocks
 static void gather_strain_block(const Response& R, const cplx* sigma, const std::vector<double>& dUr,
                                 const std::vector<double>& dUi, const std::vector<double>& dVr,
-                                const std::vector<double>& dVi, int e, cplx* ca, cplx* cb, cplx* cc, int nlm) {
+                                const std::vector<double>& dVi, const std::vector<double>& dWr,
+                                const std::vector<double>& dWi, int e, cplx* ca, cplx* cb, cplx* cc, int nlm) {
   const int nr = R.nr;
-  for (int t = 0; t < 4 * nlm; ++t) ca[t] = cb[t] = cc[t] = 0.0;
+  for (int t = 0; t < R.nlam * nlm; ++t) ca[t] = cb[t] = cc[t] = 0.0;
   for (int k = 0; k < R.nk; ++k) {
     int l = R.kdeg[k], lm = R.k2lm[k];
     double sre = sigma[lm].real(), sim = sigma[lm].imag();
@@ -449,6 +603,16 @@ static void gather_strain_block(const Response& R, const cplx* sigma, const std:
       cb[lam * nlm + lm] = cplx(br[lam], bi[lam]);
       cc[lam * nlm + lm] = cplx(cr[lam], ci[lam]);
     }
+    if (R.nlam == NLAM) continue;
+    double at[2], bt[2], ct[2], ati[2], bti[2], cti[2];
+    strain_coeffs_tor(dWr[kn + e], dWr[kn + e + 1], R.Jr[l], at, bt, ct);
+    strain_coeffs_tor(dWi[kn + e], dWi[kn + e + 1], R.Jr[l], ati, bti, cti);
+    for (int lam = 0; lam < 2; ++lam) {
+      const size_t c = (size_t)(NLAM + lam) * nlm + lm;
+      ca[c] = cplx(at[lam], ati[lam]);
+      cb[c] = cplx(bt[lam], bti[lam]);
+      cc[c] = cplx(ct[lam], cti[lam]);
+    }
   }
 }
 
@@ -457,17 +621,17 @@ static void gather_strain_block(const Response& R, const cplx* sigma, const std:
 static void advance_shape_tensor_trap(const Response& R, const Sht& s, int e, cplx* c0, const cplx* eps_n,
                                       const cplx* eps_1, double* dt0, double* den, double* de1, cplx* cdel) {
   const size_t ng = (size_t)s.nphi * s.nlat;
-  tensor_synth(s, c0, dt0);
-  tensor_synth(s, eps_n, den);
-  tensor_synth(s, eps_1, de1);
+  tensor_synth(s, c0, dt0, R.nlam);
+  tensor_synth(s, eps_n, den, R.nlam);
+  tensor_synth(s, eps_1, de1, R.nlam);
   const double* M = &R.Mk3[(size_t)e * ng];
   for (size_t g = 0; g < ng; ++g) {
     const double wtau = M[g] / (1.0 + 0.5 * M[g]), weps = R.mu[e] * M[g] / (1.0 + 0.5 * M[g]);
     for (int p = 0; p < 6; ++p)
       dt0[p * ng + g] = -wtau * dt0[p * ng + g] - weps * (den[p * ng + g] + de1[p * ng + g]);
   }
-  tensor_analysis(s, dt0, cdel);
-  for (int t = 0; t < 4 * s.nlm; ++t) c0[t] = c0[t] + cdel[t];
+  tensor_analysis(s, dt0, cdel, R.nlam);
+  for (int t = 0; t < R.nlam * s.nlm; ++t) c0[t] = c0[t] + cdel[t];
 }
 
 // vilma_response.f90:1321-1369 advance_memory_3d_trap
@@ -478,13 +642,14 @@ static void advance_memory_3d_trap(Response& R, const Sht& s, const cplx* sigma)
   const cplx* sig_n = R.sigma_primed ? R.sigma_n.data() : sigma;  // first step: sigma_{n+1} (:1398-1403)
 #pragma omp parallel
   {
+    const int nc = R.nlam * nlm;
     std::vector<cplx> c0[3], cn[3], c1[3];
     for (int q = 0; q < 3; ++q) {
-      c0[q].assign(4 * nlm, 0.0);
-      cn[q].assign(4 * nlm, 0.0);
-      c1[q].assign(4 * nlm, 0.0);
+      c0[q].assign(nc, 0.0);
+      cn[q].assign(nc, 0.0);
+      c1[q].assign(nc, 0.0);
     }
-    std::vector<cplx> cdel(4 * nlm);
+    std::vector<cplx> cdel(nc);
     std::vector<double> dt0(6 * ng), den(6 * ng), de1(6 * ng);
 #pragma omp for schedule(dynamic)
     for (int ei = 0; ei < R.ne3d; ++ei) {
@@ -498,11 +663,19 @@ static void advance_memory_3d_trap(Response& R, const Sht& s, const cplx* sigma)
           c0[1][lam * nlm + lm] = cplx(R.Bre0[o + lam], R.Bim0[o + lam]);
           c0[2][lam * nlm + lm] = cplx(R.Cre0[o + lam], R.Cim0[o + lam]);
         }
+        if (R.nlam == NLAM) continue;
+        const size_t ot = ((size_t)k * R.ne + e) * 2;
+        for (int lam = 0; lam < 2; ++lam) {
+          const size_t c = (size_t)(NLAM + lam) * nlm + lm;
+          c0[0][c] = cplx(R.Atre0[ot + lam], R.Atim0[ot + lam]);
+          c0[1][c] = cplx(R.Btre0[ot + lam], R.Btim0[ot + lam]);
+          c0[2][c] = cplx(R.Ctre0[ot + lam], R.Ctim0[ot + lam]);
+        }
       }
-      gather_strain_block(R, sig_n, R.dUn_re, R.dUn_im, R.dVn_re, R.dVn_im, e, cn[0].data(), cn[1].data(),
-                          cn[2].data(), nlm);
-      gather_strain_block(R, sigma, R.edUn_re, R.edUn_im, R.edVn_re, R.edVn_im, e, c1[0].data(), c1[1].data(),
-                          c1[2].data(), nlm);
+      gather_strain_block(R, sig_n, R.dUn_re, R.dUn_im, R.dVn_re, R.dVn_im, R.dWn_re, R.dWn_im, e, cn[0].data(),
+                          cn[1].data(), cn[2].data(), nlm);
+      gather_strain_block(R, sigma, R.edUn_re, R.edUn_im, R.edVn_re, R.edVn_im, R.edWn_re, R.edWn_im, e,
+                          c1[0].data(), c1[1].data(), c1[2].data(), nlm);
       for (int q = 0; q < 3; ++q)
         advance_shape_tensor_trap(R, s, e, c0[q].data(), cn[q].data(), c1[q].data(), dt0.data(), den.data(),
                                   de1.data(), cdel.data());
@@ -516,6 +689,17 @@ static void advance_memory_3d_trap(Response& R, const Sht& s, const cplx* sigma)
           R.Bim[o + lam] = c0[1][lam * nlm + lm].imag();
           R.Cre[o + lam] = c0[2][lam * nlm + lm].real();
           R.Cim[o + lam] = c0[2][lam * nlm + lm].imag();
+        }
+        if (R.nlam == NLAM) continue;
+        const size_t ot = ((size_t)k * R.ne + e) * 2;
+        for (int lam = 0; lam < 2; ++lam) {
+          const size_t c = (size_t)(NLAM + lam) * nlm + lm;
+          R.Atre[ot + lam] = c0[0][c].real();
+          R.Atim[ot + lam] = c0[0][c].imag();
+          R.Btre[ot + lam] = c0[1][c].real();
+          R.Btim[ot + lam] = c0[1][c].imag();
+          R.Ctre[ot + lam] = c0[2][c].real();
+          R.Ctim[ot + lam] = c0[2][c].imag();
         }
       }
     }
@@ -559,6 +743,19 @@ static void trapezoid_advance_all(Response& R, const Sht& s, const cplx* sigma) 
                           &R.Are[o], &R.Bre[o], &R.Cre[o], R.active1d.data());
       advance_memory_trap(R.ne, R.mu.data(), R.Mk.data(), Uim.data(), Vim.data(), Uin.data(), Vin.data(), R.Jr[l],
                           &R.Aim[o], &R.Bim[o], &R.Cim[o], R.active1d.data());
+      if (R.nlam > NLAM) {  // W: eps_n from tau_n's drift, eps_{n+1} from the endpoint's
+        const size_t ot = (size_t)k * R.ne * 2, n2 = (size_t)R.ne * 2;
+        std::copy(&R.Atre0[ot], &R.Atre0[ot] + n2, &R.Atre[ot]);
+        std::copy(&R.Btre0[ot], &R.Btre0[ot] + n2, &R.Btre[ot]);
+        std::copy(&R.Ctre0[ot], &R.Ctre0[ot] + n2, &R.Ctre[ot]);
+        std::copy(&R.Atim0[ot], &R.Atim0[ot] + n2, &R.Atim[ot]);
+        std::copy(&R.Btim0[ot], &R.Btim0[ot] + n2, &R.Btim[ot]);
+        std::copy(&R.Ctim0[ot], &R.Ctim0[ot] + n2, &R.Ctim[ot]);
+        advance_memory_tor(R.ne, R.mu.data(), R.Mk.data(), &R.edWn_re[kn], &R.dWn_re[kn], R.Jr[l], &R.Atre[ot],
+                           &R.Btre[ot], &R.Ctre[ot], R.active1d.data());
+        advance_memory_tor(R.ne, R.mu.data(), R.Mk.data(), &R.edWn_im[kn], &R.dWn_im[kn], R.Jr[l], &R.Atim[ot],
+                           &R.Btim[ot], &R.Ctim[ot], R.active1d.data());
+      }
     }
   }
   if (R.lat_visc) advance_memory_3d_trap(R, s, sigma);
@@ -581,6 +778,17 @@ void response_prepare_endpoint(Response& R) {
   R.edVn_re = R.dVn_re;
   R.edVn_im = R.dVn_im;
   R.dUa_prev = R.dUa;  // keep_drift (:1492-1497)
+  if (R.nlam > NLAM) {
+    R.Atre0 = R.Atre;
+    R.Atim0 = R.Atim;
+    R.Btre0 = R.Btre;
+    R.Btim0 = R.Btim;
+    R.Ctre0 = R.Ctre;
+    R.Ctim0 = R.Ctim;
+    R.edWn_re = R.dWn_re;
+    R.edWn_im = R.dWn_im;
+    R.dWa_prev = R.dWa;
+  }
 }
 
 // vilma_response.f90:1618-1646 ve_response_advance_endpoint
@@ -593,14 +801,22 @@ void response_advance_endpoint(Response& R, const Sht& s, const cplx* sigma) {
   }
   trapezoid_advance_all(R, s, sigma);
   R.sigma_next.assign(sigma, sigma + R.nlm);
-  solve_drift(R, R.edUn_re, R.edUn_im, R.edVn_re, R.edVn_im);  // solve_endpoint_drift (:1480-1490)
+  const bool tor = R.nlam > NLAM;
+  solve_drift(R, R.edUn_re, R.edUn_im, R.edVn_re, R.edVn_im, tor ? &R.edWn_re : nullptr,
+              tor ? &R.edWn_im : nullptr);  // solve_endpoint_drift (:1480-1490)
   R.couple_pass++;
   double cnorm = 0.0, snorm = 0.0;  // drift_change (:1499-1512)
   for (int k = 0; k < R.nk; ++k) {
     cnorm = std::max(cnorm, std::abs(R.dUa[k] - R.dUa_prev[k]));
     snorm = std::max(snorm, std::abs(R.dUa[k]));
   }
+  if (tor)
+    for (int k = 0; k < R.nk; ++k) {
+      cnorm = std::max(cnorm, std::abs(R.dWa[k] - R.dWa_prev[k]));
+      snorm = std::max(snorm, std::abs(R.dWa[k]));
+    }
   R.dUa_prev = R.dUa;
+  if (tor) R.dWa_prev = R.dWa;
   R.couple_done = (R.couple_pass >= 2 && cnorm <= R.couple_tol * std::max(snorm, 2.2250738585072014e-308));
 }
 
@@ -634,6 +850,14 @@ void response_save_state(Response& R) {
   R.time_s = R.time;
   R.sigma_n_s = R.sigma_n;
   R.sigma_primed_s = R.sigma_primed;
+  if (R.nlam > NLAM) {
+    R.Atre_s = R.Atre;
+    R.Atim_s = R.Atim;
+    R.Btre_s = R.Btre;
+    R.Btim_s = R.Btim;
+    R.Ctre_s = R.Ctre;
+    R.Ctim_s = R.Ctim;
+  }
 }
 void response_restore_state(Response& R) {
   R.Are = R.Are_s;
@@ -645,6 +869,14 @@ void response_restore_state(Response& R) {
   R.time = R.time_s;
   R.sigma_n = R.sigma_n_s;
   R.sigma_primed = R.sigma_primed_s;
+  if (R.nlam > NLAM) {
+    R.Atre = R.Atre_s;
+    R.Atim = R.Atim_s;
+    R.Btre = R.Btre_s;
+    R.Btim = R.Btim_s;
+    R.Ctre = R.Ctre_s;
+    R.Ctim = R.Ctim_s;
+  }
 }
 
 // vilma_response.f90:1742-1758 response_stash_coarse
@@ -655,6 +887,14 @@ void response_stash_coarse(Response& R) {
   R.Bim_c = R.Bim;
   R.Cre_c = R.Cre;
   R.Cim_c = R.Cim;
+  if (R.nlam > NLAM) {
+    R.Atre_c = R.Atre;
+    R.Atim_c = R.Atim;
+    R.Btre_c = R.Btre;
+    R.Btim_c = R.Btim;
+    R.Ctre_c = R.Ctre;
+    R.Ctim_c = R.Ctim;
+  }
 }
 
 // vilma_response.f90:1760-1781 response_coarse_fine_error: max |tau_fine - tau_coarse|, max |tau_fine|
@@ -667,6 +907,14 @@ void response_coarse_fine_error(const Response& R, double& err_inf, double& tau_
     for (size_t i = 0; i < f[q]->size(); ++i) {
       err_inf = std::max(err_inf, std::fabs((*f[q])[i] - (*c[q])[i]));
       tau_inf = std::max(tau_inf, std::fabs((*f[q])[i]));
+    }
+  if (R.nlam == NLAM) return;
+  const std::vector<double>* ft[6] = {&R.Atre, &R.Atim, &R.Btre, &R.Btim, &R.Ctre, &R.Ctim};
+  const std::vector<double>* ct[6] = {&R.Atre_c, &R.Atim_c, &R.Btre_c, &R.Btim_c, &R.Ctre_c, &R.Ctim_c};
+  for (int q = 0; q < 6; ++q)
+    for (size_t i = 0; i < ft[q]->size(); ++i) {
+      err_inf = std::max(err_inf, std::fabs((*ft[q])[i] - (*ct[q])[i]));
+      tau_inf = std::max(tau_inf, std::fabs((*ft[q])[i]));
     }
 }
 
@@ -695,6 +943,13 @@ double response_memory_norm(const Response& R) {
   for (int k = 0; k < R.nk; ++k) {
     size_t o = (size_t)k * nb;
     nrm = std::max(nrm, absmax6(nb, &R.Are[o], &R.Aim[o], &R.Bre[o], &R.Bim[o], &R.Cre[o], &R.Cim[o]));
+  }
+  if (R.nlam > NLAM) {
+    const int nbt = 2 * R.ne;
+    for (int k = 0; k < R.nk; ++k) {
+      size_t o = (size_t)k * nbt;
+      nrm = std::max(nrm, absmax6(nbt, &R.Atre[o], &R.Atim[o], &R.Btre[o], &R.Btim[o], &R.Ctre[o], &R.Ctim[o]));
+    }
   }
   return nrm;
 }
@@ -731,6 +986,35 @@ void response_enable_lateral_visc(Response& R, const Sht& s, const double* pert)
     if (!R.active1d[e]) R.e3d.push_back(e);
   R.ne3d = (int)R.e3d.size();
   R.lat_visc = true;
+  // a genuinely 3-D element couples spheroidal and toroidal (:1048-1052)
+  if (R.toroidal && R.ne3d > 0 && R.nlam == NLAM) response_enable_toroidal(R);
+}
+
+// vilma_response.f90:1055-1118 enable_toroidal: per-degree W operators and
+// constants, the W drift arrays and the toroidal memory, zero
+void response_enable_toroidal(Response& R) {
+  R.tops.assign(R.lmax + 1, TorOp());
+  R.nrmt.assign((size_t)(R.lmax + 1) * 2, 0.0);
+  R.sat.assign((size_t)(R.lmax + 1) * 4, 0.0);
+  R.sbt = R.sat;
+  R.sct = R.sat;
+  for (int l = 1; l <= R.lmax; ++l) {
+    toroidal_operator_assemble(R.tops[l], R.r, R.mu, l);
+    ve_strain_constants_tor(R.Jr[l], &R.nrmt[l * 2], &R.sat[l * 4], &R.sbt[l * 4], &R.sct[l * 4]);
+  }
+  R.dWa.assign(R.nk, 0.0);
+  R.dWa_prev = R.dWa;
+  R.dWn_re.assign((size_t)R.nk * R.nr, 0.0);
+  R.dWn_im = R.dWn_re;
+  R.edWn_re = R.dWn_re;
+  R.edWn_im = R.dWn_re;
+  R.Atre.assign((size_t)R.nk * R.ne * 2, 0.0);
+  R.Atim = R.Atre;
+  R.Btre = R.Atre;
+  R.Btim = R.Atre;
+  R.Ctre = R.Atre;
+  R.Ctim = R.Atre;
+  R.nlam = NLAM + NLAM_TOR;
 }
 
 }  // namespace orc

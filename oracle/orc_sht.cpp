@@ -170,25 +170,33 @@ void sht_init(Sht& s, int lmax, int nlat, int nphi) {
   s.n6.clear();
 }
 
-// vilma_tensor_sh.f90:99-133: per-degree spin-2 norm, a unit Z6 coefficient at
-// the sectoral order m = l sent through the synthesis and its adjoint.
+// vilma_tensor_sh.f90:99-133: per-degree spin-2 norms, a unit Z6 (and Z4)
+// coefficient at the sectoral order m = l sent through the synthesis and its
+// adjoint.
 void sht_calibrate_n6(Sht& s) {
   if (!s.n6.empty()) return;
-  std::vector<double> n6(s.lmax + 1, 0.0);
-  s.n6.assign(s.lmax + 1, 1.0);  // provisional unit norm: analysis returns the raw adjoint
-  std::vector<cplx> c4((size_t)4 * s.nlm, 0.0), craw((size_t)4 * s.nlm);
+  std::vector<double> n6(s.lmax + 1, 0.0), n4(s.lmax + 1, 0.0);
+  s.n6.assign(s.lmax + 1, 1.0);  // provisional unit norms: analysis returns the raw adjoints
+  s.n4.assign(s.lmax + 1, 1.0);
+  std::vector<cplx> c6((size_t)6 * s.nlm, 0.0), craw((size_t)6 * s.nlm);
   std::vector<double> dy((size_t)6 * s.nlat * s.nphi);
   for (int l = 2; l <= s.lmax; ++l) {
     int m = std::min(l, s.mmax);
     if (m < 1) continue;
     int lm = s.lmidx(l, m);
-    std::fill(c4.begin(), c4.end(), cplx(0.0));
-    c4[(size_t)3 * s.nlm + lm] = 1.0;
-    tensor_synth(s, c4.data(), dy.data());
-    tensor_analysis(s, dy.data(), craw.data());
+    std::fill(c6.begin(), c6.end(), cplx(0.0));
+    c6[(size_t)3 * s.nlm + lm] = 1.0;
+    tensor_synth(s, c6.data(), dy.data(), 6);
+    tensor_analysis(s, dy.data(), craw.data(), 6);
     n6[l] = craw[(size_t)3 * s.nlm + lm].real();
+    std::fill(c6.begin(), c6.end(), cplx(0.0));
+    c6[(size_t)5 * s.nlm + lm] = 1.0;  // the same coefficient as Z4
+    tensor_synth(s, c6.data(), dy.data(), 6);
+    tensor_analysis(s, dy.data(), craw.data(), 6);
+    n4[l] = craw[(size_t)5 * s.nlm + lm].real();
   }
   s.n6 = n6;
+  s.n4 = n4;
 }
 
 // vilma_sht.f90:184-202
@@ -300,6 +308,43 @@ void sht_sph_analysis(const Sht& s, const double* vt, const double* vp, cplx* sl
     }
 }
 
+// vilma_sht.f90:258-277 tor_synthesis: e_r x grad_1 T = (-F, E) with
+// (E, F) = (d/dtheta, (1/sin) d/dphi) of sum T_lm Y_lm
+void sht_tor_synth(const Sht& s, const cplx* tl, double* vt, double* vp) {
+  const size_t ng = (size_t)s.nphi * s.nlat;
+  std::vector<double> E(ng), F(ng);
+  sht_sph_synth(s, tl, E.data(), F.data());
+  for (size_t p = 0; p < ng; ++p) {
+    vt[p] = -F[p];
+    vp[p] = E[p];
+  }
+}
+
+// toroidal part of spat_to_SHsphtor in this orientation (vilma_sht.f90:294-308):
+// T_lm = (1/l(l+1)) <v, e_r x grad Y_lm> (quadrature)
+void sht_tor_analysis(const Sht& s, const double* vt, const double* vp, cplx* tl) {
+  std::vector<cplx> Ft, Fp;
+  fourier_analysis(s, vt, Ft);
+  fourier_analysis(s, vp, Fp);
+  const int nl = s.nlat;
+#pragma omp parallel for schedule(dynamic)
+  for (int m = 0; m <= s.mmax; ++m)
+    for (int l = m; l <= s.lmax; ++l) {
+      int lm = s.lmidx(l, m);
+      if (l == 0) {
+        tl[lm] = 0.0;
+        continue;
+      }
+      const double* t = &s.plm[(size_t)lm * nl];
+      const double* d = &s.dplm[(size_t)lm * nl];
+      cplx acc = 0.0;
+      for (int j = 0; j < nl; ++j)
+        acc += s.wts[j] * (cplx(0.0, (double)m * s.invsin[j]) * t[j] * Ft[(size_t)m * nl + j] +
+                           d[j] * Fp[(size_t)m * nl + j]);
+      tl[lm] = acc / ((double)l * (double)(l + 1));
+    }
+}
+
 // ------------------------------------------------------------- tensor SH
 static void byprof(const Sht& s, const double* f, const std::vector<double>& prof, double* out) {
   for (int j = 0; j < s.nlat; ++j)
@@ -326,8 +371,9 @@ static void spin2_fields(const Sht& s, const cplx* c6, double* sg, double* sh) {
     }
 }
 
-// vilma_tensor_sh.f90:168-203 tensor_sh_synth (spheroidal channels only)
-void tensor_synth(const Sht& s, const cplx* c, double* dyad) {
+// vilma_tensor_sh.f90:168-203 tensor_sh_synth, with spin2_synth_tor (:231-242)
+// for the toroidal channels
+void tensor_synth(const Sht& s, const cplx* c, double* dyad, int nch) {
   const size_t ng = (size_t)s.nphi * s.nlat;
   const int nlm = s.nlm;
   double* rr = dyad;
@@ -348,10 +394,23 @@ void tensor_synth(const Sht& s, const cplx* c, double* dyad) {
     pp[p] = tr[p] - sg[p];
     tp[p] = 4.0 * sh[p];
   }
+  if (nch == 4) return;
+  // Z3: (rt, rp) += e_r x grad_1 c5; Z4 = G e_tp - H (e_tt - e_pp): (-Sh, +Sh, Sg)
+  std::vector<double> vt(ng), vp(ng);
+  sht_tor_synth(s, c + 4 * nlm, vt.data(), vp.data());
+  spin2_fields(s, c + 5 * nlm, sg.data(), sh.data());
+  for (size_t p = 0; p < ng; ++p) {
+    rt[p] += vt[p];
+    rp[p] += vp[p];
+    tt[p] -= sh[p];
+    pp[p] += sh[p];
+    tp[p] += sg[p];
+  }
 }
 
-// vilma_tensor_sh.f90:270-358 tensor_sh_analysis + spin2_adjoint
-void tensor_analysis(const Sht& s, const double* dyad, cplx* c) {
+// vilma_tensor_sh.f90:270-358 tensor_sh_analysis + spin2_adjoint, with
+// spin2_adjoint_tor (:360-387) for the toroidal channels
+void tensor_analysis(const Sht& s, const double* dyad, cplx* c, int nch) {
   const size_t ng = (size_t)s.nphi * s.nlat;
   const int nlm = s.nlm;
   const double* rr = dyad;
@@ -387,6 +446,27 @@ void tensor_analysis(const Sht& s, const double* dyad, cplx* c) {
   for (int lm = 0; lm < nlm; ++lm) {
     double n6 = s.n6[s.ldeg[lm]];
     c[3 * nlm + lm] = n6 != 0.0 ? craw[lm] / n6 : cplx(0.0);
+  }
+  if (nch == 4) return;
+  sht_tor_analysis(s, rt, rp, c + 4 * nlm);
+  // Z4 numerator: 1/2 Sg*(tp) - Sh*(tt - pp)
+  sht_analysis(s, tp, q.data());
+  for (int lm = 0; lm < nlm; ++lm) craw[lm] = -0.5 * s.llp1[lm] * q[lm];
+  byprof(s, tp, s.cott, vt.data());
+  sht_sph_analysis(s, vt.data(), zero.data(), sv.data());
+  for (int lm = 0; lm < nlm; ++lm) craw[lm] -= s.llp1[lm] * sv[lm];
+  byprof(s, tp, s.invsin, vp.data());
+  sht_sph_analysis(s, zero.data(), vp.data(), sv.data());
+  for (int lm = 0; lm < nlm; ++lm) craw[lm] += cplx(0.0, (double)s.mord[lm]) * s.llp1[lm] * sv[lm];
+  byprof(s, D.data(), s.invsin, vt.data());
+  sht_sph_analysis(s, vt.data(), zero.data(), sv.data());
+  for (int lm = 0; lm < nlm; ++lm) craw[lm] += cplx(0.0, (double)s.mord[lm]) * s.llp1[lm] * sv[lm];
+  byprof(s, D.data(), s.cott, vp.data());
+  sht_sph_analysis(s, zero.data(), vp.data(), sv.data());
+  for (int lm = 0; lm < nlm; ++lm) craw[lm] += s.llp1[lm] * sv[lm];
+  for (int lm = 0; lm < nlm; ++lm) {
+    double n4 = s.n4.empty() ? 0.0 : s.n4[s.ldeg[lm]];
+    c[5 * nlm + lm] = n4 != 0.0 ? craw[lm] / n4 : cplx(0.0);
   }
 }
 
