@@ -776,6 +776,7 @@ extern "C" int vg_misfit(vg_handle* h, int nsteps, double dt_s, const double* si
   if (!h) return 1;
   try {
     if (!sigma_lm || !obs || !J) throw vg::Error("vg_misfit: null argument");
+    if (h->tor_on) throw vg::Error("vg_misfit: the misfit runs carry no toroidal channels (toroidal = 0)");
     *J = vg::misfit_dev(h, nsteps, dt_s, sigma_lm, nsite, site, obs);
     return 0;
   } catch (const std::exception& ex) {
@@ -790,6 +791,7 @@ extern "C" int vg_misfit_grad(vg_handle* h, int nsteps, double dt_s, const doubl
   if (!h) return 1;
   try {
     if (!sigma_lm || !obs || !J) throw vg::Error("vg_misfit_grad: null argument");
+    if (h->tor_on) throw vg::Error("vg_misfit_grad: the toroidal channels are not differentiated (toroidal = 0)");
     *J = vg::misfit_grad_dev(h, nsteps, dt_s, sigma_lm, nsite, site, obs, ckpt_every, grad_sigma, grad_pert);
     return 0;
   } catch (const std::exception& ex) {

@@ -374,6 +374,66 @@ int vg_get_state(vg_handle* h, double* Are, double* Aim, double* Bre, double* Bi
   });
 }
 
+int vg_get_toroidal(vg_handle* h, double* t_lm) {
+  return guarded(h, [&] {
+    need(h, t_lm != nullptr, "vg_get_toroidal: null argument");
+    const int nlm = h->grid.nlm, nk = h->nk;
+    for (int i = 0; i < 2 * nlm; ++i) t_lm[i] = 0.0;
+    if (!h->tor_on) return;
+    std::vector<double> w((size_t)2 * nk);
+    h->d_dWa.download(w.data(), w.size(), h->stream);
+    VG_CUDA(cudaStreamSynchronize(h->stream));
+    for (int k = 0; k < nk; ++k) {
+      t_lm[2 * h->k2lm_h[k]] = w[k];
+      t_lm[2 * h->k2lm_h[k] + 1] = w[(size_t)nk + k];
+    }
+  });
+}
+
+// toroidal restart layout (NLAM_TOR, ne, nk) <-> device [s][ri][e][lam][k]
+int vg_get_state_tor(vg_handle* h, double* Are, double* Aim, double* Bre, double* Bim, double* Cre, double* Cim,
+                     int* carried) {
+  return guarded(h, [&] {
+    need(h, carried != nullptr, "vg_get_state_tor: null argument");
+    *carried = h->tor_on ? 1 : 0;
+    if (!h->tor_on) return;
+    const int ne = h->ne, nk = h->nk;
+    const size_t per = (size_t)ne * 2 * nk;
+    std::vector<double> m(6 * per);
+    h->d_tmem[h->cur].download(m.data(), m.size(), h->stream);
+    VG_CUDA(cudaStreamSynchronize(h->stream));
+    double* outs[6] = {Are, Aim, Bre, Bim, Cre, Cim};
+    for (int q = 0; q < 6; ++q) {
+      if (!outs[q]) continue;
+      const double* src = m.data() + q * per;
+      for (int e = 0; e < ne; ++e)
+        for (int lam = 0; lam < 2; ++lam)
+          for (int k = 0; k < nk; ++k) outs[q][((size_t)k * ne + e) * 2 + lam] = src[((size_t)e * 2 + lam) * nk + k];
+    }
+  });
+}
+
+int vg_set_state_tor(vg_handle* h, const double* Are, const double* Aim, const double* Bre, const double* Bim,
+                     const double* Cre, const double* Cim) {
+  return guarded(h, [&] {
+    need(h, h->tor_on, "vg_set_state_tor: the toroidal channels are not carried by this handle");
+    const int ne = h->ne, nk = h->nk;
+    const size_t per = (size_t)ne * 2 * nk;
+    std::vector<double> m(6 * per);
+    const double* ins[6] = {Are, Aim, Bre, Bim, Cre, Cim};
+    for (int q = 0; q < 6; ++q) {
+      need(h, ins[q] != nullptr, "vg_set_state_tor: all six memory arrays are required");
+      double* dst = m.data() + q * per;
+      for (int e = 0; e < ne; ++e)
+        for (int lam = 0; lam < 2; ++lam)
+          for (int k = 0; k < nk; ++k) dst[((size_t)e * 2 + lam) * nk + k] = ins[q][((size_t)k * ne + e) * 2 + lam];
+    }
+    h->d_tmem[h->cur].upload(m.data(), m.size(), h->stream);
+    vg::compute_mem_norm(h, h->cur);
+    h->mem_norm = vg::read_mem_norm(h, h->cur);
+  });
+}
+
 int vg_get_step_state(vg_handle* h, double* dt_try_yr, double* sigma_n, int* sigma_primed) {
   return guarded(h, [&] {
     if (dt_try_yr) *dt_try_yr = h->dt_try / vg::SEC_PER_YEAR;

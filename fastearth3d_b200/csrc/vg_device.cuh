@@ -9,6 +9,27 @@ __device__ __forceinline__ size_t mem_idx(int s, int ri, int e, int lam, int k, 
   return ((size_t)((s * 2 + ri) * ne + e) * 4 + lam) * nk + k;
 }
 
+// index of toroidal memory element (s, ri, e, lam, k), lam 0 = lambda 3, 1 = lambda 4
+__device__ __forceinline__ size_t tmem_idx(int s, int ri, int e, int lam, int k, int ne, int nk) {
+  return ((size_t)((s * 2 + ri) * ne + e) * 2 + lam) * nk + k;
+}
+
+// src/vilma_viscoelastic.f90:373-390 strain_coeffs_tor: element strain (a, b, c)
+// for lam = 3, 4 from nodal W; Z4 has no harmonic below degree 2.
+__device__ __forceinline__ void strain_coeffs_tor(double w1, double w2, double Jr, double a[2], double b[2],
+                                                  double c[2]) {
+  a[0] = -w1 + w2;
+  b[0] = -w1;
+  c[0] = -w2;
+  a[1] = 0.0;
+  b[1] = w1;
+  c[1] = w2;
+  if (Jr <= 2.0) {
+    b[1] = 0.0;
+    c[1] = 0.0;
+  }
+}
+
 // max that propagates NaN, so a non-finite state never hides from the guard
 __device__ __forceinline__ double nanmax(double a, double b) { return (a != a || b != b) ? (a + b) : fmax(a, b); }
 

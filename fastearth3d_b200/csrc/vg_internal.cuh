@@ -168,6 +168,15 @@ struct vg_handle {
   vg::DArr<double> d_v3a_Yb, d_v3a_dyb, d_v3a_Rb;  // 3-D adjoint: product adjoints
   double* v3_gstore = nullptr;  // when set, the FP64 longitude pass also stores its grid there (adjoint sweeps)
   vg::DArr<double> d_lon_tw, d_lon_twt;  // FP64 longitude pass: dense twiddle tables (by order, by longitude)
+  // toroidal degree of freedom (p.toroidal and a genuinely 3-D element;
+  // vg_toroidal.cu): memory tmem[buf][((s*2 + ri)*ne + e)*2 + lam][k] with
+  // lam 0 = lambda 3, 1 = lambda 4, double-buffered with d_mem (same `cur`)
+  bool tor_on = false;
+  vg::DArr<double> d_tmem[2];
+  vg::DArr<double> d_dWn, d_dWa;           // nodal W drift [ri][node][k], surface W(a) [ri][k]
+  vg::DArr<double> d_tw, d_tib, d_tc;      // W operators l >= 2: Thomas multipliers, 1/pivots, super-diagonal (l, nr)
+  vg::DArr<double> d_tG1;                  // degree 1: W = G1W g (nr x nr, bordered solve folded in)
+  vg::DArr<double> d_edWn, d_dW_avg, d_dWa_prev, d_tmem_s, d_tmem_c;  // trapezoidal scheme
   // trapezoidal scheme (scheme = VG_SCHEME_TRAP; vg_trap.cu)
   vg::DArr<double> d_edUn, d_edVn;      // endpoint nodal drift (2 nr nk each)
   vg::DArr<double> d_dU_avg, d_dV_avg;  // mean of the entering and endpoint nodal drift
@@ -232,12 +241,12 @@ void build_grid(Grid& G, int lmax, int nlat, int nphi, cudaStream_t s);
 // response kernels (vg_radial.cu)
 // drift of memory buffer buf (-1: the current one) into the nodal targets
 // (nullptr: the handle's dUn, dVn) and the surface drift
-void launch_drift(vg_handle* h, int buf = -1, double* dUn = nullptr, double* dVn = nullptr);
+void launch_drift(vg_handle* h, int buf = -1, double* dUn = nullptr, double* dVn = nullptr, double* dWn = nullptr);
 // 1-D memory advance, current buffer -> the other one, with the strain of
 // (sigma, dUn, dVn) (nullptr: the handle's drift); trap: the trapezoidal rule
 // with sigma, dUn, dVn the means of the step's two ends
 void launch_advance_1d(vg_handle* h, const double* d_sigma, double dt, const double* dUn = nullptr,
-                       const double* dVn = nullptr, bool trap = false);
+                       const double* dVn = nullptr, bool trap = false, const double* dWn = nullptr);
 void launch_apply(vg_handle* h, const double* d_sigma, double* d_u, double* d_n);
 void compute_mem_norm(vg_handle* h, int buf);
 double read_mem_norm(vg_handle* h, int buf);
@@ -257,7 +266,7 @@ void visc3d_enable(vg_handle* h, const double* pert_host);
 // 3-D memory advance (current buffer -> the other one); dUn, dVn and trap as
 // for launch_advance_1d (the pointwise factor M / (1 + M/2) when trap)
 void visc3d_advance(vg_handle* h, const double* d_sigma, double dt, const double* dUn = nullptr,
-                    const double* dVn = nullptr, bool trap = false);
+                    const double* dVn = nullptr, bool trap = false, const double* dWn = nullptr);
 // transposed 3-D advance (FP64 path) of one step whose longitude-pass grid the
 // forward stored in gstore: lam_new (3-D entries) = lam + gather^T, E (3-D
 // elements) = strain adjoints, d J / d (M dt) accumulated into gradMdt
@@ -274,6 +283,20 @@ void rotation_advance(vg_handle* h, const double* d_sigma, double dt);
 void visc3d_tc_enable(vg_handle* h);
 void visc3d_tc_buffers(vg_handle* h, float** X, float** dy);
 void visc3d_tc_run(vg_handle* h, double dt, bool trap = false);
+// toroidal degree of freedom (vg_toroidal.cu; operator assembly in vg_setup.cu)
+void toroidal_tridiag(const std::vector<double>& r, const std::vector<double>& mu, int j, std::vector<double>& diag,
+                      std::vector<double>& off, std::vector<char>& dead);
+std::vector<double> toroidal_rotation_weights(const std::vector<double>& r, const std::vector<double>& mu,
+                                              int& nshell);
+void toroidal_enable(vg_handle* h);
+// W drift of memory buffer buf into dWn (nullptr: the handle's) and d_dWa
+void launch_drift_tor(vg_handle* h, int buf, double* dWn);
+// lambda 3, 4 advance of the spectrally advanced elements (cur -> nxt) from the
+// nodal W drift dWn (the step's mean for trap), folding |toroidal memory| of
+// every element of nxt into the per-slot norms mn
+void launch_advance_1d_tor(vg_handle* h, double dt, const double* dWn, bool trap, double* mn);
+// fold |toroidal memory of buffer buf| into the per-slot norms mn
+void mem_norm_tor(vg_handle* h, int buf, double* mn);
 // trapezoidal scheme (vg_trap.cu)
 void trap_setup(vg_handle* h);
 void trap_prepare(vg_handle* h);

@@ -432,7 +432,7 @@ __global__ void __launch_bounds__(512) k_drift_deg1(DriftArgs A) {
   }
 }
 
-void launch_drift(vg_handle* h, int buf, double* dUn, double* dVn) {
+void launch_drift(vg_handle* h, int buf, double* dUn, double* dVn, double* dWn) {
   PhaseScope ps(h, VG_PH_DRIFT);
   if (buf < 0) buf = h->cur;
   DriftArgs A;
@@ -484,6 +484,7 @@ void launch_drift(vg_handle* h, int buf, double* dUn, double* dVn) {
   k_drift_deg1<<<1, 512, shm, h->stream>>>(A);
   ++h->n_launch;
   VG_CUDA(cudaGetLastError());
+  if (h->tor_on) launch_drift_tor(h, buf, dWn);  // its own forcing, its own operator
 }
 
 // src/vilma_response.f90:842-864 ve_response_apply: u = gu(l) sigma + dUa, N = gn(l) sigma - dFa/g
@@ -595,7 +596,7 @@ __global__ void k_norm_max(const double* __restrict__ mnorm, int nk, unsigned lo
 }
 
 void launch_advance_1d(vg_handle* h, const double* d_sigma, double dt, const double* dUn, const double* dVn,
-                       bool trap) {
+                       bool trap, const double* dWn) {
   PhaseScope ps(h, VG_PH_ADVANCE_1D);
   int nxt = 1 - h->cur;
   double* mn = h->d_mnorm.p + (size_t)nxt * h->nk;
@@ -607,6 +608,7 @@ void launch_advance_1d(vg_handle* h, const double* d_sigma, double dt, const dou
                                                     h->d_mu.p, h->d_MkPerDt.p, h->d_active1d.p, mn, trap ? 1 : 0);
   ++h->n_launch;
   VG_CUDA(cudaGetLastError());
+  if (h->tor_on) launch_advance_1d_tor(h, dt, dWn, trap, mn);  // W is pure drift: no sigma x_Wn term
   k_norm_max<<<1, 1024, 0, h->stream>>>(mn, h->nk, h->d_maxbits.p + nxt);
   ++h->n_launch;
   VG_CUDA(cudaGetLastError());
@@ -625,6 +627,7 @@ void compute_mem_norm(vg_handle* h, int buf) {
   double* mn = h->d_mnorm.p + (size_t)buf * h->nk;
   k_mem_norm<<<(h->nk + 255) / 256, 256, 0, h->stream>>>(h->d_mem[buf].p, h->ne, h->nk, mn);
   VG_CUDA(cudaGetLastError());
+  if (h->tor_on) mem_norm_tor(h, buf, mn);
   k_norm_max<<<1, 1024, 0, h->stream>>>(mn, h->nk, h->d_maxbits.p + buf);
   VG_CUDA(cudaGetLastError());
 }

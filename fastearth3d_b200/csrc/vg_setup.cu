@@ -708,6 +708,63 @@ void build_fluid_deg2_band(vg_handle* h, DArr<double>& ab, DArr<double>& dr, DAr
   if (st) throw Error("rotation_init: fluid-limit degree-2 factorization failed (zero pivot)");
 }
 
+// The toroidal W operator of degree j (src/vilma_radial_fe.f90:699-729),
+// symmetric tridiagonal: per element mu_k { J [I1 - I3(b,a) - I3(a,b) + I6]
+// + J(J-2) I6 } W^a dW^b into diag (nr) and off (nr - 1, row i column i + 1).
+// Nodes all of whose elements have mu = 0 carry no W: their rows and columns
+// stay empty, and dead[i] says so (toroidal_dead_nodes, :731-743).
+void toroidal_tridiag(const std::vector<double>& r, const std::vector<double>& mu, int j, std::vector<double>& diag,
+                      std::vector<double>& off, std::vector<char>& dead) {
+  const int nr = (int)r.size(), ne = (int)mu.size();
+  const double Jr = (double)j * (double)(j + 1);
+  diag.assign(nr, 0.0);
+  off.assign(std::max(nr - 1, 0), 0.0);
+  dead.assign(nr, 1);
+  for (int e = 0; e < ne; ++e) {
+    if (mu[e] == 0.0) continue;
+    dead[e] = dead[e + 1] = 0;
+    Elem E;
+    elem_integrals(r[e], r[e + 1], false, E);
+    double v[2][2];  // [trial a][test b]
+    for (int ia = 0; ia < 2; ++ia)
+      for (int ib = 0; ib < 2; ++ib)
+        v[ia][ib] = mu[e] * (Jr * (E.i1[ia][ib] - E.i3[ib][ia] - E.i3[ia][ib] + E.i6[ia][ib]) +
+                             Jr * (Jr - 2.0) * E.i6[ia][ib]);
+    diag[e] += v[0][0];
+    diag[e + 1] += v[1][1];
+    off[e] += v[1][0];  // row e (test b = 0), column e + 1 (trial a = 1)
+  }
+}
+
+// Degree-1 net-rotation constraints, one column per solid shell (a maximal run
+// of mu > 0 elements): w_s(k) = sum_{e in s} int psi_k r^3 dr
+// (rotation_weights, src/vilma_radial_fe.f90:745-773; elem_k4,
+// src/vilma_radial_integrals.f90:117-126). Column-major (nr, nshell).
+std::vector<double> toroidal_rotation_weights(const std::vector<double>& r, const std::vector<double>& mu,
+                                              int& nshell) {
+  const int nr = (int)r.size(), ne = (int)mu.size();
+  std::vector<int> shell(ne, -1);
+  int ns = 0;
+  bool prev = false;
+  for (int e = 0; e < ne; ++e) {
+    const bool solid = mu[e] > 0.0;
+    if (solid && !prev) ++ns;
+    if (solid) shell[e] = ns - 1;
+    prev = solid;
+  }
+  std::vector<double> w((size_t)nr * ns, 0.0);
+  for (int e = 0; e < ne; ++e) {
+    if (shell[e] < 0) continue;
+    const double rk = r[e], rk1 = r[e + 1], h = rk1 - rk;
+    w[(size_t)shell[e] * nr + e] += h / 20.0 * (rk1 * rk1 * rk1 + 2.0 * rk1 * rk1 * rk + 3.0 * rk1 * rk * rk +
+                                                4.0 * rk * rk * rk);
+    w[(size_t)shell[e] * nr + e + 1] += h / 20.0 * (4.0 * rk1 * rk1 * rk1 + 3.0 * rk1 * rk1 * rk +
+                                                    2.0 * rk1 * rk * rk + rk * rk * rk);
+  }
+  nshell = ns;
+  return w;
+}
+
 void setup_handle(vg_handle* h) {
   const vg_params& p = h->p;
   if (p.scheme != VG_SCHEME_FE && p.scheme != VG_SCHEME_TRAP)

@@ -94,7 +94,18 @@ void trap_prepare(vg_handle* h) {
   d2d(h->d_edUn.p, h->d_dUn.p, nd2, h->stream);
   d2d(h->d_edVn.p, h->d_dVn.p, nd2, h->stream);
   d2d(h->d_dUa_prev.p, h->d_drift.p, (size_t)2 * h->nk, h->stream);  // keep_drift
+  if (h->tor_on) {
+    d2d(h->d_edWn.p, h->d_dWn.p, nd2, h->stream);
+    d2d(h->d_dWa_prev.p, h->d_dWa.p, (size_t)2 * h->nk, h->stream);
+  }
   h->couple_pass = 0;
+}
+
+// mean of the entering and endpoint W drift
+__global__ void k_trap_avg_w(int n, const double* __restrict__ dWn, const double* __restrict__ edWn,
+                             double* __restrict__ dWavg) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t < n) dWavg[t] = 0.5 * (dWn[t] + edWn[t]);
 }
 
 // ve_response_advance_endpoint (src/vilma_response.f90:1618-1646) with the
@@ -108,18 +119,30 @@ bool trap_endpoint_pass(vg_handle* h, double dt) {
                                             h->d_edVn.p, h->d_dV_avg.p);
   ++h->n_launch;
   VG_CUDA(cudaGetLastError());
-  if (h->lat_visc) visc3d_advance(h, h->d_sigma_avg.p, dt, h->d_dU_avg.p, h->d_dV_avg.p, true);
-  launch_advance_1d(h, h->d_sigma_avg.p, dt, h->d_dU_avg.p, h->d_dV_avg.p, true);
+  if (h->tor_on) {
+    k_trap_avg_w<<<(nd2 + 255) / 256, 256, 0, s>>>(nd2, h->d_dWn.p, h->d_edWn.p, h->d_dW_avg.p);
+    ++h->n_launch;
+    VG_CUDA(cudaGetLastError());
+  }
+  const double* dWavg = h->tor_on ? h->d_dW_avg.p : nullptr;
+  if (h->lat_visc) visc3d_advance(h, h->d_sigma_avg.p, dt, h->d_dU_avg.p, h->d_dV_avg.p, true, dWavg);
+  launch_advance_1d(h, h->d_sigma_avg.p, dt, h->d_dU_avg.p, h->d_dV_avg.p, true, dWavg);
   d2d(h->d_sigma_next.p, h->d_sigma.p, (size_t)n2lm, s);
-  launch_drift(h, 1 - h->cur, h->d_edUn.p, h->d_edVn.p);  // solve_endpoint_drift
+  launch_drift(h, 1 - h->cur, h->d_edUn.p, h->d_edVn.p, h->tor_on ? h->d_edWn.p : nullptr);  // solve_endpoint_drift
   ++h->couple_pass;
   VG_CUDA(cudaMemsetAsync(h->d_trap_red.p + 2, 0, 2 * sizeof(unsigned long long), s));
   k_trap_dchange<<<(h->nk + 255) / 256, 256, 0, s>>>(h->nk, h->d_drift.p, h->d_dUa_prev.p, h->d_trap_red.p);
   ++h->n_launch;
   VG_CUDA(cudaGetLastError());
+  if (h->tor_on) {  // W(a) joins U(a) in the convergence signal (drift_change, :1499-1512)
+    k_trap_dchange<<<(h->nk + 255) / 256, 256, 0, s>>>(h->nk, h->d_dWa.p, h->d_dWa_prev.p, h->d_trap_red.p);
+    ++h->n_launch;
+    VG_CUDA(cudaGetLastError());
+  }
   unsigned long long bits[2];
   VG_CUDA(cudaMemcpyAsync(bits, h->d_trap_red.p + 2, sizeof(bits), cudaMemcpyDeviceToHost, s));
   d2d(h->d_dUa_prev.p, h->d_drift.p, (size_t)2 * h->nk, s);  // keep_drift
+  if (h->tor_on) d2d(h->d_dWa_prev.p, h->d_dWa.p, (size_t)2 * h->nk, s);
   VG_CUDA(cudaStreamSynchronize(s));
   double cnorm, snorm;
   std::memcpy(&cnorm, &bits[0], sizeof(double));
@@ -141,18 +164,23 @@ void trap_finalize(vg_handle* h, double dt) {
 // (src/vilma_response.f90:1695-1758): memory, time, sigma_n
 void trap_save(vg_handle* h) {
   d2d(h->d_mem_s.p, h->d_mem[h->cur].p, h->d_mem_s.n, h->stream);
+  if (h->tor_on) d2d(h->d_tmem_s.p, h->d_tmem[h->cur].p, h->d_tmem_s.n, h->stream);
   d2d(h->d_sigma_n_s.p, h->d_sigma_n.p, (size_t)2 * h->grid.nlm, h->stream);
   h->time_s_saved = h->time_s;
   h->sigma_primed_s = h->sigma_primed;
 }
 void trap_restore(vg_handle* h) {
   d2d(h->d_mem[h->cur].p, h->d_mem_s.p, h->d_mem_s.n, h->stream);
+  if (h->tor_on) d2d(h->d_tmem[h->cur].p, h->d_tmem_s.p, h->d_tmem_s.n, h->stream);
   d2d(h->d_sigma_n.p, h->d_sigma_n_s.p, (size_t)2 * h->grid.nlm, h->stream);
   h->time_s = h->time_s_saved;
   h->sigma_primed = h->sigma_primed_s;
   compute_mem_norm(h, h->cur);  // the drift's skip gate reads the buffer's norms
 }
-void trap_stash_coarse(vg_handle* h) { d2d(h->d_mem_c.p, h->d_mem[h->cur].p, h->d_mem_c.n, h->stream); }
+void trap_stash_coarse(vg_handle* h) {
+  d2d(h->d_mem_c.p, h->d_mem[h->cur].p, h->d_mem_c.n, h->stream);
+  if (h->tor_on) d2d(h->d_tmem_c.p, h->d_tmem[h->cur].p, h->d_tmem_c.n, h->stream);
+}
 
 void trap_coarse_fine_error(vg_handle* h, double& err_inf, double& tau_inf) {
   cudaStream_t s = h->stream;
@@ -160,6 +188,11 @@ void trap_coarse_fine_error(vg_handle* h, double& err_inf, double& tau_inf) {
   k_trap_cf<<<1184, 256, 0, s>>>(h->d_mem_c.n, h->d_mem[h->cur].p, h->d_mem_c.p, h->d_trap_red.p);
   ++h->n_launch;
   VG_CUDA(cudaGetLastError());
+  if (h->tor_on) {
+    k_trap_cf<<<1184, 256, 0, s>>>(h->d_tmem_c.n, h->d_tmem[h->cur].p, h->d_tmem_c.p, h->d_trap_red.p);
+    ++h->n_launch;
+    VG_CUDA(cudaGetLastError());
+  }
   unsigned long long bits[2];
   VG_CUDA(cudaMemcpyAsync(bits, h->d_trap_red.p, sizeof(bits), cudaMemcpyDeviceToHost, s));
   VG_CUDA(cudaStreamSynchronize(s));

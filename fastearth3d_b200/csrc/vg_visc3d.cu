@@ -15,6 +15,12 @@
 //   analysis  per order m, the quadrature adjoints: wP, wD, wP, wP, wG, wH
 //   scatter   channel normalisations (1, 1/J, -1/(2J), 1/n6) and the increment
 //             c += Delta into the next state buffer
+// With the toroidal channels carried (lambda 3, 4 as channels 4, 5) the
+// gather adds two channels, the synthesis four products (P.X4, D.X4, G.X5,
+// H.X5: rt -= i (m/sin) P.X4, rp += D.X4, Z4 = G e_tp - H (e_tt - e_pp)), the
+// longitude pass four analysis inputs (RP, m/sin RT, TP, TT - PP) and the
+// analysis four quadratures (wD, wP, wG, wH), normalised by 1/J and 1/n4 with
+// n4 = n6 / 4 (src/vilma_tensor_sh.f90:168-203, 231-242, 270-322, 360-387).
 // G and H are the spin-2 kernels of Z6 written through P and dP/dtheta:
 //   G = -2 cot dP - l(l+1) P + 2 m^2/sin^2 P,   H = (m/sin)(dP - cot P)
 // so that Sg = sum c G e^{im phi} and Sh = i sum c H e^{im phi}
@@ -76,6 +82,10 @@ __global__ void k_visc3d_n6(int lmax, int nlat, const int* __restrict__ mbeg, co
 struct V3Args {
   const double* mem;
   double* nxt;
+  const double* tmem;  // toroidal memory (tor), current and next buffer
+  double* tnxt;
+  const double* dWn;   // nodal W drift [ri][node][k] (tor)
+  int tor;
   const double* sigma;
   const int *kdeg, *k2lm, *e3d;
   const double *Jr, *xUn, *xVn, *dUn, *dVn, *mu;
@@ -90,10 +100,10 @@ struct V3Args {
 // row's 6 x 8 entries go out as one contiguous run.
 constexpr int V3_TK = 32, V3_TE = 8, V3_TC = 6 * V3_TE, V3_TP = V3_TK + 1;  // tile: columns per row, padded slots
 
-template <class T>
+template <class T, int NC>
 __global__ void __launch_bounds__(256) k_v3_gather(V3Args A, T* __restrict__ X) {
   extern __shared__ unsigned char v3_sm[];
-  T* tile = reinterpret_cast<T*>(v3_sm);  // [4 ch][V3_TC][V3_TP]
+  T* tile = reinterpret_cast<T*>(v3_sm);  // [NC ch][V3_TC][V3_TP]
   const int kx = threadIdx.x, ey = threadIdx.y;
   const int k0 = blockIdx.x * V3_TK, e0 = blockIdx.y * V3_TE;
   const int k = k0 + kx, ei = e0 + ey;
@@ -118,35 +128,49 @@ __global__ void __launch_bounds__(256) k_v3_gather(V3Args A, T* __restrict__ X) 
           if (lam == 2) v = -Jr * v;  // trace channel enters the synthesis as -l(l+1) c
           tile[((size_t)lam * V3_TC + ey * 6 + s3 * 2 + ri) * V3_TP + kx] = (T)v;
         }
+      if (NC == 6) {  // lambda 3, 4: memory + 2 mu strain of the W drift (no load term)
+        const double W0 = A.dWn[((size_t)ri * A.nr + e) * A.nk + k];
+        const double W1 = A.dWn[((size_t)ri * A.nr + e + 1) * A.nk + k];
+        double et[3][2];
+        strain_coeffs_tor(W0, W1, Jr, et[0], et[1], et[2]);
+#pragma unroll
+        for (int s3 = 0; s3 < 3; ++s3)
+#pragma unroll
+          for (int lam = 0; lam < 2; ++lam) {
+            const double v = A.tmem[tmem_idx(s3, ri, e, lam, k, A.ne, A.nk)] + twoMu * et[s3][lam];
+            tile[((size_t)(4 + lam) * V3_TC + ey * 6 + s3 * 2 + ri) * V3_TP + kx] = (T)v;
+          }
+      }
     }
   }
   __syncthreads();
   const int nkb = min(V3_TK, A.nk - k0), w = 6 * min(V3_TE, A.ne3d - e0);
-  for (int t = threadIdx.y * V3_TK + threadIdx.x; t < nkb * 4 * w; t += V3_TK * V3_TE) {
-    const int kl = t / (4 * w), rem = t % (4 * w), lam = rem / w, c = rem % w;
-    X[((size_t)(k0 + kl) * 4 + lam) * A.ncf + 6 * e0 + c] = tile[((size_t)lam * V3_TC + c) * V3_TP + kl];
+  for (int t = threadIdx.y * V3_TK + threadIdx.x; t < nkb * NC * w; t += V3_TK * V3_TE) {
+    const int kl = t / (NC * w), rem = t % (NC * w), lam = rem / w, c = rem % w;
+    X[((size_t)(k0 + kl) * NC + lam) * A.ncf + 6 * e0 + c] = tile[((size_t)lam * V3_TC + c) * V3_TP + kl];
   }
 }
 
-template <class T>
+template <class T, int NC = 4>
 constexpr size_t v3_gather_smem() {
-  return (size_t)4 * V3_TC * V3_TP * sizeof(T);
+  return (size_t)NC * V3_TC * V3_TP * sizeof(T);
 }
 
 // ------------------------------------------------------------------ GEMMs
 
 // Per-order batched FP64 products (the Legendre stage of the tensor transforms).
 //   mode 0 (synthesis): C[j][n] = sum_{kk < K_m} T_p[mbeg + kk][j] * X[row(m + kk, m)][col_p + n]
-//                       -> S[((m * nlat + j) * 6 + p) * ncf + n]
-//   mode 1 (analysis):  C[i][n] = sum_{j} T_p[mbeg + i][j] * S[((m * nlat + j) * 6 + p) * ncf + n]
-//                       -> R[(row(m + i, m) * 6 + p) * ncf + n]
+//                       -> S[((m * nlat + j) * np + p) * ncf + n]
+//   mode 1 (analysis):  C[i][n] = sum_{j} T_p[mbeg + i][j] * S[((m * nlat + j) * np + p) * ncf + n]
+//                       -> R[(row(m + i, m) * np + p) * ncf + n]
 // row(l, m) = kbeg[l] + m for l >= 1, the zero row nk for l = 0.
 struct GemmArgs {
   int mode, lmax, nlat, nk, ncf;
-  int nin;  // synthesis input channels per slot row (4: the gathered channels; 6: per product)
+  int nin;  // synthesis input channels per slot row (4 or 6: the gathered channels; np: per product)
+  int np;   // products: 6 (spheroidal) or 10 (with the toroidal channels)
   const int *mbeg, *kbeg;
-  const double* T[6];  // per product: table [lm][j]
-  int chan[6];         // synthesis: input channel per product
+  const double* T[10];  // per product: table [lm][j]
+  int chan[10];         // synthesis: input channel per product
   const double* in;
   double* out;
 };
@@ -158,7 +182,7 @@ __device__ __forceinline__ int slot_row(const int* kbeg, int l, int m, int nk) {
 __global__ void __launch_bounds__(256) k_v3_gemm(GemmArgs A) {
   __shared__ double As[GB_K][GB_M + 1];
   __shared__ double Bs[GB_K][GB_N];
-  const int m = blockIdx.z / 6, p = blockIdx.z % 6;
+  const int m = blockIdx.z / A.np, p = blockIdx.z % A.np;
   const int Km = A.lmax - m + 1;
   const int rows = (A.mode == 0) ? A.nlat : Km;
   const int kdim = (A.mode == 0) ? Km : A.nlat;
@@ -191,7 +215,7 @@ __global__ void __launch_bounds__(256) k_v3_gemm(GemmArgs A) {
           int row = slot_row(A.kbeg, m + gk, m, A.nk);
           v = A.in[(size_t)row * A.nin * A.ncf + (size_t)A.chan[p] * A.ncf + gn];
         } else {
-          v = A.in[(((size_t)m * A.nlat + gk) * 6 + p) * A.ncf + gn];
+          v = A.in[(((size_t)m * A.nlat + gk) * A.np + p) * A.ncf + gn];
         }
       }
       Bs[kk][n] = v;
@@ -221,9 +245,9 @@ __global__ void __launch_bounds__(256) k_v3_gemm(GemmArgs A) {
       int gn = n0 + tx + 16 * u;
       if (gn >= A.ncf) continue;
       if (A.mode == 0)
-        A.out[(((size_t)m * A.nlat + gr) * 6 + p) * A.ncf + gn] = acc[q][u];
+        A.out[(((size_t)m * A.nlat + gr) * A.np + p) * A.ncf + gn] = acc[q][u];
       else
-        A.out[((size_t)slot_row(A.kbeg, m + gr, m, A.nk) * 6 + p) * A.ncf + gn] = acc[q][u];
+        A.out[((size_t)slot_row(A.kbeg, m + gr, m, A.nk) * A.np + p) * A.ncf + gn] = acc[q][u];
     }
   }
 }
@@ -399,24 +423,26 @@ constexpr int LON_LF = 3;  // fields per CTA: one element's three shape coeffici
 // the CTA's slice of the products S[m][j][q][f][ri] (fields f0 .. f0 + nft - 1,
 // a contiguous run of 2 nft doubles per (m, q)) to and from shared [m][q][2 nft]
 // (16-byte cp.async pieces, all in flight together; ncf and 2 f0 are even)
+template <int NQ = 6>
 __device__ __forceinline__ void stage_in(const double* __restrict__ S, double* __restrict__ X, int nlat, int ncf,
                                          int j, int f0, int nft, int M) {
-  const int n = M * 6 * nft;
+  const int n = M * NQ * nft;
   for (int t = threadIdx.x; t < n; t += blockDim.x) {
     const int mq = t / nft, c = t % nft;
     lon_cp16(X + (size_t)mq * 2 * nft + 2 * c,
-             S + ((size_t)(mq / 6) * nlat + j) * 6 * ncf + (size_t)(mq % 6) * ncf + 2 * f0 + 2 * c);
+             S + ((size_t)(mq / NQ) * nlat + j) * NQ * ncf + (size_t)(mq % NQ) * ncf + 2 * f0 + 2 * c);
   }
   lon_commit();
   lon_wait<0>();
 }
 
+template <int NQ = 6>
 __device__ __forceinline__ void stage_out(const double* __restrict__ X, double* __restrict__ S, int nlat, int ncf,
                                           int j, int f0, int nft, int M) {
-  const int w = 2 * nft, n = M * 6 * w;
+  const int w = 2 * nft, n = M * NQ * w;
   for (int t = threadIdx.x; t < n; t += blockDim.x) {
     const int mq = t / w, c = t % w;
-    S[((size_t)(mq / 6) * nlat + j) * 6 * ncf + (size_t)(mq % 6) * ncf + 2 * f0 + c] = X[t];
+    S[((size_t)(mq / NQ) * nlat + j) * NQ * ncf + (size_t)(mq % NQ) * ncf + 2 * f0 + c] = X[t];
   }
 }
 
@@ -425,7 +451,7 @@ __device__ __forceinline__ void stage_out(const double* __restrict__ X, double* 
 // the field's element, analysis, and the six analysis inputs, written in place
 // over the synthesis products. With gstore set, the grid before -M dt is also
 // stored, [j][field][component][i], for the adjoint.
-template <int LF>
+template <int LF, int NQ = 6>
 __global__ void __launch_bounds__(LON_THREADS, 1)
     k_v3_lon(double* __restrict__ S, int nlat, int nphi, int nf, double dt, const double* __restrict__ Mk3rate,
              LonTables T, const double* __restrict__ invsin, double* __restrict__ gstore, int trap) {
@@ -433,26 +459,38 @@ __global__ void __launch_bounds__(LON_THREADS, 1)
   const int j = blockIdx.x, f0 = blockIdx.y * LF;
   const int nft = min(LF, nf - f0);
   const int ncf = 2 * nf, half = T.half, wA = 2 * T.M2;
-  double* A = sm;                          // [6 LF][2 M2]
-  double* X = sm + (size_t)6 * LF * wA;    // [6 LF][nphi]
+  double* A = sm;                          // [6 LF][2 M2]; [m][q][2 nft] for the analysis inputs
+  double* X = sm + (size_t)NQ * LF * wA;   // [6 LF][nphi]; [m][q][2 nft] for the synthesis products
   const double is = invsin[j];
   // 1. the CTA's synthesis products, staged in X as [m][q][2 nft] (contiguous
   //    runs of 2 nft doubles in S), then the dyadic coefficients rr, rt, rp,
   //    tt, pp, tp with the synthesis weights (1 at m = 0, 2 above), zero past M
-  stage_in(S, X, nlat, ncf, j, f0, nft, T.M);
+  stage_in<NQ>(S, X, nlat, ncf, j, f0, nft, T.M);
   __syncthreads();
   for (int t = threadIdx.x; t < nft * T.M2; t += blockDim.x) {
     const int fl = t / T.M2, m = t % T.M2;
-    double pr[6][2];
-    for (int q = 0; q < 6; ++q)
-      for (int ri = 0; ri < 2; ++ri) pr[q][ri] = (m < T.M) ? X[((size_t)m * 6 + q) * 2 * nft + 2 * fl + ri] : 0.0;
+    double pr[NQ][2];
+    for (int q = 0; q < NQ; ++q)
+      for (int ri = 0; ri < 2; ++ri) pr[q][ri] = (m < T.M) ? X[((size_t)m * NQ + q) * 2 * nft + 2 * fl + ri] : 0.0;
     const double ms = m * is, w = (m == 0) ? 1.0 : 2.0;
-    const double comp[6][2] = {{pr[0][0], pr[0][1]},
-                               {pr[1][0], pr[1][1]},
-                               {-ms * pr[2][1], ms * pr[2][0]},           // i (m / sin) P.X1
-                               {pr[3][0] + pr[4][0], pr[3][1] + pr[4][1]},  // TT + PP
-                               {pr[3][0] - pr[4][0], pr[3][1] - pr[4][1]},  // TT - PP
-                               {-4.0 * pr[5][1], 4.0 * pr[5][0]}};          // 4 i H.X3
+    double comp[6][2] = {{pr[0][0], pr[0][1]},
+                         {pr[1][0], pr[1][1]},
+                         {-ms * pr[2][1], ms * pr[2][0]},             // i (m / sin) P.X1
+                         {pr[3][0] + pr[4][0], pr[3][1] + pr[4][1]},  // TT + PP
+                         {pr[3][0] - pr[4][0], pr[3][1] - pr[4][1]},  // TT - PP
+                         {-4.0 * pr[5][1], 4.0 * pr[5][0]}};          // 4 i H.X3
+    if (NQ == 10) {  // Z3: (rt, rp) += e_r x grad_1 = (-i (m/sin) P.X4, D.X4); Z4: (tt, pp, tp) += (-Sh, Sh, Sg)
+      comp[1][0] += ms * pr[6][1];
+      comp[1][1] -= ms * pr[6][0];
+      comp[2][0] += pr[7][0];
+      comp[2][1] += pr[7][1];
+      comp[3][0] += pr[9][1];  // -i H.X5
+      comp[3][1] -= pr[9][0];
+      comp[4][0] -= pr[9][1];  // +i H.X5
+      comp[4][1] += pr[9][0];
+      comp[5][0] += pr[8][0];  // G.X5
+      comp[5][1] += pr[8][1];
+    }
     for (int c = 0; c < 6; ++c) {
       A[(size_t)(fl * 6 + c) * wA + 2 * m] = w * comp[c][0];
       A[(size_t)(fl * 6 + c) * wA + 2 * m + 1] = w * comp[c][1];
@@ -490,24 +528,31 @@ __global__ void __launch_bounds__(LON_THREADS, 1)
       F[c][1] = scl * im[c];
     }
     const double ms = m * is;
-    const double out[6][2] = {{F[0][0], F[0][1]},
-                              {F[1][0], F[1][1]},
-                              {ms * F[2][0], ms * F[2][1]},
-                              {F[3][0] + F[4][0], F[3][1] + F[4][1]},
-                              {F[3][0] - F[4][0], F[3][1] - F[4][1]},
-                              {F[5][0], F[5][1]}};
-    for (int q = 0; q < 6; ++q)
-      for (int ri = 0; ri < 2; ++ri) A[((size_t)m * 6 + q) * 2 * nft + 2 * fl + ri] = out[q][ri];
+    const double out[10][2] = {{F[0][0], F[0][1]},
+                               {F[1][0], F[1][1]},
+                               {ms * F[2][0], ms * F[2][1]},
+                               {F[3][0] + F[4][0], F[3][1] + F[4][1]},
+                               {F[3][0] - F[4][0], F[3][1] - F[4][1]},
+                               {F[5][0], F[5][1]},
+                               {F[2][0], F[2][1]},                      // RP (wD)
+                               {ms * F[1][0], ms * F[1][1]},            // m/sin RT (wP)
+                               {F[5][0], F[5][1]},                      // TP (wG)
+                               {F[3][0] - F[4][0], F[3][1] - F[4][1]}};  // TT - PP (wH)
+    for (int q = 0; q < NQ; ++q)
+      for (int ri = 0; ri < 2; ++ri) A[((size_t)m * NQ + q) * 2 * nft + 2 * fl + ri] = out[q][ri];
   });
   __syncthreads();
-  stage_out(A, S, nlat, ncf, j, f0, nft, T.M);
+  stage_out<NQ>(A, S, nlat, ncf, j, f0, nft, T.M);
 }
 
-// shared memory of the longitude pass (forward: adj = 0) and its transpose
-static size_t lon_smem(const vg_handle* h, int LF, bool adj) {
+// shared memory of the longitude pass (forward: adj = 0) and its transpose;
+// nq analysis inputs (10 with the toroidal channels)
+static size_t lon_smem(const vg_handle* h, int LF, bool adj, int nq = 6) {
   const LonTables T = lon_tables(h);
   const int nphi = h->grid.nphi;
-  return (size_t)(6 * LF * 2 * T.M2 + 6 * LF * nphi + (adj ? LF * nphi : 0)) * sizeof(double);
+  const size_t a = (size_t)nq * LF * 2 * T.M2;
+  const size_t x = std::max((size_t)6 * LF * nphi, (size_t)nq * 2 * T.M * LF);
+  return (a + x + (adj ? (size_t)LF * nphi : 0)) * sizeof(double);
 }
 
 static int lon_threads(const vg_handle* h, int LF) {
@@ -520,26 +565,42 @@ constexpr size_t LON_SMEM_MAX = 220 * 1024;
 static void lon_attributes();  // the longitude kernels' shared-memory limit (defined after the transpose)
 
 static void lon_check(const vg_handle* h) {
-  if (lon_smem(h, LON_LF, true) > LON_SMEM_MAX) throw Error("visc3d: grid too large for the FP64 longitude pass");
+  if (lon_smem(h, LON_LF, true) > LON_SMEM_MAX || lon_smem(h, LON_LF, false, h->tor_on ? 10 : 6) > LON_SMEM_MAX)
+    throw Error("visc3d: grid too large for the FP64 longitude pass");
 }
 
 // ------------------------------------------------------------------ scatter
 
 // Channel normalisations and the increment form c += Delta
 // (src/vilma_response.f90:1281-1318): one thread per (slot, 3-D element).
-template <class T>
+template <class T, int NQ = 6>
 __global__ void __launch_bounds__(256) k_v3_scatter(V3Args A, const T* __restrict__ R,
                                                     const double* __restrict__ n6) {
   const int k = blockIdx.x * 32 + threadIdx.x, ei = blockIdx.y * 8 + threadIdx.y;
   if (k >= A.nk || ei >= A.ne3d) return;
   const int e = A.e3d[ei], l = A.kdeg[k];
   const double J = A.Jr[l], nn = n6[l];
-  const T* row = R + (size_t)k * 6 * A.ncf;
+  const T* row = R + (size_t)k * NQ * A.ncf;
   for (int s3 = 0; s3 < 3; ++s3) {
     const int f = 3 * ei + s3;
-    double q[6][2];
-    for (int p = 0; p < 6; ++p)
+    double q[NQ][2];
+#pragma unroll
+    for (int p = 0; p < NQ; ++p)
+#pragma unroll
       for (int ri = 0; ri < 2; ++ri) q[p][ri] = (double)row[(size_t)p * A.ncf + 2 * f + ri];
+    if (NQ == 10) {  // lambda 3: (wD.RP + i wP.(m/sin RT)) / J; lambda 4: (wG.TP / 2 + i wH.(TT - PP)) / n4
+      const double n4 = 0.25 * nn;
+      double t[2][2];
+      t[0][0] = (q[NQ - 4][0] - q[NQ - 3][1]) / J;
+      t[0][1] = (q[NQ - 4][1] + q[NQ - 3][0]) / J;
+      t[1][0] = n4 != 0.0 ? (0.5 * q[NQ - 2][0] - q[NQ - 1][1]) / n4 : 0.0;
+      t[1][1] = n4 != 0.0 ? (0.5 * q[NQ - 2][1] + q[NQ - 1][0]) / n4 : 0.0;
+      for (int ri = 0; ri < 2; ++ri)
+        for (int lam = 0; lam < 2; ++lam) {
+          const size_t idx = tmem_idx(s3, ri, e, lam, k, A.ne, A.nk);
+          A.tnxt[idx] = A.tmem[idx] + t[lam][ri];
+        }
+    }
     double d[4][2];
     d[0][0] = q[0][0];
     d[0][1] = q[0][1];
@@ -561,9 +622,11 @@ __global__ void __launch_bounds__(256) k_v3_scatter(V3Args A, const T* __restric
 static void v3_tile_attributes() {
   static bool done = false;
   if (done) return;
-  VG_CUDA(cudaFuncSetAttribute(k_v3_gather<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+  VG_CUDA(cudaFuncSetAttribute(k_v3_gather<double, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                (int)v3_gather_smem<double>()));
-  VG_CUDA(cudaFuncSetAttribute(k_v3_gather<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+  VG_CUDA(cudaFuncSetAttribute(k_v3_gather<double, 6>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)v3_gather_smem<double, 6>()));
+  VG_CUDA(cudaFuncSetAttribute(k_v3_gather<float, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                (int)v3_gather_smem<float>()));
   done = true;
 }
@@ -576,6 +639,9 @@ void visc3d_enable(vg_handle* h, const double* pert) {
   cudaStream_t s = h->stream;
   if (G.nphi % 2 != 0) throw Error("vg_enable_visc3d: the longitude pass needs an even nphi");
   if (h->lat_visc) throw Error("vg_enable_visc3d: lateral viscosity is already enabled for this handle");
+  if (h->p.toroidal && h->p.visc3d_precision != VG_VISC3D_FP64)
+    throw Error("vg_enable_visc3d: the toroidal channels are carried on the FP64 3-D path only "
+                "(toroidal = 1 needs visc3d_precision = VG_VISC3D_FP64)");
   // Maxwell-CFL rate: the grid maximum of mu/eta_eff over every Maxwell element
   // (src/vilma_response.f90:1783-1793, MkPerDt3 covers all elements)
   double rate_max = 0.0;
@@ -629,15 +695,18 @@ void visc3d_enable(vg_handle* h, const double* pert) {
   VG_CUDA(cudaGetLastError());
   h->d_kbeg.upload(h->kbeg_h, s);
   VG_CUDA(cudaStreamSynchronize(s));
+  // a genuinely 3-D element couples spheroidal and toroidal
+  // (src/vilma_response.f90:1048-1052)
+  if (h->p.toroidal) toroidal_enable(h);
   if (h->p.visc3d_precision == VG_VISC3D_SPLIT_TC) {
     visc3d_tc_enable(h);
     return;
   }
   // work buffers and longitude tables of the FP64 path
-  const int nf = 3 * h->ne3d, ncf = 2 * nf;
-  h->d_X.alloc((size_t)(h->nk + 1) * 4 * ncf);
-  h->d_Y.alloc((size_t)G.M * G.nlat * 6 * ncf);
-  h->d_dy.alloc((size_t)(h->nk + 1) * 6 * ncf);
+  const int nf = 3 * h->ne3d, ncf = 2 * nf, nch = h->tor_on ? 6 : 4, np = h->tor_on ? 10 : 6;
+  h->d_X.alloc((size_t)(h->nk + 1) * nch * ncf);
+  h->d_Y.alloc((size_t)G.M * G.nlat * np * ncf);
+  h->d_dy.alloc((size_t)(h->nk + 1) * np * ncf);
   lon_tables_build(h);
   lon_check(h);  // the grid fits the longitude pass (throws otherwise)
   lon_attributes();
@@ -645,7 +714,7 @@ void visc3d_enable(vg_handle* h, const double* pert) {
 }
 
 void visc3d_advance(vg_handle* h, const double* d_sigma, double dt, const double* dUn, const double* dVn,
-                    bool trap) {
+                    bool trap, const double* dWn) {
   if (h->ne3d == 0) return;
   PhaseScope ps(h, VG_PH_VISC3D);
   const Grid& G = h->grid;
@@ -654,6 +723,10 @@ void visc3d_advance(vg_handle* h, const double* d_sigma, double dt, const double
   V3Args A;
   A.mem = h->d_mem[h->cur].p;
   A.nxt = h->d_mem[1 - h->cur].p;
+  A.tor = h->tor_on ? 1 : 0;
+  A.tmem = h->tor_on ? h->d_tmem[h->cur].p : nullptr;
+  A.tnxt = h->tor_on ? h->d_tmem[1 - h->cur].p : nullptr;
+  A.dWn = h->tor_on ? (dWn ? dWn : h->d_dWn.p) : nullptr;
   A.sigma = d_sigma;
   A.kdeg = h->d_kdeg.p;
   A.k2lm = h->d_k2lm.p;
@@ -677,7 +750,7 @@ void visc3d_advance(vg_handle* h, const double* d_sigma, double dt, const double
     visc3d_tc_buffers(h, &X32, &dy32);
     {
       PhaseScope pg(h, VG_PH_V3_GATHER);
-      k_v3_gather<float><<<gg, dim3(32, 8), v3_gather_smem<float>(), s>>>(A, X32);
+      k_v3_gather<float, 4><<<gg, dim3(32, 8), v3_gather_smem<float>(), s>>>(A, X32);
       ++h->n_launch;
       VG_CUDA(cudaGetLastError());
     }
@@ -690,29 +763,35 @@ void visc3d_advance(vg_handle* h, const double* d_sigma, double dt, const double
   }
   {
     PhaseScope pg(h, VG_PH_V3_GATHER);
-    k_v3_gather<double><<<gg, dim3(32, 8), v3_gather_smem<double>(), s>>>(A, h->d_X.p);
+    if (h->tor_on)
+      k_v3_gather<double, 6><<<gg, dim3(32, 8), v3_gather_smem<double, 6>(), s>>>(A, h->d_X.p);
+    else
+      k_v3_gather<double, 4><<<gg, dim3(32, 8), v3_gather_smem<double>(), s>>>(A, h->d_X.p);
     ++h->n_launch;
     VG_CUDA(cudaGetLastError());
   }
   // synthesis
+  const int np = h->tor_on ? 10 : 6;
   GemmArgs S;
   S.mode = 0;
   S.lmax = G.lmax;
   S.nlat = G.nlat;
   S.nk = h->nk;
   S.ncf = ncf;
-  S.nin = 4;
+  S.nin = h->tor_on ? 6 : 4;
+  S.np = np;
   S.mbeg = G.d_mbeg.p;
   S.kbeg = h->d_kbeg.p;
-  const double* st[6] = {G.d_plm.p, G.d_dplm.p, G.d_plm.p, G.d_plm.p, h->d_G6.p, h->d_H6.p};
-  const int sc[6] = {0, 1, 1, 2, 3, 3};
-  for (int p = 0; p < 6; ++p) {
+  const double* st[10] = {G.d_plm.p, G.d_dplm.p, G.d_plm.p, G.d_plm.p, h->d_G6.p,
+                          h->d_H6.p, G.d_plm.p,  G.d_dplm.p, h->d_G6.p, h->d_H6.p};
+  const int sc[10] = {0, 1, 1, 2, 3, 3, 4, 4, 5, 5};
+  for (int p = 0; p < np; ++p) {
     S.T[p] = st[p];
     S.chan[p] = sc[p];
   }
   S.in = h->d_X.p;
   S.out = h->d_Y.p;
-  dim3 sg((ncf + GB_N - 1) / GB_N, (G.nlat + GB_M - 1) / GB_M, G.M * 6);
+  dim3 sg((ncf + GB_N - 1) / GB_N, (G.nlat + GB_M - 1) / GB_M, G.M * np);
   {
     PhaseScope pp(h, VG_PH_V3_SYNTH);
     k_v3_gemm<<<sg, 256, 0, s>>>(S);
@@ -723,19 +802,25 @@ void visc3d_advance(vg_handle* h, const double* d_sigma, double dt, const double
   {
     PhaseScope pp(h, VG_PH_V3_LON_INV);
     const dim3 lg(G.nlat, (nf + LON_LF - 1) / LON_LF);
-    k_v3_lon<LON_LF><<<lg, lon_threads(h, LON_LF), lon_smem(h, LON_LF, false), s>>>(
-        h->d_Y.p, G.nlat, G.nphi, nf, dt, h->d_MkPerDt3.p, lon_tables(h), G.d_invsin.p, h->v3_gstore, trap ? 1 : 0);
+    if (h->tor_on)
+      k_v3_lon<LON_LF, 10><<<lg, lon_threads(h, LON_LF), lon_smem(h, LON_LF, false, 10), s>>>(
+          h->d_Y.p, G.nlat, G.nphi, nf, dt, h->d_MkPerDt3.p, lon_tables(h), G.d_invsin.p, nullptr, trap ? 1 : 0);
+    else
+      k_v3_lon<LON_LF><<<lg, lon_threads(h, LON_LF), lon_smem(h, LON_LF, false), s>>>(
+          h->d_Y.p, G.nlat, G.nphi, nf, dt, h->d_MkPerDt3.p, lon_tables(h), G.d_invsin.p, h->v3_gstore,
+          trap ? 1 : 0);
     ++h->n_launch;
     VG_CUDA(cudaGetLastError());
   }
   // analysis
   GemmArgs Aa = S;
   Aa.mode = 1;
-  const double* at[6] = {h->d_wP.p, h->d_wD.p, h->d_wP.p, h->d_wP.p, h->d_wG.p, h->d_wH.p};
-  for (int p = 0; p < 6; ++p) Aa.T[p] = at[p];
+  const double* at[10] = {h->d_wP.p, h->d_wD.p, h->d_wP.p, h->d_wP.p, h->d_wG.p,
+                          h->d_wH.p, h->d_wD.p, h->d_wP.p, h->d_wG.p, h->d_wH.p};
+  for (int p = 0; p < np; ++p) Aa.T[p] = at[p];
   Aa.in = h->d_Y.p;
   Aa.out = h->d_dy.p;
-  dim3 ag((ncf + GB_N - 1) / GB_N, (G.M + GB_M - 1) / GB_M, G.M * 6);
+  dim3 ag((ncf + GB_N - 1) / GB_N, (G.M + GB_M - 1) / GB_M, G.M * np);
   {
     PhaseScope pp(h, VG_PH_V3_ANALYSIS);
     k_v3_gemm<<<ag, 256, 0, s>>>(Aa);
@@ -743,7 +828,10 @@ void visc3d_advance(vg_handle* h, const double* d_sigma, double dt, const double
     VG_CUDA(cudaGetLastError());
   }
   PhaseScope pc(h, VG_PH_V3_SCATTER);
-  k_v3_scatter<double><<<gg, dim3(32, 8), 0, s>>>(A, h->d_dy.p, h->d_n6.p);
+  if (h->tor_on)
+    k_v3_scatter<double, 10><<<gg, dim3(32, 8), 0, s>>>(A, h->d_dy.p, h->d_n6.p);
+  else
+    k_v3_scatter<double><<<gg, dim3(32, 8), 0, s>>>(A, h->d_dy.p, h->d_n6.p);
   ++h->n_launch;
   VG_CUDA(cudaGetLastError());
 }
@@ -916,7 +1004,8 @@ __global__ void __launch_bounds__(256) k_v3_gather_T(V3Args A, const double* __r
 }
 
 static void lon_attributes() {
-  for (const void* k : {(const void*)k_v3_lon<LON_LF>, (const void*)k_v3_lon_T<LON_LF>})
+  for (const void* k :
+       {(const void*)k_v3_lon<LON_LF>, (const void*)k_v3_lon<LON_LF, 10>, (const void*)k_v3_lon_T<LON_LF>})
     VG_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)LON_SMEM_MAX));
 }
 
@@ -938,6 +1027,10 @@ void visc3d_adjoint(vg_handle* h, const double* gstore, double dt, const double*
   A.mem = h->d_mem[h->cur].p;
   A.nxt = nullptr;
   A.sigma = nullptr;
+  A.tor = 0;
+  A.tmem = nullptr;
+  A.tnxt = nullptr;
+  A.dWn = nullptr;
   A.kdeg = h->d_kdeg.p;
   A.k2lm = h->d_k2lm.p;
   A.e3d = h->d_e3d.p;
@@ -961,6 +1054,7 @@ void visc3d_adjoint(vg_handle* h, const double* gstore, double dt, const double*
   S.nk = h->nk;
   S.ncf = ncf;
   S.nin = 4;
+  S.np = 6;
   S.mbeg = G.d_mbeg.p;
   S.kbeg = h->d_kbeg.p;
   const double* st[6] = {G.d_plm.p, G.d_dplm.p, G.d_plm.p, G.d_plm.p, h->d_G6.p, h->d_H6.p};

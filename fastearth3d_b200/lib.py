@@ -40,6 +40,9 @@ _SIGS = [
     ("vg_set_fields", [_VP, _P, _P, _P, _P]),
     ("vg_get_rotation_state", [_VP, _P, _P, _P]),
     ("vg_get_step_state", [_VP, _P, _P, C.POINTER(C.c_int)]),
+    ("vg_get_toroidal", [_VP, _P]),
+    ("vg_get_state_tor", [_VP, _P, _P, _P, _P, _P, _P, C.POINTER(C.c_int)]),
+    ("vg_set_state_tor", [_VP, _P, _P, _P, _P, _P, _P]),
     ("vg_set_step_state", [_VP, C.c_double, _P, C.c_int]),
     ("vg_set_rotation_state", [_VP, _P, _P, _P]),
     ("vg_spinup", [_VP, _P, C.c_double, C.c_double, _P, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
@@ -165,6 +168,24 @@ class Model:
     def set_fields(self, h_ice=None, rsl=None, z_bed=None, C_ocean=None):
         self._c(lib().vg_set_fields(self.h, *[ptr(None if a is None else np.ascontiguousarray(a, dtype=np.float64))
                                               for a in (h_ice, rsl, z_bed, C_ocean)]))
+
+    def toroidal(self):
+        """Surface toroidal drift W(a) as t_lm (lm order); zero while not carried."""
+        t = np.zeros(2 * self.nlm)
+        self._c(lib().vg_get_toroidal(self.h, ptr(t)))
+        return t[0::2] + 1j * t[1::2]
+
+    def state_tor(self):
+        """Toroidal memory (NLAM_TOR, ne, nk) x 6, or None while not carried."""
+        n = 2 * self.ne * self.nk
+        arrs = [np.zeros(n) for _ in range(6)]
+        c = C.c_int(0)
+        self._c(lib().vg_get_state_tor(self.h, *[ptr(a) for a in arrs], C.byref(c)))
+        return arrs if c.value else None
+
+    def set_state_tor(self, arrs):
+        arrs = [np.ascontiguousarray(a, dtype=np.float64) for a in arrs]
+        self._c(lib().vg_set_state_tor(self.h, *[ptr(a) for a in arrs]))
 
     def step_state(self):
         """(dt_try [yr], sigma_n as nlm complex, primed) of the time stepper."""

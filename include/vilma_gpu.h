@@ -188,6 +188,20 @@ int vg_set_state(vg_handle* h, const double* Are, const double* Aim, const doubl
  * After vg_set_reference. */
 int vg_set_fields(vg_handle* h, const double* h_ice, const double* rsl, const double* z_bed,
                   const double* C);
+/* The toroidal part of the surface horizontal displacement, t_lm of
+ * u_h = e_r x grad_1(sum t_lm Y_lm): the surface W(a) of the last drift solve
+ * (response_horizontal_toroidal, src/vilma_response.f90:884-900), nlm complex
+ * interleaved in lm order; zero while no toroidal field is carried. */
+int vg_get_toroidal(vg_handle* h, double* t_lm);
+/* Toroidal memory (lambda 3, 4) in the reference's restart order (NLAM_TOR = 2,
+ * ne, nk): the channels 5, 6 of its (6, ne, nk) restart arrays
+ * (src/vilma_io.f90:505-530). *carried = 0 (and nothing written) while the
+ * toroidal channels are not carried; set requires them carried (vg_enable_visc3d
+ * with toroidal = 1 and a genuinely 3-D element) and follows vg_set_state. */
+int vg_get_state_tor(vg_handle* h, double* Are, double* Aim, double* Bre, double* Bim, double* Cre, double* Cim,
+                     int* carried);
+int vg_set_state_tor(vg_handle* h, const double* Are, const double* Aim, const double* Bre, const double* Bim,
+                     const double* Cre, const double* Cim);
 /* Time-stepping restart state (the restart variables "dt_try", "sigma_n_re",
  * "sigma_n_im", "sigma_primed" of src/vilma_io.f90:38-46, 329-334, 457-458,
  * 599-615): the adaptive controller's next-step suggestion dt_try [yr] (used by
