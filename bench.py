@@ -47,6 +47,8 @@ def parse():
                     help="3-D stress products of the timed arm")
     ap.add_argument("--plain", default="on", choices=["on", "off"],
                     help="also time the plain FP64 arm beside split_tc (and report the rsl error between them)")
+    ap.add_argument("--toroidal", default="on", choices=["on", "off"],
+                    help="also time the FP64 path carrying the toroidal channels (toroidal = 1)")
     ap.add_argument("--grad-fwd", default="on", choices=["on", "off", "only"],
                     help="also time the adjoint gradient against its forward (grad/fwd); 'only' prints that alone")
     return ap.parse_args()
@@ -223,7 +225,7 @@ def replica_throughput(world, steps, max_ms):
     return world * steps / (max_ms * 1e-3)
 
 
-def run_arm(w, precision, args, ice_dev, local, dist, want_e2e):
+def run_arm(w, precision, args, ice_dev, local, dist, want_e2e, toroidal=False):
     """Warm-up, device-timed region, phase-timer pass and end-to-end pass of one
     model instance of the workload; returns the measurements."""
     import torch
@@ -232,6 +234,7 @@ def run_arm(w, precision, args, ice_dev, local, dist, want_e2e):
 
     p = w.params(vlib.default_params)
     p.visc3d_precision = precision
+    p.toroidal = 1 if toroidal else 0
     m = vlib.Model(p)
     zb, hi = w.reference()
     m.set_reference(zb, hi)
@@ -405,6 +408,7 @@ def main():
     split = w.visc3d and args.precision == "split_tc"
     main_arm = run_arm(w, 1 if split else 0, args, ice_dev, local, dist, True)
     plain = run_arm(w, 0, args, ice_dev, local, dist, False) if split and args.plain == "on" else None
+    tor = run_arm(w, 0, args, ice_dev, local, dist, False, True) if w.visc3d and args.toroidal == "on" else None
     if rank != 0:
         if dist:
             dist.destroy_process_group()
@@ -448,6 +452,13 @@ def main():
             "after_steps": total, "rsl": float(np.abs(r1 - r0).max() / np.abs(r0).max()),
             "z_bed": float(np.abs(z1 - z0).max() / np.abs(z0).max()), "norm": "max abs diff / max abs (FP64 GPU)",
             "rsl_target": 1e-8}
+    if tor is not None:
+        ref = plain if plain is not None else (main_arm if not split else None)
+        out["toroidal_fp64"] = {
+            "value": replica_throughput(world, args.steps, tor["ms"]), "unit": "steps/s",
+            "ms_per_step": tor["ms"] / args.steps, "gpu_launches": int(tor["launches"]), "n_sub": tor["info"].n_sub_last,
+            "cost_vs_spheroidal_fp64": (tor["ms"] / ref["ms"]) if ref is not None else None,
+            "phases": phases_of(tor), "clocks": tor["clocks"]}
     if args.grad_fwd == "on":
         out["grad_fwd"] = measure_grad_fwd(w)
     if not args.no_cpu_baseline:

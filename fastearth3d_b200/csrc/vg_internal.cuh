@@ -174,8 +174,9 @@ struct vg_handle {
   bool tor_on = false;
   vg::DArr<double> d_tmem[2];
   vg::DArr<double> d_dWn, d_dWa;           // nodal W drift [ri][node][k], surface W(a) [ri][k]
-  vg::DArr<double> d_tw, d_tib, d_tc;      // W operators l >= 2: Thomas multipliers, 1/pivots, super-diagonal (l, nr)
-  vg::DArr<double> d_tG1;                  // degree 1: W = G1W g (nr x nr, bordered solve folded in)
+  vg::DArr<double> d_tGinv;                // inverse W operators, degree l at (l - 1) nr^2 (row-major)
+  vg::DArr<double> d_tg;                   // W drift forcing [ri][node][k]
+  vg::DArr<double> d_tK;                   // forcing maps of the toroidal memory (lmax + 1, ne, 12)
   vg::DArr<double> d_edWn, d_dW_avg, d_dWa_prev, d_tmem_s, d_tmem_c;  // trapezoidal scheme
   // trapezoidal scheme (scheme = VG_SCHEME_TRAP; vg_trap.cu)
   vg::DArr<double> d_edUn, d_edVn;      // endpoint nodal drift (2 nr nk each)

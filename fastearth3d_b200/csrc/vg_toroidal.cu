@@ -16,18 +16,19 @@
 //              elements from the strain of W (the 3-D elements go through the
 //              six-channel pseudo-spectral advance of vg_visc3d.cu)
 //
-// The operators are factored once on the host at enable time: l >= 2 as a
-// Thomas factorisation (the system is symmetric positive definite on the live
-// nodes, so no pivoting; a pinned node has 1/pivot = 0, which zeroes its W),
-// l = 1 as the explicit solution map G1W (nr x nr) of the bordered system,
-// equilibrated and solved by partial-pivoting elimination.
-// Kernels:
-//   k_drift_tor     one thread per (slot, re/im): forcing and forward sweep in
-//                   one pass over the elements (the sweep output y goes
-//                   through the W target, coalesced along the slot), then the
-//                   back substitution; degree 1 leaves the raw forcing there
-//   k_drift_tor1    degree 1: W = G1W g for its two slots
-//   k_advance_1d_tor  one thread per (slot, element, re/im), like k_advance_1d
+// The W operators are small (nr x nr) and never change, so enable time inverts
+// them on the host: l >= 2 by Thomas solves of the unit forcings (the system is
+// symmetric positive definite on the live nodes, so no pivoting is needed),
+// l = 1 through the bordered system, equilibrated and solved by
+// partial-pivoting elimination; pinned rows and columns are zero. The drift is
+// then two bandwidth-friendly kernels instead of a serial sweep per slot:
+//   k_drift_tor_rhs  one thread per (slot, node, re/im): the forcing g at the
+//                    node from its two elements through per-(degree, element)
+//                    maps of the memory (the memory read along the slot)
+//   k_drift_tor_mm   per degree, W = G_l g for all 2 (l + 1) columns (slot,
+//                    re/im) of the degree: the forcing tile staged in shared
+//                    memory, the inverse streamed from L2
+//   k_advance_1d_tor one thread per (slot, element, re/im), like k_advance_1d
 #include <algorithm>
 #include <cmath>
 #include <cstring>
@@ -112,37 +113,73 @@ static std::vector<double> degree1_solution_map(const std::vector<double>& diag,
 void toroidal_enable(vg_handle* h) {
   cudaStream_t s = h->stream;
   const int nr = h->nr, nk = h->nk, L = h->grid.lmax;
-  std::vector<double> tw((size_t)(L + 1) * nr, 0.0), tib(tw.size(), 0.0), tc(tw.size(), 0.0);
-  std::vector<double> diag, off;
+  const size_t nr2 = (size_t)nr * nr;
+  std::vector<double> Ginv((size_t)L * nr2, 0.0);  // degree l at (l - 1) nr^2, row-major [i][j]
+  std::vector<double> diag, off, w(nr), ib(nr), y(nr);
   std::vector<char> dead;
   for (int l = 2; l <= L; ++l) {
     toroidal_tridiag(h->r, h->mu, l, diag, off, dead);
-    double* w = &tw[(size_t)l * nr];
-    double* ib = &tib[(size_t)l * nr];
-    double* c = &tc[(size_t)l * nr];
     double bp = 1.0;
-    for (int i = 0; i < nr; ++i) {
+    for (int i = 0; i < nr; ++i) {  // Thomas factorisation
       const double d = dead[i] ? 1.0 : diag[i];
-      const double a = i > 0 ? off[i - 1] : 0.0;  // sub-diagonal = super-diagonal of the row above
+      const double a = i > 0 ? off[i - 1] : 0.0;
       w[i] = i > 0 ? a / bp : 0.0;
       bp = d - w[i] * a;
       if (!dead[i] && !(bp > 0.0)) throw Error("toroidal operator: non-positive pivot (degree " + std::to_string(l) + ")");
       ib[i] = dead[i] ? 0.0 : 1.0 / bp;
-      c[i] = i + 1 < nr ? off[i] : 0.0;
+    }
+    double* G = &Ginv[(size_t)(l - 1) * nr2];
+    for (int j = 0; j < nr; ++j) {  // column j: the response to a unit forcing of node j
+      if (dead[j]) continue;
+      for (int i = 0; i < nr; ++i) y[i] = (i == j ? 1.0 : 0.0) - (i > 0 ? w[i] * y[i - 1] : 0.0);
+      double x = y[nr - 1] * ib[nr - 1];
+      G[(size_t)(nr - 1) * nr + j] = x;
+      for (int i = nr - 2; i >= 0; --i) {
+        x = (y[i] - (i + 1 < nr ? off[i] : 0.0) * x) * ib[i];
+        G[(size_t)i * nr + j] = x;
+      }
     }
   }
   toroidal_tridiag(h->r, h->mu, 1, diag, off, dead);
   int ns = 0;
   std::vector<double> wrot = toroidal_rotation_weights(h->r, h->mu, ns);
   std::vector<double> G1 = degree1_solution_map(diag, off, dead, wrot, nr, ns);
-  h->d_tw.upload(tw, s);
-  h->d_tib.upload(tib, s);
-  h->d_tc.upload(tc, s);
-  h->d_tG1.upload(G1, s);
+  std::copy(G1.begin(), G1.end(), Ginv.begin());
+  h->d_tGinv.upload(Ginv, s);
+  // forcing map per (degree, element): floc_t = sum_{s, m} K[t][s][m] tau_s^m, the
+  // 2-point Gauss quadrature of dissipative_rhs_tor (src/vilma_viscoelastic.f90:403-439)
+  // with the memory factored out
+  const int ne = h->ne;
+  std::vector<double> Kt((size_t)(L + 1) * ne * 12, 0.0);
+  const double xg = 0.5773502691896257;
+  for (int l = 1; l <= L; ++l) {
+    const double J = (double)l * (double)(l + 1);
+    const double nrm[2] = {0.5 * J, 0.5 * J * (J - 2.0)};
+    // unit-dof strain coefficients (strain_coeffs_tor of dW_e = 1, dW_{e+1} = 1)
+    const double sa[2][2] = {{-1.0, 0.0}, {1.0, 0.0}};
+    const double sb[2][2] = {{-1.0, J <= 2.0 ? 0.0 : 1.0}, {0.0, 0.0}};
+    const double sc[2][2] = {{0.0, 0.0}, {-1.0, J <= 2.0 ? 0.0 : 1.0}};
+    for (int e = 0; e < ne; ++e) {
+      const double rk = h->r[e], rk1 = h->r[e + 1], hh = rk1 - rk;
+      double* K = &Kt[((size_t)l * ne + e) * 12];
+      for (int ig = 0; ig < 2; ++ig) {
+        const double ra = 0.5 * (hh * (ig ? xg : -xg) + rk + rk1);
+        const double psik = (rk1 - ra) / hh, psik1 = (ra - rk) / hh;
+        const double phi[3] = {1.0 / hh, psik / ra, psik1 / ra};
+        for (int t = 0; t < 2; ++t)
+          for (int m = 0; m < 2; ++m) {
+            const double deps = sa[t][m] / hh + sb[t][m] * psik / ra + sc[t][m] * psik1 / ra;
+            for (int s3 = 0; s3 < 3; ++s3) K[(t * 3 + s3) * 2 + m] -= nrm[m] * phi[s3] * deps * ra * ra * hh * 0.5;
+          }
+      }
+    }
+  }
+  h->d_tK.upload(Kt, s);
   const size_t nmem = (size_t)6 * h->ne * 2 * nk, nd2 = (size_t)2 * nr * nk;
   h->d_tmem[0].alloc(nmem);
   h->d_tmem[1].alloc(nmem);
   h->d_dWn.alloc(nd2);
+  h->d_tg.alloc(nd2);
   h->d_dWa.alloc((size_t)2 * nk);
   if (h->p.scheme == VG_SCHEME_TRAP) {
     h->d_edWn.alloc(nd2);
@@ -162,106 +199,74 @@ struct TorDriftArgs {
   const double* mnorm;
   const unsigned long long* maxbits;
   double skip_tol;
-  const double *r, *Jr;
-  const int* kdeg;
-  const double *tw, *tib, *tc, *G1;
-  double *dWn, *dWa;
-  int ne, nr, nk, k1, n1;  // degree-1 slots k1 .. k1 + n1 - 1
+  const double* K;  // forcing maps (lmax + 1, ne, 12)
+  const int *kdeg, *kbeg;
+  const double* Ginv;
+  double *g, *dWn, *dWa;
+  int ne, nr, nk, lmax;
 };
 
-// dissipative_rhs_tor (src/vilma_viscoelastic.f90:403-439) of one element:
-// its forcing on the test dofs dW_e (f0) and dW_{e+1} (f1)
-__device__ __forceinline__ void element_floc_tor(const TorDriftArgs& A, int k, int ri, int e, double J, double& f0,
-                                                 double& f1) {
-  const double xg = 0.5773502691896257;
-  const double nrm[2] = {0.5 * J, 0.5 * J * (J - 2.0)};
-  double sa[2][2], sb[2][2], sc[2][2];
-  strain_coeffs_tor(1.0, 0.0, J, sa[0], sb[0], sc[0]);
-  strain_coeffs_tor(0.0, 1.0, J, sa[1], sb[1], sc[1]);
-  const double rk = A.r[e], rk1 = A.r[e + 1], h = rk1 - rk;
-  double Am[2], Bm[2], Cm[2];
+// g(node) = element node-1's second test dof + element node's first (the
+// reference's accumulation order) through the precomputed forcing maps; zero
+// for slots the gate skips, whose W (and W(a)) then come out zero
+__global__ void __launch_bounds__(128) k_drift_tor_rhs(TorDriftArgs A) {
+  const int k = blockIdx.x * 32 + threadIdx.x, node = blockIdx.y * 4 + threadIdx.y, ri = blockIdx.z;
+  if (k >= A.nk || node >= A.nr) return;
+  double g = 0.0;
+  if (!(A.mnorm[k] <= A.skip_tol * __longlong_as_double((long long)*A.maxbits))) {
+    const int l = A.kdeg[k];
 #pragma unroll
-  for (int m = 0; m < 2; ++m) {
-    Am[m] = A.tmem[tmem_idx(0, ri, e, m, k, A.ne, A.nk)];
-    Bm[m] = A.tmem[tmem_idx(1, ri, e, m, k, A.ne, A.nk)];
-    Cm[m] = A.tmem[tmem_idx(2, ri, e, m, k, A.ne, A.nk)];
-  }
-  double floc[2] = {0.0, 0.0};
+    for (int side = 0; side < 2; ++side) {  // element node - 1 (test dof 1), then element node (test dof 0)
+      const int e = node - 1 + side, t = 1 - side;
+      if (e < 0 || e >= A.ne) continue;
+      const double* K = A.K + ((size_t)l * A.ne + e) * 12 + t * 6;
+      double f = 0.0;
 #pragma unroll
-  for (int ig = 0; ig < 2; ++ig) {
-    const double ra = 0.5 * (h * (ig ? xg : -xg) + rk + rk1);
-    const double psik = (rk1 - ra) / h, psik1 = (ra - rk) / h;
-    double tauV[2];
+      for (int s3 = 0; s3 < 3; ++s3)
 #pragma unroll
-    for (int m = 0; m < 2; ++m) tauV[m] = Am[m] / h + Bm[m] * psik / ra + Cm[m] * psik1 / ra;
-#pragma unroll
-    for (int t = 0; t < 2; ++t) {
-      double D = 0.0;
-#pragma unroll
-      for (int m = 0; m < 2; ++m) {
-        const double deps = sa[t][m] / h + sb[t][m] * psik / ra + sc[t][m] * psik1 / ra;
-        D = D + nrm[m] * tauV[m] * deps;
-      }
-      floc[t] = floc[t] - D * ra * ra * h * 0.5;
+        for (int m = 0; m < 2; ++m) f = fma(__ldg(&K[s3 * 2 + m]), A.tmem[tmem_idx(s3, ri, e, m, k, A.ne, A.nk)], f);
+      g = g + f;
     }
   }
-  f0 = floc[0];
-  f1 = floc[1];
+  A.g[((size_t)ri * A.nr + node) * A.nk + k] = g;
 }
 
-__global__ void __launch_bounds__(128) k_drift_tor(TorDriftArgs A) {
-  const int k = blockIdx.x * blockDim.x + threadIdx.x, ri = blockIdx.y;
-  if (k >= A.nk) return;
-  double* W = A.dWn + (size_t)ri * A.nr * A.nk + k;  // node i at W[i * nk]
-  const size_t nk = A.nk;
-  const double thr = A.skip_tol * __longlong_as_double((long long)*A.maxbits);
-  if (A.mnorm[k] <= thr) {  // negligible memory => negligible drift
-    for (int i = 0; i < A.nr; ++i) W[i * nk] = 0.0;
-    A.dWa[(size_t)ri * nk + k] = 0.0;
-    return;
-  }
-  const int l = A.kdeg[k];
-  const double J = A.Jr[l];
-  const double* w = A.tw + (size_t)l * A.nr;
-  double prev1 = 0.0, y = 0.0;
-  for (int i = 0; i < A.nr; ++i) {
-    double f0 = 0.0, f1 = 0.0;
-    if (i < A.ne) element_floc_tor(A, k, ri, i, J, f0, f1);
-    const double g = prev1 + f0;  // element i - 1's second test dof, then element i's first
-    prev1 = f1;
-    y = (l == 1) ? g : g - __ldg(&w[i]) * y;
-    W[i * nk] = y;
-  }
-  if (l == 1) return;  // k_drift_tor1 applies the bordered solution map
-  const double* ib = A.tib + (size_t)l * A.nr;
-  const double* c = A.tc + (size_t)l * A.nr;
-  double x = W[(size_t)(A.nr - 1) * nk] * __ldg(&ib[A.nr - 1]);
-  W[(size_t)(A.nr - 1) * nk] = x;
-  A.dWa[(size_t)ri * nk + k] = x;
-  for (int i = A.nr - 2; i >= 0; --i) {
-    x = (W[i * nk] - __ldg(&c[i]) * x) * __ldg(&ib[i]);
-    W[i * nk] = x;
-  }
-}
-
-// degree 1: W = G1W g for each (slot, re/im) that the gate let through
-__global__ void __launch_bounds__(256) k_drift_tor1(TorDriftArgs A) {
-  extern __shared__ double g[];  // nr
-  const double thr = A.skip_tol * __longlong_as_double((long long)*A.maxbits);
-  const size_t nk = A.nk;
-  for (int q = 0; q < 2 * A.n1; ++q) {
-    const int k = A.k1 + q / 2, ri = q % 2;
-    if (A.mnorm[k] <= thr) continue;  // k_drift_tor zeroed it
-    double* W = A.dWn + (size_t)ri * A.nr * nk + k;
-    __syncthreads();
-    for (int i = threadIdx.x; i < A.nr; i += blockDim.x) g[i] = W[i * nk];
-    __syncthreads();
-    for (int i = threadIdx.x; i < A.nr; i += blockDim.x) {
-      const double* row = A.G1 + (size_t)i * A.nr;
-      double acc = 0.0;
-      for (int j = 0; j < A.nr; ++j) acc += __ldg(&row[j]) * g[j];
-      W[i * nk] = acc;
-      if (i == A.nr - 1) A.dWa[(size_t)ri * nk + k] = acc;
+// W = G_l g over the 2 (l + 1) columns (slot, re/im) of degree l = blockIdx.y + 1,
+// TOR_MC columns per CTA; the forcing tile [node][column] in shared memory, each
+// thread TOR_RB rows of one column
+constexpr int TOR_MC = 16, TOR_MR = 16, TOR_RB = 4;
+__global__ void __launch_bounds__(TOR_MC * TOR_MR) k_drift_tor_mm(TorDriftArgs A) {
+  extern __shared__ double gs[];  // [nr][TOR_MC]
+  const int l = blockIdx.y + 1, n0 = blockIdx.x * TOR_MC;
+  const int k0 = A.kbeg[l], ncol = 2 * (A.kbeg[l + 1] - k0);
+  if (n0 >= ncol) return;
+  const int c = threadIdx.x % TOR_MC, rg = threadIdx.x / TOR_MC;
+  const int n = n0 + c, k = k0 + n / 2, ri = n % 2;
+  const bool live = n < ncol;
+  for (int j = rg; j < A.nr; j += TOR_MR)
+    gs[j * TOR_MC + c] = live ? A.g[((size_t)ri * A.nr + j) * A.nk + k] : 0.0;
+  __syncthreads();
+  if (!live) return;
+  const double* G = A.Ginv + (size_t)(l - 1) * A.nr * A.nr;
+  for (int i0 = rg * TOR_RB; i0 < A.nr; i0 += TOR_MR * TOR_RB) {
+    const double* row[TOR_RB];
+    double acc[TOR_RB];
+#pragma unroll
+    for (int b = 0; b < TOR_RB; ++b) {
+      row[b] = G + (size_t)min(i0 + b, A.nr - 1) * A.nr;
+      acc[b] = 0.0;
+    }
+    for (int j = 0; j < A.nr; ++j) {
+      const double gj = gs[j * TOR_MC + c];
+#pragma unroll
+      for (int b = 0; b < TOR_RB; ++b) acc[b] = fma(__ldg(&row[b][j]), gj, acc[b]);
+    }
+#pragma unroll
+    for (int b = 0; b < TOR_RB; ++b) {
+      const int i = i0 + b;
+      if (i >= A.nr) break;
+      A.dWn[((size_t)ri * A.nr + i) * A.nk + k] = acc[b];
+      if (i == A.nr - 1) A.dWa[(size_t)ri * A.nk + k] = acc[b];
     }
   }
 }
@@ -272,24 +277,29 @@ void launch_drift_tor(vg_handle* h, int buf, double* dWn) {
   A.mnorm = h->d_mnorm.p + (size_t)buf * h->nk;
   A.maxbits = h->d_maxbits.p + buf;
   A.skip_tol = h->p.skip_tol;
-  A.r = h->d_r.p;
-  A.Jr = h->d_Jr.p;
+  A.K = h->d_tK.p;
   A.kdeg = h->d_kdeg.p;
-  A.tw = h->d_tw.p;
-  A.tib = h->d_tib.p;
-  A.tc = h->d_tc.p;
-  A.G1 = h->d_tG1.p;
+  A.kbeg = h->d_kbeg.p;
+  A.Ginv = h->d_tGinv.p;
+  A.g = h->d_tg.p;
   A.dWn = dWn ? dWn : h->d_dWn.p;
   A.dWa = h->d_dWa.p;
   A.ne = h->ne;
   A.nr = h->nr;
   A.nk = h->nk;
-  A.k1 = h->kbeg_h[1];
-  A.n1 = h->kbeg_h[2] - h->kbeg_h[1];
-  k_drift_tor<<<dim3((h->nk + 127) / 128, 2), 128, 0, h->stream>>>(A);
+  A.lmax = h->grid.lmax;
+  k_drift_tor_rhs<<<dim3((h->nk + 31) / 32, (h->nr + 3) / 4, 2), dim3(32, 4), 0, h->stream>>>(A);
   ++h->n_launch;
   VG_CUDA(cudaGetLastError());
-  k_drift_tor1<<<1, 256, (size_t)h->nr * sizeof(double), h->stream>>>(A);
+  const size_t smem = (size_t)h->nr * TOR_MC * sizeof(double);
+  static bool attr = false;
+  if (!attr) {
+    VG_CUDA(cudaFuncSetAttribute(k_drift_tor_mm, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024));
+    attr = true;
+  }
+  if (smem > 96 * 1024) throw Error("toroidal drift: too many radial nodes for the shared forcing tile");
+  const int nchunk = (2 * (h->grid.lmax + 1) + TOR_MC - 1) / TOR_MC;
+  k_drift_tor_mm<<<dim3(nchunk, h->grid.lmax), TOR_MC * TOR_MR, smem, h->stream>>>(A);
   ++h->n_launch;
   VG_CUDA(cudaGetLastError());
 }

@@ -417,20 +417,29 @@ __device__ __forceinline__ void lon_anal(const double* __restrict__ X, int nfl, 
   }
 }
 
+// the coefficient region of the toroidal longitude pass: [6 LF][2 M2] for
+// the synthesis, [m][10][2 LF] for the analysis inputs
+__host__ __device__ __forceinline__ size_t lon_areg(int LF, const LonTables& T) {
+  const size_t a6 = (size_t)6 * LF * 2 * T.M2, a10 = (size_t)10 * 2 * LF * T.M;
+  return a6 > a10 ? a6 : a10;
+}
+
 constexpr int LON_THREADS = 384;
 constexpr int LON_LF = 3;  // fields per CTA: one element's three shape coefficients (two CTAs per SM)
+constexpr int LON_LF_TOR = 3;  // with the toroidal channels: staged in two halves, two CTAs per SM
 
 // the CTA's slice of the products S[m][j][q][f][ri] (fields f0 .. f0 + nft - 1,
 // a contiguous run of 2 nft doubles per (m, q)) to and from shared [m][q][2 nft]
 // (16-byte cp.async pieces, all in flight together; ncf and 2 f0 are even)
-template <int NQ = 6>
+// products q0 .. q0 + NS - 1 of the NQ per (m, j), staged as [m][q - q0][2 nft]
+template <int NQ = 6, int NS = NQ>
 __device__ __forceinline__ void stage_in(const double* __restrict__ S, double* __restrict__ X, int nlat, int ncf,
-                                         int j, int f0, int nft, int M) {
-  const int n = M * NQ * nft;
+                                         int j, int f0, int nft, int M, int q0 = 0) {
+  const int n = M * NS * nft;
   for (int t = threadIdx.x; t < n; t += blockDim.x) {
     const int mq = t / nft, c = t % nft;
     lon_cp16(X + (size_t)mq * 2 * nft + 2 * c,
-             S + ((size_t)(mq / NQ) * nlat + j) * NQ * ncf + (size_t)(mq % NQ) * ncf + 2 * f0 + 2 * c);
+             S + ((size_t)(mq / NS) * nlat + j) * NQ * ncf + (size_t)(q0 + mq % NS) * ncf + 2 * f0 + 2 * c);
   }
   lon_commit();
   lon_wait<0>();
@@ -459,44 +468,55 @@ __global__ void __launch_bounds__(LON_THREADS, 1)
   const int j = blockIdx.x, f0 = blockIdx.y * LF;
   const int nft = min(LF, nf - f0);
   const int ncf = 2 * nf, half = T.half, wA = 2 * T.M2;
-  double* A = sm;                          // [6 LF][2 M2]; [m][q][2 nft] for the analysis inputs
-  double* X = sm + (size_t)NQ * LF * wA;   // [6 LF][nphi]; [m][q][2 nft] for the synthesis products
+  double* A = sm;  // [6 LF][2 M2]; [m][q][2 nft] for the analysis inputs
+  double* X = sm + (NQ == 6 ? (size_t)6 * LF * wA : lon_areg(LF, T));  // [6 LF][nphi]; staged products
   const double is = invsin[j];
   // 1. the CTA's synthesis products, staged in X as [m][q][2 nft] (contiguous
-  //    runs of 2 nft doubles in S), then the dyadic coefficients rr, rt, rp,
-  //    tt, pp, tp with the synthesis weights (1 at m = 0, 2 above), zero past M
-  stage_in<NQ>(S, X, nlat, ncf, j, f0, nft, T.M);
+  //    runs of 2 nft doubles in S; the spheroidal six, then the toroidal four),
+  //    then the dyadic coefficients rr, rt, rp, tt, pp, tp with the synthesis
+  //    weights (1 at m = 0, 2 above), zero past M
+  stage_in<NQ, 6>(S, X, nlat, ncf, j, f0, nft, T.M);
   __syncthreads();
   for (int t = threadIdx.x; t < nft * T.M2; t += blockDim.x) {
     const int fl = t / T.M2, m = t % T.M2;
-    double pr[NQ][2];
-    for (int q = 0; q < NQ; ++q)
-      for (int ri = 0; ri < 2; ++ri) pr[q][ri] = (m < T.M) ? X[((size_t)m * NQ + q) * 2 * nft + 2 * fl + ri] : 0.0;
+    double pr[6][2];
+    for (int q = 0; q < 6; ++q)
+      for (int ri = 0; ri < 2; ++ri) pr[q][ri] = (m < T.M) ? X[((size_t)m * 6 + q) * 2 * nft + 2 * fl + ri] : 0.0;
     const double ms = m * is, w = (m == 0) ? 1.0 : 2.0;
-    double comp[6][2] = {{pr[0][0], pr[0][1]},
-                         {pr[1][0], pr[1][1]},
-                         {-ms * pr[2][1], ms * pr[2][0]},             // i (m / sin) P.X1
-                         {pr[3][0] + pr[4][0], pr[3][1] + pr[4][1]},  // TT + PP
-                         {pr[3][0] - pr[4][0], pr[3][1] - pr[4][1]},  // TT - PP
-                         {-4.0 * pr[5][1], 4.0 * pr[5][0]}};          // 4 i H.X3
-    if (NQ == 10) {  // Z3: (rt, rp) += e_r x grad_1 = (-i (m/sin) P.X4, D.X4); Z4: (tt, pp, tp) += (-Sh, Sh, Sg)
-      comp[1][0] += ms * pr[6][1];
-      comp[1][1] -= ms * pr[6][0];
-      comp[2][0] += pr[7][0];
-      comp[2][1] += pr[7][1];
-      comp[3][0] += pr[9][1];  // -i H.X5
-      comp[3][1] -= pr[9][0];
-      comp[4][0] -= pr[9][1];  // +i H.X5
-      comp[4][1] += pr[9][0];
-      comp[5][0] += pr[8][0];  // G.X5
-      comp[5][1] += pr[8][1];
-    }
+    const double comp[6][2] = {{pr[0][0], pr[0][1]},
+                               {pr[1][0], pr[1][1]},
+                               {-ms * pr[2][1], ms * pr[2][0]},             // i (m / sin) P.X1
+                               {pr[3][0] + pr[4][0], pr[3][1] + pr[4][1]},  // TT + PP
+                               {pr[3][0] - pr[4][0], pr[3][1] - pr[4][1]},  // TT - PP
+                               {-4.0 * pr[5][1], 4.0 * pr[5][0]}};          // 4 i H.X3
     for (int c = 0; c < 6; ++c) {
       A[(size_t)(fl * 6 + c) * wA + 2 * m] = w * comp[c][0];
       A[(size_t)(fl * 6 + c) * wA + 2 * m + 1] = w * comp[c][1];
     }
   }
   __syncthreads();
+  if (NQ == 10) {  // Z3: (rt, rp) += e_r x grad_1 = (-i (m/sin) P.X4, D.X4); Z4: (tt, pp, tp) += (-Sh, Sh, Sg)
+    stage_in<NQ, 4>(S, X, nlat, ncf, j, f0, nft, T.M, 6);
+    __syncthreads();
+    for (int t = threadIdx.x; t < nft * T.M; t += blockDim.x) {
+      const int fl = t / T.M, m = t % T.M;
+      double pr[4][2];
+      for (int q = 0; q < 4; ++q)
+        for (int ri = 0; ri < 2; ++ri) pr[q][ri] = X[((size_t)m * 4 + q) * 2 * nft + 2 * fl + ri];
+      const double ms = m * is, w = (m == 0) ? 1.0 : 2.0;
+      const double add[6][2] = {{0.0, 0.0},
+                                {ms * pr[0][1], -ms * pr[0][0]},  // -i (m/sin) P.X4
+                                {pr[1][0], pr[1][1]},             // D.X4
+                                {pr[3][1], -pr[3][0]},            // -i H.X5
+                                {-pr[3][1], pr[3][0]},            // +i H.X5
+                                {pr[2][0], pr[2][1]}};            // G.X5
+      for (int c = 1; c < 6; ++c) {
+        A[(size_t)(fl * 6 + c) * wA + 2 * m] += w * add[c][0];
+        A[(size_t)(fl * 6 + c) * wA + 2 * m + 1] += w * add[c][1];
+      }
+    }
+    __syncthreads();
+  }
   // 2. synthesis, times -M dt, and the parity combinations of the analysis
   lon_synth(A, nft, T, [&](int fl, int i, const double* g1, const double* g2) {
     const int f = f0 + fl;
@@ -546,13 +566,13 @@ __global__ void __launch_bounds__(LON_THREADS, 1)
 }
 
 // shared memory of the longitude pass (forward: adj = 0) and its transpose;
-// nq analysis inputs (10 with the toroidal channels)
+// nq analysis inputs (10 with the toroidal channels, staged through the
+// coefficient region, which then grows to hold them)
 static size_t lon_smem(const vg_handle* h, int LF, bool adj, int nq = 6) {
   const LonTables T = lon_tables(h);
   const int nphi = h->grid.nphi;
-  const size_t a = (size_t)nq * LF * 2 * T.M2;
-  const size_t x = std::max((size_t)6 * LF * nphi, (size_t)nq * 2 * T.M * LF);
-  return (a + x + (adj ? (size_t)LF * nphi : 0)) * sizeof(double);
+  const size_t a = nq == 6 ? (size_t)6 * LF * 2 * T.M2 : lon_areg(LF, T);
+  return (a + (size_t)6 * LF * nphi + (adj ? (size_t)LF * nphi : 0)) * sizeof(double);
 }
 
 static int lon_threads(const vg_handle* h, int LF) {
@@ -565,7 +585,7 @@ constexpr size_t LON_SMEM_MAX = 220 * 1024;
 static void lon_attributes();  // the longitude kernels' shared-memory limit (defined after the transpose)
 
 static void lon_check(const vg_handle* h) {
-  if (lon_smem(h, LON_LF, true) > LON_SMEM_MAX || lon_smem(h, LON_LF, false, h->tor_on ? 10 : 6) > LON_SMEM_MAX)
+  if (lon_smem(h, LON_LF, true) > LON_SMEM_MAX || (h->tor_on && lon_smem(h, LON_LF_TOR, false, 10) > LON_SMEM_MAX))
     throw Error("visc3d: grid too large for the FP64 longitude pass");
 }
 
@@ -803,8 +823,10 @@ void visc3d_advance(vg_handle* h, const double* d_sigma, double dt, const double
     PhaseScope pp(h, VG_PH_V3_LON_INV);
     const dim3 lg(G.nlat, (nf + LON_LF - 1) / LON_LF);
     if (h->tor_on)
-      k_v3_lon<LON_LF, 10><<<lg, lon_threads(h, LON_LF), lon_smem(h, LON_LF, false, 10), s>>>(
-          h->d_Y.p, G.nlat, G.nphi, nf, dt, h->d_MkPerDt3.p, lon_tables(h), G.d_invsin.p, nullptr, trap ? 1 : 0);
+      k_v3_lon<LON_LF_TOR, 10>
+          <<<dim3(G.nlat, (nf + LON_LF_TOR - 1) / LON_LF_TOR), lon_threads(h, LON_LF_TOR),
+             lon_smem(h, LON_LF_TOR, false, 10), s>>>(h->d_Y.p, G.nlat, G.nphi, nf, dt, h->d_MkPerDt3.p,
+                                                      lon_tables(h), G.d_invsin.p, nullptr, trap ? 1 : 0);
     else
       k_v3_lon<LON_LF><<<lg, lon_threads(h, LON_LF), lon_smem(h, LON_LF, false), s>>>(
           h->d_Y.p, G.nlat, G.nphi, nf, dt, h->d_MkPerDt3.p, lon_tables(h), G.d_invsin.p, h->v3_gstore,
@@ -1005,7 +1027,7 @@ __global__ void __launch_bounds__(256) k_v3_gather_T(V3Args A, const double* __r
 
 static void lon_attributes() {
   for (const void* k :
-       {(const void*)k_v3_lon<LON_LF>, (const void*)k_v3_lon<LON_LF, 10>, (const void*)k_v3_lon_T<LON_LF>})
+       {(const void*)k_v3_lon<LON_LF>, (const void*)k_v3_lon<LON_LF_TOR, 10>, (const void*)k_v3_lon_T<LON_LF>})
     VG_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)LON_SMEM_MAX));
 }
 
