@@ -7,6 +7,10 @@ C-ABI. Prints one JSON line (rank 0).
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
                   [--workload NAME]
 
+--workload c4_ensemble times the batched ensemble (32 instances advanced
+together through vg_update_batch) against the same instances run one after
+the other.
+
 Multi-GPU: instances are independent (no collective on the data path), so N
 ranks run N replicas of the workload ("scaling": "weak"); value = total steps
 of all ranks / max-over-ranks device time.
@@ -375,8 +379,124 @@ def roofline(w, arm, pk, pk_kind, split):
             "traffic": None, "algorithmic_flops_per_launch": amount / 3.0}
 
 
+def run_ensemble(args):
+    """The batched ensemble (32 instances of mixed lmax, earth and viscosity,
+    half with 3-D viscosity on the split tensor-core path), advanced together
+    through vg_update_batch, against the same instances run one after the other
+    on the plain FP64 path ("32 sequential plain runs") and, to separate the
+    concurrency from the precision, sequentially on the batched precision.
+    value = instance-steps/s of the batched run."""
+    import torch
+
+    from fastearth3d_b200 import lib as vlib
+
+    members = synth.ensemble()
+    n, W, K = len(members), args.warmup, args.steps
+    DT = members[0].dt_yr
+    ice = [[np.ascontiguousarray(mb.ice_at(s + 1)) for s in range(W + K + 1)] for mb in members]
+    ice_dev = [torch.tensor(np.stack(x), device="cuda") for x in ice]
+
+    def make(mb, split):
+        p = mb.params(vlib.default_params)
+        p.visc3d_precision = 1 if (split and mb.visc3d) else 0
+        m = vlib.Model(p)
+        zb, hi = mb.reference()
+        m.set_reference(zb, hi)
+        if mb.visc3d:
+            m.enable_visc3d(mb.pert(m.p))
+        return m
+
+    def dev_timed(fn):
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        fn()
+        torch.cuda.synchronize()
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1)
+
+    # batched, split precision for the 3-D instances
+    models = [make(mb, True) for mb in members]
+    for s in range(W):
+        vlib.update_batch(models, [ice_dev[i][s].data_ptr() for i in range(n)], DT, on_device=True)
+    launches0 = sum(m.info().n_launch for m in models)
+    with ClockSampler(0) as clk:
+        ms_batch = dev_timed(lambda: [vlib.update_batch(models, [ice_dev[i][s].data_ptr() for i in range(n)], DT,
+                                                         on_device=True) for s in range(W, W + K)])
+    launches = sum(m.info().n_launch for m in models) - launches0
+    rsl_batch = [m.fields()[0] for m in models]
+    # end to end: host ice in, every instance's rsl out, each step
+    ng_tot = sum(mb.nlat * mb.nphi for mb in members)
+    rsl_out = [np.zeros(mb.nlat * mb.nphi) for mb in members]
+
+    def e2e_step():
+        vlib.update_batch(models, [ice[i][W + K] for i in range(n)], DT)
+        for i, m in enumerate(models):
+            vlib.lib().vg_get_fields(m.h, vlib.ptr(rsl_out[i]), None, None, None)
+
+    ms_e2e = dev_timed(e2e_step)
+    del models
+    torch.cuda.synchronize()
+    # sequential: each instance's W + K steps, alone, one instance after another
+    seq = {}
+    for split in (False, True):
+        tot, rsl_seq = 0.0, []
+        for i, mb in enumerate(members):
+            m = make(mb, split)
+            for s in range(W):
+                m.update_device(ice_dev[i][s].data_ptr(), DT)
+            tot += dev_timed(lambda: [m.update_device(ice_dev[i][s].data_ptr(), DT) for s in range(W, W + K)])
+            rsl_seq.append(m.fields()[0])
+            del m
+        seq[split] = (tot, rsl_seq)
+    same = all(np.array_equal(a, b) for a, b in zip(rsl_batch, seq[True][1]))
+    worst = max(float(np.abs(a - b).max() / np.abs(b).max()) for a, b, mb in zip(rsl_batch, seq[False][1], members)
+                if mb.visc3d)
+    lm = sorted({mb.lmax for mb in members})
+    out = {
+        "metric": "instance-steps/s, batched ensemble of %d (lmax %s, half 3-D) vs %d sequential plain runs" % (
+            n, "/".join(map(str, lm)), n),
+        "value": n * K / (ms_batch / 1e3),
+        "unit": "instance-steps/s",
+        "n_gpus": 1,
+        "steps": K,
+        "warmup": W,
+        "ms_per_step": ms_batch / K,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "tf32x3 3-D stress products of the 3-D instances, f64 elsewhere",
+        "data": "synthetic",
+        "config": {"workload": "c4_ensemble", "instances": n, "lmax": [mb.lmax for mb in members],
+                   "visc3d": [bool(mb.visc3d) for mb in members], "radial_elements": [mb.n_elem for mb in members],
+                   "dt_yr": DT, "sea_level": True, "parallelism": "one stream and one host thread per instance"},
+        "sequential_plain_fp64": {"value": n * K / (seq[False][0] / 1e3), "unit": "instance-steps/s",
+                                  "ms_total": seq[False][0]},
+        "sequential_same_precision": {"value": n * K / (seq[True][0] / 1e3), "unit": "instance-steps/s",
+                                      "ms_total": seq[True][0]},
+        "speedup_vs_sequential_plain": seq[False][0] / ms_batch,
+        "speedup_from_concurrency": seq[True][0] / ms_batch,
+        "batched_equals_sequential": bool(same),
+        "split_rsl_error_vs_fp64_3d_instances": worst,
+        "e2e": {"value": n / (ms_e2e / 1e3), "unit": "instance-steps/s", "h2d_bytes_per_step": ng_tot * 8,
+                "d2h_bytes_per_step": ng_tot * 8},
+        "gpu_launches": int(launches),
+        "clocks": clk.summary(),
+        "cpu_baseline": None,
+        "cpu_baseline_note": "not sampled: one oracle step of the lmax-256 3-D instances alone takes minutes",
+    }
+    print(json.dumps(out))
+
+
 def main():
     args = parse()
+    if args.workload == "c4_ensemble":
+        import torch
+
+        torch.cuda.set_device(0)
+        run_ensemble(args)
+        return
     w = synth.workloads()[args.workload]
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))

@@ -697,7 +697,7 @@ double misfit_grad_dev(vg_handle* h, int nsteps, double dt, const double* sigma,
   }
   const size_t shm1 = (size_t)(4 * (2 * nr + 1) + 4 * 2 * nr) * sizeof(double);
   const size_t ts_smem = (size_t)TS_WARPS * TS_WARP * sizeof(double);
-  static bool ts_attr = false;
+  static std::atomic<bool> ts_attr{false};  // set once; concurrent handles may race to it
   if (!ts_attr) {
     VG_CUDA(cudaFuncSetAttribute(k_drift_T, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ts_smem));
     ts_attr = true;

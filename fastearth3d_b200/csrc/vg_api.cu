@@ -1,9 +1,15 @@
 // C-ABI entry points (include/vilma_gpu.h). Every call returns an int status;
 // failures are caught here and their message is kept for vg_last_error. No
 // exit or abort inside the library.
+#include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstring>
+#include <map>
+#include <mutex>
 #include <string>
+#include <thread>
+#include <vector>
 
 #include "vg_internal.cuh"
 
@@ -32,6 +38,16 @@ static void need(vg_handle* h, bool cond, const char* msg) {
 }
 
 namespace vg {
+void raise_smem_limit(const void* kernel, size_t bytes) {
+  static std::mutex mu;
+  static std::map<const void*, size_t> limit;
+  std::lock_guard<std::mutex> lock(mu);
+  size_t& cur = limit[kernel];
+  if (bytes <= cur) return;
+  VG_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+  cur = bytes;
+}
+
 PhaseScope::PhaseScope(vg_handle* hh, int p) : h(hh), ph(p) {
   if (!h->prof.on) return;
   cudaEvent_t e;
@@ -199,6 +215,56 @@ int vg_update(vg_handle* h, const double* h_ice, double dt_yr) {
     vg::update_dev(h, h->d_ice1.p, dt_yr);
     VG_CUDA(cudaStreamSynchronize(h->stream));
   });
+}
+
+int vg_update_batch(vg_handle* const* hs, int n, const double* const* ice, int ice_on_device, double dt_yr,
+                    int nthreads, int* failed_index) {
+  if (failed_index) *failed_index = -1;
+  const int arg = guarded(nullptr, [&] {
+    need(nullptr, n >= 0, "vg_update_batch: n must be >= 0");
+    need(nullptr, n == 0 || (hs != nullptr && ice != nullptr), "vg_update_batch: null argument");
+    std::vector<vg_handle*> seen(hs, hs + n);
+    std::sort(seen.begin(), seen.end());
+    for (int i = 0; i < n; ++i) {
+      need(nullptr, seen[i] != nullptr, "vg_update_batch: null handle");
+      need(nullptr, i == 0 || seen[i] != seen[i - 1], "vg_update_batch: a handle appears twice");
+    }
+  });
+  if (arg != 0) return arg;
+  if (n == 0) return 0;
+  // costliest first (state size; 3-D elements weigh in with the transforms)
+  std::vector<int> order(n);
+  std::vector<double> cost(n);
+  for (int i = 0; i < n; ++i) {
+    order[i] = i;
+    cost[i] = (double)hs[i]->nk * hs[i]->ne * (1.0 + 4.0 * hs[i]->ne3d / std::max(hs[i]->ne, 1));
+  }
+  std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return cost[a] > cost[b]; });
+  std::vector<int> rc(n, 0);
+  std::atomic<int> next{0};
+  auto work = [&] {
+    for (int t = next++; t < n; t = next++) {
+      const int i = order[t];
+      vg_handle* h = hs[i];
+      if (cudaSetDevice(h->device) != cudaSuccess) {
+        h->err = "vg_update_batch: cudaSetDevice failed";
+        rc[i] = 1;
+        continue;
+      }
+      rc[i] = ice_on_device ? vg_update_device(h, ice[i], dt_yr) : vg_update(h, ice[i], dt_yr);
+    }
+  };
+  const int nt = std::min(n, nthreads <= 0 ? n : nthreads);
+  std::vector<std::thread> pool;
+  pool.reserve(nt);
+  for (int t = 0; t < nt; ++t) pool.emplace_back(work);
+  for (std::thread& th : pool) th.join();
+  for (int i = 0; i < n; ++i)
+    if (rc[i] != 0) {
+      if (failed_index) *failed_index = i;
+      return rc[i];
+    }
+  return 0;
 }
 
 int vg_get_fields(vg_handle* h, double* rsl, double* z_bed, double* C, double* sigma_lm) {

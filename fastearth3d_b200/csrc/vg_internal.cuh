@@ -13,6 +13,7 @@
 //   Legendre       plm/dplm[lm][j] (j fastest), lm m-major
 #pragma once
 #include <cuda_runtime.h>
+#include <atomic>
 
 #include <cmath>
 #include <cstdint>
@@ -310,6 +311,10 @@ void trap_coarse_fine_error(vg_handle* h, double& err_inf, double& tau_inf);
 void trap_prime(vg_handle* h);
 // misc
 void sync_scalars(vg_handle* h);
+// Raise a kernel's dynamic shared-memory limit to at least `bytes`, never
+// lowering it: handles of different sizes share the kernel, and may launch it
+// concurrently from different host threads (vg_update_batch).
+void raise_smem_limit(const void* kernel, size_t bytes);
 // phase timer scope: records a start event now and a stop event at scope exit
 struct PhaseScope {
   vg_handle* h;

@@ -472,7 +472,7 @@ void launch_drift(vg_handle* h, int buf, double* dUn, double* dVn, double* dWn) 
   ++h->n_launch;
   VG_CUDA(cudaGetLastError());
   const size_t sw_smem = (size_t)SW_WARPS * SW_WARP * sizeof(double);
-  static bool sw_attr = false;
+  static std::atomic<bool> sw_attr{false};  // set once; concurrent handles may race to it
   if (!sw_attr) {
     VG_CUDA(cudaFuncSetAttribute(k_drift_solve, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sw_smem));
     sw_attr = true;

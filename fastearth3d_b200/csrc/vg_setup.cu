@@ -893,8 +893,7 @@ void setup_handle(vg_handle* h) {
                                                    h->d_xVn.p);
   VG_CUDA(cudaGetLastError());
   size_t shm = 2 * (size_t)h->ns1 * sizeof(double);
-  if (shm > 48 * 1024)
-    VG_CUDA(cudaFuncSetAttribute(k_unit_load_deg1, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm));
+  if (shm > 48 * 1024) raise_smem_limit((const void*)k_unit_load_deg1, shm);
   k_unit_load_deg1<<<1, 512, shm, s>>>(nr, nd, p.r_earth, h->g, p.deg1_cm, h->d_ab1.p, h->ldab1, h->kl1, h->kv1,
                                        h->d_ipiv1.p, h->d_dr1.p, h->d_dc1.p, h->d_null1.p, h->d_gu.p, h->d_gn.p,
                                        h->d_gv.p, h->d_xUn.p, h->d_xVn.p);

@@ -657,7 +657,7 @@ static void launch_inner_loop(vg_handle* h) {
     VG_CUDA(cudaGetDevice(&dev));
     VG_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
     const size_t shm = sle_inner_smem(h);
-    VG_CUDA(cudaFuncSetAttribute(k_sle_inner, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm));
+    raise_smem_limit((const void*)k_sle_inner, shm);
     VG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_sle_inner, 512, shm));
     if (per_sm < 1) throw Error("sle_solve: the fused inner loop does not fit on an SM");
     h->sle_grid = nsm;

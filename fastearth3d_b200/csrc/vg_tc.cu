@@ -877,7 +877,7 @@ void visc3d_tc_enable(vg_handle* h) {
   a.status = h->d_maxbits.p + 2;
   P->ntile_rows_nc = (NC + tc::TM - 1) / tc::TM;
   P->ntile_rows_col = (NCOL + tc::TM - 1) / tc::TM;
-  static bool attr = false;
+  static std::atomic<bool> attr{false};  // set once; concurrent handles may race to it
   if (!attr) {
     VG_CUDA(cudaFuncSetAttribute(tc::k_tc_stage<tc::ST_SYNTH>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tc::SMEM_BYTES));
     VG_CUDA(cudaFuncSetAttribute(tc::k_tc_stage<tc::ST_INV>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tc::SMEM_BYTES));

@@ -292,7 +292,7 @@ void launch_drift_tor(vg_handle* h, int buf, double* dWn) {
   ++h->n_launch;
   VG_CUDA(cudaGetLastError());
   const size_t smem = (size_t)h->nr * TOR_MC * sizeof(double);
-  static bool attr = false;
+  static std::atomic<bool> attr{false};  // set once; concurrent handles may race to it
   if (!attr) {
     VG_CUDA(cudaFuncSetAttribute(k_drift_tor_mm, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024));
     attr = true;

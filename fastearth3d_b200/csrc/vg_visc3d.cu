@@ -640,7 +640,7 @@ __global__ void __launch_bounds__(256) k_v3_scatter(V3Args A, const T* __restric
 
 // the gather tile (the FP64 one is above the default 48 KB)
 static void v3_tile_attributes() {
-  static bool done = false;
+  static std::atomic<bool> done{false};  // set once; concurrent handles may race to it
   if (done) return;
   VG_CUDA(cudaFuncSetAttribute(k_v3_gather<double, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                (int)v3_gather_smem<double>()));

@@ -41,6 +41,8 @@ _SIGS = [
     ("vg_get_rotation_state", [_VP, _P, _P, _P]),
     ("vg_get_step_state", [_VP, _P, _P, C.POINTER(C.c_int)]),
     ("vg_get_toroidal", [_VP, _P]),
+    ("vg_update_batch", [C.POINTER(_VP), C.c_int, C.POINTER(_P), C.c_int, C.c_double, C.c_int,
+                         C.POINTER(C.c_int)]),
     ("vg_get_state_tor", [_VP, _P, _P, _P, _P, _P, _P, C.POINTER(C.c_int)]),
     ("vg_set_state_tor", [_VP, _P, _P, _P, _P, _P, _P]),
     ("vg_set_step_state", [_VP, C.c_double, _P, C.c_int]),
@@ -311,3 +313,21 @@ class Model:
         f = np.zeros(self.ng)
         self._c(lib().vg_sht_synthesis(self.h, ptr(s), ptr(f)))
         return f
+
+
+def update_batch(models, ices, dt_yr, on_device=False, nthreads=0):
+    """Advance independent models together (vg_update_batch): ices[i] is model
+    i's ice, a host array (or, on_device, a device pointer as an int)."""
+    n = len(models)
+    hs = (_VP * n)(*[m.h for m in models])
+    if on_device:
+        arr = (_P * n)(*[C.cast(int(p), _P) for p in ices])
+    else:
+        keep = [np.ascontiguousarray(x, dtype=np.float64) for x in ices]
+        arr = (_P * n)(*[ptr(x) for x in keep])
+    failed = C.c_int(-1)
+    rc = lib().vg_update_batch(hs, n, arr, 1 if on_device else 0, dt_yr, nthreads, C.byref(failed))
+    if rc != 0:
+        i = failed.value
+        msg = lib().vg_last_error(models[i].h if i >= 0 else None).decode()
+        raise VilmaError(f"vg_update_batch: instance {i}: {msg}")

@@ -184,6 +184,45 @@ class Workload:
         return out
 
 
+class EnsembleMember(Workload):
+    """One instance of the batched ensemble: its own lmax, lithosphere
+    thickness and mantle viscosities on the 4-layer earth above (radii,
+    densities and shear moduli kept), seeded ice and topography, and, for
+    half the instances, the lateral viscosity field of the 3-D workload."""
+
+    def __init__(self, name, lmax, n_elem, litho_km, eta_um, eta_lm, visc3d, seed):
+        self.litho_km, self.eta_um, self.eta_lm = litho_km, eta_um, eta_lm
+        super().__init__(name, lmax, n_elem, 50.0, 2000, 6, "sawtooth", sle=True, visc3d=visc3d, seed=seed)
+
+    def layers(self):
+        rl = 6371.0e3 - self.litho_km * 1e3
+        (_, _, r0, m0, e0, h0), (_, _, r1, m1, _, h1), (_, _, r2, m2, _, h2), core = EARTH4
+        return [(rl, 6371.0e3, r0, m0, e0, h0), (5701.0e3, rl, r1, m1, self.eta_um, h1),
+                (3480.0e3, 5701.0e3, r2, m2, self.eta_lm, h2), core]
+
+    def params(self, default_params):
+        p = super().params(default_params)
+        set_layers(p, self.layers())
+        return p
+
+
+def ensemble(n=32, seed=2024):
+    """The batched-ensemble workload: n instances, lmax drawn from
+    {64, 96, 128, 192, 256}, upper-mantle eta log-uniform in [1e20, 1e21] Pa s,
+    lower-mantle eta log-uniform in [1e21, 1e23] Pa s, lithosphere 50-120 km,
+    every other instance with 3-D viscosity; 60, 80 and 100 radial elements
+    for lmax 64, 96 and >= 128."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(n):
+        lmax = int(rng.choice([64, 96, 128, 192, 256]))
+        n_elem = {64: 60, 96: 80}.get(lmax, 100)
+        out.append(EnsembleMember(f"e{i}_l{lmax}", lmax, n_elem, float(rng.uniform(50.0, 120.0)),
+                                  float(10 ** rng.uniform(20.0, 21.0)), float(10 ** rng.uniform(21.0, 23.0)),
+                                  i % 2 == 0, seed + 17 * i))
+    return out
+
+
 def workloads():
     return {
         "c1_1d_l64": Workload("c1_1d_l64", 64, 60, 50.0, 400, 3, "ramp", sle=False, visc3d=False),

@@ -150,6 +150,21 @@ int vg_update(vg_handle* h, const double* h_ice, double dt_yr);
 /* Same, with h_ice a device pointer (nphi*nlat doubles) on the handle's GPU. */
 int vg_update_device(vg_handle* h, const double* d_h_ice, double dt_yr);
 
+/* Ensemble batching (no reference counterpart: the reference advances one
+ * model per process): advance n independent handles -- instances with their
+ * own lmax, earth, lateral viscosity and ice -- by dt_yr each, as vg_update
+ * (ice_on_device = 0: ice[i] is a host array) or vg_update_device (1: a device
+ * pointer) would, concurrently: every handle keeps its own stream, and up to
+ * nthreads host threads (<= 0: one per handle) drive them, the costliest
+ * first, so that their kernels overlap on the GPU. Results are identical to n
+ * sequential calls. The handles must be distinct. Returns 0 when every update
+ * succeeded, else the status of the first failing handle (its message in
+ * vg_last_error(hs[i])) with *failed_index = i (failed_index may be NULL);
+ * argument errors return nonzero with *failed_index = -1 and the message in
+ * vg_last_error(NULL). */
+int vg_update_batch(vg_handle* const* hs, int n, const double* const* ice, int ice_on_device, double dt_yr,
+                    int nthreads, int* failed_index);
+
 /* Outputs of the coupling record (se%rsl, se%z_bed, se%gg%C, se%sigma_lm,
  * src/vilma_coupling.f90:71-140). Any pointer may be NULL. */
 int vg_get_fields(vg_handle* h, double* rsl, double* z_bed, double* C, double* sigma_lm);
