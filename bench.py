@@ -51,8 +51,9 @@ def parse():
                     help="3-D stress products of the timed arm")
     ap.add_argument("--plain", default="on", choices=["on", "off"],
                     help="also time the plain FP64 arm beside split_tc (and report the rsl error between them)")
-    ap.add_argument("--toroidal", default="on", choices=["on", "off"],
-                    help="also time the FP64 path carrying the toroidal channels (toroidal = 1)")
+    ap.add_argument("--toroidal", default="on", choices=["on", "off", "only"],
+                    help="also time the FP64 path carrying the toroidal channels (toroidal = 1); "
+                         "only: time that path alone as the main arm")
     ap.add_argument("--grad-fwd", default="on", choices=["on", "off", "only"],
                     help="also time the adjoint gradient against its forward (grad/fwd); 'only' prints that alone")
     return ap.parse_args()
@@ -525,8 +526,9 @@ def main():
     ice_dev = torch.empty((total + n_prof + 1, ng), dtype=torch.float64, device="cuda")
     for s in range(total + n_prof + 1):
         ice_dev[s] = torch.from_numpy(w.ice_at(s + 1))
-    split = w.visc3d and args.precision == "split_tc"
-    main_arm = run_arm(w, 1 if split else 0, args, ice_dev, local, dist, True)
+    tor_only = w.visc3d and args.toroidal == "only"
+    split = w.visc3d and args.precision == "split_tc" and not tor_only
+    main_arm = run_arm(w, 1 if split else 0, args, ice_dev, local, dist, True, tor_only)
     plain = run_arm(w, 0, args, ice_dev, local, dist, False) if split and args.plain == "on" else None
     tor = run_arm(w, 0, args, ice_dev, local, dist, False, True) if w.visc3d and args.toroidal == "on" else None
     if rank != 0:
@@ -551,7 +553,8 @@ def main():
         "data": "synthetic",
         "config": {"workload": w.name, "lmax": w.lmax, "grid": f"{w.nlat}x{w.nphi}", "radial_elements": w.n_elem,
                    "dt_yr": w.dt_yr, "n_sub": info.n_sub_last, "visc3d": w.visc3d, "sea_level": w.sle,
-                   "visc3d_precision": "split_tc" if split else "fp64", "parallelism": f"replicas{world}",
+                   "visc3d_precision": "split_tc" if split else "fp64", "toroidal": bool(tor_only),
+                   "parallelism": f"replicas{world}",
                    "l2": "state larger than L2 (%.0f MB streamed per sub-step)" % (6 * 4 * info.ne * info.nk * 8 / 1e6)},
         "e2e": {"value": 1e3 / main_arm["e2e_ms"], "unit": "steps/s", "h2d_bytes_per_step": ng * 8,
                 "d2h_bytes_per_step": ng * 8},
