@@ -41,6 +41,12 @@ _SIGS = [
     ("vg_get_rotation_state", [_VP, _P, _P, _P]),
     ("vg_get_step_state", [_VP, _P, _P, C.POINTER(C.c_int)]),
     ("vg_get_toroidal", [_VP, _P]),
+    ("vg_remap_create", [_VP, _P, C.c_int, _P, C.c_int, C.POINTER(_VP)]),
+    ("vg_remap_to_gauss", [_VP, _P, _P, C.c_int]),
+    ("vg_remap_to_ll", [_VP, _P, _P]),
+    ("vg_set_reference_ll", [_VP, _P, _P, _P]),
+    ("vg_update_ll", [_VP, _P, C.c_double, _P, _P]),
+    ("vg_remap_destroy", [_VP]),
     ("vg_update_batch", [C.POINTER(_VP), C.c_int, C.POINTER(_P), C.c_int, C.c_double, C.c_int,
                          C.POINTER(C.c_int)]),
     ("vg_get_state_tor", [_VP, _P, _P, _P, _P, _P, _P, C.POINTER(C.c_int)]),
@@ -331,3 +337,49 @@ def update_batch(models, ices, dt_yr, on_device=False, nthreads=0):
         i = failed.value
         msg = lib().vg_last_error(models[i].h if i >= 0 else None).decode()
         raise VilmaError(f"vg_update_batch: instance {i}: {msg}")
+
+
+class Remap:
+    """Host lon-lat <-> Gauss-grid remap of a model (vg_remap_*); fields are
+    (nlat_src, nlon) arrays, latitude ascending."""
+
+    def __init__(self, model, lon_src, lat_src):
+        self.m = model
+        self.lon = np.ascontiguousarray(lon_src, dtype=np.float64)
+        self.lat = np.ascontiguousarray(lat_src, dtype=np.float64)
+        r = _VP()
+        model._c(lib().vg_remap_create(model.h, ptr(self.lon), len(self.lon), ptr(self.lat), len(self.lat),
+                                       C.byref(r)))
+        self.r = r
+        self.shape = (len(self.lat), len(self.lon))
+
+    def __del__(self):
+        if getattr(self, "r", None):
+            lib().vg_remap_destroy(self.r)
+            self.r = None
+
+    def _c(self, rc):
+        if rc != 0:
+            raise VilmaError(lib().vg_last_error(self.m.h).decode())
+
+    def to_gauss(self, f_ll, conserve_mass=False):
+        g = np.zeros(self.m.ng)
+        self._c(lib().vg_remap_to_gauss(self.r, ptr(np.ascontiguousarray(f_ll, dtype=np.float64)), ptr(g),
+                                        1 if conserve_mass else 0))
+        return g.reshape(self.m.p.nlat, self.m.p.nphi)
+
+    def to_ll(self, f_gauss):
+        out = np.zeros(self.shape)
+        self._c(lib().vg_remap_to_ll(self.r, ptr(np.ascontiguousarray(f_gauss, dtype=np.float64)), ptr(out)))
+        return out
+
+    def set_reference(self, z_bed_eq, h_ice_eq, h_ice_init=None):
+        a = [None if x is None else np.ascontiguousarray(x, dtype=np.float64) for x in (z_bed_eq, h_ice_eq, h_ice_init)]
+        self._c(lib().vg_set_reference_ll(self.r, ptr(a[0]), ptr(a[1]), ptr(a[2])))
+
+    def update(self, h_ice, dt_yr):
+        """(rsl, z_bed) on the host grid after the interval."""
+        rsl, zb = np.zeros(self.shape), np.zeros(self.shape)
+        self._c(lib().vg_update_ll(self.r, ptr(np.ascontiguousarray(h_ice, dtype=np.float64)), dt_yr, ptr(rsl),
+                                   ptr(zb)))
+        return rsl, zb

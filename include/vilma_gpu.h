@@ -150,6 +150,35 @@ int vg_update(vg_handle* h, const double* h_ice, double dt_yr);
 /* Same, with h_ice a device pointer (nphi*nlat doubles) on the handle's GPU. */
 int vg_update_device(vg_handle* h, const double* d_h_ice, double dt_yr);
 
+/* Host-grid coupling (src/vilma_remap.f90:56-166; src/vilma_coupling.f90:
+ * 144-176, 336-447, 625-641): when the host's lon-lat grid is not the model's
+ * Gauss grid, ice (and the reference fields) come in by first-order
+ * conservative remapping and rsl goes back by bilinear interpolation, on the
+ * device. Host fields are (nlon, nlat) with longitude fastest and latitude
+ * ascending (south first), as the reference's grid_class axes; lon_src and
+ * lat_src are the cell-centre axes in degrees, ascending (longitudes in any
+ * 360-degree window). A remap belongs to its handle, which must outlive it.
+ *   vg_remap_create      remap_init: cell boundaries at the axis midpoints
+ *   vg_remap_to_gauss    remap_to_gauss (stat "mean"; conserve_mass rescales so
+ *                        the Gauss quadrature integral equals the source area
+ *                        integral)
+ *   vg_remap_to_ll       remap_to_ll (bilinear)
+ *   vg_set_reference_ll  solid_earth_init with a host grid: z_bed_eq remapped as
+ *                        geometry, h_ice_eq / h_ice_init with the mass rescale
+ *   vg_update_ll         solid_earth_update with a host grid: the ice remapped
+ *                        in, the interval, rsl remapped out and z_bed =
+ *                        z_bed_eq - rsl on the host's own bed (either output may
+ *                        be NULL) */
+typedef struct vg_remap vg_remap;
+int vg_remap_create(vg_handle* h, const double* lon_src, int nlon, const double* lat_src, int nlat,
+                    vg_remap** out);
+int vg_remap_to_gauss(vg_remap* r, const double* f_ll, double* f_gauss, int conserve_mass);
+int vg_remap_to_ll(vg_remap* r, const double* f_gauss, double* f_ll);
+int vg_set_reference_ll(vg_remap* r, const double* z_bed_eq_ll, const double* h_ice_eq_ll,
+                        const double* h_ice_init_ll);
+int vg_update_ll(vg_remap* r, const double* h_ice_ll, double dt_yr, double* rsl_ll, double* z_bed_ll);
+int vg_remap_destroy(vg_remap* r);
+
 /* Ensemble batching (no reference counterpart: the reference advances one
  * model per process): advance n independent handles -- instances with their
  * own lmax, earth, lateral viscosity and ice -- by dt_yr each, as vg_update
