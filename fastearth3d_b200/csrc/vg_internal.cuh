@@ -135,6 +135,7 @@ struct vg_handle {
   std::vector<int> elem_layer, kdeg_h, k2lm_h, kbeg_h;
   std::vector<char> active1d_h;
   std::vector<int> e3d_h;
+  std::vector<double> pert_mean3d;  // lateral mean of the log10 perturbation per 3-D element
   // operators
   vg::DArr<double> d_ab, d_dr, d_dc, d_rdiag;  // degrees 2..lmax (band, column-major, ldab 19)
   vg::DArr<int> d_ipiv;

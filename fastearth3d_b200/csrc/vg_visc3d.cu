@@ -673,6 +673,7 @@ void visc3d_enable(vg_handle* h, const double* pert) {
   // classification (src/vilma_response.f90:1024-1046), on the host: setup only
   std::vector<double> rate3;
   h->e3d_h.clear();
+  h->pert_mean3d.clear();
   for (int e = 0; e < ne; ++e) {
     h->active1d_h[e] = 1;
     if (h->MkPerDt[e] == 0.0) continue;
@@ -685,6 +686,9 @@ void visc3d_enable(vg_handle* h, const double* pert) {
     if (mx - mn > h->p.visc3d_tol) {
       h->active1d_h[e] = 0;
       h->e3d_h.push_back(e);
+      double sum = 0.0;
+      for (int g = 0; g < ng; ++g) sum += pe[g];
+      h->pert_mean3d.push_back(sum / (double)ng);  // for the 1-D pre-equilibration of the spin-up
       for (int g = 0; g < ng; ++g) rate3.push_back(h->MkPerDt[e] * std::pow(10.0, -pe[g]));
     } else {
       double sum = 0.0;

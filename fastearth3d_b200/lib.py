@@ -53,7 +53,8 @@ _SIGS = [
     ("vg_set_state_tor", [_VP, _P, _P, _P, _P, _P, _P]),
     ("vg_set_step_state", [_VP, C.c_double, _P, C.c_int]),
     ("vg_set_rotation_state", [_VP, _P, _P, _P]),
-    ("vg_spinup", [_VP, _P, C.c_double, C.c_double, _P, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
+    ("vg_spinup", [_VP, _P, C.c_double, C.c_double, C.c_int, _P, C.POINTER(C.c_int), C.POINTER(C.c_int),
+                   C.POINTER(C.c_int)]),
     ("vg_misfit", [_VP, C.c_int, C.c_double, _P, C.c_int, C.POINTER(C.c_int), _P, _P]),
     ("vg_misfit_grad", [_VP, C.c_int, C.c_double, _P, C.c_int, C.POINTER(C.c_int), _P, C.c_int, _P, _P, _P]),
     ("vg_sht_analysis", [_VP, _P, _P]),
@@ -150,14 +151,16 @@ class Model:
     def update(self, h_ice, dt_yr):
         self._c(lib().vg_update(self.h, ptr(np.ascontiguousarray(h_ice, dtype=np.float64)), dt_yr))
 
-    def spinup(self, h_ice_lgm, t_max_yr, rate_tol):
-        """solid_earth_spinup's relaxation (vg_spinup): returns (model years
-        spent, passes, converged)."""
+    def spinup(self, h_ice_lgm, t_max_yr, rate_tol, pre_1d=False, with_1d=False):
+        """solid_earth_spinup (vg_spinup): returns (model years spent, passes,
+        converged) of the full phase, and with with_1d the 1-D phase's passes."""
         t = C.c_double(0.0)
-        n, ok = C.c_int(0), C.c_int(0)
+        n, ok, n1 = C.c_int(0), C.c_int(0), C.c_int(0)
         ice = np.ascontiguousarray(h_ice_lgm, dtype=np.float64)
-        self._c(lib().vg_spinup(self.h, ptr(ice), t_max_yr, rate_tol, C.byref(t), C.byref(n), C.byref(ok)))
-        return t.value, n.value, bool(ok.value)
+        self._c(lib().vg_spinup(self.h, ptr(ice), t_max_yr, rate_tol, 1 if pre_1d else 0, C.byref(t), C.byref(n),
+                                C.byref(ok), C.byref(n1)))
+        out = (t.value, n.value, bool(ok.value))
+        return out + (n1.value,) if with_1d else out
 
     def update_device(self, d_h_ice_ptr, dt_yr):
         self._c(lib().vg_update_device(self.h, C.c_void_p(d_h_ice_ptr), dt_yr))

@@ -263,17 +263,21 @@ int vg_set_step_state(vg_handle* h, double dt_try_yr, const double* sigma_n, int
 int vg_get_rotation_state(vg_handle* h, double* m, double* load_mem, double* tidal_mem);
 int vg_set_rotation_state(vg_handle* h, const double* m, const double* load_mem, const double* tidal_mem);
 
-/* LGM-memory spin-up, the relaxation of solid_earth_spinup (relax_hold,
- * src/vilma_coupling.f90:453-570): a zero-length update seeds the entering ice
- * with h_ice_lgm (nphi, nlat), then h_ice_lgm is held over passes of 200 yr
- * growing by 1.6 per pass (at most 60, at most t_max_yr in total) until the
- * mean bed velocity int |z_bed - z_prev| dOmega / (4 pi) / pass falls below
- * rate_tol [m/yr] (equil_rate_tol). t_max_yr <= 0 does nothing
- * (equil_time_max = 0). The 1-D pre-equilibration (pre_spinup_1d) is not
- * provided. Outputs (any may be NULL): the model time spent [yr], the passes,
- * 1 if the bed came to rest before the cap. */
-int vg_spinup(vg_handle* h, const double* h_ice_lgm, double t_max_yr, double rate_tol, double* t_done_yr,
-              int* passes, int* converged);
+/* LGM-memory spin-up, solid_earth_spinup (src/vilma_coupling.f90:453-570):
+ * a zero-length update seeds the entering ice with h_ice_lgm (nphi, nlat);
+ * with pre_1d (pre_spinup_1d) and lateral viscosity enabled, the 3-D elements
+ * first take the lateral mean of their log10-viscosity perturbation and the
+ * held load relaxes to rest with no time cap (relax_hold's internal pass cap
+ * only), after which the real 3-D field is restored; then, if t_max_yr > 0
+ * (equil_time_max), the full model relaxes (relax_hold): h_ice_lgm held over
+ * passes of 200 yr growing by 1.6 per pass (at most 60, at most t_max_yr in
+ * total) until the mean bed velocity int |z_bed - z_prev| dOmega / (4 pi) /
+ * pass falls below rate_tol [m/yr] (equil_rate_tol). Neither phase (pre_1d = 0
+ * and t_max_yr <= 0) does nothing. Outputs (any may be NULL), of the full
+ * phase: the model time spent [yr], the passes, 1 if the bed came to rest
+ * before the cap; passes_1d: the passes of the 1-D phase. */
+int vg_spinup(vg_handle* h, const double* h_ice_lgm, double t_max_yr, double rate_tol, int pre_1d,
+              double* t_done_yr, int* passes, int* converged, int* passes_1d);
 
 /* Relative-sea-level misfit of a response-level run and its gradient
  * (hand-written discrete adjoint; the reference has no counterpart). From the

@@ -173,6 +173,7 @@ struct Response {
   int ne3d = 0;
   std::vector<int> e3d;
   std::vector<double> Mk3, MkPerDt3;  // [e][j][i] (nphi fastest)
+  std::vector<double> pert_mean3d;    // lateral mean of the log10 perturbation per 3-D element
   // memory scheme and the sea-level <-> memory co-convergence
   // (vilma_response.f90:176-223, 1480-1663)
   int scheme = SCHEME_FE;

@@ -37,7 +37,8 @@ def lib():
             ("orc_set_reference", [_VP, _P, _P, _P]),
             ("orc_enable_visc3d", [_VP, _P]),
             ("orc_update", [_VP, _P, C.c_double]),
-            ("orc_spinup", [_VP, _P, C.c_double, C.c_double, _P, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
+            ("orc_spinup", [_VP, _P, C.c_double, C.c_double, C.c_int, _P, C.POINTER(C.c_int), C.POINTER(C.c_int),
+                            C.POINTER(C.c_int)]),
             ("orc_get_fields", [_VP, _P, _P, _P, _P]),
             ("orc_get_rotation", [_VP, _P, _P]),
             ("orc_rotation_update", [_VP, _P, C.c_double]),
@@ -160,12 +161,14 @@ class Oracle:
     def update(self, h_ice, dt_yr):
         self._c(lib().orc_update(self.h, ptr(np.ascontiguousarray(h_ice, dtype=np.float64)), dt_yr))
 
-    def spinup(self, h_ice_lgm, t_max_yr, rate_tol):
+    def spinup(self, h_ice_lgm, t_max_yr, rate_tol, pre_1d=False, with_1d=False):
         t = C.c_double(0.0)
-        n, ok = C.c_int(0), C.c_int(0)
+        n, ok, n1 = C.c_int(0), C.c_int(0), C.c_int(0)
         ice = np.ascontiguousarray(h_ice_lgm, dtype=np.float64)
-        self._c(lib().orc_spinup(self.h, ptr(ice), t_max_yr, rate_tol, C.byref(t), C.byref(n), C.byref(ok)))
-        return t.value, n.value, bool(ok.value)
+        self._c(lib().orc_spinup(self.h, ptr(ice), t_max_yr, rate_tol, 1 if pre_1d else 0, C.byref(t), C.byref(n),
+                                 C.byref(ok), C.byref(n1)))
+        out = (t.value, n.value, bool(ok.value))
+        return out + (n1.value,) if with_1d else out
 
     def fields(self):
         rsl, zb, Cf = np.zeros(self.ng), np.zeros(self.ng), np.zeros(self.ng)

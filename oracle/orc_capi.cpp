@@ -215,25 +215,21 @@ int orc_update(OrcHandle* h, const double* h_ice, double dt_yr) {
   return 0;
 }
 
-// vilma_coupling.f90:453-570 solid_earth_spinup's relaxation (relax_hold):
-// seed the entering ice with a zero-length update, then hold h_ice_lgm over
-// passes of 200 yr growing by 1.6 (at most 60, capped at t_cap) until the mean
+// vilma_coupling.f90:500-545 relax_hold: hold h_ice_lgm over passes of 200 yr
+// growing by 1.6 (at most 60, capped at t_cap when t_cap > 0) until the mean
 // bed velocity int |dz_bed| dOmega / (4 pi) / pass falls below tol [m/yr]
-int orc_spinup(OrcHandle* h, const double* h_ice_lgm, double t_cap, double tol, double* t_done, int* passes,
-               int* converged) {
+static int relax_hold(OrcHandle* h, const double* h_ice_lgm, double t_cap, double tol, double* t_done, int* passes,
+                      int* converged) {
   const int ng = h->sht.nphi * h->sht.nlat;
   *t_done = 0.0;
   *passes = 0;
   *converged = 0;
-  if (!(t_cap > 0.0)) return 0;
-  int rc = orc_update(h, h_ice_lgm, 0.0);
-  if (rc) return rc;
   std::vector<double> prev = h->z_bed, d(ng);
   double pass_dt = 200.0;
   for (int it = 1; it <= 60; ++it) {
-    pass_dt = std::min(pass_dt, t_cap - *t_done);
+    if (t_cap > 0.0) pass_dt = std::min(pass_dt, t_cap - *t_done);
     if (pass_dt <= 0.0) break;
-    rc = orc_update(h, h_ice_lgm, pass_dt);
+    int rc = orc_update(h, h_ice_lgm, pass_dt);
     if (rc) return rc;
     *t_done += pass_dt;
     *passes = it;
@@ -246,6 +242,52 @@ int orc_spinup(OrcHandle* h, const double* h_ice_lgm, double t_cap, double tol, 
     prev = h->z_bed;
     pass_dt = pass_dt * 1.6;
   }
+  return 0;
+}
+
+// vilma_coupling.f90:453-498 solid_earth_spinup: seed the entering ice with a
+// zero-length update; with pre_1d relax to rest under the lateral mean of the
+// 3-D viscosity (every 3-D element at mu / eta * 10^-(mean perturbation),
+// :484-493), then restore the real field; then relax_hold up to t_cap
+int orc_spinup(OrcHandle* h, const double* h_ice_lgm, double t_cap, double tol, int pre_1d, double* t_done,
+               int* passes, int* converged, int* passes_1d) {
+  *t_done = 0.0;
+  *passes = 0;
+  *converged = 0;
+  *passes_1d = 0;
+  if (!pre_1d && !(t_cap > 0.0)) return 0;
+  int rc = orc_update(h, h_ice_lgm, 0.0);
+  if (rc) return rc;
+  if (pre_1d) {
+    Response& R = h->R;
+    const bool mean = R.lat_visc && R.ne3d > 0;
+    std::vector<double> mk = R.MkPerDt;
+    std::vector<char> act = R.active1d;
+    std::vector<int> e3d = R.e3d;
+    const int ne3d = R.ne3d;
+    if (mean) {
+      for (int ei = 0; ei < ne3d; ++ei) {
+        R.MkPerDt[e3d[ei]] = mk[e3d[ei]] * std::pow(10.0, -R.pert_mean3d[ei]);
+        R.active1d[e3d[ei]] = 1;
+      }
+      R.e3d.clear();
+      R.ne3d = 0;
+      R.lat_visc = false;
+    }
+    double t1 = 0.0;
+    int c1 = 0;
+    rc = relax_hold(h, h_ice_lgm, -1.0, tol, &t1, passes_1d, &c1);
+    if (mean) {  // the real 3-D field (solid_earth_enable_visc_3d)
+      R.MkPerDt = mk;
+      R.active1d = act;
+      R.e3d = e3d;
+      R.ne3d = ne3d;
+      R.lat_visc = true;
+      for (int e = 0; e < R.ne; ++e) R.Mk[e] = R.MkPerDt[e] * R.dt;
+    }
+    if (rc) return rc;
+  }
+  if (t_cap > 0.0) return relax_hold(h, h_ice_lgm, t_cap, tol, t_done, passes, converged);
   return 0;
 }
 

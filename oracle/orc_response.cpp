@@ -959,6 +959,7 @@ void response_enable_lateral_visc(Response& R, const Sht& s, const double* pert)
   const size_t ng = (size_t)s.nphi * s.nlat;
   R.MkPerDt3.assign(ng * R.ne, 0.0);
   R.Mk3.assign(ng * R.ne, 0.0);
+  R.pert_mean3d.clear();
   for (int e = 0; e < R.ne; ++e)
     for (size_t g = 0; g < ng; ++g) R.MkPerDt3[e * ng + g] = R.MkPerDt[e] * std::pow(10.0, -pert[e * ng + g]);
   std::fill(R.active1d.begin(), R.active1d.end(), 1);
@@ -973,6 +974,8 @@ void response_enable_lateral_visc(Response& R, const Sht& s, const double* pert)
     if (mx - mn > R.visc3d_tol) {
       R.active1d[e] = 0;
       R.ne3d++;
+      for (size_t g = 0; g < ng; ++g) sum += pert[e * ng + g];
+      R.pert_mean3d.push_back(sum / (double)ng);
     } else {
       for (size_t g = 0; g < ng; ++g) sum += pert[e * ng + g];
       double mean_pert = sum / (double)ng;

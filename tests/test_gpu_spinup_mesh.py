@@ -45,6 +45,26 @@ def test_spinup_parity_with_oracle():
     assert g.spinup(ice, 0.0, 1e-3) == (0.0, 0, False)
 
 
+def test_pre_spinup_1d_parity_3d():
+    """The 1-D pre-equilibration on the lateral mean of a 3-D field, then the
+    full-model phase with the field restored: passes, model time and fields
+    as the oracle's."""
+    w = synth.Workload("s", 12, 16, 100.0, 2, 2, "sawtooth", sle=True, visc3d=True, seed=8)
+    g, o = vlib.Model(w.params(vlib.default_params)), orc.Oracle(w.params(orc.default_params))
+    zb, hi = w.reference()
+    for m in (g, o):
+        m.set_reference(zb, hi)
+        m.enable_visc3d(w.pert(m.p))
+    ne3d = g.info().ne3d
+    rg = g.spinup(w.ice_at(400), 2000.0, 1e-3, pre_1d=True, with_1d=True)
+    ro = o.spinup(w.ice_at(400), 2000.0, 1e-3, pre_1d=True, with_1d=True)
+    assert rg[1:] == ro[1:] and abs(rg[0] - ro[0]) <= 1e-9 * ro[0], (rg, ro)
+    assert rg[3] > 0 and g.info().ne3d == ne3d
+    (rsg, zg, cg, _), (rso, zo, co, _) = g.fields(), o.fields()
+    assert np.array_equal(cg, co)
+    assert rel(zg, zo) < 1e-10 and rel(rsg, rso) < 1e-10
+
+
 def test_reference_native_mesh_parity():
     w = synth.Workload("t", 16, 0, 100.0, 2, 2, "sawtooth", sle=True, visc3d=False, seed=4)
     ps = []

@@ -42,3 +42,29 @@ def test_spinup_zero_cap_does_nothing():
     o, z_eq, ice, at = setup()
     assert o.spinup(ice, 0.0, RATE_TOL) == (0.0, 0, False)
     assert np.array_equal(o.fields()[1], z_eq)
+
+
+def test_pre_spinup_1d_phase():
+    """tests/test_spinup.f90 check (2): the 1-D pre-equilibration alone
+    (pre_spinup_1d, equil_time_max = 0) drives appreciable subsidence."""
+    o, z_eq, ice, at = setup()
+    t_done, passes, converged, passes_1d = o.spinup(ice, 0.0, RATE_TOL, pre_1d=True, with_1d=True)
+    assert (t_done, passes, converged) == (0.0, 0, False) and 0 < passes_1d <= 60
+    assert z_eq[at] - o.fields()[1][at] >= 50.0
+
+
+def test_pre_spinup_1d_restores_the_3d_field():
+    """With lateral viscosity, the 1-D phase runs on the lateral mean and the
+    genuinely 3-D elements are back afterwards."""
+    from fastearth3d_b200 import synth
+
+    w = synth.Workload("s", 12, 16, 100.0, 2, 2, "sawtooth", sle=True, visc3d=True, seed=8)
+    o = orc.Oracle(w.params(orc.default_params))
+    zb, hi = w.reference()
+    o.set_reference(zb, hi)
+    o.enable_visc3d(w.pert(o.p))
+    ne3d = o.info().ne3d
+    assert ne3d > 0
+    out = o.spinup(w.ice_at(400), 2000.0, RATE_TOL, pre_1d=True, with_1d=True)
+    assert out[3] > 0 and out[1] > 0
+    assert o.info().ne3d == ne3d
