@@ -105,13 +105,14 @@ struct LateralMean {
     h->d_active1d.upload(h->active1d_h, h->stream);
     VG_CUDA(cudaStreamSynchronize(h->stream));
   }
-  ~LateralMean() {  // the real 3-D field (solid_earth_enable_visc_3d)
+  ~LateralMean() {  // the real 3-D field (solid_earth_enable_visc_3d); never throws
     h->MkPerDt = MkPerDt;
     h->active1d_h = active1d;
     h->ne3d = ne3d;
     h->max_rate = max_rate;
-    h->d_MkPerDt.upload(h->MkPerDt, h->stream);
-    h->d_active1d.upload(h->active1d_h, h->stream);
+    cudaMemcpyAsync(h->d_MkPerDt.p, h->MkPerDt.data(), h->MkPerDt.size() * sizeof(double), cudaMemcpyHostToDevice,
+                    h->stream);
+    cudaMemcpyAsync(h->d_active1d.p, h->active1d_h.data(), h->active1d_h.size(), cudaMemcpyHostToDevice, h->stream);
     cudaStreamSynchronize(h->stream);
   }
 };
