@@ -43,7 +43,7 @@ def test_adjoint_gradient_vs_central_differences():
     obs = 0.01 * rng.standard_normal((len(sigma), len(sites)))
     J, g = m.misfit_grad(sigma, dt, sites, obs, ckpt_every=4)
     assert abs(J - m.misfit(sigma, dt, sites, obs)) <= 1e-12 * J
-    for _ in range(8):
+    for _ in range(20):  # 20 seeded random directions
         d = rng.standard_normal(sigma.shape) + 1j * rng.standard_normal(sigma.shape)
         d[:, : m.p.lmax + 1] = d[:, : m.p.lmax + 1].real
         h = 1e-3 * np.abs(sigma).max() / np.abs(d).max()
@@ -103,13 +103,13 @@ def test_adjoint_3d_log_viscosity_gradient_vs_central_differences():
     J, gs, gp = m.misfit_grad(sig, dt, sites, obs, ckpt_every=2, want_pert=True)
     assert abs(J - m.misfit(sig, dt, sites, obs)) <= 1e-12 * J
     h = 1e-4
-    for _ in range(4):
+    for _ in range(20):  # 20 seeded random directions
         d = rng.standard_normal(pert.shape)
         fd = (make(pert + h * d).misfit(sig, dt, sites, obs) - make(pert - h * d).misfit(sig, dt, sites, obs)) / (2 * h)
         ad = np.sum(gp * d)
         assert abs(fd - ad) <= 1e-6 * abs(fd), (fd, ad)
     # the load gradient through the 3-D transposes
-    for _ in range(3):
+    for _ in range(20):
         d = rng.standard_normal(sig.shape) + 1j * rng.standard_normal(sig.shape)
         d[:, : m.p.lmax + 1] = d[:, : m.p.lmax + 1].real
         hs = 1e-3 * np.abs(sig).max() / np.abs(d).max()
