@@ -257,7 +257,12 @@ int vg_update_batch(vg_handle* const* hs, int n, const double* const* ice, int i
   const int nt = std::min(n, nthreads <= 0 ? n : nthreads);
   std::vector<std::thread> pool;
   pool.reserve(nt);
-  for (int t = 0; t < nt; ++t) pool.emplace_back(work);
+  try {
+    for (int t = 0; t < nt; ++t) pool.emplace_back(work);
+  } catch (const std::exception&) {
+    // no more threads to be had: the calling thread takes the rest of the queue
+  }
+  if (pool.empty()) work();
   for (std::thread& th : pool) th.join();
   for (int i = 0; i < n; ++i)
     if (rc[i] != 0) {
