@@ -51,6 +51,8 @@ def parse():
                     help="3-D stress products of the timed arm")
     ap.add_argument("--plain", default="on", choices=["on", "off"],
                     help="also time the plain FP64 arm beside split_tc (and report the rsl error between them)")
+    ap.add_argument("--ensemble-sle-ctas", default="rows", choices=["sm", "rows"],
+                    help="c4_ensemble: the fused sea-level loop's CTAs per instance (one per SM, or one per grid row)")
     ap.add_argument("--toroidal", default="on", choices=["on", "off", "only"],
                     help="also time the FP64 path carrying the toroidal channels (toroidal = 1); "
                          "only: time that path alone as the main arm")
@@ -400,6 +402,8 @@ def run_ensemble(args):
     def make(mb, split):
         p = mb.params(vlib.default_params)
         p.visc3d_precision = 1 if (split and mb.visc3d) else 0
+        if args.ensemble_sle_ctas == "rows":  # the fused sea-level loop on one CTA per grid row at most
+            p.sle_ctas = mb.nlat
         m = vlib.Model(p)
         zb, hi = mb.reference()
         m.set_reference(zb, hi)
@@ -440,14 +444,18 @@ def run_ensemble(args):
     del models
     torch.cuda.synchronize()
     # sequential: each instance's W + K steps, alone, one instance after another
-    seq = {}
+    seq, by_class = {}, {}
     for split in (False, True):
         tot, rsl_seq = 0.0, []
         for i, mb in enumerate(members):
             m = make(mb, split)
             for s in range(W):
                 m.update_device(ice_dev[i][s].data_ptr(), DT)
-            tot += dev_timed(lambda: [m.update_device(ice_dev[i][s].data_ptr(), DT) for s in range(W, W + K)])
+            t_i = dev_timed(lambda: [m.update_device(ice_dev[i][s].data_ptr(), DT) for s in range(W, W + K)])
+            tot += t_i
+            if split:
+                key = "l%d%s" % (mb.lmax, "_3d" if mb.visc3d else "_1d")
+                by_class[key] = by_class.get(key, 0.0) + t_i / K
             rsl_seq.append(m.fields()[0])
             del m
         seq[split] = (tot, rsl_seq)
@@ -469,13 +477,15 @@ def run_ensemble(args):
         "vs_baseline": None,
         "dtype": "tf32x3 3-D stress products of the 3-D instances, f64 elsewhere",
         "data": "synthetic",
-        "config": {"workload": "c4_ensemble", "instances": n, "lmax": [mb.lmax for mb in members],
+        "config": {"workload": "c4_ensemble", "instances": n, "sle_ctas": args.ensemble_sle_ctas,
+                   "lmax": [mb.lmax for mb in members],
                    "visc3d": [bool(mb.visc3d) for mb in members], "radial_elements": [mb.n_elem for mb in members],
                    "dt_yr": DT, "sea_level": True, "parallelism": "one stream and one host thread per instance"},
         "sequential_plain_fp64": {"value": n * K / (seq[False][0] / 1e3), "unit": "instance-steps/s",
                                   "ms_total": seq[False][0]},
         "sequential_same_precision": {"value": n * K / (seq[True][0] / 1e3), "unit": "instance-steps/s",
                                       "ms_total": seq[True][0]},
+        "sequential_same_precision_ms_per_step_by_class": {k: round(v, 3) for k, v in sorted(by_class.items())},
         "speedup_vs_sequential_plain": seq[False][0] / ms_batch,
         "speedup_from_concurrency": seq[True][0] / ms_batch,
         "batched_equals_sequential": bool(same),

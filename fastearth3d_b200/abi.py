@@ -41,6 +41,7 @@ class VgParams(C.Structure):
         ("sle_max_mem_iter", C.c_int),
         ("couple_tol", C.c_double),
         ("toroidal", C.c_int),
+        ("sle_ctas", C.c_int),
     ]
 
 

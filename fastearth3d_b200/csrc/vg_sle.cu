@@ -660,7 +660,7 @@ static void launch_inner_loop(vg_handle* h) {
     raise_smem_limit((const void*)k_sle_inner, shm);
     VG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_sle_inner, 512, shm));
     if (per_sm < 1) throw Error("sle_solve: the fused inner loop does not fit on an SM");
-    h->sle_grid = nsm;
+    h->sle_grid = h->p.sle_ctas > 0 ? std::min(h->p.sle_ctas, nsm * per_sm) : nsm;
     h->d_gbar.alloc(4);
     std::vector<int2> chunk;
     std::vector<int> cbeg(G.M + 1);

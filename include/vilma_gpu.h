@@ -88,6 +88,10 @@ typedef struct vg_params {
    * degree of freedom (W and the lambda 3, 4 memory) once a genuinely 3-D
    * element exists (src/vilma_response.f90:1048-1118) */
   int toroidal;
+  /* CTAs of the fused sea-level loop (no reference counterpart): 0 = one per
+   * SM; fewer leave room for other instances' kernels when several handles
+   * share the GPU (vg_update_batch). Results do not depend on it. */
+  int sle_ctas;
 } vg_params;
 
 /* Phase timers (the reference's [PROFILE] buckets: drift solve, memory

@@ -81,6 +81,7 @@ int orc_params_default(vg_params* p) {
   p->sle_max_mem_iter = 20;
   p->couple_tol = 1e-6;
   p->toroidal = 0;
+  p->sle_ctas = 0;
   return 0;
 }
 
