@@ -198,6 +198,28 @@ int vg_enable_visc3d(vg_handle* h, const double* pert) {
   });
 }
 
+int vg_enable_visc3d_from_nodes(vg_handle* h, const double* visc_node, double lid_depth, double lid_log10max,
+                                double log10_cap) {
+  return guarded(h, [&] {
+    need(h, visc_node != nullptr, "vg_enable_visc3d_from_nodes: visc_node is required");
+    const int ng = h->grid.ng, ne = h->ne, nr = h->nr;
+    const double r_top = h->r[nr - 1];
+    const double r_lid = lid_depth > 0.0 ? r_top - lid_depth : HUGE_VAL;  // no element above it: rule off
+    std::vector<double> pert((size_t)ne * ng, 0.0);
+    for (int e = 0; e < ne; ++e) {
+      if (h->MkPerDt[e] == 0.0) continue;  // elastic / fluid: stay as they are
+      const double logeta_ref = std::log10(h->mu[e] / h->MkPerDt[e]);
+      const bool in_lid = h->r[e] >= r_lid - 1.0e-6 * r_top;  // element wholly above the lid base
+      for (int g = 0; g < ng; ++g) {
+        double v = 0.5 * (visc_node[(size_t)e * ng + g] + visc_node[(size_t)(e + 1) * ng + g]);  // log10-mean
+        if (in_lid && v > lid_log10max) v = log10_cap;
+        pert[(size_t)e * ng + g] = v - logeta_ref;
+      }
+    }
+    vg::visc3d_enable(h, pert.data());
+  });
+}
+
 int vg_update_device(vg_handle* h, const double* d_h_ice, double dt_yr) {
   return guarded(h, [&] {
     need(h, h->have_reference, "vg_update: call vg_set_reference first (solid_earth_init)");

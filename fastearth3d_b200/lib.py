@@ -41,6 +41,7 @@ _SIGS = [
     ("vg_get_rotation_state", [_VP, _P, _P, _P]),
     ("vg_get_step_state", [_VP, _P, _P, C.POINTER(C.c_int)]),
     ("vg_get_toroidal", [_VP, _P]),
+    ("vg_enable_visc3d_from_nodes", [_VP, _P, C.c_double, C.c_double, C.c_double]),
     ("vg_remap_create", [_VP, _P, C.c_int, _P, C.c_int, C.POINTER(_VP)]),
     ("vg_remap_to_gauss", [_VP, _P, _P, C.c_int]),
     ("vg_remap_to_ll", [_VP, _P, _P]),
@@ -179,6 +180,11 @@ class Model:
     def set_fields(self, h_ice=None, rsl=None, z_bed=None, C_ocean=None):
         self._c(lib().vg_set_fields(self.h, *[ptr(None if a is None else np.ascontiguousarray(a, dtype=np.float64))
                                               for a in (h_ice, rsl, z_bed, C_ocean)]))
+
+    def enable_visc3d_from_nodes(self, visc_node, lid_depth=0.0, lid_log10max=0.0, log10_cap=0.0):
+        """Lateral viscosity from absolute nodal log10(eta), (nr, nlat*nphi) bottom-up."""
+        v = np.ascontiguousarray(visc_node, dtype=np.float64)
+        self._c(lib().vg_enable_visc3d_from_nodes(self.h, ptr(v), lid_depth, lid_log10max, log10_cap))
 
     def toroidal(self):
         """Surface toroidal drift W(a) as t_lm (lm order); zero while not carried."""

@@ -145,6 +145,15 @@ int vg_set_reference(vg_handle* h, const double* z_bed_eq, const double* h_ice_e
  * the Gauss grid, (nphi, nlat, ne) (response_enable_lateral_visc,
  * src/vilma_response.f90:994-1053). */
 int vg_enable_visc3d(vg_handle* h, const double* pert);
+/* The same from absolute nodal log10 viscosities (response_enable_lateral_visc_
+ * from_nodes, src/vilma_response.f90:1120-1169): visc_node is (nphi*nlat, nr),
+ * Gauss grid point fastest, radial nodes bottom-up. An element takes the mean
+ * of its two nodes; elements wholly above the lid base r_earth - lid_depth
+ * (lid_depth > 0; <= 0 turns the rule off) with a value above lid_log10max take
+ * log10_cap; the perturbation is that minus log10 of the element's radial
+ * viscosity. Elastic and fluid elements stay as they are. */
+int vg_enable_visc3d_from_nodes(vg_handle* h, const double* visc_node, double lid_depth, double lid_log10max,
+                                double log10_cap);
 
 /* solid_earth_update (src/vilma_coupling.f90:336-437):
  * advance by dt_yr years with the ice linearly interpolated from the carried

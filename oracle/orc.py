@@ -36,6 +36,7 @@ def lib():
             ("orc_destroy", [_VP]),
             ("orc_set_reference", [_VP, _P, _P, _P]),
             ("orc_enable_visc3d", [_VP, _P]),
+            ("orc_enable_visc3d_from_nodes", [_VP, _P, C.c_double, C.c_double, C.c_double]),
             ("orc_update", [_VP, _P, C.c_double]),
             ("orc_spinup", [_VP, _P, C.c_double, C.c_double, C.c_int, _P, C.POINTER(C.c_int), C.POINTER(C.c_int),
                             C.POINTER(C.c_int)]),
@@ -157,6 +158,10 @@ class Oracle:
 
     def enable_visc3d(self, pert):
         self._c(lib().orc_enable_visc3d(self.h, ptr(np.ascontiguousarray(pert, dtype=np.float64))))
+
+    def enable_visc3d_from_nodes(self, visc_node, lid_depth=0.0, lid_log10max=0.0, log10_cap=0.0):
+        v = np.ascontiguousarray(visc_node, dtype=np.float64)
+        self._c(lib().orc_enable_visc3d_from_nodes(self.h, ptr(v), lid_depth, lid_log10max, log10_cap))
 
     def update(self, h_ice, dt_yr):
         self._c(lib().orc_update(self.h, ptr(np.ascontiguousarray(h_ice, dtype=np.float64)), dt_yr))

@@ -165,6 +165,29 @@ int orc_enable_visc3d(OrcHandle* h, const double* pert) {
   return 0;
 }
 
+// vilma_response.f90:1120-1169 response_enable_lateral_visc_from_nodes:
+// visc_node (nphi*nlat, nr) absolute log10 viscosity; element = log10-mean of
+// its nodes, capped in the lid, minus log10 of the radial viscosity
+int orc_enable_visc3d_from_nodes(OrcHandle* h, const double* visc_node, double lid_depth, double lid_log10max,
+                                 double log10_cap) {
+  const Response& R = h->R;
+  const size_t ng = (size_t)h->sht.nphi * h->sht.nlat;
+  const double r_top = R.r[R.nr - 1];
+  const double r_lid = lid_depth > 0.0 ? r_top - lid_depth : 1.7976931348623157e308;
+  std::vector<double> pert((size_t)R.ne * ng, 0.0);
+  for (int e = 0; e < R.ne; ++e) {
+    if (R.MkPerDt[e] == 0.0) continue;
+    const double logeta_ref = std::log10(R.mu[e] / R.MkPerDt[e]);
+    const bool in_lid = R.r[e] >= r_lid - 1.0e-6 * r_top;
+    for (size_t g = 0; g < ng; ++g) {
+      double v = 0.5 * (visc_node[(size_t)e * ng + g] + visc_node[(size_t)(e + 1) * ng + g]);
+      if (in_lid && v > lid_log10max) v = log10_cap;
+      pert[(size_t)e * ng + g] = v - logeta_ref;
+    }
+  }
+  return orc_enable_visc3d(h, pert.data());
+}
+
 // vilma_coupling.f90:572-597 update_bsl
 static void update_bsl(OrcHandle* h) {
   const int ng = h->sht.nphi * h->sht.nlat;
