@@ -198,6 +198,38 @@ int vg_enable_visc3d(vg_handle* h, const double* pert) {
   });
 }
 
+int vg_advance(vg_handle* h, const double* ice0, const double* ice1, double t0_yr, double t1_yr, const double* s_rot,
+               double* rsl, double* C, double* sigma_lm) {
+  return guarded(h, [&] {
+    need(h, h->have_reference, "vg_advance: call vg_set_reference first (solid_earth_init)");
+    need(h, ice0 != nullptr && ice1 != nullptr, "vg_advance: ice0 and ice1 are required");
+    need(h, t1_yr >= t0_yr, "vg_advance: t1 must not precede t0");
+    need(h, !(s_rot && h->rot_on), "vg_advance: with rotation = 1 the library integrates s_rot itself");
+    const size_t ng = (size_t)h->grid.ng;
+    cudaStream_t s = h->stream;
+    h->d_h_ice.upload(ice0, ng, s);  // the entering (carried) ice
+    h->d_ice1.upload(ice1, ng, s);
+    h->time_yr = t0_yr;
+    h->time_s = t0_yr * vg::SEC_PER_YEAR;
+    if (s_rot) {
+      if (h->d_srot.n != ng) h->d_srot.alloc(ng);
+      h->d_srot.upload(s_rot, ng, s);
+    }
+    h->srot_ext = s_rot != nullptr;
+    try {
+      vg::update_dev(h, h->d_ice1.p, t1_yr - t0_yr);
+    } catch (...) {
+      h->srot_ext = false;
+      throw;
+    }
+    h->srot_ext = false;
+    if (rsl) h->d_rsl.download(rsl, ng, s);
+    if (C) h->d_C.download(C, ng, s);
+    if (sigma_lm) h->d_sigma.download(sigma_lm, 2 * (size_t)h->grid.nlm, s);
+    VG_CUDA(cudaStreamSynchronize(s));
+  });
+}
+
 int vg_enable_visc3d_from_nodes(vg_handle* h, const double* visc_node, double lid_depth, double lid_log10max,
                                 double log10_cap) {
   return guarded(h, [&] {

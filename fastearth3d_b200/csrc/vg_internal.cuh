@@ -213,6 +213,7 @@ struct vg_handle {
   vg::Prof prof;
   // rotational feedback (two degree-2 channels and the polar motion)
   bool rot_on = false;
+  bool srot_ext = false;  // vg_advance: a host-given rotational potential in d_srot for this interval
   double rot_kTe = 0, rot_hTe = 0, rot_ks = 0, rot_ks_fluid = 0, rot_ks_flat = 0;
   double rot_Fe[2] = {0, 0}, rot_Ue[2] = {0, 0};  // unit responses: load, tidal channel
   double rot_a = 0, rot_g = 0, rot_CminusA = 2.63e35, rot_Omega = 7.292115e-5, rot_dt_fe_max = HUGE_VAL;

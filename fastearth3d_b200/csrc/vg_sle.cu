@@ -695,7 +695,7 @@ static void launch_inner_loop(vg_handle* h) {
   A.gu = h->d_gu.p;
   A.gn = h->d_gn.p;
   A.drift = h->d_drift.p;
-  A.srot = h->rot_on ? h->d_srot.p : nullptr;
+  A.srot = (h->rot_on || h->srot_ext) ? h->d_srot.p : nullptr;
   A.lm_m = G.d_lm_m.p;
   A.lm_l = G.d_lm_l.p;
   A.lm2k = h->d_lm2k.p;

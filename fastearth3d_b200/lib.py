@@ -42,6 +42,7 @@ _SIGS = [
     ("vg_get_step_state", [_VP, _P, _P, C.POINTER(C.c_int)]),
     ("vg_get_toroidal", [_VP, _P]),
     ("vg_enable_visc3d_from_nodes", [_VP, _P, C.c_double, C.c_double, C.c_double]),
+    ("vg_advance", [_VP, _P, _P, C.c_double, C.c_double, _P, _P, _P, _P]),
     ("vg_remap_create", [_VP, _P, C.c_int, _P, C.c_int, C.POINTER(_VP)]),
     ("vg_remap_to_gauss", [_VP, _P, _P, C.c_int]),
     ("vg_remap_to_ll", [_VP, _P, _P]),
@@ -180,6 +181,14 @@ class Model:
     def set_fields(self, h_ice=None, rsl=None, z_bed=None, C_ocean=None):
         self._c(lib().vg_set_fields(self.h, *[ptr(None if a is None else np.ascontiguousarray(a, dtype=np.float64))
                                               for a in (h_ice, rsl, z_bed, C_ocean)]))
+
+    def advance_interval(self, ice0, ice1, t0_yr, t1_yr, s_rot=None):
+        """vg_advance (stepper_advance): (rsl, C, sigma_lm) at t1."""
+        rsl, Cf, sig = np.zeros(self.ng), np.zeros(self.ng), np.zeros(2 * self.nlm)
+        a = [np.ascontiguousarray(x, dtype=np.float64) for x in (ice0, ice1)]
+        sr = None if s_rot is None else np.ascontiguousarray(s_rot, dtype=np.float64)
+        self._c(lib().vg_advance(self.h, ptr(a[0]), ptr(a[1]), t0_yr, t1_yr, ptr(sr), ptr(rsl), ptr(Cf), ptr(sig)))
+        return rsl, Cf, _unpack(sig)
 
     def enable_visc3d_from_nodes(self, visc_node, lid_depth=0.0, lid_log10max=0.0, log10_cap=0.0):
         """Lateral viscosity from absolute nodal log10(eta), (nr, nlat*nphi) bottom-up."""

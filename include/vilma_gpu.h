@@ -162,6 +162,16 @@ int vg_enable_visc3d_from_nodes(vg_handle* h, const double* visc_node, double li
 int vg_update(vg_handle* h, const double* h_ice, double dt_yr);
 /* Same, with h_ice a device pointer (nphi*nlat doubles) on the handle's GPU. */
 int vg_update_device(vg_handle* h, const double* d_h_ice, double dt_yr);
+/* stepper_advance (src/vilma_timestep.f90:79-105) for hosts that run their own
+ * interval driver: advance from t0_yr (which becomes the model time) to t1_yr
+ * with the ice interpolated linearly from ice0 to ice1 (host arrays, nphi*nlat);
+ * s_rot (may be NULL) is the rotational-feedback term of rsl held across the
+ * interval, as the reference's caller passes it (not with rotation = 1, where
+ * the library integrates the rotation itself). Outputs (any may be NULL): rsl
+ * and C on the Gauss grid and the converged surface load sigma_lm at t1
+ * (sigma_out). */
+int vg_advance(vg_handle* h, const double* ice0, const double* ice1, double t0_yr, double t1_yr, const double* s_rot,
+               double* rsl, double* C, double* sigma_lm);
 
 /* Host-grid coupling (src/vilma_remap.f90:56-166; src/vilma_coupling.f90:
  * 144-176, 336-447, 625-641): when the host's lon-lat grid is not the model's

@@ -36,6 +36,7 @@ def lib():
             ("orc_destroy", [_VP]),
             ("orc_set_reference", [_VP, _P, _P, _P]),
             ("orc_enable_visc3d", [_VP, _P]),
+            ("orc_advance", [_VP, _P, _P, C.c_double, C.c_double, _P, _P, _P, _P]),
             ("orc_enable_visc3d_from_nodes", [_VP, _P, C.c_double, C.c_double, C.c_double]),
             ("orc_update", [_VP, _P, C.c_double]),
             ("orc_spinup", [_VP, _P, C.c_double, C.c_double, C.c_int, _P, C.POINTER(C.c_int), C.POINTER(C.c_int),
@@ -158,6 +159,14 @@ class Oracle:
 
     def enable_visc3d(self, pert):
         self._c(lib().orc_enable_visc3d(self.h, ptr(np.ascontiguousarray(pert, dtype=np.float64))))
+
+    def advance_interval(self, ice0, ice1, t0_yr, t1_yr, s_rot=None):
+        """stepper_advance driven directly: (rsl, C, sigma_lm) at t1."""
+        rsl, Cf, sig = np.zeros(self.ng), np.zeros(self.ng), np.zeros(2 * self.nlm)
+        a = [np.ascontiguousarray(x, dtype=np.float64) for x in (ice0, ice1)]
+        sr = None if s_rot is None else np.ascontiguousarray(s_rot, dtype=np.float64)
+        self._c(lib().orc_advance(self.h, ptr(a[0]), ptr(a[1]), t0_yr, t1_yr, ptr(sr), ptr(rsl), ptr(Cf), ptr(sig)))
+        return rsl, Cf, sig[0::2] + 1j * sig[1::2]
 
     def enable_visc3d_from_nodes(self, visc_node, lid_depth=0.0, lid_log10max=0.0, log10_cap=0.0):
         v = np.ascontiguousarray(visc_node, dtype=np.float64)

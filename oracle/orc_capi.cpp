@@ -315,6 +315,36 @@ int orc_spinup(OrcHandle* h, const double* h_ice_lgm, double t_cap, double tol, 
   return 0;
 }
 
+// vilma_timestep.f90:79-105 stepper_advance, driven directly: t0 becomes the
+// model time, ice0 the carried ice; s_rot may be null
+int orc_advance(OrcHandle* h, const double* ice0, const double* ice1, double t0_yr, double t1_yr,
+                const double* s_rot, double* rsl, double* C, double* sigma_lm) {
+  const int ng = h->sht.nphi * h->sht.nlat;
+  h->h_ice.assign(ice0, ice0 + ng);
+  std::vector<double> ice_new(ice1, ice1 + ng);
+  h->time_yr = t0_yr;
+  h->R.time = t0_yr * SEC_PER_YEAR;
+  int rc = stepper_advance(h->st, h->sht, h->R, h->sle, h->z_bed_eq.data(), h->h_ice.data(), ice_new.data(),
+                           h->h_ice_eq.data(), t0_yr * SEC_PER_YEAR, t1_yr * SEC_PER_YEAR, h->rsl.data(), h->C.data(),
+                           s_rot, h->sigma_lm.data());
+  if (rc) {
+    h->err = "vilma_timestep: the interval failed";
+    return rc;
+  }
+  h->h_ice = ice_new;
+  h->time_yr = t1_yr;
+  for (int i = 0; i < ng; ++i) h->z_bed[i] = h->z_bed_eq[i] - h->rsl[i];
+  update_bsl(h);
+  if (rsl) std::copy(h->rsl.begin(), h->rsl.end(), rsl);
+  if (C) std::copy(h->C.begin(), h->C.end(), C);
+  if (sigma_lm)
+    for (int lm = 0; lm < h->sht.nlm; ++lm) {
+      sigma_lm[2 * lm] = h->sigma_lm[lm].real();
+      sigma_lm[2 * lm + 1] = h->sigma_lm[lm].imag();
+    }
+  return 0;
+}
+
 // polar motion m (re, im) and the degree-2 constants kTe, hTe, k_s (fluid), k_s (flattening)
 int orc_get_rotation(OrcHandle* h, double* m, double* love) {
   if (m) {
