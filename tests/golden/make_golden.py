@@ -19,6 +19,13 @@ and writes the few numbers the tests use into tests/golden/*.json:
   data/benchmarks/rotation_spada2011/polar_motion_test3-2.txt (rows
   `load cw t m_Vb m_Gs ...`, G in the header comment).
 
+* martinec2018.npz: the Martinec et al. (2018) benchmark profiles of
+  data/benchmarks/sle_martinec2018/ as float32 (the tables are float32
+  output): A_fig10 (case A cap loading, all 721 rows: colatitude, uplift,
+  horizontal, geoid) and {C2,D3,E2,F1}_fig{10..13} (the sea-level cases, every
+  second row of the 7 columns: profile coordinate, u, th- and ph-horizontal,
+  potential increment -N g, sea surface, sea level).
+
 Run in a container where the reference is mounted:
     python tests/golden/make_golden.py /root/reference
 """
@@ -77,10 +84,23 @@ def rotation(ref):
     return out
 
 
+def martinec(ref):
+    import glob
+
+    d = os.path.join(ref, "data/benchmarks/sle_martinec2018")
+    out = {"A_fig10": np.loadtxt(os.path.join(d, "A_fig10_SBK.dat")).astype(np.float32)}
+    for fn in sorted(glob.glob(os.path.join(d, "*_fig1?_SBK.dat"))):
+        key = os.path.basename(fn)[: -len("_SBK.dat")]
+        if key != "A_fig10":
+            out[key] = np.loadtxt(fn)[::2].astype(np.float32)
+    return out
+
+
 if __name__ == "__main__":
     ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
     here = os.path.dirname(os.path.abspath(__file__))
     json.dump(love(ref), open(os.path.join(here, "love_M3L70V01.json"), "w"), indent=1)
     json.dump(disc(ref), open(os.path.join(here, "disc_spada2011.json"), "w"))
     json.dump(rotation(ref), open(os.path.join(here, "rotation_spada2011.json"), "w"), indent=1)
+    np.savez_compressed(os.path.join(here, "martinec2018.npz"), **martinec(ref))
     print("wrote golden fixtures to", here)
