@@ -229,22 +229,22 @@ __global__ void __launch_bounds__(128) k_drift_solve(DriftArgs A) {
       // dof j + 6 enters: F_{kb+1}, P_{kb+1} (no forcing), U_{kb+2}, V_{kb+2}
       w6 = (t < 2) ? 0.0 : bin[(2 * (jj >> 2) + (t - 2)) * 32 + lane];
       const double* col = bandc + jj * VG_LDAB;
+      // row interchange j <-> j + jp: every lane of the warp solves with the
+      // same degree's factor, so the branch is warp-uniform and a step
+      // without interchange costs one compare
       const int jp = (int)col[20];
-      const double x0 = w0;
-      double s = w0;
-      s = (jp == 1) ? w1 : s;
-      s = (jp == 2) ? w2 : s;
-      s = (jp == 3) ? w3 : s;
-      s = (jp == 4) ? w4 : s;
-      s = (jp == 5) ? w5 : s;
-      s = (jp == 6) ? w6 : s;
-      w1 = (jp == 1) ? x0 : w1;
-      w2 = (jp == 2) ? x0 : w2;
-      w3 = (jp == 3) ? x0 : w3;
-      w4 = (jp == 4) ? x0 : w4;
-      w5 = (jp == 5) ? x0 : w5;
-      w6 = (jp == 6) ? x0 : w6;
-      w0 = s;
+      if (jp != 0) {
+        const double x0 = w0;
+        switch (jp) {
+          case 1: w0 = w1; w1 = x0; break;
+          case 2: w0 = w2; w2 = x0; break;
+          case 3: w0 = w3; w3 = x0; break;
+          case 4: w0 = w4; w4 = x0; break;
+          case 5: w0 = w5; w5 = x0; break;
+          case 6: w0 = w6; w6 = x0; break;
+          default: break;  // offsets lie in 0 .. kl = 6 by construction
+        }
+      }
       if (valid) y[(size_t)j * nk] = w0;
       w1 -= col[13] * w0;
       w2 -= col[14] * w0;
