@@ -143,6 +143,9 @@ int vg_create(const vg_params* p, vg_handle** out) {
     VG_CUDA(cudaGetDevice(&h->device));
     VG_CUDA(cudaGetDeviceCount(&ndev));
     VG_CUDA(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
+    VG_CUDA(cudaStreamCreateWithFlags(&h->aux, cudaStreamNonBlocking));
+    VG_CUDA(cudaEventCreateWithFlags(&h->ev_fork, cudaEventDisableTiming));
+    VG_CUDA(cudaEventCreateWithFlags(&h->ev_join, cudaEventDisableTiming));
     vg::setup_handle(h);
     if (h->p.rotation) vg::rotation_setup(h);
     if (h->p.scheme == VG_SCHEME_TRAP) vg::trap_setup(h);
@@ -150,7 +153,7 @@ int vg_create(const vg_params* p, vg_handle** out) {
     h->mem_norm = vg::read_mem_norm(h, 0);
   });
   if (rc) {
-    delete h;
+    vg_destroy(h);
     return rc;
   }
   *out = h;
@@ -160,9 +163,14 @@ int vg_create(const vg_params* p, vg_handle** out) {
 int vg_destroy(vg_handle* h) {
   if (!h) return 0;
   if (h->stream) cudaStreamSynchronize(h->stream);
+  if (h->aux) cudaStreamSynchronize(h->aux);
   if (h->h_sc) cudaFreeHost(h->h_sc);
-  cudaStream_t s = h->stream;
+  cudaStream_t s = h->stream, a = h->aux;
+  cudaEvent_t e0 = h->ev_fork, e1 = h->ev_join;
   delete h;
+  if (e0) cudaEventDestroy(e0);
+  if (e1) cudaEventDestroy(e1);
+  if (a) cudaStreamDestroy(a);
   if (s) cudaStreamDestroy(s);
   return 0;
 }

@@ -124,6 +124,11 @@ struct vg_handle {
   std::string err;
   int device = 0;
   cudaStream_t stream = nullptr;
+  // second stream: the degree-1 drift (one CTA) runs there beside the band
+  // sweeps of degrees >= 2, forked after the forcing and joined before the
+  // drift is read
+  cudaStream_t aux = nullptr;
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   // sizes
   int nr = 0, ne = 0, ndof = 0, nk = 0, ne3d = 0;
   int kl = 0, ku = 0, kv = 0, ldab = 0;  // band of degrees >= 2

@@ -477,13 +477,19 @@ void launch_drift(vg_handle* h, int buf, double* dUn, double* dVn, double* dWn) 
     VG_CUDA(cudaFuncSetAttribute(k_drift_solve, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sw_smem));
     sw_attr = true;
   }
+  // degree 1 (slots 0, 1: reads their forcing, writes their drift) beside the
+  // band sweeps (slots >= 2), on the handle's second stream
+  VG_CUDA(cudaEventRecord(h->ev_fork, h->stream));
+  VG_CUDA(cudaStreamWaitEvent(h->aux, h->ev_fork, 0));
+  size_t shm = (size_t)(4 * 2 * h->nr + 4 * (2 * h->nr + 1)) * sizeof(double);
+  k_drift_deg1<<<1, 512, shm, h->aux>>>(A);
+  ++h->n_launch;
+  VG_CUDA(cudaGetLastError());
+  VG_CUDA(cudaEventRecord(h->ev_join, h->aux));
   k_drift_solve<<<(h->ntask + SW_WARPS - 1) / SW_WARPS, 32 * SW_WARPS, sw_smem, h->stream>>>(A);
   ++h->n_launch;
   VG_CUDA(cudaGetLastError());
-  size_t shm = (size_t)(4 * 2 * h->nr + 4 * (2 * h->nr + 1)) * sizeof(double);
-  k_drift_deg1<<<1, 512, shm, h->stream>>>(A);
-  ++h->n_launch;
-  VG_CUDA(cudaGetLastError());
+  VG_CUDA(cudaStreamWaitEvent(h->stream, h->ev_join, 0));
   if (h->tor_on) launch_drift_tor(h, buf, dWn);  // its own forcing, its own operator
 }
 
