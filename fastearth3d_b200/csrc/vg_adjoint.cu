@@ -574,8 +574,7 @@ void fwd_step(vg_handle* h, AdjWork& W, int n, int nsite, double dt) {
                                             W.obs.p + (size_t)n * nsite, W.resid.p + (size_t)n * nsite);
   ++h->n_launch;
   VG_CUDA(cudaGetLastError());
-  if (h->lat_visc) visc3d_advance(h, sig, dt);
-  launch_advance_1d(h, sig, dt);
+  advance_memory(h, sig, dt);
   h->cur = 1 - h->cur;
 }
 

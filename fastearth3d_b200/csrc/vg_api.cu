@@ -452,8 +452,7 @@ int vg_response_advance(vg_handle* h, const double* sigma_lm) {
   return guarded(h, [&] {
     const size_t n2 = 2 * (size_t)h->grid.nlm;
     h->d_sigma.upload(sigma_lm, n2, h->stream);
-    if (h->lat_visc) vg::visc3d_advance(h, h->d_sigma.p, h->dt);
-    vg::launch_advance_1d(h, h->d_sigma.p, h->dt);
+    vg::advance_memory(h, h->d_sigma.p, h->dt);
     h->cur = 1 - h->cur;
     h->mem_norm = vg::read_mem_norm(h, h->cur);
     h->time_s += h->dt;

@@ -251,11 +251,13 @@ void build_grid(Grid& G, int lmax, int nlat, int nphi, cudaStream_t s);
 // drift of memory buffer buf (-1: the current one) into the nodal targets
 // (nullptr: the handle's dUn, dVn) and the surface drift
 void launch_drift(vg_handle* h, int buf = -1, double* dUn = nullptr, double* dVn = nullptr, double* dWn = nullptr);
-// 1-D memory advance, current buffer -> the other one, with the strain of
-// (sigma, dUn, dVn) (nullptr: the handle's drift); trap: the trapezoidal rule
-// with sigma, dUn, dVn the means of the step's two ends
-void launch_advance_1d(vg_handle* h, const double* d_sigma, double dt, const double* dUn = nullptr,
-                       const double* dVn = nullptr, bool trap = false, const double* dWn = nullptr);
+// memory advance of one step (3-D elements pseudo-spectrally, the others per
+// slot), current buffer -> the other one, with the strain of (sigma, dUn,
+// dVn) (nullptr: the handle's drift), and the next buffer's per-slot norms and
+// their maximum; trap: the trapezoidal rule with sigma, dUn, dVn the means of
+// the step's two ends
+void advance_memory(vg_handle* h, const double* d_sigma, double dt, const double* dUn = nullptr,
+                    const double* dVn = nullptr, bool trap = false, const double* dWn = nullptr);
 void launch_apply(vg_handle* h, const double* d_sigma, double* d_u, double* d_n);
 void compute_mem_norm(vg_handle* h, int buf);
 double read_mem_norm(vg_handle* h, int buf);
@@ -272,8 +274,10 @@ void update_dev(vg_handle* h, const double* d_ice1, double dt_yr);
 void update_bsl(vg_handle* h);
 // 3-D (vg_visc3d.cu)
 void visc3d_enable(vg_handle* h, const double* pert_host);
-// 3-D memory advance (current buffer -> the other one); dUn, dVn and trap as
-// for launch_advance_1d (the pointwise factor M / (1 + M/2) when trap)
+// 3-D memory advance (current buffer -> the other one), folding the new
+// maxima into the next buffer's per-slot norms (zeroed by the caller); dUn,
+// dVn and trap as for advance_memory (the pointwise factor M / (1 + M/2) when
+// trap)
 void visc3d_advance(vg_handle* h, const double* d_sigma, double dt, const double* dUn = nullptr,
                     const double* dVn = nullptr, bool trap = false, const double* dWn = nullptr);
 // transposed 3-D advance (FP64 path) of one step whose longitude-pass grid the

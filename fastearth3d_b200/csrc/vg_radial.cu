@@ -527,8 +527,7 @@ void launch_apply(vg_handle* h, const double* d_sigma, double* d_u, double* d_n)
 // Forward-Euler memory advance (src/vilma_viscoelastic.f90:577-584) of the
 // spectrally advanced elements, out of place (cur -> nxt): one thread per
 // (slot, element, re/im). Each thread also folds |new memory| of its element
-// (or of the 3-D element the pseudo-spectral pass already wrote) into the
-// per-slot norm.
+// into the per-slot norm.
 __global__ void __launch_bounds__(256) k_advance_1d(const double* __restrict__ mem, double* __restrict__ nxt, int ne,
                                                     int nr, int nk, double dt, const double* __restrict__ sigma,
                                                     const int* __restrict__ kdeg, const int* __restrict__ k2lm,
@@ -538,6 +537,8 @@ __global__ void __launch_bounds__(256) k_advance_1d(const double* __restrict__ m
                                                     const double* __restrict__ MkPerDt,
                                                     const char* __restrict__ active, double* __restrict__ mnorm,
                                                     int trap) {
+  // 3-D elements (active[e] == 0) are advanced, and their maxima folded into
+  // mnorm, by the pseudo-spectral pass's scatter
   const int k = blockIdx.x * 32 + threadIdx.x, e = blockIdx.y * 8 + threadIdx.y, ri = blockIdx.z;
   double amax = 0.0;
   if (k < nk && e < ne) {
@@ -574,11 +575,6 @@ __global__ void __launch_bounds__(256) k_advance_1d(const double* __restrict__ m
         nxt[iC] = Cn;
         amax = nanmax(amax, nanmax(fabs(An), nanmax(fabs(Bn), fabs(Cn))));
       }
-    } else {
-#pragma unroll
-      for (int m = 0; m < 4; ++m)
-#pragma unroll
-        for (int s3 = 0; s3 < 3; ++s3) amax = nanmax(amax, fabs(nxt[mem_idx(s3, ri, e, m, k, ne, nk)]));
     }
   }
   __shared__ double red[8][33];
@@ -601,20 +597,42 @@ __global__ void k_norm_max(const double* __restrict__ mnorm, int nk, unsigned lo
   if (threadIdx.x == 0) *maxbits = (unsigned long long)__double_as_longlong(v);
 }
 
-void launch_advance_1d(vg_handle* h, const double* d_sigma, double dt, const double* dUn, const double* dVn,
-                       bool trap, const double* dWn) {
-  PhaseScope ps(h, VG_PH_ADVANCE_1D);
-  int nxt = 1 - h->cur;
+// Memory advance of one step, current buffer -> the other one: the 3-D
+// elements through the pseudo-spectral pass (its scatter folds their maxima
+// into the per-slot norms), the others spectrally (k_advance_1d). The two
+// write disjoint elements of the next buffer and fold maxima (order-free)
+// into the same norms, so without the toroidal channel the spectral advance
+// runs on the handle's second stream beside the 3-D pass; with phase timers on
+// they run one after the other so that each phase times its own kernels.
+void advance_memory(vg_handle* h, const double* d_sigma, double dt, const double* dUn, const double* dVn, bool trap,
+                    const double* dWn) {
+  const int nxt = 1 - h->cur;
   double* mn = h->d_mnorm.p + (size_t)nxt * h->nk;
   VG_CUDA(cudaMemsetAsync(mn, 0, h->nk * sizeof(double), h->stream));
-  dim3 grid((h->nk + 31) / 32, (h->ne + 7) / 8, 2);
-  k_advance_1d<<<grid, dim3(32, 8), 0, h->stream>>>(h->d_mem[h->cur].p, h->d_mem[nxt].p, h->ne, h->nr, h->nk, dt,
-                                                    d_sigma, h->d_kdeg.p, h->d_k2lm.p, h->d_Jr.p, h->d_xUn.p,
-                                                    h->d_xVn.p, dUn ? dUn : h->d_dUn.p, dVn ? dVn : h->d_dVn.p,
-                                                    h->d_mu.p, h->d_MkPerDt.p, h->d_active1d.p, mn, trap ? 1 : 0);
-  ++h->n_launch;
-  VG_CUDA(cudaGetLastError());
-  if (h->tor_on) launch_advance_1d_tor(h, dt, dWn, trap, mn);  // W is pure drift: no sigma x_Wn term
+  const bool v3 = h->lat_visc && h->ne3d > 0;
+  const bool side = v3 && !h->tor_on && !h->prof.on;
+  auto spectral = [&](cudaStream_t s) {
+    PhaseScope ps(h, VG_PH_ADVANCE_1D);
+    dim3 grid((h->nk + 31) / 32, (h->ne + 7) / 8, 2);
+    k_advance_1d<<<grid, dim3(32, 8), 0, s>>>(h->d_mem[h->cur].p, h->d_mem[nxt].p, h->ne, h->nr, h->nk, dt, d_sigma,
+                                              h->d_kdeg.p, h->d_k2lm.p, h->d_Jr.p, h->d_xUn.p, h->d_xVn.p,
+                                              dUn ? dUn : h->d_dUn.p, dVn ? dVn : h->d_dVn.p, h->d_mu.p,
+                                              h->d_MkPerDt.p, h->d_active1d.p, mn, trap ? 1 : 0);
+    ++h->n_launch;
+    VG_CUDA(cudaGetLastError());
+    if (h->tor_on) launch_advance_1d_tor(h, dt, dWn, trap, mn);  // W is pure drift: no sigma x_Wn term
+  };
+  if (side) {
+    VG_CUDA(cudaEventRecord(h->ev_fork, h->stream));
+    VG_CUDA(cudaStreamWaitEvent(h->aux, h->ev_fork, 0));
+    spectral(h->aux);
+    VG_CUDA(cudaEventRecord(h->ev_join, h->aux));
+    visc3d_advance(h, d_sigma, dt, dUn, dVn, trap, dWn);
+    VG_CUDA(cudaStreamWaitEvent(h->stream, h->ev_join, 0));
+  } else {
+    if (v3) visc3d_advance(h, d_sigma, dt, dUn, dVn, trap, dWn);
+    spectral(h->stream);
+  }
   k_norm_max<<<1, 1024, 0, h->stream>>>(mn, h->nk, h->d_maxbits.p + nxt);
   ++h->n_launch;
   VG_CUDA(cudaGetLastError());

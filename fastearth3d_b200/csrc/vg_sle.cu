@@ -793,8 +793,7 @@ void sle_solve_dev(vg_handle* h, double dt, bool report_only) {
   legendre_analysis_dev(h, h->d_F.p, 1, h->d_sigma.p);
   if (report_only) break;
   if (!trap) {
-    if (h->lat_visc) visc3d_advance(h, h->d_sigma.p, dt);
-    launch_advance_1d(h, h->d_sigma.p, dt);
+    advance_memory(h, h->d_sigma.p, dt);
     break;
   }
   if (trap_endpoint_pass(h, dt)) break;

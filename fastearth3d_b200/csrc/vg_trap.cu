@@ -125,8 +125,7 @@ bool trap_endpoint_pass(vg_handle* h, double dt) {
     VG_CUDA(cudaGetLastError());
   }
   const double* dWavg = h->tor_on ? h->d_dW_avg.p : nullptr;
-  if (h->lat_visc) visc3d_advance(h, h->d_sigma_avg.p, dt, h->d_dU_avg.p, h->d_dV_avg.p, true, dWavg);
-  launch_advance_1d(h, h->d_sigma_avg.p, dt, h->d_dU_avg.p, h->d_dV_avg.p, true, dWavg);
+  advance_memory(h, h->d_sigma_avg.p, dt, h->d_dU_avg.p, h->d_dV_avg.p, true, dWavg);
   d2d(h->d_sigma_next.p, h->d_sigma.p, (size_t)n2lm, s);
   launch_drift(h, 1 - h->cur, h->d_edUn.p, h->d_edVn.p, h->tor_on ? h->d_edWn.p : nullptr);  // solve_endpoint_drift
   ++h->couple_pass;

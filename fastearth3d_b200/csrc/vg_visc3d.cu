@@ -90,6 +90,7 @@ struct V3Args {
   const int *kdeg, *k2lm, *e3d;
   const double *Jr, *xUn, *xVn, *dUn, *dVn, *mu;
   int ne, nr, nk, ne3d, nf, ncf;  // ncf = 2 nf
+  double* mnext = nullptr;        // per-slot norms of the next buffer (the scatter folds its maxima in)
 };
 
 // one thread per (slot k, 3-D element): strain of both histories, 24 values,
@@ -592,12 +593,12 @@ static void lon_check(const vg_handle* h) {
 // ------------------------------------------------------------------ scatter
 
 // Channel normalisations and the increment form c += Delta
-// (src/vilma_response.f90:1281-1318): one thread per (slot, 3-D element).
-template <class T, int NQ = 6>
-__global__ void __launch_bounds__(256) k_v3_scatter(V3Args A, const T* __restrict__ R,
-                                                    const double* __restrict__ n6) {
-  const int k = blockIdx.x * 32 + threadIdx.x, ei = blockIdx.y * 8 + threadIdx.y;
-  if (k >= A.nk || ei >= A.ne3d) return;
+// (src/vilma_response.f90:1281-1318): one thread per (slot, 3-D element);
+// the block's maxima of |new memory| per slot go into A.mnext.
+template <class T, int NQ>
+__device__ __forceinline__ double v3_scatter_one(const V3Args& A, const T* __restrict__ R,
+                                                 const double* __restrict__ n6, int k, int ei) {
+  double amax = 0.0;
   const int e = A.e3d[ei], l = A.kdeg[k];
   const double J = A.Jr[l], nn = n6[l];
   const T* row = R + (size_t)k * NQ * A.ncf;
@@ -633,8 +634,30 @@ __global__ void __launch_bounds__(256) k_v3_scatter(V3Args A, const T* __restric
     for (int ri = 0; ri < 2; ++ri)
       for (int lam = 0; lam < 4; ++lam) {
         size_t idx = mem_idx(s3, ri, e, lam, k, A.ne, A.nk);
-        A.nxt[idx] = A.mem[idx] + d[lam][ri];
+        const double v = A.mem[idx] + d[lam][ri];
+        A.nxt[idx] = v;
+        amax = nanmax(amax, fabs(v));
       }
+  }
+  return amax;
+}
+
+template <class T, int NQ = 6>
+__global__ void __launch_bounds__(256) k_v3_scatter(V3Args A, const T* __restrict__ R,
+                                                    const double* __restrict__ n6) {
+  __shared__ double red[8][33];
+  const int k = blockIdx.x * 32 + threadIdx.x, ei = blockIdx.y * 8 + threadIdx.y;
+  double amax = 0.0;
+  if (k < A.nk && ei < A.ne3d) amax = v3_scatter_one<T, NQ>(A, R, n6, k, ei);
+  if (A.mnext) {  // the same in every thread of the block
+    red[threadIdx.y][threadIdx.x] = amax;
+    __syncthreads();
+    if (threadIdx.y == 0 && k < A.nk) {
+      double v = red[0][threadIdx.x];
+#pragma unroll
+      for (int t = 1; t < 8; ++t) v = nanmax(v, red[t][threadIdx.x]);
+      atomic_max_bits(reinterpret_cast<unsigned long long*>(A.mnext) + k, v);
+    }
   }
 }
 
@@ -767,6 +790,7 @@ void visc3d_advance(vg_handle* h, const double* d_sigma, double dt, const double
   A.ne3d = h->ne3d;
   A.nf = nf;
   A.ncf = ncf;
+  A.mnext = h->d_mnorm.p + (size_t)(1 - h->cur) * h->nk;
   dim3 gg((h->nk + 31) / 32, (h->ne3d + 7) / 8);
   v3_tile_attributes();
   if (h->p.visc3d_precision == VG_VISC3D_SPLIT_TC) {
