@@ -88,14 +88,17 @@ __device__ double integrate_rows(const double* row, const double* w, int nlat, d
   return total;
 }
 
-__global__ void k_finalize_C(SleScalars* sc, const double* __restrict__ rowpart, const double* __restrict__ w,
-                             int nlat, double dlon) {
-  const double c = integrate_rows(rowpart + RP_C * nlat, w, nlat, dlon);
-  if (threadIdx.x == 0) sc->C_int = c;
-}
+// the pass's ocean area, then (with an ocean) its ice and subgrid integrals
 __global__ void k_finalize_pass(SleScalars* sc, const double* __restrict__ rowpart, const double* __restrict__ w,
                                 int nlat, double dlon, int subgrid) {
-  if (!(sc->C_int > 0.0)) return;  // no ocean: the pass ends here (src/vilma_sle.f90:273-274)
+  __shared__ double s_c;
+  const double c = integrate_rows(rowpart + RP_C * nlat, w, nlat, dlon);  // valid in thread 0
+  if (threadIdx.x == 0) {
+    sc->C_int = c;
+    s_c = c;
+  }
+  __syncthreads();
+  if (!(s_c > 0.0)) return;  // no ocean: the pass ends here (src/vilma_sle.f90:273-274)
   const double d = integrate_rows(rowpart + RP_DIG * nlat, w, nlat, dlon);
   const double z = subgrid ? integrate_rows(rowpart + RP_ZETA * nlat, w, nlat, dlon) : 0.0;
   if (threadIdx.x == 0) {
@@ -763,7 +766,6 @@ void sle_solve_dev(vg_handle* h, double dt, bool report_only) {
     }
     k_pass_setup<<<nlat, 128, 0, s>>>(nphi, h->d_ice_now.p, h->d_dice_now.p, h->d_C.p, h->d_C0.p, h->d_z_bed_eq.p,
                                       h->d_dig.p, rp, nlat); ++h->n_launch;
-    k_finalize_C<<<1, FIN_THREADS, 0, s>>>(sc, rp, G.d_wts.p, nlat, dlon); ++h->n_launch;
     // no host round trip before the inner loop: with no ocean (C_int <= 0) the
     // kernels below return at once and the pass ends after the one read
     k_finalize_pass<<<1, FIN_THREADS, 0, s>>>(sc, rp, G.d_wts.p, nlat, dlon, p.sle_subgrid); ++h->n_launch;

@@ -130,8 +130,9 @@ def profile_points(k, c1, pfix):
     return np.clip(th, 1e-7, np.pi - 1e-7), lo
 
 
-def make_model(topo0, fixed_ocean, mk=vlib.default_params, cls=vlib.Model):
+def make_model(topo0, fixed_ocean, mk=vlib.default_params, cls=vlib.Model, scheme=0):
     p = mk()
+    p.scheme = scheme  # 0: forward Euler ("fe"), 2: trapezoidal ("trap")
     set_layers(p, M3L70V01)
     p.lmax, p.nlat, p.nphi = L, NLAT, NPHI
     p.dt_init = 20.0 * synth.SEC_PER_YEAR
@@ -144,11 +145,11 @@ def make_model(topo0, fixed_ocean, mk=vlib.default_params, cls=vlib.Model):
     return m
 
 
-def run_history(topo0, case):
+def run_history(topo0, case, scheme=0):
     h0, _, _, _, _, fixed, heaviside, _, _ = CASES[case]
     colat, w, lon = gauss_grid()
     cd = np.cos(distance(colat, lon, 25.0 * DEG, 75.0 * DEG))
-    m = make_model(topo0, fixed)
+    m = make_model(topo0, fixed, scheme=scheme)
     nsteps = NGROW if heaviside else NGROW + NHOLD
     ice = np.zeros((NLAT, NPHI))
     for istep in range(1, nsteps + 1):
@@ -156,7 +157,8 @@ def run_history(topo0, case):
         ca = np.cos(frac * 10.0 * DEG)
         ice = np.where(cd >= ca, frac * h0 * np.sqrt(np.maximum((cd - ca) / (1.0 - ca), 0.0)), 0.0)
         m.update(ice, 20.0)
-        assert m.info().n_sub_last == 1  # one 20-yr response step per interval, as the reference
+        if scheme == 0:
+            assert m.info().n_sub_last == 1  # one 20-yr response step per interval, as the reference
     return m, ice
 
 
@@ -184,8 +186,10 @@ def test_point_evaluator_matches_library_synthesis():
     assert np.abs(vph - dph).max() <= 1e-5 * np.abs(vph).max()
 
 
-@pytest.mark.parametrize("case", ["C2", "D3", "E2", "F1"])
-def test_martinec2018_sea_level_case(case, golden):
+@pytest.mark.parametrize("case,scheme", [("C2", 0), ("D3", 0), ("E2", 0), ("F1", 0), ("E2", 2)])
+def test_martinec2018_sea_level_case(case, scheme, golden):
+    """scheme 2: the trapezoidal scheme with its step-doubling controller
+    (adaptive sub-steps within each 20-yr interval) on the same case."""
     h0, bcol, blon, bmax, b0, fixed, heaviside, spin, pfix = CASES[case]
     colat, w, lon = gauss_grid()
     psi = distance(colat, lon, bcol * DEG, blon * DEG)
@@ -193,7 +197,7 @@ def test_martinec2018_sea_level_case(case, golden):
     area = (2.0 * np.pi / NPHI) * w[:, None] * np.ones(NPHI)
     topo0 = basin.copy()
     for _ in range(12 if spin else 1):
-        m, ice = run_history(topo0, case)
+        m, ice = run_history(topo0, case, scheme)
         rsl, _, C_oc, sigma = m.fields()
         rsl = rsl.reshape(NLAT, NPHI)
         if not spin:
@@ -221,10 +225,13 @@ def test_martinec2018_sea_level_case(case, golden):
     rsl_lm = m.analysis(rsl.reshape(-1))
     N_grid = m.synthesis(N_lm).reshape(NLAT, NPHI)
     u_grid = m.synthesis(u_lm).reshape(NLAT, NPHI)
-    # the sea-level equation's decomposition rsl = N - u + esl holds on the whole grid
+    # the sea-level equation's decomposition rsl = N - u + esl holds on the whole
+    # grid (trapezoidal: up to the sea-level <-> memory co-convergence tolerance,
+    # the stored drift being the last endpoint pass's)
     shift = rsl - (N_grid - u_grid)
     esl = float((area * shift).sum() / (4.0 * np.pi))
-    assert np.abs(shift - esl).max() <= 1e-6 * np.abs(rsl).max(), np.abs(shift - esl).max()
+    tol_dec = 1e-6 if scheme == 0 else 1e-3
+    assert np.abs(shift - esl).max() <= tol_dec * np.abs(rsl).max(), np.abs(shift - esl).max()
 
     errs = {}
     for k in range(4):
@@ -245,7 +252,7 @@ def test_martinec2018_sea_level_case(case, golden):
             "sle": np.abs(sle - ref[:, 6]).max() / np.abs(ref[:, 6]).max(),
         }
         errs[f"fig{10 + k}"] = e
-    print(case, "esl", esl, {f: {c: round(100 * v, 2) for c, v in e.items()} for f, e in errs.items()})
+    print(case, "scheme", scheme, "esl", esl, {f: {c: round(100 * v, 2) for c, v in e.items()} for f, e in errs.items()})
     for f, e in errs.items():
         for c, v in e.items():
             assert v <= TOL[c], (case, f, c, v)
