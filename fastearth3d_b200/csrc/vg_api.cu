@@ -146,6 +146,9 @@ int vg_create(const vg_params* p, vg_handle** out) {
     VG_CUDA(cudaStreamCreateWithFlags(&h->aux, cudaStreamNonBlocking));
     VG_CUDA(cudaEventCreateWithFlags(&h->ev_fork, cudaEventDisableTiming));
     VG_CUDA(cudaEventCreateWithFlags(&h->ev_join, cudaEventDisableTiming));
+    VG_CUDA(cudaStreamCreateWithFlags(&h->aux2, cudaStreamNonBlocking));
+    VG_CUDA(cudaEventCreateWithFlags(&h->ev_dfork, cudaEventDisableTiming));
+    VG_CUDA(cudaEventCreateWithFlags(&h->ev_djoin, cudaEventDisableTiming));
     vg::setup_handle(h);
     if (h->p.rotation) vg::rotation_setup(h);
     if (h->p.scheme == VG_SCHEME_TRAP) vg::trap_setup(h);
@@ -164,12 +167,14 @@ int vg_destroy(vg_handle* h) {
   if (!h) return 0;
   if (h->stream) cudaStreamSynchronize(h->stream);
   if (h->aux) cudaStreamSynchronize(h->aux);
+  if (h->aux2) cudaStreamSynchronize(h->aux2);
   if (h->h_sc) cudaFreeHost(h->h_sc);
-  cudaStream_t s = h->stream, a = h->aux;
-  cudaEvent_t e0 = h->ev_fork, e1 = h->ev_join;
+  cudaStream_t s = h->stream, a = h->aux, a2 = h->aux2;
+  cudaEvent_t ev[4] = {h->ev_fork, h->ev_join, h->ev_dfork, h->ev_djoin};
   delete h;
-  if (e0) cudaEventDestroy(e0);
-  if (e1) cudaEventDestroy(e1);
+  for (cudaEvent_t e : ev)
+    if (e) cudaEventDestroy(e);
+  if (a2) cudaStreamDestroy(a2);
   if (a) cudaStreamDestroy(a);
   if (s) cudaStreamDestroy(s);
   return 0;

@@ -129,6 +129,10 @@ struct vg_handle {
   // drift is read
   cudaStream_t aux = nullptr;
   cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+  // the whole drift on the second stream (its degree 1 on a third) beside the
+  // sea-level pass setup, joined before the fused loop reads it
+  cudaStream_t aux2 = nullptr;
+  cudaEvent_t ev_dfork = nullptr, ev_djoin = nullptr;
   // sizes
   int nr = 0, ne = 0, ndof = 0, nk = 0, ne3d = 0;
   int kl = 0, ku = 0, kv = 0, ldab = 0;  // band of degrees >= 2
@@ -251,6 +255,8 @@ void build_grid(Grid& G, int lmax, int nlat, int nphi, cudaStream_t s);
 // drift of memory buffer buf (-1: the current one) into the nodal targets
 // (nullptr: the handle's dUn, dVn) and the surface drift
 void launch_drift(vg_handle* h, int buf = -1, double* dUn = nullptr, double* dVn = nullptr, double* dWn = nullptr);
+// the same without the toroidal drift, the band sweeps on s0 and degree 1 on s1
+void launch_drift_on(vg_handle* h, int buf, double* dUn, double* dVn, cudaStream_t s0, cudaStream_t s1);
 // memory advance of one step (3-D elements pseudo-spectrally, the others per
 // slot), current buffer -> the other one, with the strain of (sigma, dUn,
 // dVn) (nullptr: the handle's drift), and the next buffer's per-slot norms and

@@ -432,9 +432,7 @@ __global__ void __launch_bounds__(512) k_drift_deg1(DriftArgs A) {
   }
 }
 
-void launch_drift(vg_handle* h, int buf, double* dUn, double* dVn, double* dWn) {
-  PhaseScope ps(h, VG_PH_DRIFT);
-  if (buf < 0) buf = h->cur;
+void launch_drift_on(vg_handle* h, int buf, double* dUn, double* dVn, cudaStream_t s0, cudaStream_t s1) {
   DriftArgs A;
   A.mem = h->d_mem[buf].p;
   A.mnorm = h->d_mnorm.p + (size_t)buf * h->nk;
@@ -468,7 +466,7 @@ void launch_drift(vg_handle* h, int buf, double* dUn, double* dVn, double* dWn) 
   A.tasks = h->d_tasks.p;
   A.ntask = h->ntask;
   dim3 rgrid((h->nk + 31) / 32, (h->nr + 3) / 4, 2);
-  k_drift_rhs<<<rgrid, dim3(32, 4), 0, h->stream>>>(A);
+  k_drift_rhs<<<rgrid, dim3(32, 4), 0, s0>>>(A);
   ++h->n_launch;
   VG_CUDA(cudaGetLastError());
   const size_t sw_smem = (size_t)SW_WARPS * SW_WARP * sizeof(double);
@@ -479,17 +477,24 @@ void launch_drift(vg_handle* h, int buf, double* dUn, double* dVn, double* dWn) 
   }
   // degree 1 (slots 0, 1: reads their forcing, writes their drift) beside the
   // band sweeps (slots >= 2), on the handle's second stream
-  VG_CUDA(cudaEventRecord(h->ev_fork, h->stream));
-  VG_CUDA(cudaStreamWaitEvent(h->aux, h->ev_fork, 0));
+  VG_CUDA(cudaEventRecord(h->ev_fork, s0));
+  VG_CUDA(cudaStreamWaitEvent(s1, h->ev_fork, 0));
   size_t shm = (size_t)(4 * 2 * h->nr + 4 * (2 * h->nr + 1)) * sizeof(double);
-  k_drift_deg1<<<1, 512, shm, h->aux>>>(A);
+  k_drift_deg1<<<1, 512, shm, s1>>>(A);
   ++h->n_launch;
   VG_CUDA(cudaGetLastError());
-  VG_CUDA(cudaEventRecord(h->ev_join, h->aux));
-  k_drift_solve<<<(h->ntask + SW_WARPS - 1) / SW_WARPS, 32 * SW_WARPS, sw_smem, h->stream>>>(A);
+  VG_CUDA(cudaEventRecord(h->ev_join, s1));
+  k_drift_solve<<<(h->ntask + SW_WARPS - 1) / SW_WARPS, 32 * SW_WARPS, sw_smem, s0>>>(A);
   ++h->n_launch;
   VG_CUDA(cudaGetLastError());
-  VG_CUDA(cudaStreamWaitEvent(h->stream, h->ev_join, 0));
+  VG_CUDA(cudaStreamWaitEvent(s0, h->ev_join, 0));
+}
+
+
+void launch_drift(vg_handle* h, int buf, double* dUn, double* dVn, double* dWn) {
+  PhaseScope ps(h, VG_PH_DRIFT);
+  if (buf < 0) buf = h->cur;
+  launch_drift_on(h, buf, dUn, dVn, h->stream, h->aux);
   if (h->tor_on) launch_drift_tor(h, buf, dWn);  // its own forcing, its own operator
 }
 

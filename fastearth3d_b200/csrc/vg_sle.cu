@@ -745,12 +745,28 @@ void sle_solve_dev(vg_handle* h, double dt, bool report_only) {
   if (!p.sle_warm_start) VG_CUDA(cudaMemsetAsync(h->d_rsl.p, 0, ng * sizeof(double), s));
   VG_CUDA(cudaMemsetAsync(h->d_wcorr.p, 0, ng * sizeof(double), s));
   VG_CUDA(cudaMemsetAsync(sc, 0, sizeof(SleScalars), s));
+  const bool trap = p.scheme == VG_SCHEME_TRAP && !report_only;
+  // response_begin_step. Forward Euler without the toroidal channel: the drift
+  // (its degree 1 beside the band sweeps) runs on the second stream while this
+  // stream sets up the first pass (ocean function, row integrals: none of the
+  // drift's buffers), and is joined before the fused loop reads it.
+  bool drift_pending = !trap && !h->tor_on && !h->prof.on;
+  if (drift_pending) {
+    VG_CUDA(cudaEventRecord(h->ev_dfork, s));
+    VG_CUDA(cudaStreamWaitEvent(h->aux, h->ev_dfork, 0));
+    launch_drift_on(h, h->cur, nullptr, nullptr, h->aux, h->aux2);
+    VG_CUDA(cudaEventRecord(h->ev_djoin, h->aux));
+  } else {
+    launch_drift(h);
+  }
+  auto join_drift = [&]() {
+    if (drift_pending) VG_CUDA(cudaStreamWaitEvent(s, h->ev_djoin, 0));
+    drift_pending = false;
+  };
   k_ocean0<<<eg, eb, 0, s>>>(ng, h->d_z_bed_eq.p, h->d_ice_now.p, h->d_dice_now.p, h->d_C0.p); ++h->n_launch;
-  launch_drift(h);  // response_begin_step
   // the sea-level <-> memory co-convergence (src/vilma_sle.f90:218-365): one
   // pass for forward Euler; trapezoid endpoint passes until the surface drift
   // settles for the trapezoidal scheme
-  const bool trap = p.scheme == VG_SCHEME_TRAP && !report_only;
   if (trap) trap_prepare(h);
   const int n_mem = trap ? std::max(1, p.sle_max_mem_iter) : 1;
   h->n_inner_last = 0;
@@ -771,6 +787,7 @@ void sle_solve_dev(vg_handle* h, double dt, bool report_only) {
     k_finalize_pass<<<1, FIN_THREADS, 0, s>>>(sc, rp, G.d_wts.p, nlat, dlon, p.sle_subgrid); ++h->n_launch;
     k_wcorr<<<eg, eb, 0, s>>>(sc, ng, p.sle_subgrid, h->d_z_bed_eq.p, h->d_C.p, h->d_C0.p, h->d_wcorr.p);
     ++h->n_launch;
+    join_drift();
     {
       PhaseScope ps(h, VG_PH_SLE);
       launch_inner_loop(h);
@@ -789,6 +806,7 @@ void sle_solve_dev(vg_handle* h, double dt, bool report_only) {
     h->n_flip_last = h->h_sc->flips;
     if (h->h_sc->flips == 0) break;
   }
+  join_drift();  // (already joined unless the pass loop was empty)
   // closing load, its analysis, and the memory advance (src/vilma_sle.f90:353-358)
   k_load_fourier<<<nlat, 128, nphi * sizeof(double), s>>>(nphi, nlat, M, h->d_dig.p, h->d_C.p, h->d_rsl.p,
                                                           h->d_wcorr.p, G.d_cos.p, G.d_sin.p, h->d_F.p); ++h->n_launch;
