@@ -411,6 +411,13 @@ int vg_stream(vg_handle* h, void** stream) {
   });
 }
 
+int vg_set_wait_limit(vg_handle* h, double seconds) {
+  return guarded(h, [&] {
+    if (!(seconds >= 0.0) || seconds > 60.0) throw vg::Error("vg_set_wait_limit: seconds must be in [0, 60]");
+    h->wait_ns = (unsigned long long)(seconds * 1.0e9);
+  });
+}
+
 int vg_profile_enable(vg_handle* h, int on) {
   return guarded(h, [&] {
     if (h->prof.on && !on) vg::prof_collect(h);

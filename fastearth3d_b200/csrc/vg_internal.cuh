@@ -123,6 +123,11 @@ struct vg_handle {
   vg_params p;
   std::string err;
   int device = 0;
+  // bound on the device-side waits that hand work between CTAs or warps (grid
+  // barriers of the fused sea-level loop, producer / consumer waits of the
+  // tensor-core stages); a wait that runs out raises a status the host turns
+  // into an error (vg_set_wait_limit)
+  unsigned long long wait_ns = 2000000000ull;
   cudaStream_t stream = nullptr;
   // second stream: the degree-1 drift (one CTA) runs there beside the band
   // sweeps of degrees >= 2, forked after the forcing and joined before the

@@ -3,15 +3,17 @@
 // file-scope device array, so that a call allocates no device or host memory.
 //
 // The scratch is one static array per device (the module's copy of the
-// symbol). Its address is looked up once per device, with that device
-// current, through cudaGetSymbolAddress; that first lookup may load the
-// module, so make the first call on a device before any stream capture.
+// symbol). Its device address is looked up on every call, with the handle's
+// device current, through cudaGetSymbolAddress: the address belongs to the
+// current context, so it stays right across a cudaDeviceReset or a new
+// context on the same ordinal (a cached address would then point at freed
+// memory). Once the module is loaded the lookup is a table search; the first
+// call on a device may load the module, so make it before any stream capture.
 // Nothing in the scratch has to start at zero: each call's Fourier stage
 // writes every element the Legendre stage then reads. Calls that overlap in
 // time on one device (other streams, other handles, other host threads) share
 // the array and race; order them on one stream or synchronise between them.
 #include <cstdio>
-#include <mutex>
 
 #include "vg_internal.cuh"
 
@@ -19,19 +21,12 @@ static __device__ __align__(256) double g_fourier_scratch[VG_NOALLOC_SCRATCH_DOU
 
 namespace {
 
-constexpr int kMaxDevices = 64;
-double* g_scratch_addr[kMaxDevices] = {};
-std::mutex g_scratch_mu;
-
-double* scratch_of_device(int dev) {
-  if (dev < 0 || dev >= kMaxDevices) throw vg::Error("vg_sht_analysis_noalloc: device ordinal out of range");
-  std::lock_guard<std::mutex> lock(g_scratch_mu);
-  if (!g_scratch_addr[dev]) {
-    void* p = nullptr;
-    VG_CUDA(cudaGetSymbolAddress(&p, g_fourier_scratch));
-    g_scratch_addr[dev] = static_cast<double*>(p);
-  }
-  return g_scratch_addr[dev];
+// device address of the scratch in the current context
+double* scratch_address() {
+  void* p = nullptr;
+  VG_CUDA(cudaGetSymbolAddress(&p, g_fourier_scratch));
+  if (!p) throw vg::Error("vg_sht_analysis_noalloc: no device address for the scratch array");
+  return static_cast<double*>(p);
 }
 
 }  // namespace
@@ -54,7 +49,7 @@ extern "C" int vg_sht_analysis_noalloc(vg_handle* h, const double* d_f, double* 
     int dev = -1;
     VG_CUDA(cudaGetDevice(&dev));
     if (dev != h->device) throw vg::Error("vg_sht_analysis_noalloc: the handle's device is not the current device");
-    double* F = scratch_of_device(dev);
+    double* F = scratch_address();
     vg::fourier_analysis_dev(h, d_f, batch, F);
     vg::legendre_analysis_dev(h, F, batch, d_q_lm);
     return 0;

@@ -303,9 +303,8 @@ struct InnerArgs {
   double *rsl, *F, *sigma, *ulm, *Gp, *Sraw, *rowpart;
   SleScalars* sc;
   unsigned int* bar;  // count, generation, error
+  unsigned long long wait_ns;  // bound on a grid barrier's wait (the handle's wait limit, 2 s by default)
 };
-
-constexpr unsigned long long BAR_WAIT_NS = 2000000000ull;  // 2 s bound on a grid barrier
 
 __device__ __forceinline__ unsigned long long gtimer_ns() {
   unsigned long long t;
@@ -315,7 +314,7 @@ __device__ __forceinline__ unsigned long long gtimer_ns() {
 
 // Sense-counting grid barrier with a bounded wait. Returns false (in every
 // thread of the CTA) if it timed out or another CTA reported a timeout.
-__device__ bool grid_barrier(unsigned int* bar, unsigned int& gen) {
+__device__ bool grid_barrier(unsigned int* bar, unsigned int& gen, unsigned long long wait_ns) {
   __shared__ int s_ok;
   __syncthreads();
   if (threadIdx.x == 0) {
@@ -330,7 +329,7 @@ __device__ bool grid_barrier(unsigned int* bar, unsigned int& gen) {
     } else {
       const unsigned long long t0 = gtimer_ns();
       while (*vgen == gen) {
-        if (gtimer_ns() - t0 > BAR_WAIT_NS) {
+        if (gtimer_ns() - t0 > wait_ns) {
           atomicExch(bar + 2, 1u);
           ok = 0;
           break;
@@ -410,7 +409,7 @@ __global__ void __launch_bounds__(512) k_sle_inner(InnerArgs A) {
   if (!(A.sc->C_int > 0.0)) return;  // no ocean: nothing to redistribute (every CTA reads the same value)
   // L of the first iteration
   for (int j = blockIdx.x; j < nlat; j += gridDim.x) sle_row_load(A, j, sm, part);
-  if (!grid_barrier(A.bar, gen)) return bar_fail(A);
+  if (!grid_barrier(A.bar, gen, A.wait_ns)) return bar_fail(A);
   for (int it = 1; it <= A.n_inner; ++it) {
     // A. Legendre analysis (warp per lm, four lm of a warp at once) and the
     //    affine response u, N
@@ -480,7 +479,7 @@ __global__ void __launch_bounds__(512) k_sle_inner(InnerArgs A) {
         }
       }
     }
-    if (!grid_barrier(A.bar, gen)) return bar_fail(A);
+    if (!grid_barrier(A.bar, gen, A.wait_ns)) return bar_fail(A);
     // S. Legendre synthesis of u and N in chunks of at most SLE_LCH degrees: a
     //    thread per (chunk, j), partial sums Gp[j][chunk][u re, u im, N re, N im]
     //    (one 32-byte sector per thread; a row's partials contiguous)
@@ -507,7 +506,7 @@ __global__ void __launch_bounds__(512) k_sle_inner(InnerArgs A) {
       o[2] = a2;
       o[3] = a3;
     }
-    if (!grid_barrier(A.bar, gen)) return bar_fail(A);
+    if (!grid_barrier(A.bar, gen, A.wait_ns)) return bar_fail(A);
     // R. longitude synthesis (g(i) = G_0 + 2 sum_m Re G_m e^{i m phi_i}, even and
     //    odd m apart, tpi threads per longitude pair (i, i + half)),
     //    Sraw = N - u (+ s_rot), row sums of C Sraw
@@ -587,7 +586,7 @@ __global__ void __launch_bounds__(512) k_sle_inner(InnerArgs A) {
       acc = block_sum(acc, red);
       if (tid == 0) A.rowpart[RP_CS * nlat + j] = acc;
     }
-    if (!grid_barrier(A.bar, gen)) return bar_fail(A);
+    if (!grid_barrier(A.bar, gen, A.wait_ns)) return bar_fail(A);
     // U. dphi in every CTA (rows in order by thread 0: the same value everywhere)
     {
       const double Cs = integrate_rows(A.rowpart + RP_CS * nlat, A.wts, nlat, A.dlon);
@@ -619,7 +618,7 @@ __global__ void __launch_bounds__(512) k_sle_inner(InnerArgs A) {
       }
       sle_row_load(A, j, sm, part);  // L of the next iteration (unused if this one converged)
     }
-    if (!grid_barrier(A.bar, gen)) return bar_fail(A);
+    if (!grid_barrier(A.bar, gen, A.wait_ns)) return bar_fail(A);
     // convergence (src/vilma_sle.f90:330-338), the same decision in every CTA
     {
       double dmax = 0.0, smax = 0.0;
@@ -715,6 +714,7 @@ static void launch_inner_loop(vg_handle* h) {
   A.rowpart = h->d_rowpart.p;
   A.sc = h->d_sc_.p;
   A.bar = h->d_gbar.p;
+  A.wait_ns = h->wait_ns;
   VG_CUDA(cudaMemsetAsync(h->d_gbar.p, 0, 4 * sizeof(unsigned int), s));
   const size_t shm = sle_inner_smem(h);
   void* args[] = {&A};

@@ -808,11 +808,11 @@ void visc3d_tc_enable(vg_handle* h) {
     J.info.kvalid = std::max(0, kvalid);
     if (J.info.nvalid == 0 || J.info.kvalid == 0) {
       J.info.kpad = 0;
-      J.info.npad = 8;
+      J.info.npad = 16;
       J.info.off = 0;
       return J;
     }
-    J.info.npad = round_up(J.info.nvalid, 8);
+    J.info.npad = round_up(J.info.nvalid, 16);  // M = 128 MMAs take N in steps of 16
     J.info.kpad = round_up(J.info.kvalid, KC);
     J.info.off = off;
     off += 2LL * J.info.kpad * J.info.npad;

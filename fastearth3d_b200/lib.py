@@ -64,6 +64,7 @@ _SIGS = [
     ("vg_sht_analysis_noalloc", [_VP, C.c_void_p, C.c_void_p, C.c_int]),
     ("vg_stream", [_VP, C.POINTER(C.c_void_p)]),
     ("vg_profile_enable", [_VP, C.c_int]),
+    ("vg_set_wait_limit", [_VP, C.c_double]),
     ("vg_profile_read", [_VP, _P, C.POINTER(C.c_longlong)]),
 ]
 EXPORTS = [n for n, _ in _SIGS] + ["vg_last_error"]

@@ -338,9 +338,11 @@ int vg_sht_synthesis(vg_handle* h, const double* q_lm, double* f);
  * cannot tolerate the implicit synchronisation an allocation brings. The
  * Fourier scratch is a file-scope device array of VG_NOALLOC_SCRATCH_DOUBLES
  * doubles per device, so 2 * (mmax + 1) * nlat * batch must not exceed it
- * (larger requests return an error); its address is looked up once per
- * device, with the handle's device current (make the first call before any
- * stream capture). The scratch carries nothing between calls. Calls that
+ * (larger requests return an error); its address in the current context is
+ * looked up on every call, with the handle's device current, so a
+ * cudaDeviceReset between calls is safe (the first call on a device may load
+ * the module: make it before any stream capture). The scratch carries
+ * nothing between calls. Calls that
  * overlap in time on one device share that array and race: order them on
  * one stream. */
 #define VG_NOALLOC_SCRATCH_DOUBLES (1 << 19)
@@ -349,6 +351,15 @@ int vg_sht_analysis_noalloc(vg_handle* h, const double* d_f, double* d_q_lm, int
 /* The CUDA stream (cudaStream_t) all of the handle's work is ordered on, so a
  * caller can record events on it. */
 int vg_stream(vg_handle* h, void** stream);
+/* Bound, in seconds (default 2, at most 60), on every device-side wait that
+ * hands work from one CTA or warp to another: the grid barriers of the fused
+ * sea-level loop and the producer / consumer waits of the tensor-core stages
+ * (no reference counterpart: the reference has no device code). A wait that
+ * runs out ends its kernel early with a status bit, and the call that
+ * launched it returns nonzero with a message; waits for the hardware's own
+ * copies and matrix operations keep their fixed bound. For hosts that want
+ * a hung peer reported sooner, and for tests of that error path. */
+int vg_set_wait_limit(vg_handle* h, double seconds);
 /* Enable (1) or disable (0) the phase timers; vg_profile_read returns the
  * accumulated milliseconds and call counts per phase (VG_NPHASE each) since
  * the last read and resets them. */

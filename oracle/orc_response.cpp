@@ -2,6 +2,7 @@
 // Viscoelastic field driver: per-degree operators and unit-load response,
 // Maxwell memory kernel, drift solve with the skip gate, affine apply, the
 // forward-Euler memory advance, and the pseudo-spectral 3-D advance.
+#include <string>
 #include <algorithm>
 #include <cmath>
 #include <stdexcept>
@@ -245,21 +246,34 @@ void response_init_ve(Response& R, const Earth& e, const Mesh& m, const Sht& s, 
     R.Jr[l] = (double)l * (double)(l + 1);
     ve_strain_constants(R.Jr[l], &R.nrmc[l * 4], &R.sa[l * 16], &R.sb[l * 16], &R.sc[l * 16]);
   }
+  // an exception may not leave an OpenMP region: the first failing degree's
+  // message is kept and rethrown after the loop (the reference stops there)
+  std::string first_error;
+  int first_error_l = L + 1;
 #pragma omp parallel for schedule(dynamic)
   for (int l = 1; l <= L; ++l) {
-    std::vector<double> bb(R.ndof), xx(R.ndof);
-    radial_operator_assemble(R.ops[l], e, m, l);
-    radial_operator_load_rhs(R.ops[l], 1.0, bb.data());
-    radial_operator_solve_vec(R.ops[l], bb.data(), xx.data(), nullptr);
-    if (l == 1 && R.deg1_cm) deg1_to_cm(R.ops[l], xx.data());
-    R.gu[l] = xx[idx_u(nr - 1)];
-    R.gn[l] = -xx[idx_f(nr - 1)] / R.g;
-    R.gv[l] = xx[idx_v(nr - 1)];
-    for (int node = 0; node < nr; ++node) {
-      R.xUn[(size_t)l * nr + node] = xx[idx_u(node)];
-      R.xVn[(size_t)l * nr + node] = xx[idx_v(node)];
+    try {
+      std::vector<double> bb(R.ndof), xx(R.ndof);
+      radial_operator_assemble(R.ops[l], e, m, l);
+      radial_operator_load_rhs(R.ops[l], 1.0, bb.data());
+      radial_operator_solve_vec(R.ops[l], bb.data(), xx.data(), nullptr);
+      if (l == 1 && R.deg1_cm) deg1_to_cm(R.ops[l], xx.data());
+      R.gu[l] = xx[idx_u(nr - 1)];
+      R.gn[l] = -xx[idx_f(nr - 1)] / R.g;
+      R.gv[l] = xx[idx_v(nr - 1)];
+      for (int node = 0; node < nr; ++node) {
+        R.xUn[(size_t)l * nr + node] = xx[idx_u(node)];
+        R.xVn[(size_t)l * nr + node] = xx[idx_v(node)];
+      }
+    } catch (const std::exception& ex) {
+#pragma omp critical(orc_operator_error)
+      if (l < first_error_l) {
+        first_error_l = l;
+        first_error = ex.what();
+      }
     }
   }
+  if (!first_error.empty()) throw std::runtime_error(first_error);
   if (L >= 1 && !R.deg1_cm) R.gn[1] = 0.0;
   // degree-grouped slot map
   R.nk = 0;
@@ -935,20 +949,42 @@ double response_max_rate(const Response& R) {
   return rate;
 }
 
-// vilma_response.f90:1795-1811
+// vilma_response.f90:1795-1811. The guard that reads this norm treats it as
+// non-finite for a NaN memory (vilma_timestep.f90:204, "finite = (err_inf <=
+// huge(1.0_wp)) ! .false. for NaN / +Inf"); Fortran leaves MAX with a NaN
+// argument to the processor, so the scan propagates NaN explicitly to keep
+// that stated meaning (finite values: the same maximum as absmax6).
+static inline double nan_max(double a, double b) { return (a != a || b != b) ? a + b : std::max(a, b); }
+
+static double absmax6_nan(int n, const double* x1, const double* x2, const double* x3, const double* x4,
+                          const double* x5, const double* x6) {
+  double amax = 0.0;
+  for (int i = 0; i < n; ++i) {
+    amax = nan_max(amax, std::fabs(x1[i]));
+    amax = nan_max(amax, std::fabs(x2[i]));
+    amax = nan_max(amax, std::fabs(x3[i]));
+    amax = nan_max(amax, std::fabs(x4[i]));
+    amax = nan_max(amax, std::fabs(x5[i]));
+    amax = nan_max(amax, std::fabs(x6[i]));
+  }
+  return amax;
+}
+
 double response_memory_norm(const Response& R) {
   const int nb = 4 * R.ne;
-  double nrm = 0.0;
-#pragma omp parallel for reduction(max : nrm) schedule(static)
+  std::vector<double> part((size_t)R.nk, 0.0);
+#pragma omp parallel for schedule(static)
   for (int k = 0; k < R.nk; ++k) {
     size_t o = (size_t)k * nb;
-    nrm = std::max(nrm, absmax6(nb, &R.Are[o], &R.Aim[o], &R.Bre[o], &R.Bim[o], &R.Cre[o], &R.Cim[o]));
+    part[k] = absmax6_nan(nb, &R.Are[o], &R.Aim[o], &R.Bre[o], &R.Bim[o], &R.Cre[o], &R.Cim[o]);
   }
+  double nrm = 0.0;
+  for (int k = 0; k < R.nk; ++k) nrm = nan_max(nrm, part[k]);
   if (R.nlam > NLAM) {
     const int nbt = 2 * R.ne;
     for (int k = 0; k < R.nk; ++k) {
       size_t o = (size_t)k * nbt;
-      nrm = std::max(nrm, absmax6(nbt, &R.Atre[o], &R.Atim[o], &R.Btre[o], &R.Btim[o], &R.Ctre[o], &R.Ctim[o]));
+      nrm = nan_max(nrm, absmax6_nan(nbt, &R.Atre[o], &R.Atim[o], &R.Btre[o], &R.Btim[o], &R.Ctre[o], &R.Ctim[o]));
     }
   }
   return nrm;
