@@ -41,16 +41,21 @@ METRIC = "steps/s @lmax=128 3D visc: batched vs plain GPU, rsl err<=1e-8; grad/f
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=None,
+                    help="timed steps (default: 300 for the single-instance workloads, so that each arm's timed "
+                         "region lasts over a second; 20 for c4_ensemble)")
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default=DEFAULT_WORKLOAD)
     ap.add_argument("--cpu-sample-s", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--precision", default="split_tc", choices=["split_tc", "fp64"],
-                    help="3-D stress products of the timed arm")
+    ap.add_argument("--precision", default="exact_tc", choices=["exact_tc", "split_tc", "fp64"],
+                    help="3-D stress products of the timed arm: exact int8-digit tensor-core products (default), "
+                         "two-term TF32 tensor-core products, or FP64 on the CUDA cores")
     ap.add_argument("--plain", default="on", choices=["on", "off"],
-                    help="also time the plain FP64 arm beside split_tc (and report the rsl error between them)")
+                    help="also time the plain FP64 arm beside the tensor-core arm (and report the rsl error between them)")
+    ap.add_argument("--tf32", default="on", choices=["on", "off"],
+                    help="also time the two-term TF32 tensor-core arm beside the exact one (with its rsl error)")
     ap.add_argument("--ensemble-sle-ctas", default="rows", choices=["sm", "rows"],
                     help="c4_ensemble: the fused sea-level loop's CTAs per instance (one per SM, or one per grid row)")
     ap.add_argument("--toroidal", default="on", choices=["on", "off", "only"],
@@ -59,6 +64,37 @@ def parse():
     ap.add_argument("--grad-fwd", default="on", choices=["on", "off", "only"],
                     help="also time the adjoint gradient against its forward (grad/fwd); 'only' prints that alone")
     return ap.parse_args()
+
+
+PRECISION = {"fp64": 0, "split_tc": 1, "exact_tc": 2}
+PRECISION_DTYPE = {"fp64": "f64",
+                   "split_tc": "tf32x3 3-D stress products, f64 elsewhere",
+                   "exact_tc": "int8-digit (5 x 8 bit, exact int32 accumulation) 3-D stress products, f64 elsewhere"}
+
+
+def host_cpu():
+    """The host's CPU model and logical cores (lscpu)."""
+    info = {"nproc": os.cpu_count()}
+    try:
+        out = subprocess.run(["lscpu"], capture_output=True, text=True, timeout=10).stdout
+        for line in out.splitlines():
+            k, _, v = line.partition(":")
+            if k.strip() in ("Model name", "Socket(s)", "Core(s) per socket", "Thread(s) per core"):
+                info[k.strip()] = v.strip()
+    except Exception:
+        pass
+    return info
+
+
+def workload_config(w, n_sub, world):
+    """The workload the step runs (identical in every arm, ours and the reference's)."""
+    nk = (w.lmax + 1) * (w.lmax + 2) // 2 - 1
+    ne = w.n_elem
+    return {"workload": w.name, "lmax": w.lmax, "grid": f"{w.nlat}x{w.nphi}", "radial_elements": w.n_elem,
+            "dt_yr": w.dt_yr, "n_sub": n_sub, "visc3d": w.visc3d, "sea_level": w.sle, "rotation": w.rotation,
+            "parallelism": f"replicas{world}",
+            "l2": ("state larger than L2 (%.0f MB streamed per sub-step)" if 6 * 4 * ne * nk * 8 > 126e6 else
+                   "state fits L2 (%.0f MB), not flushed") % (6 * 4 * ne * nk * 8 / 1e6)}
 
 
 def peaks():
@@ -145,7 +181,8 @@ def cpu_baseline(w, budget_s, threads):
             break
     dt = time.perf_counter() - t0
     return {"value": n / dt, "unit": "steps/s", "cores": threads, "kind": "port",
-            "sample": f"{n} consecutive steps of {w.name} after 1 warm-up step, {dt:.1f} s, OMP threads={threads}"}
+            "sample": f"{n} consecutive steps of {w.name} after 1 warm-up step, {dt:.1f} s, OMP threads={threads}",
+            "host": host_cpu()}
 
 
 def run_reference(args, w):
@@ -175,46 +212,64 @@ def run_reference(args, w):
     out = {"metric": METRIC, "value": v, "unit": "steps/s", "impl": "reference", "n_gpus": args.gpus,
            "steps": n, "warmup": args.warmup, "ms_per_step": 1e3 * dt / n, "higher_is_better": True,
            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-           "config": {"workload": w.name, "lmax": w.lmax, "grid": f"{w.nlat}x{w.nphi}", "radial_elements": w.n_elem,
-                      "dt_yr": w.dt_yr, "visc3d": w.visc3d, "sea_level": w.sle},
-           "cpu_baseline": {"value": v, "unit": "steps/s", "cores": threads, "kind": "port", "sample": sample},
+           "config": workload_config(w, o.info().n_sub_last, args.gpus),
+           "cpu_baseline": {"value": v, "unit": "steps/s", "cores": threads, "kind": "port", "sample": sample,
+                            "host": host_cpu()},
            "e2e": {"value": v, "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(out))
 
 
-def stage_work(w, info):
-    """Algorithmic work of one call of each fine-grained phase.
+def stage_work(w, info, precision):
+    """Algorithmic work of one call of each fine-grained phase, as
+    {phase: {"flop": F, "tensor_ops": T, "bytes": B}} (missing keys: not
+    applicable).
 
-    Tensor-core stages of the split path: the MMA flops the decomposition
-    needs (2 x rows x N x K per sub-GEMM, three split products), summed over
-    the stage's sub-GEMMs (parity / half-period halves, no padding). The gather
-    and scatter stream the Maxwell-element state and the FP32 operand rows.
-    Returned as {phase: (kind, amount)} with kind "flop" or "byte".
+    Tensor-core stages: F = 2 x rows x N x K summed over the stage's
+    sub-GEMMs (parity / half-period halves, no padding), one product per
+    multiply-add; T = the operations the tensor pipe executes for them (split
+    TF32: three products per multiply-add; exact int8: 15 digit-pair products);
+    B = the stage's input read once and its output written once (FP64
+    intermediates on the exact path, FP32 on the TF32 path). The gather and
+    scatter stream the Maxwell-element state and the operand rows.
     """
     L, nlat, nphi = w.lmax, w.nlat, w.nphi
     nh, half = (nlat + 1) // 2, nphi // 2
+    M = L + 1
     F = 3 * info.ne3d
     NC, NCOL = 2 * F, 6 * F
     kev, kod = 2 * (L // 2), 2 * ((L + 1) // 2)
-    legendre = 3 * 2.0 * NC * nh * info.nlm * 6  # sum over m of (K_E + K_O) = nlm, 6 products
-    inv = 3 * 2.0 * NCOL * (half - 1) * (kev + kod) * nlat
-    fwd = 3 * 2.0 * NCOL * (kev + kod) * half * nlat
+    legendre = 2.0 * NC * nh * info.nlm * 6  # sum over m of (K_E + K_O) = nlm, 6 products
+    inv = 2.0 * NCOL * (half - 1) * (kev + kod) * nlat
+    fwd = 2.0 * NCOL * (kev + kod) * half * nlat
+    products = {"exact_tc": 15, "split_tc": 3}.get(precision, 1)
+    eb = 4 if precision == "split_tc" else 8  # bytes of an intermediate value
     ne3d, nk = info.ne3d, info.nk
+    X = (nk + 1) * 4 * NC * eb
+    S = M * nlat * 6 * NC * eb
+    Gs = nlat * 2 * half * NCOL * eb
+    dy = (nk + 1) * 6 * NC * eb
+    rate = nlat * nphi * ne3d * eb
     state3 = 6 * 4 * ne3d * nk * 8  # memory of the 3-D elements, one buffer
     drift = 2 * 2 * (ne3d + 1) * nk * 8
-    gather = state3 + drift + (nk + 1) * 4 * NC * 4
-    scatter = 2 * state3 + (nk + 1) * 6 * NC * 4
-    return {"v3_synth": ("flop", legendre), "v3_analysis": ("flop", legendre), "v3_lon_inv": ("flop", inv),
-            "v3_lon_fwd": ("flop", fwd), "v3_gather": ("byte", gather), "v3_scatter": ("byte", scatter),
-            "drift": ("byte", algorithmic_bytes(info, "drift")),
-            "advance_1d": ("byte", algorithmic_bytes(info, "advance_1d"))}
+    out = {"v3_synth": {"flop": legendre, "tensor_ops": products * legendre, "bytes": X + S},
+           "v3_lon_inv": {"flop": inv, "tensor_ops": products * inv, "bytes": S + Gs + rate},
+           "v3_lon_fwd": {"flop": fwd, "tensor_ops": products * fwd, "bytes": Gs + S},
+           "v3_analysis": {"flop": legendre, "tensor_ops": products * legendre, "bytes": S + dy},
+           "v3_gather": {"bytes": state3 + drift + X},
+           "v3_scatter": {"bytes": 2 * state3 + dy},
+           "drift": {"bytes": algorithmic_bytes(info, "drift")},
+           "advance_1d": {"bytes": algorithmic_bytes(info, "advance_1d")}}
+    if precision == "fp64":  # one kernel runs the whole longitude pass
+        out["v3_lon_inv"] = {"flop": inv + fwd, "bytes": 2 * S + rate}
+    return out
 
 
 # DRAM bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum) of the
-# split-path stages, from one `ncu --set full` capture of the lmax-128 3-D
-# workload (second sub-step of `bench.py --steps 2 --warmup 1 --plain off --grad-fwd off`)
-NCU_TRAFFIC = {("c3_3d_l128", "v3_synth"): 150.75e6, ("c3_3d_l128", "v3_lon_inv"): 227.35e6,
-               ("c3_3d_l128", "v3_lon_fwd"): 223.56e6, ("c3_3d_l128", "v3_analysis"): 209.04e6}
+# tensor-core stages on the lmax-128 3-D workload, from one ncu capture per
+# stage (profiles/ names the command)
+NCU_TRAFFIC = {("c3_3d_l128", "split_tc", "v3_synth"): 150.75e6, ("c3_3d_l128", "split_tc", "v3_lon_inv"): 227.35e6,
+               ("c3_3d_l128", "split_tc", "v3_lon_fwd"): 223.56e6,
+               ("c3_3d_l128", "split_tc", "v3_analysis"): 209.04e6}
 
 
 def max_over_ranks(ms, dist, device):
@@ -348,43 +403,57 @@ def phases_of(arm):
             for i, n in enumerate(PHASE_NAMES)}
 
 
-def roofline(w, arm, pk, pk_kind, split):
+def roofline(w, arm, pk, pk_kind, precision):
     """Roofline of the dominant kernel (the fine-grained phase with the most
-    time; each such phase is one kernel launch)."""
+    time; each 3-D stage phase is one kernel launch). For a tensor-core stage
+    both bounds are evaluated, the tensor pipe (operations it executes against
+    the measured dense peak of its input type: int8 = 2 x bf16, tf32 = bf16 / 2,
+    both from the sustained bf16 figure) and HBM (algorithmic bytes against
+    the measured copy bandwidth); the binding one (larger fraction) is
+    reported, the other beside it."""
     info = arm["info"]
     ph = phases_of(arm)
-    work = stage_work(w, info)
+    work = stage_work(w, info, precision)
     # one-kernel phases first (the 3-D stages); the drift and advance phases are
     # a few kernels each and stand in only for workloads without 3-D elements
     cands = [n for n in work if n.startswith("v3_") and ph.get(n, {}).get("calls")]
     cands = cands or [n for n in work if ph.get(n, {}).get("calls")]
     dom = max(cands, key=lambda n: ph[n]["ms_total"])
-    kind, amount = work[dom]
+    wk = work[dom]
     t = ph[dom]["ms_per_call"] * 1e-3
-    if kind == "byte":
-        ach = amount / t / 1e9
-        return {"bound": "hbm", "kernel": dom, "achieved": ach, "peak": pk["hbm_gbs"], "unit": "GB/s",
-                "frac": ach / pk["hbm_gbs"], "peak_kind": pk_kind + " copy bandwidth", "traffic": None,
-                "algorithmic_bytes_per_launch": amount}
-    ach = amount / t / 1e12
-    if split:
-        peak = 0.5 * pk["bf16_tflops_sustained"]
-        traffic = NCU_TRAFFIC.get((w.name, dom))
-        return {"bound": "tensor", "kernel": dom, "achieved": ach, "peak": peak, "unit": "TFLOP/s",
-                "frac": ach / peak, "peak_kind": pk_kind + " sustained dense bf16 x 0.5 (tf32 rate)",
-                "traffic": traffic, "traffic_source": "ncu capture, bytes per launch" if traffic else None,
-                "algorithmic_flops_per_launch": amount}
-    if dom == "v3_lon_inv":  # the FP64 path's longitude pass is one kernel: synthesis and analysis
-        amount += work["v3_lon_fwd"][1]
-    fp64 = amount / 3.0 / t / 1e12  # FP64 path: one product per multiply-add instead of three
-    return {"bound": "fp64", "kernel": dom, "achieved": fp64, "peak": FP64_NOMINAL_TFLOPS, "unit": "TFLOP/s",
-            "frac": fp64 / FP64_NOMINAL_TFLOPS, "peak_kind": "nominal FP64 (no measured FP64 peak)",
-            "traffic": None, "algorithmic_flops_per_launch": amount / 3.0}
+    hbm = {"bound": "hbm", "kernel": dom, "achieved": wk["bytes"] / t / 1e9, "peak": pk["hbm_gbs"], "unit": "GB/s",
+           "peak_kind": pk_kind + " copy bandwidth", "algorithmic_bytes_per_launch": wk["bytes"]}
+    hbm["frac"] = hbm["achieved"] / hbm["peak"]
+    traffic = NCU_TRAFFIC.get((w.name, precision, dom))
+    if "tensor_ops" in wk and precision in ("exact_tc", "split_tc"):
+        if precision == "exact_tc":
+            peak, kind = 2.0 * pk["bf16_tflops_sustained"], " sustained dense bf16 x 2 (int8 rate)"
+        else:
+            peak, kind = 0.5 * pk["bf16_tflops_sustained"], " sustained dense bf16 x 0.5 (tf32 rate)"
+        ten = {"bound": "tensor", "kernel": dom, "achieved": wk["tensor_ops"] / t / 1e12, "peak": peak,
+               "unit": "TOP/s" if precision == "exact_tc" else "TFLOP/s", "peak_kind": pk_kind + kind,
+               "tensor_ops_per_launch": wk["tensor_ops"], "useful_flops_per_launch": wk["flop"]}
+        ten["frac"] = ten["achieved"] / ten["peak"]
+        main, other = (ten, hbm) if ten["frac"] >= hbm["frac"] else (hbm, ten)
+        main = dict(main)
+        main["traffic"] = traffic
+        main["traffic_source"] = "ncu capture, DRAM bytes per launch" if traffic else None
+        main["other_bound"] = {k: other[k] for k in ("bound", "achieved", "peak", "unit", "frac")}
+        return main
+    if "flop" in wk:  # the FP64 path's CUDA-core stages
+        fp64 = wk["flop"] / t / 1e12
+        out = {"bound": "fp64", "kernel": dom, "achieved": fp64, "peak": FP64_NOMINAL_TFLOPS, "unit": "TFLOP/s",
+               "frac": fp64 / FP64_NOMINAL_TFLOPS, "peak_kind": "nominal FP64 (no measured FP64 peak)",
+               "traffic": traffic, "algorithmic_flops_per_launch": wk["flop"]}
+        out["other_bound"] = {k: hbm[k] for k in ("bound", "achieved", "peak", "unit", "frac")}
+        return out
+    hbm["traffic"] = traffic
+    return hbm
 
 
 def run_ensemble(args):
     """The batched ensemble (32 instances of mixed lmax, earth and viscosity,
-    half with 3-D viscosity on the split tensor-core path), advanced together
+    half with 3-D viscosity on the tensor-core path of --precision), advanced together
     through vg_update_batch, against the same instances run one after the other
     on the plain FP64 path ("32 sequential plain runs") and, to separate the
     concurrency from the precision, sequentially on the batched precision.
@@ -401,7 +470,7 @@ def run_ensemble(args):
 
     def make(mb, split):
         p = mb.params(vlib.default_params)
-        p.visc3d_precision = 1 if (split and mb.visc3d) else 0
+        p.visc3d_precision = PRECISION[args.precision] if (split and mb.visc3d) else 0
         if args.ensemble_sle_ctas == "rows":  # the fused sea-level loop on one CTA per grid row at most
             p.sle_ctas = mb.nlat
         m = vlib.Model(p)
@@ -475,7 +544,7 @@ def run_ensemble(args):
         "higher_is_better": True,
         "scaling": "weak",
         "vs_baseline": None,
-        "dtype": "tf32x3 3-D stress products of the 3-D instances, f64 elsewhere",
+        "dtype": PRECISION_DTYPE[args.precision] + " (3-D instances)",
         "data": "synthetic",
         "config": {"workload": "c4_ensemble", "instances": n, "sle_ctas": args.ensemble_sle_ctas,
                    "lmax": [mb.lmax for mb in members],
@@ -489,7 +558,7 @@ def run_ensemble(args):
         "speedup_vs_sequential_plain": seq[False][0] / ms_batch,
         "speedup_from_concurrency": seq[True][0] / ms_batch,
         "batched_equals_sequential": bool(same),
-        "split_rsl_error_vs_fp64_3d_instances": worst,
+        "rsl_error_vs_fp64_3d_instances": worst,
         "e2e": {"value": n / (ms_e2e / 1e3), "unit": "instance-steps/s", "h2d_bytes_per_step": ng_tot * 8,
                 "d2h_bytes_per_step": ng_tot * 8},
         "gpu_launches": int(launches),
@@ -502,6 +571,8 @@ def run_ensemble(args):
 
 def main():
     args = parse()
+    if args.steps is None:
+        args.steps = 20 if args.workload == "c4_ensemble" else 300
     if args.workload == "c4_ensemble":
         import torch
 
@@ -537,9 +608,12 @@ def main():
     for s in range(total + n_prof + 1):
         ice_dev[s] = torch.from_numpy(w.ice_at(s + 1))
     tor_only = w.visc3d and args.toroidal == "only"
-    split = w.visc3d and args.precision == "split_tc" and not tor_only
-    main_arm = run_arm(w, 1 if split else 0, args, ice_dev, local, dist, True, tor_only)
-    plain = run_arm(w, 0, args, ice_dev, local, dist, False) if split and args.plain == "on" else None
+    prec = args.precision if (w.visc3d and not tor_only) else "fp64"
+    tensor = prec in ("exact_tc", "split_tc")
+    main_arm = run_arm(w, PRECISION[prec], args, ice_dev, local, dist, True, tor_only)
+    plain = run_arm(w, 0, args, ice_dev, local, dist, False) if tensor and args.plain == "on" else None
+    tf32 = (run_arm(w, PRECISION["split_tc"], args, ice_dev, local, dist, False)
+            if prec == "exact_tc" and args.tf32 == "on" else None)
     tor = run_arm(w, 0, args, ice_dev, local, dist, False, True) if w.visc3d and args.toroidal == "on" else None
     if rank != 0:
         if dist:
@@ -548,6 +622,14 @@ def main():
     pk, pk_kind = peaks()
     info = main_arm["info"]
     ms = main_arm["ms"]
+
+    def error_vs(arm, ref):
+        r0, r1 = ref["rsl"], arm["rsl"]
+        z0, z1 = ref["zbed"], arm["zbed"]
+        return {"after_steps": total, "rsl": float(np.abs(r1 - r0).max() / np.abs(r0).max()),
+                "z_bed": float(np.abs(z1 - z0).max() / np.abs(z0).max()),
+                "norm": "max abs diff / max abs (FP64 GPU path, same steps)"}
+
     out = {
         "metric": METRIC,
         "value": replica_throughput(world, args.steps, ms),
@@ -559,34 +641,36 @@ def main():
         "higher_is_better": True,
         "scaling": "weak",
         "vs_baseline": None,
-        "dtype": "tf32x3 3-D stress products, f64 elsewhere" if split else "f64",
+        "dtype": PRECISION_DTYPE[prec],
         "data": "synthetic",
-        "config": {"workload": w.name, "lmax": w.lmax, "grid": f"{w.nlat}x{w.nphi}", "radial_elements": w.n_elem,
-                   "dt_yr": w.dt_yr, "n_sub": info.n_sub_last, "visc3d": w.visc3d, "sea_level": w.sle,
-                   "visc3d_precision": "split_tc" if split else "fp64", "toroidal": bool(tor_only),
-                   "parallelism": f"replicas{world}",
-                   "l2": "state larger than L2 (%.0f MB streamed per sub-step)" % (6 * 4 * info.ne * info.nk * 8 / 1e6)},
+        "config": workload_config(w, info.n_sub_last, world),
+        "arm": {"visc3d_precision": prec, "toroidal": bool(tor_only)},
         "e2e": {"value": 1e3 / main_arm["e2e_ms"], "unit": "steps/s", "h2d_bytes_per_step": ng * 8,
                 "d2h_bytes_per_step": ng * 8},
         "gpu_launches": int(main_arm["launches"]),
-        "roofline": roofline(w, main_arm, pk, pk_kind, split),
+        "roofline": roofline(w, main_arm, pk, pk_kind, prec),
         "phases": phases_of(main_arm),
         "clocks": main_arm["clocks"],
     }
     if plain is not None:
-        r0, r1 = plain["rsl"], main_arm["rsl"]
-        z0, z1 = plain["zbed"], main_arm["zbed"]
         out["plain_fp64"] = {
             "value": replica_throughput(world, args.steps, plain["ms"]), "unit": "steps/s",
-            "ms_per_step": plain["ms"] / args.steps, "speedup_split_over_plain": plain["ms"] / ms,
+            "ms_per_step": plain["ms"] / args.steps, "speedup_over_plain": plain["ms"] / ms, "target": 3.0,
             "gpu_launches": int(plain["launches"]), "phases": phases_of(plain), "clocks": plain["clocks"],
-            "roofline": roofline(w, plain, pk, pk_kind, False)}
-        out["split_error_vs_fp64"] = {
-            "after_steps": total, "rsl": float(np.abs(r1 - r0).max() / np.abs(r0).max()),
-            "z_bed": float(np.abs(z1 - z0).max() / np.abs(z0).max()), "norm": "max abs diff / max abs (FP64 GPU)",
-            "rsl_target": 1e-8}
+            "roofline": roofline(w, plain, pk, pk_kind, "fp64")}
+        err = error_vs(main_arm, plain)
+        err["rsl_target"] = 1e-8
+        err["rsl_target_met"] = bool(err["rsl"] <= 1e-8)
+        out["error_vs_fp64"] = err
+        if tf32 is not None:
+            e32 = error_vs(tf32, plain)
+            out["split_tf32"] = {
+                "value": replica_throughput(world, args.steps, tf32["ms"]), "unit": "steps/s",
+                "ms_per_step": tf32["ms"] / args.steps, "speedup_over_plain": plain["ms"] / tf32["ms"],
+                "error_vs_fp64": e32, "rsl_target_met": bool(e32["rsl"] <= 1e-8),
+                "phases": phases_of(tf32), "clocks": tf32["clocks"]}
     if tor is not None:
-        ref = plain if plain is not None else (main_arm if not split else None)
+        ref = plain if plain is not None else (main_arm if not tensor else None)
         out["toroidal_fp64"] = {
             "value": replica_throughput(world, args.steps, tor["ms"]), "unit": "steps/s",
             "ms_per_step": tor["ms"] / args.steps, "gpu_launches": int(tor["launches"]), "n_sub": tor["info"].n_sub_last,

@@ -9,7 +9,7 @@ import ctypes as C
 
 VG_MAX_LAYER = 16
 VG_RHEOL_ELASTIC, VG_RHEOL_MAXWELL, VG_RHEOL_FLUID = 0, 1, 2
-VG_VISC3D_FP64, VG_VISC3D_SPLIT_TC = 0, 1
+VG_VISC3D_FP64, VG_VISC3D_SPLIT_TC, VG_VISC3D_EXACT_TC = 0, 1, 2
 
 _D16 = C.c_double * VG_MAX_LAYER
 _I16 = C.c_int * VG_MAX_LAYER

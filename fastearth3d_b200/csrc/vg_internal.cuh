@@ -307,6 +307,10 @@ void rotation_advance(vg_handle* h, const double* d_sigma, double dt);
 void visc3d_tc_enable(vg_handle* h);
 void visc3d_tc_buffers(vg_handle* h, float** X, float** dy);
 void visc3d_tc_run(vg_handle* h, double dt, bool trap = false);
+// 3-D exact int8 tensor-core stages (vg_oz.cu)
+void visc3d_oz_enable(vg_handle* h);
+unsigned long long* visc3d_oz_gather_max(vg_handle* h);
+void visc3d_oz_run(vg_handle* h, double dt, bool trap = false);
 // toroidal degree of freedom (vg_toroidal.cu; operator assembly in vg_setup.cu)
 void toroidal_tridiag(const std::vector<double>& r, const std::vector<double>& mu, int j, std::vector<double>& diag,
                       std::vector<double>& off, std::vector<char>& dead);

@@ -770,6 +770,9 @@ void setup_handle(vg_handle* h) {
   if (p.scheme != VG_SCHEME_FE && p.scheme != VG_SCHEME_TRAP)
     throw Error("vg_create: the memory scheme must be \"fe\" (VG_SCHEME_FE) or \"trap\" (VG_SCHEME_TRAP)");
   if (p.lmax < 2) throw Error("vg_create: lmax must be >= 2");
+  if (p.visc3d_precision != VG_VISC3D_FP64 && p.visc3d_precision != VG_VISC3D_SPLIT_TC &&
+      p.visc3d_precision != VG_VISC3D_EXACT_TC)
+    throw Error("vg_create: visc3d_precision must be VG_VISC3D_FP64, VG_VISC3D_SPLIT_TC or VG_VISC3D_EXACT_TC");
   cudaStream_t s = h->stream;
   build_grid(h->grid, p.lmax, p.nlat, p.nphi, s);
   build_mesh(h);

@@ -38,6 +38,7 @@
 
 #include "vg_device.cuh"
 #include "vg_internal.cuh"
+#include "vg_tcgen05.cuh"
 
 namespace vg {
 namespace tc {
@@ -83,14 +84,8 @@ struct Args {
 };
 
 // ------------------------------------------------------------------ PTX helpers
-
-__device__ __forceinline__ uint32_t saddr(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
-
-__device__ __forceinline__ unsigned long long gtimer() {
-  unsigned long long t;
-  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-  return t;
-}
+// (shared ones in vg_tcgen05.cuh)
+using namespace vg::ptx;
 
 __device__ __forceinline__ uint32_t to_tf32(float x) {
   uint32_t r;
@@ -98,71 +93,10 @@ __device__ __forceinline__ uint32_t to_tf32(float x) {
   return r;
 }
 
-__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
-  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(saddr(bar)), "r"(count) : "memory");
-}
-
-__device__ __forceinline__ bool mbar_try(uint64_t* bar, uint32_t parity) {
-  uint32_t ok;
-  asm volatile(
-      "{\n\t.reg .pred p;\n\t"
-      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-      "selp.b32 %0, 1, 0, p;\n\t}\n"
-      : "=r"(ok)
-      : "r"(saddr(bar)), "r"(parity)
-      : "memory");
-  return ok != 0;
-}
-
-// bounded wait: false after WAIT_NS of global time
-__device__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
-  if (mbar_try(bar, parity)) return true;
-  const unsigned long long t0 = gtimer();
-  while (true) {
-    if (mbar_try(bar, parity)) return true;
-    if (gtimer() - t0 > WAIT_NS) return false;
-  }
-}
-
-// bounded wait that also gives up once `abort_flag` is raised (the other side
-// of a producer / consumer handoff stopped)
+// bounded waits of this file: the fixed 2 s bound
+__device__ bool mbar_wait(uint64_t* bar, uint32_t parity) { return mbar_wait_ns(bar, parity, WAIT_NS); }
 __device__ bool mbar_wait_or_abort(uint64_t* bar, uint32_t parity, volatile int* abort_flag) {
-  if (mbar_try(bar, parity)) return true;
-  const unsigned long long t0 = gtimer();
-  while (true) {
-    if (mbar_try(bar, parity)) return true;
-    if (*abort_flag || gtimer() - t0 > WAIT_NS) return false;
-  }
-}
-
-__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
-  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(saddr(bar)) : "memory");
-}
-
-__device__ __forceinline__ void tmem_alloc(uint32_t* slot, uint32_t ncols) {
-  asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(saddr(slot)), "r"(ncols)
-               : "memory");
-  asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
-}
-
-__device__ __forceinline__ void tmem_dealloc(uint32_t taddr, uint32_t ncols) {
-  asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(taddr), "r"(ncols) : "memory");
-}
-
-__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
-__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
-__device__ __forceinline__ void fence_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
-__device__ __forceinline__ void fence_mbar_init() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
-
-// shared-memory matrix descriptor, canonical K-major layout without swizzle:
-// 8-row core matrices of 16-byte rows, SBO between 8-row groups, LBO between
-// the two 16-byte K halves of one k-step; version 1 (sm_100)
-__device__ __forceinline__ uint64_t sdesc(uint32_t addr, uint32_t lbo, uint32_t sbo) {
-  uint64_t d = (uint64_t)((addr >> 4) & 0x3FFFu);
-  d |= (uint64_t)((lbo >> 4) & 0x3FFFu) << 16;
-  d |= (uint64_t)((sbo >> 4) & 0x3FFFu) << 32;
-  d |= (uint64_t)1 << 46;
-  return d;
+  return mbar_wait_or_abort_ns(bar, parity, abort_flag, WAIT_NS);
 }
 
 // instruction descriptor: F32 accumulate, A and B TF32, both K-major
@@ -177,23 +111,6 @@ __device__ __forceinline__ void mma_tf32(uint32_t tmem_d, uint64_t da, uint64_t 
       "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(tmem_d),
       "l"(da), "l"(db), "r"(idesc), "r"(acc), "r"(0), "r"(0), "r"(0), "r"(0)
       : "memory");
-}
-
-// TMA bulk copy (no tensor map, no multicast): global -> this CTA's shared
-// memory, completing `bytes` on the mbarrier's transaction count
-__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
-  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(saddr(bar)), "r"(bytes) : "memory");
-}
-__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
-  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
-                   saddr(dst)),
-               "l"(src), "r"(bytes), "r"(saddr(bar))
-               : "memory");
-}
-
-__device__ __forceinline__ void mma_commit(uint64_t* bar) {
-  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(saddr(bar))
-               : "memory");
 }
 
 // 32 lanes x 16 consecutive 32-bit columns

@@ -91,6 +91,9 @@ struct V3Args {
   const double *Jr, *xUn, *xVn, *dUn, *dVn, *mu;
   int ne, nr, nk, ne3d, nf, ncf;  // ncf = 2 nf
   double* mnext = nullptr;        // per-slot norms of the next buffer (the scatter folds its maxima in)
+  // exact tensor-core path: the largest |X| per (channel, column) over all
+  // slots, as double bits (the synthesis operand rows' scale groups)
+  unsigned long long* gmax = nullptr;
 };
 
 // one thread per (slot k, 3-D element): strain of both histories, 24 values,
@@ -146,6 +149,14 @@ __global__ void __launch_bounds__(256) k_v3_gather(V3Args A, T* __restrict__ X) 
   }
   __syncthreads();
   const int nkb = min(V3_TK, A.nk - k0), w = 6 * min(V3_TE, A.ne3d - e0);
+  if (A.gmax) {  // per (channel, column) of this block: the largest |value| over its slots
+    for (int t = threadIdx.y * V3_TK + threadIdx.x; t < NC * w; t += V3_TK * V3_TE) {
+      const int lam = t / w, cc = t % w;
+      double mx = 0.0;
+      for (int kl = 0; kl < nkb; ++kl) mx = fmax(mx, fabs((double)tile[((size_t)lam * V3_TC + cc) * V3_TP + kl]));
+      atomic_max_bits(A.gmax + (size_t)lam * A.ncf + 6 * e0 + cc, mx);
+    }
+  }
   for (int t = threadIdx.y * V3_TK + threadIdx.x; t < nkb * NC * w; t += V3_TK * V3_TE) {
     const int kl = t / (NC * w), rem = t % (NC * w), lam = rem / w, c = rem % w;
     X[((size_t)(k0 + kl) * NC + lam) * A.ncf + 6 * e0 + c] = tile[((size_t)lam * V3_TC + c) * V3_TP + kl];
@@ -749,6 +760,10 @@ void visc3d_enable(vg_handle* h, const double* pert) {
     visc3d_tc_enable(h);
     return;
   }
+  if (h->p.visc3d_precision == VG_VISC3D_EXACT_TC) {
+    visc3d_oz_enable(h);
+    return;
+  }
   // work buffers and longitude tables of the FP64 path
   const int nf = 3 * h->ne3d, ncf = 2 * nf, nch = h->tor_on ? 6 : 4, np = h->tor_on ? 10 : 6;
   h->d_X.alloc((size_t)(h->nk + 1) * nch * ncf);
@@ -805,6 +820,22 @@ void visc3d_advance(vg_handle* h, const double* d_sigma, double dt, const double
     visc3d_tc_run(h, dt, trap);
     PhaseScope pc(h, VG_PH_V3_SCATTER);
     k_v3_scatter<float><<<gg, dim3(32, 8), 0, s>>>(A, dy32, h->d_n6.p);
+    ++h->n_launch;
+    VG_CUDA(cudaGetLastError());
+    return;
+  }
+  if (h->p.visc3d_precision == VG_VISC3D_EXACT_TC) {
+    {
+      PhaseScope pg(h, VG_PH_V3_GATHER);
+      A.gmax = visc3d_oz_gather_max(h);  // zeroes every scale group of the advance
+      k_v3_gather<double, 4><<<gg, dim3(32, 8), v3_gather_smem<double>(), s>>>(A, h->d_X.p);
+      ++h->n_launch;
+      VG_CUDA(cudaGetLastError());
+      A.gmax = nullptr;
+    }
+    visc3d_oz_run(h, dt, trap);
+    PhaseScope pc(h, VG_PH_V3_SCATTER);
+    k_v3_scatter<double><<<gg, dim3(32, 8), 0, s>>>(A, h->d_dy.p, h->d_n6.p);
     ++h->n_launch;
     VG_CUDA(cudaGetLastError());
     return;

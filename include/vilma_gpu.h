@@ -39,7 +39,7 @@ extern "C" {
 
 enum { VG_RHEOL_ELASTIC = 0, VG_RHEOL_MAXWELL = 1, VG_RHEOL_FLUID = 2 };
 enum { VG_SCHEME_FE = 0, VG_SCHEME_TRAP = 2 };  /* "fe" | "trap" (SCHEME_* of src/vilma_viscoelastic.f90:60-64) */
-enum { VG_VISC3D_FP64 = 0, VG_VISC3D_SPLIT_TC = 1 };
+enum { VG_VISC3D_FP64 = 0, VG_VISC3D_SPLIT_TC = 1, VG_VISC3D_EXACT_TC = 2 };
 
 /* The &vilma namelist record restricted to what the time step reads
  * (src/vilma_params.f90:26-205). Defaults: vg_params_default. */
@@ -72,9 +72,13 @@ typedef struct vg_params {
    * src/vilma_coupling.f90:399-424 */
   int rotation;
   /* arithmetic of the 3-D stress products (no reference counterpart):
-   * VG_VISC3D_FP64 (default) or VG_VISC3D_SPLIT_TC, the Legendre and longitude
-   * contractions on the tensor cores with two-term TF32 operands and FP32
-   * accumulation (rsl within ~2e-6 of the FP64 path on the lmax-128 workload) */
+   * VG_VISC3D_FP64 (default) on the CUDA cores; VG_VISC3D_EXACT_TC, the
+   * Legendre and longitude contractions on the tensor cores as 8-bit digit
+   * slices of 40-bit fixed-point operands with exact int32 accumulation
+   * (~38 significant bits per product, FP64 between the stages);
+   * VG_VISC3D_SPLIT_TC, the same contractions with two-term TF32 operands and
+   * FP32 accumulation (rsl within ~2e-6 of the FP64 path on the lmax-128
+   * workload) */
   int visc3d_precision;
   /* trapezoidal scheme (scheme = VG_SCHEME_TRAP): the step-doubling controller
    * (src/vilma_timestep.f90:40-53, 229-307; rtol, atol, safety, grow_max,

@@ -26,8 +26,8 @@ and writes the few numbers the tests use into tests/golden/*.json:
   second row of the 7 columns: profile coordinate, u, th- and ph-horizontal,
   potential increment -N g, sea surface, sea level).
 
-Run in a container where the reference is mounted:
-    python tests/golden/make_golden.py /root/reference
+Run where the reference tree is available, passing its root:
+    python tests/golden/make_golden.py <path to the reference tree>
 """
 import json
 import os
@@ -97,7 +97,9 @@ def martinec(ref):
 
 
 if __name__ == "__main__":
-    ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    if len(sys.argv) != 2 or not os.path.isdir(sys.argv[1]):
+        sys.exit("usage: make_golden.py <path to the reference tree>")
+    ref = sys.argv[1]
     here = os.path.dirname(os.path.abspath(__file__))
     json.dump(love(ref), open(os.path.join(here, "love_M3L70V01.json"), "w"), indent=1)
     json.dump(disc(ref), open(os.path.join(here, "disc_spada2011.json"), "w"))
