@@ -31,14 +31,12 @@
 // enable time with one exponent per column, laid out exactly as the shared-
 // memory image of a K chunk and copied by one TMA bulk copy per chunk.
 //
-// Kernel shape: one CTA per SM (tensor memory: 5 levels x 2 sub-GEMMs x 48
-// columns), 16 loader warps that fetch A in FP64 one chunk ahead, slice it into
-// the five digit planes in shared memory (canonical K-major no-swizzle layout)
-// and later run the epilogue, and one MMA warp whose lane 0 issues the
-// tcgen05.mma and commits each stage to its mbarrier. Handoff waits between
-// loaders and the MMA warp are bounded by the handle's wait limit; waits for the
-// hardware's own copies and MMAs by a fixed 2 s; a wait that runs out raises a
-// status bit instead of hanging.
+// Kernel shape: persistent, one CTA per SM (tensor memory: 5 levels x 2
+// sub-GEMMs x 48 columns) looping over the stage's tiles, warp-specialised
+// (producer of TMA bulk copies, MMA issuer, converters that slice the staged
+// FP64 rows into the five digit planes in the canonical K-major no-swizzle
+// layout, epilogue warps that overlap the next tile's staging); see the
+// persistent kernel below.
 #include <algorithm>
 #include <cmath>
 #include <cstdint>
@@ -55,24 +53,16 @@ using namespace vg::ptx;
 constexpr int TM = 128;        // tile rows (MMA M)
 constexpr int TN = 48;         // max columns of one sub-GEMM (MMA N)
 constexpr int KC = 32;         // K per pipeline chunk = one i8 k-step
-constexpr int NSTAGE = 4;      // shared-memory ring depth
 constexpr int NLEV = 5;        // digit levels kept (15 digit-pair products)
 constexpr int NDIG = 5;        // 8-bit digits per operand value
-constexpr int NLOAD = 512;     // loader / epilogue threads
-constexpr int MMA_WARP = NLOAD / 32;
-constexpr int NTHR_ALL = NLOAD + 32;
-static_assert(TM * KC / NLOAD == 8, "a loader thread slices eight K of one row per chunk");
 constexpr int A_PLANE = TM * KC;              // bytes of one digit plane of the A chunk
 constexpr int A_BYTES = NDIG * A_PLANE;
 constexpr int B_BYTES_MAX = NDIG * TN * KC;
-constexpr int STAGE_BYTES = A_BYTES + B_BYTES_MAX;
 constexpr int TMEM_COLS = 512;                // 2 * NLEV * TN = 480 used
 constexpr int MAX_L = 511;
 constexpr int FIX_BITS = 39;                  // |xi| < 2^39: five signed 8-bit digits
 constexpr unsigned long long HW_WAIT_NS = 2000000000ull;  // bound on waits for copies and MMAs
-constexpr size_t SMEM_BYTES = 1024 + (size_t)NSTAGE * STAGE_BYTES + 256 + 2 * 4 * TM * 8 + (MAX_L + 1) * 4;
-static_assert(SMEM_BYTES > 114 * 1024, "one CTA per SM: the tensor-memory plan takes 480 of its 512 columns");
-static_assert(STAGE_BYTES % 128 == 0, "stage buffers stay 128-byte aligned");
+static_assert(A_BYTES % 128 == 0 && B_BYTES_MAX % 128 == 0, "ring stages stay 128-byte aligned");
 
 enum { ST_SYNTH = 0, ST_INV = 1, ST_FWD = 2, ST_ANA = 3 };
 
@@ -196,500 +186,605 @@ struct Cta {
   ImgInfo sub[2];
 };
 
+// ------------------------------------------------------------------ persistent kernel
+//
+// One CTA per SM loops over the stage's tiles (static stride). Warp roles:
+//   warp 0       producer: lanes 0 .. 31 issue the TMA bulk copies of the raw
+//                FP64 A rows of each K chunk into the raw ring (one copy per K
+//                value: a run of the tile's rows, contiguous in every layout)
+//                and lane 0 the B digit image of the chunk into the B ring
+//   warp 1       MMA issuer (lane 0): 15 digit-pair MMAs per chunk into the
+//                five level accumulators, commits that free the chunk's A
+//                and B stages, and one that hands the tile's accumulators to
+//                the epilogue
+//   warps 2-9    converters: raw FP64 -> five 8-bit digit planes (16 K of
+//                one row per thread), zero outside the valid rows and K, the
+//                CUDA-core side sums of the longitude stages
+//   warps 10-17  epilogue: two per tensor-memory lane quarter, one row per
+//                thread, levels combined in FP64, scaled, the stage's outputs
+//                and the next stage's scale groups
+// The epilogue of tile t runs while the producer and converters already
+// stage tile t + 1; its accumulators are released to the MMA warp by an
+// mbarrier. Handoff waits are bounded by the handle's wait limit, waits for
+// copies and MMAs by a fixed bound; after an abort every copy and MMA in
+// flight is waited for before the tensor memory is freed.
+namespace p {
+constexpr int NCONV = 256, NEPI = 256;
+constexpr int W_PROD = 0, W_MMA = 1, W_CONV = 2, W_EPI = 10, NWARP = 18;
+constexpr int NTHR = NWARP * 32;
 template <int STAGE>
-__device__ __forceinline__ Cta cta_info(const Args& A) {
+struct Ring {
+  static constexpr int NRAW = STAGE == ST_ANA ? 2 : 3;  // raw FP64 chunks in flight
+  static constexpr int RAW_BYTES = (STAGE == ST_ANA ? 2 : 1) * KC * TM * 8;
+  static constexpr int NDST = STAGE == ST_ANA ? 2 : 3;  // A digit stages
+  static constexpr int NB = STAGE == ST_ANA ? 4 : 6;    // B digit stages
+  static constexpr size_t RAW_OFF = 0;
+  static constexpr size_t A_OFF = RAW_OFF + (size_t)NRAW * RAW_BYTES;
+  static constexpr size_t B_OFF = A_OFF + (size_t)NDST * A_BYTES;
+  static constexpr size_t SUM_OFF = B_OFF + (size_t)NB * B_BYTES_MAX;  // [2 tiles][2 subs][2 halves][TM]
+  static constexpr size_t BAR_OFF = SUM_OFF + 2 * 2 * 2 * TM * 8;
+  static constexpr int NBAR = 2 * NRAW + 2 * NDST + 2 * NB + 2 + 4;
+  static constexpr size_t BYTES = BAR_OFF + (size_t)NBAR * 8 + 16;
+  static constexpr size_t SMEM = 1024 + BYTES;
+};
+static_assert(Ring<ST_SYNTH>::SMEM <= 227 * 1024, "synthesis ring");
+static_assert(Ring<ST_ANA>::SMEM <= 227 * 1024, "analysis ring");
+static_assert(Ring<ST_SYNTH>::SMEM > 114 * 1024 && Ring<ST_ANA>::SMEM > 114 * 1024,
+              "one CTA per SM: the tensor-memory plan takes 480 of its 512 columns");
+}  // namespace p
+
+template <int STAGE>
+__device__ __forceinline__ int tile_count(const Args& A) {
+  if (STAGE == ST_SYNTH) return ((A.NC + TM - 1) / TM) * A.nts * (A.L + 1) * 6;
+  if (STAGE == ST_ANA) return ((A.NC + TM - 1) / TM) * A.nta * (A.L + 1) * 6;
+  if (STAGE == ST_INV) return ((A.NCOL + TM - 1) / TM) * A.nti * A.nlat;
+  return ((A.NCOL + TM - 1) / TM) * A.ntf * A.nlat;
+}
+
+// tile t -> (row tile, N tile, batch): the row tile fastest, so the CTAs that
+// share a batch's B images and A rows run close together
+template <int STAGE>
+__device__ __forceinline__ Cta tile_info(const Args& A, int t) {
   Cta c;
-  c.nt = blockIdx.y;
-  c.row0 = blockIdx.x * TM;
+  const int rt_n = (STAGE == ST_SYNTH || STAGE == ST_ANA) ? (A.NC + TM - 1) / TM : (A.NCOL + TM - 1) / TM;
+  const int nt_count = STAGE == ST_SYNTH ? A.nts : (STAGE == ST_ANA ? A.nta : (STAGE == ST_INV ? A.nti : A.ntf));
+  const int rt = t % rt_n, rest = t / rt_n;
+  c.nt = rest % nt_count;
+  const int bz = rest / nt_count;
+  c.row0 = rt * TM;
   if (STAGE == ST_SYNTH || STAGE == ST_ANA) {
-    c.batch_m = blockIdx.z / 6;
-    c.p = blockIdx.z % 6;
+    c.batch_m = bz / 6;
+    c.p = bz % 6;
     c.j = 0;
     c.rows = min(TM, A.NC - c.row0);
-    const int nt_count = STAGE == ST_SYNTH ? A.nts : A.nta;
     const int base = ((c.batch_m * 4 + table_of(c.p)) * 2) * nt_count;
     c.sub[0] = A.info[base + c.nt];
     c.sub[1] = A.info[base + nt_count + c.nt];
   } else {
     c.batch_m = 0;
     c.p = 0;
-    c.j = blockIdx.z;
+    c.j = bz;
     c.rows = min(TM, A.NCOL - c.row0);
-    const int nt_count = STAGE == ST_INV ? A.nti : A.ntf;
     c.sub[0] = A.info[c.nt];
     c.sub[1] = A.info[nt_count + c.nt];
   }
   return c;
 }
 
-// Loader context of one thread: its tile row, that row's base address and
-// fixed-point scale.
-struct RowCtx {
-  bool live;
-  const double* base;
-  int p;
-  double is_j;  // 1 / sin(theta_j) for the inverse stage's p = 2 rows
-  double rs;    // 2^(39 - E): value -> 40-bit fixed point
-  int e;        // the row group's exponent E (the analysis rows: E + 1, the E / O bound)
-};
-
+// the group exponent of a tile row (analysis rows: + 1, the E / O bound)
 template <int STAGE>
-__device__ __forceinline__ RowCtx row_ctx(const Args& A, const Cta& c, int r) {
-  RowCtx rc;
-  const int row = c.row0 + r;
-  rc.live = r < c.rows;
-  rc.p = 0;
-  rc.is_j = 0.0;
-  rc.e = 0;
-  rc.base = nullptr;
-  if (rc.live) {
-    if (STAGE == ST_SYNTH) {
-      const int chan = chan_of(c.p);
-      rc.base = A.X + (size_t)chan * A.NC + row;  // + slot * 4 NC
-      rc.e = group_exp(A.gX[chan * A.NC + row]);
-    } else if (STAGE == ST_INV) {
-      rc.p = row / A.F;
-      const int f = row % A.F;
-      rc.base = A.S + ((size_t)c.j * 6 + rc.p) * A.NC + 2 * f;  // + m nlat 6 NC
-      rc.is_j = A.invsin[c.j];
-      rc.e = group_exp(A.gS[rc.p * A.F + f]);
-    } else if (STAGE == ST_FWD) {
-      rc.base = A.Gs + (size_t)c.j * 2 * A.half * A.NCOL + row;  // + (sub half + i) NCOL
-      rc.e = group_exp(A.gG[row]);                                 // rows (p, f) = p F + f
-    } else {
-      rc.base = A.S + (size_t)c.batch_m * A.nlat * 6 * A.NC + (size_t)c.p * A.NC + row;  // + j 6 NC
-      rc.e = group_exp(A.gA[c.p * A.NC + row]) + 1;  // |R_j +- R_mirror| <= 2 max
-    }
-  }
-  rc.rs = pow2(FIX_BITS - rc.e);
-  return rc;
+__device__ __forceinline__ int row_exp(const Args& A, const Cta& c, int row) {
+  if (STAGE == ST_SYNTH) return group_exp(A.gX[chan_of(c.p) * A.NC + row]);
+  if (STAGE == ST_INV) return group_exp(A.gS[row]);  // rows (p, f) = p F + f
+  if (STAGE == ST_FWD) return group_exp(A.gG[row]);
+  return group_exp(A.gA[c.p * A.NC + row]) + 1;
 }
 
-// raw values of one thread's eight K of a chunk (the analysis also holds the
-// mirrored latitude's eight values)
-template <int N>
-struct OctT {
-  double v[N];
-};
+// K values of chunk (sub, kc) with data: K index k of the chunk is valid if
+// k < valid_k(...) (synthesis: l = m + sub + 2 kk <= L; inverse: m <= L, two K
+// per order; forward: i < half; analysis: j < nh)
 template <int STAGE>
-using Oct = OctT<STAGE == ST_ANA ? 16 : 8>;
-
-// Issue the global loads of eight consecutive K (zeros outside the valid range).
-template <int STAGE>
-__device__ __forceinline__ void fetch(const Args& A, const Cta& c, const RowCtx& rc, const int* slot_sm, int sub,
-                                      int k0, Oct<STAGE>& Q) {
-  constexpr int NV = STAGE == ST_ANA ? 16 : 8;
-#pragma unroll
-  for (int i = 0; i < NV; ++i) Q.v[i] = 0.0;
-  if (!rc.live) return;
+__device__ __forceinline__ int valid_k(const Args& A, const Cta& c, int sub, int kc) {
+  int kmax;
   if (STAGE == ST_SYNTH) {
-    // X[slot(l, m)][chan_p][n], l = m + par + 2 kk
-#pragma unroll
-    for (int q = 0; q < 8; ++q) {
-      const int dl = sub + 2 * (k0 + q);
-      if (c.batch_m + dl <= A.L) Q.v[q] = rc.base[(size_t)slot_sm[dl] * 4 * A.NC];
-    }
+    kmax = (A.L - c.batch_m - sub) >= 0 ? (A.L - c.batch_m - sub) / 2 + 1 : 0;
   } else if (STAGE == ST_INV) {
-    // (m, re), (m, im) for m = (sub ? 1 : 2) + 2 (k / 2)
-#pragma unroll
-    for (int h = 0; h < 4; ++h) {
-      const int m = (sub ? 1 : 2) + 2 * ((k0 >> 1) + h);
-      if (m <= A.L) {
-        const double2 z = *reinterpret_cast<const double2*>(rc.base + (size_t)m * A.nlat * 6 * A.NC);
-        Q.v[2 * h] = z.x;
-        Q.v[2 * h + 1] = z.y;
-      }
-    }
+    const int m0 = sub ? 1 : 2;
+    kmax = 2 * ((A.L - m0) >= 0 ? (A.L - m0) / 2 + 1 : 0);
   } else if (STAGE == ST_FWD) {
-    // s_i (sub 0) or d_i (sub 1), i = k
-#pragma unroll
-    for (int q = 0; q < 8; ++q) {
-      const int i = k0 + q;
-      if (i < A.half) Q.v[q] = rc.base[((size_t)sub * A.half + i) * A.NCOL];
-    }
+    kmax = A.half;
   } else {
-    // analysis: R_j and R_mirror over the northern rows j = k
-#pragma unroll
-    for (int q = 0; q < 8; ++q) {
-      const int j = k0 + q, jm = A.nlat - 1 - j;
-      if (j < A.nh) {
-        Q.v[q] = rc.base[(size_t)j * 6 * A.NC];
-        if (jm != j) Q.v[8 + q] = rc.base[(size_t)jm * 6 * A.NC];
-      }
-    }
+    kmax = A.nh;
   }
+  return max(0, min(KC, kmax - kc * KC));
 }
 
-// The eight A values of a fetched Oct (in place in Q.v[0..7]). `sum`
-// accumulates the CUDA-core side terms (inverse: column i = 0, sum_m 2 Re z_m;
-// forward: order 0, sum_i s_i).
 template <int STAGE>
-__device__ __forceinline__ void finish(const Cta& c, const RowCtx& rc, int sub, int k0, Oct<STAGE>& Q,
-                                       double& sum) {
-  if (STAGE == ST_INV) {
-#pragma unroll
-    for (int h = 0; h < 4; ++h) {
-      double re = Q.v[2 * h], im = Q.v[2 * h + 1];
-      if (rc.p == 2) {  // i (m / sin theta) z
-        const int m = (sub ? 1 : 2) + 2 * ((k0 >> 1) + h);
-        const double a = (double)m * rc.is_j;
-        const double t = re;
-        re = -a * im;
-        im = a * t;
-      } else if (rc.p == 5) {  // i z
-        const double t = re;
-        re = -im;
-        im = t;
-      }
-      Q.v[2 * h] = re;
-      Q.v[2 * h + 1] = im;
-      sum += 2.0 * re;
-    }
-  } else if (STAGE == ST_FWD) {
-    if (sub == 0)
-#pragma unroll
-      for (int q = 0; q < 8; ++q) sum += Q.v[q];
-  } else if (STAGE == ST_ANA) {  // E: R_j + sigma R_mirror; O: R_j - sigma R_mirror
-    const double sg = table_sigma(c.p) * (sub ? -1.0 : 1.0);
-#pragma unroll
-    for (int q = 0; q < 8; ++q) Q.v[q] = Q.v[q] + sg * Q.v[8 + q];
-  }
-}
-
-// ------------------------------------------------------------------ kernel
-
-template <int STAGE>
-__global__ void __launch_bounds__(NTHR_ALL, 1) k_oz_stage(Args A) {
+__global__ void __launch_bounds__(p::NTHR, 1) k_ozp_stage(Args A) {
+  using R = p::Ring<STAGE>;
   extern __shared__ unsigned char smraw[];
   unsigned char* sm = (unsigned char*)(((uintptr_t)smraw + 1023) & ~(uintptr_t)1023);
-  unsigned char* stage_base = sm;
-  uint64_t* bars = (uint64_t*)(sm + (size_t)NSTAGE * STAGE_BYTES);  // NSTAGE + 1: MMA done per stage, drain
-  uint64_t* bfull = bars + NSTAGE + 1;                               // NSTAGE: B bulk copy landed
-  uint64_t* afull = bfull + NSTAGE;                                  // NSTAGE: A stored by all loaders
-  uint32_t* tslot = (uint32_t*)(afull + NSTAGE);
+  unsigned char* raw = sm + R::RAW_OFF;
+  unsigned char* adig = sm + R::A_OFF;
+  unsigned char* bdig = sm + R::B_OFF;
+  double* rsum = (double*)(sm + R::SUM_OFF);
+  uint64_t* bar = (uint64_t*)(sm + R::BAR_OFF);
+  uint64_t* raw_full = bar;
+  uint64_t* raw_empty = raw_full + R::NRAW;
+  uint64_t* a_full = raw_empty + R::NRAW;
+  uint64_t* a_empty = a_full + R::NDST;
+  uint64_t* b_full = a_empty + R::NDST;
+  uint64_t* b_empty = b_full + R::NB;
+  uint64_t* acc_full = b_empty + R::NB;
+  uint64_t* acc_empty = acc_full + 1;
+  uint64_t* sum_full = acc_empty + 1;  // [2]
+  uint64_t* sum_empty = sum_full + 2;  // [2]
+  uint32_t* tslot = (uint32_t*)(bar + R::NBAR);
   volatile int* abort_flag = (volatile int*)(tslot + 1);
-  double* rsum = (double*)(sm + (size_t)NSTAGE * STAGE_BYTES + 256);  // [2 subs][4 quarters][TM]
-  int* slot_sm = (int*)(rsum + 2 * 4 * TM);                          // synthesis: slot(m + dl, m)
 
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  const Cta c = cta_info<STAGE>(A);
-  if (c.rows <= 0) return;
+  const int ntile = tile_count<STAGE>(A);
+  constexpr bool SIDE = (STAGE == ST_INV || STAGE == ST_FWD);
 
   if (tid == 0) {
-    for (int i = 0; i <= NSTAGE; ++i) mbar_init(&bars[i], 1);
-    for (int i = 0; i < NSTAGE; ++i) mbar_init(&bfull[i], 1);
-    for (int i = 0; i < NSTAGE; ++i) mbar_init(&afull[i], NLOAD);
+    for (int i = 0; i < R::NRAW; ++i) {
+      mbar_init(&raw_full[i], 1);
+      mbar_init(&raw_empty[i], p::NCONV);
+    }
+    for (int i = 0; i < R::NDST; ++i) {
+      mbar_init(&a_full[i], p::NCONV);
+      mbar_init(&a_empty[i], 1);
+    }
+    for (int i = 0; i < R::NB; ++i) {
+      mbar_init(&b_full[i], 1);
+      mbar_init(&b_empty[i], 1);
+    }
+    mbar_init(acc_full, 1);
+    mbar_init(acc_empty, p::NEPI);
+    for (int i = 0; i < 2; ++i) {
+      mbar_init(&sum_full[i], p::NCONV);
+      mbar_init(&sum_empty[i], p::NEPI);
+    }
     fence_mbar_init();
     *abort_flag = 0;
   }
-  if (warp == 0) tmem_alloc(tslot, TMEM_COLS);
-  for (int i = tid; i < 2 * 4 * TM; i += NTHR_ALL) rsum[i] = 0.0;
-  if (STAGE == ST_SYNTH)
-    for (int dl = tid; dl <= A.L - c.batch_m; dl += NTHR_ALL)
-      slot_sm[dl] = slot_row(A.kbeg, c.batch_m + dl, c.batch_m, A.nk);
+  if (warp == p::W_PROD) tmem_alloc(tslot, TMEM_COLS);
   tc_fence_before();
   __syncthreads();
   tc_fence_after();
   const uint32_t tmem = *tslot;
 
-  const int nch0 = c.sub[0].kpad / KC, nch1 = c.sub[1].kpad / KC, nch = nch0 + nch1;
-  // loader mapping: row lr = tid % TM, K quarter lq = tid / TM (eight K of the chunk)
-  const int lr = tid % TM, lq = tid / TM;
-  RowCtx rc;
-  if (tid < NLOAD) rc = row_ctx<STAGE>(A, c, lr);
-  double sum0 = 0.0, sum1 = 0.0;  // loader side sums of the two sub-GEMMs
-  int b_issued = 0;               // B copies issued (loader thread 0 issues them)
-  auto copy_b = [&](int b, const ImgInfo& I, int kc) {
-    if (tid == 0) {
-      unsigned char* dst = stage_base + (size_t)b * STAGE_BYTES + A_BYTES;
-      const uint32_t bytes = (uint32_t)(NDIG * 2 * I.npad * 16);
-      const unsigned char* src = A.img + I.off + (size_t)kc * bytes;
-      mbar_expect_tx(&bfull[b], bytes);
-      bulk_g2s(dst, src, bytes, &bfull[b]);
-    }
-    ++b_issued;
-  };
-  auto fetch_chunk = [&](int ch, Oct<STAGE>& Q) {
-    const int sub = ch < nch0 ? 0 : 1, kc = sub ? ch - nch0 : ch;
-    fetch<STAGE>(A, c, rc, slot_sm, sub, kc * KC + 8 * lq, Q);
-  };
-  __shared__ int s_b_issued, s_mma_issued;
-  if (warp == MMA_WARP) {
-    // ---- MMA issuer: chunk ch once its A (all loaders) and B (bulk copy) landed
-    if (lane == 0) {
-      int b_done = 0, issued = 0;
-      for (int ch = 0; ch < nch; ++ch) {
-        const int buf = ch % NSTAGE;
-        const uint32_t ph = (uint32_t)((ch / NSTAGE) & 1);
-        if (!mbar_wait_or_abort_ns(&afull[buf], ph, abort_flag, A.wait_ns)) {
-          *abort_flag = 1;
-          atomicOr(A.status, 1ull << (28 + STAGE));
-          break;
-        }
-        if (!mbar_wait_ns(&bfull[buf], ph, HW_WAIT_NS)) {
-          *abort_flag = 1;
-          atomicOr(A.status, 1ull << (20 + STAGE));
-          break;
-        }
-        ++b_done;
-        tc_fence_after();
+  if (warp == p::W_PROD) {
+    // ------------------------------------------------------------ producer
+    // every lane takes the same path: lane 0 waits, the result is broadcast
+    int gc = 0;       // chunks issued
+    int last_b = -1;  // B copies issued: chunk ids 0 .. last_b (for the exit wait)
+    bool stop = false;
+    for (int t = blockIdx.x; t < ntile && !stop; t += gridDim.x) {
+      const Cta c = tile_info<STAGE>(A, t);
+      const int nch0 = c.sub[0].kpad / KC, nch = nch0 + c.sub[1].kpad / KC;
+      if (nch == 0 || c.rows <= 0) continue;
+      const size_t rbytes = (size_t)c.rows * 8;
+      for (int ch = 0; ch < nch; ++ch, ++gc) {
         const int sub = ch < nch0 ? 0 : 1, kc = sub ? ch - nch0 : ch;
-        const ImgInfo& I = c.sub[sub];
-        const unsigned char* Ab = stage_base + (size_t)buf * STAGE_BYTES;
-        const unsigned char* Bb = Ab + A_BYTES;
-        const uint32_t idesc = idesc_i8(TM, I.npad);
-#pragma unroll
-        for (int s = 0; s < NDIG; ++s) {
-          const uint64_t da = sdesc(saddr(Ab + s * A_PLANE), TM * 16, 128);
-#pragma unroll
-          for (int t = 0; t < NLEV - s; ++t) {
-            const uint64_t db = sdesc(saddr(Bb + t * 2 * I.npad * 16), I.npad * 16, 128);
-            const uint32_t d = tmem + (uint32_t)(((s + t) * 2 + sub) * TN);
-            mma_i8(d, da, db, idesc, (kc > 0 || s > 0) ? 1u : 0u);
+        const int rs = gc % R::NRAW, bs = gc % R::NB;
+        int ok = 1;
+        if (lane == 0) {
+          if (gc >= R::NRAW &&
+              !mbar_wait_or_abort_ns(&raw_empty[rs], (uint32_t)((gc / R::NRAW - 1) & 1), abort_flag, A.wait_ns))
+            ok = 0;
+          if (ok && gc >= R::NB &&
+              !mbar_wait_or_abort_ns(&b_empty[bs], (uint32_t)((gc / R::NB - 1) & 1), abort_flag, A.wait_ns))
+            ok = 0;
+          if (!ok) {
+            atomicOr(A.status, 1ull << (24 + STAGE));
+            *abort_flag = 1;
           }
         }
-        mma_commit(&bars[buf]);
-        ++issued;
+        if (!__shfl_sync(0xffffffffu, ok, 0)) {
+          stop = true;
+          break;
+        }
+        // raw copies of this chunk: K value q of the chunk at lane q
+        const int kv = valid_k<STAGE>(A, c, sub, kc);
+        unsigned char* rdst = raw + (size_t)rs * R::RAW_BYTES;
+        const void* src[2] = {nullptr, nullptr};
+        void* dst[2] = {nullptr, nullptr};
+        uint32_t nb[2] = {0, 0};
+        if (STAGE == ST_SYNTH) {
+          if (lane < kv) {
+            const int l = c.batch_m + sub + 2 * (kc * KC + lane);
+            const int slot = slot_row(A.kbeg, l, c.batch_m, A.nk);
+            src[0] = A.X + ((size_t)slot * 4 + chan_of(c.p)) * A.NC + c.row0;
+            dst[0] = rdst + (size_t)lane * TM * 8;
+            nb[0] = (uint32_t)rbytes;
+          }
+        } else if (STAGE == ST_INV) {  // one copy per order: (re, im) of every row
+          if (2 * lane < kv) {
+            const int m = (sub ? 1 : 2) + 2 * (kc * (KC / 2) + lane);
+            src[0] = A.S + ((size_t)m * A.nlat + c.j) * 6 * A.NC + 2 * (size_t)c.row0;
+            dst[0] = rdst + (size_t)lane * TM * 16;
+            nb[0] = (uint32_t)(2 * rbytes);
+          }
+        } else if (STAGE == ST_FWD) {
+          if (lane < kv) {
+            const int i = kc * KC + lane;
+            src[0] = A.Gs + ((size_t)c.j * 2 * A.half + (size_t)sub * A.half + i) * A.NCOL + c.row0;
+            dst[0] = rdst + (size_t)lane * TM * 8;
+            nb[0] = (uint32_t)rbytes;
+          }
+        } else {
+          if (lane < kv) {
+            const int j = kc * KC + lane, jm = A.nlat - 1 - j;
+            const double* base = A.S + (size_t)c.batch_m * A.nlat * 6 * A.NC + (size_t)c.p * A.NC + c.row0;
+            src[0] = base + (size_t)j * 6 * A.NC;
+            dst[0] = rdst + (size_t)lane * TM * 8;
+            nb[0] = (uint32_t)rbytes;
+            if (jm != j) {
+              src[1] = base + (size_t)jm * 6 * A.NC;
+              dst[1] = rdst + (size_t)(KC + lane) * TM * 8;
+              nb[1] = (uint32_t)rbytes;
+            }
+          }
+        }
+        uint32_t total = nb[0] + nb[1];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) total += __shfl_xor_sync(0xffffffffu, total, o);
+        if (lane == 0) {
+          if (total > 0)
+            mbar_expect_tx(&raw_full[rs], total);
+          else
+            mbar_arrive(&raw_full[rs]);  // nothing to copy: the converters write zeros
+        }
+        __syncwarp();
+        if (nb[0]) bulk_g2s(dst[0], src[0], nb[0], &raw_full[rs]);
+        if (nb[1]) bulk_g2s(dst[1], src[1], nb[1], &raw_full[rs]);
+        // the chunk's B digit image
+        if (lane == 0) {
+          const ImgInfo& I = c.sub[sub];
+          const uint32_t bytes = (uint32_t)(NDIG * 2 * I.npad * 16);
+          mbar_expect_tx(&b_full[bs], bytes);
+          bulk_g2s(bdig + (size_t)bs * B_BYTES_MAX, A.img + I.off + (size_t)kc * bytes, bytes, &b_full[bs]);
+        }
+        last_b = gc;
+        __syncwarp();
       }
-      if (issued > 0) mma_commit(&bars[NSTAGE]);  // drain: tracks every MMA this thread issued
-      s_b_issued = b_done;
-      s_mma_issued = issued;
+    }
+    // copies still in flight (after an abort): wait for the last ones of each ring
+    if (lane == 0) {
+      for (int q = max(0, gc - R::NRAW); q < gc; ++q)
+        if (!mbar_wait_ns(&raw_full[q % R::NRAW], (uint32_t)((q / R::NRAW) & 1), HW_WAIT_NS))
+          atomicOr(A.status, 1ull << (20 + STAGE));
+      for (int q = max(0, last_b + 1 - R::NB); q <= last_b; ++q)
+        if (!mbar_wait_ns(&b_full[q % R::NB], (uint32_t)((q / R::NB) & 1), HW_WAIT_NS))
+          atomicOr(A.status, 1ull << (20 + STAGE));
     }
     __syncwarp();
-  } else {
-    // ---- loaders: A of chunk ch into stage buffer ch % NSTAGE, B bulk copies one chunk ahead
-    Oct<STAGE> cur, nxt;
-    if (nch > 0) {
-      copy_b(0, c.sub[0].kpad > 0 ? c.sub[0] : c.sub[1], 0);
-      fetch_chunk(0, cur);
-    }
-    for (int ch = 0; ch < nch; ++ch) {
-      const int buf = ch % NSTAGE;
-      const int sub = ch < nch0 ? 0 : 1, kc = sub ? ch - nch0 : ch;
-      const bool more = ch + 1 < nch;
-      if (more) {
-        // stage buffer of chunk ch + 1 was last read by the MMAs of chunk ch + 1 - NSTAGE
-        const int nb = (ch + 1) % NSTAGE;
-        if (ch + 1 >= NSTAGE &&
-            !mbar_wait_or_abort_ns(&bars[nb], (uint32_t)(((ch + 1) / NSTAGE - 1) & 1), abort_flag, A.wait_ns)) {
+  } else if (warp == p::W_MMA) {
+    // ------------------------------------------------------------ MMA issuer
+    if (lane == 0) {
+      int gc = 0, gt = 0;
+      bool stop = false;
+      for (int t = blockIdx.x; t < ntile && !stop; t += gridDim.x) {
+        const Cta c = tile_info<STAGE>(A, t);
+        const int nch0 = c.sub[0].kpad / KC, nch = nch0 + c.sub[1].kpad / KC;
+        if (nch == 0 || c.rows <= 0) continue;
+        // the epilogue has read the previous tile's accumulators
+        if (gt >= 1 && !mbar_wait_or_abort_ns(acc_empty, (uint32_t)((gt - 1) & 1), abort_flag, A.wait_ns)) {
+          atomicOr(A.status, 1ull << (28 + STAGE));
           *abort_flag = 1;
-          atomicOr(A.status, 1ull << (24 + STAGE));
+          break;
         }
-        if (*abort_flag) break;
-        const int sub1 = (ch + 1) < nch0 ? 0 : 1, kc1 = sub1 ? ch + 1 - nch0 : ch + 1;
-        copy_b(nb, c.sub[sub1], kc1);
-        fetch_chunk(ch + 1, nxt);
-      }
-      // A of chunk ch: finish, slice into digits, store
-      double part = 0.0;
-      finish<STAGE>(c, rc, sub, kc * KC + 8 * lq, cur, part);
-      if (sub)
-        sum1 += part;
-      else
-        sum0 += part;
-      uint2 pl[NDIG];
-      to_digits8(cur.v, rc.rs, pl);
-      unsigned char* Ab = stage_base + (size_t)buf * STAGE_BYTES;
-      // digit plane s, K group lq / 2 (16 K), row lr, bytes 8 (lq & 1) .. + 7
-      const size_t at = ((size_t)(lq >> 1) * TM + lr) * 16 + 8 * (lq & 1);
+        tc_fence_after();
+        for (int ch = 0; ch < nch; ++ch, ++gc) {
+          const int sub = ch < nch0 ? 0 : 1, kc = sub ? ch - nch0 : ch;
+          const int ds = gc % R::NDST, bs = gc % R::NB;
+          if (!mbar_wait_or_abort_ns(&a_full[ds], (uint32_t)((gc / R::NDST) & 1), abort_flag, A.wait_ns) ||
+              !mbar_wait_or_abort_ns(&b_full[bs], (uint32_t)((gc / R::NB) & 1), abort_flag, HW_WAIT_NS)) {
+            atomicOr(A.status, 1ull << (28 + STAGE));
+            *abort_flag = 1;
+            stop = true;
+            break;
+          }
+          tc_fence_after();
+          const ImgInfo& I = c.sub[sub];
+          const unsigned char* Ab = adig + (size_t)ds * A_BYTES;
+          const unsigned char* Bb = bdig + (size_t)bs * B_BYTES_MAX;
+          const uint32_t idesc = idesc_i8(TM, I.npad);
 #pragma unroll
-      for (int s = 0; s < NDIG; ++s) *reinterpret_cast<uint2*>(Ab + s * A_PLANE + at) = pl[s];
-      fence_async_smem();  // this thread's A stores, visible to the tensor cores
-      mbar_arrive(&afull[buf]);
-      if (more) cur = nxt;
+          for (int s = 0; s < NDIG; ++s) {
+            const uint64_t da = sdesc(saddr(Ab + s * A_PLANE), TM * 16, 128);
+#pragma unroll
+            for (int u = 0; u < NLEV - s; ++u) {
+              const uint64_t db = sdesc(saddr(Bb + u * 2 * I.npad * 16), I.npad * 16, 128);
+              const uint32_t d = tmem + (uint32_t)(((s + u) * 2 + sub) * TN);
+              mma_i8(d, da, db, idesc, (kc > 0 || s > 0) ? 1u : 0u);
+            }
+          }
+          mma_commit(&a_empty[ds]);
+          mma_commit(&b_empty[bs]);
+        }
+        if (stop) break;
+        mma_commit(acc_full);  // every MMA of the tile
+        ++gt;
+      }
+      // drain: the last commit completes once every MMA issued has
+      if (gc > 0 && !mbar_wait_ns(&a_empty[(gc - 1) % R::NDST], (uint32_t)(((gc - 1) / R::NDST) & 1), HW_WAIT_NS))
+        atomicOr(A.status, 1ull << (16 + STAGE));
     }
-  }
-  __syncthreads();
-  // B copies still in flight after an abort: wait for them before the stage
-  // ring is reused or the CTA exits
-  if (tid == 0)
-    for (int q = s_b_issued; q < b_issued; ++q)
-      if (!mbar_wait_ns(&bfull[q % NSTAGE], (uint32_t)((q / NSTAGE) & 1), HW_WAIT_NS))
-        atomicOr(A.status, 1ull << (20 + STAGE));
-  // drain: the issuer's last commit completes once every MMA has
-  bool ok = (*abort_flag == 0);
-  if (s_mma_issued > 0 && !mbar_wait_ns(&bars[NSTAGE], 0, HW_WAIT_NS)) {
-    ok = false;
-    atomicOr(A.status, 1ull << (16 + STAGE));
-  }
-  if (tid < NLOAD) {
-    rsum[(0 * 4 + lq) * TM + lr] = sum0;
-    rsum[(1 * 4 + lq) * TM + lr] = sum1;
-  }
-  ok = __syncthreads_and(ok) != 0;
-  tc_fence_after();
-
-  if (ok && tid < NLOAD) {
-    const int quad = warp & 3, cq = warp >> 2;  // lane quarter, column-block group (4 per quarter)
+    __syncwarp();
+  } else if (warp < p::W_EPI) {
+    // ------------------------------------------------------------ converters
+    const int ct = tid - p::W_CONV * 32;  // 0 .. 255
+    const int lr = ct % TM, g = ct / TM;   // row, K group of 16
+    int gc = 0, gt = 0;
+    for (int t = blockIdx.x; t < ntile && !*abort_flag; t += gridDim.x) {
+      const Cta c = tile_info<STAGE>(A, t);
+      const int nch0 = c.sub[0].kpad / KC, nch = nch0 + c.sub[1].kpad / KC;
+      if (nch == 0 || c.rows <= 0) continue;
+      const bool live = lr < c.rows;
+      const int row = c.row0 + lr;
+      const int e = live ? row_exp<STAGE>(A, c, row) : 0;
+      const double rs = pow2(FIX_BITS - e);
+      const double is_j = (STAGE == ST_INV) ? A.invsin[c.j] : 0.0;
+      const int prow = (STAGE == ST_INV) ? row / A.F : 0;
+      double side[2] = {0.0, 0.0};
+      bool ok = true;
+      for (int ch = 0; ch < nch; ++ch, ++gc) {
+        const int sub = ch < nch0 ? 0 : 1, kc = sub ? ch - nch0 : ch;
+        const int rsi = gc % R::NRAW, ds = gc % R::NDST;
+        if (!mbar_wait_or_abort_ns(&raw_full[rsi], (uint32_t)((gc / R::NRAW) & 1), abort_flag, HW_WAIT_NS) ||
+            (gc >= R::NDST &&
+             !mbar_wait_or_abort_ns(&a_empty[ds], (uint32_t)((gc / R::NDST - 1) & 1), abort_flag, A.wait_ns))) {
+          atomicOr(A.status, 1ull << (24 + STAGE));
+          *abort_flag = 1;
+          ok = false;
+          break;
+        }
+        const int kv = valid_k<STAGE>(A, c, sub, kc);
+        const double* rv = (const double*)(raw + (size_t)rsi * R::RAW_BYTES);
+        double v[16];
+#pragma unroll
+        for (int q = 0; q < 16; ++q) {
+          const int k = 16 * g + q;
+          double x = 0.0;
+          if (live && k < kv) {
+            if (STAGE == ST_INV) {
+              const int mo = k >> 1, ri = k & 1;
+              const double re = rv[(size_t)mo * TM * 2 + 2 * lr], im = rv[(size_t)mo * TM * 2 + 2 * lr + 1];
+              double tre = re, tim = im;
+              if (prow == 2) {  // i (m / sin theta) z
+                const int m = (sub ? 1 : 2) + 2 * (kc * (KC / 2) + mo);
+                const double a = (double)m * is_j;
+                tre = -a * im;
+                tim = a * re;
+              } else if (prow == 5) {  // i z
+                tre = -im;
+                tim = re;
+              }
+              x = ri ? tim : tre;
+              if (!ri) side[sub] += 2.0 * tre;
+            } else if (STAGE == ST_ANA) {
+              const int j = kc * KC + k, jm = A.nlat - 1 - j;
+              const double r0 = rv[(size_t)k * TM + lr];
+              const double r1 = (jm != j) ? rv[(size_t)(KC + k) * TM + lr] : 0.0;
+              const double sg = table_sigma(c.p) * (sub ? -1.0 : 1.0);
+              x = r0 + sg * r1;
+            } else {
+              x = rv[(size_t)k * TM + lr];
+              if (STAGE == ST_FWD && sub == 0) side[0] += x;
+            }
+          }
+          v[q] = x;
+        }
+        uint2 lo[NDIG], hi[NDIG];
+        to_digits8(v, rs, lo);
+        to_digits8(v + 8, rs, hi);
+        unsigned char* Ab = adig + (size_t)ds * A_BYTES + ((size_t)g * TM + lr) * 16;
+#pragma unroll
+        for (int s = 0; s < NDIG; ++s)
+          *reinterpret_cast<uint4*>(Ab + s * A_PLANE) = make_uint4(lo[s].x, lo[s].y, hi[s].x, hi[s].y);
+        fence_async_smem();
+        mbar_arrive(&a_full[ds]);
+        mbar_arrive(&raw_empty[rsi]);
+      }
+      if (!ok) break;
+      if (SIDE) {  // the tile's side sums, for its epilogue
+        const int tb = gt & 1;
+        if (gt >= 2 &&
+            !mbar_wait_or_abort_ns(&sum_empty[tb], (uint32_t)(((gt >> 1) - 1) & 1), abort_flag, A.wait_ns)) {
+          atomicOr(A.status, 1ull << (24 + STAGE));
+          *abort_flag = 1;
+          break;
+        }
+        rsum[((tb * 2 + 0) * 2 + g) * TM + lr] = side[0];
+        rsum[((tb * 2 + 1) * 2 + g) * TM + lr] = side[1];
+        mbar_arrive(&sum_full[tb]);
+      }
+      ++gt;
+    }
+  } else {
+    // ------------------------------------------------------------ epilogue
+    // tcgen05.ld is warp-collective: lane 0 waits, the result is broadcast
+    const int ew = warp - p::W_EPI;  // 0 .. 7
+    const int quad = warp & 3, half_id = ew >> 2;
     const int r = quad * 32 + lane;
-    const int row = c.row0 + r;
-    const bool live = r < c.rows;
     const uint32_t tbase = tmem + ((uint32_t)(quad * 32) << 16);
-    const bool has[2] = {nch0 > 0, nch1 > 0};
-    const int npad_max = max(has[0] ? c.sub[0].npad : 0, has[1] ? c.sub[1].npad : 0);
-    // the row's group exponent, as the loaders of this row used it
-    const RowCtx rrc = row_ctx<STAGE>(A, c, r);
-    const double rf = pow2(rrc.e - 7);
-    // one sub-GEMM's eight columns cb .. cb + 7, combined and scaled (zero past its N)
-    auto load_block = [&](int sub, int cb, double* out) {
-      if (!has[sub] || cb >= c.sub[sub].npad) {
-#pragma unroll
-        for (int i = 0; i < 8; ++i) out[i] = 0.0;
-        return;
-      }
-      int a[NLEV][8];
-#pragma unroll
-      for (int lv = 0; lv < NLEV; ++lv) tmem_ld8_nowait(tbase + (uint32_t)((lv * 2 + sub) * TN + cb), a[lv]);
-      tmem_wait_ld();
-      const double* cs = A.bscale + c.sub[sub].sc + cb;
-#pragma unroll
-      for (int i = 0; i < 8; ++i) out[i] = combine_levels(a[0], a[1], a[2], a[3], a[4], i) * rf * __ldg(&cs[i]);
-    };
-    if (STAGE == ST_SYNTH) {
-      const int m = c.batch_m, p = c.p;
-      const double sg = table_sigma(p);
-      double gmax = 0.0;
-      for (int cb = cq * 8; cb < npad_max; cb += 32) {
-        double e[8], o[8];
-        load_block(0, cb, e);
-        load_block(1, cb, o);
-        if (!live) continue;
-#pragma unroll
-        for (int i = 0; i < 8; ++i) {
-          const int j = c.nt * TN + cb + i;
-          if (j >= A.nh) break;
-          const int jm = A.nlat - 1 - j;
-          const double vn = e[i] + o[i];
-          A.S[(((size_t)m * A.nlat + j) * 6 + p) * A.NC + row] = vn;
-          // the inverse stage reads p = 2 as (m / sin theta) S
-          const double fj = (p == 2) ? (double)m * A.invsin[j] : 1.0;
-          gmax = fmax(gmax, fabs(vn) * fj);
-          if (jm != j) {
-            const double vs = sg * (e[i] - o[i]);
-            A.S[(((size_t)m * A.nlat + jm) * 6 + p) * A.NC + row] = vs;
-            const double fm = (p == 2) ? (double)m * A.invsin[jm] : 1.0;
-            gmax = fmax(gmax, fabs(vs) * fm);
-          }
+    int gt = 0;
+    for (int t = blockIdx.x; t < ntile; t += gridDim.x) {
+      const Cta c = tile_info<STAGE>(A, t);
+      const int nch0 = c.sub[0].kpad / KC, nch1 = c.sub[1].kpad / KC;
+      if (nch0 + nch1 == 0 || c.rows <= 0) continue;
+      int ok = 1;
+      if (lane == 0) {
+        if (!mbar_wait_or_abort_ns(acc_full, (uint32_t)(gt & 1), abort_flag, A.wait_ns)) ok = 0;
+        if (ok && SIDE &&
+            !mbar_wait_or_abort_ns(&sum_full[gt & 1], (uint32_t)((gt >> 1) & 1), abort_flag, A.wait_ns))
+          ok = 0;
+        if (!ok) {
+          atomicOr(A.status, 1ull << (28 + STAGE));
+          *abort_flag = 1;
         }
       }
-      if (live) atomic_max_bits(&A.gS[p * A.F + row / 2], gmax);
-    } else if (STAGE == ST_INV) {
-      const int p = row / A.F, f = row % A.F, e3 = f / 3;
-      double c0 = 0.0;  // m = 0 term (weight 1), the real part of z_0
-      if (live && p != 2) {
-        const double2 z = *reinterpret_cast<const double2*>(A.S + (((size_t)0 * A.nlat + c.j) * 6 + p) * A.NC + 2 * f);
-        c0 = (p == 5) ? -z.y : z.x;
+      if (!__shfl_sync(0xffffffffu, ok, 0)) break;
+      tc_fence_after();
+      double sev = 0.0, sod = 0.0;
+      if (SIDE) {
+        const int tb = gt & 1;
+        sev = rsum[((tb * 2 + 0) * 2 + 0) * TM + r] + rsum[((tb * 2 + 0) * 2 + 1) * TM + r];
+        sod = rsum[((tb * 2 + 1) * 2 + 0) * TM + r] + rsum[((tb * 2 + 1) * 2 + 1) * TM + r];
+        mbar_arrive(&sum_empty[tb]);
       }
-      // the latitude's rates mu / eta (nphi x ne3d doubles), staged once in the
-      // stage ring (free after the main loop: every MMA has completed)
-      const double* rate_g = A.rate + (size_t)c.j * A.nphi * A.ne3d;
-      const double* rate_j = rate_g + e3;
-      const bool staged = (size_t)A.nphi * A.ne3d * 8 <= (size_t)NSTAGE * STAGE_BYTES;
-      if (staged) {
-        double* rate_s = reinterpret_cast<double*>(stage_base);
-        for (int t = tid; t < A.nphi * A.ne3d; t += NLOAD) rate_s[t] = __ldg(&rate_g[t]);
-        asm volatile("bar.sync 1, %0;" ::"n"(NLOAD));  // the loader / epilogue warps only
-        rate_j = rate_s + e3;
-      }
-      double* gs = A.Gs + (size_t)c.j * 2 * A.half * A.NCOL + row;
-      double* gd = gs + (size_t)A.half * A.NCOL;
-      double gmax = 0.0;
-      auto emit = [&](int i, double ev, double od) {
-        double m1 = rate_j[(size_t)i * A.ne3d] * A.dt, m2 = rate_j[(size_t)(i + A.half) * A.ne3d] * A.dt;
-        if (A.trap) {
-          m1 = m1 / (1.0 + 0.5 * m1);
-          m2 = m2 / (1.0 + 0.5 * m2);
+      const int row = c.row0 + r;
+      const bool live = r < c.rows;
+      const bool has0 = nch0 > 0, has1 = nch1 > 0;
+      const int npad_max = max(has0 ? c.sub[0].npad : 0, has1 ? c.sub[1].npad : 0);
+      const double rf = pow2((live ? row_exp<STAGE>(A, c, row) : 0) - 7);
+      auto load_block = [&](int sub, int cb, double* out) {
+        const bool hs = sub ? has1 : has0;
+        const int np = sub ? c.sub[1].npad : c.sub[0].npad;
+        if (!hs || cb >= np) {
+#pragma unroll
+          for (int i = 0; i < 8; ++i) out[i] = 0.0;
+          return;
         }
-        const double g1 = -m1 * (ev + od), g2 = -m2 * (ev - od);
-        const double sv = g1 + g2, dv = g1 - g2;
-        gs[(size_t)i * A.NCOL] = sv;
-        gd[(size_t)i * A.NCOL] = dv;
-        gmax = fmax(gmax, fmax(fabs(sv), fabs(dv)));
+        int a[NLEV][8];
+#pragma unroll
+        for (int lv = 0; lv < NLEV; ++lv) tmem_ld8_nowait(tbase + (uint32_t)((lv * 2 + sub) * TN + cb), a[lv]);
+        tmem_wait_ld();
+        const double* cs = A.bscale + (sub ? c.sub[1].sc : c.sub[0].sc) + cb;
+#pragma unroll
+        for (int i = 0; i < 8; ++i) out[i] = combine_levels(a[0], a[1], a[2], a[3], a[4], i) * rf * __ldg(&cs[i]);
       };
-      if (live && c.nt == 0 && cq == 0) {
-        double sev = 0.0, sod = 0.0;
-        for (int q = 0; q < 4; ++q) {
-          sev += rsum[(0 * 4 + q) * TM + r];
-          sod += rsum[(1 * 4 + q) * TM + r];
-        }
-        emit(0, c0 + sev, sod);
-      }
-      for (int cb = cq * 8; cb < npad_max; cb += 32) {
-        double e[8], o[8];
-        load_block(0, cb, e);
-        load_block(1, cb, o);
-        if (!live) continue;
-#pragma unroll
-        for (int i = 0; i < 8; ++i) {
-          const int ii = 1 + c.nt * TN + cb + i;
-          if (ii >= A.half) break;
-          emit(ii, e[i] + c0, o[i]);
-        }
-      }
-      if (live) atomic_max_bits(&A.gG[row], gmax);
-    } else if (STAGE == ST_FWD) {
-      const int p = row / A.F, f = row % A.F;
-      const double isj = A.invsin[c.j];
-      const double beta_c = (p == 3 || p == 4) ? 2.0 : (p == 5 ? 4.0 : 1.0);
-      auto out = [&](int m) -> double2* {
-        return reinterpret_cast<double2*>(A.S + (((size_t)m * A.nlat + c.j) * 6 + p) * A.NC + 2 * f);
-      };
-      double gre = 0.0, gim = 0.0;
-      if (live && c.nt == 0 && cq == 0) {
-        // m = 0: F_0 = (2 pi / nphi) sum_i s_i, real
-        double s0 = 0.0;
-        for (int q = 0; q < 4; ++q) s0 += rsum[(0 * 4 + q) * TM + r];
-        const double v = (p == 2) ? 0.0 : beta_c * s0 * (2.0 * PI / (double)A.nphi);
-        *out(0) = make_double2(v, 0.0);
-        gre = fabs(v);
-      }
-      for (int sub = 0; sub < 2; ++sub) {
-        if (!has[sub]) continue;
-        const int npad = c.sub[sub].npad, nval = c.sub[sub].nvalid;
-        for (int cb = cq * 8; cb < npad; cb += 32) {
-          double v[8];
-          load_block(sub, cb, v);
-          if (!live) continue;
-#pragma unroll
-          for (int i = 0; i < 8; i += 2) {
-            const int kk = c.nt * TN + cb + i;  // (m, re) column; (m, im) follows
-            if (kk >= c.nt * TN + nval) break;
-            const int m = (sub ? 1 : 2) + 2 * (kk >> 1);
-            const double beta = (p == 2) ? (double)m * isj : beta_c;
-            const double re = beta * v[i], im = beta * v[i + 1];
-            *out(m) = make_double2(re, im);
-            gre = fmax(gre, fabs(re));
-            gim = fmax(gim, fabs(im));
-          }
-        }
-      }
-      if (live) {
-        atomic_max_bits(&A.gA[p * A.NC + 2 * f], gre);
-        atomic_max_bits(&A.gA[p * A.NC + 2 * f + 1], gim);
-      }
-    } else {
-      const int m = c.batch_m, p = c.p;
-      for (int sub = 0; sub < 2; ++sub) {
-        if (!has[sub]) continue;
-        const int npad = c.sub[sub].npad;
-        for (int cb = cq * 8; cb < npad; cb += 32) {
-          double v[8];
-          load_block(sub, cb, v);
+      if (STAGE == ST_SYNTH) {
+        const int m = c.batch_m, pp = c.p;
+        const double sg = table_sigma(pp);
+        double gmax = 0.0;
+        for (int cb = half_id * 8; cb < npad_max; cb += 16) {
+          double ev[8], od[8];
+          load_block(0, cb, ev);
+          load_block(1, cb, od);
           if (!live) continue;
 #pragma unroll
           for (int i = 0; i < 8; ++i) {
-            const int kk = c.nt * TN + cb + i;
-            const int l = m + sub + 2 * kk;
-            if (l > A.L) break;
-            A.dy[((size_t)slot_row(A.kbeg, l, m, A.nk) * 6 + p) * A.NC + row] = v[i];
+            const int j = c.nt * TN + cb + i;
+            if (j >= A.nh) break;
+            const int jm = A.nlat - 1 - j;
+            const double vn = ev[i] + od[i];
+            A.S[(((size_t)m * A.nlat + j) * 6 + pp) * A.NC + row] = vn;
+            gmax = fmax(gmax, fabs(vn) * ((pp == 2) ? (double)m * A.invsin[j] : 1.0));
+            if (jm != j) {
+              const double vs = sg * (ev[i] - od[i]);
+              A.S[(((size_t)m * A.nlat + jm) * 6 + pp) * A.NC + row] = vs;
+              gmax = fmax(gmax, fabs(vs) * ((pp == 2) ? (double)m * A.invsin[jm] : 1.0));
+            }
+          }
+        }
+        if (live) atomic_max_bits(&A.gS[pp * A.F + row / 2], gmax);
+      } else if (STAGE == ST_INV) {
+        const int pp = row / A.F, f = row % A.F, e3 = f / 3;
+        double c0 = 0.0;  // m = 0 term (weight 1), the real part of z_0
+        if (live && pp != 2) {
+          const double2 z =
+              *reinterpret_cast<const double2*>(A.S + (((size_t)0 * A.nlat + c.j) * 6 + pp) * A.NC + 2 * f);
+          c0 = (pp == 5) ? -z.y : z.x;
+        }
+        const double* rate_j = A.rate + (size_t)c.j * A.nphi * A.ne3d + e3;
+        double* gs = A.Gs + (size_t)c.j * 2 * A.half * A.NCOL + row;
+        double* gd = gs + (size_t)A.half * A.NCOL;
+        double gmax = 0.0;
+        auto emit = [&](int i, double ev, double od) {
+          double m1 = __ldg(&rate_j[(size_t)i * A.ne3d]) * A.dt;
+          double m2 = __ldg(&rate_j[(size_t)(i + A.half) * A.ne3d]) * A.dt;
+          if (A.trap) {
+            m1 = m1 / (1.0 + 0.5 * m1);
+            m2 = m2 / (1.0 + 0.5 * m2);
+          }
+          const double g1 = -m1 * (ev + od), g2 = -m2 * (ev - od);
+          const double sv = g1 + g2, dv = g1 - g2;
+          gs[(size_t)i * A.NCOL] = sv;
+          gd[(size_t)i * A.NCOL] = dv;
+          gmax = fmax(gmax, fmax(fabs(sv), fabs(dv)));
+        };
+        if (live && c.nt == 0 && half_id == 0) emit(0, c0 + sev, sod);
+        for (int cb = half_id * 8; cb < npad_max; cb += 16) {
+          double ev[8], od[8];
+          load_block(0, cb, ev);
+          load_block(1, cb, od);
+          if (!live) continue;
+#pragma unroll
+          for (int i = 0; i < 8; ++i) {
+            const int ii = 1 + c.nt * TN + cb + i;
+            if (ii >= A.half) break;
+            emit(ii, ev[i] + c0, od[i]);
+          }
+        }
+        if (live) atomic_max_bits(&A.gG[row], gmax);
+      } else if (STAGE == ST_FWD) {
+        const int pp = row / A.F, f = row % A.F;
+        const double isj = A.invsin[c.j];
+        const double beta_c = (pp == 3 || pp == 4) ? 2.0 : (pp == 5 ? 4.0 : 1.0);
+        auto out = [&](int m) -> double2* {
+          return reinterpret_cast<double2*>(A.S + (((size_t)m * A.nlat + c.j) * 6 + pp) * A.NC + 2 * f);
+        };
+        double gre = 0.0, gim = 0.0;
+        if (live && c.nt == 0 && half_id == 0) {
+          // m = 0: F_0 = (2 pi / nphi) sum_i s_i, real
+          const double v = (pp == 2) ? 0.0 : beta_c * sev * (2.0 * PI / (double)A.nphi);
+          *out(0) = make_double2(v, 0.0);
+          gre = fabs(v);
+        }
+        for (int sub = 0; sub < 2; ++sub) {
+          if (!(sub ? has1 : has0)) continue;
+          const int npad = c.sub[sub].npad, nval = c.sub[sub].nvalid;
+          for (int cb = half_id * 8; cb < npad; cb += 16) {
+            double v[8];
+            load_block(sub, cb, v);
+            if (!live) continue;
+#pragma unroll
+            for (int i = 0; i < 8; i += 2) {
+              const int kk = c.nt * TN + cb + i;  // (m, re) column; (m, im) follows
+              if (kk >= c.nt * TN + nval) break;
+              const int m = (sub ? 1 : 2) + 2 * (kk >> 1);
+              const double beta = (pp == 2) ? (double)m * isj : beta_c;
+              const double re = beta * v[i], im = beta * v[i + 1];
+              *out(m) = make_double2(re, im);
+              gre = fmax(gre, fabs(re));
+              gim = fmax(gim, fabs(im));
+            }
+          }
+        }
+        if (live) {
+          atomic_max_bits(&A.gA[pp * A.NC + 2 * f], gre);
+          atomic_max_bits(&A.gA[pp * A.NC + 2 * f + 1], gim);
+        }
+      } else {
+        const int m = c.batch_m, pp = c.p;
+        for (int sub = 0; sub < 2; ++sub) {
+          if (!(sub ? has1 : has0)) continue;
+          const int npad = c.sub[sub].npad;
+          for (int cb = half_id * 8; cb < npad; cb += 16) {
+            double v[8];
+            load_block(sub, cb, v);
+            if (!live) continue;
+#pragma unroll
+            for (int i = 0; i < 8; ++i) {
+              const int kk = c.nt * TN + cb + i;
+              const int l = m + sub + 2 * kk;
+              if (l > A.L) break;
+              A.dy[((size_t)slot_row(A.kbeg, l, m, A.nk) * 6 + pp) * A.NC + row] = v[i];
+            }
           }
         }
       }
+      tc_fence_before();
+      mbar_arrive(acc_empty);
+      ++gt;
     }
   }
   tc_fence_before();
   __syncthreads();
-  if (warp == 0) tmem_dealloc(tmem, TMEM_COLS);
+  if (warp == p::W_PROD) tmem_dealloc(tmem, TMEM_COLS);
 }
 
 // ------------------------------------------------------------------ operand images
@@ -770,6 +865,7 @@ int round_up_oz(int x, int m) { return (x + m - 1) / m * m; }
 struct OzPlan {
   oz::Args a;
   int ntile_rows_nc, ntile_rows_col;
+  int nsm = 148, tiles[4] = {0, 0, 0, 0};  // persistent grids: min(tiles, SMs) CTAs
   DArr<double> S, Gs, rate, bscale;
   DArr<unsigned char> img;
   DArr<unsigned long long> gmax;  // gX, gS, gG, gA back to back
@@ -901,10 +997,17 @@ void visc3d_oz_enable(vg_handle* h) {
   a.status = h->d_maxbits.p + 2;
   P->ntile_rows_nc = (NC + oz::TM - 1) / oz::TM;
   P->ntile_rows_col = (NCOL + oz::TM - 1) / oz::TM;
-  raise_smem_limit((const void*)oz::k_oz_stage<oz::ST_SYNTH>, oz::SMEM_BYTES);
-  raise_smem_limit((const void*)oz::k_oz_stage<oz::ST_INV>, oz::SMEM_BYTES);
-  raise_smem_limit((const void*)oz::k_oz_stage<oz::ST_FWD>, oz::SMEM_BYTES);
-  raise_smem_limit((const void*)oz::k_oz_stage<oz::ST_ANA>, oz::SMEM_BYTES);
+  raise_smem_limit((const void*)oz::k_ozp_stage<oz::ST_SYNTH>, oz::p::Ring<oz::ST_SYNTH>::SMEM);
+  raise_smem_limit((const void*)oz::k_ozp_stage<oz::ST_INV>, oz::p::Ring<oz::ST_INV>::SMEM);
+  raise_smem_limit((const void*)oz::k_ozp_stage<oz::ST_FWD>, oz::p::Ring<oz::ST_FWD>::SMEM);
+  raise_smem_limit((const void*)oz::k_ozp_stage<oz::ST_ANA>, oz::p::Ring<oz::ST_ANA>::SMEM);
+  int dev = 0;
+  VG_CUDA(cudaGetDevice(&dev));
+  VG_CUDA(cudaDeviceGetAttribute(&P->nsm, cudaDevAttrMultiProcessorCount, dev));
+  P->tiles[0] = P->ntile_rows_nc * a.nts * G.M * 6;
+  P->tiles[1] = P->ntile_rows_col * a.nti * nlat;
+  P->tiles[2] = P->ntile_rows_col * a.ntf * nlat;
+  P->tiles[3] = P->ntile_rows_nc * a.nta * G.M * 6;
   VG_CUDA(cudaStreamSynchronize(s));
 }
 
@@ -919,23 +1022,22 @@ unsigned long long* visc3d_oz_gather_max(vg_handle* h) {
 // The four exact tensor-core stages between the FP64 gather and the scatter.
 void visc3d_oz_run(vg_handle* h, double dt, bool trap) {
   OzPlan* P = static_cast<OzPlan*>(h->tc_plan);
-  const Grid& G = h->grid;
   cudaStream_t s = h->stream;
   oz::Args a = P->a;
   a.dt = dt;
   a.trap = trap ? 1 : 0;
   a.wait_ns = h->wait_ns;
-  auto launch = [&](auto kernel, int phase, const oz::ImgInfo* info, dim3 grid) {
+  auto launch = [&](auto kernel, int phase, const oz::ImgInfo* info, int tiles, size_t smem) {
     PhaseScope ps(h, phase);
     a.info = info;
-    kernel<<<grid, oz::NTHR_ALL, oz::SMEM_BYTES, s>>>(a);
+    kernel<<<std::max(1, std::min(tiles, P->nsm)), oz::p::NTHR, smem, s>>>(a);
     ++h->n_launch;
     VG_CUDA(cudaGetLastError());
   };
-  launch(oz::k_oz_stage<oz::ST_SYNTH>, VG_PH_V3_SYNTH, P->info_synth.p, dim3(P->ntile_rows_nc, a.nts, G.M * 6));
-  launch(oz::k_oz_stage<oz::ST_INV>, VG_PH_V3_LON_INV, P->info_inv.p, dim3(P->ntile_rows_col, a.nti, G.nlat));
-  launch(oz::k_oz_stage<oz::ST_FWD>, VG_PH_V3_LON_FWD, P->info_fwd.p, dim3(P->ntile_rows_col, a.ntf, G.nlat));
-  launch(oz::k_oz_stage<oz::ST_ANA>, VG_PH_V3_ANALYSIS, P->info_ana.p, dim3(P->ntile_rows_nc, a.nta, G.M * 6));
+  launch(oz::k_ozp_stage<oz::ST_SYNTH>, VG_PH_V3_SYNTH, P->info_synth.p, P->tiles[0], oz::p::Ring<oz::ST_SYNTH>::SMEM);
+  launch(oz::k_ozp_stage<oz::ST_INV>, VG_PH_V3_LON_INV, P->info_inv.p, P->tiles[1], oz::p::Ring<oz::ST_INV>::SMEM);
+  launch(oz::k_ozp_stage<oz::ST_FWD>, VG_PH_V3_LON_FWD, P->info_fwd.p, P->tiles[2], oz::p::Ring<oz::ST_FWD>::SMEM);
+  launch(oz::k_ozp_stage<oz::ST_ANA>, VG_PH_V3_ANALYSIS, P->info_ana.p, P->tiles[3], oz::p::Ring<oz::ST_ANA>::SMEM);
 }
 
 }  // namespace vg
