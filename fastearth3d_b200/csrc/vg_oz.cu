@@ -8,17 +8,18 @@
 // integer operands and exact 32-bit integer accumulation (tcgen05.mma
 // kind::i8), by digit slicing (the Ozaki scheme):
 //
-//   every FP64 operand value x of a scale group g is written as a 40-bit
-//   fixed-point integer xi = rint(x 2^(39 - E_g)), |x| < 2^E_g, and xi as five
-//   signed 8-bit digits, xi = sum_s d_s 256^(4 - s). A product of two such
+//   every FP64 operand value x of a scale group g is written as a fixed-point
+//   integer xi = rint(x 2^(38 - E_g)), |x| < 2^E_g (so |xi| < 2^38, inside the
+//   range of five balanced digits), and xi as five signed 8-bit digits,
+//   xi = sum_s d_s 256^(4 - s). A product of two such
 //   values is sum_{s,t} d_s g_t 256^(8 - s - t); the digit pairs of one level
 //   s + t = lambda share a weight, so each level is one int32 accumulator in
 //   tensor memory, summed exactly over K. Levels 0..4 are kept (15 digit-pair
-//   MMAs per K step); the dropped levels weigh < 2^-37 of |x|max |y|max per
+//   MMAs per K step); the dropped levels weigh < 2^-36 of |x|max |y|max per
 //   term. The epilogue combines the five levels in FP64 and applies the
 //   row and column scales.
 //
-// So the products carry ~38 significant bits relative to their operand
+// So the products carry ~36 significant bits relative to their operand
 // groups' maxima instead of the ~22 of a two-term TF32 split, and every stage
 // keeps its data in FP64 in HBM (S, Gs, dy) and applies the viscosity rates in
 // FP64. Scale groups: the operand rows of one stage that come from one field
@@ -60,7 +61,7 @@ constexpr int A_BYTES = NDIG * A_PLANE;
 constexpr int B_BYTES_MAX = NDIG * TN * KC;
 constexpr int TMEM_COLS = 512;                // 2 * NLEV * TN = 480 used
 constexpr int MAX_L = 511;
-constexpr int FIX_BITS = 39;                  // |xi| < 2^39: five signed 8-bit digits
+constexpr int FIX_BITS = 38;                  // |xi| < 2^38: within the five digits' range [-0x8080808080, 0x7F7F7F7F7F]
 constexpr unsigned long long HW_WAIT_NS = 2000000000ull;  // bound on waits for copies and MMAs
 static_assert(A_BYTES % 128 == 0 && B_BYTES_MAX % 128 == 0, "ring stages stay 128-byte aligned");
 
@@ -70,7 +71,7 @@ enum { ST_SYNTH = 0, ST_INV = 1, ST_FWD = 2, ST_ANA = 3 };
 struct ImgInfo {
   long long off;  // byte offset of chunk 0: chunks of NDIG x 2 x npad x 16 bytes follow
   int kpad, npad, nvalid, kvalid;
-  int sc;         // first of the image's npad column factors 2^(E_col - 7)
+  int sc;         // first of the image's npad column factors 2^(E_col - 6)
 };
 
 struct Args {
@@ -131,7 +132,7 @@ __device__ __forceinline__ int group_exp(unsigned long long bits) {
 __device__ __forceinline__ double pow2(int e) { return ldexp(1.0, e); }
 
 // five 8-bit digit planes of eight values (K consecutive) of one row:
-// xi = rint(v * rs) in [-2^39, 2^39), u = xi + sum_k 128 * 256^k in [0, 2^40),
+// xi = rint(v * rs) in [-2^38, 2^38), u = xi + sum_k 128 * 256^k in [0, 2^40),
 // digit k = byte k of u minus 128 = byte k of (u ^ 0x8080808080) as int8.
 // pl[s] holds digit s (most significant first) of the eight values.
 __device__ __forceinline__ void to_digits8(const double* v, double rs, uint2* pl) {
@@ -639,7 +640,7 @@ __global__ void __launch_bounds__(p::NTHR, 1) k_ozp_stage(Args A) {
       const bool live = r < c.rows;
       const bool has0 = nch0 > 0, has1 = nch1 > 0;
       const int npad_max = max(has0 ? c.sub[0].npad : 0, has1 ? c.sub[1].npad : 0);
-      const double rf = pow2((live ? row_exp<STAGE>(A, c, row) : 0) - 7);
+      const double rf = pow2((live ? row_exp<STAGE>(A, c, row) : 0) - (FIX_BITS - 32));
       auto load_block = [&](int sub, int cb, double* out) {
         const bool hs = sub ? has1 : has0;
         const int np = sub ? c.sub[1].npad : c.sub[0].npad;
@@ -823,7 +824,7 @@ __device__ double img_value(const ImgJob& J, int k, int n, const double* const* 
 
 // One CTA per image: per column the exponent of its largest entry, then every
 // entry's five digits at [chunk][digit][K group][n][16 bytes], and the
-// column factors 2^(E - 7) the epilogue applies.
+// column factors 2^(E - 6) the epilogue applies.
 __global__ void k_oz_images(const ImgJob* __restrict__ jobs, unsigned char* __restrict__ img,
                             double* __restrict__ bscale, const double* const* tabs, int L, int nlat, int nphi) {
   __shared__ int s_exp[TN];
@@ -835,7 +836,7 @@ __global__ void k_oz_images(const ImgJob* __restrict__ jobs, unsigned char* __re
     int e = 0;
     if (mx > 0.0) frexp(mx, &e);
     s_exp[n] = e;
-    bscale[J.info.sc + n] = ldexp(1.0, e - 7);
+    bscale[J.info.sc + n] = ldexp(1.0, e - (FIX_BITS - 32));
   }
   __syncthreads();
   unsigned char* base = img + J.info.off;

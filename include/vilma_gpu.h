@@ -74,8 +74,8 @@ typedef struct vg_params {
   /* arithmetic of the 3-D stress products (no reference counterpart):
    * VG_VISC3D_FP64 (default) on the CUDA cores; VG_VISC3D_EXACT_TC, the
    * Legendre and longitude contractions on the tensor cores as 8-bit digit
-   * slices of 40-bit fixed-point operands with exact int32 accumulation
-   * (~38 significant bits per product, FP64 between the stages);
+   * slices of 38-bit fixed-point operands with exact int32 accumulation
+   * (~36 significant bits per product, FP64 between the stages);
    * VG_VISC3D_SPLIT_TC, the same contractions with two-term TF32 operands and
    * FP32 accumulation (rsl within ~2e-6 of the FP64 path on the lmax-128
    * workload) */

@@ -233,6 +233,7 @@ struct SleSolver {
   double tol = 1e-7;
   bool fixed_ocean = false, subgrid = true, warm_start = false;
   long n_solve = 0, n_outer_tot = 0, n_inner_tot = 0;
+  int last_outer = 0, last_inner = 0, last_flips = 0;  // of the last solve (the device's vg_info counters)
 };
 struct SleResult {
   int n_outer_done = 0, n_inner_last = 0, n_coast_flip = 0, n_couple_done = 0;

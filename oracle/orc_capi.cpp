@@ -399,6 +399,9 @@ int orc_get_info(OrcHandle* h, vg_info* info) {
   info->nk = h->R.nk;
   info->ne3d = h->R.ne3d;
   info->n_sub_last = h->st.n_sub_last;
+  info->n_outer_last = h->sle.last_outer;
+  info->n_inner_last = h->sle.last_inner;
+  info->n_coast_flip_last = h->sle.last_flips;
   info->n_accept = h->st.n_accept;
   info->n_reject = h->st.n_reject;
   info->n_solve = h->st.n_solve;

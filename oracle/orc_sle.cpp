@@ -122,6 +122,9 @@ void sle_solve(SleSolver& sle, const Sht& s, Response& R, const double* d_ice, c
   else
     res.mass_resid = std::fabs(Cs_int);
   res.esl = dphi;
+  sle.last_outer = res.n_outer_done;
+  sle.last_inner = res.n_inner_last;
+  sle.last_flips = res.n_coast_flip;
 }
 
 // vilma_timestep.f90:79-227 stepper_advance, explicit (forward-Euler) branch.
