@@ -131,43 +131,53 @@ __device__ __forceinline__ int group_exp(unsigned long long bits) {
 
 __device__ __forceinline__ double pow2(int e) { return ldexp(1.0, e); }
 
-// five 8-bit digit planes of eight values (K consecutive) of one row:
-// xi = rint(v * rs) in [-2^38, 2^38), u = xi + sum_k 128 * 256^k in [0, 2^40),
-// digit k = byte k of u minus 128 = byte k of (u ^ 0x8080808080) as int8.
-// pl[s] holds digit s (most significant first) of the eight values.
-__device__ __forceinline__ void to_digits8(const double* v, double rs, uint2* pl) {
-  constexpr long long LIM = 1ll << FIX_BITS;
-  uint32_t lo[8], hi[8];
+// five 8-bit digit planes of sixteen values (K consecutive) of one row.
+// t = fma(v, rs, 2^52 + B) with B = sum_k 128 * 256^k rounds v * rs to an
+// integer xi and puts u = xi + B (0 <= u < 2^40 since |xi| < 2^38) in the low
+// mantissa bits of t; digit k = byte k of u minus 128, i.e. byte k of u with
+// its top bit flipped read as int8. pl[s] holds digit s (most significant
+// first) of the sixteen values, four values per 32-bit word.
+__device__ __forceinline__ void to_digits16(const double* v, double rs, uint4* pl) {
+  constexpr double MAGIC = 4503599627370496.0 + 551911719040.0;  // 2^52 + 0x8080808080
+  uint32_t w[5][4];
 #pragma unroll
-  for (int q = 0; q < 8; ++q) {
-    long long xi = __double2ll_rn(v[q] * rs);
-    xi = xi < -LIM ? -LIM : (xi > LIM - 1 ? LIM - 1 : xi);
-    const unsigned long long u = ((unsigned long long)(xi + 0x8080808080ll)) ^ 0x8080808080ull;
-    lo[q] = (uint32_t)u;
-    hi[q] = (uint32_t)(u >> 32);
-  }
-  auto gather4 = [](uint32_t w0, uint32_t w1, uint32_t w2, uint32_t w3, uint32_t b) {
-    const uint32_t sel = b | ((b + 4) << 4);
-    const uint32_t t01 = __byte_perm(w0, w1, sel), t23 = __byte_perm(w2, w3, sel);
-    return __byte_perm(t01, t23, 0x5410);
-  };
-  pl[0] = make_uint2(gather4(hi[0], hi[1], hi[2], hi[3], 0), gather4(hi[4], hi[5], hi[6], hi[7], 0));
+  for (int g = 0; g < 4; ++g) {
+    uint32_t lo[4], hi[4];
 #pragma unroll
-  for (int s = 1; s < NDIG; ++s) {
-    const uint32_t b = (uint32_t)(4 - s);
-    pl[s] = make_uint2(gather4(lo[0], lo[1], lo[2], lo[3], b), gather4(lo[4], lo[5], lo[6], lo[7], b));
+    for (int q = 0; q < 4; ++q) {
+      const double t = fma(v[4 * g + q], rs, MAGIC);
+      lo[q] = (uint32_t)__double2loint(t);
+      hi[q] = (uint32_t)__double2hiint(t);
+    }
+    // byte transpose of the four low words: out_b = byte b of lo[0..3]
+    const uint32_t t0 = __byte_perm(lo[0], lo[1], 0x5140), t1 = __byte_perm(lo[2], lo[3], 0x5140);
+    const uint32_t t2 = __byte_perm(lo[0], lo[1], 0x7362), t3 = __byte_perm(lo[2], lo[3], 0x7362);
+    w[4][g] = __byte_perm(t0, t1, 0x5410) ^ 0x80808080u;  // byte 0: the least significant digit
+    w[3][g] = __byte_perm(t0, t1, 0x7632) ^ 0x80808080u;
+    w[2][g] = __byte_perm(t2, t3, 0x5410) ^ 0x80808080u;
+    w[1][g] = __byte_perm(t2, t3, 0x7632) ^ 0x80808080u;
+    const uint32_t h01 = __byte_perm(hi[0], hi[1], 0x0040), h23 = __byte_perm(hi[2], hi[3], 0x0040);
+    w[0][g] = __byte_perm(h01, h23, 0x5410) ^ 0x80808080u;  // byte 4: the most significant digit
   }
+#pragma unroll
+  for (int s = 0; s < NDIG; ++s) pl[s] = make_uint4(w[s][0], w[s][1], w[s][2], w[s][3]);
+}
+
+// a signed 32-bit integer as a double, exactly: 2^52 + 2^51 + (a + 2^31)
+// assembled from its bits, less the offset (one integer and one FP64 add)
+__device__ __forceinline__ double i2d_exact(int a) {
+  return __hiloint2double(0x43380000, a ^ (int)0x80000000) - 6755401588539392.0;
 }
 
 // five int32 levels (weights 256^-lambda) -> FP64, before the row and column scales
 __device__ __forceinline__ double combine_levels(const int* a0, const int* a1, const int* a2, const int* a3,
                                                  const int* a4, int i) {
   constexpr double W = 0.00390625;  // 2^-8
-  double v = (double)a4[i];
-  v = fma(v, W, (double)a3[i]);
-  v = fma(v, W, (double)a2[i]);
-  v = fma(v, W, (double)a1[i]);
-  return fma(v, W, (double)a0[i]);
+  double v = i2d_exact(a4[i]);
+  v = fma(v, W, i2d_exact(a3[i]));
+  v = fma(v, W, i2d_exact(a2[i]));
+  v = fma(v, W, i2d_exact(a1[i]));
+  return fma(v, W, i2d_exact(a0[i]));
 }
 
 __device__ __forceinline__ int slot_row(const int* kbeg, int l, int m, int nk) {
@@ -534,9 +544,9 @@ __global__ void __launch_bounds__(p::NTHR, 1) k_ozp_stage(Args A) {
       for (int ch = 0; ch < nch; ++ch, ++gc) {
         const int sub = ch < nch0 ? 0 : 1, kc = sub ? ch - nch0 : ch;
         const int rsi = gc % R::NRAW, ds = gc % R::NDST;
-        if (!mbar_wait_or_abort_ns(&raw_full[rsi], (uint32_t)((gc / R::NRAW) & 1), abort_flag, HW_WAIT_NS) ||
+        if (!mbar_wait_sleep_ns(&raw_full[rsi], (uint32_t)((gc / R::NRAW) & 1), abort_flag, HW_WAIT_NS) ||
             (gc >= R::NDST &&
-             !mbar_wait_or_abort_ns(&a_empty[ds], (uint32_t)((gc / R::NDST - 1) & 1), abort_flag, A.wait_ns))) {
+             !mbar_wait_sleep_ns(&a_empty[ds], (uint32_t)((gc / R::NDST - 1) & 1), abort_flag, A.wait_ns))) {
           atomicOr(A.status, 1ull << (24 + STAGE));
           *abort_flag = 1;
           ok = false;
@@ -578,13 +588,11 @@ __global__ void __launch_bounds__(p::NTHR, 1) k_ozp_stage(Args A) {
           }
           v[q] = x;
         }
-        uint2 lo[NDIG], hi[NDIG];
-        to_digits8(v, rs, lo);
-        to_digits8(v + 8, rs, hi);
+        uint4 pl[NDIG];
+        to_digits16(v, rs, pl);
         unsigned char* Ab = adig + (size_t)ds * A_BYTES + ((size_t)g * TM + lr) * 16;
 #pragma unroll
-        for (int s = 0; s < NDIG; ++s)
-          *reinterpret_cast<uint4*>(Ab + s * A_PLANE) = make_uint4(lo[s].x, lo[s].y, hi[s].x, hi[s].y);
+        for (int s = 0; s < NDIG; ++s) *reinterpret_cast<uint4*>(Ab + s * A_PLANE) = pl[s];
         fence_async_smem();
         mbar_arrive(&a_full[ds]);
         mbar_arrive(&raw_empty[rsi]);
@@ -593,7 +601,7 @@ __global__ void __launch_bounds__(p::NTHR, 1) k_ozp_stage(Args A) {
       if (SIDE) {  // the tile's side sums, for its epilogue
         const int tb = gt & 1;
         if (gt >= 2 &&
-            !mbar_wait_or_abort_ns(&sum_empty[tb], (uint32_t)(((gt >> 1) - 1) & 1), abort_flag, A.wait_ns)) {
+            !mbar_wait_sleep_ns(&sum_empty[tb], (uint32_t)(((gt >> 1) - 1) & 1), abort_flag, A.wait_ns)) {
           atomicOr(A.status, 1ull << (24 + STAGE));
           *abort_flag = 1;
           break;
@@ -618,9 +626,9 @@ __global__ void __launch_bounds__(p::NTHR, 1) k_ozp_stage(Args A) {
       if (nch0 + nch1 == 0 || c.rows <= 0) continue;
       int ok = 1;
       if (lane == 0) {
-        if (!mbar_wait_or_abort_ns(acc_full, (uint32_t)(gt & 1), abort_flag, A.wait_ns)) ok = 0;
+        if (!mbar_wait_sleep_ns(acc_full, (uint32_t)(gt & 1), abort_flag, A.wait_ns)) ok = 0;
         if (ok && SIDE &&
-            !mbar_wait_or_abort_ns(&sum_full[gt & 1], (uint32_t)((gt >> 1) & 1), abort_flag, A.wait_ns))
+            !mbar_wait_sleep_ns(&sum_full[gt & 1], (uint32_t)((gt >> 1) & 1), abort_flag, A.wait_ns))
           ok = 0;
         if (!ok) {
           atomicOr(A.status, 1ull << (28 + STAGE));
@@ -844,7 +852,7 @@ __global__ void k_oz_images(const ImgJob* __restrict__ jobs, unsigned char* __re
   for (int t = threadIdx.x; t < kpad * npad; t += blockDim.x) {
     const int n = t % npad, k = t / npad;
     const double v = img_value(J, k, n, tabs, L, nlat, nphi);
-    long long xi = __double2ll_rn(ldexp(v, FIX_BITS - s_exp[n]));
+    long long xi = __double2ll_rn(ldexp(v, FIX_BITS - s_exp[n]));  // |xi| < 2^38 by the exponent
     xi = xi < -LIM ? -LIM : (xi > LIM - 1 ? LIM - 1 : xi);
     const unsigned long long u = ((unsigned long long)(xi + 0x8080808080ll)) ^ 0x8080808080ull;
     const int ch = k / KC, kg = (k % KC) / 16, kb = k % 16;

@@ -304,6 +304,7 @@ struct InnerArgs {
   const int *lm_m, *lm_l, *lm2k, *mbeg;
   double *rsl, *F, *Gp, *Sraw, *rowpart;
   double* Fc;  // longitude analysis of rho_w C per row [m][j][2] (fixed during the loop)
+  int pch;     // Legendre rows of one order staged in shared memory at a time
   SleScalars* sc;
   unsigned int* bar;  // count, generation, error
   unsigned long long wait_ns;  // bound on a grid barrier's wait (the handle's wait limit, 2 s by default)
@@ -462,11 +463,13 @@ __global__ void __launch_bounds__(512) k_sle_inner(InnerArgs A) {
       }
     }
     if (it <= A.n_inner) {
-      double* fw = sm;             // w_j F_m(j): [nlat][2]
-      double* ul = sm + 2 * nlat;  // u, N of the order: [l - m][4]
-      double* gp = ul + 4 * M;     // synthesis partials: [SYN_SPLIT][nlat][4]
+      double* fw = sm;                         // w_j F_m(j): [nlat][2]
+      double* ul = fw + 2 * nlat;              // u, N of the order: [l - m][4]
+      double* gp = ul + 4 * M;                 // synthesis partials: [SYN_SPLIT][nlat][4]
+      double* ps = gp + 4 * SYN_SPLIT * nlat;  // the order's Legendre rows, staged: [A.pch][nlat]
       for (int m = blockIdx.x; m < M; m += gridDim.x) {
         const int nl = A.lmax - m + 1, lm0 = A.mbeg[m];
+        const double* pm = A.plm + (size_t)lm0 * nlat;  // the order's rows are contiguous
         __syncthreads();
         for (int j = tid; j < nlat; j += nthr) {
           const size_t o = ((size_t)m * nlat + j) * 2;
@@ -478,59 +481,82 @@ __global__ void __launch_bounds__(512) k_sle_inner(InnerArgs A) {
           fw[2 * j] = A.wts[j] * re;
           fw[2 * j + 1] = A.wts[j] * im;
         }
-        __syncthreads();
-        // analysis + apply: a warp per degree
-        for (int q = wid; q < nl; q += nw) {
-          const int lm = lm0 + q, l = m + q;
-          const double* P = A.plm + (size_t)lm * nlat;
-          double re = 0.0, im = 0.0;
-          for (int j = lane; j < nlat; j += 32) {
-            const double pj = P[j];
-            re += pj * fw[2 * j];
-            im += pj * fw[2 * j + 1];
-          }
-          for (int o = 16; o > 0; o >>= 1) {
-            re += __shfl_down_sync(0xffffffffu, re, o);
-            im += __shfl_down_sync(0xffffffffu, im, o);
-          }
-          if (lane == 0) {
-            double* u4 = ul + 4 * q;
-            if (l == 0) {
-              u4[0] = A.gu[0] * re;
-              u4[1] = A.gu[0] * im;
-              u4[2] = A.gn[0] * re;
-              u4[3] = A.gn[0] * im;
-            } else {
-              const int k = A.lm2k[lm];
-              u4[0] = A.gu[l] * re + A.drift[(size_t)0 * A.nk + k];
-              u4[1] = A.gu[l] * im + A.drift[(size_t)1 * A.nk + k];
-              u4[2] = A.gn[l] * re - A.drift[(size_t)2 * A.nk + k] / A.g;
-              u4[3] = A.gn[l] * im - A.drift[(size_t)3 * A.nk + k] / A.g;
+        // analysis + apply, the rows staged chunk by chunk: a warp per degree
+        int staged = -1;  // first degree of the staged chunk
+        for (int c0 = 0; c0 < nl; c0 += A.pch) {
+          const int n = min(A.pch, nl - c0);
+          __syncthreads();
+          for (int t = tid; t < n * nlat; t += nthr) ps[t] = pm[(size_t)c0 * nlat + t];
+          staged = c0;
+          __syncthreads();
+          for (int q = c0 + wid; q < c0 + n; q += nw) {
+            const int lm = lm0 + q, l = m + q;
+            const double* P = ps + (size_t)(q - c0) * nlat;
+            double re = 0.0, im = 0.0;
+            for (int j = lane; j < nlat; j += 32) {
+              const double pj = P[j];
+              re += pj * fw[2 * j];
+              im += pj * fw[2 * j + 1];
+            }
+            for (int o = 16; o > 0; o >>= 1) {
+              re += __shfl_down_sync(0xffffffffu, re, o);
+              im += __shfl_down_sync(0xffffffffu, im, o);
+            }
+            if (lane == 0) {
+              double* u4 = ul + 4 * q;
+              if (l == 0) {
+                u4[0] = A.gu[0] * re;
+                u4[1] = A.gu[0] * im;
+                u4[2] = A.gn[0] * re;
+                u4[3] = A.gn[0] * im;
+              } else {
+                const int k = A.lm2k[lm];
+                u4[0] = A.gu[l] * re + A.drift[(size_t)0 * A.nk + k];
+                u4[1] = A.gu[l] * im + A.drift[(size_t)1 * A.nk + k];
+                u4[2] = A.gn[l] * re - A.drift[(size_t)2 * A.nk + k] / A.g;
+                u4[3] = A.gn[l] * im - A.drift[(size_t)3 * A.nk + k] / A.g;
+              }
             }
           }
         }
-        __syncthreads();
-        // synthesis of u and N on every latitude: SYN_SPLIT threads per latitude
+        // synthesis of u and N on every latitude: SYN_SPLIT threads per
+        // latitude, each over its run of degrees, chunk by chunk (the last
+        // staged chunk is still in place)
         const int per = (nl + SYN_SPLIT - 1) / SYN_SPLIT;
-        for (int t = tid; t < SYN_SPLIT * nlat; t += nthr) {
+        for (int base = 0; base < SYN_SPLIT * nlat; base += nthr) {
+          const int t = base + tid;
+          const bool act = t < SYN_SPLIT * nlat;
           const int j = t % nlat, sp = t / nlat;
           const int q0 = sp * per, q1 = min(nl, q0 + per);
-          const double* pc = A.plm + (size_t)lm0 * nlat + j;
           double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
-#pragma unroll 4
-          for (int q = q0; q < q1; ++q) {
-            const double pq = pc[(size_t)q * nlat];
-            const double* u4 = ul + 4 * q;
-            a0 += u4[0] * pq;
-            a1 += u4[1] * pq;
-            a2 += u4[2] * pq;
-            a3 += u4[3] * pq;
+          for (int c0 = (nl - 1) / A.pch * A.pch;; c0 -= A.pch) {  // staged chunk first, then back to 0
+            const int n = min(A.pch, nl - c0);
+            if (c0 != staged) {
+              __syncthreads();
+              for (int u = tid; u < n * nlat; u += nthr) ps[u] = pm[(size_t)c0 * nlat + u];
+              staged = c0;
+            }
+            __syncthreads();
+            if (act) {
+              const int qa = max(q0, c0), qb = min(q1, c0 + n);
+              for (int q = qa; q < qb; ++q) {
+                const double pq = ps[(size_t)(q - c0) * nlat + j];
+                const double* u4 = ul + 4 * q;
+                a0 += u4[0] * pq;
+                a1 += u4[1] * pq;
+                a2 += u4[2] * pq;
+                a3 += u4[3] * pq;
+              }
+            }
+            if (c0 == 0) break;
           }
-          double* o = gp + ((size_t)sp * nlat + j) * 4;
-          o[0] = a0;
-          o[1] = a1;
-          o[2] = a2;
-          o[3] = a3;
+          if (act) {
+            double* o = gp + ((size_t)sp * nlat + j) * 4;
+            o[0] = a0;
+            o[1] = a1;
+            o[2] = a2;
+            o[3] = a3;
+          }
         }
         __syncthreads();
         for (int j = tid; j < nlat; j += nthr) {
@@ -647,12 +673,20 @@ __global__ void __launch_bounds__(512) k_sle_inner(InnerArgs A) {
   if (blockIdx.x == 0 && tid == 0) A.sc->n_inner = final_it;
 }
 
+// Legendre rows of an order staged at a time: all of them up to lmax 128 on
+// a 129-row grid, in chunks beyond
+constexpr size_t SLE_PSTAGE_BYTES = 140 * 1024;
+static int sle_pch(const Grid& G) {
+  return std::max(1, std::min(G.lmax + 1, (int)(SLE_PSTAGE_BYTES / ((size_t)G.nlat * sizeof(double)))));
+}
+
 // dynamic shared memory of the fused loop: the row (nphi), the row's Fourier
-// sums of u and N (4 M), or an order's weighted F, its u and N and the
-// synthesis partials (2 nlat + 4 M + 4 SYN_SPLIT nlat)
+// sums of u and N (4 M), or an order's weighted F, its u and N, the
+// synthesis partials and its staged Legendre rows
 static size_t sle_inner_smem(const vg_handle* h) {
   const Grid& G = h->grid;
-  return (size_t)std::max({G.nphi, 4 * G.M, 2 * G.nlat + 4 * G.M + 4 * SYN_SPLIT * G.nlat}) * sizeof(double);
+  const size_t order = 2 * (size_t)G.nlat + 4 * G.M + 4 * SYN_SPLIT * (size_t)G.nlat + (size_t)sle_pch(G) * G.nlat;
+  return std::max({(size_t)G.nphi, (size_t)4 * G.M, order}) * sizeof(double);
 }
 
 static void launch_inner_loop(vg_handle* h) {
@@ -701,6 +735,7 @@ static void launch_inner_loop(vg_handle* h) {
   A.F = h->d_F.p;
   A.Gp = h->d_sle_Gp.p;
   A.Fc = h->d_sle_Fc.p;
+  A.pch = sle_pch(G);
   A.Sraw = h->d_Sraw.p;
   A.rowpart = h->d_rowpart.p;
   A.sc = h->d_sc_.p;

@@ -55,6 +55,19 @@ __device__ __forceinline__ bool mbar_wait_or_abort_ns(uint64_t* bar, uint32_t pa
   }
 }
 
+// the same with a short sleep between polls, for waiters that are not on the
+// critical path (they leave the issue slots to the warps that are)
+__device__ __forceinline__ bool mbar_wait_sleep_ns(uint64_t* bar, uint32_t parity, volatile int* abort_flag,
+                                                   unsigned long long wait_ns) {
+  if (mbar_try(bar, parity)) return true;
+  const unsigned long long t0 = gtimer();
+  while (true) {
+    __nanosleep(100);
+    if (mbar_try(bar, parity)) return true;
+    if (*abort_flag || gtimer() - t0 > wait_ns) return false;
+  }
+}
+
 __device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
   asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(saddr(bar)) : "memory");
 }
