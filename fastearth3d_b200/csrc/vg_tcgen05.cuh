@@ -33,12 +33,30 @@ __device__ __forceinline__ bool mbar_try(uint64_t* bar, uint32_t parity) {
   return ok != 0;
 }
 
-// bounded wait: false after wait_ns of global time
+// one potentially blocking test: the hardware suspends the thread until the
+// phase completes or about `hint_ns` have passed (no polling loop, so waiting
+// threads take no issue slots and read no timer meanwhile)
+__device__ __forceinline__ bool mbar_try_hint(uint64_t* bar, uint32_t parity, uint32_t hint_ns) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
+      "selp.b32 %0, 1, 0, p;\n\t}\n"
+      : "=r"(ok)
+      : "r"(saddr(bar)), "r"(parity), "r"(hint_ns)
+      : "memory");
+  return ok != 0;
+}
+
+constexpr uint32_t WAIT_HINT_NS = 20000;  // one suspended test: at most ~20 us
+
+// bounded wait: false after wait_ns of global time (the timer is read once
+// per suspended test)
 __device__ __forceinline__ bool mbar_wait_ns(uint64_t* bar, uint32_t parity, unsigned long long wait_ns) {
   if (mbar_try(bar, parity)) return true;
   const unsigned long long t0 = gtimer();
   while (true) {
-    if (mbar_try(bar, parity)) return true;
+    if (mbar_try_hint(bar, parity, WAIT_HINT_NS)) return true;
     if (gtimer() - t0 > wait_ns) return false;
   }
 }
@@ -50,22 +68,15 @@ __device__ __forceinline__ bool mbar_wait_or_abort_ns(uint64_t* bar, uint32_t pa
   if (mbar_try(bar, parity)) return true;
   const unsigned long long t0 = gtimer();
   while (true) {
-    if (mbar_try(bar, parity)) return true;
+    if (mbar_try_hint(bar, parity, WAIT_HINT_NS)) return true;
     if (*abort_flag || gtimer() - t0 > wait_ns) return false;
   }
 }
 
-// the same with a short sleep between polls, for waiters that are not on the
-// critical path (they leave the issue slots to the warps that are)
+// the same for waiters that are not on the critical path
 __device__ __forceinline__ bool mbar_wait_sleep_ns(uint64_t* bar, uint32_t parity, volatile int* abort_flag,
                                                    unsigned long long wait_ns) {
-  if (mbar_try(bar, parity)) return true;
-  const unsigned long long t0 = gtimer();
-  while (true) {
-    __nanosleep(100);
-    if (mbar_try(bar, parity)) return true;
-    if (*abort_flag || gtimer() - t0 > wait_ns) return false;
-  }
+  return mbar_wait_or_abort_ns(bar, parity, abort_flag, wait_ns);
 }
 
 __device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
