@@ -148,6 +148,31 @@ __device__ __forceinline__ double block_sum(double v, double* red) {
   __syncthreads();
   return r;
 }
+// The same reductions through warp shuffles (two block barriers instead of
+// one per tree level); blockDim a multiple of 32, every thread gets the
+// result; the warp partials are added in warp order.
+__device__ __forceinline__ double block_sum_w(double v, double* red) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  const int nw = blockDim.x >> 5;
+  __syncthreads();  // the previous call's readers are done with red
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
+  __syncthreads();
+  double r = red[0];
+  for (int w = 1; w < nw; ++w) r += red[w];
+  return r;
+}
+__device__ __forceinline__ double block_max_w(double v, double* red) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v = nanmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+  const int nw = blockDim.x >> 5;
+  __syncthreads();
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
+  __syncthreads();
+  double r = red[0];
+  for (int w = 1; w < nw; ++w) r = nanmax(r, red[w]);
+  return r;
+}
 __device__ __forceinline__ double block_max(double v, double* red) {
   red[threadIdx.x] = v;
   __syncthreads();

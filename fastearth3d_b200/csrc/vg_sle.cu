@@ -82,8 +82,17 @@ __device__ double integrate_rows(const double* row, const double* w, int nlat, d
     __syncthreads();
     for (int j = threadIdx.x; j < n; j += blockDim.x) term[j] = w[j0 + j] * row[j0 + j] * dlon;
     __syncthreads();
-    if (threadIdx.x == 0)
-      for (int j = 0; j < n; ++j) total += term[j];
+    if (threadIdx.x == 0) {  // in row order; the loads run ahead of the dependent adds
+      int j = 0;
+      for (; j + 8 <= n; j += 8) {
+        double t[8];
+#pragma unroll
+        for (int q = 0; q < 8; ++q) t[q] = term[j + q];
+#pragma unroll
+        for (int q = 0; q < 8; ++q) total += t[q];
+      }
+      for (; j < n; ++j) total += term[j];
+    }
   }
   return total;
 }
@@ -454,8 +463,8 @@ __global__ void __launch_bounds__(512) k_sle_inner(InnerArgs A) {
           A.rsl[p] = rn;
           smax = nanmax(smax, fabs(A.C[p] * rn));
         }
-        dmax = block_max(dmax, red);
-        smax = block_max(smax, red);
+        dmax = block_max_w(dmax, red);
+        smax = block_max_w(smax, red);
         if (tid == 0) {
           A.rowpart[RP_DMAX * nlat + j] = dmax;
           A.rowpart[RP_SMAX * nlat + j] = smax;
@@ -584,8 +593,8 @@ __global__ void __launch_bounds__(512) k_sle_inner(InnerArgs A) {
         dmax = nanmax(dmax, A.rowpart[RP_DMAX * nlat + j]);
         smax = nanmax(smax, A.rowpart[RP_SMAX * nlat + j]);
       }
-      dmax = block_max(dmax, red);
-      smax = block_max(smax, red);
+      dmax = block_max_w(dmax, red);
+      smax = block_max_w(smax, red);
       if (tid == 0) {
         s_stop = (dmax <= A.tol * fmax(smax, TINY)) ? 1 : 0;
         if (blockIdx.x == 0) {
@@ -664,7 +673,7 @@ __global__ void __launch_bounds__(512) k_sle_inner(InnerArgs A) {
         }
         __syncthreads();
       }
-      acc = block_sum(acc, red);
+      acc = block_sum_w(acc, red);
       if (tid == 0) A.rowpart[RP_CS * nlat + j] = acc;
       sle_row_load(A, j, sm, part, 1, A.F);  // Fa of this iteration (the next one's F, less dphi Fc)
     }
