@@ -210,8 +210,10 @@ struct vg_handle {
       d_C, d_C0, d_C_next, d_dig, d_wcorr, d_Sraw, d_zbed, d_tmp;
   vg::DArr<double> d_F;        // Fourier coefficients (2 * M * nlat * batch)
   vg::DArr<double> d_Gs;       // Legendre sums (2 * M * nlat * batch)
-  vg::DArr<double> d_sle_Gp;   // Legendre synthesis of u and N per (latitude, order) [j][m][4]
-  vg::DArr<double> d_sle_Fc;   // longitude analysis of rho_w C per row [m][j][2]
+  vg::DArr<int2> d_sle_chunk;  // fused sea-level loop: Legendre synthesis chunks (m, first l - m)
+  vg::DArr<int> d_sle_cbeg;    // first chunk of each order
+  vg::DArr<double> d_sle_Gp;   // partial Legendre sums (chunk, nlat, 4)
+  int sle_nchunk = 0;
   vg::DArr<double> d_sigma, d_ulm, d_nlm;  // spectra (2*nlm)
   vg::DArr<double> d_rowpart;  // per-row partial sums (8 * nlat)
   vg::DArr<unsigned int> d_gbar;  // grid barrier of the fused inner loop: count, generation, error

@@ -42,6 +42,8 @@
 #include <cmath>
 #include <cstdint>
 
+#include <cuda.h>  // CUtensorMap (encoded through the runtime's driver entry point)
+
 #include "vg_device.cuh"
 #include "vg_internal.cuh"
 #include "vg_tcgen05.cuh"
@@ -75,16 +77,19 @@ struct ImgInfo {
 };
 
 struct Args {
+  // the stage's A rows as a tensor map: one TMA tile load fetches a K chunk of
+  // a row tile (synthesis: X by lm pairs; inverse: S by order pairs; forward:
+  // Gs; analysis: S by latitude)
+  CUtensorMap tmap;
   int L, nlat, nh, nphi, half, F, NC, NCOL, nk, ne3d;
   int nts, nti, ntf, nta;
   const int* kbeg;
-  const double* X;     // [(nk + 1)][4][NC]      gathered memory + 2 mu strain
+  const int* mbeg;     // first lm of each order
+  const double* X;     // [lm][4][NC]            gathered memory + 2 mu strain, lm order
   double* S;           // [M][nlat][6][NC]       synthesis products, later the analysis inputs
   double* Gs;          // [nlat][2][half][NCOL]  even / odd longitude combinations of -M dt g
   double* dy;          // [(nk + 1)][6][NC]      analysis outputs
-  const double* rate;  // [nlat][nphi][ne3d]     mu / eta_eff
-  double dt;
-  int trap;
+  const double* nmdt;  // [nlat][nphi][ne3d]     -M dt (trapezoidal: -M dt / (1 + M dt / 2)) of the sub-step
   const double* invsin;
   const unsigned char* img;
   const double* bscale;
@@ -112,12 +117,30 @@ __device__ __forceinline__ void mma_i8(uint32_t tmem_d, uint64_t da, uint64_t db
       : "memory");
 }
 
+// TMA tile load of a 4-D box (no multicast, this GPU's memory), completing on
+// the mbarrier's transaction count; coordinates innermost first
+__device__ __forceinline__ void tma_load_4d(void* dst, const CUtensorMap* tm, int c0, int c1, int c2, int c3,
+                                            uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, %5}], "
+      "[%6];" ::"r"(saddr(dst)),
+      "l"(tm), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(saddr(bar))
+      : "memory");
+}
+
 // 32 lanes x 8 consecutive 32-bit columns (no wait: the caller waits once)
 __device__ __forceinline__ void tmem_ld8_nowait(uint32_t taddr, int* v) {
   asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
                : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7])
                : "r"(taddr));
 }
+// 32 lanes x 4 consecutive 32-bit columns (no wait)
+__device__ __forceinline__ void tmem_ld4_nowait(uint32_t taddr, int* v) {
+  asm volatile("tcgen05.ld.sync.aligned.32x32b.x4.b32 {%0,%1,%2,%3}, [%4];"
+               : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3])
+               : "r"(taddr));
+}
+
 __device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
 
 // exponent E with |x| < 2^E for every x of a group whose maximum is `bits`
@@ -169,15 +192,20 @@ __device__ __forceinline__ double i2d_exact(int a) {
   return __hiloint2double(0x43380000, a ^ (int)0x80000000) - 6755401588539392.0;
 }
 
-// five int32 levels (weights 256^-lambda) -> FP64, before the row and column scales
+// exact uint32 -> FP64 (the same bit assembly, unsigned)
+__device__ __forceinline__ double u2d_exact(unsigned a) {
+  return __hiloint2double(0x43300000, (int)a) - 4503599627370496.0;
+}
+
+// five int32 levels (weights 256^-lambda) -> sum_s a_s 2^(32 - 8 s) times the
+// power-of-two scale `sc`: the sum is formed exactly in 64-bit integers and
+// rounded once (hi 2^32 + lo, both halves exact in FP64, one FMA)
 __device__ __forceinline__ double combine_levels(const int* a0, const int* a1, const int* a2, const int* a3,
-                                                 const int* a4, int i) {
-  constexpr double W = 0.00390625;  // 2^-8
-  double v = i2d_exact(a4[i]);
-  v = fma(v, W, i2d_exact(a3[i]));
-  v = fma(v, W, i2d_exact(a2[i]));
-  v = fma(v, W, i2d_exact(a1[i]));
-  return fma(v, W, i2d_exact(a0[i]));
+                                                 const int* a4, int i, double sc) {
+  const long long t = ((long long)a0[i] << 32) + ((long long)a1[i] << 24) + ((long long)a2[i] << 16) +
+                      ((long long)a3[i] << 8) + (long long)a4[i];
+  const double hi = i2d_exact((int)(t >> 32)), lo = u2d_exact((unsigned)t);
+  return fma(hi, sc * 4294967296.0, lo * sc);
 }
 
 __device__ __forceinline__ int slot_row(const int* kbeg, int l, int m, int nk) {
@@ -186,9 +214,8 @@ __device__ __forceinline__ int slot_row(const int* kbeg, int l, int m, int nk) {
 
 // table sign under theta -> pi - theta (times (-1)^(l+m)): P, G even; dP, H odd
 __device__ __forceinline__ double table_sigma(int p) { return (p == 1 || p == 5) ? -1.0 : 1.0; }
-__device__ __forceinline__ int table_of(int p) {
-  const int t[6] = {0, 1, 0, 0, 2, 3};
-  return t[p];
+__device__ __forceinline__ int table_of(int p) {  // p -> table: 0 1 0 0 2 3
+  return p == 1 ? 1 : (p == 4 ? 2 : (p == 5 ? 3 : 0));
 }
 __device__ __forceinline__ int chan_of(int p) { return (p == 0) ? 0 : (p <= 2 ? 1 : (p == 3 ? 2 : 3)); }
 
@@ -311,7 +338,7 @@ __device__ __forceinline__ int valid_k(const Args& A, const Cta& c, int sub, int
 }
 
 template <int STAGE>
-__global__ void __launch_bounds__(p::NTHR, 1) k_ozp_stage(Args A) {
+__global__ void __launch_bounds__(p::NTHR, 1) k_ozp_stage(const __grid_constant__ Args A) {
   using R = p::Ring<STAGE>;
   extern __shared__ unsigned char smraw[];
   unsigned char* sm = (unsigned char*)(((uintptr_t)smraw + 1023) & ~(uintptr_t)1023);
@@ -375,7 +402,6 @@ __global__ void __launch_bounds__(p::NTHR, 1) k_ozp_stage(Args A) {
       const Cta c = tile_info<STAGE>(A, t);
       const int nch0 = c.sub[0].kpad / KC, nch = nch0 + c.sub[1].kpad / KC;
       if (nch == 0 || c.rows <= 0) continue;
-      const size_t rbytes = (size_t)c.rows * 8;
       for (int ch = 0; ch < nch; ++ch, ++gc) {
         const int sub = ch < nch0 ? 0 : 1, kc = sub ? ch - nch0 : ch;
         const int rs = gc % R::NRAW, bs = gc % R::NB;
@@ -396,63 +422,36 @@ __global__ void __launch_bounds__(p::NTHR, 1) k_ozp_stage(Args A) {
           stop = true;
           break;
         }
-        // raw copies of this chunk: K value q of the chunk at lane q
-        const int kv = valid_k<STAGE>(A, c, sub, kc);
-        unsigned char* rdst = raw + (size_t)rs * R::RAW_BYTES;
-        const void* src[2] = {nullptr, nullptr};
-        void* dst[2] = {nullptr, nullptr};
-        uint32_t nb[2] = {0, 0};
-        if (STAGE == ST_SYNTH) {
-          if (lane < kv) {
-            const int l = c.batch_m + sub + 2 * (kc * KC + lane);
-            const int slot = slot_row(A.kbeg, l, c.batch_m, A.nk);
-            src[0] = A.X + ((size_t)slot * 4 + chan_of(c.p)) * A.NC + c.row0;
-            dst[0] = rdst + (size_t)lane * TM * 8;
-            nb[0] = (uint32_t)rbytes;
-          }
-        } else if (STAGE == ST_INV) {  // one copy per order: (re, im) of every row
-          if (2 * lane < kv) {
-            const int m = (sub ? 1 : 2) + 2 * (kc * (KC / 2) + lane);
-            src[0] = A.S + ((size_t)m * A.nlat + c.j) * 6 * A.NC + 2 * (size_t)c.row0;
-            dst[0] = rdst + (size_t)lane * TM * 16;
-            nb[0] = (uint32_t)(2 * rbytes);
-          }
-        } else if (STAGE == ST_FWD) {
-          if (lane < kv) {
-            const int i = kc * KC + lane;
-            src[0] = A.Gs + ((size_t)c.j * 2 * A.half + (size_t)sub * A.half + i) * A.NCOL + c.row0;
-            dst[0] = rdst + (size_t)lane * TM * 8;
-            nb[0] = (uint32_t)rbytes;
-          }
-        } else {
-          if (lane < kv) {
-            const int j = kc * KC + lane, jm = A.nlat - 1 - j;
-            const double* base = A.S + (size_t)c.batch_m * A.nlat * 6 * A.NC + (size_t)c.p * A.NC + c.row0;
-            src[0] = base + (size_t)j * 6 * A.NC;
-            dst[0] = rdst + (size_t)lane * TM * 8;
-            nb[0] = (uint32_t)rbytes;
-            if (jm != j) {
-              src[1] = base + (size_t)jm * 6 * A.NC;
-              dst[1] = rdst + (size_t)(KC + lane) * TM * 8;
-              nb[1] = (uint32_t)rbytes;
-            }
-          }
-        }
-        uint32_t total = nb[0] + nb[1];
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) total += __shfl_xor_sync(0xffffffffu, total, o);
+        // raw rows of this chunk: one TMA tile load of the row tile's 32 K
+        // (the analysis: a second one for the mirrored latitudes, stored in
+        // reverse order); rows past the tile's end and K past the tensor read
+        // as zeros, K past the valid range is zeroed by the converters
         if (lane == 0) {
-          if (total > 0)
-            mbar_expect_tx(&raw_full[rs], total);
-          else
-            mbar_arrive(&raw_full[rs]);  // nothing to copy: the converters write zeros
+          unsigned char* rdst = raw + (size_t)rs * R::RAW_BYTES;
+          if (STAGE == ST_SYNTH) {
+            // lm = mbeg[m] + sub + 2 kk = 2 q + par
+            const int lm0 = __ldg(&A.mbeg[c.batch_m]) + sub + 2 * kc * KC;
+            mbar_expect_tx(&raw_full[rs], (uint32_t)R::RAW_BYTES);
+            tma_load_4d(rdst, &A.tmap, c.row0, chan_of(c.p), lm0 & 1, lm0 >> 1, &raw_full[rs]);
+          } else if (STAGE == ST_INV) {
+            // m = 2 mq + mpar: even orders from 2 (sub 0), odd orders from 1 (sub 1)
+            const int mq0 = (sub ? 0 : 1) + kc * (KC / 2);
+            mbar_expect_tx(&raw_full[rs], (uint32_t)R::RAW_BYTES);
+            tma_load_4d(rdst, &A.tmap, 2 * c.row0, c.j, sub, mq0, &raw_full[rs]);
+          } else if (STAGE == ST_FWD) {
+            mbar_expect_tx(&raw_full[rs], (uint32_t)R::RAW_BYTES);
+            tma_load_4d(rdst, &A.tmap, c.row0, kc * KC, 2 * c.j + sub, 0, &raw_full[rs]);
+          } else {
+            const int j0 = kc * KC, jm0 = A.nlat - KC - j0;  // mirrors of j0 .. j0 + 31, ascending
+            mbar_expect_tx(&raw_full[rs], (uint32_t)R::RAW_BYTES);
+            tma_load_4d(rdst, &A.tmap, c.row0, c.p, j0, c.batch_m, &raw_full[rs]);
+            tma_load_4d(rdst + (size_t)KC * TM * 8, &A.tmap, c.row0, c.p, jm0, c.batch_m, &raw_full[rs]);
+          }
         }
         __syncwarp();
-        if (nb[0]) bulk_g2s(dst[0], src[0], nb[0], &raw_full[rs]);
-        if (nb[1]) bulk_g2s(dst[1], src[1], nb[1], &raw_full[rs]);
         // the chunk's B digit image
         if (lane == 0) {
-          const ImgInfo& I = c.sub[sub];
+          const ImgInfo I = sub ? c.sub[1] : c.sub[0];
           const uint32_t bytes = (uint32_t)(NDIG * 2 * I.npad * 16);
           mbar_expect_tx(&b_full[bs], bytes);
           bulk_g2s(bdig + (size_t)bs * B_BYTES_MAX, A.img + I.off + (size_t)kc * bytes, bytes, &b_full[bs]);
@@ -498,7 +497,7 @@ __global__ void __launch_bounds__(p::NTHR, 1) k_ozp_stage(Args A) {
             break;
           }
           tc_fence_after();
-          const ImgInfo& I = c.sub[sub];
+          const ImgInfo I = sub ? c.sub[1] : c.sub[0];
           const unsigned char* Ab = adig + (size_t)ds * A_BYTES;
           const unsigned char* Bb = bdig + (size_t)bs * B_BYTES_MAX;
           const uint32_t idesc = idesc_i8(TM, I.npad);
@@ -539,7 +538,7 @@ __global__ void __launch_bounds__(p::NTHR, 1) k_ozp_stage(Args A) {
       const double rs = pow2(FIX_BITS - e);
       const double is_j = (STAGE == ST_INV) ? A.invsin[c.j] : 0.0;
       const int prow = (STAGE == ST_INV) ? row / A.F : 0;
-      double side[2] = {0.0, 0.0};
+      double side0 = 0.0, side1 = 0.0;  // the tile's side sums (sub 0, sub 1)
       bool ok = true;
       for (int ch = 0; ch < nch; ++ch, ++gc) {
         const int sub = ch < nch0 ? 0 : 1, kc = sub ? ch - nch0 : ch;
@@ -555,39 +554,55 @@ __global__ void __launch_bounds__(p::NTHR, 1) k_ozp_stage(Args A) {
         const int kv = valid_k<STAGE>(A, c, sub, kc);
         const double* rv = (const double*)(raw + (size_t)rsi * R::RAW_BYTES);
         double v[16];
+        double sacc = 0.0;  // this chunk's part of the side sum
+        if (STAGE == ST_INV) {
+          // K pairs (re, im) of one order: one 16-byte load per pair
 #pragma unroll
-        for (int q = 0; q < 16; ++q) {
-          const int k = 16 * g + q;
-          double x = 0.0;
-          if (live && k < kv) {
-            if (STAGE == ST_INV) {
-              const int mo = k >> 1, ri = k & 1;
-              const double re = rv[(size_t)mo * TM * 2 + 2 * lr], im = rv[(size_t)mo * TM * 2 + 2 * lr + 1];
-              double tre = re, tim = im;
+          for (int q = 0; q < 16; q += 2) {
+            const int k = 16 * g + q, mo = k >> 1;
+            double tre = 0.0, tim = 0.0;
+            if (live && k < kv) {
+              const double2 z = *reinterpret_cast<const double2*>(rv + (size_t)mo * TM * 2 + 2 * lr);
+              tre = z.x;
+              tim = z.y;
               if (prow == 2) {  // i (m / sin theta) z
                 const int m = (sub ? 1 : 2) + 2 * (kc * (KC / 2) + mo);
                 const double a = (double)m * is_j;
-                tre = -a * im;
-                tim = a * re;
+                tre = -a * z.y;
+                tim = a * z.x;
               } else if (prow == 5) {  // i z
-                tre = -im;
-                tim = re;
+                tre = -z.y;
+                tim = z.x;
               }
-              x = ri ? tim : tre;
-              if (!ri) side[sub] += 2.0 * tre;
-            } else if (STAGE == ST_ANA) {
-              const int j = kc * KC + k, jm = A.nlat - 1 - j;
-              const double r0 = rv[(size_t)k * TM + lr];
-              const double r1 = (jm != j) ? rv[(size_t)(KC + k) * TM + lr] : 0.0;
-              const double sg = table_sigma(c.p) * (sub ? -1.0 : 1.0);
-              x = r0 + sg * r1;
-            } else {
-              x = rv[(size_t)k * TM + lr];
-              if (STAGE == ST_FWD && sub == 0) side[0] += x;
+              sacc += 2.0 * tre;
             }
+            v[q] = tre;
+            v[q + 1] = (k + 1 < kv && live) ? tim : 0.0;
           }
-          v[q] = x;
+        } else {
+          const double sg = (STAGE == ST_ANA) ? table_sigma(c.p) * (sub ? -1.0 : 1.0) : 0.0;
+#pragma unroll
+          for (int q = 0; q < 16; ++q) {
+            const int k = 16 * g + q;
+            double x = 0.0;
+            if (live && k < kv) {
+              if (STAGE == ST_ANA) {
+                const int j = kc * KC + k, jm = A.nlat - 1 - j;
+                const double r0 = rv[(size_t)k * TM + lr];
+                const double r1 = (jm != j) ? rv[(size_t)(KC + KC - 1 - k) * TM + lr] : 0.0;
+                x = r0 + sg * r1;
+              } else {
+                x = rv[(size_t)k * TM + lr];
+                if (STAGE == ST_FWD) sacc += x;
+              }
+            }
+            v[q] = x;
+          }
         }
+        if (sub)
+          side1 += sacc;
+        else
+          side0 += sacc;
         uint4 pl[NDIG];
         to_digits16(v, rs, pl);
         unsigned char* Ab = adig + (size_t)ds * A_BYTES + ((size_t)g * TM + lr) * 16;
@@ -606,8 +621,8 @@ __global__ void __launch_bounds__(p::NTHR, 1) k_ozp_stage(Args A) {
           *abort_flag = 1;
           break;
         }
-        rsum[((tb * 2 + 0) * 2 + g) * TM + lr] = side[0];
-        rsum[((tb * 2 + 1) * 2 + g) * TM + lr] = side[1];
+        rsum[((tb * 2 + 0) * 2 + g) * TM + lr] = side0;
+        rsum[((tb * 2 + 1) * 2 + g) * TM + lr] = side1;
         mbar_arrive(&sum_full[tb]);
       }
       ++gt;
@@ -648,7 +663,7 @@ __global__ void __launch_bounds__(p::NTHR, 1) k_ozp_stage(Args A) {
       const bool live = r < c.rows;
       const bool has0 = nch0 > 0, has1 = nch1 > 0;
       const int npad_max = max(has0 ? c.sub[0].npad : 0, has1 ? c.sub[1].npad : 0);
-      const double rf = pow2((live ? row_exp<STAGE>(A, c, row) : 0) - (FIX_BITS - 32));
+      const double rf = pow2((live ? row_exp<STAGE>(A, c, row) : 0) - FIX_BITS);
       auto load_block = [&](int sub, int cb, double* out) {
         const bool hs = sub ? has1 : has0;
         const int np = sub ? c.sub[1].npad : c.sub[0].npad;
@@ -663,29 +678,60 @@ __global__ void __launch_bounds__(p::NTHR, 1) k_ozp_stage(Args A) {
         tmem_wait_ld();
         const double* cs = A.bscale + (sub ? c.sub[1].sc : c.sub[0].sc) + cb;
 #pragma unroll
-        for (int i = 0; i < 8; ++i) out[i] = combine_levels(a[0], a[1], a[2], a[3], a[4], i) * rf * __ldg(&cs[i]);
+        for (int i = 0; i < 8; ++i) out[i] = combine_levels(a[0], a[1], a[2], a[3], a[4], i, rf) * __ldg(&cs[i]);
+      };
+      // both parities of 4 columns: the tensor-memory loads are issued first,
+      // the stage's scattered global loads (rates, 1 / sin) run in their
+      // shadow, then one wait
+      auto issue_pair4 = [&](int cb, int (*a)[NLEV][4]) {
+#pragma unroll
+        for (int sb = 0; sb < 2; ++sb)
+#pragma unroll
+          for (int lv = 0; lv < NLEV; ++lv) tmem_ld4_nowait(tbase + (uint32_t)((lv * 2 + sb) * TN + cb), a[sb][lv]);
+      };
+      // the combined levels times the column scales (a few values every thread
+      // reads: cache hits); columns past a parity's image read as zero
+      auto combine_pair4 = [&](int cb, int (*a)[NLEV][4], double* ev, double* od) {
+        const bool ok0 = has0 && cb < c.sub[0].npad, ok1 = has1 && cb < c.sub[1].npad;
+        const double* cs0 = A.bscale + c.sub[0].sc + cb;
+        const double* cs1 = A.bscale + c.sub[1].sc + cb;
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+          ev[i] = ok0 ? combine_levels(a[0][0], a[0][1], a[0][2], a[0][3], a[0][4], i, rf) * __ldg(&cs0[i]) : 0.0;
+          od[i] = ok1 ? combine_levels(a[1][0], a[1][1], a[1][2], a[1][3], a[1][4], i, rf) * __ldg(&cs1[i]) : 0.0;
+        }
       };
       if (STAGE == ST_SYNTH) {
         const int m = c.batch_m, pp = c.p;
         const double sg = table_sigma(pp);
         double gmax = 0.0;
-        for (int cb = half_id * 8; cb < npad_max; cb += 16) {
-          double ev[8], od[8];
-          load_block(0, cb, ev);
-          load_block(1, cb, od);
+        for (int cb = half_id * 4; cb < npad_max; cb += 8) {
+          int a[2][NLEV][4];
+          double wn[4], ws[4];
+          issue_pair4(cb, a);
+          tmem_wait_ld();
           if (!live) continue;
 #pragma unroll
-          for (int i = 0; i < 8; ++i) {
+          for (int i = 0; i < 4; ++i) {  // the weights of the group maximum (m / sin theta for p = 2)
+            const int j = min(c.nt * TN + cb + i, A.nh - 1), jm = A.nlat - 1 - j;
+            wn[i] = (pp == 2) ? (double)m * __ldg(&A.invsin[j]) : 1.0;
+            ws[i] = (pp == 2) ? (double)m * __ldg(&A.invsin[jm]) : 1.0;
+          }
+          double ev[4], od[4];
+          combine_pair4(cb, a, ev, od);
+#pragma unroll
+          for (int i = 0; i < 4; ++i) {
             const int j = c.nt * TN + cb + i;
-            if (j >= A.nh) break;
-            const int jm = A.nlat - 1 - j;
-            const double vn = ev[i] + od[i];
-            A.S[(((size_t)m * A.nlat + j) * 6 + pp) * A.NC + row] = vn;
-            gmax = fmax(gmax, fabs(vn) * ((pp == 2) ? (double)m * A.invsin[j] : 1.0));
-            if (jm != j) {
-              const double vs = sg * (ev[i] - od[i]);
-              A.S[(((size_t)m * A.nlat + jm) * 6 + pp) * A.NC + row] = vs;
-              gmax = fmax(gmax, fabs(vs) * ((pp == 2) ? (double)m * A.invsin[jm] : 1.0));
+            if (j < A.nh) {
+              const int jm = A.nlat - 1 - j;
+              const double vn = ev[i] + od[i];
+              A.S[(((size_t)m * A.nlat + j) * 6 + pp) * A.NC + row] = vn;
+              gmax = fmax(gmax, fabs(vn) * wn[i]);
+              if (jm != j) {
+                const double vs = sg * (ev[i] - od[i]);
+                A.S[(((size_t)m * A.nlat + jm) * 6 + pp) * A.NC + row] = vs;
+                gmax = fmax(gmax, fabs(vs) * ws[i]);
+              }
             }
           }
         }
@@ -698,34 +744,39 @@ __global__ void __launch_bounds__(p::NTHR, 1) k_ozp_stage(Args A) {
               *reinterpret_cast<const double2*>(A.S + (((size_t)0 * A.nlat + c.j) * 6 + pp) * A.NC + 2 * f);
           c0 = (pp == 5) ? -z.y : z.x;
         }
-        const double* rate_j = A.rate + (size_t)c.j * A.nphi * A.ne3d + e3;
+        const double* nm_j = A.nmdt + (size_t)c.j * A.nphi * A.ne3d + e3;
         double* gs = A.Gs + (size_t)c.j * 2 * A.half * A.NCOL + row;
         double* gd = gs + (size_t)A.half * A.NCOL;
         double gmax = 0.0;
-        auto emit = [&](int i, double ev, double od) {
-          double m1 = __ldg(&rate_j[(size_t)i * A.ne3d]) * A.dt;
-          double m2 = __ldg(&rate_j[(size_t)(i + A.half) * A.ne3d]) * A.dt;
-          if (A.trap) {
-            m1 = m1 / (1.0 + 0.5 * m1);
-            m2 = m2 / (1.0 + 0.5 * m2);
-          }
-          const double g1 = -m1 * (ev + od), g2 = -m2 * (ev - od);
+        // longitudes i and i + half from the even / odd parts, times -M dt there
+        auto emit = [&](int i, double ev, double od, double n1, double n2) {
+          const double g1 = n1 * (ev + od);
+          const double g2 = n2 * (ev - od);
           const double sv = g1 + g2, dv = g1 - g2;
           gs[(size_t)i * A.NCOL] = sv;
           gd[(size_t)i * A.NCOL] = dv;
           gmax = fmax(gmax, fmax(fabs(sv), fabs(dv)));
         };
-        if (live && c.nt == 0 && half_id == 0) emit(0, c0 + sev, sod);
-        for (int cb = half_id * 8; cb < npad_max; cb += 16) {
-          double ev[8], od[8];
-          load_block(0, cb, ev);
-          load_block(1, cb, od);
+        if (live && c.nt == 0 && half_id == 0)
+          emit(0, c0 + sev, sod, __ldg(&nm_j[0]), __ldg(&nm_j[(size_t)A.half * A.ne3d]));
+        for (int cb = half_id * 4; cb < npad_max; cb += 8) {
+          int a[2][NLEV][4];
+          double n1[4], n2[4];
+          issue_pair4(cb, a);
+          tmem_wait_ld();
           if (!live) continue;
 #pragma unroll
-          for (int i = 0; i < 8; ++i) {
+          for (int i = 0; i < 4; ++i) {
+            const int ii = min(1 + c.nt * TN + cb + i, A.half - 1);
+            n1[i] = __ldg(&nm_j[(size_t)ii * A.ne3d]);
+            n2[i] = __ldg(&nm_j[(size_t)(ii + A.half) * A.ne3d]);
+          }
+          double ev[4], od[4];
+          combine_pair4(cb, a, ev, od);
+#pragma unroll
+          for (int i = 0; i < 4; ++i) {
             const int ii = 1 + c.nt * TN + cb + i;
-            if (ii >= A.half) break;
-            emit(ii, ev[i] + c0, od[i]);
+            if (ii < A.half) emit(ii, ev[i] + c0, od[i], n1[i], n2[i]);
           }
         }
         if (live) atomic_max_bits(&A.gG[row], gmax);
@@ -745,7 +796,7 @@ __global__ void __launch_bounds__(p::NTHR, 1) k_ozp_stage(Args A) {
         }
         for (int sub = 0; sub < 2; ++sub) {
           if (!(sub ? has1 : has0)) continue;
-          const int npad = c.sub[sub].npad, nval = c.sub[sub].nvalid;
+          const int npad = sub ? c.sub[1].npad : c.sub[0].npad, nval = sub ? c.sub[1].nvalid : c.sub[0].nvalid;
           for (int cb = half_id * 8; cb < npad; cb += 16) {
             double v[8];
             load_block(sub, cb, v);
@@ -771,7 +822,7 @@ __global__ void __launch_bounds__(p::NTHR, 1) k_ozp_stage(Args A) {
         const int m = c.batch_m, pp = c.p;
         for (int sub = 0; sub < 2; ++sub) {
           if (!(sub ? has1 : has0)) continue;
-          const int npad = c.sub[sub].npad;
+          const int npad = sub ? c.sub[1].npad : c.sub[0].npad;
           for (int cb = half_id * 8; cb < npad; cb += 16) {
             double v[8];
             load_block(sub, cb, v);
@@ -794,6 +845,17 @@ __global__ void __launch_bounds__(p::NTHR, 1) k_ozp_stage(Args A) {
   tc_fence_before();
   __syncthreads();
   if (warp == p::W_PROD) tmem_dealloc(tmem, TMEM_COLS);
+}
+
+// -M dt of every (latitude, longitude, element) for one sub-step (trapezoidal:
+// the implicit half-step factor M dt / (1 + M dt / 2)), negated
+__global__ void k_oz_rate_factors(const double* __restrict__ rate, double* __restrict__ nm, size_t n, double dt,
+                                  int trap) {
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    double m = rate[i] * dt;
+    if (trap) m = m / (1.0 + 0.5 * m);
+    nm[i] = -m;
+  }
 }
 
 // ------------------------------------------------------------------ operand images
@@ -873,9 +935,14 @@ int round_up_oz(int x, int m) { return (x + m - 1) / m * m; }
 
 struct OzPlan {
   oz::Args a;
+  CUtensorMap tm[4];  // per stage: synthesis, inverse, forward, analysis
   int ntile_rows_nc, ntile_rows_col;
   int nsm = 148, tiles[4] = {0, 0, 0, 0};  // persistent grids: min(tiles, SMs) CTAs
   DArr<double> S, Gs, rate, bscale;
+  // -M dt factors of the inverse stage for the last two (dt, trapezoidal) keys
+  DArr<double> nmdt[2];
+  double nm_dt[2] = {0.0, 0.0};
+  int nm_trap[2] = {-1, -1}, nm_next = 0;
   DArr<unsigned char> img;
   DArr<unsigned long long> gmax;  // gX, gS, gG, gA back to back
   size_t gmax_n = 0;
@@ -883,6 +950,35 @@ struct OzPlan {
 };
 
 static void oz_release(void* p) { delete static_cast<OzPlan*>(p); }
+
+// cuTensorMapEncodeTiled through the runtime's driver entry point (no link
+// against the driver library)
+using EncodeTiledFn = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                   const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                   CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+static EncodeTiledFn tensor_map_encoder() {
+  static EncodeTiledFn fn = nullptr;
+  if (!fn) {
+    void* f = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    VG_CUDA(cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &f, cudaEnableDefault, &q));
+    if (!f || q != cudaDriverEntryPointSuccess) throw Error("vg_enable_visc3d: cuTensorMapEncodeTiled unavailable");
+    fn = reinterpret_cast<EncodeTiledFn>(f);
+  }
+  return fn;
+}
+
+// a 4-D FP64 tensor map (dims innermost first, strides in bytes of dims 1-3)
+// with a 4-D box, no swizzle, zeros outside the tensor
+static void encode_map(CUtensorMap* tm, const double* base, const cuuint64_t dims[4], const cuuint64_t strides[3],
+                       const cuuint32_t box[4]) {
+  const cuuint32_t es[4] = {1, 1, 1, 1};
+  const CUresult r = tensor_map_encoder()(tm, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 4, const_cast<double*>(base), dims,
+                                          strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                                          CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                                          CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) throw Error("vg_enable_visc3d: tensor map encoding failed");
+}
 
 void visc3d_oz_enable(vg_handle* h) {
   const Grid& G = h->grid;
@@ -983,19 +1079,24 @@ void visc3d_oz_enable(vg_handle* h) {
         for (int i = 0; i < nphi; ++i) rt[((size_t)j * nphi + i) * h->ne3d + e] = r3[((size_t)e * nlat + j) * nphi + i];
     P->rate.upload(rt, s);
   }
-  // FP64 work buffers: the gather writes the FP64 path's X, the scatter reads dy
-  h->d_X.alloc((size_t)(h->nk + 1) * 4 * NC);
+  // FP64 work buffers: the gather writes X in lm order (an even number of
+  // rows, the l = 0 row zero), the scatter reads dy; S has an even number of
+  // order slabs (the inverse stage reads orders in pairs)
+  const int nlm2 = (G.nlm + 1) / 2 * 2, M2 = (G.M + 1) / 2 * 2;
+  h->d_X.alloc((size_t)nlm2 * 4 * NC);
   h->d_dy.alloc((size_t)(h->nk + 1) * 6 * NC);
-  P->S.alloc((size_t)G.M * nlat * 6 * NC);
+  P->S.alloc((size_t)M2 * nlat * 6 * NC);
   P->Gs.alloc((size_t)nlat * 2 * half * NCOL);
   P->gmax_n = (size_t)4 * NC + 6 * F + 6 * F + 6 * NC;
   P->gmax.alloc(P->gmax_n);
   a.kbeg = h->d_kbeg.p;
+  a.mbeg = G.d_mbeg.p;
   a.X = h->d_X.p;
   a.S = P->S.p;
   a.Gs = P->Gs.p;
   a.dy = h->d_dy.p;
-  a.rate = P->rate.p;
+  P->nmdt[0].alloc(P->rate.n);
+  P->nmdt[1].alloc(P->rate.n);
   a.invsin = G.d_invsin.p;
   a.img = P->img.p;
   a.bscale = P->bscale.p;
@@ -1013,6 +1114,30 @@ void visc3d_oz_enable(vg_handle* h) {
   int dev = 0;
   VG_CUDA(cudaGetDevice(&dev));
   VG_CUDA(cudaDeviceGetAttribute(&P->nsm, cudaDevAttrMultiProcessorCount, dev));
+  {  // the stages' tensor maps (boxes of one row tile by one K chunk, 32 KB)
+    const cuuint64_t B = sizeof(double);
+    const cuuint32_t TMr = oz::TM, KCc = oz::KC;
+    // synthesis: X[lm][chan][n], lm = 2 q + par
+    const cuuint64_t dx[4] = {(cuuint64_t)NC, 4, 2, (cuuint64_t)nlm2 / 2};
+    const cuuint64_t sx[3] = {NC * B, 4 * NC * B, 8 * NC * B};
+    const cuuint32_t bx[4] = {TMr, 1, 1, KCc};
+    encode_map(&P->tm[0], h->d_X.p, dx, sx, bx);
+    // inverse: S[m][j][(p, f, ri)], m = 2 mq + mpar
+    const cuuint64_t di[4] = {(cuuint64_t)6 * NC, (cuuint64_t)nlat, 2, (cuuint64_t)M2 / 2};
+    const cuuint64_t si[3] = {6 * NC * B, (cuuint64_t)nlat * 6 * NC * B, 2 * (cuuint64_t)nlat * 6 * NC * B};
+    const cuuint32_t bi[4] = {2 * TMr, 1, 1, KCc / 2};
+    encode_map(&P->tm[1], P->S.p, di, si, bi);
+    // forward: Gs[(j, sub)][i][row]
+    const cuuint64_t dg[4] = {(cuuint64_t)NCOL, (cuuint64_t)half, 2 * (cuuint64_t)nlat, 1};
+    const cuuint64_t sg[3] = {NCOL * B, (cuuint64_t)half * NCOL * B, 2 * (cuuint64_t)nlat * half * NCOL * B};
+    const cuuint32_t bg[4] = {TMr, KCc, 1, 1};
+    encode_map(&P->tm[2], P->Gs.p, dg, sg, bg);
+    // analysis: S[m][j][p][n]
+    const cuuint64_t da[4] = {(cuuint64_t)NC, 6, (cuuint64_t)nlat, (cuuint64_t)G.M};
+    const cuuint64_t sa[3] = {NC * B, 6 * NC * B, (cuuint64_t)nlat * 6 * NC * B};
+    const cuuint32_t ba[4] = {TMr, 1, KCc, 1};
+    encode_map(&P->tm[3], P->S.p, da, sa, ba);
+  }
   P->tiles[0] = P->ntile_rows_nc * a.nts * G.M * 6;
   P->tiles[1] = P->ntile_rows_col * a.nti * nlat;
   P->tiles[2] = P->ntile_rows_col * a.ntf * nlat;
@@ -1033,12 +1158,29 @@ void visc3d_oz_run(vg_handle* h, double dt, bool trap) {
   OzPlan* P = static_cast<OzPlan*>(h->tc_plan);
   cudaStream_t s = h->stream;
   oz::Args a = P->a;
-  a.dt = dt;
-  a.trap = trap ? 1 : 0;
+  {  // the sub-step's -M dt factors (recomputed when neither cached key matches)
+    int slot = -1;
+    for (int q = 0; q < 2; ++q)
+      if (P->nm_trap[q] == (trap ? 1 : 0) && P->nm_dt[q] == dt) slot = q;
+    if (slot < 0) {
+      slot = P->nm_next;
+      P->nm_next ^= 1;
+      const size_t n = P->rate.n;
+      oz::k_oz_rate_factors<<<(int)std::min<size_t>((n + 255) / 256, 4 * (size_t)P->nsm), 256, 0, s>>>(
+          P->rate.p, P->nmdt[slot].p, n, dt, trap ? 1 : 0);
+      ++h->n_launch;
+      VG_CUDA(cudaGetLastError());
+      P->nm_dt[slot] = dt;
+      P->nm_trap[slot] = trap ? 1 : 0;
+    }
+    a.nmdt = P->nmdt[slot].p;
+  }
   a.wait_ns = h->wait_ns;
+  int stage = 0;
   auto launch = [&](auto kernel, int phase, const oz::ImgInfo* info, int tiles, size_t smem) {
     PhaseScope ps(h, phase);
     a.info = info;
+    a.tmap = P->tm[stage++];
     kernel<<<std::max(1, std::min(tiles, P->nsm)), oz::p::NTHR, smem, s>>>(a);
     ++h->n_launch;
     VG_CUDA(cudaGetLastError());

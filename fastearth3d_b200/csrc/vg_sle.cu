@@ -285,35 +285,31 @@ __global__ void k_bsl_rows(int nphi, const double* __restrict__ hi, const double
 // ------------------------------------------------------------------ fused inner loop
 // The inner load fixed point of sle_solve (src/vilma_sle.f90:280-340) as one
 // cooperative persistent kernel: one CTA per SM, the convergence test on the
-// device, so no host round trip per iteration. Iteration `it` computes the
-// load spectrum from the load of rsl_{it-1}, the response, Sraw_it, the
-// mass-conserving dphi_it and rsl_it = Sraw_it + dphi_it. Two grid barriers
-// an iteration:
-//   R  per row (the CTA that owns it): longitude synthesis of u and N,
-//      Sraw = N - u (+ s_rot), the row sum of C Sraw, and the longitude
-//      analysis Fa of rho_ice dig + rho_w C Sraw + wcorr          | barrier
-//   X  per row: dphi of the previous iteration (every CTA, rows summed in
-//      order by one thread, so all CTAs agree), its rsl update and row
-//      maxima; per order m (the CTA that owns it, so the analysis and the
-//      synthesis of an order need no barrier between them): the load's
-//      Fourier coefficients F = Fa + dphi Fc (linearity: Fc is the
-//      analysis of rho_w C, fixed during the loop), Legendre analysis,
-//      apply (u, N = gains sigma + drift), Legendre synthesis of u and N on
-//      every latitude                                             | barrier
-//   convergence of the previous iteration (every CTA from the row maxima,
-//   the same decision everywhere), before R
-// The first iteration's F is the analysis of the entering load (prologue).
+// device, so no host round trip per iteration. Four grid barriers an
+// iteration:
+//   L  total load of each row and its longitude analysis (the CTA that owns
+//      the row; for the next iteration it runs right after U, on the rows the
+//      CTA has just updated)
+//   A  Legendre analysis + apply, warp per lm                 | barrier
+//   S  Legendre synthesis of u and N, thread per (b, m, j)    | barrier
+//   R  longitude synthesis, Sraw = N - u (+ s_rot), row sums  | barrier
+//   U  mass-conserving dphi (every CTA, rows summed in order by one thread,
+//      so all CTAs agree), rsl update, row maxima, then L     | barrier
+//   convergence (every CTA from the row maxima, the same decision everywhere)
 // The longitude transforms split the half periods (phi + pi flips odd m) and
 // spread each output's sum over several threads, so no thread runs a loop of
 // more than about nphi / 6 terms.
+constexpr int SLE_LCH = 16;  // degrees per Legendre synthesis chunk
+
 struct InnerArgs {
   int nphi, nlat, M, nlm, nk, lmax, n_inner;
   double tol, dlon, g;
   const double *dig, *C, *wcorr, *cs, *sn, *plm, *wts, *gu, *gn, *drift, *srot;
   const int *lm_m, *lm_l, *lm2k, *mbeg;
-  double *rsl, *F, *Gp, *Sraw, *rowpart;
-  double* Fc;  // longitude analysis of rho_w C per row [m][j][2] (fixed during the loop)
-  int pch;     // Legendre rows of one order staged in shared memory at a time
+  const int2* chunk;  // Legendre synthesis chunks: (m, first l - m), at most SLE_LCH degrees each
+  const int* cbeg;    // first chunk of each order (M + 1)
+  int nchunk;
+  double *rsl, *F, *sigma, *ulm, *Gp, *Sraw, *rowpart;
   SleScalars* sc;
   unsigned int* bar;  // count, generation, error
   unsigned long long wait_ns;  // bound on a grid barrier's wait (the handle's wait limit, 2 s by default)
@@ -362,21 +358,13 @@ __device__ bool grid_barrier(unsigned int* bar, unsigned int& gen, unsigned long
 // L for row j: the total surface load and its longitude analysis into F
 // (F_m = 2 pi / nphi sum_i f_i e^{-i m phi_i}; even m read f_i + f_{i+half},
 // odd m f_i - f_{i+half}); tpm threads per order, partial sums in part[2][nthr]
-// field 0: the total load rho_ice dig + rho_w C rsl + wcorr; 1: the same with
-// Sraw in place of rsl; 2: rho_w C. Its analysis goes to out[m][j][2].
-__device__ __forceinline__ void sle_row_load(const InnerArgs& A, int j, double* sm, double* part, int field,
-                                             double* out) {
+__device__ __forceinline__ void sle_row_load(const InnerArgs& A, int j, double* sm, double* part) {
   const int tid = threadIdx.x, nthr = blockDim.x, nphi = A.nphi, M = A.M, half = nphi / 2;
   const double sc_f = 2.0 * PI / (double)nphi;
   __syncthreads();
   for (int i = tid; i < nphi; i += nthr) {
     const size_t p = (size_t)j * nphi + i;
-    if (field == 0)
-      sm[i] = RHO_ICE * A.dig[p] + RHO_WATER * (A.C[p] * A.rsl[p]) + A.wcorr[p];
-    else if (field == 1)
-      sm[i] = RHO_ICE * A.dig[p] + RHO_WATER * (A.C[p] * A.Sraw[p]) + A.wcorr[p];
-    else
-      sm[i] = RHO_WATER * A.C[p];
+    sm[i] = RHO_ICE * A.dig[p] + RHO_WATER * (A.C[p] * A.rsl[p]) + A.wcorr[p];
   }
   __syncthreads();
   const int tpm = max(1, min(8, nthr / M));
@@ -405,8 +393,8 @@ __device__ __forceinline__ void sle_row_load(const InnerArgs& A, int j, double* 
         r += part[tid + c];
         s2 += part[nthr + tid + c];
       }
-      out[((size_t)m * A.nlat + j) * 2] = r * sc_f;
-      out[((size_t)m * A.nlat + j) * 2 + 1] = s2 * sc_f;
+      A.F[((size_t)m * A.nlat + j) * 2] = r * sc_f;
+      A.F[((size_t)m * A.nlat + j) * 2 + 1] = s2 * sc_f;
     }
     __syncthreads();
   }
@@ -417,209 +405,140 @@ __device__ __forceinline__ void bar_fail(const InnerArgs& A) {
   if (threadIdx.x == 0) A.sc->bar_error = 1;
 }
 
-// Legendre parts of one order per pass: analysis over all latitudes, apply,
-// synthesis on every latitude (SYN_SPLIT threads per latitude over the degrees)
-constexpr int SYN_SPLIT = 4;
-
 __global__ void __launch_bounds__(512) k_sle_inner(InnerArgs A) {
-  extern __shared__ double sm[];  // see sle_inner_smem
+  extern __shared__ double sm[];  // max(nphi, 4 M + 4 nchunk) doubles
   __shared__ double red[512];
   __shared__ double part[4 * 512];
   __shared__ double s_val;
   __shared__ int s_stop;
   const int tid = threadIdx.x, nthr = blockDim.x;
   const int lane = tid & 31, wid = tid >> 5, nw = nthr >> 5;
-  const int nphi = A.nphi, nlat = A.nlat, M = A.M, half = nphi / 2;
+  const int nphi = A.nphi, nlat = A.nlat, M = A.M, nlm = A.nlm, half = nphi / 2;
   unsigned int gen = 0;
   if (!(A.sc->C_int > 0.0)) return;  // no ocean: nothing to redistribute (every CTA reads the same value)
-  // prologue: F of the first iteration (the entering load) and Fc, per owned row
-  for (int j = blockIdx.x; j < nlat; j += gridDim.x) {
-    sle_row_load(A, j, sm, part, 0, A.F);
-    sle_row_load(A, j, sm, part, 2, A.Fc);
-  }
+  // L of the first iteration
+  for (int j = blockIdx.x; j < nlat; j += gridDim.x) sle_row_load(A, j, sm, part);
   if (!grid_barrier(A.bar, gen, A.wait_ns)) return bar_fail(A);
-  int final_it = A.n_inner;
-  for (int it = 1;; ++it) {
-    // ---- X: rows of the previous iteration, then the orders of this one
-    double dphi = 0.0;
-    if (it >= 2) {
-      const double Cs = integrate_rows(A.rowpart + RP_CS * nlat, A.wts, nlat, A.dlon);
-      if (tid == 0) {
-        const double d = (A.sc->ice_int - Cs + A.sc->zeta_int) / A.sc->C_int;
-        s_val = d;
-        if (blockIdx.x == 0) {
-          A.sc->Cs_int = Cs;
-          A.sc->dphi = d;
+  for (int it = 1; it <= A.n_inner; ++it) {
+    // A. Legendre analysis (warp per lm, four lm of a warp at once) and the
+    //    affine response u, N
+    for (int lm0 = blockIdx.x * nw + wid; lm0 < nlm; lm0 += 4 * gridDim.x * nw) {
+      constexpr int U4 = 4;
+      double re[U4], im[U4];
+      int lmv[U4];
+      const double* Fm[U4];
+      const double* P[U4];
+#pragma unroll
+      for (int u = 0; u < U4; ++u) {
+        lmv[u] = lm0 + u * gridDim.x * nw;
+        const int lmc = min(lmv[u], nlm - 1);  // past the end: a valid row, result unused
+        Fm[u] = A.F + ((size_t)A.lm_m[lmc] * nlat) * 2;
+        P[u] = A.plm + (size_t)lmc * nlat;
+        re[u] = 0.0;
+        im[u] = 0.0;
+      }
+      for (int j = lane; j < nlat; j += 32) {
+        const double w = A.wts[j];
+#pragma unroll
+        for (int u = 0; u < U4; ++u) {
+          const double wp = w * P[u][j];
+          re[u] += wp * Fm[u][2 * j];
+          im[u] += wp * Fm[u][2 * j + 1];
         }
       }
-      __syncthreads();
-      dphi = s_val;
-      for (int j = blockIdx.x; j < nlat; j += gridDim.x) {
-        double dmax = 0.0, smax = 0.0;
-        for (int i = tid; i < nphi; i += nthr) {
-          const size_t p = (size_t)j * nphi + i;
-          const double rn = A.Sraw[p] + dphi;
-          dmax = nanmax(dmax, fabs(A.C[p] * (rn - A.rsl[p])));
-          A.rsl[p] = rn;
-          smax = nanmax(smax, fabs(A.C[p] * rn));
+#pragma unroll
+      for (int u = 0; u < U4; ++u)
+        for (int o = 16; o > 0; o >>= 1) {
+          re[u] += __shfl_down_sync(0xffffffffu, re[u], o);
+          im[u] += __shfl_down_sync(0xffffffffu, im[u], o);
         }
-        dmax = block_max_w(dmax, red);
-        smax = block_max_w(smax, red);
-        if (tid == 0) {
-          A.rowpart[RP_DMAX * nlat + j] = dmax;
-          A.rowpart[RP_SMAX * nlat + j] = smax;
-        }
+      // lanes 0..3 write lm u (the sums are in lane 0; broadcast them)
+#pragma unroll
+      for (int u = 0; u < U4; ++u) {
+        re[u] = __shfl_sync(0xffffffffu, re[u], 0);
+        im[u] = __shfl_sync(0xffffffffu, im[u], 0);
       }
-    }
-    if (it <= A.n_inner) {
-      double* fw = sm;                         // w_j F_m(j): [nlat][2]
-      double* ul = fw + 2 * nlat;              // u, N of the order: [l - m][4]
-      double* gp = ul + 4 * M;                 // synthesis partials: [SYN_SPLIT][nlat][4]
-      double* ps = gp + 4 * SYN_SPLIT * nlat;  // the order's Legendre rows, staged: [A.pch][nlat]
-      for (int m = blockIdx.x; m < M; m += gridDim.x) {
-        const int nl = A.lmax - m + 1, lm0 = A.mbeg[m];
-        const double* pm = A.plm + (size_t)lm0 * nlat;  // the order's rows are contiguous
-        __syncthreads();
-        for (int j = tid; j < nlat; j += nthr) {
-          const size_t o = ((size_t)m * nlat + j) * 2;
-          double re = A.F[o], im = A.F[o + 1];
-          if (it >= 2) {
-            re += dphi * A.Fc[o];
-            im += dphi * A.Fc[o + 1];
+      if (lane < U4) {
+        double r = re[0], i2 = im[0];
+#pragma unroll
+        for (int u = 1; u < U4; ++u)
+          if (lane == u) {
+            r = re[u];
+            i2 = im[u];
           }
-          fw[2 * j] = A.wts[j] * re;
-          fw[2 * j + 1] = A.wts[j] * im;
-        }
-        // analysis + apply, the rows staged chunk by chunk: a warp per degree
-        int staged = -1;  // first degree of the staged chunk
-        for (int c0 = 0; c0 < nl; c0 += A.pch) {
-          const int n = min(A.pch, nl - c0);
-          __syncthreads();
-          for (int t = tid; t < n * nlat; t += nthr) ps[t] = pm[(size_t)c0 * nlat + t];
-          staged = c0;
-          __syncthreads();
-          for (int q = c0 + wid; q < c0 + n; q += nw) {
-            const int lm = lm0 + q, l = m + q;
-            const double* P = ps + (size_t)(q - c0) * nlat;
-            double re = 0.0, im = 0.0;
-            for (int j = lane; j < nlat; j += 32) {
-              const double pj = P[j];
-              re += pj * fw[2 * j];
-              im += pj * fw[2 * j + 1];
-            }
-            for (int o = 16; o > 0; o >>= 1) {
-              re += __shfl_down_sync(0xffffffffu, re, o);
-              im += __shfl_down_sync(0xffffffffu, im, o);
-            }
-            if (lane == 0) {
-              double* u4 = ul + 4 * q;
-              if (l == 0) {
-                u4[0] = A.gu[0] * re;
-                u4[1] = A.gu[0] * im;
-                u4[2] = A.gn[0] * re;
-                u4[3] = A.gn[0] * im;
-              } else {
-                const int k = A.lm2k[lm];
-                u4[0] = A.gu[l] * re + A.drift[(size_t)0 * A.nk + k];
-                u4[1] = A.gu[l] * im + A.drift[(size_t)1 * A.nk + k];
-                u4[2] = A.gn[l] * re - A.drift[(size_t)2 * A.nk + k] / A.g;
-                u4[3] = A.gn[l] * im - A.drift[(size_t)3 * A.nk + k] / A.g;
-              }
-            }
+        const int lm = lmv[lane];
+        if (lm < nlm) {
+          A.sigma[2 * lm] = r;
+          A.sigma[2 * lm + 1] = i2;
+          const int l = A.lm_l[lm];
+          double* uu = A.ulm;
+          double* n = A.ulm + 2 * (size_t)nlm;
+          if (l == 0) {
+            uu[2 * lm] = A.gu[0] * r;
+            uu[2 * lm + 1] = A.gu[0] * i2;
+            n[2 * lm] = A.gn[0] * r;
+            n[2 * lm + 1] = A.gn[0] * i2;
+          } else {
+            const int k = A.lm2k[lm];
+            uu[2 * lm] = A.gu[l] * r + A.drift[(size_t)0 * A.nk + k];
+            uu[2 * lm + 1] = A.gu[l] * i2 + A.drift[(size_t)1 * A.nk + k];
+            n[2 * lm] = A.gn[l] * r - A.drift[(size_t)2 * A.nk + k] / A.g;
+            n[2 * lm + 1] = A.gn[l] * i2 - A.drift[(size_t)3 * A.nk + k] / A.g;
           }
-        }
-        // synthesis of u and N on every latitude: SYN_SPLIT threads per
-        // latitude, each over its run of degrees, chunk by chunk (the last
-        // staged chunk is still in place)
-        const int per = (nl + SYN_SPLIT - 1) / SYN_SPLIT;
-        for (int base = 0; base < SYN_SPLIT * nlat; base += nthr) {
-          const int t = base + tid;
-          const bool act = t < SYN_SPLIT * nlat;
-          const int j = t % nlat, sp = t / nlat;
-          const int q0 = sp * per, q1 = min(nl, q0 + per);
-          double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
-          for (int c0 = (nl - 1) / A.pch * A.pch;; c0 -= A.pch) {  // staged chunk first, then back to 0
-            const int n = min(A.pch, nl - c0);
-            if (c0 != staged) {
-              __syncthreads();
-              for (int u = tid; u < n * nlat; u += nthr) ps[u] = pm[(size_t)c0 * nlat + u];
-              staged = c0;
-            }
-            __syncthreads();
-            if (act) {
-              const int qa = max(q0, c0), qb = min(q1, c0 + n);
-              for (int q = qa; q < qb; ++q) {
-                const double pq = ps[(size_t)(q - c0) * nlat + j];
-                const double* u4 = ul + 4 * q;
-                a0 += u4[0] * pq;
-                a1 += u4[1] * pq;
-                a2 += u4[2] * pq;
-                a3 += u4[3] * pq;
-              }
-            }
-            if (c0 == 0) break;
-          }
-          if (act) {
-            double* o = gp + ((size_t)sp * nlat + j) * 4;
-            o[0] = a0;
-            o[1] = a1;
-            o[2] = a2;
-            o[3] = a3;
-          }
-        }
-        __syncthreads();
-        for (int j = tid; j < nlat; j += nthr) {
-          double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
-          for (int sp = 0; sp < SYN_SPLIT; ++sp) {  // the parts summed in order
-            const double* o = gp + ((size_t)sp * nlat + j) * 4;
-            a0 += o[0];
-            a1 += o[1];
-            a2 += o[2];
-            a3 += o[3];
-          }
-          double* g = A.Gp + ((size_t)j * M + m) * 4;
-          g[0] = a0;
-          g[1] = a1;
-          g[2] = a2;
-          g[3] = a3;
         }
       }
     }
     if (!grid_barrier(A.bar, gen, A.wait_ns)) return bar_fail(A);
-    // ---- convergence of the previous iteration (src/vilma_sle.f90:330-338)
-    if (it >= 2) {
-      double dmax = 0.0, smax = 0.0;
-      for (int j = tid; j < nlat; j += nthr) {
-        dmax = nanmax(dmax, A.rowpart[RP_DMAX * nlat + j]);
-        smax = nanmax(smax, A.rowpart[RP_SMAX * nlat + j]);
+    // S. Legendre synthesis of u and N in chunks of at most SLE_LCH degrees: a
+    //    thread per (chunk, j), partial sums Gp[j][chunk][u re, u im, N re, N im]
+    //    (one 32-byte sector per thread; a row's partials contiguous)
+    for (int t = blockIdx.x * nthr + tid; t < A.nchunk * nlat; t += gridDim.x * nthr) {
+      const int c = t / nlat, j = t % nlat;
+      const int2 ch = A.chunk[c];
+      const int n = min(SLE_LCH, A.lmax - ch.x + 1 - ch.y);
+      const int lm = A.mbeg[ch.x] + ch.y;
+      const double* pc = A.plm + (size_t)lm * nlat + j;
+      const double* qu = A.ulm + 2 * (size_t)lm;
+      const double* qn = A.ulm + 2 * ((size_t)nlm + lm);
+      double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
+#pragma unroll 4
+      for (int q = 0; q < n; ++q) {
+        const double p = pc[(size_t)q * nlat];
+        a0 += qu[2 * q] * p;
+        a1 += qu[2 * q + 1] * p;
+        a2 += qn[2 * q] * p;
+        a3 += qn[2 * q + 1] * p;
       }
-      dmax = block_max_w(dmax, red);
-      smax = block_max_w(smax, red);
-      if (tid == 0) {
-        s_stop = (dmax <= A.tol * fmax(smax, TINY)) ? 1 : 0;
-        if (blockIdx.x == 0) {
-          A.sc->dmax = dmax;
-          A.sc->smax = smax;
-        }
-      }
-      __syncthreads();
-      if (s_stop) {
-        final_it = it - 1;
-        break;
-      }
+      double* o = A.Gp + ((size_t)j * A.nchunk + c) * 4;
+      o[0] = a0;
+      o[1] = a1;
+      o[2] = a2;
+      o[3] = a3;
     }
-    if (it > A.n_inner) break;  // not converged within n_inner iterations
-    // ---- R: rows of this iteration
+    if (!grid_barrier(A.bar, gen, A.wait_ns)) return bar_fail(A);
+    // R. longitude synthesis (g(i) = G_0 + 2 sum_m Re G_m e^{i m phi_i}, even and
+    //    odd m apart, tpi threads per longitude pair (i, i + half)),
+    //    Sraw = N - u (+ s_rot), row sums of C Sraw
     for (int j = blockIdx.x; j < nlat; j += gridDim.x) {
       double* Gu = sm;
       double* Gn = sm + 2 * M;
+      double* gp = sm + 4 * M;  // the row's partial sums, staged
       __syncthreads();
-      for (int m = tid; m < M; m += nthr) {
-        const double* g = A.Gp + ((size_t)j * M + m) * 4;
-        Gu[2 * m] = g[0];
-        Gu[2 * m + 1] = g[1];
-        Gn[2 * m] = g[2];
-        Gn[2 * m + 1] = g[3];
+      for (int t = tid; t < 4 * A.nchunk; t += nthr) gp[t] = A.Gp[(size_t)j * A.nchunk * 4 + t];
+      __syncthreads();
+      for (int m = tid; m < M; m += nthr) {  // the order's chunks summed in order
+        double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
+        for (int c = A.cbeg[m]; c < A.cbeg[m + 1]; ++c) {
+          const double* o = gp + 4 * c;
+          a0 += o[0];
+          a1 += o[1];
+          a2 += o[2];
+          a3 += o[3];
+        }
+        Gu[2 * m] = a0;
+        Gu[2 * m + 1] = a1;
+        Gn[2 * m] = a2;
+        Gn[2 * m + 1] = a3;
       }
       __syncthreads();
       const int tpi = max(1, min(8, nthr / half));
@@ -673,29 +592,72 @@ __global__ void __launch_bounds__(512) k_sle_inner(InnerArgs A) {
         }
         __syncthreads();
       }
-      acc = block_sum_w(acc, red);
+      acc = block_sum(acc, red);
       if (tid == 0) A.rowpart[RP_CS * nlat + j] = acc;
-      sle_row_load(A, j, sm, part, 1, A.F);  // Fa of this iteration (the next one's F, less dphi Fc)
     }
     if (!grid_barrier(A.bar, gen, A.wait_ns)) return bar_fail(A);
+    // U. dphi in every CTA (rows in order by thread 0: the same value everywhere)
+    {
+      const double Cs = integrate_rows(A.rowpart + RP_CS * nlat, A.wts, nlat, A.dlon);
+      if (tid == 0) {
+        const double dphi = (A.sc->ice_int - Cs + A.sc->zeta_int) / A.sc->C_int;
+        s_val = dphi;
+        if (blockIdx.x == 0) {
+          A.sc->Cs_int = Cs;
+          A.sc->dphi = dphi;
+        }
+      }
+      __syncthreads();
+    }
+    const double dphi = s_val;
+    for (int j = blockIdx.x; j < nlat; j += gridDim.x) {
+      double dmax = 0.0, smax = 0.0;
+      for (int i = tid; i < nphi; i += nthr) {
+        const size_t p = (size_t)j * nphi + i;
+        const double rn = A.Sraw[p] + dphi;
+        dmax = nanmax(dmax, fabs(A.C[p] * (rn - A.rsl[p])));
+        A.rsl[p] = rn;
+        smax = nanmax(smax, fabs(A.C[p] * rn));
+      }
+      dmax = block_max_w(dmax, red);
+      smax = block_max_w(smax, red);
+      if (tid == 0) {
+        A.rowpart[RP_DMAX * nlat + j] = dmax;
+        A.rowpart[RP_SMAX * nlat + j] = smax;
+      }
+      sle_row_load(A, j, sm, part);  // L of the next iteration (unused if this one converged)
+    }
+    if (!grid_barrier(A.bar, gen, A.wait_ns)) return bar_fail(A);
+    // convergence (src/vilma_sle.f90:330-338), the same decision in every CTA
+    {
+      double dmax = 0.0, smax = 0.0;
+      for (int j = tid; j < nlat; j += nthr) {
+        dmax = nanmax(dmax, A.rowpart[RP_DMAX * nlat + j]);
+        smax = nanmax(smax, A.rowpart[RP_SMAX * nlat + j]);
+      }
+      dmax = block_max_w(dmax, red);
+      smax = block_max_w(smax, red);
+      if (tid == 0) {
+        s_stop = (dmax <= A.tol * fmax(smax, TINY)) ? 1 : 0;
+        if (blockIdx.x == 0) {
+          A.sc->dmax = dmax;
+          A.sc->smax = smax;
+          A.sc->n_inner = it;
+        }
+      }
+      __syncthreads();
+      if (s_stop) break;
+    }
   }
-  if (blockIdx.x == 0 && tid == 0) A.sc->n_inner = final_it;
 }
 
-// Legendre rows of an order staged at a time: all of them up to lmax 128 on
-// a 129-row grid, in chunks beyond
-constexpr size_t SLE_PSTAGE_BYTES = 140 * 1024;
-static int sle_pch(const Grid& G) {
-  return std::max(1, std::min(G.lmax + 1, (int)(SLE_PSTAGE_BYTES / ((size_t)G.nlat * sizeof(double)))));
-}
-
-// dynamic shared memory of the fused loop: the row (nphi), the row's Fourier
-// sums of u and N (4 M), or an order's weighted F, its u and N, the
-// synthesis partials and its staged Legendre rows
+// dynamic shared memory of the fused loop: the row (nphi) or, in R, the
+// Fourier sums (4 M) and the row's staged partial sums (4 chunks)
 static size_t sle_inner_smem(const vg_handle* h) {
   const Grid& G = h->grid;
-  const size_t order = 2 * (size_t)G.nlat + 4 * G.M + 4 * SYN_SPLIT * (size_t)G.nlat + (size_t)sle_pch(G) * G.nlat;
-  return std::max({(size_t)G.nphi, (size_t)4 * G.M, order}) * sizeof(double);
+  int nch = 0;
+  for (int m = 0; m < G.M; ++m) nch += (G.lmax - m + SLE_LCH) / SLE_LCH;
+  return (size_t)std::max(G.nphi, 4 * G.M + 4 * nch) * sizeof(double);
 }
 
 static void launch_inner_loop(vg_handle* h) {
@@ -711,8 +673,17 @@ static void launch_inner_loop(vg_handle* h) {
     if (per_sm < 1) throw Error("sle_solve: the fused inner loop does not fit on an SM");
     h->sle_grid = h->p.sle_ctas > 0 ? std::min(h->p.sle_ctas, nsm * per_sm) : nsm;
     h->d_gbar.alloc(4);
-    h->d_sle_Gp.alloc((size_t)G.M * G.nlat * 4);
-    h->d_sle_Fc.alloc((size_t)2 * G.M * G.nlat);
+    std::vector<int2> chunk;
+    std::vector<int> cbeg(G.M + 1);
+    for (int m = 0; m < G.M; ++m) {
+      cbeg[m] = (int)chunk.size();
+      for (int l0 = 0; l0 < G.lmax - m + 1; l0 += SLE_LCH) chunk.push_back(make_int2(m, l0));
+    }
+    cbeg[G.M] = (int)chunk.size();
+    h->sle_nchunk = (int)chunk.size();
+    h->d_sle_chunk.upload(chunk, s);
+    h->d_sle_cbeg.upload(cbeg, s);
+    h->d_sle_Gp.alloc((size_t)h->sle_nchunk * G.nlat * 4);
   }
   InnerArgs A;
   A.nphi = G.nphi;
@@ -742,9 +713,12 @@ static void launch_inner_loop(vg_handle* h) {
   A.mbeg = G.d_mbeg.p;
   A.rsl = h->d_rsl.p;
   A.F = h->d_F.p;
+  A.sigma = h->d_sigma.p;
+  A.ulm = h->d_ulm.p;
+  A.chunk = h->d_sle_chunk.p;
+  A.cbeg = h->d_sle_cbeg.p;
+  A.nchunk = h->sle_nchunk;
   A.Gp = h->d_sle_Gp.p;
-  A.Fc = h->d_sle_Fc.p;
-  A.pch = sle_pch(G);
   A.Sraw = h->d_Sraw.p;
   A.rowpart = h->d_rowpart.p;
   A.sc = h->d_sc_.p;

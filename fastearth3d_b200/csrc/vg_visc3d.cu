@@ -94,6 +94,7 @@ struct V3Args {
   // exact tensor-core path: the largest |X| per (channel, column) over all
   // slots, as double bits (the synthesis operand rows' scale groups)
   unsigned long long* gmax = nullptr;
+  int lm_rows = 0;  // exact tensor-core path: X rows in lm order (k2lm) instead of slot order
 };
 
 // one thread per (slot k, 3-D element): strain of both histories, 24 values,
@@ -159,7 +160,8 @@ __global__ void __launch_bounds__(256) k_v3_gather(V3Args A, T* __restrict__ X) 
   }
   for (int t = threadIdx.y * V3_TK + threadIdx.x; t < nkb * NC * w; t += V3_TK * V3_TE) {
     const int kl = t / (NC * w), rem = t % (NC * w), lam = rem / w, c = rem % w;
-    X[((size_t)(k0 + kl) * NC + lam) * A.ncf + 6 * e0 + c] = tile[((size_t)lam * V3_TC + c) * V3_TP + kl];
+    const size_t xr = A.lm_rows ? (size_t)A.k2lm[k0 + kl] : (size_t)(k0 + kl);
+    X[(xr * NC + lam) * A.ncf + 6 * e0 + c] = tile[((size_t)lam * V3_TC + c) * V3_TP + kl];
   }
 }
 
@@ -828,6 +830,7 @@ void visc3d_advance(vg_handle* h, const double* d_sigma, double dt, const double
     {
       PhaseScope pg(h, VG_PH_V3_GATHER);
       A.gmax = visc3d_oz_gather_max(h);  // zeroes every scale group of the advance
+      A.lm_rows = 1;
       k_v3_gather<double, 4><<<gg, dim3(32, 8), v3_gather_smem<double>(), s>>>(A, h->d_X.p);
       ++h->n_launch;
       VG_CUDA(cudaGetLastError());
