@@ -227,10 +227,11 @@ struct Cta {
 // ------------------------------------------------------------------ persistent kernel
 //
 // One CTA per SM loops over the stage's tiles (static stride). Warp roles:
-//   warp 0       producer: lanes 0 .. 31 issue the TMA bulk copies of the raw
-//                FP64 A rows of each K chunk into the raw ring (one copy per K
-//                value: a run of the tile's rows, contiguous in every layout)
-//                and lane 0 the B digit image of the chunk into the B ring
+//   warp 0       producer (lane 0): one TMA tile load per K chunk of the raw
+//                FP64 A rows (the tile's rows x 32 K, through the stage's
+//                tensor map; the analysis: two, the mirrored latitudes in the
+//                second) into the raw ring, and the chunk's B digit image
+//                into the B ring
 //   warp 1       MMA issuer (lane 0): 15 digit-pair MMAs per chunk into the
 //                five level accumulators, commits that free the chunk's A
 //                and B stages, and one that hands the tile's accumulators to
@@ -254,8 +255,8 @@ template <int STAGE>
 struct Ring {
   static constexpr int NRAW = STAGE == ST_ANA ? 2 : 3;  // raw FP64 chunks in flight
   static constexpr int RAW_BYTES = (STAGE == ST_ANA ? 2 : 1) * KC * TM * 8;
-  static constexpr int NDST = STAGE == ST_ANA ? 2 : 3;  // A digit stages
-  static constexpr int NB = STAGE == ST_ANA ? 4 : 6;    // B digit stages
+  static constexpr int NDST = STAGE == ST_ANA ? 2 : 4;  // A digit stages
+  static constexpr int NB = 4;                          // B digit stages
   static constexpr size_t RAW_OFF = 0;
   static constexpr size_t A_OFF = RAW_OFF + (size_t)NRAW * RAW_BYTES;
   static constexpr size_t B_OFF = A_OFF + (size_t)NDST * A_BYTES;

@@ -17,6 +17,14 @@ __device__ __forceinline__ unsigned long long gtimer() {
   return t;
 }
 
+// Clock of the wait limits: the SM cycle counter (a register read; the global
+// timer is a slower read). A limit of `ns` nanoseconds is 2 ns cycles, at least
+// `ns` of wall time at any SM clock up to 2 GHz.
+__device__ __forceinline__ long long wclock() { return clock64(); }
+__device__ __forceinline__ long long wait_cycles(unsigned long long ns) {
+  return (long long)(ns > (1ull << 61) ? (1ull << 62) : 2 * ns);
+}
+
 __device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
   asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(saddr(bar)), "r"(count) : "memory");
 }
@@ -50,14 +58,14 @@ __device__ __forceinline__ bool mbar_try_hint(uint64_t* bar, uint32_t parity, ui
 
 constexpr uint32_t WAIT_HINT_NS = 20000;  // one suspended test: at most ~20 us
 
-// bounded wait: false after wait_ns of global time (the timer is read once
-// per suspended test)
+// bounded wait: false after about wait_ns (the clock is read once per
+// suspended test)
 __device__ __forceinline__ bool mbar_wait_ns(uint64_t* bar, uint32_t parity, unsigned long long wait_ns) {
   if (mbar_try(bar, parity)) return true;
-  const unsigned long long t0 = gtimer();
+  const long long t0 = wclock(), lim = wait_cycles(wait_ns);
   while (true) {
     if (mbar_try_hint(bar, parity, WAIT_HINT_NS)) return true;
-    if (gtimer() - t0 > wait_ns) return false;
+    if (wclock() - t0 > lim) return false;
   }
 }
 
@@ -66,10 +74,10 @@ __device__ __forceinline__ bool mbar_wait_ns(uint64_t* bar, uint32_t parity, uns
 __device__ __forceinline__ bool mbar_wait_or_abort_ns(uint64_t* bar, uint32_t parity, volatile int* abort_flag,
                                                       unsigned long long wait_ns) {
   if (mbar_try(bar, parity)) return true;
-  const unsigned long long t0 = gtimer();
+  const long long t0 = wclock(), lim = wait_cycles(wait_ns);
   while (true) {
     if (mbar_try_hint(bar, parity, WAIT_HINT_NS)) return true;
-    if (*abort_flag || gtimer() - t0 > wait_ns) return false;
+    if (*abort_flag || wclock() - t0 > lim) return false;
   }
 }
 
