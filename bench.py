@@ -269,7 +269,9 @@ def stage_work(w, info, precision):
 # stage (profiles/ names the command)
 NCU_TRAFFIC = {("c3_3d_l128", "split_tc", "v3_synth"): 150.75e6, ("c3_3d_l128", "split_tc", "v3_lon_inv"): 227.35e6,
                ("c3_3d_l128", "split_tc", "v3_lon_fwd"): 223.56e6,
-               ("c3_3d_l128", "split_tc", "v3_analysis"): 209.04e6}
+               ("c3_3d_l128", "split_tc", "v3_analysis"): 209.04e6,
+               ("c3_3d_l128", "exact_tc", "v3_lon_inv"): 490.36e6, ("c3_3d_l128", "exact_tc", "v3_lon_fwd"): 474.24e6,
+               ("c3_3d_l128", "exact_tc", "v3_analysis"): 421.21e6}
 
 
 def max_over_ranks(ms, dist, device):
