@@ -508,14 +508,200 @@ __global__ void k_transpose(int nrow, int ncol, const double* __restrict__ A, do
   AT[(size_t)c * nrow + r] = A[t];
 }
 
+
+// ------------------------------------------------------------------ sea-level misfit
+//
+// The coupled forward (vg_update: forward-Euler sub-steps, each a drift, a
+// sea-level solve and a memory advance) with its discrete decisions held
+// fixed (the sub-steps, the ocean function of every pass, the inner
+// iterations done) is linear in the ice thickness, so its adjoint runs the
+// transposes backwards through the recorded decisions. One sea-level pass
+// (src/vilma_sle.f90:248-340) with ocean function C:
+//   dig = ice (1 - C) - ice_ref (1 - C0),  ice_int = -(rho_i / rho_w) <dig>
+//   K iterations of  r <- Sraw + dphi,  Sraw = Synth(apply(A(rho_i dig + rho_w C r + wcorr)))  (N - u),
+//                    dphi = (ice_int - <C Sraw> + zeta_int) / <C>
+// (<f> = sum w_j dlon f, the surface integral), from r_0 = the previous pass's
+// r (the first pass: the previous sub-step's rsl, or zero without a warm
+// start); the closing load sigma = A(rho_i dig + rho_w C r + wcorr) drives
+// the memory advance. The transposes of the grid transforms are scaled
+// transforms: Synth^T(y) = (c_m / sc) A(y / w_j) and A^T(s) = sc w_j
+// Synth(s / c_m), with sc = 2 pi / nphi, c_0 = 1, c_m = 2.
+
+// residuals of one interval's rsl at the sites
+__global__ void k_site_resid(int nsite, const int* __restrict__ site, const double* __restrict__ rsl,
+                             const double* __restrict__ obs, double* __restrict__ resid) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s < nsite) resid[s] = rsl[site[s]] - obs[s];
+}
+
+// rbar(site) += 2 resid: one thread, sites in order (a repeated site adds up
+// in a fixed order)
+__global__ void k_site_scatter(int nsite, const int* __restrict__ site, const double* __restrict__ resid,
+                               double* __restrict__ rbar) {
+  if (blockIdx.x == 0 && threadIdx.x == 0)
+    for (int s = 0; s < nsite; ++s) rbar[site[s]] += 2.0 * resid[s];
+}
+
+// a pass's ocean function (0 / 1 doubles) as bytes
+__global__ void k_c_bytes(int ng, const double* __restrict__ C, unsigned char* __restrict__ out) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < ng) out[i] = C[i] != 0.0 ? 1 : 0;
+}
+
+// per-row sums of lam
+__global__ void k_rev_rows(int nphi, const double* __restrict__ lam, double* __restrict__ rows) {
+  __shared__ double red[128];
+  const int j = blockIdx.x;
+  double acc = 0.0;
+  for (int i = threadIdx.x; i < nphi; i += blockDim.x) acc += lam[(size_t)j * nphi + i];
+  acc = block_sum(acc, red);
+  if (threadIdx.x == 0) rows[j] = acc;
+}
+
+// dphi_bar = sum of lam (rows in order): scal[0] = <C Sraw>_bar = -dphi_bar / <C>,
+// scal[1] += ice_int_bar = dphi_bar / <C>
+__global__ void k_rev_scal(int nlat, const double* __restrict__ rows, double C_int, double* __restrict__ scal) {
+  if (blockIdx.x != 0 || threadIdx.x != 0) return;
+  double acc = 0.0;
+  for (int j = 0; j < nlat; ++j) acc += rows[j];
+  scal[0] = -acc / C_int;
+  scal[1] += acc / C_int;
+}
+
+// Sraw_bar = lam + scal[0] C w_j dlon, divided by w_j for the analysis that
+// forms the synthesis transpose
+__global__ void k_rev_y(int ng, int nphi, const double* __restrict__ lam, const unsigned char* __restrict__ C,
+                        const double* __restrict__ wts, double dlon, const double* __restrict__ scal,
+                        double* __restrict__ out) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= ng) return;
+  const double w = wts[p / nphi];
+  out[p] = (lam[p] + (C[p] ? scal[0] * w * dlon : 0.0)) / w;
+}
+
+// q_bar = (c_m / sc) q (the synthesis transpose of Sraw_bar, q the analysis of
+// Sraw_bar / w_j); apply^T: sigma_bar = (gn - gu) q_bar, the surface drift
+// adjoints dUa_bar -= q_bar, dFa_bar -= q_bar / g; out = sigma_bar / c_m for
+// the synthesis that forms the analysis transpose
+__global__ void k_rev_apply(int nlm, int nk, double g, double sc, const int* __restrict__ lm_l,
+                            const int* __restrict__ lm_m, const int* __restrict__ lm2k, const double* __restrict__ gu,
+                            const double* __restrict__ gn, const double* __restrict__ q, double* __restrict__ surf_bar,
+                            double* __restrict__ out) {
+  const int lm = blockIdx.x * blockDim.x + threadIdx.x;
+  if (lm >= nlm) return;
+  const int l = lm_l[lm], m = lm_m[lm];
+  const double cm = (m == 0) ? 1.0 : 2.0;
+  const double qr = q[2 * lm] * cm / sc, qi = (m == 0) ? 0.0 : q[2 * lm + 1] * cm / sc;
+  const double gd = gn[l] - gu[l];
+  out[2 * lm] = gd * qr / cm;
+  out[2 * lm + 1] = gd * qi / cm;
+  if (l == 0) return;
+  const int k = lm2k[lm];
+  surf_bar[(size_t)0 * nk + k] -= qr;
+  surf_bar[(size_t)1 * nk + k] -= qi;
+  surf_bar[(size_t)2 * nk + k] -= qr / g;
+  surf_bar[(size_t)3 * nk + k] -= qi / g;
+}
+
+// s / c_m (the closing load's sigma_bar, ahead of the analysis transpose)
+__global__ void k_lm_div_cm(int nlm, const int* __restrict__ lm_m, const double* __restrict__ in,
+                            double* __restrict__ out) {
+  const int lm = blockIdx.x * blockDim.x + threadIdx.x;
+  if (lm >= nlm) return;
+  const double cm = (lm_m[lm] == 0) ? 1.0 : 2.0;
+  out[2 * lm] = in[2 * lm] / cm;
+  out[2 * lm + 1] = in[2 * lm + 1] / cm;
+}
+
+// load_bar = sc w_j g (g the synthesis of sigma_bar / c_m); lam_out (= or, with
+// add, +=) rho_w C load_bar; digbar += rho_i load_bar
+__global__ void k_rev_load(int ng, int nphi, const double* __restrict__ g, const double* __restrict__ wts, double sc,
+                           const unsigned char* __restrict__ C, int add, double* __restrict__ lam_out,
+                           double* __restrict__ digbar) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= ng) return;
+  const double lb = sc * wts[p / nphi] * g[p];
+  const double v = C[p] ? RHO_WATER * lb : 0.0;
+  lam_out[p] = add ? lam_out[p] + v : v;
+  digbar[p] += RHO_ICE * lb;
+}
+
+// the end of a pass: ice_now_bar = (1 - C) (digbar - (rho_i / rho_w) ice_int_bar
+// w_j dlon), into the adjoints of this interval's end ice (frac) and of the
+// previous interval's (1 - frac; none for the first interval of the call)
+__global__ void k_rev_ice(int ng, int nphi, const unsigned char* __restrict__ C, const double* __restrict__ digbar,
+                          const double* __restrict__ wts, double dlon, const double* __restrict__ scal, int with_int,
+                          double frac, double* __restrict__ gi1, double* __restrict__ gi0) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= ng || C[p]) return;
+  double d = digbar[p];
+  if (with_int) d -= (RHO_ICE / RHO_WATER) * scal[1] * wts[p / nphi] * dlon;
+  gi1[p] += frac * d;
+  if (gi0) gi0[p] += (1.0 - frac) * d;
+}
+
+// sum over the 3-D elements' grids (n3 fields of ng) into y, divided by w_j
+// (the synthesis transpose of the lateral field's gradient)
+__global__ void k_sum_fields_w(int n3, int ng, int nphi, const double* __restrict__ f, const double* __restrict__ wts,
+                               double* __restrict__ y) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= ng) return;
+  double acc = 0.0;
+  for (int e = 0; e < n3; ++e) acc += f[(size_t)e * ng + p];
+  y[p] = acc / wts[p / nphi];
+}
+
+// q_bar = (c_m / sc) q, the imaginary part of m = 0 zero
+__global__ void k_synthT_scale(int nlm, double sc, const int* __restrict__ lm_m, double* __restrict__ q) {
+  const int lm = blockIdx.x * blockDim.x + threadIdx.x;
+  if (lm >= nlm) return;
+  const int m = lm_m[lm];
+  const double cm = (m == 0) ? 1.0 : 2.0;
+  q[2 * lm] *= cm / sc;
+  q[2 * lm + 1] = (m == 0) ? 0.0 : q[2 * lm + 1] * cm / sc;
+}
+
 // ------------------------------------------------------------------ host
 
 namespace {
+
+
+// tape of the coupled forward (sea-level misfit): per accepted forward-Euler
+// sub-step its interval, interpolation fraction, length and sea-level passes;
+// per pass its inner iterations and ocean area, its ocean function as bytes
+struct TapePass {
+  int K;         // inner iterations done (0 without an ocean)
+  double C_int;  // ocean area <C>
+};
+struct TapeSub {
+  int n;        // interval
+  double frac;  // where the sub-step ends in its interval (ice interpolation)
+  double dt;    // length [s]
+  int pass0, npass;
+};
+struct SleTape {
+  std::vector<TapeSub> subs;
+  std::vector<TapePass> passes;
+  DArr<unsigned char> cb;  // the passes' ocean functions, ng bytes each
+  size_t pass_cap = 0;
+  double* gseg = nullptr;  // the sub-steps' longitude grids (3-D elements), gsz doubles each
+  size_t gsz = 0;
+  int gcap = 0;
+  int interval = 0;
+  size_t att_pass0 = 0;
+  double att_frac = 0.0, att_dt = 0.0;
+};
 
 struct AdjWork {
   DArr<double> sig, obs, resid, lam, lam_new, dUn_bar, dVn_bar, surf_bar, qbar, w, gsig, ckpt, E, G1T;
   DArr<double> ckpt_norm, gseg, gradMdt;  // checkpoint norms, a segment's longitude grids, d J / d (M dt)
   DArr<int> site;
+  // sea-level misfit: interval-end ice, checkpoints (rsl and entering ice
+  // beside the memory), the entry state, the reverse sweep's grid and
+  // spectral work arrays, d J / d ice, the tape
+  DArr<double> ice, ck_rsl, ck_hice, sv_mem, sv_mnorm, sv_rsl, sv_hice, sv_C, sv_zbed, sv_sig;
+  DArr<double> rA, rB, digbar, ybuf, gbuf, obuf, sbuf, scal, rows, gice;
+  SleTape tape;
 };
 
 void adj_release(void* p) { delete static_cast<AdjWork*>(p); }
@@ -606,6 +792,67 @@ struct StateGuard {
   }
 };
 
+
+// buffers and one-time attributes of a reverse sweep
+void reverse_prepare(vg_handle* h, AdjWork& W) {
+  const int nk = h->nk, nr = h->nr, ne = h->ne, nd = h->ndof;
+  const size_t S = h->d_mem[0].n;
+  ensure(W.lam, S);
+  ensure(W.lam_new, S);
+  ensure(W.dUn_bar, (size_t)2 * nr * nk);
+  ensure(W.dVn_bar, (size_t)2 * nr * nk);
+  ensure(W.surf_bar, (size_t)4 * nk);
+  ensure(W.qbar, 2 * (size_t)h->grid.nlm);
+  ensure(W.w, (size_t)2 * nd * nk);
+  ensure(W.E, (size_t)5 * 2 * ne * nk);
+  const int nrow = 2 * nr + 1, ncol = 2 * nr;
+  if (W.G1T.n != (size_t)nrow * ncol) {
+    W.G1T.alloc((size_t)nrow * ncol);
+    k_transpose<<<(nrow * ncol + 255) / 256, 256, 0, h->stream>>>(nrow, ncol, h->d_G1.p, W.G1T.p);
+    VG_CUDA(cudaGetLastError());
+  }
+  static std::atomic<bool> ts_attr{false};  // set once; concurrent handles may race to it
+  if (!ts_attr) {
+    VG_CUDA(cudaFuncSetAttribute(k_drift_T, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)(TS_WARPS * TS_WARP * sizeof(double))));
+    ts_attr = true;
+  }
+}
+
+// advance^T of one step of length dt: lam -> lam_new ((1 - M) lam on the 1-D
+// elements, gather^T on the 3-D ones, whose grid the forward stored in
+// gstore; gw d J / d (M dt) into gradMdt), the nodal drift adjoints, and
+// sigma_bar += the load's share (sbar)
+void advance_T(vg_handle* h, AdjWork& W, double dt, const double* gstore, double gw, double* sbar) {
+  const int nk = h->nk, nr = h->nr, ne = h->ne;
+  const dim3 eg((nk + 31) / 32, (ne + 7) / 8, 2), ng_((nk + 31) / 32, (nr + 7) / 8, 2);
+  cudaStream_t s = h->stream;
+  k_adv1d_T_elem<<<eg, dim3(32, 8), 0, s>>>(ne, nr, nk, dt, h->d_kdeg.p, h->d_Jr.p, h->d_xUn.p, h->d_xVn.p,
+                                             h->d_mu.p, h->d_MkPerDt.p, h->d_active1d.p, W.lam.p, W.lam_new.p,
+                                             W.E.p);
+  if (h->lat_visc && h->ne3d > 0) visc3d_adjoint(h, gstore, dt, W.lam.p, W.lam_new.p, W.E.p, W.gradMdt.p, gw);
+  k_adv1d_T_node<<<ng_, dim3(32, 8), 0, s>>>(ne, nr, nk, h->d_k2lm.p, W.E.p, W.dUn_bar.p, W.dVn_bar.p, sbar);
+  h->n_launch += 2;
+  VG_CUDA(cudaGetLastError());
+}
+
+// drift^T: the nodal (dUn_bar, dVn_bar) and surface (surf_bar) drift
+// adjoints into the memory adjoint lam_new (adds)
+void drift_T(vg_handle* h, AdjWork& W) {
+  const int nk = h->nk, nr = h->nr, ne = h->ne, nd = h->ndof;
+  const dim3 eg((nk + 31) / 32, (ne + 7) / 8, 2);
+  cudaStream_t s = h->stream;
+  const size_t shm1 = (size_t)(4 * (2 * nr + 1) + 4 * 2 * nr) * sizeof(double);
+  const size_t ts_smem = (size_t)TS_WARPS * TS_WARP * sizeof(double);
+  k_drift_T<<<(h->ntask + TS_WARPS - 1) / TS_WARPS, 32 * TS_WARPS, ts_smem, s>>>(
+      nr, nd, nk, h->d_tasks.p, h->ntask, h->d_ab.p, h->d_dc.p, W.dUn_bar.p, W.dVn_bar.p, W.surf_bar.p, W.w.p);
+  k_rhs_T<<<eg, dim3(32, 8), 0, s>>>(ne, nd, nk, h->d_kdeg.p, h->d_dr.p, h->d_Krhs.p, W.w.p, W.lam_new.p);
+  k_drift_T_deg1<<<1, 512, shm1, s>>>(ne, nr, nk, h->p.deg1_cm, h->d_dr1.p, h->d_null1.p, W.G1T.p, h->d_Krhs.p,
+                                      W.dUn_bar.p, W.dVn_bar.p, W.surf_bar.p, W.lam_new.p);
+  h->n_launch += 3;
+  VG_CUDA(cudaGetLastError());
+}
+
 }  // namespace
 
 double misfit_dev(vg_handle* h, int nsteps, double dt, const double* sigma, int nsite, const int* site,
@@ -635,7 +882,7 @@ double misfit_grad_dev(vg_handle* h, int nsteps, double dt, const double* sigma,
   const Grid& G = h->grid;
   cudaStream_t s = h->stream;
   const size_t n2 = 2 * (size_t)G.nlm, S = h->d_mem[0].n;
-  const int nk = h->nk, nr = h->nr, ne = h->ne, nd = h->ndof;
+  const int nk = h->nk, ne = h->ne;
   AdjWork& W = work_of(h);
   const int cur0 = h->cur;  // the entry state is checkpoint 0, put back at the end
   upload_inputs(h, W, nsteps, sigma, nsite, site, obs);
@@ -674,33 +921,10 @@ double misfit_grad_dev(vg_handle* h, int nsteps, double dt, const double* sigma,
   h->v3_gstore = nullptr;
   const double J = sum_squares(h, W, (size_t)nsteps * nsite);
   // reverse sweep
-  ensure(W.lam, S);
-  ensure(W.lam_new, S);
-  ensure(W.dUn_bar, (size_t)2 * nr * nk);
-  ensure(W.dVn_bar, (size_t)2 * nr * nk);
-  ensure(W.surf_bar, (size_t)4 * nk);
-  ensure(W.qbar, n2);
-  ensure(W.w, (size_t)2 * nd * nk);
+  reverse_prepare(h, W);
   ensure(W.gsig, (size_t)nsteps * n2);
   VG_CUDA(cudaMemsetAsync(W.lam.p, 0, S * sizeof(double), s));  // no terminal cost: lam_N = 0
   VG_CUDA(cudaMemsetAsync(W.gsig.p, 0, (size_t)nsteps * n2 * sizeof(double), s));
-  const dim3 eg((nk + 31) / 32, (ne + 7) / 8, 2), ng_((nk + 31) / 32, (nr + 7) / 8, 2);
-  ensure(W.E, (size_t)5 * 2 * ne * nk);
-  {
-    const int nrow = 2 * nr + 1, ncol = 2 * nr;
-    if (W.G1T.n != (size_t)nrow * ncol) {
-      W.G1T.alloc((size_t)nrow * ncol);
-      k_transpose<<<(nrow * ncol + 255) / 256, 256, 0, s>>>(nrow, ncol, h->d_G1.p, W.G1T.p);
-      VG_CUDA(cudaGetLastError());
-    }
-  }
-  const size_t shm1 = (size_t)(4 * (2 * nr + 1) + 4 * 2 * nr) * sizeof(double);
-  const size_t ts_smem = (size_t)TS_WARPS * TS_WARP * sizeof(double);
-  static std::atomic<bool> ts_attr{false};  // set once; concurrent handles may race to it
-  if (!ts_attr) {
-    VG_CUDA(cudaFuncSetAttribute(k_drift_T, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ts_smem));
-    ts_attr = true;
-  }
   if (v3) {
     const size_t ngm = (size_t)h->ne3d * G.ng;
     ensure(W.gradMdt, ngm);
@@ -723,18 +947,10 @@ double misfit_grad_dev(vg_handle* h, int nsteps, double dt, const double* sigma,
     VG_CUDA(cudaMemsetAsync(W.surf_bar.p, 0, W.surf_bar.n * sizeof(double), s));
     k_apply_T<<<(G.nlm + 255) / 256, 256, 0, s>>>(G.nlm, nk, h->g, G.d_lm_l.p, h->d_lm2k.p, h->d_gu.p, h->d_gn.p,
                                                  W.qbar.p, sbar, W.surf_bar.p);
-    k_adv1d_T_elem<<<eg, dim3(32, 8), 0, s>>>(ne, nr, nk, dt, h->d_kdeg.p, h->d_Jr.p, h->d_xUn.p, h->d_xVn.p,
-                                               h->d_mu.p, h->d_MkPerDt.p, h->d_active1d.p, W.lam.p, W.lam_new.p,
-                                               W.E.p);
-    if (v3) visc3d_adjoint(h, W.gseg.p + (size_t)(n - n0) * gsz, dt, W.lam.p, W.lam_new.p, W.E.p, W.gradMdt.p);
-    k_adv1d_T_node<<<ng_, dim3(32, 8), 0, s>>>(ne, nr, nk, h->d_k2lm.p, W.E.p, W.dUn_bar.p, W.dVn_bar.p, sbar);
-    k_drift_T<<<(h->ntask + TS_WARPS - 1) / TS_WARPS, 32 * TS_WARPS, ts_smem, s>>>(
-        nr, nd, nk, h->d_tasks.p, h->ntask, h->d_ab.p, h->d_dc.p, W.dUn_bar.p, W.dVn_bar.p, W.surf_bar.p, W.w.p);
-    k_rhs_T<<<eg, dim3(32, 8), 0, s>>>(ne, nd, nk, h->d_kdeg.p, h->d_dr.p, h->d_Krhs.p, W.w.p, W.lam_new.p);
-    k_drift_T_deg1<<<1, 512, shm1, s>>>(ne, nr, nk, h->p.deg1_cm, h->d_dr1.p, h->d_null1.p, W.G1T.p, h->d_Krhs.p,
-                                        W.dUn_bar.p, W.dVn_bar.p, W.surf_bar.p, W.lam_new.p);
-    h->n_launch += 7;
+    h->n_launch += 2;
     VG_CUDA(cudaGetLastError());
+    advance_T(h, W, dt, v3 ? W.gseg.p + (size_t)(n - n0) * gsz : nullptr, 1.0, sbar);
+    drift_T(h, W);
     std::swap(W.lam.p, W.lam_new.p);
   }
   if (grad_sigma) W.gsig.download(grad_sigma, (size_t)nsteps * n2, s);
@@ -768,6 +984,432 @@ double misfit_grad_dev(vg_handle* h, int nsteps, double dt, const double* sigma,
   return J;
 }
 
+
+// ------------------------------------------------------------------ sea-level misfit (host)
+
+void tape_attempt_begin(vg_handle* h, double frac, double dt) {
+  SleTape* T = static_cast<SleTape*>(h->sle_tape);
+  if (!T) return;
+  T->att_pass0 = T->passes.size();
+  T->att_frac = frac;
+  T->att_dt = dt;
+  if (T->gseg) {
+    if ((int)T->subs.size() >= T->gcap)
+      throw Error("vg_sle_misfit_grad: a checkpoint segment has more sub-steps than its grid store (the guard "
+                  "rejected sub-steps); use a smaller ckpt_every");
+    h->v3_gstore = T->gseg + T->subs.size() * T->gsz;
+  }
+}
+
+void tape_pass(vg_handle* h, double C_int, int n_inner) {
+  SleTape* T = static_cast<SleTape*>(h->sle_tape);
+  if (!T) return;
+  if (T->passes.size() >= T->pass_cap)
+    throw Error("vg_sle_misfit_grad: a checkpoint segment has more sea-level passes than the tape holds; use a "
+                "smaller ckpt_every");
+  const int ng = h->grid.ng;
+  k_c_bytes<<<(ng + 255) / 256, 256, 0, h->stream>>>(ng, h->d_C.p, T->cb.p + T->passes.size() * (size_t)ng);
+  ++h->n_launch;
+  VG_CUDA(cudaGetLastError());
+  T->passes.push_back({C_int > 0.0 ? n_inner : 0, C_int});
+}
+
+void tape_attempt_end(vg_handle* h, bool accepted) {
+  SleTape* T = static_cast<SleTape*>(h->sle_tape);
+  if (!T) return;
+  if (accepted)
+    T->subs.push_back({T->interval, T->att_frac, T->att_dt, (int)T->att_pass0,
+                       (int)(T->passes.size() - T->att_pass0)});
+  else
+    T->passes.resize(T->att_pass0);
+  h->v3_gstore = nullptr;
+}
+
+namespace {
+
+void sle_check(vg_handle* h, int nsteps, double dt_yr, const double* ice, int nsite, const int* site,
+               const double* obs) {
+  if (!ice || !obs) throw Error("vg_sle_misfit: null argument");
+  if (nsteps < 1) throw Error("vg_sle_misfit: nsteps must be >= 1");
+  if (!(dt_yr > 0.0)) throw Error("vg_sle_misfit: dt_yr must be > 0");
+  if (nsite < 1 || !site) throw Error("vg_sle_misfit: at least one site is required");
+  for (int s = 0; s < nsite; ++s)
+    if (site[s] < 0 || site[s] >= h->grid.ng) throw Error("vg_sle_misfit: site index outside the Gauss grid");
+  if (!h->have_reference) throw Error("vg_sle_misfit: call vg_set_reference first (solid_earth_init)");
+  if (h->p.scheme != VG_SCHEME_FE) throw Error("vg_sle_misfit: the coupled misfit follows the forward-Euler scheme");
+  if (h->rot_on) throw Error("vg_sle_misfit: rotational feedback is not differentiated (rotation = 0)");
+  if (h->tor_on) throw Error("vg_sle_misfit: the toroidal channels are not differentiated (toroidal = 0)");
+}
+
+// forward-Euler sub-steps of an interval by the Maxwell-CFL rule of the driver
+int fe_substeps(const vg_handle* h, double dt_yr) {
+  const vg_params& p = h->p;
+  const double span = dt_yr * SEC_PER_YEAR;
+  double dt_stab = h->max_rate > 0.0 ? p.cfl / h->max_rate : span;
+  dt_stab = std::min(dt_stab, p.dt_max);
+  if (p.dt_min > 0.0) dt_stab = std::max(dt_stab, p.dt_min);
+  return std::max(1, (int)std::ceil(span / dt_stab - 1.0e-9));
+}
+
+// the interval driver's state at entry (memory, norms, sea-level fields and
+// the last load spectrum, clocks and counters), put back at exit, also when
+// the call fails
+struct DriverGuard {
+  vg_handle* h;
+  AdjWork& W;
+  int cur;
+  double time_s, time_yr, mem_norm, bsl, worst;
+  long long n_accept, n_reject, n_solve;
+  int n_sub, n_outer, n_inner, n_flip;
+  bool done = false;
+  DriverGuard(vg_handle* hh, AdjWork& w) : h(hh), W(w) {
+    cudaStream_t s = h->stream;
+    const size_t S = h->d_mem[0].n, nk = h->nk, ng = h->grid.ng;
+    cur = h->cur;
+    ensure(W.sv_mem, S);
+    ensure(W.sv_mnorm, nk);
+    ensure(W.sv_rsl, ng);
+    ensure(W.sv_hice, ng);
+    ensure(W.sv_C, ng);
+    ensure(W.sv_zbed, ng);
+    ensure(W.sv_sig, 2 * (size_t)h->grid.nlm);
+    VG_CUDA(cudaMemcpyAsync(W.sv_sig.p, h->d_sigma.p, 2 * (size_t)h->grid.nlm * sizeof(double),
+                            cudaMemcpyDeviceToDevice, s));
+    VG_CUDA(cudaMemcpyAsync(W.sv_mem.p, h->d_mem[cur].p, S * sizeof(double), cudaMemcpyDeviceToDevice, s));
+    VG_CUDA(cudaMemcpyAsync(W.sv_mnorm.p, h->d_mnorm.p + (size_t)cur * nk, nk * sizeof(double),
+                            cudaMemcpyDeviceToDevice, s));
+    VG_CUDA(cudaMemcpyAsync(W.sv_rsl.p, h->d_rsl.p, ng * sizeof(double), cudaMemcpyDeviceToDevice, s));
+    VG_CUDA(cudaMemcpyAsync(W.sv_hice.p, h->d_h_ice.p, ng * sizeof(double), cudaMemcpyDeviceToDevice, s));
+    VG_CUDA(cudaMemcpyAsync(W.sv_C.p, h->d_C.p, ng * sizeof(double), cudaMemcpyDeviceToDevice, s));
+    VG_CUDA(cudaMemcpyAsync(W.sv_zbed.p, h->d_zbed.p, ng * sizeof(double), cudaMemcpyDeviceToDevice, s));
+    time_s = h->time_s;
+    time_yr = h->time_yr;
+    mem_norm = h->mem_norm;
+    bsl = h->bsl;
+    worst = h->worst_mass_resid;
+    n_accept = h->n_accept;
+    n_reject = h->n_reject;
+    n_solve = h->n_solve;
+    n_sub = h->n_sub_last;
+    n_outer = h->n_outer_last;
+    n_inner = h->n_inner_last;
+    n_flip = h->n_flip_last;
+  }
+  void restore() {
+    done = true;
+    h->sle_tape = nullptr;
+    h->v3_gstore = nullptr;
+    cudaStream_t s = h->stream;
+    const size_t S = h->d_mem[0].n, nk = h->nk, ng = h->grid.ng;
+    h->cur = cur;
+    VG_CUDA(cudaMemcpyAsync(h->d_mem[cur].p, W.sv_mem.p, S * sizeof(double), cudaMemcpyDeviceToDevice, s));
+    VG_CUDA(cudaMemcpyAsync(h->d_mnorm.p + (size_t)cur * nk, W.sv_mnorm.p, nk * sizeof(double),
+                            cudaMemcpyDeviceToDevice, s));
+    VG_CUDA(cudaMemcpyAsync(h->d_rsl.p, W.sv_rsl.p, ng * sizeof(double), cudaMemcpyDeviceToDevice, s));
+    VG_CUDA(cudaMemcpyAsync(h->d_h_ice.p, W.sv_hice.p, ng * sizeof(double), cudaMemcpyDeviceToDevice, s));
+    VG_CUDA(cudaMemcpyAsync(h->d_C.p, W.sv_C.p, ng * sizeof(double), cudaMemcpyDeviceToDevice, s));
+    VG_CUDA(cudaMemcpyAsync(h->d_zbed.p, W.sv_zbed.p, ng * sizeof(double), cudaMemcpyDeviceToDevice, s));
+    VG_CUDA(cudaMemcpyAsync(h->d_sigma.p, W.sv_sig.p, 2 * (size_t)h->grid.nlm * sizeof(double),
+                            cudaMemcpyDeviceToDevice, s));
+    h->time_s = time_s;
+    h->time_yr = time_yr;
+    h->mem_norm = mem_norm;
+    h->bsl = bsl;
+    h->worst_mass_resid = worst;
+    h->n_accept = n_accept;
+    h->n_reject = n_reject;
+    h->n_solve = n_solve;
+    h->n_sub_last = n_sub;
+    h->n_outer_last = n_outer;
+    h->n_inner_last = n_inner;
+    h->n_flip_last = n_flip;
+    VG_CUDA(cudaStreamSynchronize(s));
+  }
+  ~DriverGuard() {
+    if (!done) {
+      try {
+        restore();
+      } catch (...) {
+      }
+    }
+  }
+};
+
+void sle_upload(vg_handle* h, AdjWork& W, int nsteps, const double* ice, int nsite, const int* site,
+                const double* obs) {
+  const size_t ng = h->grid.ng;
+  cudaStream_t s = h->stream;
+  ensure(W.ice, (size_t)nsteps * ng);
+  W.ice.upload(ice, (size_t)nsteps * ng, s);
+  ensure(W.obs, (size_t)nsteps * nsite);
+  W.obs.upload(obs, (size_t)nsteps * nsite, s);
+  ensure(W.resid, (size_t)nsteps * nsite);
+  ensure(W.site, (size_t)nsite);
+  W.site.upload(site, nsite, s);
+}
+
+// interval n of the coupled forward (the driver's own update) and its site residuals
+void sle_interval(vg_handle* h, AdjWork& W, int n, double dt_yr, int nsite) {
+  const size_t ng = h->grid.ng;
+  W.tape.interval = n;
+  update_dev(h, W.ice.p + (size_t)n * ng, dt_yr);
+  k_site_resid<<<(nsite + 127) / 128, 128, 0, h->stream>>>(nsite, W.site.p, h->d_rsl.p,
+                                                          W.obs.p + (size_t)n * nsite, W.resid.p + (size_t)n * nsite);
+  ++h->n_launch;
+  VG_CUDA(cudaGetLastError());
+}
+
+// One pass's adjoint iterations (the pass's K inner iterations in reverse)
+// from rb, the adjoint of the pass's final r, to the adjoint of its starting
+// r (left in rb); digbar and scal[1] (ice_int_bar) accumulate, surf_bar too.
+void rev_pass(vg_handle* h, AdjWork& W, const unsigned char* C, const TapePass& P, double*& rb, double*& rb2) {
+  const Grid& G = h->grid;
+  const int ng = G.ng, nphi = G.nphi, nlat = G.nlat, nlm = G.nlm;
+  const double dlon = 2.0 * PI / (double)nphi, sc = dlon;
+  cudaStream_t s = h->stream;
+  const int eg = (ng + 255) / 256, lg = (nlm + 255) / 256;
+  for (int k = 0; k < P.K; ++k) {
+    k_rev_rows<<<nlat, 128, 0, s>>>(nphi, rb, W.rows.p);
+    k_rev_scal<<<1, 32, 0, s>>>(nlat, W.rows.p, P.C_int, W.scal.p);
+    k_rev_y<<<eg, 256, 0, s>>>(ng, nphi, rb, C, G.d_wts.p, dlon, W.scal.p, W.ybuf.p);
+    h->n_launch += 3;
+    VG_CUDA(cudaGetLastError());
+    sht_analysis_dev(h, W.ybuf.p, W.obuf.p, 1);
+    k_rev_apply<<<lg, 256, 0, s>>>(nlm, h->nk, h->g, sc, G.d_lm_l.p, G.d_lm_m.p, h->d_lm2k.p, h->d_gu.p, h->d_gn.p,
+                                   W.obuf.p, W.surf_bar.p, W.sbuf.p);
+    ++h->n_launch;
+    VG_CUDA(cudaGetLastError());
+    sht_synthesis_dev(h, W.sbuf.p, W.gbuf.p, 1);
+    k_rev_load<<<eg, 256, 0, s>>>(ng, nphi, W.gbuf.p, G.d_wts.p, sc, C, 0, rb2, W.digbar.p);
+    ++h->n_launch;
+    VG_CUDA(cudaGetLastError());
+    std::swap(rb, rb2);
+  }
+}
+
+// the reverse of one accepted sub-step: lam = the memory adjoint after it,
+// rb = the adjoint of its final rsl; on return lam = the adjoint before it,
+// rb = the adjoint of the rsl it started from
+void rev_substep(vg_handle* h, AdjWork& W, const TapeSub& sb, double dt_ref, bool warm, double*& rb,
+                 double*& rb2) {
+  const Grid& G = h->grid;
+  const int ng = G.ng, nphi = G.nphi, nlm = G.nlm;
+  const size_t n2 = 2 * (size_t)nlm;
+  const double dlon = 2.0 * PI / (double)nphi, sc = dlon;
+  cudaStream_t s = h->stream;
+  SleTape& T = W.tape;
+  const int eg = (ng + 255) / 256, lg = (nlm + 255) / 256;
+  // memory advance^T: the closing load's adjoint sigma_bar (qbar) and the nodal drift adjoints
+  VG_CUDA(cudaMemsetAsync(W.qbar.p, 0, n2 * sizeof(double), s));
+  VG_CUDA(cudaMemsetAsync(W.surf_bar.p, 0, W.surf_bar.n * sizeof(double), s));
+  const double* gst = T.gseg ? T.gseg + (size_t)(&sb - T.subs.data()) * T.gsz : nullptr;
+  advance_T(h, W, sb.dt, gst, sb.dt / dt_ref, W.qbar.p);
+  // closing load^T: rb += rho_w C r_bar, digbar = rho_i load_bar (last pass's C)
+  VG_CUDA(cudaMemsetAsync(W.digbar.p, 0, (size_t)ng * sizeof(double), s));
+  const unsigned char* Clast = T.cb.p + (size_t)(sb.pass0 + sb.npass - 1) * ng;
+  k_lm_div_cm<<<lg, 256, 0, s>>>(nlm, G.d_lm_m.p, W.qbar.p, W.obuf.p);
+  ++h->n_launch;
+  VG_CUDA(cudaGetLastError());
+  sht_synthesis_dev(h, W.obuf.p, W.gbuf.p, 1);
+  k_rev_load<<<eg, 256, 0, s>>>(ng, nphi, W.gbuf.p, G.d_wts.p, sc, Clast, 1, rb, W.digbar.p);
+  ++h->n_launch;
+  VG_CUDA(cudaGetLastError());
+  // the passes, last first
+  double* gi1 = W.gice.p + (size_t)sb.n * ng;
+  double* gi0 = sb.n > 0 ? W.gice.p + (size_t)(sb.n - 1) * ng : nullptr;
+  for (int io = sb.npass - 1; io >= 0; --io) {
+    const TapePass& P = T.passes[sb.pass0 + io];
+    const unsigned char* C = T.cb.p + (size_t)(sb.pass0 + io) * ng;
+    if (io != sb.npass - 1) VG_CUDA(cudaMemsetAsync(W.digbar.p, 0, (size_t)ng * sizeof(double), s));
+    VG_CUDA(cudaMemsetAsync(W.scal.p, 0, 2 * sizeof(double), s));
+    rev_pass(h, W, C, P, rb, rb2);
+    k_rev_ice<<<eg, 256, 0, s>>>(ng, nphi, C, W.digbar.p, G.d_wts.p, dlon, W.scal.p, P.K > 0 ? 1 : 0, sb.frac, gi1,
+                                 gi0);
+    ++h->n_launch;
+    VG_CUDA(cudaGetLastError());
+  }
+  // the first pass started from the previous sub-step's rsl (warm start) or from zero
+  if (!warm) VG_CUDA(cudaMemsetAsync(rb, 0, (size_t)ng * sizeof(double), s));
+  // drift^T: the surface drift adjoints of every inner iteration and the nodal ones of the advance
+  drift_T(h, W);
+  std::swap(W.lam.p, W.lam_new.p);
+}
+
+}  // namespace
+
+double sle_misfit_dev(vg_handle* h, int nsteps, double dt_yr, const double* ice, int nsite, const int* site,
+                      const double* obs) {
+  sle_check(h, nsteps, dt_yr, ice, nsite, site, obs);
+  SkipOff skip(h);
+  AdjWork& W = work_of(h);
+  DriverGuard guard(h, W);
+  sle_upload(h, W, nsteps, ice, nsite, site, obs);
+  for (int n = 0; n < nsteps; ++n) sle_interval(h, W, n, dt_yr, nsite);
+  const double J = sum_squares(h, W, (size_t)nsteps * nsite);
+  guard.restore();
+  return J;
+}
+
+double sle_misfit_grad_dev(vg_handle* h, int nsteps, double dt_yr, const double* ice, int nsite, const int* site,
+                           const double* obs, int ckpt, double* grad_ice, double* grad_pert, double* grad_pert_lm) {
+  sle_check(h, nsteps, dt_yr, ice, nsite, site, obs);
+  if (ckpt < 1) throw Error("vg_sle_misfit_grad: ckpt_every must be >= 1");
+  const bool v3 = h->lat_visc && h->ne3d > 0;
+  if (v3 && h->p.visc3d_precision != VG_VISC3D_FP64)
+    throw Error("vg_sle_misfit_grad: the 3-D adjoint follows the FP64 path (visc3d_precision = FP64)");
+  SkipOff skip(h);
+  const Grid& G = h->grid;
+  cudaStream_t s = h->stream;
+  const size_t ng = G.ng, S = h->d_mem[0].n, nk = h->nk;
+  AdjWork& W = work_of(h);
+  DriverGuard guard(h, W);
+  sle_upload(h, W, nsteps, ice, nsite, site, obs);
+  const double dt_ref = dt_yr * SEC_PER_YEAR;
+  // checkpoints every ckpt intervals: memory, its per-slot norms, rsl, the
+  // entering ice and the clocks
+  const int nck = (nsteps + ckpt - 1) / ckpt, seg = std::min(ckpt, nsteps);
+  ensure(W.ckpt, (size_t)nck * S);
+  ensure(W.ckpt_norm, (size_t)nck * nk);
+  ensure(W.ck_rsl, (size_t)nck * ng);
+  ensure(W.ck_hice, (size_t)nck * ng);
+  std::vector<double> ck_ts(nck), ck_ty(nck), ck_mn(nck);
+  auto snapshot = [&](int c) {
+    VG_CUDA(cudaMemcpyAsync(W.ckpt.p + (size_t)c * S, h->d_mem[h->cur].p, S * sizeof(double),
+                            cudaMemcpyDeviceToDevice, s));
+    VG_CUDA(cudaMemcpyAsync(W.ckpt_norm.p + (size_t)c * nk, h->d_mnorm.p + (size_t)h->cur * nk, nk * sizeof(double),
+                            cudaMemcpyDeviceToDevice, s));
+    VG_CUDA(cudaMemcpyAsync(W.ck_rsl.p + (size_t)c * ng, h->d_rsl.p, ng * sizeof(double), cudaMemcpyDeviceToDevice, s));
+    VG_CUDA(cudaMemcpyAsync(W.ck_hice.p + (size_t)c * ng, h->d_h_ice.p, ng * sizeof(double),
+                            cudaMemcpyDeviceToDevice, s));
+    ck_ts[c] = h->time_s;
+    ck_ty[c] = h->time_yr;
+    ck_mn[c] = h->mem_norm;
+  };
+  auto restore = [&](int c) {
+    VG_CUDA(cudaMemcpyAsync(h->d_mem[h->cur].p, W.ckpt.p + (size_t)c * S, S * sizeof(double),
+                            cudaMemcpyDeviceToDevice, s));
+    VG_CUDA(cudaMemcpyAsync(h->d_mnorm.p + (size_t)h->cur * nk, W.ckpt_norm.p + (size_t)c * nk, nk * sizeof(double),
+                            cudaMemcpyDeviceToDevice, s));
+    VG_CUDA(cudaMemcpyAsync(h->d_rsl.p, W.ck_rsl.p + (size_t)c * ng, ng * sizeof(double), cudaMemcpyDeviceToDevice, s));
+    VG_CUDA(cudaMemcpyAsync(h->d_h_ice.p, W.ck_hice.p + (size_t)c * ng, ng * sizeof(double),
+                            cudaMemcpyDeviceToDevice, s));
+    h->time_s = ck_ts[c];
+    h->time_yr = ck_ty[c];
+    h->mem_norm = ck_mn[c];
+  };
+  // the tape of one checkpoint segment: its passes' ocean functions and, with
+  // 3-D elements, its sub-steps' longitude grids
+  SleTape& T = W.tape;
+  const int nsub = fe_substeps(h, dt_yr);
+  T.pass_cap = (size_t)seg * (nsub + 4) * std::max(1, h->p.sle_n_outer);
+  if (T.cb.n < T.pass_cap * ng) T.cb.alloc(T.pass_cap * ng);
+  T.gsz = v3 ? (size_t)G.nlat * 3 * h->ne3d * 6 * G.nphi : 0;
+  T.gcap = v3 ? seg * nsub + 4 : 0;
+  if (v3) ensure(W.gseg, (size_t)T.gcap * T.gsz);
+  T.gseg = v3 ? W.gseg.p : nullptr;
+  auto record_segment = [&](int c, bool with_resid) {
+    T.subs.clear();
+    T.passes.clear();
+    h->sle_tape = &T;
+    const int a = c * ckpt, b = std::min(nsteps, a + ckpt);
+    for (int n = a; n < b; ++n) {
+      if (with_resid) {
+        sle_interval(h, W, n, dt_yr, nsite);
+      } else {
+        T.interval = n;
+        update_dev(h, W.ice.p + (size_t)n * ng, dt_yr);
+      }
+    }
+    h->sle_tape = nullptr;
+  };
+  // forward sweep: the last segment is recorded on the way
+  for (int c = 0; c < nck; ++c) {
+    snapshot(c);
+    if (c == nck - 1) {
+      record_segment(c, true);
+    } else {
+      for (int n = c * ckpt; n < (c + 1) * ckpt; ++n) sle_interval(h, W, n, dt_yr, nsite);
+    }
+  }
+  const double J = sum_squares(h, W, (size_t)nsteps * nsite);
+  // reverse sweep
+  reverse_prepare(h, W);
+  ensure(W.rA, ng);
+  ensure(W.rB, ng);
+  ensure(W.digbar, ng);
+  ensure(W.ybuf, ng);
+  ensure(W.gbuf, ng);
+  ensure(W.obuf, 2 * (size_t)G.nlm);
+  ensure(W.sbuf, 2 * (size_t)G.nlm);
+  ensure(W.scal, 2);
+  ensure(W.rows, (size_t)G.nlat);
+  ensure(W.gice, (size_t)nsteps * ng);
+  VG_CUDA(cudaMemsetAsync(W.lam.p, 0, S * sizeof(double), s));
+  VG_CUDA(cudaMemsetAsync(W.rA.p, 0, ng * sizeof(double), s));
+  VG_CUDA(cudaMemsetAsync(W.gice.p, 0, (size_t)nsteps * ng * sizeof(double), s));
+  if (v3) {
+    ensure(W.gradMdt, (size_t)h->ne3d * ng);
+    VG_CUDA(cudaMemsetAsync(W.gradMdt.p, 0, (size_t)h->ne3d * ng * sizeof(double), s));
+  }
+  double* rb = W.rA.p;
+  double* rb2 = W.rB.p;
+  const bool warm = h->p.sle_warm_start != 0;
+  for (int c = nck - 1; c >= 0; --c) {
+    if (c != nck - 1) {
+      restore(c);
+      record_segment(c, false);
+    }
+    const int a = c * ckpt, b = std::min(nsteps, a + ckpt);
+    int q = (int)T.subs.size() - 1;
+    for (int n = b - 1; n >= a; --n) {
+      k_site_scatter<<<1, 32, 0, s>>>(nsite, W.site.p, W.resid.p + (size_t)n * nsite, rb);
+      ++h->n_launch;
+      VG_CUDA(cudaGetLastError());
+      for (; q >= 0 && T.subs[q].n == n; --q) rev_substep(h, W, T.subs[q], dt_ref, warm, rb, rb2);
+    }
+    if (q != -1) throw Error("vg_sle_misfit_grad: the recorded sub-steps do not match the segment's intervals");
+  }
+  if (grad_ice) W.gice.download(grad_ice, (size_t)nsteps * ng, s);
+  if (v3 && (grad_pert || grad_pert_lm)) {
+    const size_t n3 = (size_t)h->ne3d * ng;
+    k_grad_pert<<<(unsigned)((n3 + 255) / 256), 256, 0, s>>>(n3, -std::log(10.0) * dt_ref, h->d_MkPerDt3.p,
+                                                            W.gradMdt.p);
+    ++h->n_launch;
+    VG_CUDA(cudaGetLastError());
+  }
+  if (grad_pert) {
+    int e3 = 0;
+    for (int e = 0; e < h->ne; ++e) {
+      if (v3 && e3 < h->ne3d && h->e3d_h[e3] == e) {
+        VG_CUDA(cudaMemcpyAsync(grad_pert + (size_t)e * ng, W.gradMdt.p + (size_t)e3 * ng, ng * sizeof(double),
+                                cudaMemcpyDeviceToHost, s));
+        ++e3;
+      } else {
+        std::fill(grad_pert + (size_t)e * ng, grad_pert + (size_t)(e + 1) * ng, 0.0);
+      }
+    }
+  }
+  if (grad_pert_lm) {
+    // the lateral field shared by the 3-D elements as a spectrum: d J / d q =
+    // Synth^T(sum over the elements of d J / d pert) = (c_m / sc) A(. / w_j)
+    const size_t n2 = 2 * (size_t)G.nlm;
+    if (v3) {
+      k_sum_fields_w<<<(unsigned)((ng + 255) / 256), 256, 0, s>>>(h->ne3d, (int)ng, G.nphi, W.gradMdt.p, G.d_wts.p,
+                                                                  W.ybuf.p);
+      sht_analysis_dev(h, W.ybuf.p, W.obuf.p, 1);
+      k_synthT_scale<<<(G.nlm + 255) / 256, 256, 0, s>>>(G.nlm, 2.0 * PI / (double)G.nphi, G.d_lm_m.p, W.obuf.p);
+      h->n_launch += 2;
+      VG_CUDA(cudaGetLastError());
+      W.obuf.download(grad_pert_lm, n2, s);
+    } else {
+      std::fill(grad_pert_lm, grad_pert_lm + n2, 0.0);
+    }
+  }
+  VG_CUDA(cudaStreamSynchronize(s));
+  guard.restore();
+  return J;
+}
+
 }  // namespace vg
 
 extern "C" int vg_misfit(vg_handle* h, int nsteps, double dt_s, const double* sigma_lm, int nsite, const int* site,
@@ -792,6 +1434,34 @@ extern "C" int vg_misfit_grad(vg_handle* h, int nsteps, double dt_s, const doubl
     if (!sigma_lm || !obs || !J) throw vg::Error("vg_misfit_grad: null argument");
     if (h->tor_on) throw vg::Error("vg_misfit_grad: the toroidal channels are not differentiated (toroidal = 0)");
     *J = vg::misfit_grad_dev(h, nsteps, dt_s, sigma_lm, nsite, site, obs, ckpt_every, grad_sigma, grad_pert);
+    return 0;
+  } catch (const std::exception& ex) {
+    h->err = ex.what();
+    return 1;
+  }
+}
+
+extern "C" int vg_sle_misfit(vg_handle* h, int nsteps, double dt_yr, const double* ice, int nsite, const int* site,
+                             const double* obs, double* J) {
+  if (!h) return 1;
+  try {
+    if (!J) throw vg::Error("vg_sle_misfit: null argument");
+    *J = vg::sle_misfit_dev(h, nsteps, dt_yr, ice, nsite, site, obs);
+    return 0;
+  } catch (const std::exception& ex) {
+    h->err = ex.what();
+    return 1;
+  }
+}
+
+extern "C" int vg_sle_misfit_grad(vg_handle* h, int nsteps, double dt_yr, const double* ice, int nsite,
+                                  const int* site, const double* obs, int ckpt_every, double* J, double* grad_ice,
+                                  double* grad_pert, double* grad_pert_lm) {
+  if (!h) return 1;
+  try {
+    if (!J) throw vg::Error("vg_sle_misfit_grad: null argument");
+    *J = vg::sle_misfit_grad_dev(h, nsteps, dt_yr, ice, nsite, site, obs, ckpt_every, grad_ice, grad_pert,
+                                 grad_pert_lm);
     return 0;
   } catch (const std::exception& ex) {
     h->err = ex.what();

@@ -244,6 +244,7 @@ struct vg_handle {
   void* tc_plan = nullptr;
   void (*tc_plan_release)(void*) = nullptr;
   // work buffers of the misfit / adjoint entry points (owned, opaque here)
+  void* sle_tape = nullptr;  // while set, the coupled forward records its decisions there (vg_adjoint.cu)
   void* adj_work = nullptr;
   void (*adj_release)(void*) = nullptr;
   ~vg_handle() {
@@ -293,10 +294,17 @@ void visc3d_advance(vg_handle* h, const double* d_sigma, double dt, const double
                     const double* dVn = nullptr, bool trap = false, const double* dWn = nullptr);
 // transposed 3-D advance (FP64 path) of one step whose longitude-pass grid the
 // forward stored in gstore: lam_new (3-D entries) = lam + gather^T, E (3-D
-// elements) = strain adjoints, d J / d (M dt) accumulated into gradMdt
+// elements) = strain adjoints, gw * d J / d (M dt) accumulated into gradMdt
 // (ne3d, nlat, nphi)
 void visc3d_adjoint(vg_handle* h, const double* gstore, double dt, const double* lam, double* lam_new, double* E,
-                    double* gradMdt);
+                    double* gradMdt, double gw = 1.0);
+// Tape of the coupled forward for the sea-level adjoint (vg_adjoint.cu): with
+// h->sle_tape set, the forward-Euler driver reports every sub-step attempt
+// (interpolation fraction, length; accepted or not) and the sea-level solve
+// every pass (its ocean function, ocean area and inner iterations done)
+void tape_attempt_begin(vg_handle* h, double frac, double dt);
+void tape_pass(vg_handle* h, double C_int, int n_inner);
+void tape_attempt_end(vg_handle* h, bool accepted);
 // rotational feedback (vg_rotation.cu)
 void build_fluid_deg2_band(vg_handle* h, DArr<double>& ab, DArr<double>& dr, DArr<double>& dc, DArr<int>& ipiv);
 void rotation_setup(vg_handle* h);

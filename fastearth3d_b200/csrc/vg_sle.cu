@@ -807,6 +807,7 @@ void sle_solve_dev(vg_handle* h, double dt, bool report_only) {
       k_flips<<<1, FIN_THREADS, 0, s>>>(sc, rp, nlat); ++h->n_launch;
     }
     read_scalars(h);
+    if (h->sle_tape) tape_pass(h, h->h_sc->C_int, h->h_sc->n_inner);
     if (h->h_sc->C_int <= 0.0) break;  // no ocean: nothing to redistribute
     if (h->h_sc->bar_error) throw Error("sle_solve: grid barrier of the fused inner loop timed out");
     h->n_inner_last = h->h_sc->n_inner;
@@ -939,6 +940,7 @@ void update_dev(vg_handle* h, const double* d_ice1, double dt_yr) {
                                      h->d_dice_now.p); ++h->n_launch;
       VG_CUDA(cudaGetLastError());
       h->n_solve++;
+      if (h->sle_tape) tape_attempt_begin(h, frac, dtc);
       sle_solve_dev(h, dtc, false);
       int nxt = 1 - h->cur;
       VG_CUDA(cudaMemcpyAsync(h->h_sc, h->d_sc_.p, sizeof(SleScalars), cudaMemcpyDeviceToHost, s));
@@ -947,6 +949,7 @@ void update_dev(vg_handle* h, const double* d_ice1, double dt_yr) {
       bool finite = err_inf <= HUGE_;
       double scale = std::max(tau0, tau_run);
       bool accept = scale <= 0.0 ? finite : (finite && err_inf <= p.guard_growth * scale);
+      if (h->sle_tape) tape_attempt_end(h, accept);
       if (accept) {
         h->cur = nxt;
         h->mem_norm = err_inf;

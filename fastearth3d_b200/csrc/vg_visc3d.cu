@@ -964,7 +964,7 @@ template <int LF>
 __global__ void __launch_bounds__(LON_THREADS, 1)
     k_v3_lon_T(const double* __restrict__ gstore, double* __restrict__ Yb, int nlat, int nphi, int nf, double dt,
                const double* __restrict__ Mk3rate, LonTables T, const double* __restrict__ invsin,
-               double* __restrict__ gradMdt) {
+               double* __restrict__ gradMdt, double gw) {
   extern __shared__ double sm[];
   const int j = blockIdx.x, f0 = blockIdx.y * LF;
   const int nft = min(LF, nf - f0);
@@ -1020,7 +1020,7 @@ __global__ void __launch_bounds__(LON_THREADS, 1)
     const int el = t / nphi, i = t % nphi;
     const double acc = P[(size_t)(3 * el) * nphi + i] + P[(size_t)(3 * el + 1) * nphi + i] +
                        P[(size_t)(3 * el + 2) * nphi + i];
-    gradMdt[((size_t)(f0 / 3 + el) * nlat + j) * nphi + i] -= acc;
+    gradMdt[((size_t)(f0 / 3 + el) * nlat + j) * nphi + i] -= gw * acc;
   }
   // 4. synthesis^T: c_bar(m) = w_m sum_i g_bar(i) (cos, -sin)(m phi_i), then
   //    the dyadic components^T into the product adjoints (written over Yb)
@@ -1094,7 +1094,7 @@ static void lon_attributes() {
 }
 
 void visc3d_adjoint(vg_handle* h, const double* gstore, double dt, const double* lam, double* lam_new, double* E,
-                    double* gradMdt) {
+                    double* gradMdt, double gw) {
   if (h->ne3d == 0) return;
   if (h->p.visc3d_precision != VG_VISC3D_FP64)
     throw Error("vg_misfit_grad: the 3-D adjoint follows the FP64 path (visc3d_precision = FP64)");
@@ -1163,7 +1163,7 @@ void visc3d_adjoint(vg_handle* h, const double* gstore, double dt, const double*
   {
     const dim3 lg(G.nlat, (nf + LON_LF - 1) / LON_LF);
     k_v3_lon_T<LON_LF><<<lg, lon_threads(h, LON_LF), lon_smem(h, LON_LF, true), s>>>(
-        gstore, h->d_v3a_Yb.p, G.nlat, G.nphi, nf, dt, h->d_MkPerDt3.p, lon_tables(h), G.d_invsin.p, gradMdt);
+        gstore, h->d_v3a_Yb.p, G.nlat, G.nphi, nf, dt, h->d_MkPerDt3.p, lon_tables(h), G.d_invsin.p, gradMdt, gw);
   }
   GemmArgs Sb = S;  // synthesis^T: the unweighted tables, per product out
   Sb.mode = 1;

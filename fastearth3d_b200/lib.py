@@ -59,6 +59,9 @@ _SIGS = [
                    C.POINTER(C.c_int)]),
     ("vg_misfit", [_VP, C.c_int, C.c_double, _P, C.c_int, C.POINTER(C.c_int), _P, _P]),
     ("vg_misfit_grad", [_VP, C.c_int, C.c_double, _P, C.c_int, C.POINTER(C.c_int), _P, C.c_int, _P, _P, _P]),
+    ("vg_sle_misfit", [_VP, C.c_int, C.c_double, _P, C.c_int, C.POINTER(C.c_int), _P, _P]),
+    ("vg_sle_misfit_grad", [_VP, C.c_int, C.c_double, _P, C.c_int, C.POINTER(C.c_int), _P, C.c_int, _P, _P, _P,
+                            _P]),
     ("vg_sht_analysis", [_VP, _P, _P]),
     ("vg_sht_synthesis", [_VP, _P, _P]),
     ("vg_sht_analysis_noalloc", [_VP, C.c_void_p, C.c_void_p, C.c_int]),
@@ -267,6 +270,37 @@ class Model:
         out = (J.value, g[..., 0] + 1j * g[..., 1])
         if want_pert:
             out = out + (gp.reshape(self.ne, self.p.nlat, self.p.nphi),)
+        return out
+
+    def _sle_args(self, ice, sites, obs):
+        ice = np.ascontiguousarray(np.asarray(ice, dtype=np.float64).reshape(-1, self.ng))
+        st = np.ascontiguousarray(np.asarray(sites, dtype=np.int32))
+        ob = np.ascontiguousarray(np.asarray(obs, dtype=np.float64).reshape(len(ice), len(st)))
+        return ice, st, ob
+
+    def sle_misfit(self, ice, dt_yr, sites, obs):
+        """J of the coupled run over len(ice) intervals (ice: interval-end thickness per interval)."""
+        ice, st, ob = self._sle_args(ice, sites, obs)
+        J = C.c_double(0)
+        self._c(lib().vg_sle_misfit(self.h, len(ice), dt_yr, ptr(ice), len(st),
+                                    st.ctypes.data_as(C.POINTER(C.c_int)), ptr(ob), C.byref(J)))
+        return J.value
+
+    def sle_misfit_grad(self, ice, dt_yr, sites, obs, ckpt_every=50, want_pert=False):
+        """(J, dJ/dice[, dJ/dpert, dJ/dq]): dJ/dice shaped (nsteps, nlat, nphi); with want_pert
+        dJ/dpert shaped (ne, nlat, nphi) and dJ/dq of the shared lateral field's spectrum
+        (nlm complex, d/dRe + 1j d/dIm)."""
+        ice, st, ob = self._sle_args(ice, sites, obs)
+        J = C.c_double(0)
+        gi = np.zeros_like(ice)
+        gp = np.zeros(self.ne * self.ng) if want_pert else None
+        gq = np.zeros(2 * self.nlm) if want_pert else None
+        self._c(lib().vg_sle_misfit_grad(self.h, len(ice), dt_yr, ptr(ice), len(st),
+                                         st.ctypes.data_as(C.POINTER(C.c_int)), ptr(ob), ckpt_every, C.byref(J),
+                                         ptr(gi), ptr(gp), ptr(gq)))
+        out = (J.value, gi.reshape(len(ice), self.p.nlat, self.p.nphi))
+        if want_pert:
+            out = out + (gp.reshape(self.ne, self.p.nlat, self.p.nphi), gq[0::2] + 1j * gq[1::2])
         return out
 
     def rotation(self):

@@ -327,6 +327,42 @@ int vg_misfit(vg_handle* h, int nsteps, double dt_s, const double* sigma_lm, int
 int vg_misfit_grad(vg_handle* h, int nsteps, double dt_s, const double* sigma_lm, int nsite, const int* site,
                    const double* obs, int ckpt_every, double* J, double* grad_sigma, double* grad_pert);
 
+/* Relative-sea-level misfit of the coupled time step and its gradient
+ * (hand-written discrete adjoint; the reference has no counterpart). From the
+ * handle's current state, nsteps intervals of vg_update (solid_earth_update,
+ * src/vilma_coupling.f90:336-437: forward-Euler sub-steps, the sea-level
+ * equation of src/vilma_sle.f90:124-405 with its migrating coastline, the
+ * guard) of dt_yr each, ice[n * ng ...] the ice thickness at the end of
+ * interval n on the Gauss grid ((nphi, nlat), phi fastest):
+ *   J = sum_n sum_s (rsl_n(site[s]) - obs[n * nsite + s])^2,
+ * rsl_n the relative sea level after interval n at the grid points site[s].
+ * vg_sle_misfit_grad also returns, with the forward's discrete decisions held
+ * (its sub-steps, the ocean function of every sea-level pass, the inner
+ * iterations done):
+ *   grad_ice      dJ/d ice, nsteps x ng (NULL skips it); the ice of each
+ *                 sub-step is interpolated in time between the interval's
+ *                 ends (solve_at, src/vilma_timestep.f90:314-326), so ice[n]
+ *                 collects from intervals n and n + 1;
+ *   grad_pert     with lateral viscosity (FP64 path), dJ/d the log10-viscosity
+ *                 perturbation of vg_enable_visc3d, (ne, nlat, nphi), zero on
+ *                 elements that are not 3-D (NULL skips it);
+ *   grad_pert_lm  dJ/d the spectrum q of one lateral field shared by every
+ *                 3-D element (pert_e = the handle's synthesis of q), nlm
+ *                 complex (interleaved re/im, d/dRe and d/dIm); a caller that
+ *                 keeps degrees <= 32 reads those entries (NULL skips it).
+ * The reverse sweep keeps the interval driver's state every ckpt_every
+ * intervals and recomputes each segment from it; a segment's longitude grids
+ * (3-D elements) are held on the device, about 0.26 GB per sub-step at lmax
+ * 128 with 54 3-D elements. Forward Euler only, no rotation, no toroidal
+ * channels; the drift skip gate is off inside these calls. The handle's
+ * state (memory, rsl, ice, ocean function, z_bed, time, counters) is put
+ * back afterwards. */
+int vg_sle_misfit(vg_handle* h, int nsteps, double dt_yr, const double* ice, int nsite, const int* site,
+                  const double* obs, double* J);
+int vg_sle_misfit_grad(vg_handle* h, int nsteps, double dt_yr, const double* ice, int nsite, const int* site,
+                       const double* obs, int ckpt_every, double* J, double* grad_ice, double* grad_pert,
+                       double* grad_pert_lm);
+
 /* Gauss-grid transforms on the device (sht_grid_synthesis / _analysis,
  * src/vilma_sht.f90:204-226), host arrays in and out. */
 int vg_sht_analysis(vg_handle* h, const double* f, double* q_lm);
