@@ -49,6 +49,8 @@ def parse():
     ap.add_argument("--workload", default=DEFAULT_WORKLOAD)
     ap.add_argument("--cpu-sample-s", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-one-thread", action="store_true",
+                    help="also time one step of the oracle on one host thread (cpu_baseline_1thread)")
     ap.add_argument("--precision", default="exact_tc", choices=["exact_tc", "split_tc", "fp64"],
                     help="3-D stress products of the timed arm: exact int8-digit tensor-core products (default), "
                          "two-term TF32 tensor-core products, or FP64 on the CUDA cores")
@@ -168,6 +170,7 @@ FP64_NOMINAL_TFLOPS = 37.0  # B200 dense FP64 (vector and tensor), datasheet fig
 def cpu_baseline(w, budget_s, threads):
     from oracle import orc  # the CPU restatement: test/baseline infrastructure only
 
+    orc.set_threads(threads)
     o = orc.Oracle(w.params(orc.default_params))
     zb, hi = w.reference()
     o.set_reference(zb, hi)
@@ -727,6 +730,8 @@ def main():
             out["grad_fwd"] = measure_grad_fwd_sle(w)
     if not args.no_cpu_baseline:
         out["cpu_baseline"] = cpu_baseline(w, args.cpu_sample_s, os.cpu_count() or 1)
+        if args.cpu_one_thread:  # one step at one thread (a minute or more at lmax 128): the scalar baseline
+            out["cpu_baseline_1thread"] = cpu_baseline(w, 0.0, 1)
     print(json.dumps(out))
     if dist:
         dist.destroy_process_group()

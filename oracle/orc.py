@@ -34,6 +34,7 @@ def lib():
             ("orc_params_default", [C.POINTER(VgParams)]),
             ("orc_create", [C.POINTER(VgParams), C.POINTER(_VP)]),
             ("orc_destroy", [_VP]),
+            ("orc_set_threads", [C.c_int]),
             ("orc_set_reference", [_VP, _P, _P, _P]),
             ("orc_enable_visc3d", [_VP, _P]),
             ("orc_advance", [_VP, _P, _P, C.c_double, C.c_double, _P, _P, _P, _P]),
@@ -83,6 +84,11 @@ def ptr(a):
         return None
     assert a.dtype == np.float64 and a.flags.c_contiguous
     return a.ctypes.data_as(_P)
+
+
+def set_threads(n):
+    """OpenMP threads of the oracle's parallel loops."""
+    _check(lib().orc_set_threads(int(n)))
 
 
 def default_params():

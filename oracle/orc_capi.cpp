@@ -9,6 +9,8 @@
 #include <stdexcept>
 #include <string>
 
+#include <omp.h>
+
 #include "../include/vilma_gpu.h"
 #include "orc.hpp"
 
@@ -141,6 +143,13 @@ int orc_create(const vg_params* p, OrcHandle** out) {
 
 int orc_destroy(OrcHandle* h) {
   delete h;
+  return 0;
+}
+
+// OpenMP threads of the oracle's parallel loops (the baseline's core count)
+int orc_set_threads(int n) {
+  if (n < 1) return 1;
+  omp_set_num_threads(n);
   return 0;
 }
 
