@@ -58,8 +58,9 @@ def parse():
                     help="also time the plain FP64 arm beside the tensor-core arm (and report the rsl error between them)")
     ap.add_argument("--tf32", default="on", choices=["on", "off"],
                     help="also time the two-term TF32 tensor-core arm beside the exact one (with its rsl error)")
-    ap.add_argument("--ensemble-sle-ctas", default="rows", choices=["sm", "rows"],
-                    help="c4_ensemble: the fused sea-level loop's CTAs per instance (one per SM, or one per grid row)")
+    ap.add_argument("--ensemble-sle-ctas", default="rows", choices=["sm", "rows", "tuned"],
+                    help="c4_ensemble: the fused sea-level loop's CTAs per instance (one per SM, one per grid row, "
+                         "or the autotuner's choice, which also picks the exact stages' warp splits)")
     ap.add_argument("--toroidal", default="on", choices=["on", "off", "only"],
                     help="also time the FP64 path carrying the toroidal channels (toroidal = 1); "
                          "only: time that path alone as the main arm")
@@ -163,6 +164,9 @@ def algorithmic_bytes(info, phase):
         return 2 * state + drift_nodal
     return None
 
+
+# the autotuner's cache for this run (a fresh file: every run tunes once per model key)
+TUNE_CACHE = os.path.join(__import__("tempfile").mkdtemp(prefix="vg_tune_"), "tune.txt")
 
 FP64_NOMINAL_TFLOPS = 37.0  # B200 dense FP64 (vector and tensor), datasheet figure
 
@@ -314,6 +318,14 @@ def run_arm(w, precision, args, ice_dev, local, dist, want_e2e, toroidal=False):
     stream = torch.cuda.ExternalStream(m.stream_ptr())
     for s in range(args.warmup):
         m.update_device(ice_dev[s].data_ptr(), w.dt_yr)
+    tuned = None
+    if precision == PRECISION["exact_tc"] and w.visc3d:
+        # the project autotuner (bit-identical choices), timed from this state and put back
+        t0 = time.perf_counter()
+        cached = m.autotune(w.dt_yr, TUNE_CACHE)
+        ncw, ctas = m.tuning()
+        tuned = {"exact_stage_converter_warps": ncw, "sle_ctas": ctas, "from_cache": cached,
+                 "tuning_s": round(time.perf_counter() - t0, 3)}
     launches0 = m.info().n_launch
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     if dist:
@@ -328,7 +340,8 @@ def run_arm(w, precision, args, ice_dev, local, dist, want_e2e, toroidal=False):
             ev1.record()
         torch.cuda.synchronize()
     ms = ev0.elapsed_time(ev1)
-    out = {"ms": ms, "launches": m.info().n_launch - launches0, "info": m.info(), "clocks": clk.summary()}
+    out = {"ms": ms, "launches": m.info().n_launch - launches0, "info": m.info(), "clocks": clk.summary(),
+           "tuning": tuned}
     out["rsl"], out["zbed"] = m.fields()[:2]
     if dist:
         out["ms"] = max_over_ranks(ms, dist, "cuda")
@@ -523,6 +536,9 @@ def run_ensemble(args):
         m.set_reference(zb, hi)
         if mb.visc3d:
             m.enable_visc3d(mb.pert(m.p))
+        if args.ensemble_sle_ctas == "tuned":  # once per model key (the cache), bit-identical choices
+            p.sle_ctas = mb.nlat
+            m.autotune(DT, TUNE_CACHE, knobs=1)  # the stages; the loop keeps one CTA per grid row
         return m
 
     def dev_timed(fn):
@@ -692,7 +708,7 @@ def main():
         "dtype": PRECISION_DTYPE[prec],
         "data": "synthetic",
         "config": workload_config(w, info.n_sub_last, world),
-        "arm": {"visc3d_precision": prec, "toroidal": bool(tor_only)},
+        "arm": {"visc3d_precision": prec, "toroidal": bool(tor_only), "tuning": main_arm["tuning"]},
         "e2e": {"value": 1e3 / main_arm["e2e_ms"], "unit": "steps/s", "h2d_bytes_per_step": ng * 8,
                 "d2h_bytes_per_step": ng * 8},
         "gpu_launches": int(main_arm["launches"]),

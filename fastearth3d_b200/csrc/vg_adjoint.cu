@@ -699,7 +699,8 @@ struct AdjWork {
   // sea-level misfit: interval-end ice, checkpoints (rsl and entering ice
   // beside the memory), the entry state, the reverse sweep's grid and
   // spectral work arrays, d J / d ice, the tape
-  DArr<double> ice, ck_rsl, ck_hice, sv_mem, sv_mnorm, sv_rsl, sv_hice, sv_C, sv_zbed, sv_sig;
+  DArr<double> ice, ck_rsl, ck_hice;
+  DriverSnap entry;
   DArr<double> rA, rB, digbar, ybuf, gbuf, obuf, sbuf, scal, rows, gice;
   SleTape tape;
 };
@@ -1056,74 +1057,14 @@ int fe_substeps(const vg_handle* h, double dt_yr) {
 // the call fails
 struct DriverGuard {
   vg_handle* h;
-  AdjWork& W;
-  int cur;
-  double time_s, time_yr, mem_norm, bsl, worst;
-  long long n_accept, n_reject, n_solve;
-  int n_sub, n_outer, n_inner, n_flip;
+  DriverSnap& snap;
   bool done = false;
-  DriverGuard(vg_handle* hh, AdjWork& w) : h(hh), W(w) {
-    cudaStream_t s = h->stream;
-    const size_t S = h->d_mem[0].n, nk = h->nk, ng = h->grid.ng;
-    cur = h->cur;
-    ensure(W.sv_mem, S);
-    ensure(W.sv_mnorm, nk);
-    ensure(W.sv_rsl, ng);
-    ensure(W.sv_hice, ng);
-    ensure(W.sv_C, ng);
-    ensure(W.sv_zbed, ng);
-    ensure(W.sv_sig, 2 * (size_t)h->grid.nlm);
-    VG_CUDA(cudaMemcpyAsync(W.sv_sig.p, h->d_sigma.p, 2 * (size_t)h->grid.nlm * sizeof(double),
-                            cudaMemcpyDeviceToDevice, s));
-    VG_CUDA(cudaMemcpyAsync(W.sv_mem.p, h->d_mem[cur].p, S * sizeof(double), cudaMemcpyDeviceToDevice, s));
-    VG_CUDA(cudaMemcpyAsync(W.sv_mnorm.p, h->d_mnorm.p + (size_t)cur * nk, nk * sizeof(double),
-                            cudaMemcpyDeviceToDevice, s));
-    VG_CUDA(cudaMemcpyAsync(W.sv_rsl.p, h->d_rsl.p, ng * sizeof(double), cudaMemcpyDeviceToDevice, s));
-    VG_CUDA(cudaMemcpyAsync(W.sv_hice.p, h->d_h_ice.p, ng * sizeof(double), cudaMemcpyDeviceToDevice, s));
-    VG_CUDA(cudaMemcpyAsync(W.sv_C.p, h->d_C.p, ng * sizeof(double), cudaMemcpyDeviceToDevice, s));
-    VG_CUDA(cudaMemcpyAsync(W.sv_zbed.p, h->d_zbed.p, ng * sizeof(double), cudaMemcpyDeviceToDevice, s));
-    time_s = h->time_s;
-    time_yr = h->time_yr;
-    mem_norm = h->mem_norm;
-    bsl = h->bsl;
-    worst = h->worst_mass_resid;
-    n_accept = h->n_accept;
-    n_reject = h->n_reject;
-    n_solve = h->n_solve;
-    n_sub = h->n_sub_last;
-    n_outer = h->n_outer_last;
-    n_inner = h->n_inner_last;
-    n_flip = h->n_flip_last;
-  }
+  DriverGuard(vg_handle* hh, DriverSnap& sn) : h(hh), snap(sn) { snap.save(h); }
   void restore() {
     done = true;
     h->sle_tape = nullptr;
     h->v3_gstore = nullptr;
-    cudaStream_t s = h->stream;
-    const size_t S = h->d_mem[0].n, nk = h->nk, ng = h->grid.ng;
-    h->cur = cur;
-    VG_CUDA(cudaMemcpyAsync(h->d_mem[cur].p, W.sv_mem.p, S * sizeof(double), cudaMemcpyDeviceToDevice, s));
-    VG_CUDA(cudaMemcpyAsync(h->d_mnorm.p + (size_t)cur * nk, W.sv_mnorm.p, nk * sizeof(double),
-                            cudaMemcpyDeviceToDevice, s));
-    VG_CUDA(cudaMemcpyAsync(h->d_rsl.p, W.sv_rsl.p, ng * sizeof(double), cudaMemcpyDeviceToDevice, s));
-    VG_CUDA(cudaMemcpyAsync(h->d_h_ice.p, W.sv_hice.p, ng * sizeof(double), cudaMemcpyDeviceToDevice, s));
-    VG_CUDA(cudaMemcpyAsync(h->d_C.p, W.sv_C.p, ng * sizeof(double), cudaMemcpyDeviceToDevice, s));
-    VG_CUDA(cudaMemcpyAsync(h->d_zbed.p, W.sv_zbed.p, ng * sizeof(double), cudaMemcpyDeviceToDevice, s));
-    VG_CUDA(cudaMemcpyAsync(h->d_sigma.p, W.sv_sig.p, 2 * (size_t)h->grid.nlm * sizeof(double),
-                            cudaMemcpyDeviceToDevice, s));
-    h->time_s = time_s;
-    h->time_yr = time_yr;
-    h->mem_norm = mem_norm;
-    h->bsl = bsl;
-    h->worst_mass_resid = worst;
-    h->n_accept = n_accept;
-    h->n_reject = n_reject;
-    h->n_solve = n_solve;
-    h->n_sub_last = n_sub;
-    h->n_outer_last = n_outer;
-    h->n_inner_last = n_inner;
-    h->n_flip_last = n_flip;
-    VG_CUDA(cudaStreamSynchronize(s));
+    snap.restore(h);
   }
   ~DriverGuard() {
     if (!done) {
@@ -1242,7 +1183,7 @@ double sle_misfit_dev(vg_handle* h, int nsteps, double dt_yr, const double* ice,
   sle_check(h, nsteps, dt_yr, ice, nsite, site, obs);
   SkipOff skip(h);
   AdjWork& W = work_of(h);
-  DriverGuard guard(h, W);
+  DriverGuard guard(h, W.entry);
   sle_upload(h, W, nsteps, ice, nsite, site, obs);
   for (int n = 0; n < nsteps; ++n) sle_interval(h, W, n, dt_yr, nsite);
   const double J = sum_squares(h, W, (size_t)nsteps * nsite);
@@ -1262,7 +1203,7 @@ double sle_misfit_grad_dev(vg_handle* h, int nsteps, double dt_yr, const double*
   cudaStream_t s = h->stream;
   const size_t ng = G.ng, S = h->d_mem[0].n, nk = h->nk;
   AdjWork& W = work_of(h);
-  DriverGuard guard(h, W);
+  DriverGuard guard(h, W.entry);
   sle_upload(h, W, nsteps, ice, nsite, site, obs);
   const double dt_ref = dt_yr * SEC_PER_YEAR;
   // checkpoints every ckpt intervals: memory, its per-slot norms, rsl, the

@@ -695,3 +695,68 @@ int vg_sht_synthesis(vg_handle* h, const double* q_lm, double* f) {
 }
 
 }  // extern "C"
+
+namespace vg {
+
+void DriverSnap::save(vg_handle* h) {
+  cudaStream_t s = h->stream;
+  const size_t S = h->d_mem[0].n, nk = h->nk, ng = h->grid.ng, n2 = 2 * (size_t)h->grid.nlm;
+  cur = h->cur;
+  auto grab = [&](DArr<double>& dst, const double* src, size_t n) {
+    if (dst.n < n) dst.alloc(n);
+    VG_CUDA(cudaMemcpyAsync(dst.p, src, n * sizeof(double), cudaMemcpyDeviceToDevice, s));
+  };
+  grab(mem, h->d_mem[cur].p, S);
+  grab(mnorm, h->d_mnorm.p + (size_t)cur * nk, nk);
+  grab(rsl, h->d_rsl.p, ng);
+  grab(hice, h->d_h_ice.p, ng);
+  grab(C, h->d_C.p, ng);
+  grab(zbed, h->d_zbed.p, ng);
+  grab(sig, h->d_sigma.p, n2);
+  if (maxbits.n < 2) maxbits.alloc(2);
+  VG_CUDA(cudaMemcpyAsync(maxbits.p, h->d_maxbits.p, 2 * sizeof(unsigned long long), cudaMemcpyDeviceToDevice, s));
+  time_s = h->time_s;
+  time_yr = h->time_yr;
+  mem_norm = h->mem_norm;
+  bsl = h->bsl;
+  worst = h->worst_mass_resid;
+  n_accept = h->n_accept;
+  n_reject = h->n_reject;
+  n_solve = h->n_solve;
+  n_sub = h->n_sub_last;
+  n_outer = h->n_outer_last;
+  n_inner = h->n_inner_last;
+  n_flip = h->n_flip_last;
+}
+
+void DriverSnap::restore(vg_handle* h) {
+  cudaStream_t s = h->stream;
+  const size_t S = h->d_mem[0].n, nk = h->nk, ng = h->grid.ng, n2 = 2 * (size_t)h->grid.nlm;
+  h->cur = cur;
+  auto put = [&](double* dst, const DArr<double>& src, size_t n) {
+    VG_CUDA(cudaMemcpyAsync(dst, src.p, n * sizeof(double), cudaMemcpyDeviceToDevice, s));
+  };
+  put(h->d_mem[cur].p, mem, S);
+  put(h->d_mnorm.p + (size_t)cur * nk, mnorm, nk);
+  put(h->d_rsl.p, rsl, ng);
+  put(h->d_h_ice.p, hice, ng);
+  put(h->d_C.p, C, ng);
+  put(h->d_zbed.p, zbed, ng);
+  put(h->d_sigma.p, sig, n2);
+  VG_CUDA(cudaMemcpyAsync(h->d_maxbits.p, maxbits.p, 2 * sizeof(unsigned long long), cudaMemcpyDeviceToDevice, s));
+  h->time_s = time_s;
+  h->time_yr = time_yr;
+  h->mem_norm = mem_norm;
+  h->bsl = bsl;
+  h->worst_mass_resid = worst;
+  h->n_accept = n_accept;
+  h->n_reject = n_reject;
+  h->n_solve = n_solve;
+  h->n_sub_last = n_sub;
+  h->n_outer_last = n_outer;
+  h->n_inner_last = n_inner;
+  h->n_flip_last = n_flip;
+  VG_CUDA(cudaStreamSynchronize(s));
+}
+
+}  // namespace vg

@@ -298,6 +298,24 @@ void visc3d_advance(vg_handle* h, const double* d_sigma, double dt, const double
 // (ne3d, nlat, nphi)
 void visc3d_adjoint(vg_handle* h, const double* gstore, double dt, const double* lam, double* lam_new, double* E,
                     double* gradMdt, double gw = 1.0);
+// exact tensor-core stages (vg_oz.cu): converter warps per stage (8 or 4);
+// oz_get_ncw returns false when the handle has no exact-stage plan
+void oz_set_ncw(vg_handle* h, const int ncw[4]);
+bool oz_get_ncw(const vg_handle* h, int ncw[4]);
+// The interval driver's state (memory of the current buffer, its per-slot
+// norms and both buffers' maxima, rsl, entering ice, ocean function, z_bed, the last load spectrum,
+// clocks and counters), saved and put back by the entry points that run
+// trial intervals (the coupled adjoint, the autotuner); vg_api.cu
+struct DriverSnap {
+  DArr<double> mem, mnorm, rsl, hice, C, zbed, sig;
+  DArr<unsigned long long> maxbits;  // both buffers' max |memory| (the drift skip gate's scale)
+  int cur = 0;
+  double time_s = 0, time_yr = 0, mem_norm = 0, bsl = 0, worst = 0;
+  long long n_accept = 0, n_reject = 0, n_solve = 0;
+  int n_sub = 0, n_outer = 0, n_inner = 0, n_flip = 0;
+  void save(vg_handle* h);
+  void restore(vg_handle* h);  // synchronises the handle's stream
+};
 // Tape of the coupled forward for the sea-level adjoint (vg_adjoint.cu): with
 // h->sle_tape set, the forward-Euler driver reports every sub-step attempt
 // (interpolation fraction, length; accepted or not) and the sea-level solve

@@ -248,9 +248,18 @@ struct Cta {
 // copies and MMAs by a fixed bound; after an abort every copy and MMA in
 // flight is waited for before the tensor memory is freed.
 namespace p {
-constexpr int NCONV = 256, NEPI = 256;
-constexpr int W_PROD = 0, W_MMA = 1, W_CONV = 2, W_EPI = 10, NWARP = 18;
+constexpr int W_PROD = 0, W_MMA = 1, W_CONV = 2, NWARP = 18;
 constexpr int NTHR = NWARP * 32;
+// the 16 converter + epilogue warps split NCW : 16 - NCW (a launch-time
+// choice per stage, the autotuner's; every split gives the same results)
+template <int NCW>
+struct Roles {
+  static constexpr int NCONV = NCW * 32, NEPI = (16 - NCW) * 32;
+  static constexpr int W_EPI = W_CONV + NCW;
+  static constexpr int NPART = (16 - NCW) / 4;  // epilogue warps per tensor-memory lane quarter
+  static constexpr int GSTEP = NCONV / TM;      // a converter thread's K groups of 16: g0, g0 + GSTEP, .. < 2
+  static_assert(NCW == 4 || NCW == 8, "converter warps");
+};
 template <int STAGE>
 struct Ring {
   static constexpr int NRAW = STAGE == ST_ANA ? 2 : 3;  // raw FP64 chunks in flight
@@ -338,9 +347,10 @@ __device__ __forceinline__ int valid_k(const Args& A, const Cta& c, int sub, int
   return max(0, min(KC, kmax - kc * KC));
 }
 
-template <int STAGE>
+template <int STAGE, int NCW>
 __global__ void __launch_bounds__(p::NTHR, 1) k_ozp_stage(const __grid_constant__ Args A) {
   using R = p::Ring<STAGE>;
+  using Q = p::Roles<NCW>;
   extern __shared__ unsigned char smraw[];
   unsigned char* sm = (unsigned char*)(((uintptr_t)smraw + 1023) & ~(uintptr_t)1023);
   unsigned char* raw = sm + R::RAW_OFF;
@@ -368,10 +378,10 @@ __global__ void __launch_bounds__(p::NTHR, 1) k_ozp_stage(const __grid_constant_
   if (tid == 0) {
     for (int i = 0; i < R::NRAW; ++i) {
       mbar_init(&raw_full[i], 1);
-      mbar_init(&raw_empty[i], p::NCONV);
+      mbar_init(&raw_empty[i], Q::NCONV);
     }
     for (int i = 0; i < R::NDST; ++i) {
-      mbar_init(&a_full[i], p::NCONV);
+      mbar_init(&a_full[i], Q::NCONV);
       mbar_init(&a_empty[i], 1);
     }
     for (int i = 0; i < R::NB; ++i) {
@@ -379,10 +389,10 @@ __global__ void __launch_bounds__(p::NTHR, 1) k_ozp_stage(const __grid_constant_
       mbar_init(&b_empty[i], 1);
     }
     mbar_init(acc_full, 1);
-    mbar_init(acc_empty, p::NEPI);
+    mbar_init(acc_empty, Q::NEPI);
     for (int i = 0; i < 2; ++i) {
-      mbar_init(&sum_full[i], p::NCONV);
-      mbar_init(&sum_empty[i], p::NEPI);
+      mbar_init(&sum_full[i], Q::NCONV);
+      mbar_init(&sum_empty[i], Q::NEPI);
     }
     fence_mbar_init();
     *abort_flag = 0;
@@ -524,10 +534,10 @@ __global__ void __launch_bounds__(p::NTHR, 1) k_ozp_stage(const __grid_constant_
         atomicOr(A.status, 1ull << (16 + STAGE));
     }
     __syncwarp();
-  } else if (warp < p::W_EPI) {
+  } else if (warp < Q::W_EPI) {
     // ------------------------------------------------------------ converters
-    const int ct = tid - p::W_CONV * 32;  // 0 .. 255
-    const int lr = ct % TM, g = ct / TM;   // row, K group of 16
+    const int ct = tid - p::W_CONV * 32;  // 0 .. NCONV - 1
+    const int lr = ct % TM, g0 = ct / TM;  // row, first K group of 16
     int gc = 0, gt = 0;
     for (int t = blockIdx.x; t < ntile && !*abort_flag; t += gridDim.x) {
       const Cta c = tile_info<STAGE>(A, t);
@@ -539,7 +549,8 @@ __global__ void __launch_bounds__(p::NTHR, 1) k_ozp_stage(const __grid_constant_
       const double rs = pow2(FIX_BITS - e);
       const double is_j = (STAGE == ST_INV) ? A.invsin[c.j] : 0.0;
       const int prow = (STAGE == ST_INV) ? row / A.F : 0;
-      double side0 = 0.0, side1 = 0.0;  // the tile's side sums (sub 0, sub 1)
+      // the tile's side sums (sub 0, sub 1) of this thread's first and second K group
+      double side0a = 0.0, side0b = 0.0, side1a = 0.0, side1b = 0.0;
       bool ok = true;
       for (int ch = 0; ch < nch; ++ch, ++gc) {
         const int sub = ch < nch0 ? 0 : 1, kc = sub ? ch - nch0 : ch;
@@ -554,61 +565,72 @@ __global__ void __launch_bounds__(p::NTHR, 1) k_ozp_stage(const __grid_constant_
         }
         const int kv = valid_k<STAGE>(A, c, sub, kc);
         const double* rv = (const double*)(raw + (size_t)rsi * R::RAW_BYTES);
-        double v[16];
-        double sacc = 0.0;  // this chunk's part of the side sum
-        if (STAGE == ST_INV) {
-          // K pairs (re, im) of one order: one 16-byte load per pair
+#pragma unroll 1
+        for (int it = 0; it < 2 / Q::GSTEP; ++it) {
+          const int g = g0 + it * Q::GSTEP;
+          double v[16];
+          double sacc = 0.0;  // this chunk's part of the side sum
+          if (STAGE == ST_INV) {
+            // K pairs (re, im) of one order: one 16-byte load per pair
 #pragma unroll
-          for (int q = 0; q < 16; q += 2) {
-            const int k = 16 * g + q, mo = k >> 1;
-            double tre = 0.0, tim = 0.0;
-            if (live && k < kv) {
-              const double2 z = *reinterpret_cast<const double2*>(rv + (size_t)mo * TM * 2 + 2 * lr);
-              tre = z.x;
-              tim = z.y;
-              if (prow == 2) {  // i (m / sin theta) z
-                const int m = (sub ? 1 : 2) + 2 * (kc * (KC / 2) + mo);
-                const double a = (double)m * is_j;
-                tre = -a * z.y;
-                tim = a * z.x;
-              } else if (prow == 5) {  // i z
-                tre = -z.y;
-                tim = z.x;
+            for (int q = 0; q < 16; q += 2) {
+              const int k = 16 * g + q, mo = k >> 1;
+              double tre = 0.0, tim = 0.0;
+              if (live && k < kv) {
+                const double2 z = *reinterpret_cast<const double2*>(rv + (size_t)mo * TM * 2 + 2 * lr);
+                tre = z.x;
+                tim = z.y;
+                if (prow == 2) {  // i (m / sin theta) z
+                  const int m = (sub ? 1 : 2) + 2 * (kc * (KC / 2) + mo);
+                  const double a = (double)m * is_j;
+                  tre = -a * z.y;
+                  tim = a * z.x;
+                } else if (prow == 5) {  // i z
+                  tre = -z.y;
+                  tim = z.x;
+                }
+                sacc += 2.0 * tre;
               }
-              sacc += 2.0 * tre;
+              v[q] = tre;
+              v[q + 1] = (k + 1 < kv && live) ? tim : 0.0;
             }
-            v[q] = tre;
-            v[q + 1] = (k + 1 < kv && live) ? tim : 0.0;
-          }
-        } else {
-          const double sg = (STAGE == ST_ANA) ? table_sigma(c.p) * (sub ? -1.0 : 1.0) : 0.0;
+          } else {
+            const double sg = (STAGE == ST_ANA) ? table_sigma(c.p) * (sub ? -1.0 : 1.0) : 0.0;
 #pragma unroll
-          for (int q = 0; q < 16; ++q) {
-            const int k = 16 * g + q;
-            double x = 0.0;
-            if (live && k < kv) {
-              if (STAGE == ST_ANA) {
-                const int j = kc * KC + k, jm = A.nlat - 1 - j;
-                const double r0 = rv[(size_t)k * TM + lr];
-                const double r1 = (jm != j) ? rv[(size_t)(KC + KC - 1 - k) * TM + lr] : 0.0;
-                x = r0 + sg * r1;
-              } else {
-                x = rv[(size_t)k * TM + lr];
-                if (STAGE == ST_FWD) sacc += x;
+            for (int q = 0; q < 16; ++q) {
+              const int k = 16 * g + q;
+              double x = 0.0;
+              if (live && k < kv) {
+                if (STAGE == ST_ANA) {
+                  const int j = kc * KC + k, jm = A.nlat - 1 - j;
+                  const double r0 = rv[(size_t)k * TM + lr];
+                  const double r1 = (jm != j) ? rv[(size_t)(KC + KC - 1 - k) * TM + lr] : 0.0;
+                  x = r0 + sg * r1;
+                } else {
+                  x = rv[(size_t)k * TM + lr];
+                  if (STAGE == ST_FWD) sacc += x;
+                }
               }
+              v[q] = x;
             }
-            v[q] = x;
           }
+          if (sub) {
+            if (it)
+              side1b += sacc;
+            else
+              side1a += sacc;
+          } else {
+            if (it)
+              side0b += sacc;
+            else
+              side0a += sacc;
+          }
+          uint4 pl[NDIG];
+          to_digits16(v, rs, pl);
+          unsigned char* Ab = adig + (size_t)ds * A_BYTES + ((size_t)g * TM + lr) * 16;
+#pragma unroll
+          for (int s = 0; s < NDIG; ++s) *reinterpret_cast<uint4*>(Ab + s * A_PLANE) = pl[s];
         }
-        if (sub)
-          side1 += sacc;
-        else
-          side0 += sacc;
-        uint4 pl[NDIG];
-        to_digits16(v, rs, pl);
-        unsigned char* Ab = adig + (size_t)ds * A_BYTES + ((size_t)g * TM + lr) * 16;
-#pragma unroll
-        for (int s = 0; s < NDIG; ++s) *reinterpret_cast<uint4*>(Ab + s * A_PLANE) = pl[s];
         fence_async_smem();
         mbar_arrive(&a_full[ds]);
         mbar_arrive(&raw_empty[rsi]);
@@ -622,8 +644,12 @@ __global__ void __launch_bounds__(p::NTHR, 1) k_ozp_stage(const __grid_constant_
           *abort_flag = 1;
           break;
         }
-        rsum[((tb * 2 + 0) * 2 + g) * TM + lr] = side0;
-        rsum[((tb * 2 + 1) * 2 + g) * TM + lr] = side1;
+        rsum[((tb * 2 + 0) * 2 + g0) * TM + lr] = side0a;
+        rsum[((tb * 2 + 1) * 2 + g0) * TM + lr] = side1a;
+        if (Q::GSTEP == 1) {
+          rsum[((tb * 2 + 0) * 2 + 1) * TM + lr] = side0b;
+          rsum[((tb * 2 + 1) * 2 + 1) * TM + lr] = side1b;
+        }
         mbar_arrive(&sum_full[tb]);
       }
       ++gt;
@@ -631,8 +657,8 @@ __global__ void __launch_bounds__(p::NTHR, 1) k_ozp_stage(const __grid_constant_
   } else {
     // ------------------------------------------------------------ epilogue
     // tcgen05.ld is warp-collective: lane 0 waits, the result is broadcast
-    const int ew = warp - p::W_EPI;  // 0 .. 7
-    const int quad = warp & 3, half_id = ew >> 2;
+    const int ew = warp - Q::W_EPI;  // 0 .. NEPI / 32 - 1
+    const int quad = warp & 3, part = ew >> 2;  // lane quarter, column part
     const int r = quad * 32 + lane;
     const uint32_t tbase = tmem + ((uint32_t)(quad * 32) << 16);
     int gt = 0;
@@ -706,7 +732,7 @@ __global__ void __launch_bounds__(p::NTHR, 1) k_ozp_stage(const __grid_constant_
         const int m = c.batch_m, pp = c.p;
         const double sg = table_sigma(pp);
         double gmax = 0.0;
-        for (int cb = half_id * 4; cb < npad_max; cb += 8) {
+        for (int cb = part * 4; cb < npad_max; cb += 4 * Q::NPART) {
           int a[2][NLEV][4];
           double wn[4], ws[4];
           issue_pair4(cb, a);
@@ -758,9 +784,9 @@ __global__ void __launch_bounds__(p::NTHR, 1) k_ozp_stage(const __grid_constant_
           gd[(size_t)i * A.NCOL] = dv;
           gmax = fmax(gmax, fmax(fabs(sv), fabs(dv)));
         };
-        if (live && c.nt == 0 && half_id == 0)
+        if (live && c.nt == 0 && part == 0)
           emit(0, c0 + sev, sod, __ldg(&nm_j[0]), __ldg(&nm_j[(size_t)A.half * A.ne3d]));
-        for (int cb = half_id * 4; cb < npad_max; cb += 8) {
+        for (int cb = part * 4; cb < npad_max; cb += 4 * Q::NPART) {
           int a[2][NLEV][4];
           double n1[4], n2[4];
           issue_pair4(cb, a);
@@ -789,7 +815,7 @@ __global__ void __launch_bounds__(p::NTHR, 1) k_ozp_stage(const __grid_constant_
           return reinterpret_cast<double2*>(A.S + (((size_t)m * A.nlat + c.j) * 6 + pp) * A.NC + 2 * f);
         };
         double gre = 0.0, gim = 0.0;
-        if (live && c.nt == 0 && half_id == 0) {
+        if (live && c.nt == 0 && part == 0) {
           // m = 0: F_0 = (2 pi / nphi) sum_i s_i, real
           const double v = (pp == 2) ? 0.0 : beta_c * sev * (2.0 * PI / (double)A.nphi);
           *out(0) = make_double2(v, 0.0);
@@ -798,7 +824,7 @@ __global__ void __launch_bounds__(p::NTHR, 1) k_ozp_stage(const __grid_constant_
         for (int sub = 0; sub < 2; ++sub) {
           if (!(sub ? has1 : has0)) continue;
           const int npad = sub ? c.sub[1].npad : c.sub[0].npad, nval = sub ? c.sub[1].nvalid : c.sub[0].nvalid;
-          for (int cb = half_id * 8; cb < npad; cb += 16) {
+          for (int cb = part * 8; cb < npad; cb += 8 * Q::NPART) {
             double v[8];
             load_block(sub, cb, v);
             if (!live) continue;
@@ -824,7 +850,7 @@ __global__ void __launch_bounds__(p::NTHR, 1) k_ozp_stage(const __grid_constant_
         for (int sub = 0; sub < 2; ++sub) {
           if (!(sub ? has1 : has0)) continue;
           const int npad = sub ? c.sub[1].npad : c.sub[0].npad;
-          for (int cb = half_id * 8; cb < npad; cb += 16) {
+          for (int cb = part * 8; cb < npad; cb += 8 * Q::NPART) {
             double v[8];
             load_block(sub, cb, v);
             if (!live) continue;
@@ -939,6 +965,7 @@ struct OzPlan {
   CUtensorMap tm[4];  // per stage: synthesis, inverse, forward, analysis
   int ntile_rows_nc, ntile_rows_col;
   int nsm = 148, tiles[4] = {0, 0, 0, 0};  // persistent grids: min(tiles, SMs) CTAs
+  int ncw[4] = {8, 8, 8, 8};  // converter warps per stage (8 or 4; the autotuner's choice)
   DArr<double> S, Gs, rate, bscale;
   // -M dt factors of the inverse stage for the last two (dt, trapezoidal) keys
   DArr<double> nmdt[2];
@@ -1108,10 +1135,14 @@ void visc3d_oz_enable(vg_handle* h) {
   a.status = h->d_maxbits.p + 2;
   P->ntile_rows_nc = (NC + oz::TM - 1) / oz::TM;
   P->ntile_rows_col = (NCOL + oz::TM - 1) / oz::TM;
-  raise_smem_limit((const void*)oz::k_ozp_stage<oz::ST_SYNTH>, oz::p::Ring<oz::ST_SYNTH>::SMEM);
-  raise_smem_limit((const void*)oz::k_ozp_stage<oz::ST_INV>, oz::p::Ring<oz::ST_INV>::SMEM);
-  raise_smem_limit((const void*)oz::k_ozp_stage<oz::ST_FWD>, oz::p::Ring<oz::ST_FWD>::SMEM);
-  raise_smem_limit((const void*)oz::k_ozp_stage<oz::ST_ANA>, oz::p::Ring<oz::ST_ANA>::SMEM);
+  raise_smem_limit((const void*)oz::k_ozp_stage<oz::ST_SYNTH, 8>, oz::p::Ring<oz::ST_SYNTH>::SMEM);
+  raise_smem_limit((const void*)oz::k_ozp_stage<oz::ST_INV, 8>, oz::p::Ring<oz::ST_INV>::SMEM);
+  raise_smem_limit((const void*)oz::k_ozp_stage<oz::ST_FWD, 8>, oz::p::Ring<oz::ST_FWD>::SMEM);
+  raise_smem_limit((const void*)oz::k_ozp_stage<oz::ST_ANA, 8>, oz::p::Ring<oz::ST_ANA>::SMEM);
+  raise_smem_limit((const void*)oz::k_ozp_stage<oz::ST_SYNTH, 4>, oz::p::Ring<oz::ST_SYNTH>::SMEM);
+  raise_smem_limit((const void*)oz::k_ozp_stage<oz::ST_INV, 4>, oz::p::Ring<oz::ST_INV>::SMEM);
+  raise_smem_limit((const void*)oz::k_ozp_stage<oz::ST_FWD, 4>, oz::p::Ring<oz::ST_FWD>::SMEM);
+  raise_smem_limit((const void*)oz::k_ozp_stage<oz::ST_ANA, 4>, oz::p::Ring<oz::ST_ANA>::SMEM);
   int dev = 0;
   VG_CUDA(cudaGetDevice(&dev));
   VG_CUDA(cudaDeviceGetAttribute(&P->nsm, cudaDevAttrMultiProcessorCount, dev));
@@ -1155,6 +1186,22 @@ unsigned long long* visc3d_oz_gather_max(vg_handle* h) {
 }
 
 // The four exact tensor-core stages between the FP64 gather and the scatter.
+// converter warps per exact stage (8 or 4 each; the rest of the 16 are epilogue warps)
+void oz_set_ncw(vg_handle* h, const int ncw[4]) {
+  OzPlan* P = static_cast<OzPlan*>(h->tc_plan);
+  if (!P || h->p.visc3d_precision != VG_VISC3D_EXACT_TC) return;
+  for (int i = 0; i < 4; ++i) {
+    if (ncw[i] != 4 && ncw[i] != 8) throw Error("exact stages: converter warps must be 4 or 8");
+    P->ncw[i] = ncw[i];
+  }
+}
+bool oz_get_ncw(const vg_handle* h, int ncw[4]) {
+  const OzPlan* P = static_cast<const OzPlan*>(h->tc_plan);
+  if (!P || h->p.visc3d_precision != VG_VISC3D_EXACT_TC) return false;
+  for (int i = 0; i < 4; ++i) ncw[i] = P->ncw[i];
+  return true;
+}
+
 void visc3d_oz_run(vg_handle* h, double dt, bool trap) {
   OzPlan* P = static_cast<OzPlan*>(h->tc_plan);
   cudaStream_t s = h->stream;
@@ -1186,10 +1233,23 @@ void visc3d_oz_run(vg_handle* h, double dt, bool trap) {
     ++h->n_launch;
     VG_CUDA(cudaGetLastError());
   };
-  launch(oz::k_ozp_stage<oz::ST_SYNTH>, VG_PH_V3_SYNTH, P->info_synth.p, P->tiles[0], oz::p::Ring<oz::ST_SYNTH>::SMEM);
-  launch(oz::k_ozp_stage<oz::ST_INV>, VG_PH_V3_LON_INV, P->info_inv.p, P->tiles[1], oz::p::Ring<oz::ST_INV>::SMEM);
-  launch(oz::k_ozp_stage<oz::ST_FWD>, VG_PH_V3_LON_FWD, P->info_fwd.p, P->tiles[2], oz::p::Ring<oz::ST_FWD>::SMEM);
-  launch(oz::k_ozp_stage<oz::ST_ANA>, VG_PH_V3_ANALYSIS, P->info_ana.p, P->tiles[3], oz::p::Ring<oz::ST_ANA>::SMEM);
+  using namespace oz;
+  if (P->ncw[0] == 4)
+    launch(k_ozp_stage<ST_SYNTH, 4>, VG_PH_V3_SYNTH, P->info_synth.p, P->tiles[0], p::Ring<ST_SYNTH>::SMEM);
+  else
+    launch(k_ozp_stage<ST_SYNTH, 8>, VG_PH_V3_SYNTH, P->info_synth.p, P->tiles[0], p::Ring<ST_SYNTH>::SMEM);
+  if (P->ncw[1] == 4)
+    launch(k_ozp_stage<ST_INV, 4>, VG_PH_V3_LON_INV, P->info_inv.p, P->tiles[1], p::Ring<ST_INV>::SMEM);
+  else
+    launch(k_ozp_stage<ST_INV, 8>, VG_PH_V3_LON_INV, P->info_inv.p, P->tiles[1], p::Ring<ST_INV>::SMEM);
+  if (P->ncw[2] == 4)
+    launch(k_ozp_stage<ST_FWD, 4>, VG_PH_V3_LON_FWD, P->info_fwd.p, P->tiles[2], p::Ring<ST_FWD>::SMEM);
+  else
+    launch(k_ozp_stage<ST_FWD, 8>, VG_PH_V3_LON_FWD, P->info_fwd.p, P->tiles[2], p::Ring<ST_FWD>::SMEM);
+  if (P->ncw[3] == 4)
+    launch(k_ozp_stage<ST_ANA, 4>, VG_PH_V3_ANALYSIS, P->info_ana.p, P->tiles[3], p::Ring<ST_ANA>::SMEM);
+  else
+    launch(k_ozp_stage<ST_ANA, 8>, VG_PH_V3_ANALYSIS, P->info_ana.p, P->tiles[3], p::Ring<ST_ANA>::SMEM);
 }
 
 }  // namespace vg

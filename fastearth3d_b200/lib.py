@@ -60,6 +60,8 @@ _SIGS = [
     ("vg_misfit", [_VP, C.c_int, C.c_double, _P, C.c_int, C.POINTER(C.c_int), _P, _P]),
     ("vg_misfit_grad", [_VP, C.c_int, C.c_double, _P, C.c_int, C.POINTER(C.c_int), _P, C.c_int, _P, _P, _P]),
     ("vg_sle_misfit", [_VP, C.c_int, C.c_double, _P, C.c_int, C.POINTER(C.c_int), _P, _P]),
+    ("vg_autotune", [_VP, C.c_double, C.c_int, C.c_char_p, C.POINTER(C.c_int)]),
+    ("vg_get_tuning", [_VP, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
     ("vg_sle_misfit_grad", [_VP, C.c_int, C.c_double, _P, C.c_int, C.POINTER(C.c_int), _P, C.c_int, _P, _P, _P,
                             _P]),
     ("vg_sht_analysis", [_VP, _P, _P]),
@@ -302,6 +304,21 @@ class Model:
         if want_pert:
             out = out + (gp.reshape(self.ne, self.p.nlat, self.p.nphi), gq[0::2] + 1j * gq[1::2])
         return out
+
+    def autotune(self, dt_yr, cache_path=None, knobs=3):
+        """vg_autotune (knobs: 1 the exact stages' warp splits, 2 the sea-level loop's CTAs);
+        returns True when the choices came from the cache file."""
+        fc = C.c_int(0)
+        path = None if cache_path is None else str(cache_path).encode()
+        self._c(lib().vg_autotune(self.h, dt_yr, knobs, path, C.byref(fc)))
+        return bool(fc.value)
+
+    def tuning(self):
+        """(converter warps of the four exact stages, sea-level loop CTAs)."""
+        ncw = (C.c_int * 4)()
+        ctas = C.c_int(0)
+        self._c(lib().vg_get_tuning(self.h, ncw, C.byref(ctas)))
+        return list(ncw), ctas.value
 
     def rotation(self):
         """Polar motion m (complex, rad) and (kTe, hTe, k_s fluid, k_s flattening)."""

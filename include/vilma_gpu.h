@@ -388,6 +388,28 @@ int vg_sht_synthesis(vg_handle* h, const double* q_lm, double* f);
 #define VG_NOALLOC_SCRATCH_DOUBLES (1 << 19)
 int vg_sht_analysis_noalloc(vg_handle* h, const double* d_f, double* d_q_lm, int batch);
 
+/* Autotuner of the launch shapes (no reference counterpart: the reference's
+ * OpenMP loops have none). Times a few intervals of the handle's own model on
+ * the ice it holds, from its current state (put back afterwards), for each
+ * candidate of the knobs selected in `knobs` (VG_TUNE_STAGES | VG_TUNE_SLE;
+ * an ensemble that shares the GPU keeps its own sea-level CTA count and
+ * tunes the stages only), both leaving the results unchanged bit for bit: the
+ * exact tensor-core stages' split of their worker warps between converters
+ * and epilogue (8 : 8 or 4 : 12, per stage) and the fused sea-level loop's CTA
+ * count (one per SM, one per Gauss row, two per SM). The fastest choices are
+ * applied to the handle and appended to the text file cache_path (NULL: no
+ * cache), keyed by lmax, grid, elements, 3-D elements, precision, ocean and
+ * knobs;
+ * a later call for a model of the same key reads them from there instead of
+ * timing (*from_cache = 1). Needs vg_set_reference first. */
+#define VG_TUNE_STAGES 1 /* the exact stages' warp splits */
+#define VG_TUNE_SLE 2    /* the fused sea-level loop's CTA count */
+int vg_autotune(vg_handle* h, double dt_yr, int knobs, const char* cache_path, int* from_cache);
+/* The current choices: converter warps of the four exact stages (zeros
+ * without an exact-stage plan) and the sea-level loop's CTA count (0: one per
+ * SM). */
+int vg_get_tuning(vg_handle* h, int* ncw, int* sle_ctas);
+
 /* The CUDA stream (cudaStream_t) all of the handle's work is ordered on, so a
  * caller can record events on it. */
 int vg_stream(vg_handle* h, void** stream);
