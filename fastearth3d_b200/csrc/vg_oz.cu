@@ -82,6 +82,9 @@ struct Args {
   // Gs; analysis: S by latitude)
   CUtensorMap tmap;
   int L, nlat, nh, nphi, half, F, NC, NCOL, nk, ne3d;
+  // toroidal channels carried (1): 6 gathered channels, 12 product slots in
+  // S, 10 synthesis and analysis tile types, 10 analysis outputs per slot
+  int tor, nslot, ntype, nq;
   int nts, nti, ntf, nta;
   const int* kbeg;
   const int* mbeg;     // first lm of each order
@@ -219,6 +222,26 @@ __device__ __forceinline__ int table_of(int p) {  // p -> table: 0 1 0 0 2 3
 }
 __device__ __forceinline__ int chan_of(int p) { return (p == 0) ? 0 : (p <= 2 ? 1 : (p == 3 ? 2 : 3)); }
 
+// With the toroidal channels (TOR) the synthesis has ten tile types and the
+// analysis ten. Synthesis types 6-9 are the toroidal products P.X4, D.X4,
+// H.X5, G.X5, written to the product slots 7, 8, 10, 11 of S: each is the
+// partner (slot + 6) of the dyadic component it adds to in the inverse stage
+// (rt += -i (m/sin) P.X4, rp += D.X4, tt - pp += -2 i H.X5 (slot 4's factor 2
+// is applied later), tp += G.X5 (slot 5's factor 4 likewise)); slots 6 and 9
+// stay zero. Analysis types 6-9 are the toroidal quadratures of the
+// components rp (wD), (m/sin) rt (wP), tp (wG), tt - pp (wH).
+__device__ __forceinline__ int tab_sign_idx(int table) { return (table == 1 || table == 3) ? -1 : 1; }
+__device__ __forceinline__ int syn_table(int t) {  // 0 1 0 0 2 3 | 0 1 3 2
+  return t < 6 ? table_of(t) : (t == 6 ? 0 : (t == 7 ? 1 : (t == 8 ? 3 : 2)));
+}
+__device__ __forceinline__ int syn_chan(int t) { return t < 6 ? chan_of(t) : (t < 8 ? 4 : 5); }
+__device__ __forceinline__ int syn_slot(int t) { return t < 6 ? t : (t == 6 ? 7 : (t == 7 ? 8 : (t == 8 ? 10 : 11))); }
+__device__ __forceinline__ int ana_table(int t) {  // 0 1 0 0 2 3 | 1 0 2 3
+  return t < 6 ? table_of(t) : (t == 6 ? 1 : (t == 7 ? 0 : (t == 8 ? 2 : 3)));
+}
+__device__ __forceinline__ int ana_src(int t) { return t < 6 ? t : (t == 6 ? 2 : (t == 7 ? 1 : (t == 8 ? 5 : 4))); }
+__device__ __forceinline__ int ana_group(int t) { return t < 6 ? t : (t == 6 ? 6 : (t == 7 ? 7 : (t == 8 ? 5 : 4))); }
+
 struct Cta {
   int rows, row0, batch_m, p, j, nt;
   ImgInfo sub[2];
@@ -260,11 +283,13 @@ struct Roles {
   static constexpr int GSTEP = NCONV / TM;      // a converter thread's K groups of 16: g0, g0 + GSTEP, .. < 2
   static_assert(NCW == 4 || NCW == 8, "converter warps");
 };
-template <int STAGE>
+// TWO: a raw chunk is two row boxes (the analysis: the mirrored latitudes;
+// the inverse with the toroidal channels: the partner slots' rows)
+template <int STAGE, bool TWO = (STAGE == ST_ANA)>
 struct Ring {
-  static constexpr int NRAW = STAGE == ST_ANA ? 2 : 3;  // raw FP64 chunks in flight
-  static constexpr int RAW_BYTES = (STAGE == ST_ANA ? 2 : 1) * KC * TM * 8;
-  static constexpr int NDST = STAGE == ST_ANA ? 2 : 4;  // A digit stages
+  static constexpr int NRAW = TWO ? 2 : 3;  // raw FP64 chunks in flight
+  static constexpr int RAW_BYTES = (TWO ? 2 : 1) * KC * TM * 8;
+  static constexpr int NDST = TWO ? 2 : 4;  // A digit stages
   static constexpr int NB = 4;                          // B digit stages
   static constexpr size_t RAW_OFF = 0;
   static constexpr size_t A_OFF = RAW_OFF + (size_t)NRAW * RAW_BYTES;
@@ -277,22 +302,25 @@ struct Ring {
 };
 static_assert(Ring<ST_SYNTH>::SMEM <= 227 * 1024, "synthesis ring");
 static_assert(Ring<ST_ANA>::SMEM <= 227 * 1024, "analysis ring");
+static_assert(Ring<ST_INV, true>::SMEM <= 227 * 1024, "inverse ring with the toroidal partner rows");
 static_assert(Ring<ST_SYNTH>::SMEM > 114 * 1024 && Ring<ST_ANA>::SMEM > 114 * 1024,
               "one CTA per SM: the tensor-memory plan takes 480 of its 512 columns");
 }  // namespace p
 
-template <int STAGE>
+template <int STAGE, bool TOR>
 __device__ __forceinline__ int tile_count(const Args& A) {
-  if (STAGE == ST_SYNTH) return ((A.NC + TM - 1) / TM) * A.nts * (A.L + 1) * 6;
-  if (STAGE == ST_ANA) return ((A.NC + TM - 1) / TM) * A.nta * (A.L + 1) * 6;
+  constexpr int NTY = TOR ? 10 : 6;
+  if (STAGE == ST_SYNTH) return ((A.NC + TM - 1) / TM) * A.nts * (A.L + 1) * NTY;
+  if (STAGE == ST_ANA) return ((A.NC + TM - 1) / TM) * A.nta * (A.L + 1) * NTY;
   if (STAGE == ST_INV) return ((A.NCOL + TM - 1) / TM) * A.nti * A.nlat;
   return ((A.NCOL + TM - 1) / TM) * A.ntf * A.nlat;
 }
 
 // tile t -> (row tile, N tile, batch): the row tile fastest, so the CTAs that
 // share a batch's B images and A rows run close together
-template <int STAGE>
+template <int STAGE, bool TOR>
 __device__ __forceinline__ Cta tile_info(const Args& A, int t) {
+  constexpr int NTY = TOR ? 10 : 6;
   Cta c;
   const int rt_n = (STAGE == ST_SYNTH || STAGE == ST_ANA) ? (A.NC + TM - 1) / TM : (A.NCOL + TM - 1) / TM;
   const int nt_count = STAGE == ST_SYNTH ? A.nts : (STAGE == ST_ANA ? A.nta : (STAGE == ST_INV ? A.nti : A.ntf));
@@ -301,11 +329,12 @@ __device__ __forceinline__ Cta tile_info(const Args& A, int t) {
   const int bz = rest / nt_count;
   c.row0 = rt * TM;
   if (STAGE == ST_SYNTH || STAGE == ST_ANA) {
-    c.batch_m = bz / 6;
-    c.p = bz % 6;
+    c.batch_m = bz / NTY;
+    c.p = bz % NTY;
     c.j = 0;
     c.rows = min(TM, A.NC - c.row0);
-    const int base = ((c.batch_m * 4 + table_of(c.p)) * 2) * nt_count;
+    const int tab = !TOR ? table_of(c.p) : (STAGE == ST_SYNTH ? syn_table(c.p) : ana_table(c.p));
+    const int base = ((c.batch_m * 4 + tab) * 2) * nt_count;
     c.sub[0] = A.info[base + c.nt];
     c.sub[1] = A.info[base + nt_count + c.nt];
   } else {
@@ -320,12 +349,17 @@ __device__ __forceinline__ Cta tile_info(const Args& A, int t) {
 }
 
 // the group exponent of a tile row (analysis rows: + 1, the E / O bound)
-template <int STAGE>
+template <int STAGE, bool TOR>
 __device__ __forceinline__ int row_exp(const Args& A, const Cta& c, int row) {
-  if (STAGE == ST_SYNTH) return group_exp(A.gX[chan_of(c.p) * A.NC + row]);
-  if (STAGE == ST_INV) return group_exp(A.gS[row]);  // rows (p, f) = p F + f
+  if (STAGE == ST_SYNTH) return group_exp(A.gX[(TOR ? syn_chan(c.p) : chan_of(c.p)) * A.NC + row]);
+  if (STAGE == ST_INV) {  // rows (p, f) = p F + f; with the toroidal channels plus the partner slot's bound
+    if (!TOR) return group_exp(A.gS[row]);
+    const double s = __longlong_as_double((long long)A.gS[row]) +
+                     __longlong_as_double((long long)A.gS[row + 6 * A.F]);
+    return group_exp((unsigned long long)__double_as_longlong(s));
+  }
   if (STAGE == ST_FWD) return group_exp(A.gG[row]);
-  return group_exp(A.gA[c.p * A.NC + row]) + 1;
+  return group_exp(A.gA[(TOR ? ana_group(c.p) : c.p) * A.NC + row]) + 1;
 }
 
 // K values of chunk (sub, kc) with data: K index k of the chunk is valid if
@@ -347,10 +381,11 @@ __device__ __forceinline__ int valid_k(const Args& A, const Cta& c, int sub, int
   return max(0, min(KC, kmax - kc * KC));
 }
 
-template <int STAGE, int NCW>
+template <int STAGE, int NCW, bool TOR = false>
 __global__ void __launch_bounds__(p::NTHR, 1) k_ozp_stage(const __grid_constant__ Args A) {
-  using R = p::Ring<STAGE>;
+  using R = p::Ring<STAGE, STAGE == ST_ANA || (STAGE == ST_INV && TOR)>;
   using Q = p::Roles<NCW>;
+  constexpr int NSL = TOR ? 12 : 6, NQO = TOR ? 10 : 6;  // product slots of S, analysis outputs per slot
   extern __shared__ unsigned char smraw[];
   unsigned char* sm = (unsigned char*)(((uintptr_t)smraw + 1023) & ~(uintptr_t)1023);
   unsigned char* raw = sm + R::RAW_OFF;
@@ -372,7 +407,7 @@ __global__ void __launch_bounds__(p::NTHR, 1) k_ozp_stage(const __grid_constant_
   volatile int* abort_flag = (volatile int*)(tslot + 1);
 
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  const int ntile = tile_count<STAGE>(A);
+  const int ntile = tile_count<STAGE, TOR>(A);
   constexpr bool SIDE = (STAGE == ST_INV || STAGE == ST_FWD);
 
   if (tid == 0) {
@@ -410,7 +445,7 @@ __global__ void __launch_bounds__(p::NTHR, 1) k_ozp_stage(const __grid_constant_
     int last_b = -1;  // B copies issued: chunk ids 0 .. last_b (for the exit wait)
     bool stop = false;
     for (int t = blockIdx.x; t < ntile && !stop; t += gridDim.x) {
-      const Cta c = tile_info<STAGE>(A, t);
+      const Cta c = tile_info<STAGE, TOR>(A, t);
       const int nch0 = c.sub[0].kpad / KC, nch = nch0 + c.sub[1].kpad / KC;
       if (nch == 0 || c.rows <= 0) continue;
       for (int ch = 0; ch < nch; ++ch, ++gc) {
@@ -443,20 +478,22 @@ __global__ void __launch_bounds__(p::NTHR, 1) k_ozp_stage(const __grid_constant_
             // lm = mbeg[m] + sub + 2 kk = 2 q + par
             const int lm0 = __ldg(&A.mbeg[c.batch_m]) + sub + 2 * kc * KC;
             mbar_expect_tx(&raw_full[rs], (uint32_t)R::RAW_BYTES);
-            tma_load_4d(rdst, &A.tmap, c.row0, chan_of(c.p), lm0 & 1, lm0 >> 1, &raw_full[rs]);
+            tma_load_4d(rdst, &A.tmap, c.row0, TOR ? syn_chan(c.p) : chan_of(c.p), lm0 & 1, lm0 >> 1, &raw_full[rs]);
           } else if (STAGE == ST_INV) {
             // m = 2 mq + mpar: even orders from 2 (sub 0), odd orders from 1 (sub 1)
             const int mq0 = (sub ? 0 : 1) + kc * (KC / 2);
             mbar_expect_tx(&raw_full[rs], (uint32_t)R::RAW_BYTES);
             tma_load_4d(rdst, &A.tmap, 2 * c.row0, c.j, sub, mq0, &raw_full[rs]);
+            if (TOR && STAGE == ST_INV)  // the partner slots' rows (6 F further), after the tile's own
+              tma_load_4d(rdst + (size_t)KC * TM * 8, &A.tmap, 2 * (c.row0 + 6 * A.F), c.j, sub, mq0, &raw_full[rs]);
           } else if (STAGE == ST_FWD) {
             mbar_expect_tx(&raw_full[rs], (uint32_t)R::RAW_BYTES);
             tma_load_4d(rdst, &A.tmap, c.row0, kc * KC, 2 * c.j + sub, 0, &raw_full[rs]);
           } else {
             const int j0 = kc * KC, jm0 = A.nlat - KC - j0;  // mirrors of j0 .. j0 + 31, ascending
             mbar_expect_tx(&raw_full[rs], (uint32_t)R::RAW_BYTES);
-            tma_load_4d(rdst, &A.tmap, c.row0, c.p, j0, c.batch_m, &raw_full[rs]);
-            tma_load_4d(rdst + (size_t)KC * TM * 8, &A.tmap, c.row0, c.p, jm0, c.batch_m, &raw_full[rs]);
+            tma_load_4d(rdst, &A.tmap, c.row0, TOR ? ana_src(c.p) : c.p, j0, c.batch_m, &raw_full[rs]);
+            tma_load_4d(rdst + (size_t)KC * TM * 8, &A.tmap, c.row0, TOR ? ana_src(c.p) : c.p, jm0, c.batch_m, &raw_full[rs]);
           }
         }
         __syncwarp();
@@ -487,7 +524,7 @@ __global__ void __launch_bounds__(p::NTHR, 1) k_ozp_stage(const __grid_constant_
       int gc = 0, gt = 0;
       bool stop = false;
       for (int t = blockIdx.x; t < ntile && !stop; t += gridDim.x) {
-        const Cta c = tile_info<STAGE>(A, t);
+        const Cta c = tile_info<STAGE, TOR>(A, t);
         const int nch0 = c.sub[0].kpad / KC, nch = nch0 + c.sub[1].kpad / KC;
         if (nch == 0 || c.rows <= 0) continue;
         // the epilogue has read the previous tile's accumulators
@@ -540,12 +577,12 @@ __global__ void __launch_bounds__(p::NTHR, 1) k_ozp_stage(const __grid_constant_
     const int lr = ct % TM, g0 = ct / TM;  // row, first K group of 16
     int gc = 0, gt = 0;
     for (int t = blockIdx.x; t < ntile && !*abort_flag; t += gridDim.x) {
-      const Cta c = tile_info<STAGE>(A, t);
+      const Cta c = tile_info<STAGE, TOR>(A, t);
       const int nch0 = c.sub[0].kpad / KC, nch = nch0 + c.sub[1].kpad / KC;
       if (nch == 0 || c.rows <= 0) continue;
       const bool live = lr < c.rows;
       const int row = c.row0 + lr;
-      const int e = live ? row_exp<STAGE>(A, c, row) : 0;
+      const int e = live ? row_exp<STAGE, TOR>(A, c, row) : 0;
       const double rs = pow2(FIX_BITS - e);
       const double is_j = (STAGE == ST_INV) ? A.invsin[c.j] : 0.0;
       const int prow = (STAGE == ST_INV) ? row / A.F : 0;
@@ -589,13 +626,34 @@ __global__ void __launch_bounds__(p::NTHR, 1) k_ozp_stage(const __grid_constant_
                   tre = -z.y;
                   tim = z.x;
                 }
+                if (TOR) {  // the partner slot: rt -= i (m/sin) P.X4, rp += D.X4, (tt - pp) -= i H.X5, tp += G.X5 / 4
+                  const double2 w = *reinterpret_cast<const double2*>(rv + (size_t)KC * TM + (size_t)mo * TM * 2 + 2 * lr);
+                  if (prow == 1) {
+                    const int m = (sub ? 1 : 2) + 2 * (kc * (KC / 2) + mo);
+                    const double a = (double)m * is_j;
+                    tre += a * w.y;
+                    tim -= a * w.x;
+                  } else if (prow == 2) {
+                    tre += w.x;
+                    tim += w.y;
+                  } else if (prow == 4) {
+                    tre += w.y;
+                    tim -= w.x;
+                  } else if (prow == 5) {
+                    tre += 0.25 * w.x;
+                    tim += 0.25 * w.y;
+                  }
+                }
                 sacc += 2.0 * tre;
               }
               v[q] = tre;
               v[q + 1] = (k + 1 < kv && live) ? tim : 0.0;
             }
           } else {
-            const double sg = (STAGE == ST_ANA) ? table_sigma(c.p) * (sub ? -1.0 : 1.0) : 0.0;
+            const double sg = (STAGE == ST_ANA) ? (TOR ? (double)tab_sign_idx(ana_table(c.p)) : table_sigma(c.p)) * (sub ? -1.0 : 1.0) : 0.0;
+            // with the toroidal channels the forward stage leaves rp without its m / sin theta: types 2
+            // ((m/sin) rp) and 7 ((m/sin) rt) apply it here, per latitude (the mirror has the same sin)
+            const bool msf = (STAGE == ST_ANA) && TOR && (c.p == 2 || c.p == 7);
 #pragma unroll
             for (int q = 0; q < 16; ++q) {
               const int k = 16 * g + q;
@@ -606,6 +664,7 @@ __global__ void __launch_bounds__(p::NTHR, 1) k_ozp_stage(const __grid_constant_
                   const double r0 = rv[(size_t)k * TM + lr];
                   const double r1 = (jm != j) ? rv[(size_t)(KC + KC - 1 - k) * TM + lr] : 0.0;
                   x = r0 + sg * r1;
+                  if (msf) x *= (double)c.batch_m * __ldg(&A.invsin[j]);
                 } else {
                   x = rv[(size_t)k * TM + lr];
                   if (STAGE == ST_FWD) sacc += x;
@@ -663,7 +722,7 @@ __global__ void __launch_bounds__(p::NTHR, 1) k_ozp_stage(const __grid_constant_
     const uint32_t tbase = tmem + ((uint32_t)(quad * 32) << 16);
     int gt = 0;
     for (int t = blockIdx.x; t < ntile; t += gridDim.x) {
-      const Cta c = tile_info<STAGE>(A, t);
+      const Cta c = tile_info<STAGE, TOR>(A, t);
       const int nch0 = c.sub[0].kpad / KC, nch1 = c.sub[1].kpad / KC;
       if (nch0 + nch1 == 0 || c.rows <= 0) continue;
       int ok = 1;
@@ -690,7 +749,7 @@ __global__ void __launch_bounds__(p::NTHR, 1) k_ozp_stage(const __grid_constant_
       const bool live = r < c.rows;
       const bool has0 = nch0 > 0, has1 = nch1 > 0;
       const int npad_max = max(has0 ? c.sub[0].npad : 0, has1 ? c.sub[1].npad : 0);
-      const double rf = pow2((live ? row_exp<STAGE>(A, c, row) : 0) - FIX_BITS);
+      const double rf = pow2((live ? row_exp<STAGE, TOR>(A, c, row) : 0) - FIX_BITS);
       auto load_block = [&](int sub, int cb, double* out) {
         const bool hs = sub ? has1 : has0;
         const int np = sub ? c.sub[1].npad : c.sub[0].npad;
@@ -729,8 +788,12 @@ __global__ void __launch_bounds__(p::NTHR, 1) k_ozp_stage(const __grid_constant_
         }
       };
       if (STAGE == ST_SYNTH) {
-        const int m = c.batch_m, pp = c.p;
-        const double sg = table_sigma(pp);
+        const int m = c.batch_m, pp = TOR ? syn_slot(c.p) : c.p;  // the product slot
+        const double sg = TOR ? (double)tab_sign_idx(syn_table(c.p)) : table_sigma(c.p);
+        // the group weights: the inverse stage's factor on this slot (m / sin theta on slots 2 and 7,
+        // 1 / 4 on slot 11)
+        const bool wms = (pp == 2 || (TOR && pp == 7));
+        const double wq = (TOR && pp == 11) ? 0.25 : 1.0;
         double gmax = 0.0;
         for (int cb = part * 4; cb < npad_max; cb += 4 * Q::NPART) {
           int a[2][NLEV][4];
@@ -741,8 +804,8 @@ __global__ void __launch_bounds__(p::NTHR, 1) k_ozp_stage(const __grid_constant_
 #pragma unroll
           for (int i = 0; i < 4; ++i) {  // the weights of the group maximum (m / sin theta for p = 2)
             const int j = min(c.nt * TN + cb + i, A.nh - 1), jm = A.nlat - 1 - j;
-            wn[i] = (pp == 2) ? (double)m * __ldg(&A.invsin[j]) : 1.0;
-            ws[i] = (pp == 2) ? (double)m * __ldg(&A.invsin[jm]) : 1.0;
+            wn[i] = wms ? (double)m * __ldg(&A.invsin[j]) : 1.0;
+            ws[i] = wms ? (double)m * __ldg(&A.invsin[jm]) : 1.0;
           }
           double ev[4], od[4];
           combine_pair4(cb, a, ev, od);
@@ -752,24 +815,29 @@ __global__ void __launch_bounds__(p::NTHR, 1) k_ozp_stage(const __grid_constant_
             if (j < A.nh) {
               const int jm = A.nlat - 1 - j;
               const double vn = ev[i] + od[i];
-              A.S[(((size_t)m * A.nlat + j) * 6 + pp) * A.NC + row] = vn;
+              A.S[(((size_t)m * A.nlat + j) * NSL + pp) * A.NC + row] = vn;
               gmax = fmax(gmax, fabs(vn) * wn[i]);
               if (jm != j) {
                 const double vs = sg * (ev[i] - od[i]);
-                A.S[(((size_t)m * A.nlat + jm) * 6 + pp) * A.NC + row] = vs;
+                A.S[(((size_t)m * A.nlat + jm) * NSL + pp) * A.NC + row] = vs;
                 gmax = fmax(gmax, fabs(vs) * ws[i]);
               }
             }
           }
         }
-        if (live) atomic_max_bits(&A.gS[pp * A.F + row / 2], gmax);
+        if (live) atomic_max_bits(&A.gS[pp * A.F + row / 2], gmax * wq);
       } else if (STAGE == ST_INV) {
         const int pp = row / A.F, f = row % A.F, e3 = f / 3;
-        double c0 = 0.0;  // m = 0 term (weight 1), the real part of z_0
+        double c0 = 0.0;  // m = 0 term (weight 1), the real part of z_0 (and of the partner slot's share)
         if (live && pp != 2) {
           const double2 z =
-              *reinterpret_cast<const double2*>(A.S + (((size_t)0 * A.nlat + c.j) * 6 + pp) * A.NC + 2 * f);
+              *reinterpret_cast<const double2*>(A.S + (((size_t)0 * A.nlat + c.j) * NSL + pp) * A.NC + 2 * f);
           c0 = (pp == 5) ? -z.y : z.x;
+        }
+        if (live && TOR) {
+          const double2 w =
+              *reinterpret_cast<const double2*>(A.S + (((size_t)0 * A.nlat + c.j) * NSL + pp + 6) * A.NC + 2 * f);
+          c0 += (pp == 2) ? w.x : (pp == 4 ? w.y : (pp == 5 ? 0.25 * w.x : 0.0));
         }
         const double* nm_j = A.nmdt + (size_t)c.j * A.nphi * A.ne3d + e3;
         double* gs = A.Gs + (size_t)c.j * 2 * A.half * A.NCOL + row;
@@ -812,14 +880,20 @@ __global__ void __launch_bounds__(p::NTHR, 1) k_ozp_stage(const __grid_constant_
         const double isj = A.invsin[c.j];
         const double beta_c = (pp == 3 || pp == 4) ? 2.0 : (pp == 5 ? 4.0 : 1.0);
         auto out = [&](int m) -> double2* {
-          return reinterpret_cast<double2*>(A.S + (((size_t)m * A.nlat + c.j) * 6 + pp) * A.NC + 2 * f);
+          return reinterpret_cast<double2*>(A.S + (((size_t)m * A.nlat + c.j) * NSL + pp) * A.NC + 2 * f);
         };
-        double gre = 0.0, gim = 0.0;
+        // with the toroidal channels rp is stored without m / sin theta (the analysis applies it) and
+        // rp, rt carry a second scale group: plain rp (type 6) and (m/sin) rt (type 7)
+        const bool tor2 = TOR && pp == 2, tor1 = TOR && pp == 1;
+        double gre = 0.0, gim = 0.0, hre = 0.0, him = 0.0;  // hre, him: the second group
         if (live && c.nt == 0 && part == 0) {
           // m = 0: F_0 = (2 pi / nphi) sum_i s_i, real
-          const double v = (pp == 2) ? 0.0 : beta_c * sev * (2.0 * PI / (double)A.nphi);
+          const double v = (pp == 2 && !tor2) ? 0.0 : beta_c * sev * (2.0 * PI / (double)A.nphi);
           *out(0) = make_double2(v, 0.0);
-          gre = fabs(v);
+          if (tor2)
+            hre = fabs(v);  // (m/sin) rp is zero at m = 0
+          else
+            gre = fabs(v);
         }
         for (int sub = 0; sub < 2; ++sub) {
           if (!(sub ? has1 : has0)) continue;
@@ -833,17 +907,34 @@ __global__ void __launch_bounds__(p::NTHR, 1) k_ozp_stage(const __grid_constant_
               const int kk = c.nt * TN + cb + i;  // (m, re) column; (m, im) follows
               if (kk >= c.nt * TN + nval) break;
               const int m = (sub ? 1 : 2) + 2 * (kk >> 1);
-              const double beta = (pp == 2) ? (double)m * isj : beta_c;
+              const double ms = (double)m * isj;
+              const double beta = (pp == 2 && !tor2) ? ms : beta_c;
               const double re = beta * v[i], im = beta * v[i + 1];
               *out(m) = make_double2(re, im);
-              gre = fmax(gre, fabs(re));
-              gim = fmax(gim, fabs(im));
+              if (tor2) {  // type 2 groups (m/sin) rp, type 6 plain rp
+                gre = fmax(gre, fabs(ms * re));
+                gim = fmax(gim, fabs(ms * im));
+                hre = fmax(hre, fabs(re));
+                him = fmax(him, fabs(im));
+              } else {
+                gre = fmax(gre, fabs(re));
+                gim = fmax(gim, fabs(im));
+                if (tor1) {  // type 7 groups (m/sin) rt
+                  hre = fmax(hre, fabs(ms * re));
+                  him = fmax(him, fabs(ms * im));
+                }
+              }
             }
           }
         }
         if (live) {
           atomic_max_bits(&A.gA[pp * A.NC + 2 * f], gre);
           atomic_max_bits(&A.gA[pp * A.NC + 2 * f + 1], gim);
+          if (tor1 || tor2) {
+            const int g2 = tor2 ? 6 : 7;
+            atomic_max_bits(&A.gA[g2 * A.NC + 2 * f], hre);
+            atomic_max_bits(&A.gA[g2 * A.NC + 2 * f + 1], him);
+          }
         }
       } else {
         const int m = c.batch_m, pp = c.p;
@@ -859,7 +950,7 @@ __global__ void __launch_bounds__(p::NTHR, 1) k_ozp_stage(const __grid_constant_
               const int kk = c.nt * TN + cb + i;
               const int l = m + sub + 2 * kk;
               if (l > A.L) break;
-              A.dy[((size_t)slot_row(A.kbeg, l, m, A.nk) * 6 + pp) * A.NC + row] = v[i];
+              A.dy[((size_t)slot_row(A.kbeg, l, m, A.nk) * NQO + pp) * A.NC + row] = v[i];
             }
           }
         }
@@ -1030,6 +1121,15 @@ void visc3d_oz_enable(vg_handle* h) {
   a.NCOL = NCOL;
   a.nk = h->nk;
   a.ne3d = h->ne3d;
+  // the toroidal channels: two more gathered channels, the partner product
+  // slots 6-11 of S, four more synthesis and analysis tile types
+  const bool tor = h->tor_on;
+  const int nch = tor ? 6 : 4;
+  a.tor = tor ? 1 : 0;
+  a.nslot = tor ? 12 : 6;
+  a.ntype = tor ? 10 : 6;
+  a.nq = tor ? 10 : 6;
+  const int NSLOT = a.nslot;
   const int TN = oz::TN, KC = oz::KC;
   a.nts = (nh + TN - 1) / TN;
   const int kev = 2 * (L / 2), kod = 2 * ((L + 1) / 2);  // (m, re/im) counts: even m >= 2, odd m
@@ -1111,11 +1211,14 @@ void visc3d_oz_enable(vg_handle* h) {
   // rows, the l = 0 row zero), the scatter reads dy; S has an even number of
   // order slabs (the inverse stage reads orders in pairs)
   const int nlm2 = (G.nlm + 1) / 2 * 2, M2 = (G.M + 1) / 2 * 2;
-  h->d_X.alloc((size_t)nlm2 * 4 * NC);
-  h->d_dy.alloc((size_t)(h->nk + 1) * 6 * NC);
-  P->S.alloc((size_t)M2 * nlat * 6 * NC);
+  h->d_X.alloc((size_t)nlm2 * nch * NC);
+  h->d_dy.alloc((size_t)(h->nk + 1) * a.nq * NC);
+  P->S.alloc((size_t)M2 * nlat * NSLOT * NC);  // zeroed: slots 6 and 9 (no toroidal partner) stay zero
   P->Gs.alloc((size_t)nlat * 2 * half * NCOL);
-  P->gmax_n = (size_t)4 * NC + 6 * F + 6 * F + 6 * NC;
+  // scale groups: gathered channels x columns, product slots x fields, the
+  // inverse outputs (components x fields), analysis inputs x columns (8 with
+  // the toroidal channels: plain rp and (m/sin) rt beside the six)
+  P->gmax_n = (size_t)nch * NC + (size_t)NSLOT * F + 6 * F + (size_t)(tor ? 8 : 6) * NC;
   P->gmax.alloc(P->gmax_n);
   a.kbeg = h->d_kbeg.p;
   a.mbeg = G.d_mbeg.p;
@@ -1129,8 +1232,8 @@ void visc3d_oz_enable(vg_handle* h) {
   a.img = P->img.p;
   a.bscale = P->bscale.p;
   a.gX = P->gmax.p;
-  a.gS = a.gX + 4 * NC;
-  a.gG = a.gS + 6 * F;
+  a.gS = a.gX + (size_t)nch * NC;
+  a.gG = a.gS + (size_t)NSLOT * F;
   a.gA = a.gG + 6 * F;
   a.status = h->d_maxbits.p + 2;
   P->ntile_rows_nc = (NC + oz::TM - 1) / oz::TM;
@@ -1143,6 +1246,14 @@ void visc3d_oz_enable(vg_handle* h) {
   raise_smem_limit((const void*)oz::k_ozp_stage<oz::ST_INV, 4>, oz::p::Ring<oz::ST_INV>::SMEM);
   raise_smem_limit((const void*)oz::k_ozp_stage<oz::ST_FWD, 4>, oz::p::Ring<oz::ST_FWD>::SMEM);
   raise_smem_limit((const void*)oz::k_ozp_stage<oz::ST_ANA, 4>, oz::p::Ring<oz::ST_ANA>::SMEM);
+  raise_smem_limit((const void*)oz::k_ozp_stage<oz::ST_SYNTH, 8, true>, oz::p::Ring<oz::ST_SYNTH>::SMEM);
+  raise_smem_limit((const void*)oz::k_ozp_stage<oz::ST_INV, 8, true>, oz::p::Ring<oz::ST_INV, true>::SMEM);
+  raise_smem_limit((const void*)oz::k_ozp_stage<oz::ST_FWD, 8, true>, oz::p::Ring<oz::ST_FWD>::SMEM);
+  raise_smem_limit((const void*)oz::k_ozp_stage<oz::ST_ANA, 8, true>, oz::p::Ring<oz::ST_ANA>::SMEM);
+  raise_smem_limit((const void*)oz::k_ozp_stage<oz::ST_SYNTH, 4, true>, oz::p::Ring<oz::ST_SYNTH>::SMEM);
+  raise_smem_limit((const void*)oz::k_ozp_stage<oz::ST_INV, 4, true>, oz::p::Ring<oz::ST_INV, true>::SMEM);
+  raise_smem_limit((const void*)oz::k_ozp_stage<oz::ST_FWD, 4, true>, oz::p::Ring<oz::ST_FWD>::SMEM);
+  raise_smem_limit((const void*)oz::k_ozp_stage<oz::ST_ANA, 4, true>, oz::p::Ring<oz::ST_ANA>::SMEM);
   int dev = 0;
   VG_CUDA(cudaGetDevice(&dev));
   VG_CUDA(cudaDeviceGetAttribute(&P->nsm, cudaDevAttrMultiProcessorCount, dev));
@@ -1150,13 +1261,15 @@ void visc3d_oz_enable(vg_handle* h) {
     const cuuint64_t B = sizeof(double);
     const cuuint32_t TMr = oz::TM, KCc = oz::KC;
     // synthesis: X[lm][chan][n], lm = 2 q + par
-    const cuuint64_t dx[4] = {(cuuint64_t)NC, 4, 2, (cuuint64_t)nlm2 / 2};
-    const cuuint64_t sx[3] = {NC * B, 4 * NC * B, 8 * NC * B};
+    const cuuint64_t dx[4] = {(cuuint64_t)NC, (cuuint64_t)nch, 2, (cuuint64_t)nlm2 / 2};
+    const cuuint64_t sx[3] = {NC * B, (cuuint64_t)nch * NC * B, 2 * (cuuint64_t)nch * NC * B};
     const cuuint32_t bx[4] = {TMr, 1, 1, KCc};
     encode_map(&P->tm[0], h->d_X.p, dx, sx, bx);
-    // inverse: S[m][j][(p, f, ri)], m = 2 mq + mpar
-    const cuuint64_t di[4] = {(cuuint64_t)6 * NC, (cuuint64_t)nlat, 2, (cuuint64_t)M2 / 2};
-    const cuuint64_t si[3] = {6 * NC * B, (cuuint64_t)nlat * 6 * NC * B, 2 * (cuuint64_t)nlat * 6 * NC * B};
+    // inverse: S[m][j][(p, f, ri)], m = 2 mq + mpar (with the toroidal channels the partner slots
+    // follow at 6 F rows)
+    const cuuint64_t di[4] = {(cuuint64_t)NSLOT * NC, (cuuint64_t)nlat, 2, (cuuint64_t)M2 / 2};
+    const cuuint64_t si[3] = {(cuuint64_t)NSLOT * NC * B, (cuuint64_t)nlat * NSLOT * NC * B,
+                              2 * (cuuint64_t)nlat * NSLOT * NC * B};
     const cuuint32_t bi[4] = {2 * TMr, 1, 1, KCc / 2};
     encode_map(&P->tm[1], P->S.p, di, si, bi);
     // forward: Gs[(j, sub)][i][row]
@@ -1165,15 +1278,15 @@ void visc3d_oz_enable(vg_handle* h) {
     const cuuint32_t bg[4] = {TMr, KCc, 1, 1};
     encode_map(&P->tm[2], P->Gs.p, dg, sg, bg);
     // analysis: S[m][j][p][n]
-    const cuuint64_t da[4] = {(cuuint64_t)NC, 6, (cuuint64_t)nlat, (cuuint64_t)G.M};
-    const cuuint64_t sa[3] = {NC * B, 6 * NC * B, (cuuint64_t)nlat * 6 * NC * B};
+    const cuuint64_t da[4] = {(cuuint64_t)NC, (cuuint64_t)NSLOT, (cuuint64_t)nlat, (cuuint64_t)G.M};
+    const cuuint64_t sa[3] = {NC * B, (cuuint64_t)NSLOT * NC * B, (cuuint64_t)nlat * NSLOT * NC * B};
     const cuuint32_t ba[4] = {TMr, 1, KCc, 1};
     encode_map(&P->tm[3], P->S.p, da, sa, ba);
   }
-  P->tiles[0] = P->ntile_rows_nc * a.nts * G.M * 6;
+  P->tiles[0] = P->ntile_rows_nc * a.nts * G.M * a.ntype;
   P->tiles[1] = P->ntile_rows_col * a.nti * nlat;
   P->tiles[2] = P->ntile_rows_col * a.ntf * nlat;
-  P->tiles[3] = P->ntile_rows_nc * a.nta * G.M * 6;
+  P->tiles[3] = P->ntile_rows_nc * a.nta * G.M * a.ntype;
   VG_CUDA(cudaStreamSynchronize(s));
 }
 
@@ -1234,22 +1347,30 @@ void visc3d_oz_run(vg_handle* h, double dt, bool trap) {
     VG_CUDA(cudaGetLastError());
   };
   using namespace oz;
-  if (P->ncw[0] == 4)
-    launch(k_ozp_stage<ST_SYNTH, 4>, VG_PH_V3_SYNTH, P->info_synth.p, P->tiles[0], p::Ring<ST_SYNTH>::SMEM);
-  else
-    launch(k_ozp_stage<ST_SYNTH, 8>, VG_PH_V3_SYNTH, P->info_synth.p, P->tiles[0], p::Ring<ST_SYNTH>::SMEM);
-  if (P->ncw[1] == 4)
-    launch(k_ozp_stage<ST_INV, 4>, VG_PH_V3_LON_INV, P->info_inv.p, P->tiles[1], p::Ring<ST_INV>::SMEM);
-  else
-    launch(k_ozp_stage<ST_INV, 8>, VG_PH_V3_LON_INV, P->info_inv.p, P->tiles[1], p::Ring<ST_INV>::SMEM);
-  if (P->ncw[2] == 4)
-    launch(k_ozp_stage<ST_FWD, 4>, VG_PH_V3_LON_FWD, P->info_fwd.p, P->tiles[2], p::Ring<ST_FWD>::SMEM);
-  else
-    launch(k_ozp_stage<ST_FWD, 8>, VG_PH_V3_LON_FWD, P->info_fwd.p, P->tiles[2], p::Ring<ST_FWD>::SMEM);
-  if (P->ncw[3] == 4)
-    launch(k_ozp_stage<ST_ANA, 4>, VG_PH_V3_ANALYSIS, P->info_ana.p, P->tiles[3], p::Ring<ST_ANA>::SMEM);
-  else
-    launch(k_ozp_stage<ST_ANA, 8>, VG_PH_V3_ANALYSIS, P->info_ana.p, P->tiles[3], p::Ring<ST_ANA>::SMEM);
+  // every stage in its converter-warp split; the toroidal instantiations carry the partner slots
+  auto stage_k = [&](auto k8, auto k4, int i, int phase, const ImgInfo* info, size_t smem) {
+    if (P->ncw[i] == 4)
+      launch(k4, phase, info, P->tiles[i], smem);
+    else
+      launch(k8, phase, info, P->tiles[i], smem);
+  };
+  if (a.tor) {
+    stage_k(k_ozp_stage<ST_SYNTH, 8, true>, k_ozp_stage<ST_SYNTH, 4, true>, 0, VG_PH_V3_SYNTH, P->info_synth.p,
+            p::Ring<ST_SYNTH>::SMEM);
+    stage_k(k_ozp_stage<ST_INV, 8, true>, k_ozp_stage<ST_INV, 4, true>, 1, VG_PH_V3_LON_INV, P->info_inv.p,
+            p::Ring<ST_INV, true>::SMEM);
+    stage_k(k_ozp_stage<ST_FWD, 8, true>, k_ozp_stage<ST_FWD, 4, true>, 2, VG_PH_V3_LON_FWD, P->info_fwd.p,
+            p::Ring<ST_FWD>::SMEM);
+    stage_k(k_ozp_stage<ST_ANA, 8, true>, k_ozp_stage<ST_ANA, 4, true>, 3, VG_PH_V3_ANALYSIS, P->info_ana.p,
+            p::Ring<ST_ANA>::SMEM);
+  } else {
+    stage_k(k_ozp_stage<ST_SYNTH, 8>, k_ozp_stage<ST_SYNTH, 4>, 0, VG_PH_V3_SYNTH, P->info_synth.p,
+            p::Ring<ST_SYNTH>::SMEM);
+    stage_k(k_ozp_stage<ST_INV, 8>, k_ozp_stage<ST_INV, 4>, 1, VG_PH_V3_LON_INV, P->info_inv.p, p::Ring<ST_INV>::SMEM);
+    stage_k(k_ozp_stage<ST_FWD, 8>, k_ozp_stage<ST_FWD, 4>, 2, VG_PH_V3_LON_FWD, P->info_fwd.p, p::Ring<ST_FWD>::SMEM);
+    stage_k(k_ozp_stage<ST_ANA, 8>, k_ozp_stage<ST_ANA, 4>, 3, VG_PH_V3_ANALYSIS, P->info_ana.p,
+            p::Ring<ST_ANA>::SMEM);
+  }
 }
 
 }  // namespace vg

@@ -695,9 +695,9 @@ void visc3d_enable(vg_handle* h, const double* pert) {
   cudaStream_t s = h->stream;
   if (G.nphi % 2 != 0) throw Error("vg_enable_visc3d: the longitude pass needs an even nphi");
   if (h->lat_visc) throw Error("vg_enable_visc3d: lateral viscosity is already enabled for this handle");
-  if (h->p.toroidal && h->p.visc3d_precision != VG_VISC3D_FP64)
-    throw Error("vg_enable_visc3d: the toroidal channels are carried on the FP64 3-D path only "
-                "(toroidal = 1 needs visc3d_precision = VG_VISC3D_FP64)");
+  if (h->p.toroidal && h->p.visc3d_precision == VG_VISC3D_SPLIT_TC)
+    throw Error("vg_enable_visc3d: the toroidal channels are carried on the FP64 and exact tensor-core 3-D paths "
+                "(toroidal = 1 needs visc3d_precision = VG_VISC3D_FP64 or VG_VISC3D_EXACT_TC)");
   // Maxwell-CFL rate: the grid maximum of mu/eta_eff over every Maxwell element
   // (src/vilma_response.f90:1783-1793, MkPerDt3 covers all elements)
   double rate_max = 0.0;
@@ -831,14 +831,20 @@ void visc3d_advance(vg_handle* h, const double* d_sigma, double dt, const double
       PhaseScope pg(h, VG_PH_V3_GATHER);
       A.gmax = visc3d_oz_gather_max(h);  // zeroes every scale group of the advance
       A.lm_rows = 1;
-      k_v3_gather<double, 4><<<gg, dim3(32, 8), v3_gather_smem<double>(), s>>>(A, h->d_X.p);
+      if (h->tor_on)
+        k_v3_gather<double, 6><<<gg, dim3(32, 8), v3_gather_smem<double, 6>(), s>>>(A, h->d_X.p);
+      else
+        k_v3_gather<double, 4><<<gg, dim3(32, 8), v3_gather_smem<double>(), s>>>(A, h->d_X.p);
       ++h->n_launch;
       VG_CUDA(cudaGetLastError());
       A.gmax = nullptr;
     }
     visc3d_oz_run(h, dt, trap);
     PhaseScope pc(h, VG_PH_V3_SCATTER);
-    k_v3_scatter<double><<<gg, dim3(32, 8), 0, s>>>(A, h->d_dy.p, h->d_n6.p);
+    if (h->tor_on)
+      k_v3_scatter<double, 10><<<gg, dim3(32, 8), 0, s>>>(A, h->d_dy.p, h->d_n6.p);
+    else
+      k_v3_scatter<double><<<gg, dim3(32, 8), 0, s>>>(A, h->d_dy.p, h->d_n6.p);
     ++h->n_launch;
     VG_CUDA(cudaGetLastError());
     return;

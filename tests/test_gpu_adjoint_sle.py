@@ -21,7 +21,7 @@ from oracle import orc
 
 pytestmark = pytest.mark.gpu
 
-LMAX, NE, DT, NSTEPS, NSITE, FIRST = 24, 30, 50.0, 8, 60, 160
+LMAX, NE, DT, NSTEPS, NSITE, FIRST = 32, 40, 50.0, 8, 60, 160
 TOL = 1e-6
 
 
