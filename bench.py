@@ -679,6 +679,8 @@ def main():
     tf32 = (run_arm(w, PRECISION["split_tc"], args, ice_dev, local, dist, False)
             if prec == "exact_tc" and args.tf32 == "on" else None)
     tor = run_arm(w, 0, args, ice_dev, local, dist, False, True) if w.visc3d and args.toroidal == "on" else None
+    tor_ex = (run_arm(w, PRECISION["exact_tc"], args, ice_dev, local, dist, False, True)
+              if tor is not None and prec == "exact_tc" else None)
     if rank != 0:
         if dist:
             dist.destroy_process_group()
@@ -740,6 +742,12 @@ def main():
             "ms_per_step": tor["ms"] / args.steps, "gpu_launches": int(tor["launches"]), "n_sub": tor["info"].n_sub_last,
             "cost_vs_spheroidal_fp64": (tor["ms"] / ref["ms"]) if ref is not None else None,
             "phases": phases_of(tor), "clocks": tor["clocks"]}
+        if tor_ex is not None:
+            out["toroidal_exact"] = {
+                "value": replica_throughput(world, args.steps, tor_ex["ms"]), "unit": "steps/s",
+                "ms_per_step": tor_ex["ms"] / args.steps, "speedup_over_toroidal_fp64": tor["ms"] / tor_ex["ms"],
+                "error_vs_toroidal_fp64": error_vs(tor_ex, tor), "tuning": tor_ex["tuning"],
+                "phases": phases_of(tor_ex), "clocks": tor_ex["clocks"]}
     if args.grad_fwd == "on":
         out["grad_fwd_response"] = measure_grad_fwd(w)
         if w.sle:

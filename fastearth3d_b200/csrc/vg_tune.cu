@@ -35,9 +35,9 @@ const int PH_STAGE[4] = {VG_PH_V3_SYNTH, VG_PH_V3_LON_INV, VG_PH_V3_LON_FWD, VG_
 
 std::string tune_key(const vg_handle* h, int knobs) {
   char k[220];
-  std::snprintf(k, sizeof(k), "lmax=%d nlat=%d nphi=%d ne=%d ne3d=%d precision=%d sle=%d knobs=%d", h->grid.lmax,
-                h->grid.nlat, h->grid.nphi, h->ne, h->lat_visc ? h->ne3d : 0, h->p.visc3d_precision,
-                h->p.sle_fixed_ocean ? 0 : 1, knobs);
+  std::snprintf(k, sizeof(k), "lmax=%d nlat=%d nphi=%d ne=%d ne3d=%d precision=%d toroidal=%d sle=%d knobs=%d",
+                h->grid.lmax, h->grid.nlat, h->grid.nphi, h->ne, h->lat_visc ? h->ne3d : 0, h->p.visc3d_precision,
+                h->tor_on ? 1 : 0, h->p.sle_fixed_ocean ? 0 : 1, knobs);
   return k;
 }
 

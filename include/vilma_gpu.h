@@ -398,8 +398,8 @@ int vg_sht_analysis_noalloc(vg_handle* h, const double* d_f, double* d_q_lm, int
  * and epilogue (8 : 8 or 4 : 12, per stage) and the fused sea-level loop's CTA
  * count (one per SM, one per Gauss row, two per SM). The fastest choices are
  * applied to the handle and appended to the text file cache_path (NULL: no
- * cache), keyed by lmax, grid, elements, 3-D elements, precision, ocean and
- * knobs;
+ * cache), keyed by lmax, grid, elements, 3-D elements, precision, toroidal
+ * channels, ocean and knobs;
  * a later call for a model of the same key reads them from there instead of
  * timing (*from_cache = 1). Needs vg_set_reference first. */
 #define VG_TUNE_STAGES 1 /* the exact stages' warp splits */
