@@ -713,6 +713,14 @@ void DriverSnap::save(vg_handle* h) {
   grab(C, h->d_C.p, ng);
   grab(zbed, h->d_zbed.p, ng);
   grab(sig, h->d_sigma.p, n2);
+  if (h->tor_on) grab(tmem, h->d_tmem[cur].p, h->d_tmem[cur].n);
+  sigma_primed = h->sigma_primed;
+  dt_try = h->dt_try;
+  if (h->d_sigma_n.p) grab(sig_n, h->d_sigma_n.p, h->d_sigma_n.n);
+  if (h->rot_on) {
+    grab(rot_sc, h->d_rot_sc.p, h->d_rot_sc.n);
+    grab(rot_mem, h->d_rot_mem.p, h->d_rot_mem.n);
+  }
   if (maxbits.n < 2) maxbits.alloc(2);
   VG_CUDA(cudaMemcpyAsync(maxbits.p, h->d_maxbits.p, 2 * sizeof(unsigned long long), cudaMemcpyDeviceToDevice, s));
   time_s = h->time_s;
@@ -743,6 +751,14 @@ void DriverSnap::restore(vg_handle* h) {
   put(h->d_C.p, C, ng);
   put(h->d_zbed.p, zbed, ng);
   put(h->d_sigma.p, sig, n2);
+  if (h->tor_on) put(h->d_tmem[cur].p, tmem, h->d_tmem[cur].n);
+  h->sigma_primed = sigma_primed;
+  h->dt_try = dt_try;
+  if (h->d_sigma_n.p && sig_n.n >= h->d_sigma_n.n) put(h->d_sigma_n.p, sig_n, h->d_sigma_n.n);
+  if (h->rot_on) {
+    put(h->d_rot_sc.p, rot_sc, h->d_rot_sc.n);
+    put(h->d_rot_mem.p, rot_mem, h->d_rot_mem.n);
+  }
   VG_CUDA(cudaMemcpyAsync(h->d_maxbits.p, maxbits.p, 2 * sizeof(unsigned long long), cudaMemcpyDeviceToDevice, s));
   h->time_s = time_s;
   h->time_yr = time_yr;

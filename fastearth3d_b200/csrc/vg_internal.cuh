@@ -302,14 +302,21 @@ void visc3d_adjoint(vg_handle* h, const double* gstore, double dt, const double*
 // oz_get_ncw returns false when the handle has no exact-stage plan
 void oz_set_ncw(vg_handle* h, const int ncw[4]);
 bool oz_get_ncw(const vg_handle* h, int ncw[4]);
-// The interval driver's state (memory of the current buffer, its per-slot
-// norms and both buffers' maxima, rsl, entering ice, ocean function, z_bed, the last load spectrum,
-// clocks and counters), saved and put back by the entry points that run
-// trial intervals (the coupled adjoint, the autotuner); vg_api.cu
+// The interval driver's state (memory of the current buffer, spheroidal and
+// toroidal, its per-slot norms and both buffers' maxima, rsl, entering ice,
+// ocean function, z_bed, the last load spectrum, the trapezoidal scheme's
+// carried step and sigma_n, the rotational feedback's state, clocks and
+// counters), saved and put back by the entry points that run trial intervals
+// (the coupled adjoint, the autotuner); vg_api.cu
 struct DriverSnap {
   DArr<double> mem, mnorm, rsl, hice, C, zbed, sig;
+  DArr<double> tmem;                 // the toroidal memory of the current buffer (toroidal channels)
+  DArr<double> sig_n;                // the trapezoidal scheme's sigma_n
+  DArr<double> rot_sc, rot_mem;      // rotational feedback: polar motion and scalars, channel memories
   DArr<unsigned long long> maxbits;  // both buffers' max |memory| (the drift skip gate's scale)
   int cur = 0;
+  bool sigma_primed = false;
+  double dt_try = 0;
   double time_s = 0, time_yr = 0, mem_norm = 0, bsl = 0, worst = 0;
   long long n_accept = 0, n_reject = 0, n_solve = 0;
   int n_sub = 0, n_outer = 0, n_inner = 0, n_flip = 0;

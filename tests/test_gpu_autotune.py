@@ -104,3 +104,35 @@ def test_tuned_full_size_workload_continues_bit_for_bit(tmp_path):
         b.update(w.ice_at(s), w.dt_yr)
     for x, y in zip(a.fields()[:3], b.fields()[:3]):
         assert np.array_equal(x, y)
+
+
+@pytest.mark.parametrize("toroidal,scheme", [(1, 0), (0, 2), (1, 2)])
+def test_tuning_keeps_toroidal_and_trapezoidal_state(tmp_path, toroidal, scheme):
+    """Tuning from a state that carries the toroidal memory or the
+    trapezoidal scheme's carried step and sigma_n puts those back too: the
+    tuned handle continues bit for bit like an untuned one."""
+    w = workload()
+
+    def build():
+        p = w.params(vlib.default_params)
+        p.visc3d_precision = VG_VISC3D_EXACT_TC
+        p.toroidal = toroidal
+        p.scheme = scheme
+        m = vlib.Model(p)
+        m.set_reference(*w.reference())
+        m.enable_visc3d(w.pert(m.p))
+        for s in (100, 101):
+            m.update(w.ice_at(s), w.dt_yr)
+        return m
+
+    a, b = build(), build()
+    a.autotune(w.dt_yr, tmp_path / "tune.txt")
+    for s in range(102, 106):
+        a.update(w.ice_at(s), w.dt_yr)
+        b.update(w.ice_at(s), w.dt_yr)
+    assert np.array_equal(a.fields()[0], b.fields()[0])
+    for x, y in zip(a.state()[0], b.state()[0]):
+        assert np.array_equal(x, y)
+    if toroidal:
+        for x, y in zip(a.state_tor(), b.state_tor()):
+            assert np.array_equal(x, y)
