@@ -44,11 +44,31 @@ struct RotArgs {
 // per (channel, re/im); the dissipative right-hand side in the reference's
 // element order (src/vilma_viscoelastic.f90:441-480), then the equilibrated
 // band solve (src/vilma_radial_fe.f90:578-605).
-__global__ void k_rot_begin(RotArgs A) {
+// With shared memory to spare (rot_smem below) the degree-2 band factor, its
+// pivots and the four right-hand sides are staged there by the whole warp
+// first, so that the four sequential sweeps read on-chip memory; the
+// arithmetic and its order are the same either way.
+__global__ void k_rot_begin(RotArgs A, int staged) {
+  extern __shared__ double rsm[];
   const int t = threadIdx.x;
+  const int ne = A.ne, nr = A.nr, nd = A.nd;
+  const double* ab = A.ab;
+  const int* ipiv = A.ipiv;
+  double* fbase = A.f;
+  if (staged) {
+    double* sab = rsm;                                       // [nd][VG_LDAB]
+    double* sf = sab + (size_t)nd * VG_LDAB;                 // [4][nd]
+    int* sip = reinterpret_cast<int*>(sf + (size_t)4 * nd);  // [nd]
+    for (int i = t; i < nd * VG_LDAB; i += blockDim.x) sab[i] = A.ab[i];
+    for (int i = t; i < nd; i += blockDim.x) sip[i] = A.ipiv[i];
+    __syncthreads();
+    ab = sab;
+    ipiv = sip;
+    fbase = sf;
+  }
   if (t >= 4) return;
-  const int ch = t >> 1, ri = t & 1, ne = A.ne, nr = A.nr, nd = A.nd;
-  double* f = A.f + (size_t)t * nd;
+  const int ch = t >> 1, ri = t & 1;
+  double* f = fbase + (size_t)t * nd;
   for (int i = 0; i < nd; ++i) f[i] = 0.0;
   const double* mem = A.mem + (size_t)ch * 6 * ne * 4;
   const double* Am = mem + (size_t)(0 * 2 + ri) * ne * 4;
@@ -79,7 +99,7 @@ __global__ void k_rot_begin(RotArgs A) {
     f[4 * (e + 1) + 1] += floc[3];
   }
   for (int i = 0; i < nd; ++i) f[i] = A.dr[i] * f[i];
-  band_solve_strided(A.ab, VG_LDAB, nd, 6, 12, A.ipiv, f, 1);
+  band_solve_strided(ab, VG_LDAB, nd, 6, 12, ipiv, f, 1);
   for (int i = 0; i < nd; ++i) f[i] = A.dc[i] * f[i];
   const int base = ch == 0 ? RS_DF_LOAD : RS_DF_TID;
   A.scal[base + ri] = f[4 * (nr - 1) + 2];      // dF
@@ -303,8 +323,18 @@ void rotation_setup(vg_handle* h) {
 }
 
 // rotation_begin_step (src/vilma_rotation.f90:154-168): drift of both channels
+// shared memory of the staged k_rot_begin (0: the band stays in global memory)
+static size_t rot_smem(const vg_handle* h) {
+  const size_t b = (size_t)h->ndof * VG_LDAB * sizeof(double) + (size_t)4 * h->ndof * sizeof(double) +
+                   (size_t)h->ndof * sizeof(int);
+  if (b > 200 * 1024) return 0;
+  raise_smem_limit((const void*)k_rot_begin, b);
+  return b;
+}
+
 void rotation_begin(vg_handle* h) {
-  k_rot_begin<<<1, 32, 0, h->stream>>>(rot_args(h));
+  const size_t sm = rot_smem(h);
+  k_rot_begin<<<1, 32, sm, h->stream>>>(rot_args(h), sm > 0 ? 1 : 0);
   ++h->n_launch;
   VG_CUDA(cudaGetLastError());
 }
@@ -344,8 +374,9 @@ void rotation_advance(vg_handle* h, const double* d_sigma, double dt) {
   S.w = G.d_wts.p;
   S.rows = h->d_rot_rows.p;
   const RotArgs A = rot_args(h);
+  const size_t sm = rot_smem(h);
   for (int k = 0; k < n_sub; ++k) {
-    k_rot_begin<<<1, 32, 0, s>>>(A);
+    k_rot_begin<<<1, 32, sm, s>>>(A, sm > 0 ? 1 : 0);
     k_rot_solve_commit<<<1, 256, 0, s>>>(A, S);
     h->n_launch += 2;
     VG_CUDA(cudaGetLastError());
