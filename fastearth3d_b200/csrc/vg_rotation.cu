@@ -44,38 +44,38 @@ struct RotArgs {
 // per (channel, re/im); the dissipative right-hand side in the reference's
 // element order (src/vilma_viscoelastic.f90:441-480), then the equilibrated
 // band solve (src/vilma_radial_fe.f90:578-605).
-// With shared memory to spare (rot_smem below) the degree-2 band factor, its
-// pivots and the four right-hand sides are staged there by the whole warp
-// first, so that the four sequential sweeps read on-chip memory; the
-// arithmetic and its order are the same either way.
+// The block computes the element contributions of all four right-hand sides
+// in parallel (one thread per (channel, re/im, element); the FP64 divisions
+// there were the kernel's cost) and stages the degree-2 band factor and its
+// pivots in shared memory when they fit (rot_smem below); then one thread per
+// right-hand side assembles the nodal forcing in the reference's order (node
+// n: element n-1's second test dof, then element n's first) and runs the
+// sequential sweeps. The arithmetic and its order are the reference's either way.
 __global__ void k_rot_begin(RotArgs A, int staged) {
   extern __shared__ double rsm[];
   const int t = threadIdx.x;
   const int ne = A.ne, nr = A.nr, nd = A.nd;
+  double* sfl = rsm;  // [4][ne][4] element contributions
   const double* ab = A.ab;
   const int* ipiv = A.ipiv;
   double* fbase = A.f;
   if (staged) {
-    double* sab = rsm;                                       // [nd][VG_LDAB]
+    double* sab = sfl + (size_t)16 * ne;                     // [nd][VG_LDAB]
     double* sf = sab + (size_t)nd * VG_LDAB;                 // [4][nd]
     int* sip = reinterpret_cast<int*>(sf + (size_t)4 * nd);  // [nd]
     for (int i = t; i < nd * VG_LDAB; i += blockDim.x) sab[i] = A.ab[i];
     for (int i = t; i < nd; i += blockDim.x) sip[i] = A.ipiv[i];
-    __syncthreads();
     ab = sab;
     ipiv = sip;
     fbase = sf;
   }
-  if (t >= 4) return;
-  const int ch = t >> 1, ri = t & 1;
-  double* f = fbase + (size_t)t * nd;
-  for (int i = 0; i < nd; ++i) f[i] = 0.0;
-  const double* mem = A.mem + (size_t)ch * 6 * ne * 4;
-  const double* Am = mem + (size_t)(0 * 2 + ri) * ne * 4;
-  const double* Bm = mem + (size_t)(1 * 2 + ri) * ne * 4;
-  const double* Cm = mem + (size_t)(2 * 2 + ri) * ne * 4;
   const double xg = 0.5773502691896257;
-  for (int e = 0; e < ne; ++e) {
+  for (int w = t; w < 4 * ne; w += blockDim.x) {
+    const int q = w / ne, e = w % ne, ch = q >> 1, ri = q & 1;
+    const double* mem = A.mem + (size_t)ch * 6 * ne * 4;
+    const double* Am = mem + (size_t)(0 * 2 + ri) * ne * 4;
+    const double* Bm = mem + (size_t)(1 * 2 + ri) * ne * 4;
+    const double* Cm = mem + (size_t)(2 * 2 + ri) * ne * 4;
     const double rk = A.r[e], rk1 = A.r[e + 1], h = rk1 - rk;
     double floc[4] = {0.0, 0.0, 0.0, 0.0};
     for (int ig = 0; ig < 2; ++ig) {
@@ -93,10 +93,26 @@ __global__ void k_rot_begin(RotArgs A, int staged) {
         floc[tt] = floc[tt] - D * ra * ra * h * 0.5;
       }
     }
-    f[4 * e] += floc[0];
-    f[4 * (e + 1)] += floc[1];
-    f[4 * e + 1] += floc[2];
-    f[4 * (e + 1) + 1] += floc[3];
+    for (int tt = 0; tt < 4; ++tt) sfl[((size_t)q * ne + e) * 4 + tt] = floc[tt];
+  }
+  __syncthreads();
+  if (t >= 4) return;
+  const int ch = t >> 1, ri = t & 1;
+  double* f = fbase + (size_t)t * nd;
+  const double* fl = sfl + (size_t)t * ne * 4;
+  for (int i = 0; i < nd; ++i) f[i] = 0.0;
+  for (int n = 0; n < nr; ++n) {  // (0 + element n-1's share) + element n's share, as the serial loop adds them
+    double u = 0.0, v = 0.0;
+    if (n >= 1) {
+      u += fl[(n - 1) * 4 + 1];
+      v += fl[(n - 1) * 4 + 3];
+    }
+    if (n < ne) {
+      u += fl[n * 4 + 0];
+      v += fl[n * 4 + 2];
+    }
+    f[4 * n] = u;
+    f[4 * n + 1] = v;
   }
   for (int i = 0; i < nd; ++i) f[i] = A.dr[i] * f[i];
   band_solve_strided(ab, VG_LDAB, nd, 6, 12, ipiv, f, 1);
@@ -323,18 +339,23 @@ void rotation_setup(vg_handle* h) {
 }
 
 // rotation_begin_step (src/vilma_rotation.f90:154-168): drift of both channels
-// shared memory of the staged k_rot_begin (0: the band stays in global memory)
-static size_t rot_smem(const vg_handle* h) {
-  const size_t b = (size_t)h->ndof * VG_LDAB * sizeof(double) + (size_t)4 * h->ndof * sizeof(double) +
+// shared memory of k_rot_begin
+// (the element contributions always; the band, pivots and right-hand sides
+// when they fit; `staged` says which)
+static size_t rot_smem(const vg_handle* h, int& staged) {
+  const size_t fl = (size_t)16 * h->ne * sizeof(double);
+  const size_t b = fl + (size_t)h->ndof * VG_LDAB * sizeof(double) + (size_t)4 * h->ndof * sizeof(double) +
                    (size_t)h->ndof * sizeof(int);
-  if (b > 200 * 1024) return 0;
-  raise_smem_limit((const void*)k_rot_begin, b);
-  return b;
+  staged = b <= 200 * 1024 ? 1 : 0;
+  const size_t need = staged ? b : fl;
+  raise_smem_limit((const void*)k_rot_begin, need);
+  return need;
 }
 
 void rotation_begin(vg_handle* h) {
-  const size_t sm = rot_smem(h);
-  k_rot_begin<<<1, 32, sm, h->stream>>>(rot_args(h), sm > 0 ? 1 : 0);
+  int staged = 0;
+  const size_t sm = rot_smem(h, staged);
+  k_rot_begin<<<1, 128, sm, h->stream>>>(rot_args(h), staged);
   ++h->n_launch;
   VG_CUDA(cudaGetLastError());
 }
@@ -374,9 +395,10 @@ void rotation_advance(vg_handle* h, const double* d_sigma, double dt) {
   S.w = G.d_wts.p;
   S.rows = h->d_rot_rows.p;
   const RotArgs A = rot_args(h);
-  const size_t sm = rot_smem(h);
+  int staged = 0;
+  const size_t sm = rot_smem(h, staged);
   for (int k = 0; k < n_sub; ++k) {
-    k_rot_begin<<<1, 32, sm, s>>>(A, sm > 0 ? 1 : 0);
+    k_rot_begin<<<1, 128, sm, s>>>(A, staged);
     k_rot_solve_commit<<<1, 256, 0, s>>>(A, S);
     h->n_launch += 2;
     VG_CUDA(cudaGetLastError());
