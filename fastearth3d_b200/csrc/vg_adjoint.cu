@@ -695,6 +695,8 @@ struct SleTape {
 struct AdjWork {
   DArr<double> sig, obs, resid, lam, lam_new, dUn_bar, dVn_bar, surf_bar, qbar, w, gsig, ckpt, E, G1T;
   DArr<double> ckpt_norm, gseg, gradMdt;  // checkpoint norms, a segment's longitude grids, d J / d (M dt)
+  // the toroidal channels: memory adjoints, element and nodal W adjoints, forcing adjoints, checkpoints
+  DArr<double> lam_t, lam_t_new, Et, Wb, gb, ckpt_t;
   DArr<int> site;
   // sea-level misfit: interval-end ice, checkpoints (rsl and entering ice
   // beside the memory), the entry state, the reverse sweep's grid and
@@ -778,16 +780,25 @@ double sum_squares(vg_handle* h, const AdjWork& W, size_t count) {
 struct StateGuard {
   vg_handle* h;
   DArr<double>& saved;
+  DArr<double>& saved_t;
   int cur;
-  StateGuard(vg_handle* hh, DArr<double>& buf) : h(hh), saved(buf), cur(hh->cur) {
+  StateGuard(vg_handle* hh, DArr<double>& buf, DArr<double>& buf_t) : h(hh), saved(buf), saved_t(buf_t), cur(hh->cur) {
     const size_t S = h->d_mem[h->cur].n;
     ensure(saved, S);
     VG_CUDA(cudaMemcpyAsync(saved.p, h->d_mem[h->cur].p, S * sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
+    if (h->tor_on) {
+      ensure(saved_t, h->d_tmem[h->cur].n);
+      VG_CUDA(cudaMemcpyAsync(saved_t.p, h->d_tmem[h->cur].p, h->d_tmem[h->cur].n * sizeof(double),
+                              cudaMemcpyDeviceToDevice, h->stream));
+    }
   }
   void restore() {
     h->cur = cur;
     VG_CUDA(cudaMemcpyAsync(h->d_mem[h->cur].p, saved.p, h->d_mem[h->cur].n * sizeof(double),
                             cudaMemcpyDeviceToDevice, h->stream));
+    if (h->tor_on)
+      VG_CUDA(cudaMemcpyAsync(h->d_tmem[h->cur].p, saved_t.p, h->d_tmem[h->cur].n * sizeof(double),
+                              cudaMemcpyDeviceToDevice, h->stream));
     compute_mem_norm(h, h->cur);
     h->mem_norm = read_mem_norm(h, h->cur);
   }
@@ -806,6 +817,14 @@ void reverse_prepare(vg_handle* h, AdjWork& W) {
   ensure(W.qbar, 2 * (size_t)h->grid.nlm);
   ensure(W.w, (size_t)2 * nd * nk);
   ensure(W.E, (size_t)5 * 2 * ne * nk);
+  if (h->tor_on) {
+    ensure(W.lam_t, h->d_tmem[0].n);
+    ensure(W.lam_t_new, h->d_tmem[0].n);
+    ensure(W.Et, (size_t)2 * 2 * ne * nk);
+    ensure(W.Wb, (size_t)2 * nr * nk);
+    ensure(W.gb, (size_t)2 * nr * nk);
+    VG_CUDA(cudaMemsetAsync(W.lam_t.p, 0, W.lam_t.n * sizeof(double), h->stream));  // no terminal cost
+  }
   const int nrow = 2 * nr + 1, ncol = 2 * nr;
   if (W.G1T.n != (size_t)nrow * ncol) {
     W.G1T.alloc((size_t)nrow * ncol);
@@ -831,7 +850,10 @@ void advance_T(vg_handle* h, AdjWork& W, double dt, const double* gstore, double
   k_adv1d_T_elem<<<eg, dim3(32, 8), 0, s>>>(ne, nr, nk, dt, h->d_kdeg.p, h->d_Jr.p, h->d_xUn.p, h->d_xVn.p,
                                              h->d_mu.p, h->d_MkPerDt.p, h->d_active1d.p, W.lam.p, W.lam_new.p,
                                              W.E.p);
-  if (h->lat_visc && h->ne3d > 0) visc3d_adjoint(h, gstore, dt, W.lam.p, W.lam_new.p, W.E.p, W.gradMdt.p, gw);
+  if (h->tor_on) advance_1d_tor_T(h, dt, W.lam_t.p, W.lam_t_new.p, W.Et.p);
+  if (h->lat_visc && h->ne3d > 0)
+    visc3d_adjoint(h, gstore, dt, W.lam.p, W.lam_new.p, W.E.p, W.gradMdt.p, gw, h->tor_on ? W.lam_t.p : nullptr,
+                   h->tor_on ? W.lam_t_new.p : nullptr, h->tor_on ? W.Et.p : nullptr);
   k_adv1d_T_node<<<ng_, dim3(32, 8), 0, s>>>(ne, nr, nk, h->d_k2lm.p, W.E.p, W.dUn_bar.p, W.dVn_bar.p, sbar);
   h->n_launch += 2;
   VG_CUDA(cudaGetLastError());
@@ -852,6 +874,13 @@ void drift_T(vg_handle* h, AdjWork& W) {
                                       W.dUn_bar.p, W.dVn_bar.p, W.surf_bar.p, W.lam_new.p);
   h->n_launch += 3;
   VG_CUDA(cudaGetLastError());
+  if (h->tor_on) drift_tor_T(h, W.Et.p, W.Wb.p, W.gb.p, W.lam_t_new.p);
+}
+
+// the memory adjoints of the next step become the current ones
+void swap_adjoints(vg_handle* h, AdjWork& W) {
+  std::swap(W.lam.p, W.lam_new.p);
+  if (h->tor_on) std::swap(W.lam_t.p, W.lam_t_new.p);
 }
 
 }  // namespace
@@ -862,7 +891,7 @@ double misfit_dev(vg_handle* h, int nsteps, double dt, const double* sigma, int 
   if (h->p.scheme != VG_SCHEME_FE) throw Error("vg_misfit: the response-level run follows the forward-Euler scheme");
   SkipOff skip(h);
   AdjWork& W = work_of(h);
-  StateGuard guard(h, W.lam_new);
+  StateGuard guard(h, W.lam_new, W.lam_t_new);
   upload_inputs(h, W, nsteps, sigma, nsite, site, obs);
   compute_mem_norm(h, h->cur);
   for (int n = 0; n < nsteps; ++n) fwd_step(h, W, n, nsite, dt);
@@ -894,15 +923,23 @@ double misfit_grad_dev(vg_handle* h, int nsteps, double dt, const double* sigma,
   ensure(W.ckpt, (size_t)nck * S);
   ensure(W.ckpt_norm, (size_t)nck * nk);
   compute_mem_norm(h, h->cur);
-  auto snapshot = [&](double* st, double* nm) {  // the state and its per-slot norms (the drift's gate)
+  const size_t ST = h->tor_on ? h->d_tmem[0].n : 0;  // the toroidal memory beside it
+  if (ST) ensure(W.ckpt_t, (size_t)nck * ST);
+  auto snapshot = [&](double* st, double* nm, int c) {  // the state and its per-slot norms (the drift's gate)
     VG_CUDA(cudaMemcpyAsync(st, h->d_mem[h->cur].p, S * sizeof(double), cudaMemcpyDeviceToDevice, s));
     VG_CUDA(cudaMemcpyAsync(nm, h->d_mnorm.p + (size_t)h->cur * nk, nk * sizeof(double), cudaMemcpyDeviceToDevice,
                             s));
+    if (ST)
+      VG_CUDA(cudaMemcpyAsync(W.ckpt_t.p + (size_t)c * ST, h->d_tmem[h->cur].p, ST * sizeof(double),
+                              cudaMemcpyDeviceToDevice, s));
   };
-  auto restore = [&](const double* st, const double* nm) {
+  auto restore = [&](const double* st, const double* nm, int c) {
     VG_CUDA(cudaMemcpyAsync(h->d_mem[h->cur].p, st, S * sizeof(double), cudaMemcpyDeviceToDevice, s));
     VG_CUDA(cudaMemcpyAsync(h->d_mnorm.p + (size_t)h->cur * nk, nm, nk * sizeof(double), cudaMemcpyDeviceToDevice,
                             s));
+    if (ST)
+      VG_CUDA(cudaMemcpyAsync(h->d_tmem[h->cur].p, W.ckpt_t.p + (size_t)c * ST, ST * sizeof(double),
+                              cudaMemcpyDeviceToDevice, s));
   };
   // with 3-D elements the reverse sweep needs every step's longitude grid; the
   // last segment's are kept from this sweep, the others recomputed from their
@@ -915,7 +952,8 @@ double misfit_grad_dev(vg_handle* h, int nsteps, double dt, const double* sigma,
     ~GridStore() { h->v3_gstore = nullptr; }
   } gstore_off{h};
   for (int n = 0; n < nsteps; ++n) {
-    if (n % ckpt == 0) snapshot(W.ckpt.p + (size_t)(n / ckpt) * S, W.ckpt_norm.p + (size_t)(n / ckpt) * nk);
+    if (n % ckpt == 0)
+      snapshot(W.ckpt.p + (size_t)(n / ckpt) * S, W.ckpt_norm.p + (size_t)(n / ckpt) * nk, n / ckpt);
     h->v3_gstore = (v3 && n >= last0) ? W.gseg.p + (size_t)(n - last0) * gsz : nullptr;
     fwd_step(h, W, n, nsite, dt);
   }
@@ -936,7 +974,7 @@ double misfit_grad_dev(vg_handle* h, int nsteps, double dt, const double* sigma,
     const int n0 = (n / ckpt) * ckpt;
     if (v3 && n < last0 && n % ckpt == ckpt - 1) {
       // this segment's longitude grids, recomputed from its checkpoint
-      restore(W.ckpt.p + (size_t)(n / ckpt) * S, W.ckpt_norm.p + (size_t)(n / ckpt) * nk);
+      restore(W.ckpt.p + (size_t)(n / ckpt) * S, W.ckpt_norm.p + (size_t)(n / ckpt) * nk, n / ckpt);
       for (int q = n0; q <= n; ++q) {
         h->v3_gstore = W.gseg.p + (size_t)(q - n0) * gsz;
         fwd_step(h, W, q, nsite, dt);
@@ -952,7 +990,7 @@ double misfit_grad_dev(vg_handle* h, int nsteps, double dt, const double* sigma,
     VG_CUDA(cudaGetLastError());
     advance_T(h, W, dt, v3 ? W.gseg.p + (size_t)(n - n0) * gsz : nullptr, 1.0, sbar);
     drift_T(h, W);
-    std::swap(W.lam.p, W.lam_new.p);
+    swap_adjoints(h, W);
   }
   if (grad_sigma) W.gsig.download(grad_sigma, (size_t)nsteps * n2, s);
   if (grad_pert) {
@@ -980,6 +1018,8 @@ double misfit_grad_dev(vg_handle* h, int nsteps, double dt, const double* sigma,
   }
   h->cur = cur0;
   VG_CUDA(cudaMemcpyAsync(h->d_mem[h->cur].p, W.ckpt.p, S * sizeof(double), cudaMemcpyDeviceToDevice, s));
+  if (ST)
+    VG_CUDA(cudaMemcpyAsync(h->d_tmem[h->cur].p, W.ckpt_t.p, ST * sizeof(double), cudaMemcpyDeviceToDevice, s));
   compute_mem_norm(h, h->cur);
   h->mem_norm = read_mem_norm(h, h->cur);
   return J;
@@ -1039,7 +1079,6 @@ void sle_check(vg_handle* h, int nsteps, double dt_yr, const double* ice, int ns
   if (!h->have_reference) throw Error("vg_sle_misfit: call vg_set_reference first (solid_earth_init)");
   if (h->p.scheme != VG_SCHEME_FE) throw Error("vg_sle_misfit: the coupled misfit follows the forward-Euler scheme");
   if (h->rot_on) throw Error("vg_sle_misfit: rotational feedback is not differentiated (rotation = 0)");
-  if (h->tor_on) throw Error("vg_sle_misfit: the toroidal channels are not differentiated (toroidal = 0)");
 }
 
 // forward-Euler sub-steps of an interval by the Maxwell-CFL rule of the driver
@@ -1173,7 +1212,7 @@ void rev_substep(vg_handle* h, AdjWork& W, const TapeSub& sb, double dt_ref, boo
   if (!warm) VG_CUDA(cudaMemsetAsync(rb, 0, (size_t)ng * sizeof(double), s));
   // drift^T: the surface drift adjoints of every inner iteration and the nodal ones of the advance
   drift_T(h, W);
-  std::swap(W.lam.p, W.lam_new.p);
+  swap_adjoints(h, W);
 }
 
 }  // namespace
@@ -1213,6 +1252,8 @@ double sle_misfit_grad_dev(vg_handle* h, int nsteps, double dt_yr, const double*
   ensure(W.ckpt_norm, (size_t)nck * nk);
   ensure(W.ck_rsl, (size_t)nck * ng);
   ensure(W.ck_hice, (size_t)nck * ng);
+  const size_t STt = h->tor_on ? h->d_tmem[0].n : 0;  // the toroidal memory
+  if (STt) ensure(W.ckpt_t, (size_t)nck * STt);
   std::vector<double> ck_ts(nck), ck_ty(nck), ck_mn(nck);
   auto snapshot = [&](int c) {
     VG_CUDA(cudaMemcpyAsync(W.ckpt.p + (size_t)c * S, h->d_mem[h->cur].p, S * sizeof(double),
@@ -1222,6 +1263,9 @@ double sle_misfit_grad_dev(vg_handle* h, int nsteps, double dt_yr, const double*
     VG_CUDA(cudaMemcpyAsync(W.ck_rsl.p + (size_t)c * ng, h->d_rsl.p, ng * sizeof(double), cudaMemcpyDeviceToDevice, s));
     VG_CUDA(cudaMemcpyAsync(W.ck_hice.p + (size_t)c * ng, h->d_h_ice.p, ng * sizeof(double),
                             cudaMemcpyDeviceToDevice, s));
+    if (STt)
+      VG_CUDA(cudaMemcpyAsync(W.ckpt_t.p + (size_t)c * STt, h->d_tmem[h->cur].p, STt * sizeof(double),
+                              cudaMemcpyDeviceToDevice, s));
     ck_ts[c] = h->time_s;
     ck_ty[c] = h->time_yr;
     ck_mn[c] = h->mem_norm;
@@ -1234,6 +1278,9 @@ double sle_misfit_grad_dev(vg_handle* h, int nsteps, double dt_yr, const double*
     VG_CUDA(cudaMemcpyAsync(h->d_rsl.p, W.ck_rsl.p + (size_t)c * ng, ng * sizeof(double), cudaMemcpyDeviceToDevice, s));
     VG_CUDA(cudaMemcpyAsync(h->d_h_ice.p, W.ck_hice.p + (size_t)c * ng, ng * sizeof(double),
                             cudaMemcpyDeviceToDevice, s));
+    if (STt)
+      VG_CUDA(cudaMemcpyAsync(h->d_tmem[h->cur].p, W.ckpt_t.p + (size_t)c * STt, STt * sizeof(double),
+                              cudaMemcpyDeviceToDevice, s));
     h->time_s = ck_ts[c];
     h->time_yr = ck_ty[c];
     h->mem_norm = ck_mn[c];
@@ -1358,7 +1405,6 @@ extern "C" int vg_misfit(vg_handle* h, int nsteps, double dt_s, const double* si
   if (!h) return 1;
   try {
     if (!sigma_lm || !obs || !J) throw vg::Error("vg_misfit: null argument");
-    if (h->tor_on) throw vg::Error("vg_misfit: the misfit runs carry no toroidal channels (toroidal = 0)");
     *J = vg::misfit_dev(h, nsteps, dt_s, sigma_lm, nsite, site, obs);
     return 0;
   } catch (const std::exception& ex) {
@@ -1373,7 +1419,6 @@ extern "C" int vg_misfit_grad(vg_handle* h, int nsteps, double dt_s, const doubl
   if (!h) return 1;
   try {
     if (!sigma_lm || !obs || !J) throw vg::Error("vg_misfit_grad: null argument");
-    if (h->tor_on) throw vg::Error("vg_misfit_grad: the toroidal channels are not differentiated (toroidal = 0)");
     *J = vg::misfit_grad_dev(h, nsteps, dt_s, sigma_lm, nsite, site, obs, ckpt_every, grad_sigma, grad_pert);
     return 0;
   } catch (const std::exception& ex) {

@@ -191,6 +191,7 @@ struct vg_handle {
   vg::DArr<double> d_tmem[2];
   vg::DArr<double> d_dWn, d_dWa;           // nodal W drift [ri][node][k], surface W(a) [ri][k]
   vg::DArr<double> d_tGinv;                // inverse W operators, degree l at (l - 1) nr^2 (row-major)
+  vg::DArr<double> d_tGinvT, d_tWa_scratch;  // their transposes (the adjoint, built at first use), a W(a) sink
   vg::DArr<double> d_tg;                   // W drift forcing [ri][node][k]
   vg::DArr<double> d_tK;                   // forcing maps of the toroidal memory (lmax + 1, ne, 12)
   vg::DArr<double> d_edWn, d_dW_avg, d_dWa_prev, d_tmem_s, d_tmem_c;  // trapezoidal scheme
@@ -296,8 +297,11 @@ void visc3d_advance(vg_handle* h, const double* d_sigma, double dt, const double
 // forward stored in gstore: lam_new (3-D entries) = lam + gather^T, E (3-D
 // elements) = strain adjoints, gw * d J / d (M dt) accumulated into gradMdt
 // (ne3d, nlat, nphi)
+// (with the toroidal channels also lam_t -> lam_t_new and the toroidal
+// strain adjoints Et (W0, W1 planes) of the 3-D elements)
 void visc3d_adjoint(vg_handle* h, const double* gstore, double dt, const double* lam, double* lam_new, double* E,
-                    double* gradMdt, double gw = 1.0);
+                    double* gradMdt, double gw = 1.0, const double* lam_t = nullptr, double* lam_t_new = nullptr,
+                    double* Et = nullptr);
 // exact tensor-core stages (vg_oz.cu): converter warps per stage (8 or 4);
 // oz_get_ncw returns false when the handle has no exact-stage plan
 void oz_set_ncw(vg_handle* h, const int ncw[4]);
@@ -358,6 +362,11 @@ void launch_drift_tor(vg_handle* h, int buf, double* dWn);
 void launch_advance_1d_tor(vg_handle* h, double dt, const double* dWn, bool trap, double* mn);
 // fold |toroidal memory of buffer buf| into the per-slot norms mn
 void mem_norm_tor(vg_handle* h, int buf, double* mn);
+// toroidal adjoint pieces (vg_toroidal.cu): the 1-D lambda 3, 4 advance
+// transposed (lam_t -> lam_t_new, the element W adjoints Et), and the W drift
+// transposed from Et into lam_t_new (adds; Wb, gb (2, nr, nk) work arrays)
+void advance_1d_tor_T(vg_handle* h, double dt, const double* lam_t, double* lam_t_new, double* Et);
+void drift_tor_T(vg_handle* h, const double* Et, double* Wb, double* gb, double* lam_t_new);
 // trapezoidal scheme (vg_trap.cu)
 void trap_setup(vg_handle* h);
 void trap_prepare(vg_handle* h);

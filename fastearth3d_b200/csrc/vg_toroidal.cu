@@ -388,3 +388,138 @@ void mem_norm_tor(vg_handle* h, int buf, double* mn) {
 }
 
 }  // namespace vg
+
+// ------------------------------------------------------------------ adjoint
+
+namespace vg {
+
+// advance_memory_tor transposed for the spectrally advanced (1-D) elements, a
+// thread per (slot, element, re/im): lam_t_new = (1 - M) lam_t; the strain
+// adjoint -2 mu M lam_t through strain_coeffs_tor transposed into the W
+// adjoints of the element's two nodes (Et planes W0, W1; zero for elements
+// that are not spectrally advanced: the 3-D pass writes its own)
+__global__ void __launch_bounds__(256) k_adv1d_tor_T(int ne, int nk, double dt, const int* __restrict__ kdeg,
+                                                     const double* __restrict__ Jrv, const double* __restrict__ mu,
+                                                     const double* __restrict__ MkPerDt,
+                                                     const char* __restrict__ active, const double* __restrict__ lam_t,
+                                                     double* __restrict__ lam_t_new, double* __restrict__ Et) {
+  const int k = blockIdx.x * 32 + threadIdx.x, e = blockIdx.y * 8 + threadIdx.y, ri = blockIdx.z;
+  if (k >= nk || e >= ne) return;
+  const size_t plane = (size_t)2 * ne * nk, at = ((size_t)ri * ne + e) * nk + k;
+  if (!active[e]) {  // (3-D elements: the 3-D pass's adjoint overwrites both)
+    Et[0 * plane + at] = 0.0;
+    Et[1 * plane + at] = 0.0;
+#pragma unroll
+    for (int m = 0; m < 2; ++m)
+#pragma unroll
+      for (int s3 = 0; s3 < 3; ++s3) lam_t_new[tmem_idx(s3, ri, e, m, k, ne, nk)] = 0.0;
+    return;
+  }
+  const double J = Jrv[kdeg[k]];
+  const double Me = MkPerDt[e] * dt, om = 1.0 - Me, two_muM = 2.0 * mu[e] * Me;
+  double w1 = 0.0, w2 = 0.0;
+#pragma unroll
+  for (int m = 0; m < 2; ++m) {
+    const size_t iA = tmem_idx(0, ri, e, m, k, ne, nk), iB = tmem_idx(1, ri, e, m, k, ne, nk),
+                 iC = tmem_idx(2, ri, e, m, k, ne, nk);
+    const double la = lam_t[iA], lb = lam_t[iB], lc = lam_t[iC];
+    lam_t_new[iA] = om * la;
+    lam_t_new[iB] = om * lb;
+    lam_t_new[iC] = om * lc;
+    const double ga = -two_muM * la, gb = -two_muM * lb, gc = -two_muM * lc;
+    if (m == 0) {  // a = -w1 + w2, b = -w1, c = -w2
+      w1 += -ga - gb;
+      w2 += ga - gc;
+    } else if (J > 2.0) {  // b = w1, c = w2 (a[1] = 0)
+      w1 += gb;
+      w2 += gc;
+    }
+  }
+  Et[0 * plane + at] = w1;
+  Et[1 * plane + at] = w2;
+}
+
+// the nodal W adjoints from the two elements that share each node
+__global__ void __launch_bounds__(256) k_tor_node_T(int ne, int nr, int nk, const double* __restrict__ Et,
+                                                    double* __restrict__ Wb) {
+  const int k = blockIdx.x * 32 + threadIdx.x, node = blockIdx.y * 8 + threadIdx.y, ri = blockIdx.z;
+  if (k >= nk || node >= nr) return;
+  const size_t plane = (size_t)2 * ne * nk;
+  const double* Er = Et + (size_t)ri * ne * nk + k;
+  double w = 0.0;
+  if (node < ne) w += Er[0 * plane + (size_t)node * nk];
+  if (node >= 1) w += Er[1 * plane + (size_t)(node - 1) * nk];
+  Wb[((size_t)ri * nr + node) * nk + k] = w;
+}
+
+// the forcing maps transposed: lam_t_new += K^T g_bar (element e's test dof 1
+// at node e + 1, test dof 0 at node e)
+__global__ void __launch_bounds__(256) k_drift_tor_rhs_T(int ne, int nr, int nk, const int* __restrict__ kdeg,
+                                                         const double* __restrict__ K, const double* __restrict__ gb,
+                                                         double* __restrict__ lam_t_new) {
+  const int k = blockIdx.x * 32 + threadIdx.x, e = blockIdx.y * 8 + threadIdx.y, ri = blockIdx.z;
+  if (k >= nk || e >= ne) return;
+  const int l = kdeg[k];
+  const double g0 = gb[((size_t)ri * nr + e) * nk + k], g1 = gb[((size_t)ri * nr + e + 1) * nk + k];
+  const double* K0 = K + ((size_t)l * ne + e) * 12;  // test dof 0 (node e), then test dof 1 (node e + 1)
+#pragma unroll
+  for (int s3 = 0; s3 < 3; ++s3)
+#pragma unroll
+    for (int m = 0; m < 2; ++m)
+      lam_t_new[tmem_idx(s3, ri, e, m, k, ne, nk)] += K0[s3 * 2 + m] * g0 + K0[6 + s3 * 2 + m] * g1;
+}
+
+void advance_1d_tor_T(vg_handle* h, double dt, const double* lam_t, double* lam_t_new, double* Et) {
+  dim3 grid((h->nk + 31) / 32, (h->ne + 7) / 8, 2);
+  k_adv1d_tor_T<<<grid, dim3(32, 8), 0, h->stream>>>(h->ne, h->nk, dt, h->d_kdeg.p, h->d_Jr.p, h->d_mu.p,
+                                                     h->d_MkPerDt.p, h->d_active1d.p, lam_t, lam_t_new, Et);
+  ++h->n_launch;
+  VG_CUDA(cudaGetLastError());
+}
+
+// W drift transposed: the nodal W adjoints (from the element strain adjoints
+// Et) through the transposed inverse W operators, then the forcing maps
+// transposed into lam_t_new (adds); Wb and gb are (2, nr, nk) work arrays
+void drift_tor_T(vg_handle* h, const double* Et, double* Wb, double* gb, double* lam_t_new) {
+  const int nr = h->nr, nk = h->nk, ne = h->ne, L = h->grid.lmax;
+  cudaStream_t s = h->stream;
+  k_tor_node_T<<<dim3((nk + 31) / 32, (nr + 7) / 8, 2), dim3(32, 8), 0, s>>>(ne, nr, nk, Et, Wb);
+  if (h->d_tGinvT.n != h->d_tGinv.n) {  // the transposed inverses, once
+    std::vector<double> G(h->d_tGinv.n), GT(h->d_tGinv.n);
+    h->d_tGinv.download(G.data(), G.size(), s);
+    VG_CUDA(cudaStreamSynchronize(s));
+    const size_t nr2 = (size_t)nr * nr;
+    for (int l = 1; l <= L; ++l)
+      for (int i = 0; i < nr; ++i)
+        for (int j = 0; j < nr; ++j) GT[(l - 1) * nr2 + (size_t)j * nr + i] = G[(l - 1) * nr2 + (size_t)i * nr + j];
+    h->d_tGinvT.upload(GT, s);
+    if (h->d_tWa_scratch.n < (size_t)2 * nk) h->d_tWa_scratch.alloc((size_t)2 * nk);
+  }
+  TorDriftArgs A;
+  A.tmem = nullptr;
+  A.mnorm = nullptr;
+  A.maxbits = nullptr;
+  A.skip_tol = 0.0;
+  A.K = h->d_tK.p;
+  A.kdeg = h->d_kdeg.p;
+  A.kbeg = h->d_kbeg.p;
+  A.Ginv = h->d_tGinvT.p;
+  A.g = Wb;
+  A.dWn = gb;
+  A.dWa = h->d_tWa_scratch.p;
+  A.ne = ne;
+  A.nr = nr;
+  A.nk = nk;
+  A.lmax = L;
+  const size_t smem = (size_t)nr * TOR_MC * sizeof(double);
+  if (smem > 96 * 1024) throw Error("toroidal drift: too many radial nodes for the shared forcing tile");
+  VG_CUDA(cudaFuncSetAttribute(k_drift_tor_mm, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024));
+  const int nchunk = (2 * (L + 1) + TOR_MC - 1) / TOR_MC;
+  k_drift_tor_mm<<<dim3(nchunk, L), TOR_MC * TOR_MR, smem, s>>>(A);
+  k_drift_tor_rhs_T<<<dim3((nk + 31) / 32, (ne + 7) / 8, 2), dim3(32, 8), 0, s>>>(ne, nr, nk, h->d_kdeg.p, h->d_tK.p,
+                                                                                   gb, lam_t_new);
+  h->n_launch += 3;
+  VG_CUDA(cudaGetLastError());
+}
+
+}  // namespace vg

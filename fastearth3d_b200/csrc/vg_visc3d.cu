@@ -894,7 +894,7 @@ void visc3d_advance(vg_handle* h, const double* d_sigma, double dt, const double
       k_v3_lon<LON_LF_TOR, 10>
           <<<dim3(G.nlat, (nf + LON_LF_TOR - 1) / LON_LF_TOR), lon_threads(h, LON_LF_TOR),
              lon_smem(h, LON_LF_TOR, false, 10), s>>>(h->d_Y.p, G.nlat, G.nphi, nf, dt, h->d_MkPerDt3.p,
-                                                      lon_tables(h), G.d_invsin.p, nullptr, trap ? 1 : 0);
+                                                      lon_tables(h), G.d_invsin.p, h->v3_gstore, trap ? 1 : 0);
     else
       k_v3_lon<LON_LF><<<lg, lon_threads(h, LON_LF), lon_smem(h, LON_LF, false), s>>>(
           h->d_Y.p, G.nlat, G.nphi, nf, dt, h->d_MkPerDt3.p, lon_tables(h), G.d_invsin.p, h->v3_gstore,
@@ -930,13 +930,17 @@ void visc3d_advance(vg_handle* h, const double* d_sigma, double dt, const double
 
 // scatter^T: the memory adjoint of a 3-D element's increment back to the six
 // products' analysis outputs (the normalisations of k_v3_scatter transposed)
+// (with the toroidal channels, NQ = 10: also lambda 3, 4's normalisations,
+// from the toroidal memory adjoint lam_t)
+template <int NQ = 6>
 __global__ void __launch_bounds__(256) k_v3_scatter_T(V3Args A, const double* __restrict__ lam,
-                                                      const double* __restrict__ n6, double* __restrict__ dyb) {
+                                                      const double* __restrict__ n6, double* __restrict__ dyb,
+                                                      const double* __restrict__ lam_t) {
   const int k = blockIdx.x * 32 + threadIdx.x, ei = blockIdx.y * 8 + threadIdx.y;
   if (k >= A.nk || ei >= A.ne3d) return;
   const int e = A.e3d[ei], l = A.kdeg[k];
   const double J = A.Jr[l], nn = n6[l];
-  double* row = dyb + (size_t)k * 6 * A.ncf;
+  double* row = dyb + (size_t)k * NQ * A.ncf;
   for (int s3 = 0; s3 < 3; ++s3) {
     const int f = 3 * ei + s3;
     double L[4][2];
@@ -957,6 +961,18 @@ __global__ void __launch_bounds__(256) k_v3_scatter_T(V3Args A, const double* __
     q[5][1] = nn != 0.0 ? 2.0 * L[3][0] / nn : 0.0;
     for (int p = 0; p < 6; ++p)
       for (int ri = 0; ri < 2; ++ri) row[(size_t)p * A.ncf + 2 * f + ri] = q[p][ri];
+    if (NQ == 10) {  // t0 = (q6 - i q7) / J, t1 = (q8 / 2 - i q9) / n4, transposed
+      double T[2][2];
+      for (int ri = 0; ri < 2; ++ri)
+        for (int lam_ = 0; lam_ < 2; ++lam_) T[lam_][ri] = lam_t[tmem_idx(s3, ri, e, lam_, k, A.ne, A.nk)];
+      const double n4 = 0.25 * nn;
+      const double qt[4][2] = {{T[0][0] / J, T[0][1] / J},
+                               {T[0][1] / J, -T[0][0] / J},
+                               {n4 != 0.0 ? 0.5 * T[1][0] / n4 : 0.0, n4 != 0.0 ? 0.5 * T[1][1] / n4 : 0.0},
+                               {n4 != 0.0 ? T[1][1] / n4 : 0.0, n4 != 0.0 ? -T[1][0] / n4 : 0.0}};
+      for (int p = 0; p < 4; ++p)
+        for (int ri = 0; ri < 2; ++ri) row[(size_t)(6 + p) * A.ncf + 2 * f + ri] = qt[p][ri];
+    }
   }
 }
 
@@ -966,7 +982,10 @@ __global__ void __launch_bounds__(256) k_v3_scatter_T(V3Args A, const double* __
 // with weights 1 at m = 0, 2 above), dyadic components^T; and
 // d J / d (M dt)(j, i) += -sum over components and shapes of G_bar g, g the
 // forward grid that the forward pass stored in gstore
-template <int LF>
+// With the toroidal channels (NQ = 10) the four more analysis-input adjoints
+// join the component adjoints (RP, m/sin RT, TP, TT - PP) and the four
+// toroidal products' adjoints come out beside the six.
+template <int LF, int NQ = 6>
 __global__ void __launch_bounds__(LON_THREADS, 1)
     k_v3_lon_T(const double* __restrict__ gstore, double* __restrict__ Yb, int nlat, int nphi, int nf, double dt,
                const double* __restrict__ Mk3rate, LonTables T, const double* __restrict__ invsin,
@@ -975,14 +994,14 @@ __global__ void __launch_bounds__(LON_THREADS, 1)
   const int j = blockIdx.x, f0 = blockIdx.y * LF;
   const int nft = min(LF, nf - f0);
   const int ncf = 2 * nf, half = T.half, wA = 2 * T.M2;
-  double* A = sm;                          // [6 LF][2 M2] adjoint Fourier coefficients
-  double* X = A + (size_t)6 * LF * wA;     // [6 LF][nphi] adjoint grid, parity combinations
+  double* A = sm;  // [6 LF][2 M2] adjoint Fourier coefficients; [m][NQ][2 nft] product adjoints
+  double* X = A + (NQ == 6 ? (size_t)6 * LF * wA : lon_areg(LF, T));  // [6 LF][nphi] adjoint grid
   double* P = X + (size_t)6 * LF * nphi;   // [LF][nphi] per-field G_bar . g
   const double is = invsin[j];
   const double scl = 2.0 * PI / (double)nphi;
   // 1. adjoint dyadic Fourier coefficients from the analysis-input adjoints
   //    (staged in X as [m][q][2 nft])
-  stage_in(Yb, X, nlat, ncf, j, f0, nft, T.M);
+  stage_in<NQ, 6>(Yb, X, nlat, ncf, j, f0, nft, T.M);
   __syncthreads();
   for (int t = threadIdx.x; t < nft * T.M2; t += blockDim.x) {
     const int fl = t / T.M2, m = t % T.M2;
@@ -1002,6 +1021,28 @@ __global__ void __launch_bounds__(LON_THREADS, 1)
     }
   }
   __syncthreads();
+  if (NQ == 10) {  // out6 = F2 (RP), out7 = ms F1, out8 = F5, out9 = F3 - F4, transposed and added
+    stage_in<NQ, 4>(Yb, X, nlat, ncf, j, f0, nft, T.M, 6);
+    __syncthreads();
+    for (int t = threadIdx.x; t < nft * T.M; t += blockDim.x) {
+      const int fl = t / T.M, m = t % T.M;
+      double o[4][2];
+      for (int q = 0; q < 4; ++q)
+        for (int ri = 0; ri < 2; ++ri) o[q][ri] = X[((size_t)m * 4 + q) * 2 * nft + 2 * fl + ri];
+      const double ms = m * is;
+      const double add[6][2] = {{0.0, 0.0},
+                                {ms * o[1][0], ms * o[1][1]},
+                                {o[0][0], o[0][1]},
+                                {o[3][0], o[3][1]},
+                                {-o[3][0], -o[3][1]},
+                                {o[2][0], o[2][1]}};
+      for (int c = 1; c < 6; ++c) {
+        A[(size_t)(fl * 6 + c) * wA + 2 * m] += scl * add[c][0];
+        A[(size_t)(fl * 6 + c) * wA + 2 * m + 1] += scl * add[c][1];
+      }
+    }
+    __syncthreads();
+  }
   // 2. analysis^T: G_bar(i) = scl sum_m (Fre cos(m phi_i) - Fim sin(m phi_i));
   //    the per-field G_bar . g and g_bar = -M dt G_bar in parity form
   lon_synth(A, nft, T, [&](int fl, int i, const double* b1, const double* b2) {
@@ -1045,28 +1086,66 @@ __global__ void __launch_bounds__(LON_THREADS, 1)
                              {cb[3][0] - cb[4][0], cb[3][1] - cb[4][1]},
                              {4.0 * cb[5][1], -4.0 * cb[5][0]}};
     for (int q = 0; q < 6; ++q)
-      for (int ri = 0; ri < 2; ++ri) A[((size_t)m * 6 + q) * 2 * nft + 2 * fl + ri] = Sb[q][ri];
+      for (int ri = 0; ri < 2; ++ri) A[((size_t)m * NQ + q) * 2 * nft + 2 * fl + ri] = Sb[q][ri];
+    if (NQ == 10) {  // P.X4 (rt -= i ms), D.X4 (rp), G.X5 (tp), H.X5 (tt -= i, pp += i), transposed
+      const double St[4][2] = {{-ms * cb[1][1], ms * cb[1][0]},
+                               {cb[2][0], cb[2][1]},
+                               {cb[5][0], cb[5][1]},
+                               {-cb[3][1] + cb[4][1], cb[3][0] - cb[4][0]}};
+      for (int q = 0; q < 4; ++q)
+        for (int ri = 0; ri < 2; ++ri) A[((size_t)m * NQ + 6 + q) * 2 * nft + 2 * fl + ri] = St[q][ri];
+    }
   });
   __syncthreads();
-  stage_out(A, Yb, nlat, ncf, j, f0, nft, T.M);
+  stage_out<NQ>(A, Yb, nlat, ncf, j, f0, nft, T.M);
 }
 
 // gather^T: the synthesis-input adjoint (per product, combined into the four
 // channels) back to the memory (identity of tau + Delta plus G) and to the
 // strain, whose transposed coefficients go to the nodal drift adjoints per
 // element (E planes: U0, U1, V0, V1, sigma_bar share)
+// (with the toroidal channels, NP = 10: channels 4, 5 = P.X4 + D.X4 and
+// G.X5 + H.X5 back to the toroidal memory adjoint and, through the toroidal
+// strain transposed, to the nodal W adjoint per element, Et planes W0, W1)
+template <int NP = 6>
 __global__ void __launch_bounds__(256) k_v3_gather_T(V3Args A, const double* __restrict__ Rb,
                                                      const double* __restrict__ lam, double* __restrict__ lam_new,
-                                                     double* __restrict__ E) {
+                                                     double* __restrict__ E, const double* __restrict__ lam_t,
+                                                     double* __restrict__ lam_t_new, double* __restrict__ Et) {
   const int k = blockIdx.x * 32 + threadIdx.x, ei = blockIdx.y * 8 + threadIdx.y;
   if (k >= A.nk || ei >= A.ne3d) return;
   const int e = A.e3d[ei], l = A.kdeg[k];
   const double Jr = A.Jr[l], twoMu = 2.0 * A.mu[e];
   const double* xu = A.xUn + (size_t)l * A.nr;
   const double* xv = A.xVn + (size_t)l * A.nr;
-  const double* row = Rb + (size_t)k * 6 * A.ncf;
+  const double* row = Rb + (size_t)k * NP * A.ncf;
   const size_t plane = (size_t)2 * A.ne * A.nk;
   for (int ri = 0; ri < 2; ++ri) {
+    if (NP == 10) {  // strain_coeffs_tor transposed: a = -w1 + w2, b = (-w1, w1), c = (-w2, w2)
+      double w1 = 0.0, w2 = 0.0;
+      for (int s3 = 0; s3 < 3; ++s3) {
+        const int n = (3 * ei + s3) * 2 + ri;
+        const double xt[2] = {row[(size_t)6 * A.ncf + n] + row[(size_t)7 * A.ncf + n],
+                              row[(size_t)8 * A.ncf + n] + row[(size_t)9 * A.ncf + n]};
+        double g[2];
+        for (int lt = 0; lt < 2; ++lt) {
+          const size_t idx = tmem_idx(s3, ri, e, lt, k, A.ne, A.nk);
+          lam_t_new[idx] = lam_t[idx] + xt[lt];
+          g[lt] = twoMu * xt[lt];
+        }
+        if (s3 == 0) {  // a[0] = -w1 + w2 (a[1] = 0)
+          w1 -= g[0];
+          w2 += g[0];
+        } else if (s3 == 1) {  // b = (-w1, w1 or 0)
+          w1 += -g[0] + (Jr <= 2.0 ? 0.0 : g[1]);
+        } else {  // c = (-w2, w2 or 0)
+          w2 += -g[0] + (Jr <= 2.0 ? 0.0 : g[1]);
+        }
+      }
+      const size_t at = ((size_t)ri * A.ne + e) * A.nk + k;
+      Et[0 * plane + at] = w1;
+      Et[1 * plane + at] = w2;
+    }
     double eb[3][4];
     for (int s3 = 0; s3 < 3; ++s3) {
       const int n = (3 * ei + s3) * 2 + ri;
@@ -1095,19 +1174,22 @@ __global__ void __launch_bounds__(256) k_v3_gather_T(V3Args A, const double* __r
 
 static void lon_attributes() {
   for (const void* k :
-       {(const void*)k_v3_lon<LON_LF>, (const void*)k_v3_lon<LON_LF_TOR, 10>, (const void*)k_v3_lon_T<LON_LF>})
+       {(const void*)k_v3_lon<LON_LF>, (const void*)k_v3_lon<LON_LF_TOR, 10>, (const void*)k_v3_lon_T<LON_LF>,
+        (const void*)k_v3_lon_T<LON_LF_TOR, 10>})
     VG_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)LON_SMEM_MAX));
 }
 
 void visc3d_adjoint(vg_handle* h, const double* gstore, double dt, const double* lam, double* lam_new, double* E,
-                    double* gradMdt, double gw) {
+                    double* gradMdt, double gw, const double* lam_t, double* lam_t_new, double* Et) {
   if (h->ne3d == 0) return;
   if (h->p.visc3d_precision != VG_VISC3D_FP64)
     throw Error("vg_misfit_grad: the 3-D adjoint follows the FP64 path (visc3d_precision = FP64)");
+  const bool tor = h->tor_on;
+  if (tor && !(lam_t && lam_t_new && Et)) throw Error("visc3d_adjoint: the toroidal adjoint buffers are required");
   const Grid& G = h->grid;
   cudaStream_t s = h->stream;
-  const int nf = 3 * h->ne3d, ncf = 2 * nf;
-  const size_t ny = (size_t)G.M * G.nlat * 6 * ncf, nr6 = (size_t)(h->nk + 1) * 6 * ncf;
+  const int nf = 3 * h->ne3d, ncf = 2 * nf, np = tor ? 10 : 6;
+  const size_t ny = (size_t)G.M * G.nlat * np * ncf, nr6 = (size_t)(h->nk + 1) * np * ncf;
   if (h->d_v3a_Yb.n != ny) {
     h->d_v3a_Yb.alloc(ny);
     h->d_v3a_dyb.alloc(nr6);  // slot row nk (degree 0) stays zero
@@ -1117,7 +1199,7 @@ void visc3d_adjoint(vg_handle* h, const double* gstore, double dt, const double*
   A.mem = h->d_mem[h->cur].p;
   A.nxt = nullptr;
   A.sigma = nullptr;
-  A.tor = 0;
+  A.tor = tor ? 1 : 0;
   A.tmem = nullptr;
   A.tnxt = nullptr;
   A.dWn = nullptr;
@@ -1143,30 +1225,39 @@ void visc3d_adjoint(vg_handle* h, const double* gstore, double dt, const double*
   S.nlat = G.nlat;
   S.nk = h->nk;
   S.ncf = ncf;
-  S.nin = 4;
-  S.np = 6;
+  S.nin = tor ? 6 : 4;
+  S.np = np;
   S.mbeg = G.d_mbeg.p;
   S.kbeg = h->d_kbeg.p;
-  const double* st[6] = {G.d_plm.p, G.d_dplm.p, G.d_plm.p, G.d_plm.p, h->d_G6.p, h->d_H6.p};
-  const double* at[6] = {h->d_wP.p, h->d_wD.p, h->d_wP.p, h->d_wP.p, h->d_wG.p, h->d_wH.p};
-  const int sc[6] = {0, 1, 1, 2, 3, 3};
-  for (int p = 0; p < 6; ++p) {
+  const double* st[10] = {G.d_plm.p, G.d_dplm.p, G.d_plm.p, G.d_plm.p, h->d_G6.p,
+                          h->d_H6.p, G.d_plm.p,  G.d_dplm.p, h->d_G6.p, h->d_H6.p};
+  const double* at[10] = {h->d_wP.p, h->d_wD.p, h->d_wP.p, h->d_wP.p, h->d_wG.p,
+                          h->d_wH.p, h->d_wD.p, h->d_wP.p, h->d_wG.p, h->d_wH.p};
+  const int sc[10] = {0, 1, 1, 2, 3, 3, 4, 4, 5, 5};
+  for (int p = 0; p < np; ++p) {
     S.T[p] = st[p];
     S.chan[p] = sc[p];
   }
-  dim3 sgrid((ncf + GB_N - 1) / GB_N, (G.nlat + GB_M - 1) / GB_M, G.M * 6);
+  dim3 sgrid((ncf + GB_N - 1) / GB_N, (G.nlat + GB_M - 1) / GB_M, G.M * np);
   // adjoint chain
-  k_v3_scatter_T<<<gg, dim3(32, 8), 0, s>>>(A, lam, h->d_n6.p, h->d_v3a_dyb.p);
+  if (tor)
+    k_v3_scatter_T<10><<<gg, dim3(32, 8), 0, s>>>(A, lam, h->d_n6.p, h->d_v3a_dyb.p, lam_t);
+  else
+    k_v3_scatter_T<6><<<gg, dim3(32, 8), 0, s>>>(A, lam, h->d_n6.p, h->d_v3a_dyb.p, nullptr);
   GemmArgs Ab = S;  // analysis^T: the weighted tables, per-product input rows
-  Ab.nin = 6;
-  for (int p = 0; p < 6; ++p) {
+  Ab.nin = np;
+  for (int p = 0; p < np; ++p) {
     Ab.T[p] = at[p];
     Ab.chan[p] = p;
   }
   Ab.in = h->d_v3a_dyb.p;
   Ab.out = h->d_v3a_Yb.p;
   k_v3_gemm<<<sgrid, 256, 0, s>>>(Ab);
-  {
+  if (tor) {
+    const dim3 lg(G.nlat, (nf + LON_LF_TOR - 1) / LON_LF_TOR);
+    k_v3_lon_T<LON_LF_TOR, 10><<<lg, lon_threads(h, LON_LF_TOR), lon_smem(h, LON_LF_TOR, true, 10), s>>>(
+        gstore, h->d_v3a_Yb.p, G.nlat, G.nphi, nf, dt, h->d_MkPerDt3.p, lon_tables(h), G.d_invsin.p, gradMdt, gw);
+  } else {
     const dim3 lg(G.nlat, (nf + LON_LF - 1) / LON_LF);
     k_v3_lon_T<LON_LF><<<lg, lon_threads(h, LON_LF), lon_smem(h, LON_LF, true), s>>>(
         gstore, h->d_v3a_Yb.p, G.nlat, G.nphi, nf, dt, h->d_MkPerDt3.p, lon_tables(h), G.d_invsin.p, gradMdt, gw);
@@ -1175,9 +1266,12 @@ void visc3d_adjoint(vg_handle* h, const double* gstore, double dt, const double*
   Sb.mode = 1;
   Sb.in = h->d_v3a_Yb.p;
   Sb.out = h->d_v3a_Rb.p;
-  dim3 agrid((ncf + GB_N - 1) / GB_N, (G.M + GB_M - 1) / GB_M, G.M * 6);
+  dim3 agrid((ncf + GB_N - 1) / GB_N, (G.M + GB_M - 1) / GB_M, G.M * np);
   k_v3_gemm<<<agrid, 256, 0, s>>>(Sb);
-  k_v3_gather_T<<<gg, dim3(32, 8), 0, s>>>(A, h->d_v3a_Rb.p, lam, lam_new, E);
+  if (tor)
+    k_v3_gather_T<10><<<gg, dim3(32, 8), 0, s>>>(A, h->d_v3a_Rb.p, lam, lam_new, E, lam_t, lam_t_new, Et);
+  else
+    k_v3_gather_T<6><<<gg, dim3(32, 8), 0, s>>>(A, h->d_v3a_Rb.p, lam, lam_new, E, nullptr, nullptr, nullptr);
   h->n_launch += 5;
   VG_CUDA(cudaGetLastError());
 }

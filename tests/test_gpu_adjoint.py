@@ -68,7 +68,7 @@ def test_adjoint_checkpoint_interval_and_state_kept():
         assert np.array_equal(a, b)
 
 
-def setup_3d(lmax=10, nsteps=5, nsite=30, seed=5):
+def setup_3d(lmax=10, nsteps=5, nsite=30, seed=5, toroidal=0):
     """A model whose Maxwell elements are all carried as 3-D, with a seeded
     lateral log-viscosity field; returns a factory so finite differences can
     rebuild the model with a perturbed field."""
@@ -80,6 +80,7 @@ def setup_3d(lmax=10, nsteps=5, nsite=30, seed=5):
         for i, c in enumerate([2, 4, 3, 3]):
             p.ne_layer[i] = c
         p.visc3d_tol = -1.0  # every Maxwell element 3-D
+        p.toroidal = toroidal
         m = vlib.Model(p)
         m.enable_visc3d(pert)
         return m
@@ -96,10 +97,16 @@ def setup_3d(lmax=10, nsteps=5, nsite=30, seed=5):
     return make, pert, sig, sites, obs, 50.0 * synth.SEC_PER_YEAR, rng
 
 
-def test_adjoint_3d_log_viscosity_gradient_vs_central_differences():
-    make, pert, sig, sites, obs, dt, rng = setup_3d()
+@pytest.mark.parametrize("toroidal", [0, 1])
+def test_adjoint_3d_log_viscosity_gradient_vs_central_differences(toroidal):
+    """With toroidal = 1 the lateral viscosity also drives W: the reverse
+    sweep runs the lambda 3, 4 advance, the W drift and the ten-product 3-D
+    chain transposed."""
+    make, pert, sig, sites, obs, dt, rng = setup_3d(toroidal=toroidal)
     m = make(pert)
     assert m.info().ne3d > 0
+    if toroidal:
+        assert m.state_tor() is not None
     J, gs, gp = m.misfit_grad(sig, dt, sites, obs, ckpt_every=2, want_pert=True)
     assert abs(J - m.misfit(sig, dt, sites, obs)) <= 1e-12 * J
     h = 1e-4
@@ -118,14 +125,20 @@ def test_adjoint_3d_log_viscosity_gradient_vs_central_differences():
         assert abs(fd - ad) <= 1e-6 * abs(fd), (fd, ad)
 
 
-def test_adjoint_3d_checkpoint_interval_and_state_kept():
+@pytest.mark.parametrize("toroidal", [0, 1])
+def test_adjoint_3d_checkpoint_interval_and_state_kept(toroidal):
     """The 3-D reverse sweep reads each step's longitude grid: kept from the
     forward sweep for the last segment, recomputed from a checkpoint for the
     others. Every interval gives the same gradients, bit for bit, and the
-    handle's memory is left as it was."""
-    make, pert, sig, sites, obs, dt, rng = setup_3d(nsteps=5)
+    handle's memory (the toroidal one too) is left as it was."""
+    make, pert, sig, sites, obs, dt, rng = setup_3d(nsteps=5, toroidal=toroidal)
     m = make(pert)
+    m.set_dt(dt)
+    for _ in range(2):  # a state with memory in it, toroidal included
+        m.begin_step()
+        m.advance(sig[0])
     s0, _ = m.state()
+    t0 = m.state_tor()
     out = [m.misfit_grad(sig, dt, sites, obs, ckpt_every=c, want_pert=True) for c in (1, 2, 5, 9)]
     J0, gs0, gp0 = out[0]
     for J, gs, gp in out[1:]:
@@ -134,3 +147,6 @@ def test_adjoint_3d_checkpoint_interval_and_state_kept():
     s1, _ = m.state()
     for a, b in zip(s0, s1):
         assert np.array_equal(a, b)
+    if toroidal:
+        for a, b in zip(t0, m.state_tor()):
+            assert np.array_equal(a, b)

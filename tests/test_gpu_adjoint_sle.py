@@ -38,10 +38,11 @@ def spectrum(rng, lmax_field, scale):
     return q
 
 
-def build(kind, w, q):
+def build(kind, w, q, toroidal=0):
     mk = vlib if kind == "gpu" else orc
     p = w.params(mk.default_params)
     p.skip_tol = 0.0
+    p.toroidal = toroidal
     if kind == "gpu":
         p.visc3d_precision = VG_VISC3D_FP64
     m = vlib.Model(p) if kind == "gpu" else orc.Oracle(p)
@@ -171,4 +172,33 @@ def test_sle_gradient_viscosity_vs_central_differences(case, forward):
             jm = run_misfit(build("orc", w, q0 - h * dq), ice, sites, obs)
         check((jp - jm) / (2 * h), ad, scale, worst)
     print("viscosity gradient vs central differences of the %s forward: worst relative error %.2e" % (
+        forward, max(worst)))
+
+
+@pytest.mark.parametrize("forward", ["gpu", "oracle"])
+def test_sle_gradient_with_toroidal_channels_vs_central_differences(case, forward):
+    """With toroidal = 1 the lateral viscosity also drives W, and the reverse
+    sweep runs its transposes (the lambda 3, 4 advance, the W drift, the
+    ten-product 3-D chain): the viscosity gradient against central
+    differences along 10 seeded directions, of the GPU and the oracle
+    forwards with W carried."""
+    w, rng, q0, ice, sites, obs = case
+    g = build("gpu", w, q0, toroidal=1)
+    assert g.state_tor() is not None
+    J, gi, gp, gq = g.sle_misfit_grad(ice, DT, sites, obs, ckpt_every=3, want_pert=True)
+    rs = np.random.default_rng(303)
+    h = 1e-6
+    worst = []
+    for _ in range(10):
+        dq = spectrum(rs, 12, 1.0)
+        ad = float(np.sum(gq.real * dq.real + gq.imag * dq.imag))
+        scale = np.sqrt(np.sum(np.abs(gq) ** 2) * np.sum(np.abs(dq) ** 2)) * 1e-3
+        if forward == "gpu":
+            jp = build("gpu", w, q0 + h * dq, toroidal=1).sle_misfit(ice, DT, sites, obs)
+            jm = build("gpu", w, q0 - h * dq, toroidal=1).sle_misfit(ice, DT, sites, obs)
+        else:
+            jp = run_misfit(build("orc", w, q0 + h * dq, toroidal=1), ice, sites, obs)
+            jm = run_misfit(build("orc", w, q0 - h * dq, toroidal=1), ice, sites, obs)
+        check((jp - jm) / (2 * h), ad, scale, worst)
+    print("viscosity gradient with W vs central differences of the %s forward: worst relative error %.2e" % (
         forward, max(worst)))
