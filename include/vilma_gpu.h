@@ -353,10 +353,10 @@ int vg_misfit_grad(vg_handle* h, int nsteps, double dt_s, const double* sigma_lm
  * The reverse sweep keeps the interval driver's state every ckpt_every
  * intervals and recomputes each segment from it; a segment's longitude grids
  * (3-D elements) are held on the device, about 0.26 GB per sub-step at lmax
- * 128 with 54 3-D elements. Forward Euler only, no rotation, no toroidal
- * channels; the drift skip gate is off inside these calls. The handle's
- * state (memory, rsl, ice, ocean function, z_bed, time, counters) is put
- * back afterwards. */
+ * 128 with 54 3-D elements. Forward Euler only, no rotation; the toroidal
+ * channels are differentiated with the rest (FP64 path); the drift skip
+ * gate is off inside these calls. The handle's state (memory, rsl, ice,
+ * ocean function, z_bed, time, counters) is put back afterwards. */
 int vg_sle_misfit(vg_handle* h, int nsteps, double dt_yr, const double* ice, int nsite, const int* site,
                   const double* obs, double* J);
 int vg_sle_misfit_grad(vg_handle* h, int nsteps, double dt_yr, const double* ice, int nsite, const int* site,
