@@ -35,6 +35,7 @@ sys.path.insert(0, ROOT)
 from fastearth3d_b200 import synth  # noqa: E402
 
 DEFAULT_WORKLOAD = "c3_3d_l128"
+DEFAULT_STEPS = {"c4_ensemble": 20, "c2_1d_sle_l128": 1000, "c1_1d_l64": 4000}
 METRIC = "steps/s @lmax=128 3D visc: batched vs plain GPU, rsl err<=1e-8; grad/fwd"
 
 
@@ -42,8 +43,8 @@ def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=None,
-                    help="timed steps (default: 300 for the single-instance workloads, so that each arm's timed "
-                         "region lasts over a second; 20 for c4_ensemble)")
+                    help="timed steps (default: enough for each arm's timed region to last over a second: 300 "
+                         "for the 3-D workload, 1000 for c2_1d_sle_l128, 4000 for c1_1d_l64; 20 for c4_ensemble)")
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default=DEFAULT_WORKLOAD)
@@ -633,7 +634,7 @@ def run_ensemble(args):
 def main():
     args = parse()
     if args.steps is None:
-        args.steps = 20 if args.workload == "c4_ensemble" else 300
+        args.steps = DEFAULT_STEPS.get(args.workload, 300)
     if args.workload == "c4_ensemble":
         import torch
 

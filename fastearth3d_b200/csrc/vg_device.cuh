@@ -210,4 +210,95 @@ __device__ __forceinline__ void band_solve_strided(const double* __restrict__ ab
 #undef AB
 }
 
+// The same solve as band_solve_strided (unit stride), operation for operation
+// and in the same order, for compile-time bandwidths: the sweep's active
+// window of the right-hand side is held in registers (forward: x[k .. k + KL],
+// the row interchange a select within it; backward: x[k - KV .. k]), so that
+// each element is read once before its sweep and written once after it
+// instead of going through memory at every update, and the next step's
+// operands (pivot, band column, the entering element) are loaded one step
+// ahead, so their latency overlaps the current step's arithmetic. For one
+// thread per right-hand side, whose sweeps are otherwise a chain of dependent
+// memory round trips.
+template <int KL, int KV>
+__device__ __forceinline__ void band_solve_window(const double* __restrict__ ab, int ldab, int n,
+                                                  const int* __restrict__ ipiv, double* __restrict__ x) {
+  double w[KL + 1];  // w[i] = x[k + i]
+#pragma unroll
+  for (int i = 0; i <= KL; ++i) w[i] = i < n ? x[i] : 0.0;
+  // operands of step k: the interchange offset, AB(KV + 1 + i, k + 1) for
+  // i = 1 .. KL, and x[k + 1 + KL], the element that enters after the step
+  int ip = 0;
+  double cn[KL + 1];
+  double xn = (KL + 1 < n) ? x[KL + 1] : 0.0;
+  if (n > 1) {
+    ip = ipiv[0];
+#pragma unroll
+    for (int i = 1; i <= KL; ++i) cn[i] = ab[KV + i];
+  }
+  for (int k = 0; k < n - 1; ++k) {
+    const int d = ip - k;  // the interchange partner row k + d, 0 <= d <= KL
+    double cc[KL + 1];
+#pragma unroll
+    for (int i = 1; i <= KL; ++i) cc[i] = cn[i];
+    const double xe = xn;
+    if (k + 1 < n - 1) {
+      ip = ipiv[k + 1];
+      const double* col = ab + (size_t)(k + 1) * ldab + KV;
+#pragma unroll
+      for (int i = 1; i <= KL; ++i) cn[i] = col[i];
+    }
+    xn = (k + 2 + KL < n) ? x[k + 2 + KL] : 0.0;
+#pragma unroll
+    for (int i = 1; i <= KL; ++i)
+      if (d == i) {
+        const double s = w[0];
+        w[0] = w[i];
+        w[i] = s;
+      }
+    const double t = w[0];
+    const int lm = min(KL, n - 1 - k);
+#pragma unroll
+    for (int i = 1; i <= KL; ++i)
+      if (i <= lm) w[i] -= cc[i] * t;
+    x[k] = w[0];
+#pragma unroll
+    for (int i = 0; i < KL; ++i) w[i] = w[i + 1];
+    w[KL] = xe;
+  }
+  if (n >= 1) x[n - 1] = w[0];
+  double v[KV + 1];  // v[i] = x[k - i]
+#pragma unroll
+  for (int i = 0; i <= KV; ++i) v[i] = (n - 1 - i >= 0) ? x[n - 1 - i] : 0.0;
+  // operands of step k: AB(KV + 1 - i, k + 1) for i = 0 .. KV and x[k - 1 - KV]
+  double bn[KV + 1];
+  double yn = (n - 2 - KV >= 0) ? x[n - 2 - KV] : 0.0;
+  if (n >= 1) {
+    const double* col = ab + (size_t)(n - 1) * ldab + KV;
+#pragma unroll
+    for (int i = 0; i <= KV; ++i) bn[i] = col[-i];
+  }
+  for (int k = n - 1; k >= 0; --k) {
+    double bc[KV + 1];
+#pragma unroll
+    for (int i = 0; i <= KV; ++i) bc[i] = bn[i];
+    const double ye = yn;
+    if (k >= 1) {
+      const double* col = ab + (size_t)(k - 1) * ldab + KV;
+#pragma unroll
+      for (int i = 0; i <= KV; ++i) bn[i] = col[-i];
+    }
+    yn = (k - 2 - KV >= 0) ? x[k - 2 - KV] : 0.0;
+    const double xk = v[0] / bc[0];
+    x[k] = xk;
+    const int lm = min(KV, k);
+#pragma unroll
+    for (int i = 1; i <= KV; ++i)
+      if (i <= lm) v[i] -= bc[i] * xk;
+#pragma unroll
+    for (int i = 0; i < KV; ++i) v[i] = v[i + 1];
+    v[KV] = ye;
+  }
+}
+
 }  // namespace vg

@@ -238,6 +238,7 @@ struct vg_handle {
   vg::DArr<double> d_rot_dn;    // nodal drift [ch][dUn re, dUn im, dVn re, dVn im][nr]
   vg::DArr<double> d_rot_sc;    // scalars (see vg_rotation.cu)
   vg::DArr<double> d_rot_f;     // channel solve work (4 x ndof)
+  vg::DArr<double> d_rot_fl;    // channel element contributions (4 x ne x 4)
   vg::DArr<double> d_rot_rows;  // per-row partial inertia sums (2 x nlat)
   vg::DArr<double> d_rot_geo;   // sin(theta)cos(theta) [nlat], cos(lon), sin(lon) [nphi each]
   vg::DArr<double> d_srot, d_rot_load;  // grid fields

@@ -37,30 +37,68 @@ struct RotArgs {
   const double *sa, *sb, *sc, *nrm;  // degree-2 strain constants (16, 16, 16, 4)
   const double *ab, *dr, *dc;        // degree-2 band factor (equilibrated)
   const int* ipiv;
-  double *mem, *dn, *scal, *f;
+  double *mem, *dn, *scal, *f, *fl;  // fl: element contributions [4][ne][4]
 };
 
-// channel_begin of both channels (src/vilma_rotation.f90:442-463): one thread
-// per (channel, re/im); the dissipative right-hand side in the reference's
+// channel_begin of both channels (src/vilma_rotation.f90:442-463): the
+// dissipative right-hand side of each (channel, re/im) in the reference's
 // element order (src/vilma_viscoelastic.f90:441-480), then the equilibrated
-// band solve (src/vilma_radial_fe.f90:578-605).
-// The block computes the element contributions of all four right-hand sides
-// in parallel (one thread per (channel, re/im, element); the FP64 divisions
-// there were the kernel's cost) and stages the degree-2 band factor and its
-// pivots in shared memory when they fit (rot_smem below); then one thread per
-// right-hand side assembles the nodal forcing in the reference's order (node
-// n: element n-1's second test dof, then element n's first) and runs the
-// sequential sweeps. The arithmetic and its order are the reference's either way.
-__global__ void k_rot_begin(RotArgs A, int staged) {
+// band solve (src/vilma_radial_fe.f90:578-605), in two kernels:
+//   k_rot_elem   one thread per (channel, re/im, element): the element's
+//                contributions to its four test dofs (two Gauss points, the
+//                FP64 divisions of the strain constants), into A.fl
+//   k_rot_begin  one block: the nodal forcing of the four right-hand sides
+//                (node n: element n-1's second test dof, then element n's
+//                first, as the serial loop adds them) times the row scales,
+//                the degree-2 band factor and its pivots staged in shared
+//                memory when they fit (rot_smem below), one thread per
+//                right-hand side for the sequential sweeps with their active
+//                window in registers (band_solve_window), then the column
+//                scales and the outputs.
+// The arithmetic and its order are the reference's throughout.
+constexpr int ROT_THREADS = 256;
+constexpr int ROT_ELEM_THREADS = 64;
+
+__global__ void __launch_bounds__(ROT_ELEM_THREADS) k_rot_elem(RotArgs A) {
+  const int w = blockIdx.x * blockDim.x + threadIdx.x;
+  const int ne = A.ne;
+  if (w >= 4 * ne) return;
+  const double xg = 0.5773502691896257;
+  const int q = w / ne, e = w % ne, ch = q >> 1, ri = q & 1;
+  const double* mem = A.mem + (size_t)ch * 6 * ne * 4;
+  const double* Am = mem + (size_t)(0 * 2 + ri) * ne * 4;
+  const double* Bm = mem + (size_t)(1 * 2 + ri) * ne * 4;
+  const double* Cm = mem + (size_t)(2 * 2 + ri) * ne * 4;
+  const double rk = A.r[e], rk1 = A.r[e + 1], h = rk1 - rk;
+  double floc[4] = {0.0, 0.0, 0.0, 0.0};
+  for (int ig = 0; ig < 2; ++ig) {
+    const double gp = ig == 0 ? -xg : xg;
+    const double ra = 0.5 * (h * gp + rk + rk1);
+    const double psik = (rk1 - ra) / h, psik1 = (ra - rk) / h;
+    double tauV[4];
+    for (int m = 0; m < 4; ++m) tauV[m] = Am[e * 4 + m] / h + Bm[e * 4 + m] * psik / ra + Cm[e * 4 + m] * psik1 / ra;
+    for (int tt = 0; tt < 4; ++tt) {
+      double D = 0.0;
+      for (int m = 0; m < 4; ++m) {
+        const double deps = A.sa[tt * 4 + m] / h + A.sb[tt * 4 + m] * psik / ra + A.sc[tt * 4 + m] * psik1 / ra;
+        D = D + A.nrm[m] * tauV[m] * deps;
+      }
+      floc[tt] = floc[tt] - D * ra * ra * h * 0.5;
+    }
+  }
+  for (int tt = 0; tt < 4; ++tt) A.fl[((size_t)q * ne + e) * 4 + tt] = floc[tt];
+}
+
+__global__ void __launch_bounds__(ROT_THREADS) k_rot_begin(RotArgs A, int staged) {
   extern __shared__ double rsm[];
   const int t = threadIdx.x;
   const int ne = A.ne, nr = A.nr, nd = A.nd;
-  double* sfl = rsm;  // [4][ne][4] element contributions
+  const double* sfl = A.fl;  // [4][ne][4] element contributions
   const double* ab = A.ab;
   const int* ipiv = A.ipiv;
   double* fbase = A.f;
   if (staged) {
-    double* sab = sfl + (size_t)16 * ne;                     // [nd][VG_LDAB]
+    double* sab = rsm;                                       // [nd][VG_LDAB]
     double* sf = sab + (size_t)nd * VG_LDAB;                 // [4][nd]
     int* sip = reinterpret_cast<int*>(sf + (size_t)4 * nd);  // [nd]
     for (int i = t; i < nd * VG_LDAB; i += blockDim.x) sab[i] = A.ab[i];
@@ -69,59 +107,37 @@ __global__ void k_rot_begin(RotArgs A, int staged) {
     ipiv = sip;
     fbase = sf;
   }
-  const double xg = 0.5773502691896257;
-  for (int w = t; w < 4 * ne; w += blockDim.x) {
-    const int q = w / ne, e = w % ne, ch = q >> 1, ri = q & 1;
-    const double* mem = A.mem + (size_t)ch * 6 * ne * 4;
-    const double* Am = mem + (size_t)(0 * 2 + ri) * ne * 4;
-    const double* Bm = mem + (size_t)(1 * 2 + ri) * ne * 4;
-    const double* Cm = mem + (size_t)(2 * 2 + ri) * ne * 4;
-    const double rk = A.r[e], rk1 = A.r[e + 1], h = rk1 - rk;
-    double floc[4] = {0.0, 0.0, 0.0, 0.0};
-    for (int ig = 0; ig < 2; ++ig) {
-      const double gp = ig == 0 ? -xg : xg;
-      const double ra = 0.5 * (h * gp + rk + rk1);
-      const double psik = (rk1 - ra) / h, psik1 = (ra - rk) / h;
-      double tauV[4];
-      for (int m = 0; m < 4; ++m) tauV[m] = Am[e * 4 + m] / h + Bm[e * 4 + m] * psik / ra + Cm[e * 4 + m] * psik1 / ra;
-      for (int tt = 0; tt < 4; ++tt) {
-        double D = 0.0;
-        for (int m = 0; m < 4; ++m) {
-          const double deps = A.sa[tt * 4 + m] / h + A.sb[tt * 4 + m] * psik / ra + A.sc[tt * 4 + m] * psik1 / ra;
-          D = D + A.nrm[m] * tauV[m] * deps;
-        }
-        floc[tt] = floc[tt] - D * ra * ra * h * 0.5;
-      }
+  __syncthreads();
+  // the nodal forcing of the four right-hand sides times the row scales
+  for (int w = t; w < 4 * nd; w += blockDim.x) {
+    const int q = w / nd, i = w % nd, n = i >> 2, c = i & 3;
+    const double* fl = sfl + (size_t)q * ne * 4;
+    double u = 0.0;
+    if (c < 2 && n < nr) {
+      if (n >= 1) u += fl[(n - 1) * 4 + (c == 0 ? 1 : 3)];
+      if (n < ne) u += fl[n * 4 + (c == 0 ? 0 : 2)];
     }
-    for (int tt = 0; tt < 4; ++tt) sfl[((size_t)q * ne + e) * 4 + tt] = floc[tt];
+    fbase[(size_t)q * nd + i] = A.dr[i] * u;
   }
   __syncthreads();
-  if (t >= 4) return;
-  const int ch = t >> 1, ri = t & 1;
-  double* f = fbase + (size_t)t * nd;
-  const double* fl = sfl + (size_t)t * ne * 4;
-  for (int i = 0; i < nd; ++i) f[i] = 0.0;
-  for (int n = 0; n < nr; ++n) {  // (0 + element n-1's share) + element n's share, as the serial loop adds them
-    double u = 0.0, v = 0.0;
-    if (n >= 1) {
-      u += fl[(n - 1) * 4 + 1];
-      v += fl[(n - 1) * 4 + 3];
-    }
-    if (n < ne) {
-      u += fl[n * 4 + 0];
-      v += fl[n * 4 + 2];
-    }
-    f[4 * n] = u;
-    f[4 * n + 1] = v;
+  if (t < 4) band_solve_window<6, 12>(ab, VG_LDAB, nd, ipiv, fbase + (size_t)t * nd);
+  __syncthreads();
+  for (int w = t; w < 4 * nd; w += blockDim.x) {
+    const int i = w % nd;
+    fbase[w] = A.dc[i] * fbase[w];
   }
-  for (int i = 0; i < nd; ++i) f[i] = A.dr[i] * f[i];
-  band_solve_strided(ab, VG_LDAB, nd, 6, 12, ipiv, f, 1);
-  for (int i = 0; i < nd; ++i) f[i] = A.dc[i] * f[i];
-  const int base = ch == 0 ? RS_DF_LOAD : RS_DF_TID;
-  A.scal[base + ri] = f[4 * (nr - 1) + 2];      // dF
-  A.scal[base + 2 + ri] = f[4 * (nr - 1)];      // dU
-  double* dn = A.dn + (size_t)ch * 4 * nr;
-  for (int node = 0; node < nr; ++node) {
+  __syncthreads();
+  if (t < 4) {
+    const int ch = t >> 1, ri = t & 1;
+    const double* f = fbase + (size_t)t * nd;
+    const int base = ch == 0 ? RS_DF_LOAD : RS_DF_TID;
+    A.scal[base + ri] = f[4 * (nr - 1) + 2];  // dF
+    A.scal[base + 2 + ri] = f[4 * (nr - 1)];  // dU
+  }
+  for (int w = t; w < 4 * nr; w += blockDim.x) {
+    const int q = w / nr, node = w % nr, ch = q >> 1, ri = q & 1;
+    const double* f = fbase + (size_t)q * nd;
+    double* dn = A.dn + (size_t)ch * 4 * nr;
     dn[(size_t)(0 + ri) * nr + node] = f[4 * node];      // dUn
     dn[(size_t)(2 + ri) * nr + node] = f[4 * node + 1];  // dVn
   }
@@ -279,6 +295,7 @@ static RotArgs rot_args(vg_handle* h) {
   A.dn = h->d_rot_dn.p;
   A.scal = h->d_rot_sc.p;
   A.f = h->d_rot_f.p;
+  A.fl = h->d_rot_fl.p;
   return A;
 }
 
@@ -303,6 +320,7 @@ void rotation_setup(vg_handle* h) {
   h->d_rot_dn.alloc((size_t)2 * 4 * nr);
   h->d_rot_sc.alloc(RS_N);
   h->d_rot_f.alloc((size_t)4 * nd);
+  h->d_rot_fl.alloc((size_t)16 * ne);
   h->d_rot_rows.alloc((size_t)2 * G.nlat);
   h->d_srot.alloc(G.ng);
   h->d_rot_load.alloc(G.ng);
@@ -343,21 +361,26 @@ void rotation_setup(vg_handle* h) {
 // (the element contributions always; the band, pivots and right-hand sides
 // when they fit; `staged` says which)
 static size_t rot_smem(const vg_handle* h, int& staged) {
-  const size_t fl = (size_t)16 * h->ne * sizeof(double);
-  const size_t b = fl + (size_t)h->ndof * VG_LDAB * sizeof(double) + (size_t)4 * h->ndof * sizeof(double) +
+  const size_t b = (size_t)h->ndof * VG_LDAB * sizeof(double) + (size_t)4 * h->ndof * sizeof(double) +
                    (size_t)h->ndof * sizeof(int);
   staged = b <= 200 * 1024 ? 1 : 0;
-  const size_t need = staged ? b : fl;
-  raise_smem_limit((const void*)k_rot_begin, need);
+  const size_t need = staged ? b : 0;
+  if (need > 48 * 1024) raise_smem_limit((const void*)k_rot_begin, need);
   return need;
+}
+
+// the drift of both channels from the entering memory
+static void rot_begin_launch(vg_handle* h, const RotArgs& A, size_t sm, int staged, cudaStream_t s) {
+  k_rot_elem<<<(4 * A.ne + ROT_ELEM_THREADS - 1) / ROT_ELEM_THREADS, ROT_ELEM_THREADS, 0, s>>>(A);
+  k_rot_begin<<<1, ROT_THREADS, sm, s>>>(A, staged);
+  h->n_launch += 2;
+  VG_CUDA(cudaGetLastError());
 }
 
 void rotation_begin(vg_handle* h) {
   int staged = 0;
   const size_t sm = rot_smem(h, staged);
-  k_rot_begin<<<1, 128, sm, h->stream>>>(rot_args(h), staged);
-  ++h->n_launch;
-  VG_CUDA(cudaGetLastError());
+  rot_begin_launch(h, rot_args(h), sm, staged, h->stream);
 }
 
 // the rotational sea-level term held across the interval
@@ -398,9 +421,9 @@ void rotation_advance(vg_handle* h, const double* d_sigma, double dt) {
   int staged = 0;
   const size_t sm = rot_smem(h, staged);
   for (int k = 0; k < n_sub; ++k) {
-    k_rot_begin<<<1, 128, sm, s>>>(A, staged);
+    rot_begin_launch(h, A, sm, staged, s);
     k_rot_solve_commit<<<1, 256, 0, s>>>(A, S);
-    h->n_launch += 2;
+    ++h->n_launch;
     VG_CUDA(cudaGetLastError());
   }
 }
