@@ -187,7 +187,7 @@ __device__ __forceinline__ double block_max(double v, double* red) {
 
 // dgbtrs-style solve with the factor of band_factor_dev (column-major band
 // storage, leading dimension ldab), right-hand side with element stride st
-__device__ __forceinline__ void band_solve_strided(const double* __restrict__ ab, int ldab, int n, int kl, int kv,
+__host__ __device__ __forceinline__ void band_solve_strided(const double* __restrict__ ab, int ldab, int n, int kl, int kv,
                                                    const int* __restrict__ ipiv, double* x, size_t st) {
 #define AB(row1, col1) ab[(size_t)((col1)-1) * ldab + ((row1)-1)]
   for (int j = 1; j <= n - 1; ++j) {
@@ -221,7 +221,7 @@ __device__ __forceinline__ void band_solve_strided(const double* __restrict__ ab
 // thread per right-hand side, whose sweeps are otherwise a chain of dependent
 // memory round trips.
 template <int KL, int KV>
-__device__ __forceinline__ void band_solve_window(const double* __restrict__ ab, int ldab, int n,
+__host__ __device__ __forceinline__ void band_solve_window(const double* __restrict__ ab, int ldab, int n,
                                                   const int* __restrict__ ipiv, double* __restrict__ x) {
   double w[KL + 1];  // w[i] = x[k + i]
 #pragma unroll
