@@ -30,7 +30,7 @@ double earth_moi(const Earth& e) {
   return I;
 }
 
-// vilma_earth_structure.f90 build_M3L70V01 (:220-238 of the survey numbering)
+// src/vilma_earth_structure.f90:220-238 build_M3L70V01 (Spada et al. 2011, Table 3)
 Earth build_M3L70V01() {
   const double km = 1e3;
   Earth e;
