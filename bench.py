@@ -65,6 +65,10 @@ def parse():
     ap.add_argument("--toroidal", default="on", choices=["on", "off", "only"],
                     help="also time the FP64 path carrying the toroidal channels (toroidal = 1); "
                          "only: time that path alone as the main arm")
+    ap.add_argument("--timeline", type=int, default=0, metavar="N",
+                    help="instead of the benchmark: the kernel timeline of N steps of the main arm after the warm-up "
+                         "(CUPTI kernel records through torch.profiler): per kernel its launches and device time a "
+                         "step, and the step's busy and idle device time")
     ap.add_argument("--grad-fwd", default="on", choices=["on", "off", "only"],
                     help="also time the adjoint gradients against their forwards (grad/fwd: the coupled step's, "
                          "100 intervals with checkpoints every 50, and the response-level one); 'only' prints those "
@@ -631,6 +635,59 @@ def run_ensemble(args):
     print(json.dumps(out))
 
 
+def run_timeline(args, w):
+    """Kernel timeline of args.timeline steps of the main arm (after the warm-up
+    and the autotuner), from the CUPTI kernel and copy records that
+    torch.profiler collects: per kernel its launches and device time a step,
+    the union of the busy intervals and the span. A profiling aid: nothing
+    here is a bench value."""
+    import collections
+
+    import torch
+    from torch.profiler import ProfilerActivity, profile
+
+    from fastearth3d_b200 import lib as vlib
+
+    prec = args.precision if w.visc3d else "fp64"
+    p = w.params(vlib.default_params)
+    p.visc3d_precision = PRECISION[prec]
+    m = vlib.Model(p)
+    m.set_reference(*w.reference())
+    if w.visc3d:
+        m.enable_visc3d(w.pert(m.p))
+    n = args.timeline
+    ice = torch.stack([torch.from_numpy(w.ice_at(s + 1)) for s in range(args.warmup + n)]).cuda()
+    for s in range(args.warmup):
+        m.update_device(ice[s].data_ptr(), w.dt_yr)
+    if prec == "exact_tc" and w.visc3d:
+        m.autotune(w.dt_yr, TUNE_CACHE)
+    torch.cuda.synchronize()
+    with profile(activities=[ProfilerActivity.CUDA]) as prof:
+        for s in range(args.warmup, args.warmup + n):
+            m.update_device(ice[s].data_ptr(), w.dt_yr)
+        torch.cuda.synchronize()
+    recs = sorted((e.time_range.start, e.time_range.end, e.name.split("(")[0])
+                  for e in prof.events() if e.device_type == torch.autograd.DeviceType.CUDA)
+    tot, cnt = collections.defaultdict(float), collections.Counter()
+    busy, cur_a, cur_b = 0.0, recs[0][0], recs[0][1]
+    for a, b, name in recs:
+        tot[name] += b - a
+        cnt[name] += 1
+        if a > cur_b:
+            busy += cur_b - cur_a
+            cur_a, cur_b = a, b
+        else:
+            cur_b = max(cur_b, b)
+    busy += cur_b - cur_a
+    span = recs[-1][1] - recs[0][0]
+    kernels = [{"name": k, "launches_per_step": cnt[k] / n, "us_per_step": round(v / n, 2),
+                "us_per_launch": round(v / cnt[k], 2), "share": round(v / sum(tot.values()), 4)}
+               for k, v in sorted(tot.items(), key=lambda x: -x[1])]
+    print(json.dumps({"workload": w.name, "precision": prec, "steps": n, "warmup": args.warmup,
+                      "span_ms_per_step": round(span / n / 1e3, 4), "busy_ms_per_step": round(busy / n / 1e3, 4),
+                      "records_per_step": len(recs) / n, "kernels": kernels}))
+
+
 def main():
     args = parse()
     if args.steps is None:
@@ -650,6 +707,12 @@ def main():
             run_reference(args, w)
         return
     import torch
+
+    if args.timeline > 0:
+        if rank == 0:
+            torch.cuda.set_device(local)
+            run_timeline(args, w)
+        return
 
     torch.cuda.set_device(local)
     if args.grad_fwd == "only":
