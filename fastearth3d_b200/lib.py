@@ -124,8 +124,9 @@ class Model:
 
     def __init__(self, p):
         self.p = p
+        self._L = lib()  # held by the instance, so that close() at interpreter exit needs no module global
         h = _VP()
-        rc = lib().vg_create(C.byref(p), C.byref(h))
+        rc = self._L.vg_create(C.byref(p), C.byref(h))
         if rc != 0:
             raise VilmaError(lib().vg_last_error(None).decode())
         self.h = h
@@ -134,8 +135,9 @@ class Model:
         self.ng = p.nphi * p.nlat
 
     def close(self):
-        if getattr(self, "h", None):
-            lib().vg_destroy(self.h)
+        L = getattr(self, "_L", None)
+        if getattr(self, "h", None) and L is not None:
+            L.vg_destroy(self.h)
             self.h = None
 
     __del__ = close
@@ -418,14 +420,16 @@ class Remap:
         self.lon = np.ascontiguousarray(lon_src, dtype=np.float64)
         self.lat = np.ascontiguousarray(lat_src, dtype=np.float64)
         r = _VP()
-        model._c(lib().vg_remap_create(model.h, ptr(self.lon), len(self.lon), ptr(self.lat), len(self.lat),
+        self._L = lib()
+        model._c(self._L.vg_remap_create(model.h, ptr(self.lon), len(self.lon), ptr(self.lat), len(self.lat),
                                        C.byref(r)))
         self.r = r
         self.shape = (len(self.lat), len(self.lon))
 
     def __del__(self):
-        if getattr(self, "r", None):
-            lib().vg_remap_destroy(self.r)
+        L = getattr(self, "_L", None)
+        if getattr(self, "r", None) and L is not None:
+            L.vg_remap_destroy(self.r)
             self.r = None
 
     def _c(self, rc):
