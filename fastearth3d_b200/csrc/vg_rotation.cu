@@ -10,8 +10,8 @@
 // only their right-hand sides differ (load_rhs / tidal_rhs,
 // src/vilma_radial_fe.f90:616-645). Per interval:
 //   begin   freeze both channels' drift from the entering memory (dF, dU,
-//           nodal strain drift), one thread per (channel, re/im): the
-//           dissipative right-hand side and a band solve
+//           nodal strain drift): the dissipative right-hand side of each
+//           (channel, re/im) and a band solve (k_rot_elem, k_rot_begin)
 //   s_rot   the rotational sea-level term N_rot - u_rot on the Gauss grid from
 //           the entering m, held across the interval and added in the
 //           sea-level equation
