@@ -52,3 +52,52 @@ def test_bad_arguments_return_status_not_abort():
     L = vlib.lib()
     assert L.vg_create(None, None) != 0
     assert b"null" in L.vg_last_error(None)
+
+
+C_PROGRAM = r"""
+#include <stddef.h>
+#include <stdio.h>
+#include "vilma_gpu.h"
+
+int main(void) {
+  vg_params p;
+  vg_handle* h = NULL;
+  if (vg_params_default(&p) != 0) return 2;
+  /* sizes and a few offsets for the ctypes mirror */
+  printf("%zu %zu %zu %zu %zu\n", sizeof(vg_params), sizeof(vg_info), offsetof(vg_params, toroidal),
+         offsetof(vg_params, sle_ctas), offsetof(vg_info, n_launch));
+  printf("%d %d\n", p.n_layer, p.deg1_cm);
+  /* a null argument is a status and a message, not an abort */
+  if (vg_create(NULL, &h) == 0) return 3;
+  printf("%s\n", vg_last_error(NULL));
+  return 0;
+}
+"""
+
+
+def test_header_is_plain_c_and_links(tmp_path):
+    """include/vilma_gpu.h compiles as C99 and a C program links against the
+    library (the drop-in boundary: no C++ or torch types); the struct sizes
+    and offsets a C caller sees are the ctypes mirror's."""
+    import shutil
+    import subprocess
+
+    cc = shutil.which("gcc") or shutil.which("cc")
+    if cc is None:
+        pytest.skip("no C compiler")
+    src = tmp_path / "abi_c.c"
+    src.write_text(C_PROGRAM)
+    exe = tmp_path / "abi_c"
+    libdir = os.path.dirname(vlib.LIB_PATH)
+    r = subprocess.run([cc, "-std=c99", "-Wall", "-Werror", "-I", os.path.dirname(HDR), str(src), "-o", str(exe),
+                        "-L", libdir, "-lvilma_gpu", "-Wl,-rpath," + libdir], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    run = subprocess.run([str(exe)], capture_output=True, text=True)
+    assert run.returncode == 0, run.stdout + run.stderr
+    lines = run.stdout.splitlines()
+    sp, si, o_tor, o_ctas, o_launch = map(int, lines[0].split())
+    assert sp == C.sizeof(VgParams) and si == C.sizeof(VgInfo)
+    assert o_tor == VgParams.toroidal.offset and o_ctas == VgParams.sle_ctas.offset
+    assert o_launch == VgInfo.n_launch.offset
+    assert lines[1] == "4 1"
+    assert "null" in lines[2]
