@@ -101,3 +101,18 @@ def test_header_is_plain_c_and_links(tmp_path):
     assert o_launch == VgInfo.n_launch.offset
     assert lines[1] == "4 1"
     assert "null" in lines[2]
+
+
+def test_library_exports_nothing_undeclared():
+    """Every vg_* symbol the library exports is declared in the header."""
+    import shutil
+    import subprocess
+
+    nm = shutil.which("nm")
+    if nm is None:
+        pytest.skip("no nm")
+    r = subprocess.run([nm, "-D", "--defined-only", vlib.LIB_PATH], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    exported = {ln.split()[-1] for ln in r.stdout.splitlines() if ln.split() and ln.split()[-1].startswith("vg_")}
+    assert exported, "no vg_ symbols exported"
+    assert exported <= set(declared()), sorted(exported - set(declared()))
