@@ -34,17 +34,17 @@ void sle_solve(SleSolver& sle, const Sht& s, Response& R, const double* d_ice, c
   res.n_outer_done = 0;
   res.n_coast_flip = 0;
   for (int i = 0; i < ng; ++i) ice_ref[i] = ice[i] - d_ice[i];
-  ocean_function(ng, topo0, ice_ref.data(), C0.data());
+  ocean_function(ng, topo0, ice_ref.data(), C0.data());  // the reference ocean, :212
   response_begin_step(R, s);
   if (!report_only) response_prepare_endpoint(R);
-  auto assemble_load = [&]() {
+  auto assemble_load = [&]() {  // assemble_load, :386-405
     for (int i = 0; i < ng; ++i) load[i] = RHO_ICE * d_ice_g[i] + RHO_WATER * (C[i] * rsl[i]) + wcorr[i];
   };
   const int n_mem = report_only ? 1 : sle.max_mem_iter;
   res.n_couple_done = 0;
-  for (int im = 1; im <= n_mem; ++im) {
-  for (int io = 1; io <= sle.n_outer; ++io) {
-    if (sle.fixed_ocean) {
+  for (int im = 1; im <= n_mem; ++im) {    // co-convergence, :230
+  for (int io = 1; io <= sle.n_outer; ++io) {  // coastline passes, :231-345
+    if (sle.fixed_ocean) {  // the ocean of this pass, :233-247
       if (io == 1)
         for (int i = 0; i < ng; ++i) C[i] = C0[i];
     } else if (io == 1) {
@@ -53,6 +53,7 @@ void sle_solve(SleSolver& sle, const Sht& s, Response& R, const double* d_ice, c
     } else {
       for (int i = 0; i < ng; ++i) C[i] = C_next[i];
     }
+    // grounded-ice increment and the pass's integrals, :249-294
     for (int i = 0; i < ng; ++i) d_ice_g[i] = ice[i] * (1.0 - C[i]) - (ice[i] - d_ice[i]) * (1.0 - C0[i]);
     C_int = sht_surface_integral(s, C);
     if (C_int <= 0.0) break;
@@ -67,7 +68,7 @@ void sle_solve(SleSolver& sle, const Sht& s, Response& R, const double* d_ice, c
       std::fill(wcorr.begin(), wcorr.end(), 0.0);
       zeta_int = 0.0;
     }
-    for (int ii = 1; ii <= sle.n_inner; ++ii) {
+    for (int ii = 1; ii <= sle.n_inner; ++ii) {  // the water-load fixed point, :296-318
       assemble_load();
       sht_analysis(s, load.data(), load_lm.data());
       response_apply(R, s, load_lm.data(), u_lm.data(), N_lm.data());
@@ -79,7 +80,7 @@ void sle_solve(SleSolver& sle, const Sht& s, Response& R, const double* d_ice, c
         tmp[i] = C[i] * Sraw[i];
       }
       Cs_int = sht_surface_integral(s, tmp.data());
-      dphi = (ice_int - Cs_int + zeta_int) / C_int;
+      dphi = (ice_int - Cs_int + zeta_int) / C_int;  // mass-conservation offset, :310
       double dmax = 0.0, smax = 0.0;
       for (int i = 0; i < ng; ++i) {
         rsl_new[i] = Sraw[i] + dphi;
@@ -91,12 +92,13 @@ void sle_solve(SleSolver& sle, const Sht& s, Response& R, const double* d_ice, c
       }
       res.n_inner_last = ii;
       res.resid = dmax;
-      if (dmax <= sle.tol * std::max(smax, 2.2250738585072014e-308)) break;
+      if (dmax <= sle.tol * std::max(smax, 2.2250738585072014e-308)) break;  // :317
     }
     res.n_outer_done = io;
     sle.n_outer_tot++;
     sle.n_inner_tot += res.n_inner_last;
     if (sle.fixed_ocean) break;
+    // the migrated coastline; C_next becomes C at the top of the next pass, :342-344
     for (int i = 0; i < ng; ++i) tmp[i] = topo0[i] - rsl[i];
     ocean_function(ng, tmp.data(), ice, C_next.data());
     int flips = 0;
@@ -104,6 +106,7 @@ void sle_solve(SleSolver& sle, const Sht& s, Response& R, const double* d_ice, c
     res.n_coast_flip = flips;
     if (flips == 0) break;
   }
+  // the closing load and the endpoint advance, :346-364
   assemble_load();
   sht_analysis(s, load.data(), load_lm.data());
   if (report_only) break;
@@ -114,6 +117,7 @@ void sle_solve(SleSolver& sle, const Sht& s, Response& R, const double* d_ice, c
   if (!report_only) response_finalize_step(R);
   if (sigma_out)
     for (int lm = 0; lm < nlm; ++lm) sigma_out[lm] = load_lm[lm];
+  // ocean-mass conservation check and the converged offset, :372-381
   for (int i = 0; i < ng; ++i) tmp[i] = C[i] * rsl[i];
   Cs_int = sht_surface_integral(s, tmp.data()) - zeta_int;
   res.ocean_frac = C_int / (16.0 * std::atan(1.0));
