@@ -116,3 +116,32 @@ def test_library_exports_nothing_undeclared():
     exported = {ln.split()[-1] for ln in r.stdout.splitlines() if ln.split() and ln.split()[-1].startswith("vg_")}
     assert exported, "no vg_ symbols exported"
     assert exported <= set(declared()), sorted(exported - set(declared()))
+
+
+def test_fortran_binding_matches_header():
+    """The iso_c_binding module INTEGRATION.md gives a maintainer binds
+    header functions by their C names with the C argument count, and every
+    header entry point a Fortran host can use is bound."""
+    root = os.path.dirname(HDR)
+    txt = open(os.path.join(os.path.dirname(root), "INTEGRATION.md")).read()
+    mod = txt[txt.index("module vilma_gpu"): txt.index("end module vilma_gpu")]
+    hdr = open(HDR).read()
+    c_args = {}
+    for name, args in re.findall(r"^(?:int|const char\*)\s+(vg_[a-z0-9_]+)\s*\(([^)]*)\)\s*;", hdr, re.M):
+        a = args.strip()
+        c_args[name] = 0 if a in ("", "void") else a.count(",") + 1
+    f_sigs = re.findall(r"function\s+(vg_[a-z0-9_]+)\s*\(([^)]*)\)\s*&?\s*(?:bind\(c,\s*name=\"(vg_[a-z0-9_]+)\"\))?",
+                        mod.replace("&\n", " "))
+    bound = {}
+    for fname, args, cname in f_sigs:
+        if fname in ("vg_check",):
+            continue
+        n = len([x for x in args.replace("&", " ").split(",") if x.strip()])
+        bound[cname or fname] = n
+    assert bound, "no bound functions found"
+    for name, n in bound.items():
+        assert name in c_args, name
+        assert n == c_args[name], (name, n, c_args[name])
+    device_only = {"vg_update_device", "vg_rsl_device", "vg_stream", "vg_sht_analysis_noalloc", "vg_profile_enable",
+                   "vg_profile_read"}
+    assert set(c_args) - device_only <= set(bound), sorted(set(c_args) - device_only - set(bound))
